@@ -1,0 +1,142 @@
+// bp_internal.h -- device-resident graph shared by the engine's .cu files.
+//
+// HBM layout (one graph, S_max states, "position" = index in the
+// destination-sorted edge order, i.e. the reference's dest_nodes_to_edges
+// order, graph.c:285-313):
+//
+//   in_ptr   u32 [V+1]        row starts of each node's in-edges
+//   in_src   u32 [E]          source node of the edge at position p
+//   pos_edge u32 [E]          edge id at position p      (dest_nodes_to_edges_edge_list)
+//   edge_pos u32 [E]          position of edge id e
+//   pos_dims u8  [E]          x | y<<4 (source / destination state count); mixed graphs only
+//   node_s   u8  [V]          state count per node; mixed graphs only
+//   joint    f32 [E][MS][MS]  joint tables in position order, zero padded
+//   belief   f32 [V][MS]      beliefs, zero beyond S_v
+//   msg[2]   f32 [E][MS]      the two message arrays (struct graph's
+//                             edges_messages / last_edges_messages), position order
+//   q[2]     f32 [V][MS]      send buffers of the fused flooding schedule
+//
+// Messages are stored by destination so a node's incoming messages are one
+// contiguous run: the gather needs no atomics and reads whole sectors.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "bp.h"
+
+namespace bpx {
+
+constexpr int kMaxStates = BP_MAX_STATES;
+
+// Control block of one loopy run, resident in device memory.  Kernels read it
+// at entry (iteration index, buffer parities, stop flag) and the last block
+// of each iteration updates it, so a CUDA graph of identical launches can run
+// the whole loop with the reference's stopping rule evaluated on the device.
+struct LoopyCtl {
+    uint32_t it;           // iterations executed so far in this run
+    uint32_t done;         // 0 running, 1 stopping rule fired, 2 ran out of iterations
+    uint32_t ret;          // the reference's return value
+    uint32_t counter;      // last-block-done ticket
+    uint32_t num_iter;     // _acc variants: completed batches * check_every
+    uint32_t final_i;      // the reference's loop variable at exit
+    uint32_t max_it;
+    uint32_t check_every;
+    uint32_t msg_parity0;  // slot holding the latest messages when the run started
+    uint32_t q_parity0;
+    uint32_t serial;       // 1 = serial fp32 delta kernel decides
+    uint32_t acc_edge;     // edge schedule, _acc variant
+    float tol;
+    float delta_f, prev_f;
+    uint32_t pad0;
+    double delta_d, prev_d;
+};
+
+struct TreeData {
+    bool ready = false;
+    uint32_t num_levels = 0;
+    uint32_t *levels_host = nullptr;   // copy of the level lists (2V)
+    // per node: level and index within level (host + device)
+    uint32_t *d_node_level = nullptr, *d_node_lidx = nullptr;
+    // waves: nodes of each (level, wave) contiguous
+    uint32_t *d_wave_nodes = nullptr;
+    uint32_t *wave_off = nullptr;      // host [num_waves_total + 1]
+    uint32_t *level_wave_begin = nullptr; // host [num_levels + 1] index into waves
+    uint32_t total_waves = 0;
+};
+
+}  // namespace bpx
+
+struct bp_graph {
+    uint32_t V = 0, E = 0;
+    uint32_t ms = 1;         // storage stride = max state count
+    uint32_t uniform = 0;    // common state count, or 0 when mixed
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+
+    uint32_t *in_ptr = nullptr, *in_src = nullptr, *pos_edge = nullptr, *edge_pos = nullptr;
+    uint8_t *pos_dims = nullptr, *node_s = nullptr;
+    float *joint = nullptr;
+    float *belief = nullptr;
+    float *msg[2] = {nullptr, nullptr};
+    float *q[2] = {nullptr, nullptr};
+    int latest = 0;
+
+    // src-CSR, built on first use (tree schedule)
+    uint32_t *out_ptr = nullptr, *out_pos = nullptr, *out_dst = nullptr, *pos_dst = nullptr;
+
+    // scratch
+    double *partials = nullptr;
+    uint32_t partials_cap = 0;
+    float *absdiff = nullptr;
+    bpx::LoopyCtl *ctl = nullptr;
+    bpx::LoopyCtl *ctl_host = nullptr;   // pinned
+    uint8_t *visited = nullptr;
+    float *staging = nullptr;
+    size_t staging_bytes = 0;
+
+    // host-side copies of small structure arrays (tree waves, edge-variant runs)
+    uint8_t *node_s_host = nullptr;      // [V] state counts
+    uint32_t *in_ptr_host = nullptr;     // [V+1], on demand
+    uint32_t *run_len = nullptr;         // [nruns] runs of equal state count (device)
+    uint8_t *run_s = nullptr;
+    uint32_t nruns = 0;
+
+    bpx::TreeData tree;
+
+    // cached CUDA graphs of the iteration loop
+    struct CachedGraph {
+        cudaGraphExec_t exec = nullptr;
+        uint64_t key = 0;
+    } loop_graph[4];
+
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    uint64_t device_bytes = 0;
+};
+
+namespace bpx {
+
+// error plumbing (engine.cu)
+int set_error(int status, const char *fmt, ...);
+int cuda_fail(cudaError_t e, const char *what, const char *file, int line);
+
+#define BP_CUDA(call)                                                      \
+    do {                                                                   \
+        cudaError_t e_ = (call);                                           \
+        if (e_ != cudaSuccess) return bpx::cuda_fail(e_, #call, __FILE__, __LINE__); \
+    } while (0)
+
+int dev_alloc(bp_graph *g, void **p, size_t bytes);
+int ensure_staging(bp_graph *g, size_t bytes);
+int ensure_out_csr(bp_graph *g);
+int ensure_host_in_ptr(bp_graph *g);
+
+inline unsigned grid_for(uint64_t n, unsigned block) {
+    uint64_t b = (n + block - 1) / block;
+    if (b == 0) b = 1;
+    if (b > 0x7fffffffull) b = 0x7fffffffull;
+    return (unsigned)b;
+}
+
+}  // namespace bpx

@@ -1,0 +1,693 @@
+// engine.cu -- device graph construction, state transfer, error plumbing.
+//
+// bp_graph_create turns an edge list in insertion order into the
+// destination-sorted layout described in bp_internal.h.  The sort is a
+// stable LSD radix sort by destination, so within a node the in-edges keep
+// insertion order -- exactly the order of the reference's dest-CSR
+// (graph.c:285-313) -- unless the caller passes that CSR explicitly.
+#include <cub/device/device_radix_sort.cuh>
+
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "bp_device.cuh"
+#include "bp_internal.h"
+
+namespace bpx {
+
+static thread_local char g_last_error[512] = "";
+
+int set_error(int status, const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_last_error, sizeof(g_last_error), fmt, ap);
+    va_end(ap);
+    return status;
+}
+
+int cuda_fail(cudaError_t e, const char *what, const char *file, int line) {
+    int st = (e == cudaErrorMemoryAllocation) ? BP_ERR_NOMEM
+           : (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) ? BP_ERR_NO_DEVICE
+           : BP_ERR_CUDA;
+    return set_error(st, "%s failed: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
+}
+
+int dev_alloc(bp_graph *g, void **p, size_t bytes) {
+    *p = nullptr;
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return cuda_fail(e, "cudaMalloc", __FILE__, __LINE__);
+    }
+    g->device_bytes += bytes;
+    return BP_OK;
+}
+
+int ensure_staging(bp_graph *g, size_t bytes) {
+    if (g->staging_bytes >= bytes) return BP_OK;
+    if (g->staging) {
+        cudaFree(g->staging);
+        g->device_bytes -= g->staging_bytes;
+        g->staging = nullptr;
+        g->staging_bytes = 0;
+    }
+    int st = dev_alloc(g, (void **)&g->staging, bytes);
+    if (st == BP_OK) g->staging_bytes = bytes;
+    return st;
+}
+
+// ---------------------------------------------------------------- kernels --
+
+// in_ptr from destination keys sorted ascending: in_ptr[v] = first position
+// whose key >= v
+__global__ void k_fill_ptr_from_sorted(const uint32_t *__restrict__ keys, uint32_t E, uint32_t V,
+                                       uint32_t *__restrict__ ptr) {
+    uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p > E) return;
+    uint32_t lo = (p == 0) ? 0u : keys[p - 1] + 1u;       // first node starting here
+    uint32_t hi = (p == E) ? V : keys[p];                  // last node starting here
+    for (uint32_t v = lo; v <= hi && v <= V; ++v) {
+        ptr[v] = (uint32_t)p;
+        if (v == 0xffffffffu) break;
+    }
+}
+
+// node_list (V entries, struct graph layout) -> ptr[V+1]
+__global__ void k_ptr_from_node_list(const uint32_t *__restrict__ nl, uint32_t V, uint32_t E,
+                                     uint32_t *__restrict__ ptr) {
+    uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v < V) ptr[v] = nl[v];
+    if (v == V) ptr[V] = E;
+}
+
+__global__ void k_positions(const uint32_t *__restrict__ pos_edge, const uint32_t *__restrict__ src,
+                            const uint32_t *__restrict__ dst, uint32_t E,
+                            const uint8_t *__restrict__ node_s, uint32_t *__restrict__ in_src,
+                            uint32_t *__restrict__ edge_pos, uint8_t *__restrict__ pos_dims) {
+    uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= E) return;
+    uint32_t e = pos_edge[p];
+    uint32_t s = src[e];
+    in_src[p] = s;
+    edge_pos[e] = (uint32_t)p;
+    if (pos_dims) pos_dims[p] = (uint8_t)(node_s[s] | (node_s[dst[e]] << 4));
+}
+
+__global__ void k_states_u8(const uint32_t *__restrict__ s32, uint32_t V, uint32_t uniform,
+                            uint8_t *__restrict__ s8) {
+    uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v < V) s8[v] = (uint8_t)(s32 ? s32[v] : uniform);
+}
+
+// joint tables, edge-id order with caller strides -> position order [MS][MS]
+template <int MS>
+__global__ void k_gather_joint(const float *__restrict__ jin, uint32_t rs, uint64_t es,
+                               const uint32_t *__restrict__ pos_edge, const uint32_t *__restrict__ in_src,
+                               const uint32_t *__restrict__ dst_of_edge, const uint8_t *__restrict__ node_s,
+                               uint32_t uniform, uint32_t E, float *__restrict__ jout) {
+    uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t p = t / (MS * MS);
+    if (p >= E) return;
+    int k = (int)(t % (MS * MS));
+    int i = k / MS, j = k % MS;
+    uint32_t e = pos_edge[p];
+    int x = uniform ? (int)uniform : node_s[in_src[p]];
+    int y = uniform ? (int)uniform : node_s[dst_of_edge[e]];
+    float v = 0.0f;
+    if (i < x && j < y) v = jin[(uint64_t)e * es + (uint64_t)i * rs + j];
+    jout[p * (MS * MS) + k] = v;
+}
+
+// beliefs [V][ld] <-> [V][MS] (zero beyond S_v)
+__global__ void k_beliefs_in(const float *__restrict__ in, uint32_t ld, uint32_t V, uint32_t ms,
+                             const uint8_t *__restrict__ node_s, uint32_t uniform, float *__restrict__ b) {
+    uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t v = t / ms;
+    if (v >= V) return;
+    uint32_t i = (uint32_t)(t % ms);
+    uint32_t s = uniform ? uniform : node_s[v];
+    b[t] = (i < s) ? in[v * ld + i] : 0.0f;
+}
+
+__global__ void k_beliefs_out(const float *__restrict__ b, uint32_t ld, uint32_t V, uint32_t ms,
+                              const uint8_t *__restrict__ node_s, uint32_t uniform, float *__restrict__ out) {
+    uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t v = t / ms;
+    if (v >= V) return;
+    uint32_t i = (uint32_t)(t % ms);
+    uint32_t s = uniform ? uniform : node_s[v];
+    if (i < ld && i < s) out[v * ld + i] = b[t];
+}
+
+// messages [E][ld] edge-id order <-> [E][MS] position order (zero beyond x)
+__global__ void k_messages_in(const float *__restrict__ in, uint32_t ld, uint32_t E, uint32_t ms,
+                              const uint32_t *__restrict__ pos_edge, const uint32_t *__restrict__ in_src,
+                              const uint8_t *__restrict__ node_s, uint32_t uniform, float *__restrict__ m) {
+    uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t p = t / ms;
+    if (p >= E) return;
+    uint32_t i = (uint32_t)(t % ms);
+    uint32_t x = uniform ? uniform : node_s[in_src[p]];
+    uint32_t e = pos_edge[p];
+    m[t] = (i < x && i < ld) ? in[(uint64_t)e * ld + i] : 0.0f;
+}
+
+__global__ void k_messages_out(const float *__restrict__ m, uint32_t ld, uint32_t E, uint32_t ms,
+                               const uint32_t *__restrict__ pos_edge, const uint32_t *__restrict__ in_src,
+                               const uint8_t *__restrict__ node_s, uint32_t uniform, float *__restrict__ out) {
+    uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t p = t / ms;
+    if (p >= E) return;
+    uint32_t i = (uint32_t)(t % ms);
+    uint32_t x = uniform ? uniform : node_s[in_src[p]];
+    uint32_t e = pos_edge[p];
+    if (i < x && i < ld) out[(uint64_t)e * ld + i] = m[t];
+}
+
+__global__ void k_validate_edges(const uint32_t *__restrict__ src, const uint32_t *__restrict__ dst,
+                                 uint32_t E, uint32_t V, uint32_t *__restrict__ bad) {
+    uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < E && (src[e] >= V || dst[e] >= V)) atomicOr(bad, 1u);
+}
+
+__global__ void k_iota(uint32_t *__restrict__ a, uint32_t n) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = (uint32_t)i;
+}
+
+// position -> destination node
+__global__ void k_pos_dst(const uint32_t *__restrict__ ptr, uint32_t V, uint32_t *__restrict__ pos_dst) {
+    uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= V) return;
+    for (uint32_t p = ptr[v]; p < ptr[v + 1]; ++p) pos_dst[p] = (uint32_t)v;
+}
+
+__global__ void k_src_of_edges(const uint32_t *__restrict__ edge_pos, const uint32_t *__restrict__ in_src,
+                               uint32_t E, uint32_t *__restrict__ src_e, uint32_t *__restrict__ iota) {
+    uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= E) return;
+    src_e[e] = in_src[edge_pos[e]];
+    iota[e] = (uint32_t)e;
+}
+
+__global__ void k_out_arrays(const uint32_t *__restrict__ out_edges, const uint32_t *__restrict__ edge_pos,
+                             const uint32_t *__restrict__ pos_dst, uint32_t E, uint32_t *__restrict__ out_pos,
+                             uint32_t *__restrict__ out_dst) {
+    uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= E) return;
+    uint32_t p = edge_pos[out_edges[q]];
+    out_pos[q] = p;
+    out_dst[q] = pos_dst[p];
+}
+
+static int bits_for(uint32_t n) {
+    int b = 1;
+    while (b < 32 && (1ull << b) < (uint64_t)n) ++b;
+    return b;
+}
+
+// stable sort of (key, value) pairs by key, device memory
+static int radix_sort_pairs(bp_graph *g, const uint32_t *keys_in, uint32_t *keys_out,
+                            const uint32_t *vals_in, uint32_t *vals_out, uint32_t n, uint32_t key_range) {
+    if (n == 0) return BP_OK;
+    size_t temp = 0;
+    int end_bit = bits_for(key_range + 1);
+    BP_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp, keys_in, keys_out, vals_in, vals_out, (int64_t)n, 0,
+                                            end_bit, g->stream));
+    void *tmp = nullptr;
+    BP_CUDA(cudaMallocAsync(&tmp, temp, g->stream));
+    cudaError_t e = cub::DeviceRadixSort::SortPairs(tmp, temp, keys_in, keys_out, vals_in, vals_out, (int64_t)n, 0,
+                                                    end_bit, g->stream);
+    cudaFreeAsync(tmp, g->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "DeviceRadixSort::SortPairs", __FILE__, __LINE__);
+    return BP_OK;
+}
+
+template <int MS, bool UNI>
+static int launch_gather_joint(bp_graph *g, const float *jin, uint32_t rs, uint64_t es, const uint32_t *dst_e) {
+    uint64_t n = (uint64_t)g->E * MS * MS;
+    if (n == 0) return BP_OK;
+    k_gather_joint<MS><<<grid_for(n, 256), 256, 0, g->stream>>>(jin, rs, es, g->pos_edge, g->in_src, dst_e,
+                                                                 g->node_s, g->uniform, g->E, g->joint);
+    BP_CUDA(cudaGetLastError());
+    return BP_OK;
+}
+
+static int gather_joint(bp_graph *g, const float *jin, uint32_t rs, uint64_t es, const uint32_t *dst_e) {
+    BP_DISPATCH_MS(g->ms, true, launch_gather_joint, g, jin, rs, es, dst_e);
+}
+
+// copy a host or device array to a device buffer that this call owns
+static int to_device(bp_graph *g, const void *src, size_t bytes, int memory, void **dev, bool *owned) {
+    if (memory == BP_MEM_DEVICE) {
+        *dev = const_cast<void *>(src);
+        *owned = false;
+        return BP_OK;
+    }
+    BP_CUDA(cudaMallocAsync(dev, bytes ? bytes : 16, g->stream));
+    *owned = true;
+    if (bytes) BP_CUDA(cudaMemcpyAsync(*dev, src, bytes, cudaMemcpyHostToDevice, g->stream));
+    return BP_OK;
+}
+
+int ensure_host_in_ptr(bp_graph *g) {
+    if (g->in_ptr_host) return BP_OK;
+    g->in_ptr_host = (uint32_t *)malloc(sizeof(uint32_t) * ((size_t)g->V + 1));
+    if (!g->in_ptr_host) return set_error(BP_ERR_NOMEM, "host allocation failed");
+    BP_CUDA(cudaMemcpyAsync(g->in_ptr_host, g->in_ptr, sizeof(uint32_t) * ((size_t)g->V + 1),
+                            cudaMemcpyDeviceToHost, g->stream));
+    BP_CUDA(cudaStreamSynchronize(g->stream));
+    return BP_OK;
+}
+
+// src-sorted CSR for the tree schedule: out-edges of a node in insertion
+// order (graph.c:249-283), as positions and destination nodes
+int ensure_out_csr(bp_graph *g) {
+    if (g->out_ptr) return BP_OK;
+    int st;
+    uint32_t E = g->E, V = g->V;
+    if ((st = dev_alloc(g, (void **)&g->out_ptr, sizeof(uint32_t) * ((size_t)V + 1)))) return st;
+    if ((st = dev_alloc(g, (void **)&g->out_pos, sizeof(uint32_t) * (size_t)E))) return st;
+    if ((st = dev_alloc(g, (void **)&g->out_dst, sizeof(uint32_t) * (size_t)E))) return st;
+    if ((st = dev_alloc(g, (void **)&g->pos_dst, sizeof(uint32_t) * (size_t)E))) return st;
+    k_pos_dst<<<grid_for(V, 256), 256, 0, g->stream>>>(g->in_ptr, V, g->pos_dst);
+    BP_CUDA(cudaGetLastError());
+    uint32_t *src_e = nullptr, *iota = nullptr, *keys = nullptr, *order = nullptr;
+    BP_CUDA(cudaMallocAsync((void **)&src_e, sizeof(uint32_t) * (E ? E : 1), g->stream));
+    BP_CUDA(cudaMallocAsync((void **)&iota, sizeof(uint32_t) * (E ? E : 1), g->stream));
+    BP_CUDA(cudaMallocAsync((void **)&keys, sizeof(uint32_t) * (E ? E : 1), g->stream));
+    BP_CUDA(cudaMallocAsync((void **)&order, sizeof(uint32_t) * (E ? E : 1), g->stream));
+    if (E) {
+        k_src_of_edges<<<grid_for(E, 256), 256, 0, g->stream>>>(g->edge_pos, g->in_src, E, src_e, iota);
+        BP_CUDA(cudaGetLastError());
+    }
+    if ((st = radix_sort_pairs(g, src_e, keys, iota, order, E, V))) return st;
+    k_fill_ptr_from_sorted<<<grid_for((uint64_t)E + 1, 256), 256, 0, g->stream>>>(keys, E, V, g->out_ptr);
+    BP_CUDA(cudaGetLastError());
+    if (E) {
+        k_out_arrays<<<grid_for(E, 256), 256, 0, g->stream>>>(order, g->edge_pos, g->pos_dst, E, g->out_pos,
+                                                              g->out_dst);
+        BP_CUDA(cudaGetLastError());
+    }
+    cudaFreeAsync(src_e, g->stream);
+    cudaFreeAsync(iota, g->stream);
+    cudaFreeAsync(keys, g->stream);
+    cudaFreeAsync(order, g->stream);
+    BP_CUDA(cudaStreamSynchronize(g->stream));
+    return BP_OK;
+}
+
+static void free_graph(bp_graph *g) {
+    if (!g) return;
+    void *ptrs[] = {g->in_ptr, g->in_src, g->pos_edge, g->edge_pos, g->pos_dims, g->node_s, g->joint,
+                    g->belief, g->msg[0], g->msg[1], g->q[0], g->q[1], g->out_ptr, g->out_pos,
+                    g->out_dst, g->pos_dst, g->partials, g->absdiff, g->ctl, g->visited, g->staging,
+                    g->run_len, g->run_s, g->tree.d_node_level, g->tree.d_node_lidx, g->tree.d_wave_nodes};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    for (auto &c : g->loop_graph)
+        if (c.exec) cudaGraphExecDestroy(c.exec);
+    if (g->ctl_host) cudaFreeHost(g->ctl_host);
+    if (g->ev0) cudaEventDestroy(g->ev0);
+    if (g->ev1) cudaEventDestroy(g->ev1);
+    if (g->own_stream && g->stream) cudaStreamDestroy(g->stream);
+    free(g->node_s_host);
+    free(g->in_ptr_host);
+    free(g->tree.levels_host);
+    free(g->tree.wave_off);
+    free(g->tree.level_wave_begin);
+    delete g;
+}
+
+static int create_impl(bp_graph *g, const bp_graph_desc *d) {
+    const uint32_t V = d->num_nodes, E = d->num_edges;
+    int st;
+    // ---- state counts (validated on the host when they are host memory)
+    std::vector<uint32_t> s32;
+    const uint32_t *states = d->node_num_states;
+    uint32_t smax = 0, smin = 0xffffffffu;
+    if (!states) {
+        if (d->uniform_states < 1 || d->uniform_states > BP_MAX_STATES)
+            return set_error(BP_ERR_SHAPE, "uniform_states %u not in [1, %d]", d->uniform_states, BP_MAX_STATES);
+        smax = smin = d->uniform_states;
+    } else {
+        if (d->memory == BP_MEM_DEVICE) {
+            s32.resize(V);
+            if (V) BP_CUDA(cudaMemcpy(s32.data(), states, sizeof(uint32_t) * V, cudaMemcpyDeviceToHost));
+            states = s32.data();
+        }
+        for (uint32_t v = 0; v < V; ++v) {
+            if (states[v] < 1 || states[v] > BP_MAX_STATES)
+                return set_error(BP_ERR_SHAPE, "node %u has %u states (must be 1..%d)", v, states[v], BP_MAX_STATES);
+            smax = std::max(smax, states[v]);
+            smin = std::min(smin, states[v]);
+        }
+        if (V == 0) smax = smin = 1;
+    }
+    g->ms = smax;
+    g->uniform = (smax == smin) ? smax : 0;
+    g->node_s_host = (uint8_t *)malloc(V ? V : 1);
+    for (uint32_t v = 0; v < V; ++v) g->node_s_host[v] = (uint8_t)(states ? states[v] : d->uniform_states);
+
+    // ---- device arrays
+    const size_t ms = g->ms;
+    if ((st = dev_alloc(g, (void **)&g->in_ptr, sizeof(uint32_t) * ((size_t)V + 1)))) return st;
+    if ((st = dev_alloc(g, (void **)&g->in_src, sizeof(uint32_t) * (size_t)E))) return st;
+    if ((st = dev_alloc(g, (void **)&g->pos_edge, sizeof(uint32_t) * (size_t)E))) return st;
+    if ((st = dev_alloc(g, (void **)&g->edge_pos, sizeof(uint32_t) * (size_t)E))) return st;
+    if ((st = dev_alloc(g, (void **)&g->node_s, (size_t)V))) return st;
+    if (!g->uniform && (st = dev_alloc(g, (void **)&g->pos_dims, (size_t)E))) return st;
+    if ((st = dev_alloc(g, (void **)&g->joint, sizeof(float) * ms * ms * (size_t)E))) return st;
+    if ((st = dev_alloc(g, (void **)&g->belief, sizeof(float) * ms * (size_t)V))) return st;
+    for (int k = 0; k < 2; ++k) {
+        if ((st = dev_alloc(g, (void **)&g->msg[k], sizeof(float) * ms * (size_t)E))) return st;
+        if ((st = dev_alloc(g, (void **)&g->q[k], sizeof(float) * ms * (size_t)V))) return st;
+        BP_CUDA(cudaMemsetAsync(g->msg[k], 0, sizeof(float) * ms * (size_t)E, g->stream));
+        BP_CUDA(cudaMemsetAsync(g->q[k], 0, sizeof(float) * ms * (size_t)V, g->stream));
+    }
+    BP_CUDA(cudaMemsetAsync(g->belief, 0, sizeof(float) * ms * (size_t)V, g->stream));
+    if ((st = dev_alloc(g, (void **)&g->ctl, sizeof(bpx::LoopyCtl)))) return st;
+    BP_CUDA(cudaMallocHost((void **)&g->ctl_host, sizeof(bpx::LoopyCtl)));
+    if ((st = dev_alloc(g, (void **)&g->visited, (size_t)V))) return st;
+    BP_CUDA(cudaMemsetAsync(g->visited, 0, (size_t)V, g->stream));
+
+    // state counts -> u8
+    {
+        void *s_dev = nullptr;
+        bool owned = false;
+        if (d->node_num_states) {
+            if ((st = to_device(g, d->node_num_states, sizeof(uint32_t) * V, d->memory, &s_dev, &owned))) return st;
+        }
+        if (V) {
+            k_states_u8<<<grid_for(V, 256), 256, 0, g->stream>>>((const uint32_t *)s_dev, V, d->uniform_states,
+                                                                g->node_s);
+            BP_CUDA(cudaGetLastError());
+        }
+        if (owned) cudaFreeAsync(s_dev, g->stream);
+    }
+
+    // ---- edges
+    void *src = nullptr, *dst = nullptr;
+    bool own_src = false, own_dst = false;
+    if ((st = to_device(g, d->edge_src, sizeof(uint32_t) * (size_t)E, d->memory, &src, &own_src))) return st;
+    if ((st = to_device(g, d->edge_dst, sizeof(uint32_t) * (size_t)E, d->memory, &dst, &own_dst))) return st;
+    if (E) {
+        uint32_t *bad = nullptr;
+        BP_CUDA(cudaMallocAsync((void **)&bad, sizeof(uint32_t), g->stream));
+        BP_CUDA(cudaMemsetAsync(bad, 0, sizeof(uint32_t), g->stream));
+        k_validate_edges<<<grid_for(E, 256), 256, 0, g->stream>>>((const uint32_t *)src, (const uint32_t *)dst, E,
+                                                                  V, bad);
+        BP_CUDA(cudaGetLastError());
+        uint32_t hbad = 0;
+        BP_CUDA(cudaMemcpyAsync(&hbad, bad, sizeof(uint32_t), cudaMemcpyDeviceToHost, g->stream));
+        BP_CUDA(cudaStreamSynchronize(g->stream));
+        cudaFreeAsync(bad, g->stream);
+        if (hbad) {
+            if (own_src) cudaFreeAsync(src, g->stream);
+            if (own_dst) cudaFreeAsync(dst, g->stream);
+            return set_error(BP_ERR_INVALID, "an edge endpoint is >= num_nodes (%u)", V);
+        }
+    }
+
+
+    if (d->dest_node_list && d->dest_edge_list) {
+        // the caller's dest-CSR (struct graph's dest_nodes_to_edges_*)
+        void *nl = nullptr, *el = nullptr;
+        bool own_nl = false, own_el = false;
+        if ((st = to_device(g, d->dest_node_list, sizeof(uint32_t) * V, d->memory, &nl, &own_nl))) return st;
+        if ((st = to_device(g, d->dest_edge_list, sizeof(uint32_t) * (size_t)E, d->memory, &el, &own_el))) return st;
+        k_ptr_from_node_list<<<grid_for((uint64_t)V + 1, 256), 256, 0, g->stream>>>((const uint32_t *)nl, V, E,
+                                                                                     g->in_ptr);
+        BP_CUDA(cudaGetLastError());
+        if (E) BP_CUDA(cudaMemcpyAsync(g->pos_edge, el, sizeof(uint32_t) * (size_t)E, cudaMemcpyDeviceToDevice,
+                                       g->stream));
+        if (own_nl) cudaFreeAsync(nl, g->stream);
+        if (own_el) cudaFreeAsync(el, g->stream);
+    } else {
+        // stable sort of edge ids by destination
+        uint32_t *iota = nullptr, *keys = nullptr;
+        BP_CUDA(cudaMallocAsync((void **)&iota, sizeof(uint32_t) * (E ? E : 1), g->stream));
+        BP_CUDA(cudaMallocAsync((void **)&keys, sizeof(uint32_t) * (E ? E : 1), g->stream));
+        if (E) {
+            k_iota<<<grid_for(E, 256), 256, 0, g->stream>>>(iota, E);
+            BP_CUDA(cudaGetLastError());
+        }
+        if ((st = radix_sort_pairs(g, (const uint32_t *)dst, keys, iota, g->pos_edge, E, V))) return st;
+        k_fill_ptr_from_sorted<<<grid_for((uint64_t)E + 1, 256), 256, 0, g->stream>>>(keys, E, V, g->in_ptr);
+        BP_CUDA(cudaGetLastError());
+        cudaFreeAsync(iota, g->stream);
+        cudaFreeAsync(keys, g->stream);
+    }
+    if (E) {
+        k_positions<<<grid_for(E, 256), 256, 0, g->stream>>>(g->pos_edge, (const uint32_t *)src,
+                                                             (const uint32_t *)dst, E, g->node_s, g->in_src,
+                                                             g->edge_pos, g->pos_dims);
+        BP_CUDA(cudaGetLastError());
+    }
+
+    // ---- joint tables: stage host tables in edge-id order, then gather
+    if (E) {
+        const uint32_t rs = d->joint_row_stride;
+        const uint64_t es = d->joint_edge_stride;
+        if (rs < g->ms || es < (uint64_t)rs * (g->ms - 1) + g->ms)
+            return set_error(BP_ERR_SHAPE, "joint strides (%u, %llu) too small for %u states", rs,
+                             (unsigned long long)es, g->ms);
+        const size_t jbytes = sizeof(float) * (es * (uint64_t)(E - 1) + (uint64_t)rs * (g->ms - 1) + g->ms);
+        void *jd = nullptr;
+        bool own_j = false;
+        if ((st = to_device(g, d->edge_joint, jbytes, d->memory, &jd, &own_j))) return st;
+        if ((st = gather_joint(g, (const float *)jd, rs, es, (const uint32_t *)dst))) return st;
+        if (own_j) cudaFreeAsync(jd, g->stream);
+    }
+    if (own_src) cudaFreeAsync(src, g->stream);
+    if (own_dst) cudaFreeAsync(dst, g->stream);
+    BP_CUDA(cudaEventCreate(&g->ev0));
+    BP_CUDA(cudaEventCreate(&g->ev1));
+    BP_CUDA(cudaStreamSynchronize(g->stream));
+    return BP_OK;
+}
+
+}  // namespace bpx
+
+using namespace bpx;
+
+extern "C" {
+
+int bp_version(void) { return 1; }
+
+const char *bp_last_error(void) { return bpx::g_last_error; }
+
+const char *bp_status_string(int status) {
+    switch (status) {
+    case BP_OK: return "ok";
+    case BP_ERR_INVALID: return "invalid argument";
+    case BP_ERR_SHAPE: return "shape out of range";
+    case BP_ERR_CUDA: return "CUDA error";
+    case BP_ERR_NOMEM: return "out of device memory";
+    case BP_ERR_NO_DEVICE: return "no CUDA device";
+    case BP_ERR_GRAPH: return "graph has nodes unreachable from the tree seed set";
+    case BP_ERR_STATE: return "call out of order";
+    case BP_ERR_TIMEOUT: return "bounded device wait timed out";
+    default: return "unknown status";
+    }
+}
+
+int bp_graph_create(bp_graph **out, const bp_graph_desc *d, void *stream) {
+    if (!out || !d) return set_error(BP_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (d->num_edges && (!d->edge_src || !d->edge_dst || !d->edge_joint))
+        return set_error(BP_ERR_INVALID, "edge arrays missing");
+    if (d->memory != BP_MEM_HOST && d->memory != BP_MEM_DEVICE)
+        return set_error(BP_ERR_INVALID, "memory must be BP_MEM_HOST or BP_MEM_DEVICE");
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) return set_error(BP_ERR_NO_DEVICE, "no CUDA device available");
+    bp_graph *g = new bp_graph();
+    cudaGetDevice(&g->device);
+    g->V = d->num_nodes;
+    g->E = d->num_edges;
+    if (stream) {
+        g->stream = (cudaStream_t)stream;
+    } else {
+        if (cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            delete g;
+            return set_error(BP_ERR_CUDA, "cudaStreamCreate failed");
+        }
+        g->own_stream = true;
+    }
+    int st = create_impl(g, d);
+    if (st != BP_OK) {
+        char keep[512];
+        snprintf(keep, sizeof keep, "%s", bp_last_error());
+        free_graph(g);
+        set_error(st, "%s", keep);
+        return st;
+    }
+    *out = g;
+    return BP_OK;
+}
+
+void bp_graph_destroy(bp_graph *g) {
+    if (!g) return;
+    if (g->stream) cudaStreamSynchronize(g->stream);
+    free_graph(g);
+}
+
+int bp_graph_info(const bp_graph *g, uint32_t *V, uint32_t *E, uint32_t *ms, uint32_t *uni) {
+    if (!g) return set_error(BP_ERR_INVALID, "null graph");
+    if (V) *V = g->V;
+    if (E) *E = g->E;
+    if (ms) *ms = g->ms;
+    if (uni) *uni = g->uniform;
+    return BP_OK;
+}
+
+int bp_graph_device_bytes(const bp_graph *g, uint64_t *bytes) {
+    if (!g || !bytes) return set_error(BP_ERR_INVALID, "null argument");
+    *bytes = g->device_bytes;
+    return BP_OK;
+}
+
+int bp_set_stream(bp_graph *g, void *stream) {
+    if (!g) return set_error(BP_ERR_INVALID, "null graph");
+    BP_CUDA(cudaStreamSynchronize(g->stream));
+    if (g->own_stream) cudaStreamDestroy(g->stream);
+    g->own_stream = false;
+    if (stream) {
+        g->stream = (cudaStream_t)stream;
+    } else {
+        BP_CUDA(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+        g->own_stream = true;
+    }
+    return BP_OK;
+}
+
+int bp_synchronize(bp_graph *g) {
+    if (!g) return set_error(BP_ERR_INVALID, "null graph");
+    BP_CUDA(cudaStreamSynchronize(g->stream));
+    return BP_OK;
+}
+
+// ---- beliefs / messages --------------------------------------------------
+static int staged_in(bp_graph *g, const float *src, size_t bytes, int memory, const float **dev) {
+    if (memory == BP_MEM_DEVICE) {
+        *dev = src;
+        return BP_OK;
+    }
+    int st = ensure_staging(g, bytes);
+    if (st) return st;
+    if (bytes) BP_CUDA(cudaMemcpyAsync(g->staging, src, bytes, cudaMemcpyHostToDevice, g->stream));
+    *dev = g->staging;
+    return BP_OK;
+}
+
+int bp_set_beliefs(bp_graph *g, const float *b, uint32_t ld, int memory) {
+    if (!g || (!b && g->V)) return set_error(BP_ERR_INVALID, "null argument");
+    if (ld < g->ms) return set_error(BP_ERR_SHAPE, "ld %u < max states %u", ld, g->ms);
+    if (g->V == 0) return BP_OK;
+    const float *dev = nullptr;
+    int st = staged_in(g, b, sizeof(float) * (size_t)ld * g->V, memory, &dev);
+    if (st) return st;
+    uint64_t n = (uint64_t)g->V * g->ms;
+    k_beliefs_in<<<grid_for(n, 256), 256, 0, g->stream>>>(dev, ld, g->V, g->ms, g->node_s, g->uniform, g->belief);
+    BP_CUDA(cudaGetLastError());
+    if (memory == BP_MEM_HOST) BP_CUDA(cudaStreamSynchronize(g->stream));
+    return BP_OK;
+}
+
+int bp_get_beliefs(bp_graph *g, float *b, uint32_t ld, int memory) {
+    if (!g || (!b && g->V)) return set_error(BP_ERR_INVALID, "null argument");
+    if (g->V == 0) return BP_OK;
+    uint64_t n = (uint64_t)g->V * g->ms;
+    if (memory == BP_MEM_DEVICE) {
+        k_beliefs_out<<<grid_for(n, 256), 256, 0, g->stream>>>(g->belief, ld, g->V, g->ms, g->node_s, g->uniform, b);
+        BP_CUDA(cudaGetLastError());
+        return BP_OK;
+    }
+    if (ld == g->ms) {
+        BP_CUDA(cudaMemcpyAsync(b, g->belief, sizeof(float) * n, cudaMemcpyDeviceToHost, g->stream));
+        BP_CUDA(cudaStreamSynchronize(g->stream));
+        return BP_OK;
+    }
+    size_t bytes = sizeof(float) * (size_t)ld * g->V;
+    int st = ensure_staging(g, bytes);
+    if (st) return st;
+    // keep the caller's slots beyond each node's state count intact
+    BP_CUDA(cudaMemcpyAsync(g->staging, b, bytes, cudaMemcpyHostToDevice, g->stream));
+    k_beliefs_out<<<grid_for(n, 256), 256, 0, g->stream>>>(g->belief, ld, g->V, g->ms, g->node_s, g->uniform,
+                                                           g->staging);
+    BP_CUDA(cudaGetLastError());
+    BP_CUDA(cudaMemcpyAsync(b, g->staging, bytes, cudaMemcpyDeviceToHost, g->stream));
+    BP_CUDA(cudaStreamSynchronize(g->stream));
+    return BP_OK;
+}
+
+int bp_set_messages(bp_graph *g, int slot, const float *m, uint32_t ld, int memory) {
+    if (!g || (!m && g->E) || slot < 0 || slot > 1) return set_error(BP_ERR_INVALID, "bad argument");
+    if (g->E == 0) return BP_OK;
+    const float *dev = nullptr;
+    int st = staged_in(g, m, sizeof(float) * (size_t)ld * g->E, memory, &dev);
+    if (st) return st;
+    uint64_t n = (uint64_t)g->E * g->ms;
+    k_messages_in<<<grid_for(n, 256), 256, 0, g->stream>>>(dev, ld, g->E, g->ms, g->pos_edge, g->in_src, g->node_s,
+                                                           g->uniform, g->msg[slot]);
+    BP_CUDA(cudaGetLastError());
+    if (memory == BP_MEM_HOST) BP_CUDA(cudaStreamSynchronize(g->stream));
+    return BP_OK;
+}
+
+int bp_get_messages(bp_graph *g, int slot, float *m, uint32_t ld, int memory) {
+    if (!g || (!m && g->E) || slot < 0 || slot > 1) return set_error(BP_ERR_INVALID, "bad argument");
+    if (g->E == 0) return BP_OK;
+    uint64_t n = (uint64_t)g->E * g->ms;
+    if (memory == BP_MEM_DEVICE) {
+        k_messages_out<<<grid_for(n, 256), 256, 0, g->stream>>>(g->msg[slot], ld, g->E, g->ms, g->pos_edge, g->in_src,
+                                                                g->node_s, g->uniform, m);
+        BP_CUDA(cudaGetLastError());
+        return BP_OK;
+    }
+    size_t bytes = sizeof(float) * (size_t)ld * g->E;
+    int st = ensure_staging(g, bytes);
+    if (st) return st;
+    BP_CUDA(cudaMemcpyAsync(g->staging, m, bytes, cudaMemcpyHostToDevice, g->stream));
+    k_messages_out<<<grid_for(n, 256), 256, 0, g->stream>>>(g->msg[slot], ld, g->E, g->ms, g->pos_edge, g->in_src,
+                                                            g->node_s, g->uniform, g->staging);
+    BP_CUDA(cudaGetLastError());
+    BP_CUDA(cudaMemcpyAsync(m, g->staging, bytes, cudaMemcpyDeviceToHost, g->stream));
+    BP_CUDA(cudaStreamSynchronize(g->stream));
+    return BP_OK;
+}
+
+int bp_set_latest_slot(bp_graph *g, int slot) {
+    if (!g || slot < 0 || slot > 1) return set_error(BP_ERR_INVALID, "bad argument");
+    g->latest = slot;
+    return BP_OK;
+}
+
+int bp_get_latest_slot(const bp_graph *g, int *slot) {
+    if (!g || !slot) return set_error(BP_ERR_INVALID, "bad argument");
+    *slot = g->latest;
+    return BP_OK;
+}
+
+int bp_set_visited(bp_graph *g, const char *visited) {
+    if (!g || (!visited && g->V)) return set_error(BP_ERR_INVALID, "bad argument");
+    if (g->V) BP_CUDA(cudaMemcpyAsync(g->visited, visited, g->V, cudaMemcpyHostToDevice, g->stream));
+    BP_CUDA(cudaStreamSynchronize(g->stream));
+    return BP_OK;
+}
+
+int bp_get_visited(bp_graph *g, char *visited) {
+    if (!g || (!visited && g->V)) return set_error(BP_ERR_INVALID, "bad argument");
+    if (g->V) BP_CUDA(cudaMemcpyAsync(visited, g->visited, g->V, cudaMemcpyDeviceToHost, g->stream));
+    BP_CUDA(cudaStreamSynchronize(g->stream));
+    return BP_OK;
+}
+
+}  // extern "C"

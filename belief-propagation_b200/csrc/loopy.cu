@@ -1,0 +1,808 @@
+// loopy.cu -- synchronous flooding BP on the destination-sorted layout.
+//
+// One reference iteration (loopy_propagate_one_iteration, graph.c:1121-1183,
+// then the delta of loopy_propagate_until, graph.c:1294-1310) is ONE launch of
+// k_flood here.  The reference computes, per iteration t,
+//     Q_t(v)  = b_{t-1}(v) * prod_{in-edges, order} m_{t-1}        (send buffer)
+//     m_t(e)  = normalise(J_e . Q_t(src e))                          (send)
+//     b_t(v)  = normalise(b_{t-1}(v) * prod_{in-edges} m_t)          (marginalise)
+// and Q_{t+1}(v) is b_t(v) times the same incoming m_t, so the node step of
+// iteration t can emit Q_{t+1} while the messages are still on chip.  k_flood
+// therefore computes, for a tile of consecutive destination nodes:
+//   phase 1 (edge-parallel over the tile's in-edges, contiguous in HBM):
+//       m_t = normalise(J . Q_t[src]), |m_{t-1} - m_t| into the delta,
+//       m_t to HBM and to shared memory;
+//   phase 2 (node-parallel): P = prod m_t, b_t = normalise(b_{t-1} * P),
+//       Q_{t+1} = b_t * prod m_t (from shared memory);
+// and the last block to finish reduces the delta and applies the stopping
+// rule, so the loop runs as a CUDA graph without host round trips.  Each value
+// goes through the same fp32 operations in the same order as the reference.
+//
+// HBM bytes per iteration (S states, fp32, u32 indices): per edge
+// 4S^2 (J) + 4 (src) + 4S (Q[src] gather) + 4S (old m) + 4S (new m), per node
+// 4 (row ptr) + 4S (b read) + 4S (b write) + 4S (Q write) + 4S (Q read is
+// counted per edge).  For S = 2: 44 B/edge + 28 B/node.
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+
+#include <vector>
+
+#include "bp_device.cuh"
+#include "bp_internal.h"
+
+namespace bpx {
+
+template <int MS> constexpr int flood_nt() { return MS <= 4 ? 256 : 128; }
+template <int MS> constexpr int flood_smem_floats() { return MS <= 2 ? 4096 : 8192; }
+
+struct FloodArgs {
+    uint32_t V;
+    const uint32_t *in_ptr, *in_src, *pos_edge;
+    const uint8_t *node_s, *pos_dims;
+    const float *joint;
+    float *belief;
+    float *msg0, *msg1, *q0, *q1;
+    double *partials;
+    float *absdiff;
+    LoopyCtl *ctl;
+};
+
+// the reference's stopping rule (graph.c:1313-1318; _acc: :1410-1414) and
+// loop bookkeeping, evaluated by one thread after the iteration's delta
+__device__ void finalize(LoopyCtl *c, bool has_delta, float df, double dd) {
+    const uint32_t it = c->it, ce = c->check_every, max_it = c->max_it;
+    bool stop = false;
+    if (has_delta) {
+        if (c->serial)
+            stop = (df < c->tol) || (fabsf(FSUB(df, c->prev_f)) < c->tol);
+        else
+            stop = (dd < (double)c->tol) || (fabs(dd - c->prev_d) < (double)c->tol);
+        c->delta_f = df;
+        c->delta_d = dd;
+    }
+    if (ce <= 1) {
+        if (stop) {
+            c->done = 1;
+            c->ret = it;
+            c->final_i = it;
+        } else {
+            if (it < max_it - 1) {
+                c->prev_f = df;
+                c->prev_d = dd;
+            }
+            if (it + 1 >= max_it) {
+                c->done = 2;
+                c->ret = max_it;
+                c->final_i = max_it;
+            }
+        }
+    } else if (has_delta) {
+        const uint32_t i_ref = it + 1 - ce;
+        if (stop) {
+            c->done = 1;
+            c->ret = c->num_iter;
+            c->final_i = i_ref;
+        } else {
+            c->prev_f = df;
+            c->prev_d = dd;
+            c->num_iter += ce;
+            if (i_ref + ce >= max_it) {
+                c->done = 2;
+                c->ret = c->num_iter;
+                c->final_i = i_ref + ce;
+            }
+        }
+    }
+    c->it = it + 1;
+}
+
+// grid-wide deterministic delta: per-block partial, last block sums the
+// partials in a fixed order and finalizes
+template <int NT>
+__device__ __forceinline__ void reduce_and_finalize(LoopyCtl *ctl, double *partials, double dsum, bool want,
+                                                    double *red, bool *s_last) {
+    double t = block_sum<NT>(dsum, red);
+    if (threadIdx.x == 0) {
+        partials[blockIdx.x] = t;
+        __threadfence();
+        unsigned ticket = atomicAdd(&ctl->counter, 1u);
+        *s_last = (ticket == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (*s_last) {
+        __threadfence();
+        double acc = 0.0;
+        for (uint32_t k = threadIdx.x; k < gridDim.x; k += NT) acc += __ldcg(partials + k);
+        double tot = block_sum<NT>(acc, red);
+        if (threadIdx.x == 0) {
+            ctl->counter = 0;
+            finalize(ctl, want, (float)tot, tot);
+        }
+    }
+}
+
+template <int MS, bool UNI>
+__global__ void __launch_bounds__(flood_nt<MS>()) k_flood(const FloodArgs a) {
+    constexpr int NT = flood_nt<MS>();
+    constexpr uint32_t EMAX = flood_smem_floats<MS>() / MS;
+    __shared__ __align__(16) float sm[EMAX * MS];
+    __shared__ double red[NT / 32];
+    __shared__ bool s_last;
+
+    LoopyCtl *ctl = a.ctl;
+    if (*(volatile uint32_t *)&ctl->done) return;
+    const uint32_t it = ctl->it, ce = ctl->check_every;
+    const bool serial = ctl->serial != 0;
+    const bool want = (ce <= 1) || ((it + 1) % ce == 0);
+    const int mp = (int)((ctl->msg_parity0 + it) & 1u), qp = (int)((ctl->q_parity0 + it) & 1u);
+    const float *__restrict__ m_old = mp ? a.msg1 : a.msg0;
+    float *__restrict__ m_new = mp ? a.msg0 : a.msg1;
+    const float *__restrict__ q_in = qp ? a.q1 : a.q0;
+    float *__restrict__ q_out = qp ? a.q0 : a.q1;
+
+    const uint32_t V = a.V, tid = threadIdx.x, v0 = blockIdx.x * NT;
+    const uint32_t vend = min(v0 + NT, V);
+    const uint32_t e0 = a.in_ptr[v0], e1 = a.in_ptr[vend];
+    const uint32_t v = v0 + tid;
+    const bool has = v < V;
+    uint32_t r0 = 0, r1 = 0;
+    int S = MS;
+    if (has) {
+        r0 = a.in_ptr[v];
+        r1 = a.in_ptr[v + 1];
+        if (!UNI) S = a.node_s[v];
+    }
+    float prod[MS];
+#pragma unroll
+    for (int i = 0; i < MS; ++i) prod[i] = 1.0f;
+    double dsum = 0.0;
+
+    for (uint32_t c0 = e0; c0 < e1; c0 += EMAX) {
+        const uint32_t c1 = min(e1, c0 + EMAX);
+        // phase 1: messages of this chunk of in-edges
+        for (uint32_t p = c0 + tid; p < c1; p += NT) {
+            const uint32_t s = __ldcs(a.in_src + p);
+            int x = MS, y = MS;
+            if (!UNI) {
+                const uint8_t d = a.pos_dims[p];
+                x = d & 15;
+                y = d >> 4;
+            }
+            float q[MS], m[MS];
+            ldv<MS>(q_in + (size_t)s * MS, q);
+            send_msg<MS, UNI>(a.joint + (size_t)p * (MS * MS), q, x, y, m);
+            if (want) {
+                float o[MS], ad[MS];
+                ldv<MS, kStream>(m_old + (size_t)p * MS, o);
+#pragma unroll
+                for (int k = 0; k < MS; ++k) {
+                    float d = 0.0f;
+                    if (UNI || k < x) {
+                        d = FSUB(o[k], m[k]);
+                        if (d != d) d = 0.0f;
+                        d = fabsf(d);
+                    }
+                    ad[k] = d;
+                    dsum += (double)d;
+                }
+                if (serial) stv<MS>(a.absdiff + (size_t)__ldg(a.pos_edge + p) * MS, ad);
+            }
+            stv<MS, kStream>(m_new + (size_t)p * MS, m);
+            stv<MS>(sm + (size_t)(p - c0) * MS, m);
+        }
+        __syncthreads();
+        // phase 2a: this node's product over its in-edges inside the chunk
+        if (has) {
+            const uint32_t lo = max(r0, c0), hi = min(r1, c1);
+            for (uint32_t p = lo; p < hi; ++p) {
+                float mm[MS];
+                ldv<MS>(sm + (size_t)(p - c0) * MS, mm);
+                combine<MS, UNI>(prod, mm, S);
+            }
+        }
+        __syncthreads();
+    }
+
+    // phase 2b: marginalise (graph.c:1003-1023), then the next send buffer
+    // (graph.c:850-882) from the same messages
+    if (has) {
+        float b[MS];
+        ldv<MS, kStream>(a.belief + (size_t)v * MS, b);
+        if (r1 > r0) {
+#pragma unroll
+            for (int i = 0; i < MS; ++i)
+                if (UNI || i < S) b[i] = FMUL(b[i], prod[i]);
+        }
+        normalise<MS, UNI>(b, S);
+        stv<MS, kStream>(a.belief + (size_t)v * MS, b);
+        float qo[MS];
+#pragma unroll
+        for (int i = 0; i < MS; ++i) qo[i] = b[i];
+        if (e1 - e0 <= EMAX) {
+            for (uint32_t p = r0; p < r1; ++p) {
+                float mm[MS];
+                ldv<MS>(sm + (size_t)(p - e0) * MS, mm);
+                combine<MS, UNI>(qo, mm, S);
+            }
+        } else {
+            for (uint32_t p = r0; p < r1; ++p) {
+                float mm[MS];
+                ldv<MS>(m_new + (size_t)p * MS, mm);
+                combine<MS, UNI>(qo, mm, S);
+            }
+        }
+        stv<MS>(q_out + (size_t)v * MS, qo);
+    }
+
+    if (!serial) reduce_and_finalize<NT>(ctl, a.partials, dsum, want, red, &s_last);
+}
+
+// prologue: Q_1 = b * prod of the latest messages (read_incoming_messages,
+// graph.c:860-882, on the messages init_previous_edge left)
+template <int MS, bool UNI>
+__global__ void k_gather_q(uint32_t V, const uint32_t *__restrict__ in_ptr, const uint8_t *__restrict__ node_s,
+                           const float *__restrict__ belief, const float *__restrict__ msg, float *__restrict__ q) {
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= V) return;
+    const int S = UNI ? MS : node_s[v];
+    float b[MS];
+    ldv<MS>(belief + (size_t)v * MS, b);
+    for (uint32_t p = in_ptr[v]; p < in_ptr[v + 1]; ++p) {
+        float mm[MS];
+        ldv<MS>(msg + (size_t)p * MS, mm);
+        combine<MS, UNI>(b, mm, S);
+    }
+    stv<MS>(q + (size_t)v * MS, b);
+}
+
+// init_previous_edge (graph.c:725-751): every edge carries normalise(J . b_src)
+template <int MS, bool UNI>
+__global__ void k_send_from_beliefs(uint32_t E, const uint32_t *__restrict__ in_src,
+                                    const uint8_t *__restrict__ pos_dims, const float *__restrict__ joint,
+                                    const float *__restrict__ belief, float *__restrict__ msg) {
+    const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= E) return;
+    const uint32_t s = in_src[p];
+    int x = MS, y = MS;
+    if (!UNI) {
+        const uint8_t d = pos_dims[p];
+        x = d & 15;
+        y = d >> 4;
+    }
+    float buf[MS], m[MS];
+    ldv<MS>(belief + (size_t)s * MS, buf);
+    send_msg<MS, UNI>(joint + p * (MS * MS), buf, x, y, m);
+    stv<MS>(msg + p * MS, m);
+}
+
+// the reference's own delta: fp32, serial, edge-id order (graph.c:1300-1309).
+// The |diff| values were written in edge-id order by the iteration kernel;
+// zero entries (slots past an edge's x_dim) leave a non-negative sum unchanged.
+__global__ void __launch_bounds__(256) k_delta_serial(LoopyCtl *ctl, const float *__restrict__ absdiff, uint64_t n) {
+    __shared__ __align__(16) float buf[4096];
+    if (*(volatile uint32_t *)&ctl->done) return;
+    const uint32_t it = ctl->it, ce = ctl->check_every;
+    const bool want = (ce <= 1) || ((it + 1) % ce == 0);
+    float s = 0.0f;
+    if (want) {
+        for (uint64_t base = 0; base < n; base += 4096) {
+            const uint32_t cnt = (uint32_t)min((uint64_t)4096, n - base);
+            for (uint32_t k = threadIdx.x; k < cnt; k += blockDim.x) buf[k] = absdiff[base + k];
+            __syncthreads();
+            if (threadIdx.x == 0) {
+#pragma unroll 8
+                for (uint32_t k = 0; k < cnt; ++k) s = FADD(s, buf[k]);
+            }
+            __syncthreads();
+        }
+    }
+    if (threadIdx.x == 0) finalize(ctl, want, s, (double)s);
+}
+
+// ------------------------------------------------------------------------
+// Edge-centric schedule (loopy_propagate_until_edge, graph.c:1186-1276, and
+// its _acc form, graph.c:1444-1547), reproduced with its quirks:
+//  * copy: num_edges * MAX_STATES BYTES of current into previous
+//    (graph.c:1211), i.e. the first 2.5E floats of the reference's padded
+//    array; the _acc form copies every float;
+//  * send from the beliefs themselves (no incoming product);
+//  * combine: belief(dest) *= message for each edge in edge order, no NaN
+//    check; the _acc form multiplies by the message of edge i, the batch's
+//    first iteration index (graph.c:1485);
+//  * normalise: node 0's belief, once per node with that node's state count
+//    (the base pointer is passed, graph.c:1225, :1505).
+struct EdgeArgs {
+    uint32_t V, E;
+    const uint32_t *in_ptr, *in_src, *pos_edge, *edge_pos;
+    const uint8_t *node_s, *pos_dims;
+    const float *joint;
+    float *belief;
+    float *msg0, *msg1;
+    double *partials;
+    float *absdiff;
+    LoopyCtl *ctl;
+    const uint32_t *run_len;
+    const uint8_t *run_s;
+    uint32_t nruns;
+};
+
+// previous/current roles: the _acc form swaps local pointers every iteration
+__device__ __forceinline__ void edge_roles(const EdgeArgs &a, uint32_t it, float *&prev, float *&curr) {
+    const LoopyCtl *c = a.ctl;
+    int p = (int)(c->msg_parity0 & 1u);
+    if (c->acc_edge && (it & 1u)) p ^= 1;
+    prev = p ? a.msg1 : a.msg0;
+    curr = p ? a.msg0 : a.msg1;
+}
+
+template <int MS>
+__global__ void k_edge_copy(const EdgeArgs a) {
+    if (*(volatile uint32_t *)&a.ctl->done) return;
+    float *prev, *curr;
+    edge_roles(a, a.ctl->it, prev, curr);
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t p = t / MS;
+    if (p >= a.E) return;
+    const uint32_t k = (uint32_t)(t % MS);
+    if (a.ctl->acc_edge) {
+        prev[t] = curr[t];
+        return;
+    }
+    const uint64_t f = (uint64_t)a.pos_edge[p] * 10u + k;   // float index in the padded layout
+    const uint64_t nbytes = (uint64_t)a.E * 10u;
+    const uint64_t nfull = nbytes / 4u;
+    if (f < nfull) {
+        prev[t] = curr[t];
+    } else if (f == nfull && (nbytes & 3u)) {
+        const uint32_t keep = 0xffffffffu << (8u * (uint32_t)(nbytes & 3u));
+        const uint32_t cb = __float_as_uint(curr[t]), pb = __float_as_uint(prev[t]);
+        prev[t] = __uint_as_float((pb & keep) | (cb & ~keep));
+    }
+}
+
+template <int MS, bool UNI>
+__global__ void k_edge_send(const EdgeArgs a) {
+    if (*(volatile uint32_t *)&a.ctl->done) return;
+    float *prev, *curr;
+    edge_roles(a, a.ctl->it, prev, curr);
+    const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= a.E) return;
+    const uint32_t s = a.in_src[p];
+    int x = MS, y = MS;
+    if (!UNI) {
+        const uint8_t d = a.pos_dims[p];
+        x = d & 15;
+        y = d >> 4;
+    }
+    float buf[MS], m[MS];
+    ldv<MS>(a.belief + (size_t)s * MS, buf);
+    send_msg<MS, UNI>(a.joint + p * (MS * MS), buf, x, y, m);
+    stv<MS>(curr + p * MS, m);
+}
+
+template <int MS, bool UNI>
+__global__ void k_edge_combine(const EdgeArgs a) {
+    if (*(volatile uint32_t *)&a.ctl->done) return;
+    const uint32_t it = a.ctl->it;
+    float *prev, *curr;
+    edge_roles(a, it, prev, curr);
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= a.V) return;
+    const int S = UNI ? MS : a.node_s[v];
+    const uint32_t r0 = a.in_ptr[v], r1 = a.in_ptr[v + 1];
+    if (r0 == r1) return;
+    float b[MS];
+    ldv<MS>(a.belief + (size_t)v * MS, b);
+    if (a.ctl->acc_edge) {
+        const uint32_t i_batch = (it / 10u) * 10u;
+        if (i_batch >= a.E) return;
+        float mm[MS];
+        ldv<MS>(curr + (size_t)a.edge_pos[i_batch] * MS, mm);
+        for (uint32_t p = r0; p < r1; ++p) {
+#pragma unroll
+            for (int i = 0; i < MS; ++i)
+                if (UNI || i < S) b[i] = FMUL(b[i], mm[i]);
+        }
+    } else {
+        for (uint32_t p = r0; p < r1; ++p) {
+            float mm[MS];
+            ldv<MS>(curr + (size_t)p * MS, mm);
+#pragma unroll
+            for (int i = 0; i < MS; ++i)
+                if (UNI || i < S) b[i] = FMUL(b[i], mm[i]);
+        }
+    }
+    stv<MS>(a.belief + (size_t)v * MS, b);
+}
+
+// node 0 normalised once per node, in node order; within a run of equal
+// state counts the map is applied until it stops changing node 0 (it is then
+// the identity for the rest of the run)
+template <int MS>
+__global__ void k_edge_normalise_node0(const EdgeArgs a) {
+    if (*(volatile uint32_t *)&a.ctl->done) return;
+    if (threadIdx.x != 0 || blockIdx.x != 0 || a.V == 0) return;
+    float b[MS];
+    ldv<MS>(a.belief, b);
+    for (uint32_t r = 0; r < a.nruns; ++r) {
+        const int s = a.run_s[r];
+        const uint32_t len = a.run_len[r];
+        for (uint32_t k = 0; k < len; ++k) {
+            float sum = 0.0f;
+#pragma unroll
+            for (int i = 0; i < MS; ++i)
+                if (i < s) sum = FADD(sum, b[i]);
+            if (!(sum > 0.0f)) break;
+            bool changed = false;
+#pragma unroll
+            for (int i = 0; i < MS; ++i) {
+                if (i < s) {
+                    float nb = FDIV(b[i], sum);
+                    changed |= __float_as_uint(nb) != __float_as_uint(b[i]);
+                    b[i] = nb;
+                }
+            }
+            if (!changed) break;
+        }
+    }
+    stv<MS>(a.belief, b);
+}
+
+template <int MS, bool UNI>
+__global__ void __launch_bounds__(256) k_edge_delta(const EdgeArgs a) {
+    __shared__ double red[8];
+    __shared__ bool s_last;
+    LoopyCtl *ctl = a.ctl;
+    if (*(volatile uint32_t *)&ctl->done) return;
+    const uint32_t it = ctl->it, ce = ctl->check_every;
+    const bool want = (ce <= 1) || ((it + 1) % ce == 0);
+    const bool serial = ctl->serial != 0;
+    // the delta reads the local prev/curr AFTER this iteration's swap (_acc)
+    float *prev, *curr;
+    edge_roles(a, ctl->acc_edge ? it + 1 : it, prev, curr);
+    double dsum = 0.0;
+    const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (want && p < a.E) {
+        int x = MS;
+        if (!UNI) x = a.pos_dims[p] & 15;
+        float o[MS], c[MS], ad[MS];
+        ldv<MS>(prev + p * MS, o);
+        ldv<MS>(curr + p * MS, c);
+#pragma unroll
+        for (int k = 0; k < MS; ++k) {
+            float d = 0.0f;
+            if (UNI || k < x) {
+                d = FSUB(o[k], c[k]);
+                if (d != d) d = 0.0f;
+                d = fabsf(d);
+            }
+            ad[k] = d;
+            dsum += (double)d;
+        }
+        if (serial) stv<MS>(a.absdiff + (size_t)a.pos_edge[p] * MS, ad);
+    }
+    if (!serial) reduce_and_finalize<256>(ctl, a.partials, dsum, want, red, &s_last);
+}
+
+// ---------------------------------------------------------------- driver --
+
+static int ensure_partials(bp_graph *g, uint32_t n) {
+    if (g->partials_cap >= n) return BP_OK;
+    if (g->partials) {
+        cudaFree(g->partials);
+        g->partials = nullptr;
+    }
+    for (auto &c : g->loop_graph)
+        if (c.exec) {
+            cudaGraphExecDestroy(c.exec);
+            c.exec = nullptr;
+            c.key = 0;
+        }
+    int st = dev_alloc(g, (void **)&g->partials, sizeof(double) * n);
+    if (st == BP_OK) g->partials_cap = n;
+    return st;
+}
+
+static int ensure_absdiff(bp_graph *g) {
+    if (g->absdiff) return BP_OK;
+    for (auto &c : g->loop_graph)
+        if (c.exec) {
+            cudaGraphExecDestroy(c.exec);
+            c.exec = nullptr;
+            c.key = 0;
+        }
+    int st = dev_alloc(g, (void **)&g->absdiff, sizeof(float) * (size_t)g->ms * ((size_t)g->E + 1));
+    if (st) return st;
+    BP_CUDA(cudaMemsetAsync(g->absdiff, 0, sizeof(float) * (size_t)g->ms * ((size_t)g->E + 1), g->stream));
+    return BP_OK;
+}
+
+// runs of equal state count over node order, for the node-0 normalisation
+static int ensure_runs(bp_graph *g) {
+    if (g->run_len || g->V == 0) return BP_OK;
+    std::vector<uint32_t> len;
+    std::vector<uint8_t> s;
+    for (uint32_t v = 0; v < g->V; ++v) {
+        if (s.empty() || s.back() != g->node_s_host[v]) {
+            s.push_back(g->node_s_host[v]);
+            len.push_back(0);
+        }
+        len.back()++;
+    }
+    int st;
+    if ((st = dev_alloc(g, (void **)&g->run_len, sizeof(uint32_t) * len.size()))) return st;
+    if ((st = dev_alloc(g, (void **)&g->run_s, s.size()))) return st;
+    BP_CUDA(cudaMemcpy(g->run_len, len.data(), sizeof(uint32_t) * len.size(), cudaMemcpyHostToDevice));
+    BP_CUDA(cudaMemcpy(g->run_s, s.data(), s.size(), cudaMemcpyHostToDevice));
+    g->nruns = (uint32_t)len.size();
+    return BP_OK;
+}
+
+template <int MS, bool UNI>
+static int launch_init(bp_graph *g) {
+    if (g->E == 0) return BP_OK;
+    k_send_from_beliefs<MS, UNI><<<grid_for(g->E, 256), 256, 0, g->stream>>>(g->E, g->in_src, g->pos_dims, g->joint,
+                                                                             g->belief, g->msg[g->latest]);
+    BP_CUDA(cudaGetLastError());
+    return BP_OK;
+}
+
+template <int MS, bool UNI>
+static int launch_gather(bp_graph *g) {
+    if (g->V == 0) return BP_OK;
+    k_gather_q<MS, UNI><<<grid_for(g->V, 256), 256, 0, g->stream>>>(g->V, g->in_ptr, g->node_s, g->belief,
+                                                                     g->msg[g->latest], g->q[0]);
+    BP_CUDA(cudaGetLastError());
+    return BP_OK;
+}
+
+static FloodArgs flood_args(bp_graph *g) {
+    FloodArgs a;
+    a.V = g->V;
+    a.in_ptr = g->in_ptr;
+    a.in_src = g->in_src;
+    a.pos_edge = g->pos_edge;
+    a.node_s = g->node_s;
+    a.pos_dims = g->pos_dims;
+    a.joint = g->joint;
+    a.belief = g->belief;
+    a.msg0 = g->msg[0];
+    a.msg1 = g->msg[1];
+    a.q0 = g->q[0];
+    a.q1 = g->q[1];
+    a.partials = g->partials;
+    a.absdiff = g->absdiff;
+    a.ctl = g->ctl;
+    return a;
+}
+
+static EdgeArgs edge_args(bp_graph *g) {
+    EdgeArgs a;
+    a.V = g->V;
+    a.E = g->E;
+    a.in_ptr = g->in_ptr;
+    a.in_src = g->in_src;
+    a.pos_edge = g->pos_edge;
+    a.edge_pos = g->edge_pos;
+    a.node_s = g->node_s;
+    a.pos_dims = g->pos_dims;
+    a.joint = g->joint;
+    a.belief = g->belief;
+    a.msg0 = g->msg[0];
+    a.msg1 = g->msg[1];
+    a.partials = g->partials;
+    a.absdiff = g->absdiff;
+    a.ctl = g->ctl;
+    a.run_len = g->run_len;
+    a.run_s = g->run_s;
+    a.nruns = g->nruns;
+    return a;
+}
+
+template <int MS, bool UNI>
+static int enqueue_node_iterations(bp_graph *g, uint32_t k, bool serial) {
+    constexpr int NT = flood_nt<MS>();
+    const unsigned grid = grid_for(g->V, NT);
+    const FloodArgs a = flood_args(g);
+    const uint64_t n = (uint64_t)g->E * MS;
+    for (uint32_t i = 0; i < k; ++i) {
+        k_flood<MS, UNI><<<grid, NT, 0, g->stream>>>(a);
+        BP_CUDA(cudaGetLastError());
+        if (serial) {
+            k_delta_serial<<<1, 256, 0, g->stream>>>(g->ctl, g->absdiff, n);
+            BP_CUDA(cudaGetLastError());
+        }
+    }
+    return BP_OK;
+}
+
+template <int MS, bool UNI>
+static int enqueue_edge_iterations(bp_graph *g, uint32_t k, bool serial) {
+    const EdgeArgs a = edge_args(g);
+    const uint64_t n = (uint64_t)g->E * MS;
+    for (uint32_t i = 0; i < k; ++i) {
+        k_edge_copy<MS><<<grid_for(n, 256), 256, 0, g->stream>>>(a);
+        k_edge_send<MS, UNI><<<grid_for(g->E, 256), 256, 0, g->stream>>>(a);
+        k_edge_combine<MS, UNI><<<grid_for(g->V, 256), 256, 0, g->stream>>>(a);
+        k_edge_normalise_node0<MS><<<1, 32, 0, g->stream>>>(a);
+        k_edge_delta<MS, UNI><<<grid_for(g->E, 256), 256, 0, g->stream>>>(a);
+        BP_CUDA(cudaGetLastError());
+        if (serial) {
+            k_delta_serial<<<1, 256, 0, g->stream>>>(g->ctl, g->absdiff, n);
+            BP_CUDA(cudaGetLastError());
+        }
+    }
+    return BP_OK;
+}
+
+static int enqueue_iterations(bp_graph *g, int schedule, uint32_t k, bool serial) {
+    if (schedule == BP_SCHEDULE_NODE) BP_DISPATCH_MS(g->ms, g->uniform != 0, enqueue_node_iterations, g, k, serial);
+    BP_DISPATCH_MS(g->ms, g->uniform != 0, enqueue_edge_iterations, g, k, serial);
+}
+
+static int flood_grid(bp_graph *g) {
+    const int nt = g->ms <= 4 ? 256 : 128;
+    return (int)grid_for(g->V, nt);
+}
+
+}  // namespace bpx
+
+using namespace bpx;
+
+extern "C" {
+
+void bp_loopy_default_options(bp_loopy_options *o) {
+    if (!o) return;
+    o->tolerance = 1e-3f;
+    o->max_iterations = 200;
+    o->check_every = 1;
+    o->schedule = BP_SCHEDULE_NODE;
+    o->delta_mode = BP_DELTA_AUTO;
+    o->verbose = 0;
+    o->graph_chunk = 0;
+    o->reserved = 0;
+}
+
+int bp_init_messages(bp_graph *g) {
+    if (!g) return set_error(BP_ERR_INVALID, "null graph");
+    BP_DISPATCH_MS(g->ms, g->uniform != 0, launch_init, g);
+}
+
+int bp_loopy(bp_graph *g, const bp_loopy_options *opt, bp_loopy_result *res) {
+    if (!g || !opt) return set_error(BP_ERR_INVALID, "null argument");
+    if (opt->schedule != BP_SCHEDULE_NODE && opt->schedule != BP_SCHEDULE_EDGE)
+        return set_error(BP_ERR_INVALID, "unknown schedule %d", opt->schedule);
+    if (opt->delta_mode < BP_DELTA_AUTO || opt->delta_mode > BP_DELTA_F64)
+        return set_error(BP_ERR_INVALID, "unknown delta mode %d", opt->delta_mode);
+    const uint32_t ce = opt->check_every <= 1 ? 1u : opt->check_every;
+    const uint32_t max_it = opt->max_iterations;
+    bp_loopy_result r = {};
+    r.previous_delta = -1.0f;
+    const bool serial = opt->delta_mode == BP_DELTA_SERIAL_F32 ||
+                        (opt->delta_mode == BP_DELTA_AUTO && (uint64_t)g->E * g->ms <= (1ull << 20));
+    // degenerate loops: nothing launches (the reference's loop body never
+    // runs, or there is no node to hold a delta)
+    if (max_it == 0 || g->V == 0) {
+        float prev = -1.0f, delta = 0.0f;
+        uint32_t i = 0, executed = 0, num_iter = 0;
+        if (ce <= 1) {
+            for (i = 0; i < max_it; ++i) {
+                ++executed;
+                delta = 0.0f;
+                if (delta < opt->tolerance || fabsf(delta - prev) < opt->tolerance) break;
+                if (i < max_it - 1) prev = delta;
+            }
+            r.iterations = i;
+        } else {
+            for (i = 0; i < max_it; i += ce) {
+                executed += ce;
+                delta = 0.0f;
+                if (delta < opt->tolerance || fabsf(delta - prev) < opt->tolerance) break;
+                prev = delta;
+                num_iter += ce;
+            }
+            r.iterations = num_iter;
+        }
+        r.executed = executed;
+        r.converged = i < max_it;
+        r.delta = delta;
+        r.previous_delta = prev;
+        r.delta_f64 = delta;
+        if (i == max_it && opt->verbose)
+            printf("No Convergence: previous: %f vs current: %f\n", (double)prev, (double)delta);
+        if (opt->schedule == BP_SCHEDULE_NODE && ce <= 1 && (executed & 1u)) g->latest ^= 1;
+        if (res) *res = r;
+        return BP_OK;
+    }
+    int st;
+    const uint32_t grid_blocks = opt->schedule == BP_SCHEDULE_NODE ? (uint32_t)flood_grid(g) : grid_for(g->E, 256);
+    if ((st = ensure_partials(g, grid_blocks))) return st;
+    if (serial && (st = ensure_absdiff(g))) return st;
+    if (opt->schedule == BP_SCHEDULE_EDGE && (st = ensure_runs(g))) return st;
+
+    const uint32_t n_launch = ce <= 1 ? max_it : ((max_it + ce - 1) / ce) * ce;
+    uint32_t chunk = opt->graph_chunk;
+    if (chunk == 0) chunk = opt->schedule == BP_SCHEDULE_NODE ? 32 : 8;
+    if (chunk > n_launch) chunk = n_launch;
+
+    LoopyCtl c = {};
+    c.max_it = max_it;
+    c.check_every = ce;
+    c.msg_parity0 = (uint32_t)g->latest;
+    c.q_parity0 = 0;
+    c.serial = serial ? 1u : 0u;
+    c.acc_edge = (opt->schedule == BP_SCHEDULE_EDGE && ce > 1) ? 1u : 0u;
+    c.tol = opt->tolerance;
+    c.prev_f = -1.0f;
+    c.prev_d = -1.0;
+    *g->ctl_host = c;
+    BP_CUDA(cudaMemcpyAsync(g->ctl, g->ctl_host, sizeof(LoopyCtl), cudaMemcpyHostToDevice, g->stream));
+    if (opt->schedule == BP_SCHEDULE_NODE) {
+        auto gather = [&]() -> int { BP_DISPATCH_MS(g->ms, g->uniform != 0, launch_gather, g); };
+        if ((st = gather())) return st;
+    }
+
+    // CUDA graph of `chunk` iterations, cached per (schedule, delta, chunk)
+    const uint64_t key = 1ull | ((uint64_t)opt->schedule << 1) | ((uint64_t)serial << 2) | ((uint64_t)chunk << 8);
+    bp_graph::CachedGraph *slot = nullptr;
+    for (auto &cg : g->loop_graph)
+        if (cg.exec && cg.key == key) slot = &cg;
+    if (!slot) {
+        slot = &g->loop_graph[0];
+        for (auto &cg : g->loop_graph)
+            if (!cg.exec) {
+                slot = &cg;
+                break;
+            }
+        if (slot->exec) {
+            cudaGraphExecDestroy(slot->exec);
+            slot->exec = nullptr;
+        }
+        cudaGraph_t graph = nullptr;
+        BP_CUDA(cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal));
+        st = enqueue_iterations(g, opt->schedule, chunk, serial);
+        cudaError_t ce2 = cudaStreamEndCapture(g->stream, &graph);
+        if (st) {
+            if (graph) cudaGraphDestroy(graph);
+            return st;
+        }
+        if (ce2 != cudaSuccess) return cuda_fail(ce2, "cudaStreamEndCapture", __FILE__, __LINE__);
+        cudaError_t ie = cudaGraphInstantiate(&slot->exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ie != cudaSuccess) return cuda_fail(ie, "cudaGraphInstantiate", __FILE__, __LINE__);
+        slot->key = key;
+    }
+
+    BP_CUDA(cudaEventRecord(g->ev0, g->stream));
+    for (uint32_t launched = 0; launched < n_launch; launched += chunk) {
+        BP_CUDA(cudaGraphLaunch(slot->exec, g->stream));
+        if (launched + chunk < n_launch) {
+            BP_CUDA(cudaMemcpyAsync(&g->ctl_host->done, &g->ctl->done, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                    g->stream));
+            BP_CUDA(cudaStreamSynchronize(g->stream));
+            if (g->ctl_host->done) break;
+        }
+    }
+    BP_CUDA(cudaEventRecord(g->ev1, g->stream));
+    BP_CUDA(cudaMemcpyAsync(g->ctl_host, g->ctl, sizeof(LoopyCtl), cudaMemcpyDeviceToHost, g->stream));
+    BP_CUDA(cudaStreamSynchronize(g->stream));
+    c = *g->ctl_host;
+    if (!c.done) return set_error(BP_ERR_STATE, "loop ended without a stop decision (it=%u)", c.it);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, g->ev0, g->ev1);
+    r.iterations = c.ret;
+    r.executed = c.it;
+    r.converged = c.done == 1;
+    r.delta = serial ? c.delta_f : (float)c.delta_d;
+    r.previous_delta = serial ? c.prev_f : (float)c.prev_d;
+    r.delta_f64 = c.delta_d;
+    r.elapsed_ms = ms;
+    if (opt->schedule == BP_SCHEDULE_NODE) g->latest = (int)((c.msg_parity0 + c.it) & 1u);
+    if (c.done == 2 && c.final_i == max_it && opt->verbose)
+        printf("No Convergence: previous: %f vs current: %f\n", (double)r.previous_delta, (double)r.delta);
+    if (res) *res = r;
+    return BP_OK;
+}
+
+}  // extern "C"

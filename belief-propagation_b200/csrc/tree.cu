@@ -1,0 +1,303 @@
+// tree.cu -- tree BP as level-synchronous frontier passes.
+//
+// The reference's schedule (c_benchmark/main.c:224-236):
+//   propagate_using_levels_start   level 0 sends its beliefs on every out-edge
+//   propagate_using_levels(l)      l = 1 .. L-2, then (after reset_visited)
+//                                  l = L-1 .. 1: each node of the level, in
+//                                  order, marks itself visited, multiplies its
+//                                  incoming messages (no prior) and sends to
+//                                  the out-neighbours not yet visited
+//   marginalize                    belief = normalise(prod of incoming messages)
+// A level is split into waves (levels.c); one wave is one launch of
+// k_tree_wave with a thread per node.  "Not yet visited" at node u's turn is
+//   visited-before-this-call[w]  or  (w in this level and index(w) <= index(u)),
+// which is what the sequential loop sees, so any call order the reference
+// accepts gives the reference's messages.  All messages live in slot 0
+// (struct graph's edges_messages), position order.
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+#include "bp_device.cuh"
+#include "bp_internal.h"
+#include "bp_levels.h"
+
+namespace bpx {
+
+// propagate_using_levels_start (graph.c:376-424)
+template <int MS, bool UNI>
+__global__ void k_tree_start(const uint32_t *__restrict__ nodes, uint32_t n, const uint32_t *__restrict__ out_ptr,
+                             const uint32_t *__restrict__ out_pos, const uint32_t *__restrict__ out_dst,
+                             const uint8_t *__restrict__ node_s, const float *__restrict__ joint,
+                             const float *__restrict__ belief, float *__restrict__ msg, uint8_t *__restrict__ visited) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const uint32_t u = nodes[k];
+    visited[u] = 1;
+    const int x = UNI ? MS : node_s[u];
+    float buf[MS];
+    ldv<MS>(belief + (size_t)u * MS, buf);
+    for (uint32_t q = out_ptr[u]; q < out_ptr[u + 1]; ++q) {
+        const uint32_t p = out_pos[q];
+        const int y = UNI ? MS : node_s[out_dst[q]];
+        float m[MS];
+        send_msg<MS, UNI>(joint + (size_t)p * (MS * MS), buf, x, y, m);
+        stv<MS>(msg + (size_t)p * MS, m);
+    }
+}
+
+// one wave of propagate_node_using_levels (graph.c:461-522)
+template <int MS, bool UNI>
+__global__ void k_tree_wave(const uint32_t *__restrict__ nodes, uint32_t n, uint32_t level,
+                            const uint32_t *__restrict__ in_ptr, const uint32_t *__restrict__ out_ptr,
+                            const uint32_t *__restrict__ out_pos, const uint32_t *__restrict__ out_dst,
+                            const uint32_t *__restrict__ node_level, const uint32_t *__restrict__ node_lidx,
+                            const uint8_t *__restrict__ node_s, const float *__restrict__ joint,
+                            float *__restrict__ msg, const uint8_t *__restrict__ visited) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const uint32_t u = nodes[k];
+    const int S = UNI ? MS : node_s[u];
+    const uint32_t my_idx = node_lidx[u];
+    float buf[MS];
+#pragma unroll
+    for (int i = 0; i < MS; ++i) buf[i] = (UNI || i < S) ? 1.0f : 0.0f;
+    for (uint32_t p = in_ptr[u]; p < in_ptr[u + 1]; ++p) {
+        float mm[MS];
+        ldv<MS>(msg + (size_t)p * MS, mm);
+        combine<MS, UNI>(buf, mm, S);
+    }
+    for (uint32_t q = out_ptr[u]; q < out_ptr[u + 1]; ++q) {
+        const uint32_t w = out_dst[q];
+        const bool seen = visited[w] || (node_level[w] == level && node_lidx[w] <= my_idx);
+        if (seen) continue;
+        const uint32_t p = out_pos[q];
+        const int y = UNI ? MS : node_s[w];
+        float m[MS];
+        send_msg<MS, UNI>(joint + (size_t)p * (MS * MS), buf, S, y, m);
+        stv<MS>(msg + (size_t)p * MS, m);
+    }
+}
+
+__global__ void k_mark_visited(const uint32_t *__restrict__ nodes, uint32_t n, uint8_t *__restrict__ visited) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) visited[nodes[k]] = 1;
+}
+
+// marginalize (graph.c:540-596): the belief is replaced by the product of
+// the incoming messages when there is one, then normalised
+template <int MS, bool UNI>
+__global__ void k_tree_marginalize(uint32_t V, const uint32_t *__restrict__ in_ptr, const uint8_t *__restrict__ node_s,
+                                   const float *__restrict__ msg, float *__restrict__ belief) {
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= V) return;
+    const int S = UNI ? MS : node_s[v];
+    float b[MS];
+    const uint32_t r0 = in_ptr[v], r1 = in_ptr[v + 1];
+    if (r1 > r0) {
+#pragma unroll
+        for (int i = 0; i < MS; ++i) b[i] = (UNI || i < S) ? 1.0f : 0.0f;
+        for (uint32_t p = r0; p < r1; ++p) {
+            float mm[MS];
+            ldv<MS>(msg + (size_t)p * MS, mm);
+            combine<MS, UNI>(b, mm, S);
+        }
+    } else {
+        ldv<MS>(belief + (size_t)v * MS, b);
+    }
+    normalise<MS, UNI>(b, S);
+    stv<MS>(belief + (size_t)v * MS, b);
+}
+
+static void tree_clear(bp_graph *g) {
+    TreeData &t = g->tree;
+    if (t.d_node_level) cudaFree(t.d_node_level);
+    if (t.d_node_lidx) cudaFree(t.d_node_lidx);
+    if (t.d_wave_nodes) cudaFree(t.d_wave_nodes);
+    free(t.levels_host);
+    free(t.wave_off);
+    free(t.level_wave_begin);
+    t = TreeData();
+}
+
+static int tree_prepare(bp_graph *g, const uint32_t *levels, uint32_t num_levels) {
+    const uint32_t V = g->V;
+    TreeData &t = g->tree;
+    if (t.ready && t.num_levels == num_levels &&
+        (V == 0 || memcmp(t.levels_host, levels, sizeof(uint32_t) * 2 * (size_t)V) == 0))
+        return BP_OK;
+    tree_clear(g);
+    if (num_levels == 0) return set_error(BP_ERR_STATE, "no levels (call init_levels_to_nodes first)");
+    int st;
+    if ((st = ensure_out_csr(g))) return st;
+    if ((st = ensure_host_in_ptr(g))) return st;
+    std::vector<uint32_t> in_src(g->E ? g->E : 1);
+    if (g->E) BP_CUDA(cudaMemcpy(in_src.data(), g->in_src, sizeof(uint32_t) * g->E, cudaMemcpyDeviceToHost));
+    std::vector<uint32_t> node_level(V ? V : 1), node_lidx(V ? V : 1), wave_nodes(V ? V : 1);
+    t.level_wave_begin = (uint32_t *)malloc(sizeof(uint32_t) * ((size_t)num_levels + 1));
+    t.levels_host = (uint32_t *)malloc(sizeof(uint32_t) * (2 * (size_t)V + 1));
+    if (V) memcpy(t.levels_host, levels, sizeof(uint32_t) * 2 * (size_t)V);
+    uint32_t total = 0;
+    int rc = bp_tree_waves(V, levels, num_levels, g->in_ptr_host, in_src.data(), node_level.data(),
+                           node_lidx.data(), wave_nodes.data(), &t.wave_off, t.level_wave_begin, &total);
+    if (rc != 0) {
+        tree_clear(g);
+        return set_error(rc == -2 ? BP_ERR_NOMEM : BP_ERR_INVALID, "malformed level lists");
+    }
+    for (uint32_t v = 0; v < V; ++v)
+        if (node_level[v] == 0xffffffffu) {
+            tree_clear(g);
+            return set_error(BP_ERR_GRAPH, "node %u is in no level", v);
+        }
+    t.total_waves = total;
+    t.num_levels = num_levels;
+    const size_t bytes = sizeof(uint32_t) * (V ? V : 1);
+    BP_CUDA(cudaMalloc((void **)&t.d_node_level, bytes));
+    BP_CUDA(cudaMalloc((void **)&t.d_node_lidx, bytes));
+    BP_CUDA(cudaMalloc((void **)&t.d_wave_nodes, bytes));
+    BP_CUDA(cudaMemcpy(t.d_node_level, node_level.data(), bytes, cudaMemcpyHostToDevice));
+    BP_CUDA(cudaMemcpy(t.d_node_lidx, node_lidx.data(), bytes, cudaMemcpyHostToDevice));
+    BP_CUDA(cudaMemcpy(t.d_wave_nodes, wave_nodes.data(), bytes, cudaMemcpyHostToDevice));
+    t.ready = true;
+    return BP_OK;
+}
+
+template <int MS, bool UNI>
+static int launch_start(bp_graph *g) {
+    TreeData &t = g->tree;
+    const uint32_t w0 = t.level_wave_begin[0], w1 = t.level_wave_begin[1];
+    if (w1 == w0) return BP_OK;
+    const uint32_t lo = t.wave_off[w0], hi = t.wave_off[w1];
+    const uint32_t n = hi - lo;
+    k_tree_start<MS, UNI><<<grid_for(n, 128), 128, 0, g->stream>>>(t.d_wave_nodes + lo, n, g->out_ptr, g->out_pos,
+                                                                    g->out_dst, g->node_s, g->joint, g->belief,
+                                                                    g->msg[0], g->visited);
+    BP_CUDA(cudaGetLastError());
+    return BP_OK;
+}
+
+template <int MS, bool UNI>
+static int launch_level(bp_graph *g, uint32_t level) {
+    TreeData &t = g->tree;
+    const uint32_t w0 = t.level_wave_begin[level], w1 = t.level_wave_begin[level + 1];
+    for (uint32_t w = w0; w < w1; ++w) {
+        const uint32_t lo = t.wave_off[w], n = t.wave_off[w + 1] - lo;
+        if (!n) continue;
+        k_tree_wave<MS, UNI><<<grid_for(n, 128), 128, 0, g->stream>>>(
+            t.d_wave_nodes + lo, n, level, g->in_ptr, g->out_ptr, g->out_pos, g->out_dst, t.d_node_level,
+            t.d_node_lidx, g->node_s, g->joint, g->msg[0], g->visited);
+        BP_CUDA(cudaGetLastError());
+    }
+    if (w1 > w0) {
+        const uint32_t lo = t.wave_off[w0], n = t.wave_off[w1] - lo;
+        k_mark_visited<<<grid_for(n, 256), 256, 0, g->stream>>>(t.d_wave_nodes + lo, n, g->visited);
+        BP_CUDA(cudaGetLastError());
+    }
+    return BP_OK;
+}
+
+template <int MS, bool UNI>
+static int launch_marginalize(bp_graph *g) {
+    if (g->V == 0) return BP_OK;
+    k_tree_marginalize<MS, UNI><<<grid_for(g->V, 256), 256, 0, g->stream>>>(g->V, g->in_ptr, g->node_s, g->msg[0],
+                                                                             g->belief);
+    BP_CUDA(cudaGetLastError());
+    return BP_OK;
+}
+
+static int dispatch_start(bp_graph *g) { BP_DISPATCH_MS(g->ms, g->uniform != 0, launch_start, g); }
+static int dispatch_level(bp_graph *g, uint32_t l) { BP_DISPATCH_MS(g->ms, g->uniform != 0, launch_level, g, l); }
+static int dispatch_marginalize(bp_graph *g) { BP_DISPATCH_MS(g->ms, g->uniform != 0, launch_marginalize, g); }
+
+}  // namespace bpx
+
+using namespace bpx;
+
+extern "C" {
+
+int bp_tree_build_levels(bp_graph *g, uint32_t *levels, uint32_t *num_levels) {
+    if (!g || !num_levels) return set_error(BP_ERR_INVALID, "null argument");
+    int st;
+    if ((st = ensure_out_csr(g))) return st;
+    if ((st = ensure_host_in_ptr(g))) return st;
+    const uint32_t V = g->V, E = g->E;
+    std::vector<uint32_t> out_ptr((size_t)V + 1), out_dst(E ? E : 1);
+    BP_CUDA(cudaMemcpy(out_ptr.data(), g->out_ptr, sizeof(uint32_t) * ((size_t)V + 1), cudaMemcpyDeviceToHost));
+    if (E) BP_CUDA(cudaMemcpy(out_dst.data(), g->out_dst, sizeof(uint32_t) * E, cudaMemcpyDeviceToHost));
+    std::vector<uint32_t> lv(2 * (size_t)V + 1, 0);
+    uint32_t nl = *num_levels;
+    int rc = bp_levels_from_csr(V, g->in_ptr_host, out_ptr.data(), out_dst.data(), lv.data(), &nl);
+    if (rc == -2) return set_error(BP_ERR_NOMEM, "host allocation failed");
+    if (rc == -1) return set_error(BP_ERR_GRAPH, "a node is unreachable from the in-degree<=2 seed set");
+    *num_levels = nl;
+    if (levels) memcpy(levels, lv.data(), sizeof(uint32_t) * 2 * (size_t)V);
+    return tree_prepare(g, lv.data(), nl);
+}
+
+int bp_tree_set_levels(bp_graph *g, const uint32_t *levels, uint32_t num_levels) {
+    if (!g || (!levels && g->V)) return set_error(BP_ERR_INVALID, "null argument");
+    return tree_prepare(g, levels, num_levels);
+}
+
+int bp_tree_start(bp_graph *g) {
+    if (!g) return set_error(BP_ERR_INVALID, "null graph");
+    if (!g->tree.ready) return set_error(BP_ERR_STATE, "tree levels not set");
+    return dispatch_start(g);
+}
+
+int bp_tree_level(bp_graph *g, uint32_t level) {
+    if (!g) return set_error(BP_ERR_INVALID, "null graph");
+    if (!g->tree.ready) return set_error(BP_ERR_STATE, "tree levels not set");
+    if (level >= g->tree.num_levels) return set_error(BP_ERR_INVALID, "level %u >= num_levels %u", level,
+                                                      g->tree.num_levels);
+    return dispatch_level(g, level);
+}
+
+int bp_tree_reset_visited(bp_graph *g) {
+    if (!g) return set_error(BP_ERR_INVALID, "null graph");
+    if (g->V) BP_CUDA(cudaMemsetAsync(g->visited, 0, g->V, g->stream));
+    return BP_OK;
+}
+
+int bp_tree_marginalize(bp_graph *g) {
+    if (!g) return set_error(BP_ERR_INVALID, "null graph");
+    return dispatch_marginalize(g);
+}
+
+int bp_tree(bp_graph *g, bp_tree_result *res) {
+    if (!g) return set_error(BP_ERR_INVALID, "null graph");
+    int st;
+    if (!g->tree.ready) {
+        uint32_t nl = 0;
+        if ((st = bp_tree_build_levels(g, nullptr, &nl))) return st;
+    }
+    const uint32_t L = g->tree.num_levels;
+    BP_CUDA(cudaEventRecord(g->ev0, g->stream));
+    if ((st = bp_tree_reset_visited(g))) return st;
+    if ((st = dispatch_start(g))) return st;
+    uint32_t waves = g->tree.level_wave_begin[1] - g->tree.level_wave_begin[0] ? 1 : 0;
+    for (uint32_t l = 1; l + 1 < L; ++l) {
+        if ((st = dispatch_level(g, l))) return st;
+        waves += g->tree.level_wave_begin[l + 1] - g->tree.level_wave_begin[l];
+    }
+    if ((st = bp_tree_reset_visited(g))) return st;
+    for (uint32_t l = L - 1; l > 0; --l) {
+        if ((st = dispatch_level(g, l))) return st;
+        waves += g->tree.level_wave_begin[l + 1] - g->tree.level_wave_begin[l];
+    }
+    if ((st = dispatch_marginalize(g))) return st;
+    BP_CUDA(cudaEventRecord(g->ev1, g->stream));
+    BP_CUDA(cudaStreamSynchronize(g->stream));
+    if (res) {
+        res->num_levels = L;
+        res->num_waves = waves;
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, g->ev0, g->ev1);
+        res->elapsed_ms = ms;
+    }
+    return BP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,183 @@
+"""Python front end of the device-resident engine (include/bp.h).
+
+    g = BPGraph.from_network(net)          # upload + destination sort on the GPU
+    g.set_beliefs(net.beliefs)
+    g.init_messages()                      # init_previous_edge
+    r = g.loopy(tol=1e-3, max_iterations=100)
+    b = g.beliefs()                        # [V, S_max] numpy
+
+Arrays may be numpy (host) or torch CUDA tensors (device pointers are passed
+through without copies).  All work happens in lib/libbp.so.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import native as N
+
+_DELTA = {"auto": N.BP_DELTA_AUTO, "serial": N.BP_DELTA_SERIAL_F32, "f64": N.BP_DELTA_F64}
+_SCHED = {"node": N.BP_SCHEDULE_NODE, "edge": N.BP_SCHEDULE_EDGE}
+
+
+def _is_torch(a):
+    return a is not None and not isinstance(a, np.ndarray) and hasattr(a, "data_ptr")
+
+
+def _memory_of(*arrays):
+    kinds = {("dev" if (_is_torch(a) and a.is_cuda) else "host") for a in arrays if a is not None}
+    if len(kinds) > 1:
+        raise ValueError("mix of host and device arrays")
+    return N.BP_MEM_DEVICE if kinds == {"dev"} else N.BP_MEM_HOST
+
+
+class BPGraph:
+    """A graph resident in GPU memory (bp_graph)."""
+
+    def __init__(self, num_nodes, src, dst, joint, num_states=None, uniform_states=0,
+                 joint_row_stride=None, joint_edge_stride=None, dest_csr=None, stream=None):
+        self.lib = N.load()
+        V, E = int(num_nodes), int(len(src))
+        if not _is_torch(src):
+            src = np.ascontiguousarray(src, np.uint32)
+            dst = np.ascontiguousarray(dst, np.uint32)
+            joint = np.ascontiguousarray(joint, np.float32)
+            if num_states is not None:
+                num_states = np.ascontiguousarray(num_states, np.uint32)
+        s_max = int(joint.shape[-1]) if joint.ndim == 3 else int(uniform_states)
+        d = N.GraphDesc()
+        d.num_nodes, d.num_edges = V, E
+        d.uniform_states = int(uniform_states)
+        d.node_num_states = N.ptr(num_states)
+        d.edge_src, d.edge_dst, d.edge_joint = N.ptr(src), N.ptr(dst), N.ptr(joint)
+        d.joint_row_stride = int(joint_row_stride or s_max)
+        d.joint_edge_stride = int(joint_edge_stride or s_max * s_max)
+        if dest_csr is not None:
+            d.dest_node_list, d.dest_edge_list = N.ptr(dest_csr[0]), N.ptr(dest_csr[1])
+        d.memory = _memory_of(src, dst, joint, num_states)
+        self._keep = (src, dst, joint, num_states)
+        h = C.c_void_p()
+        N.check(self.lib.bp_graph_create(C.byref(h), C.byref(d), stream))
+        self.h = h
+        self._keep = None
+        V_, E_, ms, uni = (C.c_uint32() for _ in range(4))
+        N.check(self.lib.bp_graph_info(h, C.byref(V_), C.byref(E_), C.byref(ms), C.byref(uni)))
+        self.V, self.E, self.ms, self.uniform = V_.value, E_.value, ms.value, uni.value
+
+    @classmethod
+    def from_network(cls, net, stream=None, with_beliefs=True):
+        uni = net.uniform_states
+        g = cls(net.V, net.src, net.dst, net.joint, None if uni else net.num_states, uni, stream=stream)
+        if with_beliefs:
+            g.set_beliefs(net.beliefs)
+        return g
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.bp_graph_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- state ----------------------------------------------------------
+    def set_beliefs(self, b):
+        if not _is_torch(b):
+            b = np.ascontiguousarray(b, np.float32)
+        ld = int(b.shape[1]) if b.ndim == 2 else self.ms
+        N.check(self.lib.bp_set_beliefs(self.h, N.ptr(b), ld, _memory_of(b)))
+
+    def beliefs(self, out=None, ld=None):
+        ld = ld or self.ms
+        if out is None:
+            out = np.zeros((self.V, ld), np.float32)
+        N.check(self.lib.bp_get_beliefs(self.h, N.ptr(out), out.shape[1], _memory_of(out)))
+        return out
+
+    def set_messages(self, slot, m):
+        if not _is_torch(m):
+            m = np.ascontiguousarray(m, np.float32)
+        N.check(self.lib.bp_set_messages(self.h, int(slot), N.ptr(m), int(m.shape[1]), _memory_of(m)))
+
+    def messages(self, slot=None, ld=None):
+        if slot is None:
+            slot = self.latest_slot
+        ld = ld or self.ms
+        out = np.zeros((self.E, ld), np.float32)
+        N.check(self.lib.bp_get_messages(self.h, int(slot), N.ptr(out), ld, N.BP_MEM_HOST))
+        return out
+
+    @property
+    def latest_slot(self):
+        s = C.c_int()
+        N.check(self.lib.bp_get_latest_slot(self.h, C.byref(s)))
+        return s.value
+
+    @latest_slot.setter
+    def latest_slot(self, slot):
+        N.check(self.lib.bp_set_latest_slot(self.h, int(slot)))
+
+    def device_bytes(self):
+        b = C.c_uint64()
+        N.check(self.lib.bp_graph_device_bytes(self.h, C.byref(b)))
+        return b.value
+
+    def synchronize(self):
+        N.check(self.lib.bp_synchronize(self.h))
+
+    # ---- loopy -----------------------------------------------------------
+    def init_messages(self):
+        N.check(self.lib.bp_init_messages(self.h))
+
+    def loopy(self, tol=1e-3, max_iterations=200, check_every=1, schedule="node", delta="auto",
+              verbose=False, graph_chunk=0):
+        o = N.LoopyOptions()
+        self.lib.bp_loopy_default_options(C.byref(o))
+        o.tolerance = float(tol)
+        o.max_iterations = int(max_iterations)
+        o.check_every = int(check_every)
+        o.schedule = _SCHED[schedule]
+        o.delta_mode = _DELTA[delta]
+        o.verbose = int(bool(verbose))
+        o.graph_chunk = int(graph_chunk)
+        r = N.LoopyResult()
+        N.check(self.lib.bp_loopy(self.h, C.byref(o), C.byref(r)))
+        return r.as_dict()
+
+    # ---- tree ------------------------------------------------------------
+    def build_levels(self):
+        lv = np.zeros(2 * max(self.V, 1), np.uint32)
+        n = C.c_uint32(0)
+        N.check(self.lib.bp_tree_build_levels(self.h, lv.ctypes.data, C.byref(n)))
+        return lv[: 2 * self.V], n.value
+
+    def set_levels(self, levels, num_levels):
+        levels = np.ascontiguousarray(levels, np.uint32)
+        N.check(self.lib.bp_tree_set_levels(self.h, levels.ctypes.data, int(num_levels)))
+
+    def tree(self):
+        r = N.TreeResult()
+        N.check(self.lib.bp_tree(self.h, C.byref(r)))
+        return {"num_levels": r.num_levels, "num_waves": r.num_waves, "elapsed_ms": r.elapsed_ms}
+
+    def tree_start(self):
+        N.check(self.lib.bp_tree_start(self.h))
+
+    def tree_level(self, level):
+        N.check(self.lib.bp_tree_level(self.h, int(level)))
+
+    def tree_reset_visited(self):
+        N.check(self.lib.bp_tree_reset_visited(self.h))
+
+    def tree_marginalize(self):
+        N.check(self.lib.bp_tree_marginalize(self.h))

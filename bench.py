@@ -1,0 +1,345 @@
+#!/usr/bin/env python3
+"""Loopy belief-propagation throughput on one B200 (or N, one process each).
+
+Workload (default): loopy BP on a 16,777,216-node, 67,108,864-edge graph with
+power-law out-degree (exponent 2.5, min 1, mean 4), uniform destinations,
+2 states, row-normalised U(0,1) joint tables, Dirichlet(1) priors, 10%
+one-hot evidence, synchronous flooding schedule, 100 fixed iterations
+(tolerance 0), seed 1.  One step = one BP solve as the reference times it
+(c_benchmark/main.c:277-281): reset beliefs to the priors,
+init_previous_edge, loopy_propagate_until.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl bp|reference]
+
+value  edge-msg updates/s over the whole job (E * iterations * N / max-rank time),
+       graph resident in HBM.
+e2e    the same metric through the public C-ABI with host (pinned) buffers:
+       every step uploads the graph (edges, tables, priors), builds the
+       destination-sorted layout on the GPU, runs, and reads the beliefs back.
+Multi-GPU: independent replicas, one per rank (weak scaling), no collective
+on the data path; the timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "edge-msg updates/s"
+UNIT = "edge-msg updates/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["bp", "reference"], default="bp")
+    ap.add_argument("--iterations", type=int, default=100)
+    ap.add_argument("--nodes", type=int, default=1 << 24)
+    ap.add_argument("--edges", type=int, default=1 << 26)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload_name(a):
+    return (f"loopy BP, power-law out-degree graph: {a.nodes:,} nodes, {a.edges:,} edges, 2 states, "
+            f"{a.iterations} fixed iterations, seed 1")
+
+
+def measured_hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def profiled_traffic(name):
+    """DRAM bytes per launch of the flooding kernel from the committed ncu
+    summary (profiles/<name>), or None."""
+    p = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("traffic_bytes_per_launch:"):
+            return float(line.split(":", 1)[1])
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) == 7:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[3 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def flood_bytes_per_iteration(V, E, S):
+    """Compulsory HBM bytes of one fused flooding iteration (loopy.cu header)."""
+    return E * (4 * S * S + 4 + 4 * S * 3) + V * (4 + 4 * S * 3)
+
+
+# ---------------------------------------------------------------- CPU side
+def reference_sample(iterations=None, target_s=10.0):
+    """The reference's own graph.c (OpenMP build, all host cores) on a bounded
+    sample of the same workload: 1,048,576 nodes / 4,194,304 edges of the same
+    generator, fixed iterations.  Returns the baseline dict or None."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    import belief_network_wrapper as W
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    kind = "reference"
+    if O.reference_available(openmp=True):
+        ref = O.Reference(openmp=True)
+    else:
+        kind, cores = "port", 1
+        ref = None
+    net = W.bp.synth.power_law_loopy(1 << 20, 1 << 22, 2, 0.10, seed=1)
+
+    def run(iters):
+        if ref is not None:
+            g = ref.build_graph(net)
+            t0 = time.perf_counter()
+            ref.lib.init_previous_edge(g)
+            ref.lib.loopy_propagate_until(g, 0.0, iters)
+            dt = time.perf_counter() - t0
+            ref.lib.graph_destroy(g)
+            return dt
+        R = O.Restatement()
+        og = O.OracleGraph(net)
+        t0 = time.perf_counter()
+        R.loopy(og, 0.0, iters)
+        return time.perf_counter() - t0
+
+    if iterations is None:
+        probe = run(2)
+        iterations = int(max(2, min(200, target_s / max(probe / 2, 1e-6))))
+    dt = run(iterations)
+    return {"value": net.E * iterations / dt, "unit": UNIT, "cores": int(os.environ.get("OMP_NUM_THREADS", cores))
+            if kind == "reference" else 1, "kind": kind,
+            "sample": f"{net.V:,} nodes / {net.E:,} edges of the same generator, {iterations} fixed iterations, "
+                      f"init_previous_edge + loopy_propagate_until timed ({dt:.2f} s)",
+            "seconds": dt, "iterations": iterations}
+
+
+def run_reference_arm(a, rank, world):
+    if rank != 0:
+        return 0
+    iters = None
+    steps = []
+    for i in range(a.warmup + a.steps):
+        r = reference_sample(iterations=iters, target_s=3.0)
+        iters = r["iterations"]
+        if i >= a.warmup:
+            steps.append(r)
+    tot = sum(s["seconds"] for s in steps)
+    value = sum(s["value"] * s["seconds"] for s in steps) / tot
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * tot / len(steps),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": {"workload": workload_name(a), "arm": "reference CPU (OpenMP graph.c)",
+                                            "step": steps[0]["sample"]},
+            "cpu_baseline": {k: steps[0][k] for k in ("kind", "cores", "sample")} | {"value": value, "unit": UNIT},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------- GPU side
+def main():
+    a = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        return run_reference_arm(a, rank, world)
+
+    import torch
+    import belief_network_wrapper as W
+    from belief_propagation_b200.engine import BPGraph
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    t0 = time.time()
+    net = W.bp.synth.power_law_loopy(a.nodes, a.edges, 2, 0.10, seed=1)
+    V, E, S = net.V, net.E, 2
+    gen_s = time.time() - t0
+    # a dedicated stream: the library's kernels, the CUDA graphs it captures
+    # and the timing events all live on it
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    handle = stream.cuda_stream
+
+    # ---- resident graph
+    g = BPGraph(V, net.src, net.dst, net.joint, uniform_states=2, stream=handle)
+    prior = torch.from_numpy(net.beliefs).cuda()
+
+    def step():
+        g.set_beliefs(prior)
+        g.init_messages()
+        return g.loopy(0.0, a.iterations, delta="f64")
+
+    for _ in range(a.warmup):
+        step()
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    ev0.record(stream)
+    kernel_ms = []
+    for _ in range(a.steps):
+        r = step()
+        kernel_ms.append(r["elapsed_ms"] / max(r["executed"], 1))
+    ev1.record(stream)
+    barrier()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / a.steps
+    updates = float(E) * a.iterations * world
+    value = updates / (ms_per_step / 1e3)
+
+    # ---- roofline of the flooding kernel (one launch = one iteration)
+    it_ms = statistics.median(kernel_ms)
+    algo = flood_bytes_per_iteration(V, E, S)
+    achieved = algo / (it_ms / 1e3) / 1e9
+    peak, peak_src = measured_hbm_peak()
+    traffic = profiled_traffic("k_flood_power_law_traffic.txt")
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "kernel": "k_flood<2,true>", "peak_source": peak_src,
+                "algorithmic_bytes_per_launch": algo, "launch_ms": it_ms}
+    g.close()
+    del prior
+    torch.cuda.empty_cache()
+
+    # ---- end to end through the C-ABI with host buffers
+    e2e = None
+    if not a.no_e2e:
+        pin = lambda x: torch.from_numpy(np.ascontiguousarray(x)).pin_memory()
+        src_h, dst_h, joint_h, bel_h = pin(net.src), pin(net.dst), pin(net.joint), pin(net.beliefs)
+        out_h = torch.empty((V, S), dtype=torch.float32).pin_memory()
+
+        def e2e_step():
+            g2 = BPGraph(V, src_h, dst_h, joint_h, uniform_states=2, stream=handle)
+            g2.set_beliefs(bel_h)
+            g2.init_messages()
+            g2.loopy(0.0, a.iterations, delta="f64")
+            g2.beliefs(out=out_h)
+            g2.close()
+
+        e2e_step()
+        barrier()
+        t0 = time.perf_counter()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(a.e2e_steps):
+            e2e_step()
+        e1.record(stream)
+        barrier()
+        ems = e0.elapsed_time(e1) / a.e2e_steps
+        wall = (time.perf_counter() - t0) / a.e2e_steps * 1e3
+        ems = max(ems, wall)
+        if dist is not None:
+            t = torch.tensor([ems], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": float(E) * a.iterations * world / (ems / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": int(E * (4 + 4 + 4 * S * S) + V * 4 * S), "d2h_bytes_per_step": int(V * 4 * S),
+               "ms_per_step": ems}
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        try:
+            cpu = reference_sample()
+            cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        except Exception as ex:  # reported, not fatal
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "unavailable", "sample": str(ex)[:200]}
+
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    launches_per_step = 1 + 1 + 1 + a.iterations   # set_beliefs, init, gather, flood x iterations
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": workload_name(a), "nodes": V, "edges": E, "states": S,
+                       "iterations": a.iterations, "l2": "inputs larger than L2 (working set ~3.4 GB per replica)",
+                       "parallelism": f"replicas x{world}", "generator_s": round(gen_s, 1)},
+            "hbm_gbs_algorithmic": achieved, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": launches_per_step * a.steps, "clocks": clk}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

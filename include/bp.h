@@ -1,0 +1,168 @@
+/*
+ * bp.h -- device-resident C-ABI of the B200 belief-propagation engine.
+ *
+ * graph.h is the drop-in (the reference's API, host struct layout kept);
+ * this header is the layer underneath it, usable directly by callers that
+ * want the graph to stay in GPU memory between calls, pass device pointers,
+ * or run the batched / differentiable modes.  Plain C types only: pointers,
+ * sizes, status codes.  `memory` arguments say whether a pointer is host
+ * (BP_MEM_HOST) or device (BP_MEM_DEVICE) memory; `stream` arguments are
+ * cudaStream_t values passed as void* (NULL = the graph's own stream).
+ *
+ * Layouts
+ *   beliefs   [V][ld]  node v uses slots [0, S_v); slots at or beyond S_v
+ *             are read as zero and written as zero
+ *   messages  [E][ld]  in edge-id (insertion) order, edge e uses [0, S_src(e))
+ *   joint     per edge, rows i < S_src, columns j < S_dst, row stride and
+ *             edge stride given by the caller (MAX_STATES and MAX_STATES^2
+ *             for struct graph's edges_joint_probabilities)
+ *
+ * Every entry point returns a bp_status; bp_last_error() gives the message
+ * of the most recent failure on the calling thread.
+ */
+#ifndef BP_H_
+#define BP_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BP_MAX_STATES 10
+
+typedef enum {
+    BP_OK = 0,
+    BP_ERR_INVALID = 1,     /* null pointer, bad enum, index out of range */
+    BP_ERR_SHAPE = 2,       /* state count 0 or > BP_MAX_STATES, sizes too large */
+    BP_ERR_CUDA = 3,        /* a CUDA runtime call failed */
+    BP_ERR_NOMEM = 4,       /* device allocation failed */
+    BP_ERR_NO_DEVICE = 5,   /* no CUDA device */
+    BP_ERR_GRAPH = 6,       /* tree levels: a node is unreachable from the seed set */
+    BP_ERR_STATE = 7,       /* call out of order (e.g. a tree level before levels exist) */
+    BP_ERR_TIMEOUT = 8      /* a bounded device wait gave up */
+} bp_status;
+
+typedef enum { BP_MEM_HOST = 0, BP_MEM_DEVICE = 1 } bp_memory;
+
+typedef enum {
+    BP_SCHEDULE_NODE = 0,   /* loopy_propagate_until / _acc (graph.c:1121, :1326) */
+    BP_SCHEDULE_EDGE = 1    /* loopy_propagate_until_edge / _edge_acc (graph.c:1186, :1444) */
+} bp_schedule;
+
+typedef enum {
+    BP_DELTA_AUTO = 0,       /* SERIAL_F32 up to 2^20 message entries, F64 above */
+    BP_DELTA_SERIAL_F32 = 1, /* the reference's own fp32 sum in edge order: same
+                                iteration count as the reference, always */
+    BP_DELTA_F64 = 2         /* parallel fp64 sum, deterministic order */
+} bp_delta_mode;
+
+typedef enum { BP_SYNC_EAGER = 0, BP_SYNC_LAZY = 1 } bp_sync_mode;
+
+typedef struct bp_graph bp_graph;
+
+typedef struct {
+    uint32_t num_nodes;
+    uint32_t num_edges;
+    uint32_t uniform_states;          /* states of every node when node_num_states is NULL */
+    const uint32_t *node_num_states;  /* [num_nodes] or NULL */
+    const uint32_t *edge_src;         /* [num_edges] */
+    const uint32_t *edge_dst;         /* [num_edges] */
+    const float *edge_joint;          /* see "Layouts" */
+    uint32_t joint_row_stride;        /* floats between rows of one table */
+    uint64_t joint_edge_stride;       /* floats between consecutive edges' tables */
+    /* optional CSR as in struct graph (node_list has num_nodes entries, the
+     * last row ends at num_edges); NULL = stable sort by node, which is the
+     * order set_up_*_nodes_to_edges produce */
+    const uint32_t *dest_node_list, *dest_edge_list;
+    const uint32_t *src_node_list, *src_edge_list;
+    int32_t memory;                   /* bp_memory of every pointer above */
+} bp_graph_desc;
+
+typedef struct {
+    float tolerance;          /* the reference's `convergence` */
+    uint32_t max_iterations;
+    uint32_t check_every;     /* 1: loopy_propagate_until[_edge]; 10 (BATCH_SIZE): the _acc variants */
+    int32_t schedule;         /* bp_schedule */
+    int32_t delta_mode;       /* bp_delta_mode */
+    int32_t verbose;          /* print the reference's "No Convergence" line */
+    uint32_t graph_chunk;     /* iterations per CUDA-graph launch; 0 = automatic */
+    int32_t reserved;
+} bp_loopy_options;
+
+typedef struct {
+    uint32_t iterations;      /* the reference's return value */
+    uint32_t executed;        /* iterations actually run */
+    int32_t converged;        /* 1 when the stopping rule fired */
+    float delta;              /* the reference's `delta` at return */
+    float previous_delta;     /* the reference's `previous_delta` at return */
+    double delta_f64;
+    float elapsed_ms;         /* device time of the iteration loop */
+} bp_loopy_result;
+
+typedef struct {
+    uint32_t num_levels;
+    uint32_t num_waves;       /* kernel launches the forward + backward passes used */
+    float elapsed_ms;
+} bp_tree_result;
+
+const char *bp_status_string(int status);
+const char *bp_last_error(void);
+int bp_version(void);
+
+/* ---- graph lifetime -------------------------------------------------- */
+int bp_graph_create(bp_graph **out, const bp_graph_desc *desc, void *stream);
+void bp_graph_destroy(bp_graph *g);
+int bp_graph_info(const bp_graph *g, uint32_t *num_nodes, uint32_t *num_edges,
+                  uint32_t *max_states, uint32_t *uniform_states);
+int bp_set_stream(bp_graph *g, void *stream);
+int bp_synchronize(bp_graph *g);
+/* bytes of device memory the graph holds */
+int bp_graph_device_bytes(const bp_graph *g, uint64_t *bytes);
+
+/* ---- state ----------------------------------------------------------- */
+int bp_set_beliefs(bp_graph *g, const float *beliefs, uint32_t ld, int memory);
+int bp_get_beliefs(bp_graph *g, float *beliefs, uint32_t ld, int memory);
+/* the two message arrays: slot 0 and slot 1 (edges_messages and
+ * last_edges_messages of struct graph); `latest` is the slot
+ * *previous_edge_messages points at */
+int bp_set_messages(bp_graph *g, int slot, const float *messages, uint32_t ld, int memory);
+int bp_get_messages(bp_graph *g, int slot, float *messages, uint32_t ld, int memory);
+int bp_set_latest_slot(bp_graph *g, int slot);
+int bp_get_latest_slot(const bp_graph *g, int *slot);
+
+/* ---- loopy BP -------------------------------------------------------- */
+void bp_loopy_default_options(bp_loopy_options *opt);
+/* init_previous_edge (graph.c:725-751): latest = normalise(J . belief_src) */
+int bp_init_messages(bp_graph *g);
+/* loopy_propagate_until / _edge / _acc / _edge_acc (graph.c:1186-1547) */
+int bp_loopy(bp_graph *g, const bp_loopy_options *opt, bp_loopy_result *res);
+
+/* ---- tree BP --------------------------------------------------------- */
+/* init_levels_to_nodes (graph.c:806-827); levels may be NULL (kept on device
+ * side only), else receives 2*V entries in the reference's layout */
+int bp_tree_build_levels(bp_graph *g, uint32_t *levels, uint32_t *num_levels);
+/* use level lists computed elsewhere (struct graph's levels_to_nodes) */
+int bp_tree_set_levels(bp_graph *g, const uint32_t *levels, uint32_t num_levels);
+int bp_tree_start(bp_graph *g);                       /* graph.c:376-424 */
+int bp_tree_level(bp_graph *g, uint32_t level);       /* graph.c:524-538 */
+int bp_tree_reset_visited(bp_graph *g);               /* graph.c:598-605 */
+int bp_tree_marginalize(bp_graph *g);                 /* graph.c:588-596 */
+/* the whole driver sequence (c_benchmark/main.c:224-236) in one call */
+int bp_tree(bp_graph *g, bp_tree_result *res);
+int bp_set_visited(bp_graph *g, const char *visited); /* host [V] */
+int bp_get_visited(bp_graph *g, char *visited);       /* host [V] */
+
+/* ---- drop-in support (struct graph from graph.h) ---------------------- */
+struct graph;
+int bp_set_sync_mode(struct graph *g, int mode);
+int bp_sync_host(struct graph *g);
+/* the device mirror of a struct graph, creating it if needed */
+int bp_graph_of(struct graph *g, bp_graph **out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BP_H_ */

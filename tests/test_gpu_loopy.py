@@ -1,0 +1,197 @@
+"""Loopy BP on the GPU against the oracle: bit-exact beliefs and messages and
+the same returned iteration index as the reference on the same inputs.
+
+Slot convention: slot 0 = struct graph's edges_messages, slot 1 =
+last_edges_messages; the reference starts with *previous_edge_messages ->
+last_edges_messages, so init_previous_edge writes slot 1."""
+import numpy as np
+import pytest
+
+from conftest import load_golden
+import golden_nets as GN
+
+pytestmark = pytest.mark.gpu
+
+
+def gpu_loopy(bp, net, tol, max_it, check_every=1, schedule="node", delta="serial", init=True,
+              msgs=None, graph_chunk=0):
+    from belief_propagation_b200.engine import BPGraph
+    g = BPGraph.from_network(net)
+    try:
+        if msgs is not None:
+            g.set_messages(1, msgs[0][:, : net.s_max])
+            g.set_messages(0, msgs[1][:, : net.s_max])
+        g.latest_slot = 1
+        if init:
+            g.init_messages()
+        r = g.loopy(tol, max_it, check_every=check_every, schedule=schedule, delta=delta,
+                    graph_chunk=graph_chunk)
+        out = dict(r, beliefs=g.beliefs(), slot1=g.messages(1), slot0=g.messages(0), latest=g.latest_slot)
+    finally:
+        g.close()
+    return out
+
+
+def assert_same(gpu, ora, S):
+    np.testing.assert_array_equal(gpu["beliefs"][:, :S], ora["beliefs"][:, :S])
+    np.testing.assert_array_equal(gpu["slot1"][:, :S], ora["prev_arr"][:, :S])
+    np.testing.assert_array_equal(gpu["slot0"][:, :S], ora["cur_arr"][:, :S])
+    assert gpu["iterations"] == ora["ret"]
+    assert gpu["executed"] == ora["executed"]
+
+
+def test_loopy_random_10k_matches_reference_fixture(bp):
+    """The reference-runnable workload: 10,000 nodes, 40,000 edges, 2 states,
+    tol 1e-3, max 100 -- against the reference's own outputs."""
+    fx = load_golden("loopy_random_10000_40000.npz")
+    net = GN.network_from_fixture(fx)
+    for delta in ("serial", "f64"):
+        r = gpu_loopy(bp, net, float(fx["loopy_tol"]), int(fx["loopy_max_it"]), delta=delta)
+        assert r["iterations"] == int(fx["loopy_ret"])
+        np.testing.assert_array_equal(r["beliefs"], fx["loopy_beliefs"])
+        latest = r["slot1"] if r["latest"] == 1 else r["slot0"]
+        older = r["slot0"] if r["latest"] == 1 else r["slot1"]
+        np.testing.assert_array_equal(latest, fx["loopy_latest"])
+        np.testing.assert_array_equal(older, fx["loopy_older"])
+
+
+@pytest.mark.parametrize("name", ["loopy_random_s3_500.npz", "bif_asia.npz", "bif_cancer.npz",
+                                  "bif_earthquake.npz", "bif_sachs.npz", "example_4node.npz",
+                                  "tree_random_2000.npz"])
+def test_loopy_fixtures(bp, name):
+    fx = load_golden(name)
+    net = GN.network_from_fixture(fx)
+    r = gpu_loopy(bp, net, float(fx["loopy_tol"]), int(fx["loopy_max_it"]))
+    assert r["iterations"] == int(fx["loopy_ret"])
+    S = fx["loopy_beliefs"].shape[1]
+    np.testing.assert_array_equal(r["beliefs"][:, :S], fx["loopy_beliefs"])
+
+
+CASES = [
+    dict(V=3000, E=12000, S=2, seed=31),
+    dict(V=1000, E=5000, S=3, seed=32),
+    dict(V=800, E=4000, S=4, seed=33),
+    dict(V=500, E=2500, S=5, seed=34),
+    dict(V=400, E=2000, S=8, seed=35),
+    dict(V=300, E=1201, S=10, seed=36),
+]
+
+
+@pytest.mark.parametrize("case", CASES, ids=lambda c: f"S{c['S']}")
+@pytest.mark.parametrize("tol,max_it", [(1e-3, 40), (0.0, 15)])
+def test_loopy_node_parity(bp, synth, restatement, O, case, tol, max_it):
+    net = synth.random_loopy(case["V"], case["E"], case["S"], 0.1, seed=case["seed"])
+    ora = restatement.loopy(O.OracleGraph(net), tol, max_it)
+    gpu = gpu_loopy(bp, net, tol, max_it)
+    assert_same(gpu, ora, case["S"])
+
+
+@pytest.mark.parametrize("check,sched", [(10, "node"), (1, "edge"), (10, "edge")])
+@pytest.mark.parametrize("case", CASES[:3] + CASES[4:5], ids=lambda c: f"S{c['S']}")
+def test_loopy_variants_parity(bp, synth, restatement, O, case, check, sched):
+    net = synth.random_loopy(case["V"], case["E"], case["S"], 0.1, seed=case["seed"])
+    for tol, max_it in ((1e-3, 60), (0.0, 25)):
+        ora = restatement.loopy(O.OracleGraph(net), tol, max_it, check_every=check, schedule=sched)
+        gpu = gpu_loopy(bp, net, tol, max_it, check_every=check, schedule=sched)
+        assert_same(gpu, ora, case["S"])
+
+
+def test_loopy_edge_byte_copy_odd_edges(bp, synth, restatement, O):
+    """E odd: the reference's byte-count memcpy copies half of one float."""
+    net = synth.random_loopy(101, 401, 2, 0.1, seed=40)
+    ora = restatement.loopy(O.OracleGraph(net), 0.0, 7, schedule="edge")
+    gpu = gpu_loopy(bp, net, 0.0, 7, schedule="edge")
+    assert_same(gpu, ora, 2)
+
+
+def test_loopy_mixed_states(bp, synth, restatement, O):
+    """Nodes with different state counts: the zero-padding convention, same
+    as the restatement."""
+    nets = synth.batch_of_networks(count=1, v_range=(300, 300), seed=3)
+    net = nets[0]
+    rng = np.random.default_rng(5)
+    ns = rng.choice(np.array([2, 3, 4, 8], np.uint32), size=net.V)
+    S = 8
+    b = rng.random((net.V, S), dtype=np.float32) * (np.arange(S)[None] < ns[:, None])
+    j = rng.random((net.E, S, S), dtype=np.float32)
+    j *= (np.arange(S)[None, :, None] < ns[net.src][:, None, None])
+    j *= (np.arange(S)[None, None, :] < ns[net.dst][:, None, None])
+    mixed = synth.Network(ns, b.astype(np.float32), net.observed, net.src, net.dst, j.astype(np.float32))
+    for check, sched in ((1, "node"), (10, "node"), (1, "edge")):
+        ora = restatement.loopy(O.OracleGraph(mixed), 1e-3, 30, check_every=check, schedule=sched)
+        gpu = gpu_loopy(bp, mixed, 1e-3, 30, check_every=check, schedule=sched)
+        assert_same(gpu, ora, S)
+
+
+def test_loopy_hub_node_chunked(bp, synth, restatement, O):
+    """A node with far more in-edges than one tile's shared memory holds."""
+    V = 9000
+    src = np.arange(1, V, dtype=np.uint32)
+    dst = np.zeros(V - 1, np.uint32)
+    rng = np.random.default_rng(9)
+    extra_s = rng.integers(0, V, 4000).astype(np.uint32)
+    extra_d = rng.integers(1, V, 4000).astype(np.uint32)
+    keep = extra_s != extra_d
+    src = np.concatenate([src, extra_s[keep]])
+    dst = np.concatenate([dst, extra_d[keep]])
+    key = src.astype(np.int64) * V + dst
+    _, first = np.unique(key, return_index=True)
+    first.sort()
+    src, dst = src[first], dst[first]
+    E = len(src)
+    j = rng.random((E, 2, 2), dtype=np.float32)
+    j /= j.sum(axis=2, keepdims=True)
+    b = rng.random((V, 2), dtype=np.float32) + 0.5
+    net = synth.Network(np.full(V, 2, np.uint32), b, np.zeros(V, np.uint8), src, dst, j)
+    ora = restatement.loopy(O.OracleGraph(net), 0.0, 6)
+    gpu = gpu_loopy(bp, net, 0.0, 6)
+    assert_same(gpu, ora, 2)
+
+
+def test_loopy_nan_messages_skipped(bp, synth, restatement, O):
+    """NaN entries in incoming messages are skipped by combine (graph.c:455)
+    and count 0 in the delta."""
+    net = synth.random_loopy(200, 800, 2, 0.1, seed=41)
+    rng = np.random.default_rng(2)
+    prev = rng.random((net.E, 10), dtype=np.float32)
+    prev[rng.random(net.E) < 0.05, 0] = np.nan
+    cur = np.zeros((net.E, 10), np.float32)
+    ora = restatement.loopy(O.OracleGraph(net), 1e-3, 5, init=False, msgs=(prev, cur))
+    gpu = gpu_loopy(bp, net, 1e-3, 5, init=False, msgs=(prev, cur))
+    np.testing.assert_array_equal(gpu["beliefs"][:, :2], ora["beliefs"][:, :2])
+    assert gpu["iterations"] == ora["ret"]
+
+
+@pytest.mark.parametrize("V,E", [(1, 0), (5, 0), (2, 1), (2, 2)])
+def test_loopy_degenerate_graphs(bp, synth, restatement, O, V, E):
+    rng = np.random.default_rng(V * 10 + E)
+    src = np.array([0, 1][:E], np.uint32)
+    dst = np.array([1, 0][:E], np.uint32)
+    j = rng.random((E, 2, 2), dtype=np.float32)
+    b = rng.random((V, 2), dtype=np.float32)
+    net = synth.Network(np.full(V, 2, np.uint32), b, np.zeros(V, np.uint8), src, dst, j)
+    for tol, max_it, check in ((1e-3, 10, 1), (0.0, 3, 1), (1e-3, 0, 1), (1e-3, 25, 10)):
+        ora = restatement.loopy(O.OracleGraph(net), tol, max_it, check_every=check)
+        gpu = gpu_loopy(bp, net, tol, max_it, check_every=check)
+        assert_same(gpu, ora, 2)
+
+
+def test_loopy_graph_chunks_agree(bp, synth):
+    """The CUDA-graph chunk size changes nothing but launch grouping."""
+    net = synth.random_loopy(2000, 8000, 2, 0.1, seed=42)
+    a = gpu_loopy(bp, net, 1e-3, 50, graph_chunk=1)
+    b = gpu_loopy(bp, net, 1e-3, 50, graph_chunk=7)
+    c = gpu_loopy(bp, net, 1e-3, 50, graph_chunk=64)
+    for x in (b, c):
+        assert x["iterations"] == a["iterations"]
+        np.testing.assert_array_equal(x["beliefs"], a["beliefs"])
+
+
+def test_loopy_power_law_scale(bp, synth, restatement, O):
+    """Power-law out-degree graph, fixed iterations, 1M edges."""
+    net = synth.power_law_loopy(1 << 18, 1 << 20, 2, 0.1, seed=1)
+    ora = restatement.loopy(O.OracleGraph(net), 0.0, 5)
+    gpu = gpu_loopy(bp, net, 0.0, 5, delta="f64")
+    np.testing.assert_array_equal(gpu["beliefs"][:, :2], ora["beliefs"][:, :2])
+    np.testing.assert_array_equal(gpu["slot1"][:, :2], ora["prev_arr"][:, :2])
+    assert abs(gpu["delta_f64"] - ora["delta"]) <= 1e-4 * max(1.0, ora["delta"])
