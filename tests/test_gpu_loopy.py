@@ -194,4 +194,8 @@ def test_loopy_power_law_scale(bp, synth, restatement, O):
     gpu = gpu_loopy(bp, net, 0.0, 5, delta="f64")
     np.testing.assert_array_equal(gpu["beliefs"][:, :2], ora["beliefs"][:, :2])
     np.testing.assert_array_equal(gpu["slot1"][:, :2], ora["prev_arr"][:, :2])
-    assert abs(gpu["delta_f64"] - ora["delta"]) <= 1e-4 * max(1.0, ora["delta"])
+    # the GPU's fp64 delta against an fp64 sum of the oracle's own |m_t - m_(t-1)|
+    # (the reference's fp32 serial sum of 2M terms carries ~1e-3 relative error)
+    d = np.abs(ora["prev_arr"][:, :2].astype(np.float64) - ora["cur_arr"][:, :2].astype(np.float64))
+    d64 = float(np.nan_to_num(d).sum())
+    assert abs(gpu["delta_f64"] - d64) <= 1e-9 * max(1.0, d64)

@@ -81,10 +81,11 @@ def test_tree_unreachable_reports_error(bp, synth):
     forever; the engine returns BP_ERR_GRAPH."""
     from belief_propagation_b200.engine import BPGraph
     from belief_propagation_b200.native import BPError
-    # a 4-cycle in both directions plus a triangle whose nodes all have in-degree 3
-    src = [0, 1, 2, 3, 1, 2, 3, 0, 4, 5, 6, 5, 6, 4, 4, 5]
-    dst = [1, 2, 3, 0, 0, 1, 2, 3, 5, 6, 4, 4, 5, 6, 0, 0]
-    V = 7
+    # a complete directed graph on 4 nodes: every in-degree is 3, so no node
+    # qualifies as a level-0 seed and nothing is ever reached
+    src = [u for u in range(4) for w in range(4) if u != w]
+    dst = [w for u in range(4) for w in range(4) if u != w]
+    V = 4
     src = np.array(src, np.uint32)
     dst = np.array(dst, np.uint32)
     net = synth.Network(np.full(V, 2, np.uint32), np.ones((V, 2), np.float32), np.zeros(V, np.uint8), src, dst,
