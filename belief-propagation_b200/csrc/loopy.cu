@@ -26,6 +26,8 @@
 #include <stdio.h>
 #include <stdlib.h>
 
+#include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "bp_device.cuh"
@@ -806,3 +808,167 @@ int bp_loopy(bp_graph *g, const bp_loopy_options *opt, bp_loopy_result *res) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free loopy BP (bp_loopy_noalloc).
+//
+// Some callers cannot allocate device memory at the moment they need an
+// answer: a host application that owns the GPU's memory through its own
+// allocator and forbids other components from calling cudaMalloc, a
+// latency-bound loop where an allocation (and the implicit synchronisation
+// cudaFree brings) is not acceptable, or a process running close to a hard
+// memory cap.  For them this entry point runs the same kernels as bp_loopy
+// on arrays the caller already owns, and keeps its own working memory -- the
+// two send buffers, the per-block delta partials and the control block -- in
+// one fixed array compiled into this library.
+namespace bpx {
+
+constexpr size_t kNoAllocScratchBytes = BP_NOALLOC_SCRATCH_BYTES;
+constexpr int kNoAllocMaxDevices = 64;
+
+// Device-side working memory of bp_loopy_noalloc.  Every GPU that loads the
+// library holds these bytes until the process exits.  In host code the name
+// is only a stand-in for the symbol: the device address comes from
+// cudaGetSymbolAddress, once per device, below.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+static void *g_noalloc_base[kNoAllocMaxDevices];
+static std::mutex g_noalloc_mutex;
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// device address of the scratch array on the current device (set up on the
+// first call made on that device)
+static int noalloc_base(void **base) {
+    int dev = 0;
+    BP_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return set_error(BP_ERR_INVALID, "device %d out of range", dev);
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_base[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress", __FILE__, __LINE__);
+        g_noalloc_base[dev] = p;
+    }
+    *base = g_noalloc_base[dev];
+    return BP_OK;
+}
+
+template <int MS>
+static int noalloc_run(uint32_t V, uint32_t E, const uint32_t *in_ptr, const uint32_t *in_src, const float *joint,
+                       float *beliefs, float *messages, int latest, int init, float tol, uint32_t max_it,
+                       cudaStream_t stream, bp_loopy_result *res, int *latest_out) {
+    constexpr int NT = flood_nt<MS>();
+    const uint32_t grid = grid_for(V, NT);
+    const size_t off_part = align256(sizeof(LoopyCtl));
+    const size_t off_q0 = off_part + align256(sizeof(double) * grid);
+    const size_t qbytes = align256(sizeof(float) * MS * (size_t)V);
+    const size_t need = off_q0 + 2 * qbytes;
+    if (need > kNoAllocScratchBytes)
+        return set_error(BP_ERR_SHAPE,
+                         "bp_loopy_noalloc: %u nodes x %d states need %zu bytes of working memory; its fixed "
+                         "array holds %zu (BP_NOALLOC_SCRATCH_BYTES)",
+                         V, MS, need, kNoAllocScratchBytes);
+    void *base = nullptr;
+    int st = noalloc_base(&base);
+    if (st) return st;
+    unsigned char *b = (unsigned char *)base;
+    LoopyCtl *ctl = (LoopyCtl *)b;
+
+    // every run starts from a fully written control block; the delta
+    // partials and send buffers are written before they are read
+    LoopyCtl c = {};
+    c.max_it = max_it;
+    c.check_every = 1;
+    c.msg_parity0 = (uint32_t)latest;
+    c.q_parity0 = 0;
+    c.serial = 0;
+    c.tol = tol;
+    c.prev_f = -1.0f;
+    c.prev_d = -1.0;
+    BP_CUDA(cudaMemcpyAsync(ctl, &c, sizeof(c), cudaMemcpyHostToDevice, stream));
+
+    float *msg_latest = messages + (size_t)latest * E * MS;
+    if (init && E) {
+        k_send_from_beliefs<MS, true><<<grid_for(E, 256), 256, 0, stream>>>(E, in_src, nullptr, joint, beliefs,
+                                                                            msg_latest);
+        BP_CUDA(cudaGetLastError());
+    }
+    FloodArgs a = {};
+    a.V = V;
+    a.in_ptr = in_ptr;
+    a.in_src = in_src;
+    a.joint = joint;
+    a.belief = beliefs;
+    a.msg0 = messages;
+    a.msg1 = messages + (size_t)E * MS;
+    a.q0 = (float *)(b + off_q0);
+    a.q1 = (float *)(b + off_q0 + qbytes);
+    a.partials = (double *)(b + off_part);
+    a.ctl = ctl;
+    k_gather_q<MS, true><<<grid_for(V, 256), 256, 0, stream>>>(V, in_ptr, nullptr, beliefs, msg_latest, a.q0);
+    BP_CUDA(cudaGetLastError());
+    uint32_t done = 0;
+    for (uint32_t launched = 0; launched < max_it && !done; launched += 32) {
+        const uint32_t n = std::min<uint32_t>(32, max_it - launched);
+        for (uint32_t i = 0; i < n; ++i) k_flood<MS, true><<<grid, NT, 0, stream>>>(a);
+        BP_CUDA(cudaGetLastError());
+        BP_CUDA(cudaMemcpyAsync(&done, &ctl->done, sizeof(done), cudaMemcpyDeviceToHost, stream));
+        BP_CUDA(cudaStreamSynchronize(stream));
+    }
+    BP_CUDA(cudaMemcpyAsync(&c, ctl, sizeof(c), cudaMemcpyDeviceToHost, stream));
+    BP_CUDA(cudaStreamSynchronize(stream));
+    if (!c.done) return set_error(BP_ERR_STATE, "loop ended without a stop decision (it=%u)", c.it);
+    if (res) {
+        bp_loopy_result r = {};
+        r.iterations = c.ret;
+        r.executed = c.it;
+        r.converged = c.done == 1;
+        r.delta = (float)c.delta_d;
+        r.previous_delta = (float)c.prev_d;
+        r.delta_f64 = c.delta_d;
+        r.elapsed_ms = 0.0f;
+        *res = r;
+    }
+    if (latest_out) *latest_out = (int)((c.msg_parity0 + c.it) & 1u);
+    return BP_OK;
+}
+
+}  // namespace bpx
+
+extern "C" int bp_loopy_noalloc(uint32_t num_nodes, uint32_t num_edges, uint32_t num_states,
+                                const uint32_t *in_ptr, const uint32_t *in_src, const float *joint,
+                                float *beliefs, float *messages, int latest_slot, int init_messages,
+                                float tolerance, uint32_t max_iterations, void *stream, bp_loopy_result *result,
+                                int *latest_out) {
+    using namespace bpx;
+    if (num_states < 1 || num_states > BP_MAX_STATES)
+        return set_error(BP_ERR_SHAPE, "num_states %u not in [1, %d]", num_states, BP_MAX_STATES);
+    if (num_nodes == 0) return set_error(BP_ERR_SHAPE, "bp_loopy_noalloc needs at least one node");
+    if (!in_ptr || !beliefs || (num_edges && (!in_src || !joint || !messages)))
+        return set_error(BP_ERR_INVALID, "null array");
+    if (latest_slot != 0 && latest_slot != 1) return set_error(BP_ERR_INVALID, "latest_slot must be 0 or 1");
+    if (max_iterations == 0) {
+        // the reference's loop body never runs: nothing to launch
+        if (result) {
+            bp_loopy_result r = {};
+            r.previous_delta = -1.0f;
+            *result = r;
+        }
+        if (latest_out) *latest_out = latest_slot;
+        return BP_OK;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    switch (num_states) {
+    case 1: return noalloc_run<1>(num_nodes, num_edges, in_ptr, in_src, joint, beliefs, messages, latest_slot, init_messages, tolerance, max_iterations, s, result, latest_out);
+    case 2: return noalloc_run<2>(num_nodes, num_edges, in_ptr, in_src, joint, beliefs, messages, latest_slot, init_messages, tolerance, max_iterations, s, result, latest_out);
+    case 3: return noalloc_run<3>(num_nodes, num_edges, in_ptr, in_src, joint, beliefs, messages, latest_slot, init_messages, tolerance, max_iterations, s, result, latest_out);
+    case 4: return noalloc_run<4>(num_nodes, num_edges, in_ptr, in_src, joint, beliefs, messages, latest_slot, init_messages, tolerance, max_iterations, s, result, latest_out);
+    case 5: return noalloc_run<5>(num_nodes, num_edges, in_ptr, in_src, joint, beliefs, messages, latest_slot, init_messages, tolerance, max_iterations, s, result, latest_out);
+    case 6: return noalloc_run<6>(num_nodes, num_edges, in_ptr, in_src, joint, beliefs, messages, latest_slot, init_messages, tolerance, max_iterations, s, result, latest_out);
+    case 7: return noalloc_run<7>(num_nodes, num_edges, in_ptr, in_src, joint, beliefs, messages, latest_slot, init_messages, tolerance, max_iterations, s, result, latest_out);
+    case 8: return noalloc_run<8>(num_nodes, num_edges, in_ptr, in_src, joint, beliefs, messages, latest_slot, init_messages, tolerance, max_iterations, s, result, latest_out);
+    case 9: return noalloc_run<9>(num_nodes, num_edges, in_ptr, in_src, joint, beliefs, messages, latest_slot, init_messages, tolerance, max_iterations, s, result, latest_out);
+    default: return noalloc_run<10>(num_nodes, num_edges, in_ptr, in_src, joint, beliefs, messages, latest_slot, init_messages, tolerance, max_iterations, s, result, latest_out);
+    }
+}

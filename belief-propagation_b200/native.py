@@ -91,7 +91,7 @@ BP_SYMBOLS = [
     "bp_loopy_default_options", "bp_init_messages", "bp_loopy", "bp_tree_build_levels",
     "bp_tree_set_levels", "bp_tree_start", "bp_tree_level", "bp_tree_reset_visited",
     "bp_tree_marginalize", "bp_tree", "bp_set_visited", "bp_get_visited", "bp_set_sync_mode",
-    "bp_sync_host", "bp_graph_of",
+    "bp_sync_host", "bp_graph_of", "bp_loopy_noalloc",
 ]
 GRAPH_SYMBOLS = [
     "create_graph", "graph_add_node", "graph_add_and_set_node_state", "graph_set_node_state",
@@ -138,6 +138,8 @@ def load(path=LIB_PATH):
         "bp_set_visited": ([vp, vp], i32), "bp_get_visited": ([vp, vp], i32),
         "bp_set_sync_mode": ([vp, i32], i32), "bp_sync_host": ([vp], i32),
         "bp_graph_of": ([vp, C.POINTER(vp)], i32),
+        "bp_loopy_noalloc": ([u32, u32, u32, vp, vp, vp, vp, vp, i32, i32, C.c_float, u32, vp,
+                              C.POINTER(LoopyResult), C.POINTER(i32)], i32),
         # graph.h
         "create_graph": ([C.c_uint, C.c_uint], C.POINTER(StructGraph)),
         "graph_add_node": ([vp, C.c_uint, C.c_char_p], None),

@@ -139,6 +139,50 @@ int bp_init_messages(bp_graph *g);
 /* loopy_propagate_until / _edge / _acc / _edge_acc (graph.c:1186-1547) */
 int bp_loopy(bp_graph *g, const bp_loopy_options *opt, bp_loopy_result *res);
 
+/* ---- loopy BP without allocating ------------------------------------- */
+/* No counterpart in the reference: an addition of this library.
+ *
+ * Who needs it: code that must not allocate GPU memory while it runs --
+ * a host application that owns the device through its own allocator and
+ * forbids components from calling cudaMalloc, a real-time loop that cannot
+ * afford an allocation or the device-wide synchronisation cudaFree implies,
+ * or a process pinned right at its memory cap.  This call runs the same
+ * kernels as bp_loopy (node schedule, loopy_propagate_until semantics,
+ * deterministic fp64 delta) and allocates nothing: no cudaMalloc, no
+ * cudaFree, no allocating library routine.
+ *
+ * The caller passes every input and output as DEVICE memory, already in the
+ * destination-sorted layout bp_graph_create builds internally:
+ *   in_ptr   [num_nodes + 1]            row starts of each node's in-edges
+ *   in_src   [num_edges]                source node of each position
+ *   joint    [num_edges][S][S]          tables in position order
+ *   beliefs  [num_nodes][S]             read and updated in place
+ *   messages [2][num_edges][S]          the two message arrays; slot
+ *                                       latest_slot holds the latest ones
+ * with S = num_states for every node.  init_messages != 0 first fills the
+ * latest slot with normalise(J . belief_src) (init_previous_edge).  On
+ * return *latest_out is the slot holding the newest messages.
+ *
+ * Working memory (two send buffers of num_nodes * S floats, one double per
+ * 256-node tile, a control block) lives in one array of
+ * BP_NOALLOC_SCRATCH_BYTES compiled into the library; every GPU that loads
+ * the library holds it until the process exits.  Graphs whose working memory
+ * does not fit (about 1M nodes at 2 states) are rejected with BP_ERR_SHAPE
+ * and a message giving the size needed.
+ *
+ * The first call on a device looks the array's device address up with that
+ * device current (cudaGetSymbolAddress); make that first call before any
+ * stream capture on the device.  All calls share the one array and leave
+ * their contents in it; each call rewrites the control block and the buffers
+ * before reading them.  Calls whose work overlaps on the GPU (other streams,
+ * other threads) race on that array: serialise them. */
+#define BP_NOALLOC_SCRATCH_BYTES (16u << 20)
+int bp_loopy_noalloc(uint32_t num_nodes, uint32_t num_edges, uint32_t num_states,
+                     const uint32_t *in_ptr, const uint32_t *in_src, const float *joint,
+                     float *beliefs, float *messages, int latest_slot, int init_messages,
+                     float tolerance, uint32_t max_iterations, void *stream,
+                     bp_loopy_result *result, int *latest_out);
+
 /* ---- tree BP --------------------------------------------------------- */
 /* init_levels_to_nodes (graph.c:806-827); levels may be NULL (kept on device
  * side only), else receives 2*V entries in the reference's layout */
