@@ -85,6 +85,26 @@ __device__ __forceinline__ void stv(float *__restrict__ p, const float *v) {
 // graph.c:884-910 (send_message_for_edge), :426-448 (send_message).
 // buf slots at or beyond the source's state count are zero (the reference
 // reads stale slots there, graph.c:851-857).  Slots i >= x come out 0.
+// the same arithmetic on a table already held in registers (row-major MS x MS)
+template <int MS, bool UNI>
+__device__ __forceinline__ void send_msg_regs(const float *j, const float *buf, int x, int y, float *m) {
+    float sum = 0.0f;
+#pragma unroll
+    for (int i = 0; i < MS; ++i) {
+        float partial = 0.0f;
+        if (UNI || i < x) {
+#pragma unroll
+            for (int c = 0; c < MS; ++c)
+                if (UNI || c < y) partial = FADD(partial, FMUL(j[i * MS + c], buf[c]));
+            sum = FADD(sum, partial);
+        }
+        m[i] = partial;
+    }
+    if (sum <= 0.0f) sum = 1.0f;
+#pragma unroll
+    for (int i = 0; i < MS; ++i) m[i] = (UNI || i < x) ? FDIV(m[i], sum) : 0.0f;
+}
+
 template <int MS, bool UNI>
 __device__ __forceinline__ void send_msg(const float *__restrict__ J, const float *buf, int x, int y,
                                          float *m) {

@@ -240,6 +240,154 @@ __global__ void __launch_bounds__(flood_nt<MS>()) k_flood(const FloodArgs a) {
     if (!serial) reduce_and_finalize<NT>(ctl, a.partials, dsum, want, red, &s_last);
 }
 
+// Warp-tiled form of k_flood: each warp owns 32 consecutive destination
+// nodes and their in-edges, so the two phases synchronise a warp instead of
+// the block (the block meets once, for the delta).  Phase 1 issues the loads
+// of U edges per lane before using any of them (source ids, tables and old
+// messages first, then the dependent Q[src] gathers), so each warp keeps
+// U times more bytes in flight; the node's belief is loaded at entry.  The
+// arithmetic per value is k_flood's, in the same order.
+template <int MS> constexpr uint32_t wflood_we() { return MS <= 2 ? 256 : (MS <= 4 ? 192 : 96); }
+template <int MS> constexpr int wflood_unroll() { return MS <= 2 ? 4 : (MS <= 4 ? 2 : 1); }
+
+template <int MS, bool UNI, int U>
+__global__ void __launch_bounds__(256) k_flood_w(const FloodArgs a) {
+    constexpr int NW = 8, NT = 256;
+    constexpr uint32_t WE = wflood_we<MS>();
+    constexpr bool JREG = MS * MS <= 16;
+    __shared__ __align__(16) float sm[NW * WE * MS];
+    __shared__ double red[NW];
+    __shared__ bool s_last;
+
+    LoopyCtl *ctl = a.ctl;
+    if (*(volatile uint32_t *)&ctl->done) return;
+    const uint32_t it = ctl->it, ce = ctl->check_every;
+    const bool serial = ctl->serial != 0;
+    const bool want = (ce <= 1) || ((it + 1) % ce == 0);
+    const int mp = (int)((ctl->msg_parity0 + it) & 1u), qp = (int)((ctl->q_parity0 + it) & 1u);
+    const float *__restrict__ m_old = mp ? a.msg1 : a.msg0;
+    float *__restrict__ m_new = mp ? a.msg0 : a.msg1;
+    const float *__restrict__ q_in = qp ? a.q1 : a.q0;
+    float *__restrict__ q_out = qp ? a.q0 : a.q1;
+
+    const uint32_t V = a.V, lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    float *wsm = sm + warp * (WE * MS);
+    const uint32_t v0 = (blockIdx.x * NW + warp) * 32u;
+    double dsum = 0.0;
+    if (v0 < V) {
+        const uint32_t v = v0 + lane;
+        const bool has = v < V;
+        const uint32_t last = min(v0 + 32u, V) - 1u - v0;
+        uint32_t r0 = 0, r1 = 0;
+        int S = MS;
+        float b[MS];
+#pragma unroll
+        for (int i = 0; i < MS; ++i) b[i] = 0.0f;
+        if (has) {
+            r0 = a.in_ptr[v];
+            r1 = a.in_ptr[v + 1];
+            if (!UNI) S = a.node_s[v];
+            ldv<MS, kStream>(a.belief + (size_t)v * MS, b);
+        }
+        const uint32_t e0 = __shfl_sync(0xffffffffu, r0, 0);
+        const uint32_t e1 = __shfl_sync(0xffffffffu, r1, last);
+        float prod[MS];
+#pragma unroll
+        for (int i = 0; i < MS; ++i) prod[i] = 1.0f;
+
+        for (uint32_t c0 = e0; c0 < e1; c0 += WE) {
+            const uint32_t c1 = min(e1, c0 + WE);
+            for (uint32_t base = c0 + lane; base < c1; base += 32u * U) {
+                uint32_t src[U];
+                float jr[JREG ? U : 1][JREG ? MS * MS : 1];
+                float o[U][MS];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const uint32_t p = base + 32u * u;
+                    src[u] = 0;
+                    if (p < c1) {
+                        src[u] = __ldcs(a.in_src + p);
+                        if constexpr (JREG) ldv<MS * MS, kStream>(a.joint + (size_t)p * (MS * MS), jr[u]);
+                        if (want) ldv<MS, kStream>(m_old + (size_t)p * MS, o[u]);
+                    }
+                }
+                float q[U][MS];
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                    if (base + 32u * u < c1) ldv<MS>(q_in + (size_t)src[u] * MS, q[u]);
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const uint32_t p = base + 32u * u;
+                    if (p >= c1) continue;
+                    int x = MS, y = MS;
+                    if (!UNI) {
+                        const uint8_t d = a.pos_dims[p];
+                        x = d & 15;
+                        y = d >> 4;
+                    }
+                    float m[MS];
+                    if constexpr (JREG) send_msg_regs<MS, UNI>(jr[u], q[u], x, y, m);
+                    else send_msg<MS, UNI>(a.joint + (size_t)p * (MS * MS), q[u], x, y, m);
+                    if (want) {
+                        float ad[MS];
+#pragma unroll
+                        for (int k = 0; k < MS; ++k) {
+                            float d = 0.0f;
+                            if (UNI || k < x) {
+                                d = FSUB(o[u][k], m[k]);
+                                if (d != d) d = 0.0f;
+                                d = fabsf(d);
+                            }
+                            ad[k] = d;
+                            dsum += (double)d;
+                        }
+                        if (serial) stv<MS>(a.absdiff + (size_t)__ldg(a.pos_edge + p) * MS, ad);
+                    }
+                    stv<MS, kStream>(m_new + (size_t)p * MS, m);
+                    stv<MS>(wsm + (size_t)(p - c0) * MS, m);
+                }
+            }
+            __syncwarp();
+            if (has) {
+                const uint32_t lo = max(r0, c0), hi = min(r1, c1);
+                for (uint32_t p = lo; p < hi; ++p) {
+                    float mm[MS];
+                    ldv<MS>(wsm + (size_t)(p - c0) * MS, mm);
+                    combine<MS, UNI>(prod, mm, S);
+                }
+            }
+            __syncwarp();
+        }
+        if (has) {
+            if (r1 > r0) {
+#pragma unroll
+                for (int i = 0; i < MS; ++i)
+                    if (UNI || i < S) b[i] = FMUL(b[i], prod[i]);
+            }
+            normalise<MS, UNI>(b, S);
+            stv<MS, kStream>(a.belief + (size_t)v * MS, b);
+            float qo[MS];
+#pragma unroll
+            for (int i = 0; i < MS; ++i) qo[i] = b[i];
+            if (e1 - e0 <= WE) {
+                for (uint32_t p = r0; p < r1; ++p) {
+                    float mm[MS];
+                    ldv<MS>(wsm + (size_t)(p - e0) * MS, mm);
+                    combine<MS, UNI>(qo, mm, S);
+                }
+            } else {
+                for (uint32_t p = r0; p < r1; ++p) {
+                    float mm[MS];
+                    ldv<MS>(m_new + (size_t)p * MS, mm);
+                    combine<MS, UNI>(qo, mm, S);
+                }
+            }
+            stv<MS>(q_out + (size_t)v * MS, qo);
+        }
+    }
+    if (!serial) reduce_and_finalize<NT>(ctl, a.partials, dsum, want, red, &s_last);
+}
+
 // prologue: Q_1 = b * prod of the latest messages (read_incoming_messages,
 // graph.c:860-882, on the messages init_previous_edge left)
 template <int MS, bool UNI>
@@ -603,13 +751,29 @@ static EdgeArgs edge_args(bp_graph *g) {
 }
 
 template <int MS, bool UNI>
-static int enqueue_node_iterations(bp_graph *g, uint32_t k, bool serial) {
+static int enqueue_node_iterations(bp_graph *g, uint32_t k, bool serial, int variant) {
     constexpr int NT = flood_nt<MS>();
-    const unsigned grid = grid_for(g->V, NT);
+    const bool warp_tiled = variant != BP_KERNEL_BLOCK_TILE;
+    const unsigned grid = warp_tiled ? grid_for(g->V, 256) : grid_for(g->V, NT);
     const FloodArgs a = flood_args(g);
     const uint64_t n = (uint64_t)g->E * MS;
+    // edges in flight per lane: BP_FLOOD_UNROLL=1|2|4 overrides the default
+    // for 1- and 2-state graphs (all variants give identical results)
+    int unroll = wflood_unroll<MS>();
+    if constexpr (MS <= 2) {
+        const char *env = getenv("BP_FLOOD_UNROLL");
+        if (env && (env[0] == '1' || env[0] == '2' || env[0] == '4')) unroll = env[0] - '0';
+    }
     for (uint32_t i = 0; i < k; ++i) {
-        k_flood<MS, UNI><<<grid, NT, 0, g->stream>>>(a);
+        if (!warp_tiled) {
+            k_flood<MS, UNI><<<grid, NT, 0, g->stream>>>(a);
+        } else if constexpr (MS <= 2) {
+            if (unroll == 1) k_flood_w<MS, UNI, 1><<<grid, 256, 0, g->stream>>>(a);
+            else if (unroll == 2) k_flood_w<MS, UNI, 2><<<grid, 256, 0, g->stream>>>(a);
+            else k_flood_w<MS, UNI, 4><<<grid, 256, 0, g->stream>>>(a);
+        } else {
+            k_flood_w<MS, UNI, wflood_unroll<MS>()><<<grid, 256, 0, g->stream>>>(a);
+        }
         BP_CUDA(cudaGetLastError());
         if (serial) {
             k_delta_serial<<<1, 256, 0, g->stream>>>(g->ctl, g->absdiff, n);
@@ -620,7 +784,7 @@ static int enqueue_node_iterations(bp_graph *g, uint32_t k, bool serial) {
 }
 
 template <int MS, bool UNI>
-static int enqueue_edge_iterations(bp_graph *g, uint32_t k, bool serial) {
+static int enqueue_edge_iterations(bp_graph *g, uint32_t k, bool serial, int) {
     const EdgeArgs a = edge_args(g);
     const uint64_t n = (uint64_t)g->E * MS;
     for (uint32_t i = 0; i < k; ++i) {
@@ -638,13 +802,14 @@ static int enqueue_edge_iterations(bp_graph *g, uint32_t k, bool serial) {
     return BP_OK;
 }
 
-static int enqueue_iterations(bp_graph *g, int schedule, uint32_t k, bool serial) {
-    if (schedule == BP_SCHEDULE_NODE) BP_DISPATCH_MS(g->ms, g->uniform != 0, enqueue_node_iterations, g, k, serial);
-    BP_DISPATCH_MS(g->ms, g->uniform != 0, enqueue_edge_iterations, g, k, serial);
+static int enqueue_iterations(bp_graph *g, int schedule, uint32_t k, bool serial, int variant) {
+    if (schedule == BP_SCHEDULE_NODE)
+        BP_DISPATCH_MS(g->ms, g->uniform != 0, enqueue_node_iterations, g, k, serial, variant);
+    BP_DISPATCH_MS(g->ms, g->uniform != 0, enqueue_edge_iterations, g, k, serial, variant);
 }
 
-static int flood_grid(bp_graph *g) {
-    const int nt = g->ms <= 4 ? 256 : 128;
+static int flood_grid(bp_graph *g, int variant) {
+    const int nt = (variant != BP_KERNEL_BLOCK_TILE || g->ms <= 4) ? 256 : 128;
     return (int)grid_for(g->V, nt);
 }
 
@@ -663,7 +828,7 @@ void bp_loopy_default_options(bp_loopy_options *o) {
     o->delta_mode = BP_DELTA_AUTO;
     o->verbose = 0;
     o->graph_chunk = 0;
-    o->reserved = 0;
+    o->kernel_variant = BP_KERNEL_AUTO;
 }
 
 int bp_init_messages(bp_graph *g) {
@@ -718,7 +883,15 @@ int bp_loopy(bp_graph *g, const bp_loopy_options *opt, bp_loopy_result *res) {
         return BP_OK;
     }
     int st;
-    const uint32_t grid_blocks = opt->schedule == BP_SCHEDULE_NODE ? (uint32_t)flood_grid(g) : grid_for(g->E, 256);
+    int variant = opt->kernel_variant;
+    if (variant == BP_KERNEL_AUTO) {
+        const char *env = getenv("BP_FLOOD_KERNEL");
+        variant = (env && env[0] == 'w') ? BP_KERNEL_WARP_TILE : BP_KERNEL_BLOCK_TILE;
+    }
+    if (variant != BP_KERNEL_BLOCK_TILE && variant != BP_KERNEL_WARP_TILE)
+        return set_error(BP_ERR_INVALID, "unknown kernel variant %d", opt->kernel_variant);
+    const uint32_t grid_blocks = opt->schedule == BP_SCHEDULE_NODE ? (uint32_t)flood_grid(g, variant)
+                                                                   : grid_for(g->E, 256);
     if ((st = ensure_partials(g, grid_blocks))) return st;
     if (serial && (st = ensure_absdiff(g))) return st;
     if (opt->schedule == BP_SCHEDULE_EDGE && (st = ensure_runs(g))) return st;
@@ -746,7 +919,8 @@ int bp_loopy(bp_graph *g, const bp_loopy_options *opt, bp_loopy_result *res) {
     }
 
     // CUDA graph of `chunk` iterations, cached per (schedule, delta, chunk)
-    const uint64_t key = 1ull | ((uint64_t)opt->schedule << 1) | ((uint64_t)serial << 2) | ((uint64_t)chunk << 8);
+    const uint64_t key = 1ull | ((uint64_t)opt->schedule << 1) | ((uint64_t)serial << 2) |
+                         ((uint64_t)variant << 4) | ((uint64_t)chunk << 8);
     bp_graph::CachedGraph *slot = nullptr;
     for (auto &cg : g->loop_graph)
         if (cg.exec && cg.key == key) slot = &cg;
@@ -763,7 +937,7 @@ int bp_loopy(bp_graph *g, const bp_loopy_options *opt, bp_loopy_result *res) {
         }
         cudaGraph_t graph = nullptr;
         BP_CUDA(cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal));
-        st = enqueue_iterations(g, opt->schedule, chunk, serial);
+        st = enqueue_iterations(g, opt->schedule, chunk, serial, variant);
         cudaError_t ce2 = cudaStreamEndCapture(g->stream, &graph);
         if (st) {
             if (graph) cudaGraphDestroy(graph);

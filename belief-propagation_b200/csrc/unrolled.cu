@@ -1,0 +1,608 @@
+// unrolled.cu -- T-step unrolled loopy BP and its adjoint.
+//
+// The forward pass is the reference's update (graph.c:725-751, :1121-1183)
+// on a pairwise model whose priors are softmax(log_unary) and whose joint
+// tables are exp(log_pair) shared by many edges (edge e uses table
+// tab[e] & 0x7f, transposed when tab[e] & 0x80):
+//   b_0 = softmax(theta)            m_0(e) = normalise(J_e . b_0(src))
+//   Q_1 = b_0 * prod_in m_0
+//   t = 1..T:  m_t(e) = normalise(J_e . Q_t(src))
+//              b_t    = normalise(b_{t-1} * prod_in m_t)
+//              Q_{t+1}= b_t * prod_in m_t
+// The state carried between iterations is (b, Q); messages are recomputed
+// from Q wherever needed and never stored.  The forward keeps (b_t, Q_{t+1})
+// every `checkpoint_every` iterations; the backward recomputes the states of
+// one segment from its checkpoint and runs the adjoint of each step in
+// reverse:
+//   from Q_{t+1} = b_t * P:  bbar_t += Qbar_{t+1} * P,  Pbar = Qbar_{t+1} * b_t
+//   from b_t = u / sum(u):   ubar = (bbar_t - <bbar_t, b_t>) / sum(u)
+//   from u = b_{t-1} * P:    bbar_{t-1} = ubar * P,     Pbar += ubar * b_{t-1}
+//   from P = prod_e m_e:     mbar_e = Pbar * prod_{e' != e} m_e'
+//   from m = r / sum(r):     rbar = (mbar - <mbar, m>) / sum(r)
+//   from r = J Q(src):       Qbar_t(src) += J^T rbar,   Ebar += rbar (x) Q(src)
+// and finally theta_bar = b_0 * (bbar_0 - <bbar_0, b_0>), log_pair_bar =
+// Ebar * exp(log_pair).  The Q(src) adjoint is a gather over the
+// source-sorted edge list, so no atomics and the result is deterministic.
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "bp_device.cuh"
+#include "bp_internal.h"
+
+namespace bpx {
+
+constexpr int kUThreads = 256;
+constexpr uint32_t kUMaxTables = 16;
+
+struct UGraph {
+    uint32_t V, K;
+    const uint32_t *in_ptr, *in_src, *out_ptr, *out_pos;
+    const uint8_t *pos_tab;
+    const float *tables;   // [K][S][S] = exp(log_pair)
+};
+
+template <int S>
+__device__ __forceinline__ void load_tables_smem(const UGraph &g, float *sm) {
+    // sm[2k] = table k, sm[2k+1] = its transpose
+    for (uint32_t i = threadIdx.x; i < g.K * S * S; i += blockDim.x) {
+        const uint32_t k = i / (S * S), r = (i % (S * S)) / S, c = i % S;
+        const float v = g.tables[i];
+        sm[(2 * k) * S * S + r * S + c] = v;
+        sm[(2 * k + 1) * S * S + c * S + r] = v;
+    }
+    __syncthreads();
+}
+
+template <int S>
+__device__ __forceinline__ const float *edge_table(const float *sm, uint8_t tab) {
+    return sm + (2u * (tab & 0x7fu) + ((tab & 0x80u) ? 1u : 0u)) * S * S;
+}
+
+// r = J q, R = sum r (<= 0 -> 1), m = r / R
+template <int S>
+__device__ __forceinline__ float msg_r(const float *J, const float *q, float *m) {
+    float R = 0.0f;
+#pragma unroll
+    for (int i = 0; i < S; ++i) {
+        float r = 0.0f;
+#pragma unroll
+        for (int j = 0; j < S; ++j) r = FADD(r, FMUL(J[i * S + j], q[j]));
+        m[i] = r;
+        R = FADD(R, r);
+    }
+    if (R <= 0.0f) R = 1.0f;
+#pragma unroll
+    for (int i = 0; i < S; ++i) m[i] = FDIV(m[i], R);
+    return R;
+}
+
+template <int S>
+__global__ void k_u_exp(const float *__restrict__ logp, uint32_t n, float *__restrict__ tab) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) tab[i] = expf(logp[i]);
+}
+
+template <int S>
+__global__ void k_u_softmax(uint32_t V, const float *__restrict__ theta, float *__restrict__ b0) {
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= V) return;
+    float t[S], mx = -INFINITY;
+    ldv<S>(theta + (size_t)v * S, t);
+#pragma unroll
+    for (int i = 0; i < S; ++i) mx = fmaxf(mx, t[i]);
+    float z = 0.0f;
+#pragma unroll
+    for (int i = 0; i < S; ++i) {
+        t[i] = expf(t[i] - mx);
+        z += t[i];
+    }
+#pragma unroll
+    for (int i = 0; i < S; ++i) t[i] = t[i] / z;
+    stv<S>(b0 + (size_t)v * S, t);
+}
+
+// Q = b * prod_in normalise(J . send(src))   (graph.c:860-882 after :725-751)
+template <int S>
+__global__ void __launch_bounds__(kUThreads) k_u_gather_q(const UGraph g, const float *__restrict__ b,
+                                                          const float *__restrict__ send, float *__restrict__ q) {
+    __shared__ float sm[2 * kUMaxTables * S * S];
+    load_tables_smem<S>(g, sm);
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= g.V) return;
+    float qo[S];
+    ldv<S>(b + (size_t)v * S, qo);
+    for (uint32_t p = g.in_ptr[v]; p < g.in_ptr[v + 1]; ++p) {
+        float x[S], m[S];
+        ldv<S>(send + (size_t)g.in_src[p] * S, x);
+        msg_r<S>(edge_table<S>(sm, g.pos_tab[p]), x, m);
+#pragma unroll
+        for (int i = 0; i < S; ++i) qo[i] = FMUL(qo[i], m[i]);
+    }
+    stv<S>(q + (size_t)v * S, qo);
+}
+
+// one forward iteration: (b_{t-1}, Q_t) -> (b_t, Q_{t+1})
+template <int S>
+__global__ void __launch_bounds__(kUThreads) k_u_iter(const UGraph g, const float *__restrict__ b_in,
+                                                      const float *__restrict__ q_in, float *__restrict__ b_out,
+                                                      float *__restrict__ q_out) {
+    __shared__ float sm[2 * kUMaxTables * S * S];
+    load_tables_smem<S>(g, sm);
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= g.V) return;
+    const uint32_t r0 = g.in_ptr[v], r1 = g.in_ptr[v + 1];
+    float P[S], b[S];
+#pragma unroll
+    for (int i = 0; i < S; ++i) P[i] = 1.0f;
+    for (uint32_t p = r0; p < r1; ++p) {
+        float x[S], m[S];
+        ldv<S>(q_in + (size_t)g.in_src[p] * S, x);
+        msg_r<S>(edge_table<S>(sm, g.pos_tab[p]), x, m);
+#pragma unroll
+        for (int i = 0; i < S; ++i) P[i] = FMUL(P[i], m[i]);
+    }
+    ldv<S>(b_in + (size_t)v * S, b);
+    if (r1 > r0) {
+#pragma unroll
+        for (int i = 0; i < S; ++i) b[i] = FMUL(b[i], P[i]);
+    }
+    normalise<S, true>(b, S);
+    stv<S>(b_out + (size_t)v * S, b);
+    float qo[S];
+#pragma unroll
+    for (int i = 0; i < S; ++i) qo[i] = b[i];
+    for (uint32_t p = r0; p < r1; ++p) {
+        float x[S], m[S];
+        ldv<S>(q_in + (size_t)g.in_src[p] * S, x);
+        msg_r<S>(edge_table<S>(sm, g.pos_tab[p]), x, m);
+#pragma unroll
+        for (int i = 0; i < S; ++i) qo[i] = FMUL(qo[i], m[i]);
+    }
+    stv<S>(q_out + (size_t)v * S, qo);
+}
+
+// adjoint of one node step.  mode 0: iteration (b_t = normalise(b_{t-1} P),
+// Q_{t+1} = b_t P, messages from send = Q_t); mode 1: the initial step
+// (Q_1 = b_0 P, messages from send = b_0).  Writes bbar_out (bbar_{t-1}, or
+// the total bbar_0 without its send term), rbar per in-edge, and adds the
+// block's Ebar into epart[blockIdx].
+template <int S>
+__global__ void __launch_bounds__(kUThreads) k_u_bwd_node(const UGraph g, int mode, const float *__restrict__ b_prev,
+                                                          const float *__restrict__ send,
+                                                          const float *__restrict__ b_t,
+                                                          const float *__restrict__ bbar_t,
+                                                          const float *__restrict__ qbar_next,
+                                                          float *__restrict__ bbar_out, float *__restrict__ rbar,
+                                                          double *__restrict__ epart) {
+    __shared__ float sm[2 * kUMaxTables * S * S];
+    __shared__ float wred[kUThreads / 32][S * S];
+    load_tables_smem<S>(g, sm);
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    float acc[S * S];
+#pragma unroll
+    for (int k = 0; k < S * S; ++k) acc[k] = 0.0f;
+    if (v < g.V) {
+        const uint32_t r0 = g.in_ptr[v], r1 = g.in_ptr[v + 1];
+        float P[S];
+#pragma unroll
+        for (int i = 0; i < S; ++i) P[i] = 1.0f;
+        for (uint32_t p = r0; p < r1; ++p) {
+            float x[S], m[S];
+            ldv<S>(send + (size_t)g.in_src[p] * S, x);
+            msg_r<S>(edge_table<S>(sm, g.pos_tab[p]), x, m);
+#pragma unroll
+            for (int i = 0; i < S; ++i) P[i] = FMUL(P[i], m[i]);
+        }
+        float bp[S], bt[S], bb[S], qb[S], Pbar[S];
+        ldv<S>(b_prev + (size_t)v * S, bp);
+#pragma unroll
+        for (int i = 0; i < S; ++i) {
+            bb[i] = 0.0f;
+            qb[i] = 0.0f;
+        }
+        if (bbar_t) ldv<S>(bbar_t + (size_t)v * S, bb);
+        if (qbar_next) ldv<S>(qbar_next + (size_t)v * S, qb);
+        if (mode == 0) {
+            ldv<S>(b_t + (size_t)v * S, bt);
+            float tot[S], dot = 0.0f, Z = 0.0f;
+#pragma unroll
+            for (int i = 0; i < S; ++i) {
+                tot[i] = bb[i] + qb[i] * P[i];
+                Pbar[i] = qb[i] * bt[i];
+                dot += tot[i] * bt[i];
+                Z += (r1 > r0) ? bp[i] * P[i] : bp[i];
+            }
+            if (Z <= 0.0f) Z = 1.0f;
+            float out[S];
+#pragma unroll
+            for (int i = 0; i < S; ++i) {
+                const float ub = (tot[i] - dot) / Z;
+                out[i] = (r1 > r0) ? ub * P[i] : ub;
+                Pbar[i] += ub * bp[i];
+            }
+            stv<S>(bbar_out + (size_t)v * S, out);
+        } else {
+            float out[S];
+#pragma unroll
+            for (int i = 0; i < S; ++i) {
+                out[i] = bb[i] + qb[i] * P[i];
+                Pbar[i] = qb[i] * bp[i];
+            }
+            stv<S>(bbar_out + (size_t)v * S, out);
+        }
+        for (uint32_t p = r0; p < r1; ++p) {
+            const uint8_t tab = g.pos_tab[p];
+            const float *J = edge_table<S>(sm, tab);
+            float x[S], m[S];
+            ldv<S>(send + (size_t)g.in_src[p] * S, x);
+            const float R = msg_r<S>(J, x, m);
+            float mb[S], dot = 0.0f;
+#pragma unroll
+            for (int i = 0; i < S; ++i) {
+                float loo;
+                if (m[i] != 0.0f) {
+                    loo = P[i] / m[i];
+                } else {  // product of the other messages, recomputed
+                    loo = 1.0f;
+                    for (uint32_t p2 = r0; p2 < r1; ++p2) {
+                        if (p2 == p) continue;
+                        float x2[S], m2[S];
+                        ldv<S>(send + (size_t)g.in_src[p2] * S, x2);
+                        msg_r<S>(edge_table<S>(sm, g.pos_tab[p2]), x2, m2);
+                        loo *= m2[i];
+                    }
+                }
+                mb[i] = Pbar[i] * loo;
+                dot += mb[i] * m[i];
+            }
+            float rb[S];
+#pragma unroll
+            for (int i = 0; i < S; ++i) rb[i] = (mb[i] - dot) / R;
+            stv<S>(rbar + (size_t)p * S, rb);
+            // Ebar of the shared table: J_e = E (or E^T when transposed)
+            if (tab & 0x80u) {
+#pragma unroll
+                for (int i = 0; i < S; ++i)
+#pragma unroll
+                    for (int j = 0; j < S; ++j) acc[j * S + i] += rb[i] * x[j];
+            } else {
+#pragma unroll
+                for (int i = 0; i < S; ++i)
+#pragma unroll
+                    for (int j = 0; j < S; ++j) acc[i * S + j] += rb[i] * x[j];
+            }
+        }
+    }
+    // block sum of acc (fixed order), added to this block's running partial
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < S * S; ++k) {
+        float x = acc[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) wred[w][k] = x;
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < S * S; k += blockDim.x) {
+        double t = 0.0;
+        for (int ww = 0; ww < (int)(blockDim.x >> 5); ++ww) t += (double)wred[ww][k];
+        epart[(size_t)blockIdx.x * S * S + k] += t;
+    }
+}
+
+// Qbar(s) = sum over s's out-edges of J_e^T rbar_e (+ add(s))
+template <int S>
+__global__ void __launch_bounds__(kUThreads) k_u_bwd_src(const UGraph g, const float *__restrict__ rbar,
+                                                         const float *__restrict__ add, float *__restrict__ out) {
+    __shared__ float sm[2 * kUMaxTables * S * S];
+    load_tables_smem<S>(g, sm);
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= g.V) return;
+    float acc[S];
+    if (add) ldv<S>(add + (size_t)s * S, acc);
+    else {
+#pragma unroll
+        for (int j = 0; j < S; ++j) acc[j] = 0.0f;
+    }
+    for (uint32_t qq = g.out_ptr[s]; qq < g.out_ptr[s + 1]; ++qq) {
+        const uint32_t p = g.out_pos[qq];
+        const float *J = edge_table<S>(sm, g.pos_tab[p]);
+        float rb[S];
+        ldv<S>(rbar + (size_t)p * S, rb);
+#pragma unroll
+        for (int j = 0; j < S; ++j) {
+            float t = 0.0f;
+#pragma unroll
+            for (int i = 0; i < S; ++i) t += J[i * S + j] * rb[i];
+            acc[j] += t;
+        }
+    }
+    stv<S>(out + (size_t)s * S, acc);
+}
+
+template <int S>
+__global__ void k_u_softmax_bwd(uint32_t V, const float *__restrict__ b0, const float *__restrict__ bbar,
+                                float *__restrict__ theta_bar) {
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= V) return;
+    float b[S], gb[S], dot = 0.0f;
+    ldv<S>(b0 + (size_t)v * S, b);
+    ldv<S>(bbar + (size_t)v * S, gb);
+#pragma unroll
+    for (int i = 0; i < S; ++i) dot += gb[i] * b[i];
+#pragma unroll
+    for (int i = 0; i < S; ++i) gb[i] = b[i] * (gb[i] - dot);
+    stv<S>(theta_bar + (size_t)v * S, gb);
+}
+
+// log_pair_bar[k] = (sum of the block partials, fixed order) * exp(log_pair)
+__global__ void k_u_reduce_pair(const double *__restrict__ epart, uint32_t nblk, uint32_t n,
+                                const float *__restrict__ tables, float *__restrict__ out) {
+    __shared__ double red[32];
+    for (uint32_t k = 0; k < n; ++k) {
+        double t = 0.0;
+        for (uint32_t b = threadIdx.x; b < nblk; b += blockDim.x) t += epart[(size_t)b * n + k];
+        t = warp_sum(t);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double s = 0.0;
+            for (uint32_t w = 0; w < (blockDim.x >> 5); ++w) s += red[w];
+            out[k] = (float)(s * (double)tables[k]);
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace bpx
+
+struct bp_unrolled {
+    uint32_t V = 0, E = 0, S = 0, K = 0, T = 0, ck = 1, nck = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    uint32_t *in_ptr = nullptr, *in_src = nullptr, *out_ptr = nullptr, *out_pos = nullptr;
+    uint8_t *pos_tab = nullptr;
+    float *tables = nullptr;
+    float *ck_b = nullptr, *ck_q = nullptr;    // [nck][V][S]
+    float *seg_b = nullptr, *seg_q = nullptr;  // [ck][V][S] (slot 0 unused)
+    float *pp_b = nullptr, *pp_q = nullptr;    // [2][V][S]
+    float *bT = nullptr;
+    float *bbar[2] = {nullptr, nullptr}, *qbar[2] = {nullptr, nullptr};
+    float *rbar = nullptr;
+    double *epart = nullptr;
+    uint32_t nblk = 0;
+    bool forward_done = false;
+    float fwd_ms = 0.0f, bwd_ms = 0.0f;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace bpx {
+
+template <int S>
+static int u_forward(bp_unrolled *u, const float *theta, const float *logp, float *beliefs) {
+    const UGraph g{u->V, u->K, u->in_ptr, u->in_src, u->out_ptr, u->out_pos, u->pos_tab, u->tables};
+    const size_t VS = (size_t)u->V * S;
+    const unsigned gv = grid_for(u->V, kUThreads);
+    cudaStream_t st = u->stream;
+    k_u_exp<S><<<grid_for(u->K * S * S, 64), 64, 0, st>>>(logp, u->K * S * S, u->tables);
+    k_u_softmax<S><<<gv, kUThreads, 0, st>>>(u->V, theta, u->ck_b);
+    k_u_gather_q<S><<<gv, kUThreads, 0, st>>>(g, u->ck_b, u->ck_b, u->ck_q);
+    BP_CUDA(cudaGetLastError());
+    // state t lives in checkpoint slot t/ck when t % ck == 0, else in pp[t&1]
+    auto loc_b = [&](uint32_t t) { return (t % u->ck == 0) ? u->ck_b + (t / u->ck) * VS : u->pp_b + (t & 1) * VS; };
+    auto loc_q = [&](uint32_t t) { return (t % u->ck == 0) ? u->ck_q + (t / u->ck) * VS : u->pp_q + (t & 1) * VS; };
+    for (uint32_t t = 1; t <= u->T; ++t) {
+        float *bo = (t == u->T) ? u->bT : loc_b(t);
+        float *qo = (t == u->T) ? u->pp_q + (t & 1) * VS : loc_q(t);
+        if (t != u->T && t % u->ck == 0 && t / u->ck >= u->nck) return set_error(BP_ERR_STATE, "checkpoint slots");
+        k_u_iter<S><<<gv, kUThreads, 0, st>>>(g, loc_b(t - 1), loc_q(t - 1), bo, qo);
+    }
+    BP_CUDA(cudaGetLastError());
+    BP_CUDA(cudaMemcpyAsync(beliefs, u->bT, sizeof(float) * VS, cudaMemcpyDeviceToDevice, st));
+    return BP_OK;
+}
+
+template <int S>
+static int u_backward(bp_unrolled *u, const float *grad_b, float *grad_theta, float *grad_logp) {
+    const UGraph g{u->V, u->K, u->in_ptr, u->in_src, u->out_ptr, u->out_pos, u->pos_tab, u->tables};
+    const size_t VS = (size_t)u->V * S;
+    const unsigned gv = grid_for(u->V, kUThreads);
+    cudaStream_t st = u->stream;
+    BP_CUDA(cudaMemsetAsync(u->epart, 0, sizeof(double) * u->nblk * S * S, st));
+    BP_CUDA(cudaMemcpyAsync(u->bbar[0], grad_b, sizeof(float) * VS, cudaMemcpyDeviceToDevice, st));
+    int bc = 0, qc = -1;   // current bbar buffer; current qbar buffer (-1 = zero)
+    const uint32_t nseg = (u->T + u->ck - 1) / u->ck;
+    for (int s = (int)nseg - 1; s >= 0; --s) {
+        const uint32_t t0 = (uint32_t)s * u->ck, t_end = std::min(t0 + u->ck, u->T);
+        const float *ckb = u->ck_b + (size_t)s * VS, *ckq = u->ck_q + (size_t)s * VS;
+        // recompute states t0+1 .. t_end-1 into seg slots 1..
+        for (uint32_t j = 1; j + t0 < t_end; ++j) {
+            const float *bi = (j == 1) ? ckb : u->seg_b + (j - 1) * VS;
+            const float *qi = (j == 1) ? ckq : u->seg_q + (j - 1) * VS;
+            k_u_iter<S><<<gv, kUThreads, 0, st>>>(g, bi, qi, u->seg_b + j * VS, u->seg_q + j * VS);
+        }
+        for (uint32_t t = t_end; t > t0; --t) {
+            const uint32_t j = t - t0 - 1;
+            const float *b_prev = (j == 0) ? ckb : u->seg_b + j * VS;
+            const float *q_t = (j == 0) ? ckq : u->seg_q + j * VS;
+            const float *b_t = (t == u->T) ? u->bT
+                               : (t == t_end) ? u->ck_b + (size_t)(s + 1) * VS
+                                              : u->seg_b + (j + 1) * VS;
+            const float *qb = qc < 0 ? nullptr : u->qbar[qc];
+            k_u_bwd_node<S><<<gv, kUThreads, 0, st>>>(g, 0, b_prev, q_t, b_t, u->bbar[bc], qb, u->bbar[bc ^ 1],
+                                                      u->rbar, u->epart);
+            const int qn = qc < 0 ? 0 : qc ^ 1;
+            k_u_bwd_src<S><<<gv, kUThreads, 0, st>>>(g, u->rbar, nullptr, u->qbar[qn]);
+            bc ^= 1;
+            qc = qn;
+        }
+    }
+    BP_CUDA(cudaGetLastError());
+    // initial step: Q_1 = b_0 * prod normalise(J . b_0(src))
+    const float *b0 = u->ck_b;
+    k_u_bwd_node<S><<<gv, kUThreads, 0, st>>>(g, 1, b0, b0, nullptr, u->bbar[bc], qc < 0 ? nullptr : u->qbar[qc],
+                                              u->bbar[bc ^ 1], u->rbar, u->epart);
+    k_u_bwd_src<S><<<gv, kUThreads, 0, st>>>(g, u->rbar, u->bbar[bc ^ 1], u->bbar[bc]);
+    k_u_softmax_bwd<S><<<gv, kUThreads, 0, st>>>(u->V, b0, u->bbar[bc], grad_theta);
+    k_u_reduce_pair<<<1, 256, 0, st>>>(u->epart, u->nblk, u->K * S * S, u->tables, grad_logp);
+    BP_CUDA(cudaGetLastError());
+    return BP_OK;
+}
+
+static void u_free(bp_unrolled *u) {
+    if (!u) return;
+    void *ptrs[] = {u->in_ptr, u->in_src, u->out_ptr, u->out_pos, u->pos_tab, u->tables, u->ck_b, u->ck_q,
+                    u->seg_b, u->seg_q, u->pp_b, u->pp_q, u->bT, u->bbar[0], u->bbar[1], u->qbar[0],
+                    u->qbar[1], u->rbar, u->epart};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    if (u->ev0) cudaEventDestroy(u->ev0);
+    if (u->ev1) cudaEventDestroy(u->ev1);
+    if (u->own_stream && u->stream) cudaStreamDestroy(u->stream);
+    delete u;
+}
+
+}  // namespace bpx
+
+using namespace bpx;
+
+#define BP_DISPATCH_S(S_, FN, ...)                                 \
+    switch (S_) {                                                  \
+    case 1: return FN<1>(__VA_ARGS__);                             \
+    case 2: return FN<2>(__VA_ARGS__);                             \
+    case 3: return FN<3>(__VA_ARGS__);                             \
+    case 4: return FN<4>(__VA_ARGS__);                             \
+    case 5: return FN<5>(__VA_ARGS__);                             \
+    case 6: return FN<6>(__VA_ARGS__);                             \
+    case 7: return FN<7>(__VA_ARGS__);                             \
+    case 8: return FN<8>(__VA_ARGS__);                             \
+    case 9: return FN<9>(__VA_ARGS__);                             \
+    default: return FN<10>(__VA_ARGS__);                           \
+    }
+
+extern "C" {
+
+int bp_unrolled_create(bp_unrolled **out, uint32_t V, uint32_t E, uint32_t S, uint32_t K, const uint32_t *src,
+                       const uint32_t *dst, const uint8_t *tab, uint32_t T, uint32_t ck, void *stream) {
+    if (!out || (E && (!src || !dst || !tab))) return set_error(BP_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (S < 1 || S > BP_MAX_STATES) return set_error(BP_ERR_SHAPE, "num_states %u", S);
+    if (K < 1 || K > kUMaxTables) return set_error(BP_ERR_SHAPE, "num_tables %u not in [1, %u]", K, kUMaxTables);
+    if (V == 0 || T == 0) return set_error(BP_ERR_SHAPE, "need nodes and at least one iteration");
+    if (ck == 0) ck = 1;
+    for (uint32_t e = 0; e < E; ++e) {
+        if (src[e] >= V || dst[e] >= V) return set_error(BP_ERR_INVALID, "edge %u endpoint out of range", e);
+        if ((tab[e] & 0x7fu) >= K) return set_error(BP_ERR_INVALID, "edge %u table %u >= %u", e, tab[e] & 0x7f, K);
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_error(BP_ERR_NO_DEVICE, "no CUDA device");
+    bp_unrolled *u = new bp_unrolled();
+    u->V = V, u->E = E, u->S = S, u->K = K, u->T = T, u->ck = ck;
+    u->nck = (T - 1) / ck + 1;
+    if (stream) {
+        u->stream = (cudaStream_t)stream;
+    } else {
+        cudaStreamCreateWithFlags(&u->stream, cudaStreamNonBlocking);
+        u->own_stream = true;
+    }
+    // destination-sorted (stable) and source-sorted edge orders, on the host
+    std::vector<uint32_t> in_ptr(V + 1, 0), out_ptr(V + 1, 0), perm(E), in_src(E), out_pos(E);
+    std::vector<uint8_t> ptab(E);
+    for (uint32_t e = 0; e < E; ++e) {
+        in_ptr[dst[e] + 1]++;
+        out_ptr[src[e] + 1]++;
+    }
+    for (uint32_t v = 0; v < V; ++v) {
+        in_ptr[v + 1] += in_ptr[v];
+        out_ptr[v + 1] += out_ptr[v];
+    }
+    std::vector<uint32_t> fill(in_ptr.begin(), in_ptr.end() - 1), pos_of(E);
+    for (uint32_t e = 0; e < E; ++e) {
+        const uint32_t p = fill[dst[e]]++;
+        pos_of[e] = p;
+        in_src[p] = src[e];
+        ptab[p] = tab[e];
+    }
+    std::vector<uint32_t> ofill(out_ptr.begin(), out_ptr.end() - 1);
+    for (uint32_t e = 0; e < E; ++e) out_pos[ofill[src[e]]++] = pos_of[e];
+    const size_t VS = (size_t)V * S;
+    u->nblk = grid_for(V, kUThreads);
+    auto alloc = [&](void **p, size_t bytes) {
+        return cudaMalloc(p, bytes ? bytes : 16) == cudaSuccess;
+    };
+    bool ok = alloc((void **)&u->in_ptr, sizeof(uint32_t) * (V + 1)) && alloc((void **)&u->in_src, 4 * (size_t)E) &&
+              alloc((void **)&u->out_ptr, sizeof(uint32_t) * (V + 1)) && alloc((void **)&u->out_pos, 4 * (size_t)E) &&
+              alloc((void **)&u->pos_tab, (size_t)E) && alloc((void **)&u->tables, sizeof(float) * K * S * S) &&
+              alloc((void **)&u->ck_b, sizeof(float) * VS * u->nck) &&
+              alloc((void **)&u->ck_q, sizeof(float) * VS * u->nck) &&
+              alloc((void **)&u->seg_b, sizeof(float) * VS * ck) && alloc((void **)&u->seg_q, sizeof(float) * VS * ck) &&
+              alloc((void **)&u->pp_b, sizeof(float) * VS * 2) && alloc((void **)&u->pp_q, sizeof(float) * VS * 2) &&
+              alloc((void **)&u->bT, sizeof(float) * VS) && alloc((void **)&u->bbar[0], sizeof(float) * VS) &&
+              alloc((void **)&u->bbar[1], sizeof(float) * VS) && alloc((void **)&u->qbar[0], sizeof(float) * VS) &&
+              alloc((void **)&u->qbar[1], sizeof(float) * VS) && alloc((void **)&u->rbar, sizeof(float) * S * (size_t)E) &&
+              alloc((void **)&u->epart, sizeof(double) * u->nblk * S * S);
+    if (!ok) {
+        u_free(u);
+        return set_error(BP_ERR_NOMEM, "device allocation failed for the unrolled graph");
+    }
+    cudaMemcpyAsync(u->in_ptr, in_ptr.data(), 4 * (V + 1), cudaMemcpyHostToDevice, u->stream);
+    cudaMemcpyAsync(u->out_ptr, out_ptr.data(), 4 * (V + 1), cudaMemcpyHostToDevice, u->stream);
+    if (E) {
+        cudaMemcpyAsync(u->in_src, in_src.data(), 4 * (size_t)E, cudaMemcpyHostToDevice, u->stream);
+        cudaMemcpyAsync(u->out_pos, out_pos.data(), 4 * (size_t)E, cudaMemcpyHostToDevice, u->stream);
+        cudaMemcpyAsync(u->pos_tab, ptab.data(), (size_t)E, cudaMemcpyHostToDevice, u->stream);
+    }
+    cudaEventCreate(&u->ev0);
+    cudaEventCreate(&u->ev1);
+    if (cudaStreamSynchronize(u->stream) != cudaSuccess) {
+        u_free(u);
+        return set_error(BP_ERR_CUDA, "upload of the unrolled graph failed");
+    }
+    *out = u;
+    return BP_OK;
+}
+
+void bp_unrolled_destroy(bp_unrolled *u) {
+    if (!u) return;
+    cudaStreamSynchronize(u->stream);
+    u_free(u);
+}
+
+int bp_unrolled_forward(bp_unrolled *u, const float *log_unary, const float *log_pair, float *beliefs) {
+    if (!u || !log_unary || !log_pair || !beliefs) return set_error(BP_ERR_INVALID, "null argument");
+    BP_CUDA(cudaEventRecord(u->ev0, u->stream));
+    int st;
+    auto run = [&]() -> int { BP_DISPATCH_S(u->S, u_forward, u, log_unary, log_pair, beliefs); };
+    if ((st = run())) return st;
+    BP_CUDA(cudaEventRecord(u->ev1, u->stream));
+    u->forward_done = true;
+    return BP_OK;
+}
+
+int bp_unrolled_backward(bp_unrolled *u, const float *grad_beliefs, float *grad_log_unary, float *grad_log_pair) {
+    if (!u || !grad_beliefs || !grad_log_unary || !grad_log_pair) return set_error(BP_ERR_INVALID, "null argument");
+    if (!u->forward_done) return set_error(BP_ERR_STATE, "backward before forward");
+    auto run = [&]() -> int { BP_DISPATCH_S(u->S, u_backward, u, grad_beliefs, grad_log_unary, grad_log_pair); };
+    return run();
+}
+
+int bp_unrolled_set_stream(bp_unrolled *u, void *stream) {
+    if (!u) return set_error(BP_ERR_INVALID, "null argument");
+    BP_CUDA(cudaStreamSynchronize(u->stream));
+    if (u->own_stream) cudaStreamDestroy(u->stream);
+    u->own_stream = false;
+    if (stream) {
+        u->stream = (cudaStream_t)stream;
+    } else {
+        BP_CUDA(cudaStreamCreateWithFlags(&u->stream, cudaStreamNonBlocking));
+        u->own_stream = true;
+    }
+    return BP_OK;
+}
+
+}  // extern "C"

@@ -140,7 +140,7 @@ class BPGraph:
         N.check(self.lib.bp_init_messages(self.h))
 
     def loopy(self, tol=1e-3, max_iterations=200, check_every=1, schedule="node", delta="auto",
-              verbose=False, graph_chunk=0):
+              verbose=False, graph_chunk=0, kernel="auto"):
         o = N.LoopyOptions()
         self.lib.bp_loopy_default_options(C.byref(o))
         o.tolerance = float(tol)
@@ -150,6 +150,7 @@ class BPGraph:
         o.delta_mode = _DELTA[delta]
         o.verbose = int(bool(verbose))
         o.graph_chunk = int(graph_chunk)
+        o.kernel_variant = {"auto": 0, "block": 1, "warp": 2}[kernel]
         r = N.LoopyResult()
         N.check(self.lib.bp_loopy(self.h, C.byref(o), C.byref(r)))
         return r.as_dict()
@@ -181,3 +182,109 @@ class BPGraph:
 
     def tree_marginalize(self):
         N.check(self.lib.bp_tree_marginalize(self.h))
+
+
+class BPBatch:
+    """Many independent networks solved together (bp_batch): one persistent
+    launch per state count, each network with its own stopping rule."""
+
+    def __init__(self, nets, stream=None):
+        self.lib = N.load()
+        self.nets = nets
+        descs = (N.GraphDesc * len(nets))()
+        keep = []
+        for d, net in zip(descs, nets):
+            S = net.uniform_states
+            if S == 0:
+                raise ValueError(f"{net.name}: batched networks need one state count per network")
+            src = np.ascontiguousarray(net.src, np.uint32)
+            dst = np.ascontiguousarray(net.dst, np.uint32)
+            joint = np.ascontiguousarray(net.joint[:, :S, :S], np.float32)
+            keep.append((src, dst, joint))
+            d.num_nodes, d.num_edges, d.uniform_states = net.V, net.E, S
+            d.edge_src, d.edge_dst, d.edge_joint = src.ctypes.data, dst.ctypes.data, joint.ctypes.data
+            d.joint_row_stride, d.joint_edge_stride = S, S * S
+            d.memory = N.BP_MEM_HOST
+        h = C.c_void_p()
+        N.check(self.lib.bp_batch_create(C.byref(h), len(nets), descs, stream))
+        self.h = h
+        n = len(nets)
+        self.belief_off = np.zeros(n + 1, np.uint64)
+        self.msg_off = np.zeros(n + 1, np.uint64)
+        N.check(self.lib.bp_batch_layout(h, self.belief_off.ctypes.data, self.msg_off.ctypes.data))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.bp_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def pack_beliefs(self):
+        out = np.zeros(int(self.belief_off[-1]), np.float32)
+        for k, net in enumerate(self.nets):
+            S = net.uniform_states
+            a, b = int(self.belief_off[k]), int(self.belief_off[k + 1])
+            out[a:b] = net.beliefs[:, :S].ravel()
+        return out
+
+    def set_beliefs(self, flat=None):
+        flat = self.pack_beliefs() if flat is None else flat
+        mem = N.BP_MEM_DEVICE if (hasattr(flat, "is_cuda") and flat.is_cuda) else N.BP_MEM_HOST
+        if mem == N.BP_MEM_HOST:
+            flat = np.ascontiguousarray(flat, np.float32)
+        N.check(self.lib.bp_batch_set_beliefs(self.h, N.ptr(flat), mem))
+
+    def beliefs(self, k=None):
+        flat = np.zeros(int(self.belief_off[-1]), np.float32)
+        N.check(self.lib.bp_batch_get_beliefs(self.h, flat.ctypes.data, N.BP_MEM_HOST))
+        if k is None:
+            return flat
+        S = self.nets[k].uniform_states
+        return flat[int(self.belief_off[k]):int(self.belief_off[k + 1])].reshape(-1, S)
+
+    def messages(self, k=None):
+        flat = np.zeros(max(int(self.msg_off[-1]), 1), np.float32)
+        N.check(self.lib.bp_batch_get_messages(self.h, flat.ctypes.data, N.BP_MEM_HOST))
+        if k is None:
+            return flat
+        S = self.nets[k].uniform_states
+        return flat[int(self.msg_off[k]):int(self.msg_off[k + 1])].reshape(-1, S)
+
+    def options(self, tol=1e-4, max_iterations=200, delta="f64", block_threads=0, init=True):
+        o = N.BatchOptions()
+        self.lib.bp_batch_default_options(C.byref(o))
+        o.tolerance, o.max_iterations = float(tol), int(max_iterations)
+        o.delta_mode = _DELTA[delta]
+        o.block_threads, o.init_messages = int(block_threads), int(bool(init))
+        return o
+
+    def autotune(self, **kw):
+        N.check(self.lib.bp_batch_autotune(self.h, C.byref(self.options(**kw))))
+        return self.block_threads()
+
+    def block_threads(self):
+        n = C.c_uint32(16)
+        st = np.zeros(16, np.uint32)
+        bl = np.zeros(16, np.uint32)
+        N.check(self.lib.bp_batch_get_block_threads(self.h, st.ctypes.data, bl.ctypes.data, C.byref(n)))
+        return {int(st[i]): int(bl[i]) for i in range(n.value)}
+
+    def loopy(self, **kw):
+        r = N.BatchResult()
+        N.check(self.lib.bp_batch_loopy(self.h, C.byref(self.options(**kw)), C.byref(r)))
+        return r.as_dict()
+
+    def results(self):
+        n = len(self.nets)
+        it = np.zeros(n, np.uint32)
+        ex = np.zeros(n, np.uint32)
+        cv = np.zeros(n, np.int32)
+        dl = np.zeros(n, np.float32)
+        N.check(self.lib.bp_batch_network_results(self.h, it.ctypes.data, ex.ctypes.data, cv.ctypes.data,
+                                                  dl.ctypes.data))
+        return dict(iterations=it, executed=ex, converged=cv, delta=dl)

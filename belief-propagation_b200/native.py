@@ -42,12 +42,25 @@ class GraphDesc(C.Structure):
 class LoopyOptions(C.Structure):
     _fields_ = [("tolerance", C.c_float), ("max_iterations", C.c_uint32), ("check_every", C.c_uint32),
                 ("schedule", C.c_int32), ("delta_mode", C.c_int32), ("verbose", C.c_int32),
-                ("graph_chunk", C.c_uint32), ("reserved", C.c_int32)]
+                ("graph_chunk", C.c_uint32), ("kernel_variant", C.c_int32)]
 
 
 class LoopyResult(C.Structure):
     _fields_ = [("iterations", C.c_uint32), ("executed", C.c_uint32), ("converged", C.c_int32),
                 ("delta", C.c_float), ("previous_delta", C.c_float), ("delta_f64", C.c_double),
+                ("elapsed_ms", C.c_float)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class BatchOptions(C.Structure):
+    _fields_ = [("tolerance", C.c_float), ("max_iterations", C.c_uint32), ("delta_mode", C.c_int32),
+                ("block_threads", C.c_uint32), ("init_messages", C.c_int32), ("reserved", C.c_int32)]
+
+
+class BatchResult(C.Structure):
+    _fields_ = [("num_networks", C.c_uint32), ("converged", C.c_uint32), ("max_executed", C.c_uint32),
                 ("elapsed_ms", C.c_float)]
 
     def as_dict(self):
@@ -91,7 +104,11 @@ BP_SYMBOLS = [
     "bp_loopy_default_options", "bp_init_messages", "bp_loopy", "bp_tree_build_levels",
     "bp_tree_set_levels", "bp_tree_start", "bp_tree_level", "bp_tree_reset_visited",
     "bp_tree_marginalize", "bp_tree", "bp_set_visited", "bp_get_visited", "bp_set_sync_mode",
-    "bp_sync_host", "bp_graph_of", "bp_loopy_noalloc",
+    "bp_sync_host", "bp_graph_of", "bp_loopy_noalloc", "bp_batch_create", "bp_batch_destroy",
+    "bp_batch_layout", "bp_batch_set_beliefs", "bp_batch_get_beliefs", "bp_batch_get_messages",
+    "bp_batch_default_options", "bp_batch_autotune", "bp_batch_get_block_threads", "bp_batch_loopy",
+    "bp_batch_network_results", "bp_unrolled_create", "bp_unrolled_destroy", "bp_unrolled_set_stream",
+    "bp_unrolled_forward", "bp_unrolled_backward",
 ]
 GRAPH_SYMBOLS = [
     "create_graph", "graph_add_node", "graph_add_and_set_node_state", "graph_set_node_state",
@@ -140,6 +157,19 @@ def load(path=LIB_PATH):
         "bp_graph_of": ([vp, C.POINTER(vp)], i32),
         "bp_loopy_noalloc": ([u32, u32, u32, vp, vp, vp, vp, vp, i32, i32, C.c_float, u32, vp,
                               C.POINTER(LoopyResult), C.POINTER(i32)], i32),
+        "bp_batch_create": ([C.POINTER(vp), u32, C.POINTER(GraphDesc), vp], i32),
+        "bp_batch_destroy": ([vp], None),
+        "bp_batch_layout": ([vp, vp, vp], i32),
+        "bp_batch_set_beliefs": ([vp, vp, i32], i32), "bp_batch_get_beliefs": ([vp, vp, i32], i32),
+        "bp_batch_get_messages": ([vp, vp, i32], i32),
+        "bp_batch_default_options": ([C.POINTER(BatchOptions)], None),
+        "bp_batch_autotune": ([vp, C.POINTER(BatchOptions)], i32),
+        "bp_batch_get_block_threads": ([vp, vp, vp, C.POINTER(u32)], i32),
+        "bp_batch_loopy": ([vp, C.POINTER(BatchOptions), C.POINTER(BatchResult)], i32),
+        "bp_batch_network_results": ([vp, vp, vp, vp, vp], i32),
+        "bp_unrolled_create": ([C.POINTER(vp), u32, u32, u32, u32, vp, vp, vp, u32, u32, vp], i32),
+        "bp_unrolled_destroy": ([vp], None), "bp_unrolled_set_stream": ([vp, vp], i32),
+        "bp_unrolled_forward": ([vp, vp, vp, vp], i32), "bp_unrolled_backward": ([vp, vp, vp, vp], i32),
         # graph.h
         "create_graph": ([C.c_uint, C.c_uint], C.POINTER(StructGraph)),
         "graph_add_node": ([vp, C.c_uint, C.c_char_p], None),

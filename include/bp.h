@@ -60,6 +60,13 @@ typedef enum {
 
 typedef enum { BP_SYNC_EAGER = 0, BP_SYNC_LAZY = 1 } bp_sync_mode;
 
+/* the node-schedule iteration kernel: same results, different tiling */
+typedef enum {
+    BP_KERNEL_AUTO = 0,        /* block tiles (BP_FLOOD_KERNEL=warp in the environment selects warp tiles) */
+    BP_KERNEL_BLOCK_TILE = 1,  /* 256-node block tiles, block-wide barriers between phases */
+    BP_KERNEL_WARP_TILE = 2    /* 32-node warp tiles, unrolled edge loads */
+} bp_kernel_variant;
+
 typedef struct bp_graph bp_graph;
 
 typedef struct {
@@ -88,7 +95,7 @@ typedef struct {
     int32_t delta_mode;       /* bp_delta_mode */
     int32_t verbose;          /* print the reference's "No Convergence" line */
     uint32_t graph_chunk;     /* iterations per CUDA-graph launch; 0 = automatic */
-    int32_t reserved;
+    int32_t kernel_variant;   /* bp_kernel_variant of the node-schedule iteration kernel */
 } bp_loopy_options;
 
 typedef struct {
@@ -197,6 +204,77 @@ int bp_tree_marginalize(bp_graph *g);                 /* graph.c:588-596 */
 int bp_tree(bp_graph *g, bp_tree_result *res);
 int bp_set_visited(bp_graph *g, const char *visited); /* host [V] */
 int bp_get_visited(bp_graph *g, char *visited);       /* host [V] */
+
+/* ---- batched loopy BP -------------------------------------------------- */
+/* Many independent networks, each with its own stopping rule
+ * (loopy_propagate_until per network), solved in one persistent launch per
+ * state count: a thread block takes the next network from a work queue
+ * (largest first) and iterates it to convergence.  Each network's result is
+ * what bp_loopy gives for it alone.  Every node of one network has the same
+ * state count; networks may differ.
+ *
+ * Layout of the batch-wide arrays (bp_batch_layout): network n's beliefs are
+ * [V_n][S_n] floats at belief_offsets[n], its messages [E_n][S_n] (edge-id
+ * order) at message_offsets[n]; offsets[N] is the total. */
+typedef struct bp_batch bp_batch;
+
+typedef struct {
+    float tolerance;          /* per network, the reference's `convergence` */
+    uint32_t max_iterations;  /* per network */
+    int32_t delta_mode;       /* BP_DELTA_F64 (default) or BP_DELTA_SERIAL_F32 */
+    uint32_t block_threads;   /* threads per network block; 0 = as tuned (bp_batch_autotune) */
+    int32_t init_messages;    /* 1: init_previous_edge first */
+    int32_t reserved;
+} bp_batch_options;
+
+typedef struct {
+    uint32_t num_networks;
+    uint32_t converged;       /* networks whose stopping rule fired */
+    uint32_t max_executed;    /* most iterations any network ran */
+    float elapsed_ms;         /* device time of the batched solve */
+} bp_batch_result;
+
+/* descs: one bp_graph_desc per network, host memory */
+int bp_batch_create(bp_batch **out, uint32_t num_networks, const bp_graph_desc *descs, void *stream);
+void bp_batch_destroy(bp_batch *b);
+int bp_batch_layout(const bp_batch *b, uint64_t *belief_offsets, uint64_t *message_offsets);
+/* setting beliefs marks slot 1 as the latest messages of every network, as
+ * create_graph leaves struct graph */
+int bp_batch_set_beliefs(bp_batch *b, const float *beliefs, int memory);
+int bp_batch_get_beliefs(bp_batch *b, float *beliefs, int memory);
+int bp_batch_get_messages(bp_batch *b, float *messages, int memory);
+void bp_batch_default_options(bp_batch_options *o);
+/* times 64/128/256/512 threads per network block for each state-count group
+ * on this batch, keeps the fastest (results cached in $BP_AUTOTUNE_CACHE,
+ * default ~/.cache/bp_b200_autotune.txt); beliefs and messages are restored */
+int bp_batch_autotune(bp_batch *b, const bp_batch_options *o);
+int bp_batch_get_block_threads(const bp_batch *b, uint32_t *states, uint32_t *block, uint32_t *count);
+/* the whole batch: one CUDA graph launch */
+int bp_batch_loopy(bp_batch *b, const bp_batch_options *o, bp_batch_result *r);
+int bp_batch_network_results(bp_batch *b, uint32_t *iterations, uint32_t *executed, int32_t *converged,
+                             float *delta);
+
+/* ---- differentiable unrolled loopy BP --------------------------------- */
+/* T synchronous iterations of the reference's update on a pairwise model:
+ * priors softmax(log_unary[v]), joint tables exp(log_pair[k]) shared by the
+ * edges that name table k (edge_table[e] & 0x7f; bit 0x80 = the edge uses
+ * the transposed table).  bp_unrolled_forward writes the beliefs after T
+ * iterations; bp_unrolled_backward maps d loss / d beliefs to gradients with
+ * respect to log_unary and log_pair with a hand-written adjoint.  The forward
+ * keeps the iteration state every checkpoint_every iterations; the backward
+ * recomputes each segment from its checkpoint.  All tensor arguments of
+ * forward/backward are device memory; the graph arrays of create are host
+ * memory.  At most 16 tables. */
+typedef struct bp_unrolled bp_unrolled;
+int bp_unrolled_create(bp_unrolled **out, uint32_t num_nodes, uint32_t num_edges, uint32_t num_states,
+                       uint32_t num_tables, const uint32_t *edge_src, const uint32_t *edge_dst,
+                       const uint8_t *edge_table, uint32_t iterations, uint32_t checkpoint_every,
+                       void *stream);
+void bp_unrolled_destroy(bp_unrolled *u);
+int bp_unrolled_set_stream(bp_unrolled *u, void *stream);
+int bp_unrolled_forward(bp_unrolled *u, const float *log_unary, const float *log_pair, float *beliefs);
+int bp_unrolled_backward(bp_unrolled *u, const float *grad_beliefs, float *grad_log_unary,
+                         float *grad_log_pair);
 
 /* ---- drop-in support (struct graph from graph.h) ---------------------- */
 struct graph;

@@ -1,0 +1,102 @@
+"""Differentiable unrolled BP: forward against a pure-torch unrolled
+reference of the same update, gradients against that reference's autograd
+and against FP64 finite differences on a 16x16 grid."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(side, S, T, seed, ck=5):
+    import torch
+    from belief_propagation_b200.unrolled import UnrolledBP, grid_tables
+    src, dst, tab = grid_tables(side)
+    rng = np.random.default_rng(seed)
+    V = side * side
+    theta = torch.tensor(rng.normal(0, 1, (V, S)), dtype=torch.float32, device="cuda", requires_grad=True)
+    W = torch.tensor(rng.normal(0, 0.5, (1, S, S)), dtype=torch.float32, device="cuda", requires_grad=True)
+    labels = torch.tensor(rng.integers(0, S, V), device="cuda")
+    eng = UnrolledBP(V, src, dst, tab, S, T, checkpoint_every=ck)
+    return eng, theta, W, labels, (src, dst, tab)
+
+
+def _loss(b, labels):
+    import torch
+    return torch.nn.functional.nll_loss(torch.log(b), labels)
+
+
+@pytest.mark.parametrize("side,S,T,ck", [(16, 4, 30, 5), (32, 8, 20, 5), (24, 3, 7, 3), (16, 4, 30, 1),
+                                         (16, 2, 6, 100)])
+def test_unrolled_matches_torch_reference(bp, side, S, T, ck):
+    import torch
+    from belief_propagation_b200.unrolled import torch_unrolled
+    eng, theta, W, labels, (src, dst, tab) = _setup(side, S, T, seed=side * 7 + S, ck=ck)
+    b = eng(theta, W)
+    loss = _loss(b, labels)
+    loss.backward()
+    g_theta, g_W = theta.grad.detach().clone(), W.grad.detach().clone()
+    th64 = theta.detach().double().requires_grad_(True)
+    W64 = W.detach().double().requires_grad_(True)
+    b64 = torch_unrolled(th64, W64, src, dst, tab, T)
+    _loss(b64, labels).backward()
+    np.testing.assert_allclose(b.detach().cpu().numpy(), b64.detach().cpu().numpy(), atol=2e-5)
+    scale_t = th64.grad.abs().max().item()
+    scale_w = W64.grad.abs().max().item()
+    np.testing.assert_allclose(g_theta.cpu().numpy(), th64.grad.cpu().numpy(), atol=2e-4 * scale_t + 1e-7)
+    np.testing.assert_allclose(g_W.cpu().numpy(), W64.grad.cpu().numpy(), atol=2e-4 * scale_w + 1e-7)
+    eng.close()
+
+
+def test_unrolled_gradient_fp64_finite_differences(bp):
+    """16x16 grid, 4 states, T = 30: central differences in FP64 through the
+    torch reference, on a sample of coordinates of both parameters."""
+    import torch
+    from belief_propagation_b200.unrolled import torch_unrolled
+    side, S, T = 16, 4, 30
+    eng, theta, W, labels, (src, dst, tab) = _setup(side, S, T, seed=3)
+    _loss(eng(theta, W), labels).backward()
+    th0, W0 = theta.detach().double(), W.detach().double()
+
+    def f(th, w):
+        with torch.no_grad():
+            return _loss(torch_unrolled(th, w, src, dst, tab, T), labels).item()
+
+    h = 1e-5
+    rng = np.random.default_rng(0)
+    for _ in range(12):
+        v, i = int(rng.integers(0, side * side)), int(rng.integers(0, S))
+        tp, tm = th0.clone(), th0.clone()
+        tp[v, i] += h
+        tm[v, i] -= h
+        fd = (f(tp, W0) - f(tm, W0)) / (2 * h)
+        assert abs(theta.grad[v, i].item() - fd) <= 1e-4 * max(1e-3, abs(fd)) + 2e-6, (v, i)
+    for i in range(S):
+        for j in range(S):
+            wp, wm = W0.clone(), W0.clone()
+            wp[0, i, j] += h
+            wm[0, i, j] -= h
+            fd = (f(th0, wp) - f(th0, wm)) / (2 * h)
+            assert abs(W.grad[0, i, j].item() - fd) <= 2e-4 * max(1e-3, abs(fd)) + 2e-6, (i, j)
+    eng.close()
+
+
+def test_unrolled_forward_equals_plain_engine_update(bp, synth):
+    """The unrolled forward is the reference's update: with the same tables
+    and priors the plain engine (tolerance 0, T fixed iterations) gives the
+    same beliefs up to fp32 rounding of exp/softmax inputs."""
+    import torch
+    from belief_propagation_b200.engine import BPGraph
+    side, S, T = 20, 4, 12
+    eng, theta, W, labels, (src, dst, tab) = _setup(side, S, T, seed=11)
+    b = eng(theta, W).detach().cpu().numpy()
+    E = np.exp(W.detach().cpu().numpy()[0])
+    joint = np.where((tab & 0x80)[:, None, None] != 0, E.T[None], E[None]).astype(np.float32)
+    prior = torch.softmax(theta.detach(), 1).cpu().numpy()
+    net = synth.Network(np.full(side * side, S, np.uint32), prior, np.zeros(side * side, np.uint8), src, dst, joint)
+    g = BPGraph.from_network(net)
+    g.latest_slot = 1
+    g.init_messages()
+    g.loopy(0.0, T, delta="f64")
+    np.testing.assert_allclose(g.beliefs(), b, atol=1e-5)
+    g.close()
+    eng.close()
