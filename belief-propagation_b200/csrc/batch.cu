@@ -393,6 +393,12 @@ static int batch_create_impl(bp_batch *bt, uint32_t N, const bp_graph_desc *desc
         if (d.num_nodes == 0) return set_error(BP_ERR_SHAPE, "network %u has no nodes", n);
         if (d.joint_row_stride < S || d.joint_edge_stride < (uint64_t)d.joint_row_stride * (S - 1) + S)
             return set_error(BP_ERR_SHAPE, "network %u: joint strides too small", n);
+        // every network's arrays start on a 16-byte boundary: the kernels load
+        // S, S*S floats at a time as float2/float4 when S allows it
+        node_f = (node_f + 3) & ~(uint64_t)3;
+        msg_f = (msg_f + 3) & ~(uint64_t)3;
+        joint_f = (joint_f + 3) & ~(uint64_t)3;
+        h_joint.resize(joint_f, 0.0f);
         NetInfo &ni = bt->info[n];
         ni.V = d.num_nodes;
         ni.E = d.num_edges;
@@ -430,6 +436,11 @@ static int batch_create_impl(bp_batch *bt, uint32_t N, const bp_graph_desc *desc
         edges += ni.E;
         nodes += ni.V;
     }
+    node_f = (node_f + 3) & ~(uint64_t)3;
+    msg_f = (msg_f + 3) & ~(uint64_t)3;
+    for (const NetInfo &ni : bt->info)
+        if ((ni.node_off | ni.msg_off | ni.joint_off) & 3u)
+            return set_error(BP_ERR_STATE, "internal: unaligned network offsets");
     bt->totV = nodes;
     bt->totE = edges;
     bt->totNodeF = node_f;

@@ -76,6 +76,9 @@ struct bp_graph {
     bool own_stream = false;
 
     uint32_t *in_ptr = nullptr, *in_src = nullptr, *pos_edge = nullptr, *edge_pos = nullptr;
+    // node renumbering (BP_GRAPH_REORDER_BY_OUT_DEGREE): internal id i holds the
+    // caller's node new_to_old[i]; null when ids are the caller's
+    uint32_t *new_to_old = nullptr;
     uint8_t *pos_dims = nullptr, *node_s = nullptr;
     float *joint = nullptr;
     float *belief = nullptr;

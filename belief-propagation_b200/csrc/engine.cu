@@ -126,23 +126,57 @@ __global__ void k_gather_joint(const float *__restrict__ jin, uint32_t rs, uint6
 
 // beliefs [V][ld] <-> [V][MS] (zero beyond S_v)
 __global__ void k_beliefs_in(const float *__restrict__ in, uint32_t ld, uint32_t V, uint32_t ms,
-                             const uint8_t *__restrict__ node_s, uint32_t uniform, float *__restrict__ b) {
+                             const uint8_t *__restrict__ node_s, uint32_t uniform, const uint32_t *__restrict__ perm,
+                             float *__restrict__ b) {
     uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     uint64_t v = t / ms;
     if (v >= V) return;
     uint32_t i = (uint32_t)(t % ms);
     uint32_t s = uniform ? uniform : node_s[v];
-    b[t] = (i < s) ? in[v * ld + i] : 0.0f;
+    const uint64_t row = perm ? perm[v] : v;
+    b[t] = (i < s) ? in[row * ld + i] : 0.0f;
 }
 
 __global__ void k_beliefs_out(const float *__restrict__ b, uint32_t ld, uint32_t V, uint32_t ms,
-                              const uint8_t *__restrict__ node_s, uint32_t uniform, float *__restrict__ out) {
+                              const uint8_t *__restrict__ node_s, uint32_t uniform, const uint32_t *__restrict__ perm,
+                              float *__restrict__ out) {
     uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     uint64_t v = t / ms;
     if (v >= V) return;
     uint32_t i = (uint32_t)(t % ms);
     uint32_t s = uniform ? uniform : node_s[v];
-    if (i < ld && i < s) out[v * ld + i] = b[t];
+    const uint64_t row = perm ? perm[v] : v;
+    if (i < ld && i < s) out[row * ld + i] = b[t];
+}
+
+// out-degree histogram and the renumbering by decreasing out-degree
+__global__ void k_out_degree(const uint32_t *__restrict__ src, uint32_t E, uint32_t *__restrict__ deg) {
+    uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < E) atomicAdd(deg + src[e], 1u);
+}
+
+__global__ void k_degree_keys(uint32_t *__restrict__ deg, uint32_t V, uint32_t *__restrict__ iota) {
+    uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= V) return;
+    deg[v] = 0xffffffffu - deg[v];
+    iota[v] = (uint32_t)v;
+}
+
+__global__ void k_invert_perm(const uint32_t *__restrict__ new_to_old, uint32_t V, uint32_t *__restrict__ old_to_new) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < V) old_to_new[new_to_old[i]] = (uint32_t)i;
+}
+
+__global__ void k_relabel(const uint32_t *__restrict__ in, uint64_t n, const uint32_t *__restrict__ old_to_new,
+                          uint32_t *__restrict__ out) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = old_to_new[in[i]];
+}
+
+__global__ void k_permute_u8(const uint8_t *__restrict__ in, const uint32_t *__restrict__ new_to_old, uint32_t V,
+                             uint8_t *__restrict__ out) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < V) out[i] = in[new_to_old[i]];
 }
 
 // messages [E][ld] edge-id order <-> [E][MS] position order (zero beyond x)
@@ -305,7 +339,7 @@ int ensure_out_csr(bp_graph *g) {
 
 static void free_graph(bp_graph *g) {
     if (!g) return;
-    void *ptrs[] = {g->in_ptr, g->in_src, g->pos_edge, g->edge_pos, g->pos_dims, g->node_s, g->joint,
+    void *ptrs[] = {g->new_to_old, g->in_ptr, g->in_src, g->pos_edge, g->edge_pos, g->pos_dims, g->node_s, g->joint,
                     g->belief, g->msg[0], g->msg[1], g->q[0], g->q[1], g->out_ptr, g->out_pos,
                     g->out_dst, g->pos_dst, g->partials, g->absdiff, g->ctl, g->visited, g->staging,
                     g->run_len, g->run_s, g->tree.d_node_level, g->tree.d_node_lidx, g->tree.d_wave_nodes};
@@ -415,6 +449,63 @@ static int create_impl(bp_graph *g, const bp_graph_desc *d) {
         }
     }
 
+
+    if (d->flags & BP_GRAPH_REORDER_BY_OUT_DEGREE) {
+        if (d->dest_node_list) return set_error(BP_ERR_INVALID, "renumbering ignores a caller CSR: pass none");
+        // internal id = rank by (out-degree descending, id ascending)
+        uint32_t *deg = nullptr, *iota = nullptr, *keys = nullptr, *old_to_new = nullptr;
+        BP_CUDA(cudaMallocAsync((void **)&deg, sizeof(uint32_t) * (V ? V : 1), g->stream));
+        BP_CUDA(cudaMallocAsync((void **)&iota, sizeof(uint32_t) * (V ? V : 1), g->stream));
+        BP_CUDA(cudaMallocAsync((void **)&keys, sizeof(uint32_t) * (V ? V : 1), g->stream));
+        BP_CUDA(cudaMallocAsync((void **)&old_to_new, sizeof(uint32_t) * (V ? V : 1), g->stream));
+        if ((st = dev_alloc(g, (void **)&g->new_to_old, sizeof(uint32_t) * (size_t)V))) return st;
+        BP_CUDA(cudaMemsetAsync(deg, 0, sizeof(uint32_t) * V, g->stream));
+        if (E) k_out_degree<<<grid_for(E, 256), 256, 0, g->stream>>>((const uint32_t *)src, E, deg);
+        if (V) k_degree_keys<<<grid_for(V, 256), 256, 0, g->stream>>>(deg, V, iota);
+        BP_CUDA(cudaGetLastError());
+        if (V) {
+            size_t temp = 0;
+            BP_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp, deg, keys, iota, g->new_to_old, (int64_t)V, 0, 32,
+                                                    g->stream));
+            void *tmp = nullptr;
+            BP_CUDA(cudaMallocAsync(&tmp, temp, g->stream));
+            cudaError_t se = cub::DeviceRadixSort::SortPairs(tmp, temp, deg, keys, iota, g->new_to_old, (int64_t)V, 0,
+                                                             32, g->stream);
+            cudaFreeAsync(tmp, g->stream);
+            if (se != cudaSuccess) return cuda_fail(se, "DeviceRadixSort::SortPairs", __FILE__, __LINE__);
+            k_invert_perm<<<grid_for(V, 256), 256, 0, g->stream>>>(g->new_to_old, V, old_to_new);
+        }
+        uint32_t *src2 = nullptr, *dst2 = nullptr;
+        BP_CUDA(cudaMallocAsync((void **)&src2, sizeof(uint32_t) * (E ? E : 1), g->stream));
+        BP_CUDA(cudaMallocAsync((void **)&dst2, sizeof(uint32_t) * (E ? E : 1), g->stream));
+        if (E) {
+            k_relabel<<<grid_for(E, 256), 256, 0, g->stream>>>((const uint32_t *)src, E, old_to_new, src2);
+            k_relabel<<<grid_for(E, 256), 256, 0, g->stream>>>((const uint32_t *)dst, E, old_to_new, dst2);
+        }
+        if (V) {
+            uint8_t *s8 = nullptr;
+            BP_CUDA(cudaMallocAsync((void **)&s8, V, g->stream));
+            k_permute_u8<<<grid_for(V, 256), 256, 0, g->stream>>>(g->node_s, g->new_to_old, V, s8);
+            BP_CUDA(cudaMemcpyAsync(g->node_s, s8, V, cudaMemcpyDeviceToDevice, g->stream));
+            cudaFreeAsync(s8, g->stream);
+            std::vector<uint32_t> perm(V);
+            BP_CUDA(cudaMemcpyAsync(perm.data(), g->new_to_old, sizeof(uint32_t) * V, cudaMemcpyDeviceToHost,
+                                    g->stream));
+            BP_CUDA(cudaStreamSynchronize(g->stream));
+            std::vector<uint8_t> s_old(g->node_s_host, g->node_s_host + V);
+            for (uint32_t i = 0; i < V; ++i) g->node_s_host[i] = s_old[perm[i]];
+        }
+        BP_CUDA(cudaGetLastError());
+        cudaFreeAsync(deg, g->stream);
+        cudaFreeAsync(iota, g->stream);
+        cudaFreeAsync(keys, g->stream);
+        cudaFreeAsync(old_to_new, g->stream);
+        if (own_src) cudaFreeAsync(src, g->stream);
+        if (own_dst) cudaFreeAsync(dst, g->stream);
+        src = src2;
+        dst = dst2;
+        own_src = own_dst = true;
+    }
 
     if (d->dest_node_list && d->dest_edge_list) {
         // the caller's dest-CSR (struct graph's dest_nodes_to_edges_*)
@@ -595,7 +686,8 @@ int bp_set_beliefs(bp_graph *g, const float *b, uint32_t ld, int memory) {
     int st = staged_in(g, b, sizeof(float) * (size_t)ld * g->V, memory, &dev);
     if (st) return st;
     uint64_t n = (uint64_t)g->V * g->ms;
-    k_beliefs_in<<<grid_for(n, 256), 256, 0, g->stream>>>(dev, ld, g->V, g->ms, g->node_s, g->uniform, g->belief);
+    k_beliefs_in<<<grid_for(n, 256), 256, 0, g->stream>>>(dev, ld, g->V, g->ms, g->node_s, g->uniform, g->new_to_old,
+                                                          g->belief);
     BP_CUDA(cudaGetLastError());
     if (memory == BP_MEM_HOST) BP_CUDA(cudaStreamSynchronize(g->stream));
     return BP_OK;
@@ -606,11 +698,12 @@ int bp_get_beliefs(bp_graph *g, float *b, uint32_t ld, int memory) {
     if (g->V == 0) return BP_OK;
     uint64_t n = (uint64_t)g->V * g->ms;
     if (memory == BP_MEM_DEVICE) {
-        k_beliefs_out<<<grid_for(n, 256), 256, 0, g->stream>>>(g->belief, ld, g->V, g->ms, g->node_s, g->uniform, b);
+        k_beliefs_out<<<grid_for(n, 256), 256, 0, g->stream>>>(g->belief, ld, g->V, g->ms, g->node_s, g->uniform,
+                                                               g->new_to_old, b);
         BP_CUDA(cudaGetLastError());
         return BP_OK;
     }
-    if (ld == g->ms) {
+    if (ld == g->ms && !g->new_to_old) {
         BP_CUDA(cudaMemcpyAsync(b, g->belief, sizeof(float) * n, cudaMemcpyDeviceToHost, g->stream));
         BP_CUDA(cudaStreamSynchronize(g->stream));
         return BP_OK;
@@ -621,7 +714,7 @@ int bp_get_beliefs(bp_graph *g, float *b, uint32_t ld, int memory) {
     // keep the caller's slots beyond each node's state count intact
     BP_CUDA(cudaMemcpyAsync(g->staging, b, bytes, cudaMemcpyHostToDevice, g->stream));
     k_beliefs_out<<<grid_for(n, 256), 256, 0, g->stream>>>(g->belief, ld, g->V, g->ms, g->node_s, g->uniform,
-                                                           g->staging);
+                                                           g->new_to_old, g->staging);
     BP_CUDA(cudaGetLastError());
     BP_CUDA(cudaMemcpyAsync(b, g->staging, bytes, cudaMemcpyDeviceToHost, g->stream));
     BP_CUDA(cudaStreamSynchronize(g->stream));

@@ -842,6 +842,8 @@ int bp_loopy(bp_graph *g, const bp_loopy_options *opt, bp_loopy_result *res) {
         return set_error(BP_ERR_INVALID, "unknown schedule %d", opt->schedule);
     if (opt->delta_mode < BP_DELTA_AUTO || opt->delta_mode > BP_DELTA_F64)
         return set_error(BP_ERR_INVALID, "unknown delta mode %d", opt->delta_mode);
+    if (opt->schedule == BP_SCHEDULE_EDGE && g->new_to_old)
+        return set_error(BP_ERR_STATE, "edge schedule on a renumbered graph (BP_GRAPH_REORDER_BY_OUT_DEGREE)");
     const uint32_t ce = opt->check_every <= 1 ? 1u : opt->check_every;
     const uint32_t max_it = opt->max_iterations;
     bp_loopy_result r = {};
@@ -1122,6 +1124,9 @@ extern "C" int bp_loopy_noalloc(uint32_t num_nodes, uint32_t num_edges, uint32_t
     if (!in_ptr || !beliefs || (num_edges && (!in_src || !joint || !messages)))
         return set_error(BP_ERR_INVALID, "null array");
     if (latest_slot != 0 && latest_slot != 1) return set_error(BP_ERR_INVALID, "latest_slot must be 0 or 1");
+    // the kernels read S (and S*S) floats at a time as float2/float4
+    if (((uintptr_t)joint | (uintptr_t)beliefs | (uintptr_t)messages) & 15u)
+        return set_error(BP_ERR_INVALID, "joint, beliefs and messages must be 16-byte aligned");
     if (max_iterations == 0) {
         // the reference's loop body never runs: nothing to launch
         if (result) {

@@ -124,6 +124,7 @@ static void tree_clear(bp_graph *g) {
 
 static int tree_prepare(bp_graph *g, const uint32_t *levels, uint32_t num_levels) {
     const uint32_t V = g->V;
+    if (g->new_to_old) return set_error(BP_ERR_STATE, "tree BP on a renumbered graph (BP_GRAPH_REORDER_BY_OUT_DEGREE)");
     TreeData &t = g->tree;
     if (t.ready && t.num_levels == num_levels &&
         (V == 0 || memcmp(t.levels_host, levels, sizeof(uint32_t) * 2 * (size_t)V) == 0))
@@ -219,6 +220,7 @@ extern "C" {
 
 int bp_tree_build_levels(bp_graph *g, uint32_t *levels, uint32_t *num_levels) {
     if (!g || !num_levels) return set_error(BP_ERR_INVALID, "null argument");
+    if (g->new_to_old) return set_error(BP_ERR_STATE, "tree BP on a renumbered graph (BP_GRAPH_REORDER_BY_OUT_DEGREE)");
     int st;
     if ((st = ensure_out_csr(g))) return st;
     if ((st = ensure_host_in_ptr(g))) return st;

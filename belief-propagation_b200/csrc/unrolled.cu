@@ -1,28 +1,30 @@
-// unrolled.cu -- T-step unrolled loopy BP and its adjoint.
+// unrolled.cu -- T-step unrolled loopy BP and its adjoint, in the log domain.
 //
 // The forward pass is the reference's update (graph.c:725-751, :1121-1183)
 // on a pairwise model whose priors are softmax(log_unary) and whose joint
 // tables are exp(log_pair) shared by many edges (edge e uses table
-// tab[e] & 0x7f, transposed when tab[e] & 0x80):
-//   b_0 = softmax(theta)            m_0(e) = normalise(J_e . b_0(src))
-//   Q_1 = b_0 * prod_in m_0
-//   t = 1..T:  m_t(e) = normalise(J_e . Q_t(src))
-//              b_t    = normalise(b_{t-1} * prod_in m_t)
-//              Q_{t+1}= b_t * prod_in m_t
-// The state carried between iterations is (b, Q); messages are recomputed
-// from Q wherever needed and never stored.  The forward keeps (b_t, Q_{t+1})
-// every `checkpoint_every` iterations; the backward recomputes the states of
-// one segment from its checkpoint and runs the adjoint of each step in
-// reverse:
-//   from Q_{t+1} = b_t * P:  bbar_t += Qbar_{t+1} * P,  Pbar = Qbar_{t+1} * b_t
-//   from b_t = u / sum(u):   ubar = (bbar_t - <bbar_t, b_t>) / sum(u)
-//   from u = b_{t-1} * P:    bbar_{t-1} = ubar * P,     Pbar += ubar * b_{t-1}
-//   from P = prod_e m_e:     mbar_e = Pbar * prod_{e' != e} m_e'
-//   from m = r / sum(r):     rbar = (mbar - <mbar, m>) / sum(r)
-//   from r = J Q(src):       Qbar_t(src) += J^T rbar,   Ebar += rbar (x) Q(src)
-// and finally theta_bar = b_0 * (bbar_0 - <bbar_0, b_0>), log_pair_bar =
-// Ebar * exp(log_pair).  The Q(src) adjoint is a gather over the
-// source-sorted edge list, so no atomics and the result is deterministic.
+// tab[e] & 0x7f, transposed when tab[e] & 0x80), carried in logs so that
+// beliefs compounding towards 0 (the reference's update multiplies the
+// belief into itself every iteration) never underflow:
+//   lb_0 = log_softmax(theta)
+//   lm(e)[i] = r_i - LSE_i r,  r_i = LSE_j (logJ_e[i][j] + x_src[j])
+//   lQ_1 = lb_0 + sum_in lm_0            (messages from x = lb_0)
+//   t = 1..T:  lP = sum_in lm_t          (messages from x = lQ_t)
+//              lb_t = lb_{t-1} + lP - LSE(lb_{t-1} + lP)
+//              lQ_{t+1} = lb_t + lP
+// The output is lb_T (log-beliefs).  The state between iterations is
+// (lb, lQ); messages are recomputed from lQ wherever needed and never stored.
+// The forward keeps the state every `checkpoint_every` iterations; the
+// backward recomputes one segment from its checkpoint and runs the adjoint
+// of each step in reverse:
+//   g = lbbar_t + lQbar_{t+1};  abar = g - b_t * sum(g)  (b_t = exp lb_t)
+//   lbbar_{t-1} = abar;  lPbar = abar + lQbar_{t+1};  lmbar_e = lPbar (every in-edge)
+//   rbar = lmbar - m * sum(lmbar)  (m = exp lm);   w_ij = exp(logJ_ij + x_j - r_i)
+//   xbar_src[j] += sum_i rbar_i w_ij;   logJbar_ij += rbar_i w_ij
+// and finally theta_bar = lbbar_0 - softmax(theta) * sum(lbbar_0).  The
+// x_src adjoint is a gather over the source-sorted edge list (w recomputed
+// from the source's own state), so no atomics and the result is
+// deterministic.
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -43,7 +45,7 @@ struct UGraph {
     uint32_t V, K;
     const uint32_t *in_ptr, *in_src, *out_ptr, *out_pos;
     const uint8_t *pos_tab;
-    const float *tables;   // [K][S][S] = exp(log_pair)
+    const float *tables;   // [K][S][S] = log_pair (log joint tables)
 };
 
 template <int S>
@@ -63,121 +65,108 @@ __device__ __forceinline__ const float *edge_table(const float *sm, uint8_t tab)
     return sm + (2u * (tab & 0x7fu) + ((tab & 0x80u) ? 1u : 0u)) * S * S;
 }
 
-// r = J q, R = sum r (<= 0 -> 1), m = r / R
+template <int N>
+__device__ __forceinline__ float lse(const float *a) {
+    float mx = a[0];
+#pragma unroll
+    for (int i = 1; i < N; ++i) mx = fmaxf(mx, a[i]);
+    if (mx == -INFINITY) return -INFINITY;
+    float s = 0.0f;
+#pragma unroll
+    for (int i = 0; i < N; ++i) s += expf(a[i] - mx);
+    return mx + logf(s);
+}
+
+// log-message of one edge: r_i = LSE_j(L_ij + x_j), lm_i = r_i - LSE(r)
 template <int S>
-__device__ __forceinline__ float msg_r(const float *J, const float *q, float *m) {
-    float R = 0.0f;
+__device__ __forceinline__ void log_msg(const float *L, const float *x, float *r, float *lm) {
 #pragma unroll
     for (int i = 0; i < S; ++i) {
-        float r = 0.0f;
+        float t[S];
 #pragma unroll
-        for (int j = 0; j < S; ++j) r = FADD(r, FMUL(J[i * S + j], q[j]));
-        m[i] = r;
-        R = FADD(R, r);
+        for (int j = 0; j < S; ++j) t[j] = L[i * S + j] + x[j];
+        r[i] = lse<S>(t);
     }
-    if (R <= 0.0f) R = 1.0f;
+    const float z = lse<S>(r);
 #pragma unroll
-    for (int i = 0; i < S; ++i) m[i] = FDIV(m[i], R);
-    return R;
+    for (int i = 0; i < S; ++i) lm[i] = r[i] - z;
 }
 
 template <int S>
-__global__ void k_u_exp(const float *__restrict__ logp, uint32_t n, float *__restrict__ tab) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) tab[i] = expf(logp[i]);
-}
-
-template <int S>
-__global__ void k_u_softmax(uint32_t V, const float *__restrict__ theta, float *__restrict__ b0) {
+__global__ void k_u_logsoftmax(uint32_t V, const float *__restrict__ theta, float *__restrict__ lb0) {
     const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= V) return;
-    float t[S], mx = -INFINITY;
+    float t[S];
     ldv<S>(theta + (size_t)v * S, t);
+    const float z = lse<S>(t);
 #pragma unroll
-    for (int i = 0; i < S; ++i) mx = fmaxf(mx, t[i]);
-    float z = 0.0f;
+    for (int i = 0; i < S; ++i) t[i] -= z;
+    stv<S>(lb0 + (size_t)v * S, t);
+}
+
+// lQ = lb + sum_in lm(send)   (graph.c:860-882 after :725-751)
+template <int S>
+__global__ void __launch_bounds__(kUThreads) k_u_gather_q(const UGraph g, const float *__restrict__ lb,
+                                                          const float *__restrict__ send, float *__restrict__ lq) {
+    __shared__ float sm[2 * kUMaxTables * S * S];
+    load_tables_smem<S>(g, sm);
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= g.V) return;
+    float qo[S];
+    ldv<S>(lb + (size_t)v * S, qo);
+    for (uint32_t p = g.in_ptr[v]; p < g.in_ptr[v + 1]; ++p) {
+        float x[S], r[S], m[S];
+        ldv<S>(send + (size_t)g.in_src[p] * S, x);
+        log_msg<S>(edge_table<S>(sm, g.pos_tab[p]), x, r, m);
+#pragma unroll
+        for (int i = 0; i < S; ++i) qo[i] += m[i];
+    }
+    stv<S>(lq + (size_t)v * S, qo);
+}
+
+// one forward iteration: (lb_{t-1}, lQ_t) -> (lb_t, lQ_{t+1})
+template <int S>
+__global__ void __launch_bounds__(kUThreads) k_u_iter(const UGraph g, const float *__restrict__ lb_in,
+                                                      const float *__restrict__ lq_in, float *__restrict__ lb_out,
+                                                      float *__restrict__ lq_out) {
+    __shared__ float sm[2 * kUMaxTables * S * S];
+    load_tables_smem<S>(g, sm);
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= g.V) return;
+    float P[S], a[S];
+#pragma unroll
+    for (int i = 0; i < S; ++i) P[i] = 0.0f;
+    for (uint32_t p = g.in_ptr[v]; p < g.in_ptr[v + 1]; ++p) {
+        float x[S], r[S], m[S];
+        ldv<S>(lq_in + (size_t)g.in_src[p] * S, x);
+        log_msg<S>(edge_table<S>(sm, g.pos_tab[p]), x, r, m);
+#pragma unroll
+        for (int i = 0; i < S; ++i) P[i] += m[i];
+    }
+    ldv<S>(lb_in + (size_t)v * S, a);
+#pragma unroll
+    for (int i = 0; i < S; ++i) a[i] += P[i];
+    const float z = lse<S>(a);
+    float qo[S];
 #pragma unroll
     for (int i = 0; i < S; ++i) {
-        t[i] = expf(t[i] - mx);
-        z += t[i];
+        a[i] -= z;
+        qo[i] = a[i] + P[i];
     }
-#pragma unroll
-    for (int i = 0; i < S; ++i) t[i] = t[i] / z;
-    stv<S>(b0 + (size_t)v * S, t);
+    stv<S>(lb_out + (size_t)v * S, a);
+    stv<S>(lq_out + (size_t)v * S, qo);
 }
 
-// Q = b * prod_in normalise(J . send(src))   (graph.c:860-882 after :725-751)
+// adjoint of one node step.  mode 0: iteration; mode 1: the initial step
+// (lQ_1 = lb_0 + lP, messages from send = lb_0).  Writes lbbar_out
+// (lbbar_{t-1}; mode 1: lbbar_0 without its send term), rbar per in-edge,
+// and adds the block's logJ adjoint into epart[blockIdx].
 template <int S>
-__global__ void __launch_bounds__(kUThreads) k_u_gather_q(const UGraph g, const float *__restrict__ b,
-                                                          const float *__restrict__ send, float *__restrict__ q) {
-    __shared__ float sm[2 * kUMaxTables * S * S];
-    load_tables_smem<S>(g, sm);
-    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= g.V) return;
-    float qo[S];
-    ldv<S>(b + (size_t)v * S, qo);
-    for (uint32_t p = g.in_ptr[v]; p < g.in_ptr[v + 1]; ++p) {
-        float x[S], m[S];
-        ldv<S>(send + (size_t)g.in_src[p] * S, x);
-        msg_r<S>(edge_table<S>(sm, g.pos_tab[p]), x, m);
-#pragma unroll
-        for (int i = 0; i < S; ++i) qo[i] = FMUL(qo[i], m[i]);
-    }
-    stv<S>(q + (size_t)v * S, qo);
-}
-
-// one forward iteration: (b_{t-1}, Q_t) -> (b_t, Q_{t+1})
-template <int S>
-__global__ void __launch_bounds__(kUThreads) k_u_iter(const UGraph g, const float *__restrict__ b_in,
-                                                      const float *__restrict__ q_in, float *__restrict__ b_out,
-                                                      float *__restrict__ q_out) {
-    __shared__ float sm[2 * kUMaxTables * S * S];
-    load_tables_smem<S>(g, sm);
-    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= g.V) return;
-    const uint32_t r0 = g.in_ptr[v], r1 = g.in_ptr[v + 1];
-    float P[S], b[S];
-#pragma unroll
-    for (int i = 0; i < S; ++i) P[i] = 1.0f;
-    for (uint32_t p = r0; p < r1; ++p) {
-        float x[S], m[S];
-        ldv<S>(q_in + (size_t)g.in_src[p] * S, x);
-        msg_r<S>(edge_table<S>(sm, g.pos_tab[p]), x, m);
-#pragma unroll
-        for (int i = 0; i < S; ++i) P[i] = FMUL(P[i], m[i]);
-    }
-    ldv<S>(b_in + (size_t)v * S, b);
-    if (r1 > r0) {
-#pragma unroll
-        for (int i = 0; i < S; ++i) b[i] = FMUL(b[i], P[i]);
-    }
-    normalise<S, true>(b, S);
-    stv<S>(b_out + (size_t)v * S, b);
-    float qo[S];
-#pragma unroll
-    for (int i = 0; i < S; ++i) qo[i] = b[i];
-    for (uint32_t p = r0; p < r1; ++p) {
-        float x[S], m[S];
-        ldv<S>(q_in + (size_t)g.in_src[p] * S, x);
-        msg_r<S>(edge_table<S>(sm, g.pos_tab[p]), x, m);
-#pragma unroll
-        for (int i = 0; i < S; ++i) qo[i] = FMUL(qo[i], m[i]);
-    }
-    stv<S>(q_out + (size_t)v * S, qo);
-}
-
-// adjoint of one node step.  mode 0: iteration (b_t = normalise(b_{t-1} P),
-// Q_{t+1} = b_t P, messages from send = Q_t); mode 1: the initial step
-// (Q_1 = b_0 P, messages from send = b_0).  Writes bbar_out (bbar_{t-1}, or
-// the total bbar_0 without its send term), rbar per in-edge, and adds the
-// block's Ebar into epart[blockIdx].
-template <int S>
-__global__ void __launch_bounds__(kUThreads) k_u_bwd_node(const UGraph g, int mode, const float *__restrict__ b_prev,
-                                                          const float *__restrict__ send,
-                                                          const float *__restrict__ b_t,
-                                                          const float *__restrict__ bbar_t,
-                                                          const float *__restrict__ qbar_next,
-                                                          float *__restrict__ bbar_out, float *__restrict__ rbar,
+__global__ void __launch_bounds__(kUThreads) k_u_bwd_node(const UGraph g, int mode, const float *__restrict__ send,
+                                                          const float *__restrict__ lb_t,
+                                                          const float *__restrict__ lbbar_t,
+                                                          const float *__restrict__ lqbar_next,
+                                                          float *__restrict__ lbbar_out, float *__restrict__ rbar,
                                                           double *__restrict__ epart) {
     __shared__ float sm[2 * kUMaxTables * S * S];
     __shared__ float wred[kUThreads / 32][S * S];
@@ -187,94 +176,56 @@ __global__ void __launch_bounds__(kUThreads) k_u_bwd_node(const UGraph g, int mo
 #pragma unroll
     for (int k = 0; k < S * S; ++k) acc[k] = 0.0f;
     if (v < g.V) {
-        const uint32_t r0 = g.in_ptr[v], r1 = g.in_ptr[v + 1];
-        float P[S];
-#pragma unroll
-        for (int i = 0; i < S; ++i) P[i] = 1.0f;
-        for (uint32_t p = r0; p < r1; ++p) {
-            float x[S], m[S];
-            ldv<S>(send + (size_t)g.in_src[p] * S, x);
-            msg_r<S>(edge_table<S>(sm, g.pos_tab[p]), x, m);
-#pragma unroll
-            for (int i = 0; i < S; ++i) P[i] = FMUL(P[i], m[i]);
-        }
-        float bp[S], bt[S], bb[S], qb[S], Pbar[S];
-        ldv<S>(b_prev + (size_t)v * S, bp);
+        float gb[S], gq[S], Pbar[S];
 #pragma unroll
         for (int i = 0; i < S; ++i) {
-            bb[i] = 0.0f;
-            qb[i] = 0.0f;
+            gb[i] = 0.0f;
+            gq[i] = 0.0f;
         }
-        if (bbar_t) ldv<S>(bbar_t + (size_t)v * S, bb);
-        if (qbar_next) ldv<S>(qbar_next + (size_t)v * S, qb);
+        if (lbbar_t) ldv<S>(lbbar_t + (size_t)v * S, gb);
+        if (lqbar_next) ldv<S>(lqbar_next + (size_t)v * S, gq);
+        float out[S];
         if (mode == 0) {
-            ldv<S>(b_t + (size_t)v * S, bt);
-            float tot[S], dot = 0.0f, Z = 0.0f;
+            float lb[S], gs = 0.0f;
+            ldv<S>(lb_t + (size_t)v * S, lb);
 #pragma unroll
             for (int i = 0; i < S; ++i) {
-                tot[i] = bb[i] + qb[i] * P[i];
-                Pbar[i] = qb[i] * bt[i];
-                dot += tot[i] * bt[i];
-                Z += (r1 > r0) ? bp[i] * P[i] : bp[i];
+                gb[i] += gq[i];
+                gs += gb[i];
             }
-            if (Z <= 0.0f) Z = 1.0f;
-            float out[S];
 #pragma unroll
             for (int i = 0; i < S; ++i) {
-                const float ub = (tot[i] - dot) / Z;
-                out[i] = (r1 > r0) ? ub * P[i] : ub;
-                Pbar[i] += ub * bp[i];
+                out[i] = gb[i] - expf(lb[i]) * gs;
+                Pbar[i] = out[i] + gq[i];
             }
-            stv<S>(bbar_out + (size_t)v * S, out);
         } else {
-            float out[S];
 #pragma unroll
             for (int i = 0; i < S; ++i) {
-                out[i] = bb[i] + qb[i] * P[i];
-                Pbar[i] = qb[i] * bp[i];
+                out[i] = gb[i] + gq[i];
+                Pbar[i] = gq[i];
             }
-            stv<S>(bbar_out + (size_t)v * S, out);
         }
-        for (uint32_t p = r0; p < r1; ++p) {
+        stv<S>(lbbar_out + (size_t)v * S, out);
+        float ps = 0.0f;
+#pragma unroll
+        for (int i = 0; i < S; ++i) ps += Pbar[i];
+        for (uint32_t p = g.in_ptr[v]; p < g.in_ptr[v + 1]; ++p) {
             const uint8_t tab = g.pos_tab[p];
-            const float *J = edge_table<S>(sm, tab);
-            float x[S], m[S];
+            const float *L = edge_table<S>(sm, tab);
+            float x[S], r[S], lm[S], rb[S];
             ldv<S>(send + (size_t)g.in_src[p] * S, x);
-            const float R = msg_r<S>(J, x, m);
-            float mb[S], dot = 0.0f;
+            log_msg<S>(L, x, r, lm);
+#pragma unroll
+            for (int i = 0; i < S; ++i) rb[i] = Pbar[i] - expf(lm[i]) * ps;
+            stv<S>(rbar + (size_t)p * S, rb);
 #pragma unroll
             for (int i = 0; i < S; ++i) {
-                float loo;
-                if (m[i] != 0.0f) {
-                    loo = P[i] / m[i];
-                } else {  // product of the other messages, recomputed
-                    loo = 1.0f;
-                    for (uint32_t p2 = r0; p2 < r1; ++p2) {
-                        if (p2 == p) continue;
-                        float x2[S], m2[S];
-                        ldv<S>(send + (size_t)g.in_src[p2] * S, x2);
-                        msg_r<S>(edge_table<S>(sm, g.pos_tab[p2]), x2, m2);
-                        loo *= m2[i];
-                    }
+#pragma unroll
+                for (int j = 0; j < S; ++j) {
+                    const float w = expf(L[i * S + j] + x[j] - r[i]);
+                    if (tab & 0x80u) acc[j * S + i] += rb[i] * w;
+                    else acc[i * S + j] += rb[i] * w;
                 }
-                mb[i] = Pbar[i] * loo;
-                dot += mb[i] * m[i];
-            }
-            float rb[S];
-#pragma unroll
-            for (int i = 0; i < S; ++i) rb[i] = (mb[i] - dot) / R;
-            stv<S>(rbar + (size_t)p * S, rb);
-            // Ebar of the shared table: J_e = E (or E^T when transposed)
-            if (tab & 0x80u) {
-#pragma unroll
-                for (int i = 0; i < S; ++i)
-#pragma unroll
-                    for (int j = 0; j < S; ++j) acc[j * S + i] += rb[i] * x[j];
-            } else {
-#pragma unroll
-                for (int i = 0; i < S; ++i)
-#pragma unroll
-                    for (int j = 0; j < S; ++j) acc[i * S + j] += rb[i] * x[j];
             }
         }
     }
@@ -295,54 +246,58 @@ __global__ void __launch_bounds__(kUThreads) k_u_bwd_node(const UGraph g, int mo
     }
 }
 
-// Qbar(s) = sum over s's out-edges of J_e^T rbar_e (+ add(s))
+// xbar(s) = sum over s's out-edges of sum_i rbar_i w_ij (+ add(s)), with w
+// recomputed from s's own state x = send(s)
 template <int S>
-__global__ void __launch_bounds__(kUThreads) k_u_bwd_src(const UGraph g, const float *__restrict__ rbar,
+__global__ void __launch_bounds__(kUThreads) k_u_bwd_src(const UGraph g, const float *__restrict__ send,
+                                                         const float *__restrict__ rbar,
                                                          const float *__restrict__ add, float *__restrict__ out) {
     __shared__ float sm[2 * kUMaxTables * S * S];
     load_tables_smem<S>(g, sm);
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= g.V) return;
-    float acc[S];
+    float acc[S], x[S];
     if (add) ldv<S>(add + (size_t)s * S, acc);
     else {
 #pragma unroll
         for (int j = 0; j < S; ++j) acc[j] = 0.0f;
     }
+    ldv<S>(send + (size_t)s * S, x);
     for (uint32_t qq = g.out_ptr[s]; qq < g.out_ptr[s + 1]; ++qq) {
         const uint32_t p = g.out_pos[qq];
-        const float *J = edge_table<S>(sm, g.pos_tab[p]);
+        const float *L = edge_table<S>(sm, g.pos_tab[p]);
         float rb[S];
         ldv<S>(rbar + (size_t)p * S, rb);
 #pragma unroll
-        for (int j = 0; j < S; ++j) {
-            float t = 0.0f;
+        for (int i = 0; i < S; ++i) {
+            float t[S];
 #pragma unroll
-            for (int i = 0; i < S; ++i) t += J[i * S + j] * rb[i];
-            acc[j] += t;
+            for (int j = 0; j < S; ++j) t[j] = L[i * S + j] + x[j];
+            const float r = lse<S>(t);
+#pragma unroll
+            for (int j = 0; j < S; ++j) acc[j] += rb[i] * expf(t[j] - r);
         }
     }
     stv<S>(out + (size_t)s * S, acc);
 }
 
 template <int S>
-__global__ void k_u_softmax_bwd(uint32_t V, const float *__restrict__ b0, const float *__restrict__ bbar,
-                                float *__restrict__ theta_bar) {
+__global__ void k_u_logsoftmax_bwd(uint32_t V, const float *__restrict__ lb0, const float *__restrict__ gbar,
+                                   float *__restrict__ theta_bar) {
     const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= V) return;
-    float b[S], gb[S], dot = 0.0f;
-    ldv<S>(b0 + (size_t)v * S, b);
-    ldv<S>(bbar + (size_t)v * S, gb);
+    float lb[S], gb[S], s = 0.0f;
+    ldv<S>(lb0 + (size_t)v * S, lb);
+    ldv<S>(gbar + (size_t)v * S, gb);
 #pragma unroll
-    for (int i = 0; i < S; ++i) dot += gb[i] * b[i];
+    for (int i = 0; i < S; ++i) s += gb[i];
 #pragma unroll
-    for (int i = 0; i < S; ++i) gb[i] = b[i] * (gb[i] - dot);
+    for (int i = 0; i < S; ++i) gb[i] = gb[i] - expf(lb[i]) * s;
     stv<S>(theta_bar + (size_t)v * S, gb);
 }
 
-// log_pair_bar[k] = (sum of the block partials, fixed order) * exp(log_pair)
-__global__ void k_u_reduce_pair(const double *__restrict__ epart, uint32_t nblk, uint32_t n,
-                                const float *__restrict__ tables, float *__restrict__ out) {
+// log_pair_bar[k] = sum of the block partials (fixed order)
+__global__ void k_u_reduce_pair(const double *__restrict__ epart, uint32_t nblk, uint32_t n, float *__restrict__ out) {
     __shared__ double red[32];
     for (uint32_t k = 0; k < n; ++k) {
         double t = 0.0;
@@ -353,7 +308,7 @@ __global__ void k_u_reduce_pair(const double *__restrict__ epart, uint32_t nblk,
         if (threadIdx.x == 0) {
             double s = 0.0;
             for (uint32_t w = 0; w < (blockDim.x >> 5); ++w) s += red[w];
-            out[k] = (float)(s * (double)tables[k]);
+            out[k] = (float)s;
         }
         __syncthreads();
     }
@@ -389,8 +344,8 @@ static int u_forward(bp_unrolled *u, const float *theta, const float *logp, floa
     const size_t VS = (size_t)u->V * S;
     const unsigned gv = grid_for(u->V, kUThreads);
     cudaStream_t st = u->stream;
-    k_u_exp<S><<<grid_for(u->K * S * S, 64), 64, 0, st>>>(logp, u->K * S * S, u->tables);
-    k_u_softmax<S><<<gv, kUThreads, 0, st>>>(u->V, theta, u->ck_b);
+    BP_CUDA(cudaMemcpyAsync(u->tables, logp, sizeof(float) * u->K * S * S, cudaMemcpyDeviceToDevice, st));
+    k_u_logsoftmax<S><<<gv, kUThreads, 0, st>>>(u->V, theta, u->ck_b);
     k_u_gather_q<S><<<gv, kUThreads, 0, st>>>(g, u->ck_b, u->ck_b, u->ck_q);
     BP_CUDA(cudaGetLastError());
     // state t lives in checkpoint slot t/ck when t % ck == 0, else in pp[t&1]
@@ -428,16 +383,15 @@ static int u_backward(bp_unrolled *u, const float *grad_b, float *grad_theta, fl
         }
         for (uint32_t t = t_end; t > t0; --t) {
             const uint32_t j = t - t0 - 1;
-            const float *b_prev = (j == 0) ? ckb : u->seg_b + j * VS;
             const float *q_t = (j == 0) ? ckq : u->seg_q + j * VS;
             const float *b_t = (t == u->T) ? u->bT
                                : (t == t_end) ? u->ck_b + (size_t)(s + 1) * VS
                                               : u->seg_b + (j + 1) * VS;
             const float *qb = qc < 0 ? nullptr : u->qbar[qc];
-            k_u_bwd_node<S><<<gv, kUThreads, 0, st>>>(g, 0, b_prev, q_t, b_t, u->bbar[bc], qb, u->bbar[bc ^ 1],
-                                                      u->rbar, u->epart);
+            k_u_bwd_node<S><<<gv, kUThreads, 0, st>>>(g, 0, q_t, b_t, u->bbar[bc], qb, u->bbar[bc ^ 1], u->rbar,
+                                                      u->epart);
             const int qn = qc < 0 ? 0 : qc ^ 1;
-            k_u_bwd_src<S><<<gv, kUThreads, 0, st>>>(g, u->rbar, nullptr, u->qbar[qn]);
+            k_u_bwd_src<S><<<gv, kUThreads, 0, st>>>(g, q_t, u->rbar, nullptr, u->qbar[qn]);
             bc ^= 1;
             qc = qn;
         }
@@ -445,11 +399,11 @@ static int u_backward(bp_unrolled *u, const float *grad_b, float *grad_theta, fl
     BP_CUDA(cudaGetLastError());
     // initial step: Q_1 = b_0 * prod normalise(J . b_0(src))
     const float *b0 = u->ck_b;
-    k_u_bwd_node<S><<<gv, kUThreads, 0, st>>>(g, 1, b0, b0, nullptr, u->bbar[bc], qc < 0 ? nullptr : u->qbar[qc],
+    k_u_bwd_node<S><<<gv, kUThreads, 0, st>>>(g, 1, b0, nullptr, u->bbar[bc], qc < 0 ? nullptr : u->qbar[qc],
                                               u->bbar[bc ^ 1], u->rbar, u->epart);
-    k_u_bwd_src<S><<<gv, kUThreads, 0, st>>>(g, u->rbar, u->bbar[bc ^ 1], u->bbar[bc]);
-    k_u_softmax_bwd<S><<<gv, kUThreads, 0, st>>>(u->V, b0, u->bbar[bc], grad_theta);
-    k_u_reduce_pair<<<1, 256, 0, st>>>(u->epart, u->nblk, u->K * S * S, u->tables, grad_logp);
+    k_u_bwd_src<S><<<gv, kUThreads, 0, st>>>(g, b0, u->rbar, u->bbar[bc ^ 1], u->bbar[bc]);
+    k_u_logsoftmax_bwd<S><<<gv, kUThreads, 0, st>>>(u->V, b0, u->bbar[bc], grad_theta);
+    k_u_reduce_pair<<<1, 256, 0, st>>>(u->epart, u->nblk, u->K * S * S, grad_logp);
     BP_CUDA(cudaGetLastError());
     return BP_OK;
 }
@@ -575,6 +529,8 @@ void bp_unrolled_destroy(bp_unrolled *u) {
 
 int bp_unrolled_forward(bp_unrolled *u, const float *log_unary, const float *log_pair, float *beliefs) {
     if (!u || !log_unary || !log_pair || !beliefs) return set_error(BP_ERR_INVALID, "null argument");
+    if (((uintptr_t)log_unary | (uintptr_t)beliefs) & 15u)
+        return set_error(BP_ERR_INVALID, "log_unary and beliefs must be 16-byte aligned");
     BP_CUDA(cudaEventRecord(u->ev0, u->stream));
     int st;
     auto run = [&]() -> int { BP_DISPATCH_S(u->S, u_forward, u, log_unary, log_pair, beliefs); };
@@ -586,6 +542,8 @@ int bp_unrolled_forward(bp_unrolled *u, const float *log_unary, const float *log
 
 int bp_unrolled_backward(bp_unrolled *u, const float *grad_beliefs, float *grad_log_unary, float *grad_log_pair) {
     if (!u || !grad_beliefs || !grad_log_unary || !grad_log_pair) return set_error(BP_ERR_INVALID, "null argument");
+    if (((uintptr_t)grad_beliefs | (uintptr_t)grad_log_unary) & 15u)
+        return set_error(BP_ERR_INVALID, "grad_beliefs and grad_log_unary must be 16-byte aligned");
     if (!u->forward_done) return set_error(BP_ERR_STATE, "backward before forward");
     auto run = [&]() -> int { BP_DISPATCH_S(u->S, u_backward, u, grad_beliefs, grad_log_unary, grad_log_pair); };
     return run();

@@ -36,7 +36,7 @@ class BPGraph:
     """A graph resident in GPU memory (bp_graph)."""
 
     def __init__(self, num_nodes, src, dst, joint, num_states=None, uniform_states=0,
-                 joint_row_stride=None, joint_edge_stride=None, dest_csr=None, stream=None):
+                 joint_row_stride=None, joint_edge_stride=None, dest_csr=None, stream=None, reorder=False):
         self.lib = N.load()
         V, E = int(num_nodes), int(len(src))
         if not _is_torch(src):
@@ -56,6 +56,7 @@ class BPGraph:
         if dest_csr is not None:
             d.dest_node_list, d.dest_edge_list = N.ptr(dest_csr[0]), N.ptr(dest_csr[1])
         d.memory = _memory_of(src, dst, joint, num_states)
+        d.flags = N.BP_GRAPH_REORDER_BY_OUT_DEGREE if reorder else 0
         self._keep = (src, dst, joint, num_states)
         h = C.c_void_p()
         N.check(self.lib.bp_graph_create(C.byref(h), C.byref(d), stream))
@@ -66,9 +67,10 @@ class BPGraph:
         self.V, self.E, self.ms, self.uniform = V_.value, E_.value, ms.value, uni.value
 
     @classmethod
-    def from_network(cls, net, stream=None, with_beliefs=True):
+    def from_network(cls, net, stream=None, with_beliefs=True, reorder=False):
         uni = net.uniform_states
-        g = cls(net.V, net.src, net.dst, net.joint, None if uni else net.num_states, uni, stream=stream)
+        g = cls(net.V, net.src, net.dst, net.joint, None if uni else net.num_states, uni, stream=stream,
+                reorder=reorder)
         if with_beliefs:
             g.set_beliefs(net.beliefs)
         return g
@@ -228,8 +230,8 @@ class BPBatch:
         out = np.zeros(int(self.belief_off[-1]), np.float32)
         for k, net in enumerate(self.nets):
             S = net.uniform_states
-            a, b = int(self.belief_off[k]), int(self.belief_off[k + 1])
-            out[a:b] = net.beliefs[:, :S].ravel()
+            a = int(self.belief_off[k])
+            out[a:a + net.V * S] = net.beliefs[:, :S].ravel()
         return out
 
     def set_beliefs(self, flat=None):
@@ -244,16 +246,20 @@ class BPBatch:
         N.check(self.lib.bp_batch_get_beliefs(self.h, flat.ctypes.data, N.BP_MEM_HOST))
         if k is None:
             return flat
-        S = self.nets[k].uniform_states
-        return flat[int(self.belief_off[k]):int(self.belief_off[k + 1])].reshape(-1, S)
+        net = self.nets[k]
+        S = net.uniform_states
+        a = int(self.belief_off[k])
+        return flat[a:a + net.V * S].reshape(net.V, S)
 
     def messages(self, k=None):
         flat = np.zeros(max(int(self.msg_off[-1]), 1), np.float32)
         N.check(self.lib.bp_batch_get_messages(self.h, flat.ctypes.data, N.BP_MEM_HOST))
         if k is None:
             return flat
-        S = self.nets[k].uniform_states
-        return flat[int(self.msg_off[k]):int(self.msg_off[k + 1])].reshape(-1, S)
+        net = self.nets[k]
+        S = net.uniform_states
+        a = int(self.msg_off[k])
+        return flat[a:a + net.E * S].reshape(net.E, S)
 
     def options(self, tol=1e-4, max_iterations=200, delta="f64", block_threads=0, init=True):
         o = N.BatchOptions()

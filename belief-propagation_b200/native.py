@@ -20,6 +20,7 @@ BP_MEM_HOST, BP_MEM_DEVICE = 0, 1
 BP_SCHEDULE_NODE, BP_SCHEDULE_EDGE = 0, 1
 BP_DELTA_AUTO, BP_DELTA_SERIAL_F32, BP_DELTA_F64 = 0, 1, 2
 BP_SYNC_EAGER, BP_SYNC_LAZY = 0, 1
+BP_GRAPH_REORDER_BY_OUT_DEGREE = 1
 STATUS = {0: "BP_OK", 1: "BP_ERR_INVALID", 2: "BP_ERR_SHAPE", 3: "BP_ERR_CUDA", 4: "BP_ERR_NOMEM",
           5: "BP_ERR_NO_DEVICE", 6: "BP_ERR_GRAPH", 7: "BP_ERR_STATE", 8: "BP_ERR_TIMEOUT"}
 
@@ -36,7 +37,7 @@ class GraphDesc(C.Structure):
                 ("edge_joint", C.c_void_p), ("joint_row_stride", C.c_uint32),
                 ("joint_edge_stride", C.c_uint64), ("dest_node_list", C.c_void_p),
                 ("dest_edge_list", C.c_void_p), ("src_node_list", C.c_void_p),
-                ("src_edge_list", C.c_void_p), ("memory", C.c_int32)]
+                ("src_edge_list", C.c_void_p), ("memory", C.c_int32), ("flags", C.c_int32)]
 
 
 class LoopyOptions(C.Structure):

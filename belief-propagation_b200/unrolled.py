@@ -2,14 +2,15 @@
 behind torch.autograd.Function.
 
     bp = UnrolledBP(num_nodes, src, dst, edge_table, states=4, iterations=30)
-    beliefs = bp(log_unary, log_pair)       # [V, S], differentiable
-    loss = torch.nn.functional.nll_loss(beliefs.log(), labels)
+    log_beliefs = bp(log_unary, log_pair)   # [V, S], differentiable
+    loss = torch.nn.functional.nll_loss(log_beliefs, labels)   # cross-entropy
     loss.backward()                          # log_unary.grad, log_pair.grad
 
 edge_table[e] names the shared table edge e uses (bit 0x80: transposed).
 The forward is the reference's update (beliefs compound across iterations,
-graph.c:1010, :1157); the backward is a hand-written adjoint kernel with
-state checkpoints every `checkpoint_every` iterations recomputed per segment.
+graph.c:1010, :1157), run in the log domain; the backward is a hand-written
+adjoint kernel with state checkpoints every `checkpoint_every` iterations
+recomputed per segment.
 """
 from __future__ import annotations
 
@@ -35,6 +36,8 @@ class _UnrolledFn(torch.autograd.Function):
     def backward(ctx, grad_b):
         eng = ctx.engine
         grad_b = grad_b.contiguous().float()
+        if grad_b.data_ptr() % 16:
+            grad_b = grad_b.clone()
         gu = torch.empty(ctx.shapes[0], device=grad_b.device, dtype=torch.float32)
         gp = torch.empty(ctx.shapes[1], device=grad_b.device, dtype=torch.float32)
         eng._run(lambda h: eng.lib.bp_unrolled_backward(h, grad_b.data_ptr(), gu.data_ptr(), gp.data_ptr()))
@@ -64,7 +67,10 @@ class UnrolledBP:
     def __call__(self, log_unary, log_pair):
         if log_unary.dtype != torch.float32 or log_pair.dtype != torch.float32:
             raise TypeError("log-potentials must be float32 CUDA tensors")
-        return _UnrolledFn.apply(log_unary.contiguous(), log_pair.contiguous(), self)
+        def fresh(t):  # contiguous and 16-byte aligned (views with an offset are copied)
+            t = t.contiguous()
+            return t if t.data_ptr() % 16 == 0 else t.clone()
+        return _UnrolledFn.apply(fresh(log_unary), fresh(log_pair), self)
 
     def close(self):
         if getattr(self, "h", None):
@@ -90,29 +96,29 @@ def grid_tables(side):
 
 def torch_unrolled(log_unary, log_pair, src, dst, edge_table, iterations):
     """Pure-torch unrolled reference of the same update (autograd through
-    every step), any dtype; products over in-edges via index_add of logs."""
+    every step), any dtype, log domain; returns log-beliefs."""
     V, S = log_unary.shape
-    src = torch.as_tensor(np.asarray(src, np.int64), device=log_unary.device)
-    dst = torch.as_tensor(np.asarray(dst, np.int64), device=log_unary.device)
+    dev = log_unary.device
+    src = torch.as_tensor(np.asarray(src, np.int64), device=dev)
+    dst = torch.as_tensor(np.asarray(dst, np.int64), device=dev)
     tab = np.asarray(edge_table)
-    tid = torch.as_tensor((tab & 0x7F).astype(np.int64), device=log_unary.device)
-    tr = torch.as_tensor((tab & 0x80) != 0, device=log_unary.device)
-    E = torch.exp(log_pair)
-    J = E[tid]
-    J = torch.where(tr[:, None, None], J.transpose(1, 2), J)
+    tid = torch.as_tensor((tab & 0x7F).astype(np.int64), device=dev)
+    tr = torch.as_tensor((tab & 0x80) != 0, device=dev)
+    L = log_pair[tid]
+    L = torch.where(tr[:, None, None], L.transpose(1, 2), L)
 
-    def send(x):
-        r = torch.einsum("eij,ej->ei", J, x[src])
-        return r / r.sum(1, keepdim=True)
+    def lmsg(x):
+        r = torch.logsumexp(L + x[src][:, None, :], dim=2)
+        return r - torch.logsumexp(r, dim=1, keepdim=True)
 
-    def prod_in(m):
-        return torch.exp(torch.zeros(V, S, dtype=m.dtype, device=m.device).index_add(0, dst, torch.log(m)))
+    def sum_in(lm):
+        return torch.zeros(V, S, dtype=lm.dtype, device=dev).index_add(0, dst, lm)
 
-    b = torch.softmax(log_unary, dim=1)
-    Q = b * prod_in(send(b))
+    lb = torch.log_softmax(log_unary, dim=1)
+    lq = lb + sum_in(lmsg(lb))
     for _ in range(iterations):
-        P = prod_in(send(Q))
-        u = b * P
-        b = u / u.sum(1, keepdim=True)
-        Q = b * P
-    return b
+        lp = sum_in(lmsg(lq))
+        a = lb + lp
+        lb = a - torch.logsumexp(a, dim=1, keepdim=True)
+        lq = lb + lp
+    return lb

@@ -52,8 +52,13 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", choices=["power_law", "batched"], default="power_law",
-                    help="power_law: the headline loopy workload; batched: 4096 independent networks")
+    ap.add_argument("--workload", choices=["power_law", "batched", "tree", "unrolled", "unrolled_batch"],
+                    default="power_law",
+                    help="power_law: the headline loopy workload; batched: 4096 independent networks; "
+                         "tree: tree BP on a 2M-node random recursive tree")
+    ap.add_argument("--tree-nodes", type=int, default=2_000_000)
+    ap.add_argument("--reorder", type=int, default=1,
+                    help="1: renumber nodes by out-degree inside the engine (results unchanged)")
     ap.add_argument("--networks", type=int, default=4096)
     ap.add_argument("--solo-sample", type=int, default=256,
                     help="batched: networks solved one launch sequence each, for the comparison")
@@ -309,6 +314,204 @@ def run_batched(a, rank, world):
     return 0
 
 
+def run_tree(a, rank, world):
+    """Tree BP (c_benchmark/main.c:224-236) on a random recursive tree: parent
+    of node i uniform in [0, i), both directions, states per node uniform in
+    {2,3,4,8}, row-normalised U(0,1) tables, 5% evidence, seed 1.  One step =
+    start pass, forward levels, reset, backward levels, marginalize, on the
+    device; the O(V+E) level build is timed separately (the reference's is
+    O(V^2)).  Checked bit for bit against the oracle's restatement at full
+    size, which is also the CPU baseline (port, 1 core)."""
+    import torch
+    import belief_network_wrapper as W
+    from belief_propagation_b200.engine import BPGraph
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    net = W.bp.synth.random_tree(a.tree_nodes, (2, 3, 4, 8), 0.05, seed=1)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    g = BPGraph.from_network(net, stream=stream.cuda_stream)
+    t0 = time.perf_counter()
+    lv, nl = g.build_levels()
+    levels_s = time.perf_counter() - t0
+    prior = torch.from_numpy(net.beliefs).cuda()
+
+    def step():
+        g.set_beliefs(prior)
+        return g.tree()
+
+    for _ in range(a.warmup):
+        r = step()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0.record(stream)
+    for _ in range(a.steps):
+        r = step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / a.steps
+    b_gpu = g.beliefs()
+    g.close()
+    cpu = None
+    if rank == 0:
+        R = O.Restatement()
+        og = O.OracleGraph(net)
+        t0 = time.perf_counter()
+        ora = R.tree(og)
+        cpu_s = time.perf_counter() - t0
+        same = bool(np.array_equal(b_gpu, ora["beliefs"][:, : net.s_max]))
+        cpu = {"value": 1e3 * cpu_s, "unit": "ms per tree (levels + passes)", "cores": 1, "kind": "port",
+               "sample": f"the full tree, oracle restatement (O(V+E) levels), bit-identical to the GPU: {same}"}
+    if rank != 0:
+        return 0
+    line = {"metric": "tree BP ms per tree", "value": ms, "unit": "ms", "n_gpus": 1, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "replicas",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"tree BP, random recursive tree, {net.V:,} nodes, {net.E:,} edges, "
+                                   "states {2,3,4,8}, 5% evidence, seed 1",
+                       "levels": nl, "waves": r["num_waves"], "level_build_s": levels_s},
+            "nodes_per_s": net.V / (ms / 1e3), "cpu_baseline": cpu, "gpu_launches": (r["num_waves"] + 5) * a.steps,
+            "clocks": clk}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def _time_cuda(fn, stream, reps):
+    import torch
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def run_unrolled(a, rank, world, batch):
+    """Differentiable unrolled loopy BP.
+    unrolled:       512x512 4-neighbour grid, 4 states, unary N(0,1), one shared
+                    4x4 pairwise log-potential N(0,0.5), T=30, checkpoints every 5,
+                    cross-entropy against uniform random labels, seed 3.
+    unrolled_batch: 256 grids of side U[32,256], 8 states, same potentials,
+                    T=20, one forward and one backward over the whole batch (its
+                    disjoint union), then 50 SGD steps (lr 0.1) on the shared table,
+                    seed 4.
+    Reports forward ms, forward+backward ms and their ratio, next to the plain
+    engine's forward (bp_loopy, T fixed iterations) on the same graph."""
+    import torch
+    import belief_network_wrapper as W
+    from belief_propagation_b200.engine import BPGraph
+    from belief_propagation_b200.unrolled import UnrolledBP
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    synth = W.bp.synth
+    if batch:
+        rng = np.random.default_rng(4)
+        sides = rng.integers(32, 257, size=256)
+        S, T = 8, 20
+    else:
+        rng = np.random.default_rng(3)
+        sides = np.array([512])
+        S, T = 4, 30
+    srcs, dsts, tabs, off = [], [], [], 0
+    for side in sides:
+        s_, d_, fwd = synth.grid_edges(int(side))
+        srcs.append(s_.astype(np.int64) + off)
+        dsts.append(d_.astype(np.int64) + off)
+        tabs.append(np.where(fwd, 0, 0x80).astype(np.uint8))
+        off += int(side) * int(side)
+    V = off
+    src = np.concatenate(srcs).astype(np.uint32)
+    dst = np.concatenate(dsts).astype(np.uint32)
+    tab = np.concatenate(tabs)
+    E = len(src)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    theta = torch.tensor(rng.normal(0, 1, (V, S)), dtype=torch.float32, device="cuda", requires_grad=True)
+    Wp = torch.tensor(rng.normal(0, 0.5, (1, S, S)), dtype=torch.float32, device="cuda", requires_grad=True)
+    labels = torch.tensor(rng.integers(0, S, V), device="cuda")
+    eng = UnrolledBP(V, src, dst, tab, S, T, checkpoint_every=5)
+
+    def fwd():
+        with torch.no_grad():
+            return eng(theta, Wp)
+
+    def fwd_bwd():
+        theta.grad = None
+        Wp.grad = None
+        lb = eng(theta, Wp)
+        loss = torch.nn.functional.nll_loss(lb, labels)
+        loss.backward()
+        return loss
+
+    for _ in range(a.warmup):
+        fwd_bwd()
+    clocks = ClockSampler(local)
+    clocks.start()
+    reps = max(a.steps, 3)
+    f_ms = _time_cuda(fwd, stream, reps)
+    fb_ms = _time_cuda(fwd_bwd, stream, reps)
+    clk = clocks.stop()
+    # the plain engine's forward on the same graph and tables, T iterations
+    E_tab = np.exp(Wp.detach().cpu().numpy()[0])
+    joint = np.where((tab & 0x80)[:, None, None] != 0, E_tab.T[None], E_tab[None]).astype(np.float32)
+    prior = torch.softmax(theta.detach(), 1)
+    g = BPGraph(V, src, dst, joint, uniform_states=S, stream=stream.cuda_stream)
+
+    def plain():
+        g.set_beliefs(prior)
+        g.latest_slot = 1
+        g.init_messages()
+        g.loopy(0.0, T, delta="f64")
+
+    plain()
+    p_ms = _time_cuda(plain, stream, reps)
+    b_plain = g.beliefs()
+    g.close()
+    b_unrolled = np.exp(fwd().cpu().numpy())
+    max_diff = float(np.abs(b_plain - b_unrolled).max())
+    extra = {}
+    if batch:
+        losses = []
+        opt = torch.optim.SGD([Wp], lr=0.1)
+        t0 = time.perf_counter()
+        for _ in range(50):
+            opt.zero_grad()
+            lb = eng(theta.detach(), Wp)
+            loss = torch.nn.functional.nll_loss(lb, labels)
+            loss.backward()
+            opt.step()
+            losses.append(float(loss.item()))
+        torch.cuda.synchronize()
+        extra = {"sgd_steps": 50, "lr": 0.1, "loss_first": losses[0], "loss_last": losses[-1],
+                 "sgd_ms_per_step": 1e3 * (time.perf_counter() - t0) / 50,
+                 "networks_per_s_fwd_bwd": len(sides) / (fb_ms / 1e3)}
+    eng.close()
+    if rank != 0:
+        return 0
+    line = {"metric": "BP fwd+bwd ms", "value": fb_ms, "unit": "ms", "n_gpus": 1, "steps": reps,
+            "warmup": a.warmup, "ms_per_step": fb_ms, "higher_is_better": False, "scaling": "replicas",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": (f"{len(sides)} grid MRFs, side U[32,256], " if batch else "512x512 grid MRF, ")
+                       + f"{S} states, T={T}, checkpoints every 5, shared pairwise table",
+                       "nodes": V, "edges": E},
+            "forward_ms": f_ms, "fwd_bwd_over_fwd": fb_ms / f_ms, "plain_forward_ms": p_ms,
+            "fwd_bwd_over_plain_forward": fb_ms / p_ms, "max_abs_belief_diff_vs_plain": max_diff,
+            "clocks": clk, **extra}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     a = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -318,6 +521,10 @@ def main():
         return run_reference_arm(a, rank, world)
     if a.workload == "batched":
         return run_batched(a, rank, world)
+    if a.workload == "tree":
+        return run_tree(a, rank, world)
+    if a.workload in ("unrolled", "unrolled_batch"):
+        return run_unrolled(a, rank, world, a.workload == "unrolled_batch")
 
     import torch
     import belief_network_wrapper as W
@@ -346,7 +553,7 @@ def main():
     handle = stream.cuda_stream
 
     # ---- resident graph
-    g = BPGraph(V, net.src, net.dst, net.joint, uniform_states=2, stream=handle)
+    g = BPGraph(V, net.src, net.dst, net.joint, uniform_states=2, stream=handle, reorder=bool(a.reorder))
     prior = torch.from_numpy(net.beliefs).cuda()
 
     def step():
@@ -400,7 +607,7 @@ def main():
         out_h = torch.empty((V, S), dtype=torch.float32).pin_memory()
 
         def e2e_step():
-            g2 = BPGraph(V, src_h, dst_h, joint_h, uniform_states=2, stream=handle)
+            g2 = BPGraph(V, src_h, dst_h, joint_h, uniform_states=2, stream=handle, reorder=bool(a.reorder))
             g2.set_beliefs(bel_h)
             g2.init_messages()
             g2.loopy(0.0, a.iterations, delta="f64")
@@ -447,6 +654,7 @@ def main():
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": workload_name(a), "nodes": V, "edges": E, "states": S,
                        "iterations": a.iterations, "l2": "inputs larger than L2 (working set ~3.4 GB per replica)",
+                       "node_order": "renumbered by out-degree" if a.reorder else "caller ids",
                        "parallelism": f"replicas x{world}", "generator_s": round(gen_s, 1)},
             "hbm_gbs_algorithmic": achieved, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches_per_step * a.steps, "clocks": clk}

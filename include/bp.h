@@ -85,7 +85,17 @@ typedef struct {
     const uint32_t *dest_node_list, *dest_edge_list;
     const uint32_t *src_node_list, *src_edge_list;
     int32_t memory;                   /* bp_memory of every pointer above */
+    int32_t flags;                    /* bp_graph_flags */
 } bp_graph_desc;
+
+typedef enum {
+    /* renumber nodes internally by decreasing out-degree (ties by id) so the
+     * send buffers of frequent sources share cache sectors; results are
+     * unchanged (each node's in-edges keep their order), node ids at the API
+     * stay the caller's.  Node-schedule loopy BP only: tree BP and the edge
+     * schedule return BP_ERR_STATE on such a graph. */
+    BP_GRAPH_REORDER_BY_OUT_DEGREE = 1
+} bp_graph_flags;
 
 typedef struct {
     float tolerance;          /* the reference's `convergence` */
@@ -215,7 +225,8 @@ int bp_get_visited(bp_graph *g, char *visited);       /* host [V] */
  *
  * Layout of the batch-wide arrays (bp_batch_layout): network n's beliefs are
  * [V_n][S_n] floats at belief_offsets[n], its messages [E_n][S_n] (edge-id
- * order) at message_offsets[n]; offsets[N] is the total. */
+ * order) at message_offsets[n]; offsets[N] is the total.  Offsets are
+ * multiples of 4 floats; the gaps between networks are padding. */
 typedef struct bp_batch bp_batch;
 
 typedef struct {
@@ -258,13 +269,16 @@ int bp_batch_network_results(bp_batch *b, uint32_t *iterations, uint32_t *execut
 /* T synchronous iterations of the reference's update on a pairwise model:
  * priors softmax(log_unary[v]), joint tables exp(log_pair[k]) shared by the
  * edges that name table k (edge_table[e] & 0x7f; bit 0x80 = the edge uses
- * the transposed table).  bp_unrolled_forward writes the beliefs after T
- * iterations; bp_unrolled_backward maps d loss / d beliefs to gradients with
- * respect to log_unary and log_pair with a hand-written adjoint.  The forward
- * keeps the iteration state every checkpoint_every iterations; the backward
- * recomputes each segment from its checkpoint.  All tensor arguments of
- * forward/backward are device memory; the graph arrays of create are host
- * memory.  At most 16 tables. */
+ * the transposed table).  The iteration runs in the log domain (the
+ * reference's update multiplies each belief into itself every iteration, so
+ * beliefs head to 0 faster than fp32 can follow in linear form).
+ * bp_unrolled_forward writes the LOG-beliefs after T iterations;
+ * bp_unrolled_backward maps d loss / d log-beliefs to gradients with respect
+ * to log_unary and log_pair with a hand-written adjoint.  The forward keeps
+ * the iteration state every checkpoint_every iterations; the backward
+ * recomputes each segment from its checkpoint.  Tensor arguments of
+ * forward/backward are device memory, 16-byte aligned; the graph arrays of
+ * create are host memory.  At most 16 tables. */
 typedef struct bp_unrolled bp_unrolled;
 int bp_unrolled_create(bp_unrolled **out, uint32_t num_nodes, uint32_t num_edges, uint32_t num_states,
                        uint32_t num_tables, const uint32_t *edge_src, const uint32_t *edge_dst,
@@ -272,8 +286,8 @@ int bp_unrolled_create(bp_unrolled **out, uint32_t num_nodes, uint32_t num_edges
                        void *stream);
 void bp_unrolled_destroy(bp_unrolled *u);
 int bp_unrolled_set_stream(bp_unrolled *u, void *stream);
-int bp_unrolled_forward(bp_unrolled *u, const float *log_unary, const float *log_pair, float *beliefs);
-int bp_unrolled_backward(bp_unrolled *u, const float *grad_beliefs, float *grad_log_unary,
+int bp_unrolled_forward(bp_unrolled *u, const float *log_unary, const float *log_pair, float *log_beliefs);
+int bp_unrolled_backward(bp_unrolled *u, const float *grad_log_beliefs, float *grad_log_unary,
                          float *grad_log_pair);
 
 /* ---- drop-in support (struct graph from graph.h) ---------------------- */

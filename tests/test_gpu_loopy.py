@@ -14,9 +14,9 @@ pytestmark = pytest.mark.gpu
 
 
 def gpu_loopy(bp, net, tol, max_it, check_every=1, schedule="node", delta="serial", init=True,
-              msgs=None, graph_chunk=0):
+              msgs=None, graph_chunk=0, reorder=False):
     from belief_propagation_b200.engine import BPGraph
-    g = BPGraph.from_network(net)
+    g = BPGraph.from_network(net, reorder=reorder)
     try:
         if msgs is not None:
             g.set_messages(1, msgs[0][:, : net.s_max])
@@ -77,13 +77,47 @@ CASES = [
 ]
 
 
+@pytest.mark.parametrize("reorder", [False, True], ids=["ids", "renumbered"])
 @pytest.mark.parametrize("case", CASES, ids=lambda c: f"S{c['S']}")
 @pytest.mark.parametrize("tol,max_it", [(1e-3, 40), (0.0, 15)])
-def test_loopy_node_parity(bp, synth, restatement, O, case, tol, max_it):
+def test_loopy_node_parity(bp, synth, restatement, O, case, tol, max_it, reorder):
     net = synth.random_loopy(case["V"], case["E"], case["S"], 0.1, seed=case["seed"])
     ora = restatement.loopy(O.OracleGraph(net), tol, max_it)
-    gpu = gpu_loopy(bp, net, tol, max_it)
+    gpu = gpu_loopy(bp, net, tol, max_it, reorder=reorder)
     assert_same(gpu, ora, case["S"])
+
+
+def test_loopy_renumbered_power_law_and_mixed(bp, synth, restatement, O):
+    """Renumbering by out-degree changes nothing in the results: a power-law
+    graph and a mixed-state graph, bit for bit."""
+    net = synth.power_law_loopy(1 << 15, 1 << 17, 2, 0.1, seed=3)
+    ora = restatement.loopy(O.OracleGraph(net), 1e-3, 30)
+    assert_same(gpu_loopy(bp, net, 1e-3, 30, reorder=True), ora, 2)
+    base = synth.random_loopy(400, 1600, 2, 0.1, seed=8)
+    rng = np.random.default_rng(4)
+    ns = rng.choice(np.array([2, 3, 5], np.uint32), size=base.V)
+    S = 5
+    b = rng.random((base.V, S), dtype=np.float32) * (np.arange(S)[None] < ns[:, None])
+    j = rng.random((base.E, S, S), dtype=np.float32)
+    j *= (np.arange(S)[None, :, None] < ns[base.src][:, None, None])
+    j *= (np.arange(S)[None, None, :] < ns[base.dst][:, None, None])
+    mixed = synth.Network(ns, b.astype(np.float32), base.observed, base.src, base.dst, j.astype(np.float32))
+    ora = restatement.loopy(O.OracleGraph(mixed), 1e-3, 20)
+    assert_same(gpu_loopy(bp, mixed, 1e-3, 20, reorder=True), ora, S)
+
+
+def test_renumbered_graph_refuses_tree_and_edge_schedule(bp, synth):
+    from belief_propagation_b200.engine import BPGraph
+    from belief_propagation_b200.native import BPError
+    net = synth.random_loopy(100, 300, 2, 0.1, seed=1)
+    g = BPGraph.from_network(net, reorder=True)
+    try:
+        with pytest.raises(BPError):
+            g.build_levels()
+        with pytest.raises(BPError):
+            g.loopy(1e-3, 5, schedule="edge")
+    finally:
+        g.close()
 
 
 @pytest.mark.parametrize("check,sched", [(10, "node"), (1, "edge"), (10, "edge")])
