@@ -50,10 +50,10 @@ struct UGraph {
 
 template <int S>
 __device__ __forceinline__ void load_tables_smem(const UGraph &g, float *sm) {
-    // sm[2k] = table k, sm[2k+1] = its transpose
+    // sm[2k] = exp(table k), sm[2k+1] = its transpose
     for (uint32_t i = threadIdx.x; i < g.K * S * S; i += blockDim.x) {
         const uint32_t k = i / (S * S), r = (i % (S * S)) / S, c = i % S;
-        const float v = g.tables[i];
+        const float v = expf(g.tables[i]);
         sm[(2 * k) * S * S + r * S + c] = v;
         sm[(2 * k + 1) * S * S + c * S + r] = v;
     }
@@ -77,16 +77,37 @@ __device__ __forceinline__ float lse(const float *a) {
     return mx + logf(s);
 }
 
-// log-message of one edge: r_i = LSE_j(L_ij + x_j), lm_i = r_i - LSE(r)
+// shifted exponentials of a log-state: e_j = exp(x_j - mx)
 template <int S>
-__device__ __forceinline__ void log_msg(const float *L, const float *x, float *r, float *lm) {
+__device__ __forceinline__ float shifted_exp(const float *x, float *e) {
+    float mx = x[0];
+#pragma unroll
+    for (int j = 1; j < S; ++j) mx = fmaxf(mx, x[j]);
+#pragma unroll
+    for (int j = 0; j < S; ++j) e[j] = expf(x[j] - mx);
+    return mx;
+}
+
+// row sums s_i = sum_j J_ij e_j (J linear, > 0), so r_i = mx + log s_i
+template <int S>
+__device__ __forceinline__ void row_sums(const float *J, const float *e, float *sr) {
 #pragma unroll
     for (int i = 0; i < S; ++i) {
-        float t[S];
+        float t = 0.0f;
 #pragma unroll
-        for (int j = 0; j < S; ++j) t[j] = L[i * S + j] + x[j];
-        r[i] = lse<S>(t);
+        for (int j = 0; j < S; ++j) t += J[i * S + j] * e[j];
+        sr[i] = fmaxf(t, 1e-37f);
     }
+}
+
+// log-message: r_i = LSE_j(logJ_ij + x_j) = mx + log s_i, lm = r - LSE(r)
+template <int S>
+__device__ __forceinline__ void log_msg(const float *J, const float *x, float *e, float *sr, float *lm) {
+    const float mx = shifted_exp<S>(x, e);
+    row_sums<S>(J, e, sr);
+    float r[S];
+#pragma unroll
+    for (int i = 0; i < S; ++i) r[i] = mx + logf(sr[i]);
     const float z = lse<S>(r);
 #pragma unroll
     for (int i = 0; i < S; ++i) lm[i] = r[i] - z;
@@ -115,9 +136,9 @@ __global__ void __launch_bounds__(kUThreads) k_u_gather_q(const UGraph g, const 
     float qo[S];
     ldv<S>(lb + (size_t)v * S, qo);
     for (uint32_t p = g.in_ptr[v]; p < g.in_ptr[v + 1]; ++p) {
-        float x[S], r[S], m[S];
+        float x[S], e[S], sr[S], m[S];
         ldv<S>(send + (size_t)g.in_src[p] * S, x);
-        log_msg<S>(edge_table<S>(sm, g.pos_tab[p]), x, r, m);
+        log_msg<S>(edge_table<S>(sm, g.pos_tab[p]), x, e, sr, m);
 #pragma unroll
         for (int i = 0; i < S; ++i) qo[i] += m[i];
     }
@@ -137,9 +158,9 @@ __global__ void __launch_bounds__(kUThreads) k_u_iter(const UGraph g, const floa
 #pragma unroll
     for (int i = 0; i < S; ++i) P[i] = 0.0f;
     for (uint32_t p = g.in_ptr[v]; p < g.in_ptr[v + 1]; ++p) {
-        float x[S], r[S], m[S];
+        float x[S], e[S], sr[S], m[S];
         ldv<S>(lq_in + (size_t)g.in_src[p] * S, x);
-        log_msg<S>(edge_table<S>(sm, g.pos_tab[p]), x, r, m);
+        log_msg<S>(edge_table<S>(sm, g.pos_tab[p]), x, e, sr, m);
 #pragma unroll
         for (int i = 0; i < S; ++i) P[i] += m[i];
     }
@@ -157,17 +178,41 @@ __global__ void __launch_bounds__(kUThreads) k_u_iter(const UGraph g, const floa
     stv<S>(lq_out + (size_t)v * S, qo);
 }
 
-// adjoint of one node step.  mode 0: iteration; mode 1: the initial step
-// (lQ_1 = lb_0 + lP, messages from send = lb_0).  Writes lbbar_out
-// (lbbar_{t-1}; mode 1: lbbar_0 without its send term), rbar per in-edge,
-// and adds the block's logJ adjoint into epart[blockIdx].
+// x adjoint of node s through its out-edges: sum_e sum_i rbar_e,i w_e,ij,
+// w recomputed from s's own log-state x
 template <int S>
-__global__ void __launch_bounds__(kUThreads) k_u_bwd_node(const UGraph g, int mode, const float *__restrict__ send,
-                                                          const float *__restrict__ lb_t,
-                                                          const float *__restrict__ lbbar_t,
-                                                          const float *__restrict__ lqbar_next,
-                                                          float *__restrict__ lbbar_out, float *__restrict__ rbar,
-                                                          double *__restrict__ epart) {
+__device__ __forceinline__ void gather_xbar(const UGraph &g, const float *sm, uint32_t s, const float *x,
+                                            const float *__restrict__ rbar, float *acc) {
+    float e[S];
+    shifted_exp<S>(x, e);
+    for (uint32_t qq = g.out_ptr[s]; qq < g.out_ptr[s + 1]; ++qq) {
+        const uint32_t p = g.out_pos[qq];
+        const float *J = edge_table<S>(sm, g.pos_tab[p]);
+        float rb[S], sr[S];
+        ldv<S>(rbar + (size_t)p * S, rb);
+        row_sums<S>(J, e, sr);
+#pragma unroll
+        for (int i = 0; i < S; ++i) {
+            const float c = rb[i] / sr[i];
+#pragma unroll
+            for (int j = 0; j < S; ++j) acc[j] += c * J[i * S + j] * e[j];
+        }
+    }
+}
+
+// adjoint of iteration t at node v (mode 0), or of the initial step
+// (mode 1: lQ_1 = lb_0 + lP, messages from send = lb_0), fused with the
+// gather of lQbar_{t+1}(v) from iteration t+1's rbar (rbar_next, null at t=T).
+// Writes lbbar_out (mode 1: lbbar_0 without its own send term), this
+// iteration's rbar, and adds the block's log-table adjoint into epart.
+template <int S>
+__global__ void __launch_bounds__(kUThreads) k_u_bwd(const UGraph g, int mode, const float *__restrict__ send,
+                                                     const float *__restrict__ lb_t,
+                                                     const float *__restrict__ lbbar_t,
+                                                     const float *__restrict__ send_next,
+                                                     const float *__restrict__ rbar_next,
+                                                     float *__restrict__ lbbar_out, float *__restrict__ rbar,
+                                                     double *__restrict__ epart) {
     __shared__ float sm[2 * kUMaxTables * S * S];
     __shared__ float wred[kUThreads / 32][S * S];
     load_tables_smem<S>(g, sm);
@@ -183,7 +228,11 @@ __global__ void __launch_bounds__(kUThreads) k_u_bwd_node(const UGraph g, int mo
             gq[i] = 0.0f;
         }
         if (lbbar_t) ldv<S>(lbbar_t + (size_t)v * S, gb);
-        if (lqbar_next) ldv<S>(lqbar_next + (size_t)v * S, gq);
+        if (rbar_next) {
+            float xn[S];
+            ldv<S>(send_next + (size_t)v * S, xn);
+            gather_xbar<S>(g, sm, v, xn, rbar_next, gq);
+        }
         float out[S];
         if (mode == 0) {
             float lb[S], gs = 0.0f;
@@ -211,20 +260,21 @@ __global__ void __launch_bounds__(kUThreads) k_u_bwd_node(const UGraph g, int mo
         for (int i = 0; i < S; ++i) ps += Pbar[i];
         for (uint32_t p = g.in_ptr[v]; p < g.in_ptr[v + 1]; ++p) {
             const uint8_t tab = g.pos_tab[p];
-            const float *L = edge_table<S>(sm, tab);
-            float x[S], r[S], lm[S], rb[S];
+            const float *J = edge_table<S>(sm, tab);
+            float x[S], e[S], sr[S], lm[S], rb[S];
             ldv<S>(send + (size_t)g.in_src[p] * S, x);
-            log_msg<S>(L, x, r, lm);
+            log_msg<S>(J, x, e, sr, lm);
 #pragma unroll
             for (int i = 0; i < S; ++i) rb[i] = Pbar[i] - expf(lm[i]) * ps;
             stv<S>(rbar + (size_t)p * S, rb);
 #pragma unroll
             for (int i = 0; i < S; ++i) {
+                const float c = rb[i] / sr[i];
 #pragma unroll
                 for (int j = 0; j < S; ++j) {
-                    const float w = expf(L[i * S + j] + x[j] - r[i]);
-                    if (tab & 0x80u) acc[j * S + i] += rb[i] * w;
-                    else acc[i * S + j] += rb[i] * w;
+                    const float w = c * J[i * S + j] * e[j];
+                    if (tab & 0x80u) acc[j * S + i] += w;
+                    else acc[i * S + j] += w;
                 }
             }
         }
@@ -246,8 +296,7 @@ __global__ void __launch_bounds__(kUThreads) k_u_bwd_node(const UGraph g, int mo
     }
 }
 
-// xbar(s) = sum over s's out-edges of sum_i rbar_i w_ij (+ add(s)), with w
-// recomputed from s's own state x = send(s)
+// out(s) = add(s) + x adjoint of s through its out-edges (initial step)
 template <int S>
 __global__ void __launch_bounds__(kUThreads) k_u_bwd_src(const UGraph g, const float *__restrict__ send,
                                                          const float *__restrict__ rbar,
@@ -257,27 +306,9 @@ __global__ void __launch_bounds__(kUThreads) k_u_bwd_src(const UGraph g, const f
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= g.V) return;
     float acc[S], x[S];
-    if (add) ldv<S>(add + (size_t)s * S, acc);
-    else {
-#pragma unroll
-        for (int j = 0; j < S; ++j) acc[j] = 0.0f;
-    }
+    ldv<S>(add + (size_t)s * S, acc);
     ldv<S>(send + (size_t)s * S, x);
-    for (uint32_t qq = g.out_ptr[s]; qq < g.out_ptr[s + 1]; ++qq) {
-        const uint32_t p = g.out_pos[qq];
-        const float *L = edge_table<S>(sm, g.pos_tab[p]);
-        float rb[S];
-        ldv<S>(rbar + (size_t)p * S, rb);
-#pragma unroll
-        for (int i = 0; i < S; ++i) {
-            float t[S];
-#pragma unroll
-            for (int j = 0; j < S; ++j) t[j] = L[i * S + j] + x[j];
-            const float r = lse<S>(t);
-#pragma unroll
-            for (int j = 0; j < S; ++j) acc[j] += rb[i] * expf(t[j] - r);
-        }
-    }
+    gather_xbar<S>(g, sm, s, x, rbar, acc);
     stv<S>(out + (size_t)s * S, acc);
 }
 
@@ -327,9 +358,11 @@ struct bp_unrolled {
     float *seg_b = nullptr, *seg_q = nullptr;  // [ck][V][S] (slot 0 unused)
     float *pp_b = nullptr, *pp_q = nullptr;    // [2][V][S]
     float *bT = nullptr;
-    float *bbar[2] = {nullptr, nullptr}, *qbar[2] = {nullptr, nullptr};
-    float *rbar = nullptr;
+    float *bbar[2] = {nullptr, nullptr};
+    float *rbar[2] = {nullptr, nullptr};
     double *epart = nullptr;
+    float *theta_buf = nullptr, *gtheta_buf = nullptr, *glogp_buf = nullptr;
+    cudaGraphExec_t fwd_exec = nullptr, bwd_exec = nullptr;
     uint32_t nblk = 0;
     bool forward_done = false;
     float fwd_ms = 0.0f, bwd_ms = 0.0f;
@@ -338,14 +371,15 @@ struct bp_unrolled {
 
 namespace bpx {
 
+// the forward on the engine's own buffers (theta_buf, tables): captured once
+// into a CUDA graph, replayed on every call
 template <int S>
-static int u_forward(bp_unrolled *u, const float *theta, const float *logp, float *beliefs) {
+static int u_forward(bp_unrolled *u) {
     const UGraph g{u->V, u->K, u->in_ptr, u->in_src, u->out_ptr, u->out_pos, u->pos_tab, u->tables};
     const size_t VS = (size_t)u->V * S;
     const unsigned gv = grid_for(u->V, kUThreads);
     cudaStream_t st = u->stream;
-    BP_CUDA(cudaMemcpyAsync(u->tables, logp, sizeof(float) * u->K * S * S, cudaMemcpyDeviceToDevice, st));
-    k_u_logsoftmax<S><<<gv, kUThreads, 0, st>>>(u->V, theta, u->ck_b);
+    k_u_logsoftmax<S><<<gv, kUThreads, 0, st>>>(u->V, u->theta_buf, u->ck_b);
     k_u_gather_q<S><<<gv, kUThreads, 0, st>>>(g, u->ck_b, u->ck_b, u->ck_q);
     BP_CUDA(cudaGetLastError());
     // state t lives in checkpoint slot t/ck when t % ck == 0, else in pp[t&1]
@@ -354,23 +388,23 @@ static int u_forward(bp_unrolled *u, const float *theta, const float *logp, floa
     for (uint32_t t = 1; t <= u->T; ++t) {
         float *bo = (t == u->T) ? u->bT : loc_b(t);
         float *qo = (t == u->T) ? u->pp_q + (t & 1) * VS : loc_q(t);
-        if (t != u->T && t % u->ck == 0 && t / u->ck >= u->nck) return set_error(BP_ERR_STATE, "checkpoint slots");
         k_u_iter<S><<<gv, kUThreads, 0, st>>>(g, loc_b(t - 1), loc_q(t - 1), bo, qo);
     }
     BP_CUDA(cudaGetLastError());
-    BP_CUDA(cudaMemcpyAsync(beliefs, u->bT, sizeof(float) * VS, cudaMemcpyDeviceToDevice, st));
     return BP_OK;
 }
 
+// the backward on the engine's own buffers (bbar[0] holds d loss / d lb_T on
+// entry; gtheta_buf, glogp_buf receive the gradients)
 template <int S>
-static int u_backward(bp_unrolled *u, const float *grad_b, float *grad_theta, float *grad_logp) {
+static int u_backward(bp_unrolled *u) {
     const UGraph g{u->V, u->K, u->in_ptr, u->in_src, u->out_ptr, u->out_pos, u->pos_tab, u->tables};
     const size_t VS = (size_t)u->V * S;
     const unsigned gv = grid_for(u->V, kUThreads);
     cudaStream_t st = u->stream;
     BP_CUDA(cudaMemsetAsync(u->epart, 0, sizeof(double) * u->nblk * S * S, st));
-    BP_CUDA(cudaMemcpyAsync(u->bbar[0], grad_b, sizeof(float) * VS, cudaMemcpyDeviceToDevice, st));
-    int bc = 0, qc = -1;   // current bbar buffer; current qbar buffer (-1 = zero)
+    int bc = 0, rn = 0;
+    const float *rb_next = nullptr;   // rbar of iteration t+1 (none at t = T)
     const uint32_t nseg = (u->T + u->ck - 1) / u->ck;
     for (int s = (int)nseg - 1; s >= 0; --s) {
         const uint32_t t0 = (uint32_t)s * u->ck, t_end = std::min(t0 + u->ck, u->T);
@@ -383,27 +417,28 @@ static int u_backward(bp_unrolled *u, const float *grad_b, float *grad_theta, fl
         }
         for (uint32_t t = t_end; t > t0; --t) {
             const uint32_t j = t - t0 - 1;
-            const float *q_t = (j == 0) ? ckq : u->seg_q + j * VS;
+            const float *q_t = (j == 0) ? ckq : u->seg_q + j * VS;           // lQ_t
             const float *b_t = (t == u->T) ? u->bT
                                : (t == t_end) ? u->ck_b + (size_t)(s + 1) * VS
-                                              : u->seg_b + (j + 1) * VS;
-            const float *qb = qc < 0 ? nullptr : u->qbar[qc];
-            k_u_bwd_node<S><<<gv, kUThreads, 0, st>>>(g, 0, q_t, b_t, u->bbar[bc], qb, u->bbar[bc ^ 1], u->rbar,
-                                                      u->epart);
-            const int qn = qc < 0 ? 0 : qc ^ 1;
-            k_u_bwd_src<S><<<gv, kUThreads, 0, st>>>(g, q_t, u->rbar, nullptr, u->qbar[qn]);
+                                              : u->seg_b + (j + 1) * VS;     // lb_t
+            const float *q_next = (t == u->T) ? nullptr
+                                  : (t == t_end) ? u->ck_q + (size_t)(s + 1) * VS
+                                                 : u->seg_q + (j + 1) * VS;  // lQ_{t+1}
+            k_u_bwd<S><<<gv, kUThreads, 0, st>>>(g, 0, q_t, b_t, u->bbar[bc], q_next, rb_next, u->bbar[bc ^ 1],
+                                                 u->rbar[rn], u->epart);
             bc ^= 1;
-            qc = qn;
+            rb_next = u->rbar[rn];
+            rn ^= 1;
         }
     }
     BP_CUDA(cudaGetLastError());
-    // initial step: Q_1 = b_0 * prod normalise(J . b_0(src))
-    const float *b0 = u->ck_b;
-    k_u_bwd_node<S><<<gv, kUThreads, 0, st>>>(g, 1, b0, nullptr, u->bbar[bc], qc < 0 ? nullptr : u->qbar[qc],
-                                              u->bbar[bc ^ 1], u->rbar, u->epart);
-    k_u_bwd_src<S><<<gv, kUThreads, 0, st>>>(g, b0, u->rbar, u->bbar[bc ^ 1], u->bbar[bc]);
-    k_u_logsoftmax_bwd<S><<<gv, kUThreads, 0, st>>>(u->V, b0, u->bbar[bc], grad_theta);
-    k_u_reduce_pair<<<1, 256, 0, st>>>(u->epart, u->nblk, u->K * S * S, grad_logp);
+    // initial step: lQ_1 = lb_0 + sum lm(lb_0); its own x adjoint goes to lb_0
+    const float *b0 = u->ck_b, *q1 = u->ck_q;
+    k_u_bwd<S><<<gv, kUThreads, 0, st>>>(g, 1, b0, nullptr, u->bbar[bc], q1, rb_next, u->bbar[bc ^ 1], u->rbar[rn],
+                                         u->epart);
+    k_u_bwd_src<S><<<gv, kUThreads, 0, st>>>(g, b0, u->rbar[rn], u->bbar[bc ^ 1], u->bbar[bc]);
+    k_u_logsoftmax_bwd<S><<<gv, kUThreads, 0, st>>>(u->V, b0, u->bbar[bc], u->gtheta_buf);
+    k_u_reduce_pair<<<1, 256, 0, st>>>(u->epart, u->nblk, u->K * S * S, u->glogp_buf);
     BP_CUDA(cudaGetLastError());
     return BP_OK;
 }
@@ -411,10 +446,12 @@ static int u_backward(bp_unrolled *u, const float *grad_b, float *grad_theta, fl
 static void u_free(bp_unrolled *u) {
     if (!u) return;
     void *ptrs[] = {u->in_ptr, u->in_src, u->out_ptr, u->out_pos, u->pos_tab, u->tables, u->ck_b, u->ck_q,
-                    u->seg_b, u->seg_q, u->pp_b, u->pp_q, u->bT, u->bbar[0], u->bbar[1], u->qbar[0],
-                    u->qbar[1], u->rbar, u->epart};
+                    u->seg_b, u->seg_q, u->pp_b, u->pp_q, u->bT, u->bbar[0], u->bbar[1], u->rbar[0],
+                    u->rbar[1], u->epart, u->theta_buf, u->gtheta_buf, u->glogp_buf};
     for (void *p : ptrs)
         if (p) cudaFree(p);
+    if (u->fwd_exec) cudaGraphExecDestroy(u->fwd_exec);
+    if (u->bwd_exec) cudaGraphExecDestroy(u->bwd_exec);
     if (u->ev0) cudaEventDestroy(u->ev0);
     if (u->ev1) cudaEventDestroy(u->ev1);
     if (u->own_stream && u->stream) cudaStreamDestroy(u->stream);
@@ -497,9 +534,12 @@ int bp_unrolled_create(bp_unrolled **out, uint32_t V, uint32_t E, uint32_t S, ui
               alloc((void **)&u->seg_b, sizeof(float) * VS * ck) && alloc((void **)&u->seg_q, sizeof(float) * VS * ck) &&
               alloc((void **)&u->pp_b, sizeof(float) * VS * 2) && alloc((void **)&u->pp_q, sizeof(float) * VS * 2) &&
               alloc((void **)&u->bT, sizeof(float) * VS) && alloc((void **)&u->bbar[0], sizeof(float) * VS) &&
-              alloc((void **)&u->bbar[1], sizeof(float) * VS) && alloc((void **)&u->qbar[0], sizeof(float) * VS) &&
-              alloc((void **)&u->qbar[1], sizeof(float) * VS) && alloc((void **)&u->rbar, sizeof(float) * S * (size_t)E) &&
-              alloc((void **)&u->epart, sizeof(double) * u->nblk * S * S);
+              alloc((void **)&u->bbar[1], sizeof(float) * VS) &&
+              alloc((void **)&u->rbar[0], sizeof(float) * S * (size_t)E) &&
+              alloc((void **)&u->rbar[1], sizeof(float) * S * (size_t)E) &&
+              alloc((void **)&u->epart, sizeof(double) * u->nblk * S * S) &&
+              alloc((void **)&u->theta_buf, sizeof(float) * VS) && alloc((void **)&u->gtheta_buf, sizeof(float) * VS) &&
+              alloc((void **)&u->glogp_buf, sizeof(float) * K * S * S);
     if (!ok) {
         u_free(u);
         return set_error(BP_ERR_NOMEM, "device allocation failed for the unrolled graph");
@@ -527,26 +567,55 @@ void bp_unrolled_destroy(bp_unrolled *u) {
     u_free(u);
 }
 
-int bp_unrolled_forward(bp_unrolled *u, const float *log_unary, const float *log_pair, float *beliefs) {
-    if (!u || !log_unary || !log_pair || !beliefs) return set_error(BP_ERR_INVALID, "null argument");
-    if (((uintptr_t)log_unary | (uintptr_t)beliefs) & 15u)
-        return set_error(BP_ERR_INVALID, "log_unary and beliefs must be 16-byte aligned");
-    BP_CUDA(cudaEventRecord(u->ev0, u->stream));
+static int capture(bp_unrolled *u, cudaGraphExec_t *exec, int (*body)(bp_unrolled *)) {
+    cudaGraph_t graph = nullptr;
+    BP_CUDA(cudaStreamBeginCapture(u->stream, cudaStreamCaptureModeThreadLocal));
+    int st = body(u);
+    cudaError_t ce = cudaStreamEndCapture(u->stream, &graph);
+    if (st) {
+        if (graph) cudaGraphDestroy(graph);
+        return st;
+    }
+    if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture", __FILE__, __LINE__);
+    cudaError_t ie = cudaGraphInstantiate(exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) return cuda_fail(ie, "cudaGraphInstantiate", __FILE__, __LINE__);
+    return BP_OK;
+}
+
+static int fwd_body(bp_unrolled *u) { BP_DISPATCH_S(u->S, u_forward, u); }
+static int bwd_body(bp_unrolled *u) { BP_DISPATCH_S(u->S, u_backward, u); }
+
+int bp_unrolled_forward(bp_unrolled *u, const float *log_unary, const float *log_pair, float *log_beliefs) {
+    if (!u || !log_unary || !log_pair || !log_beliefs) return set_error(BP_ERR_INVALID, "null argument");
+    if (((uintptr_t)log_unary | (uintptr_t)log_beliefs) & 15u)
+        return set_error(BP_ERR_INVALID, "log_unary and log_beliefs must be 16-byte aligned");
+    const size_t VS = (size_t)u->V * u->S;
+    BP_CUDA(cudaMemcpyAsync(u->theta_buf, log_unary, sizeof(float) * VS, cudaMemcpyDeviceToDevice, u->stream));
+    BP_CUDA(cudaMemcpyAsync(u->tables, log_pair, sizeof(float) * u->K * u->S * u->S, cudaMemcpyDeviceToDevice,
+                            u->stream));
     int st;
-    auto run = [&]() -> int { BP_DISPATCH_S(u->S, u_forward, u, log_unary, log_pair, beliefs); };
-    if ((st = run())) return st;
-    BP_CUDA(cudaEventRecord(u->ev1, u->stream));
+    if (!u->fwd_exec && (st = capture(u, &u->fwd_exec, fwd_body))) return st;
+    BP_CUDA(cudaGraphLaunch(u->fwd_exec, u->stream));
+    BP_CUDA(cudaMemcpyAsync(log_beliefs, u->bT, sizeof(float) * VS, cudaMemcpyDeviceToDevice, u->stream));
     u->forward_done = true;
     return BP_OK;
 }
 
-int bp_unrolled_backward(bp_unrolled *u, const float *grad_beliefs, float *grad_log_unary, float *grad_log_pair) {
-    if (!u || !grad_beliefs || !grad_log_unary || !grad_log_pair) return set_error(BP_ERR_INVALID, "null argument");
-    if (((uintptr_t)grad_beliefs | (uintptr_t)grad_log_unary) & 15u)
-        return set_error(BP_ERR_INVALID, "grad_beliefs and grad_log_unary must be 16-byte aligned");
+int bp_unrolled_backward(bp_unrolled *u, const float *grad_log_beliefs, float *grad_log_unary, float *grad_log_pair) {
+    if (!u || !grad_log_beliefs || !grad_log_unary || !grad_log_pair) return set_error(BP_ERR_INVALID, "null argument");
+    if (((uintptr_t)grad_log_beliefs | (uintptr_t)grad_log_unary) & 15u)
+        return set_error(BP_ERR_INVALID, "grad_log_beliefs and grad_log_unary must be 16-byte aligned");
     if (!u->forward_done) return set_error(BP_ERR_STATE, "backward before forward");
-    auto run = [&]() -> int { BP_DISPATCH_S(u->S, u_backward, u, grad_beliefs, grad_log_unary, grad_log_pair); };
-    return run();
+    const size_t VS = (size_t)u->V * u->S;
+    BP_CUDA(cudaMemcpyAsync(u->bbar[0], grad_log_beliefs, sizeof(float) * VS, cudaMemcpyDeviceToDevice, u->stream));
+    int st;
+    if (!u->bwd_exec && (st = capture(u, &u->bwd_exec, bwd_body))) return st;
+    BP_CUDA(cudaGraphLaunch(u->bwd_exec, u->stream));
+    BP_CUDA(cudaMemcpyAsync(grad_log_unary, u->gtheta_buf, sizeof(float) * VS, cudaMemcpyDeviceToDevice, u->stream));
+    BP_CUDA(cudaMemcpyAsync(grad_log_pair, u->glogp_buf, sizeof(float) * u->K * u->S * u->S,
+                            cudaMemcpyDeviceToDevice, u->stream));
+    return BP_OK;
 }
 
 int bp_unrolled_set_stream(bp_unrolled *u, void *stream) {

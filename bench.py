@@ -606,13 +606,23 @@ def main():
         src_h, dst_h, joint_h, bel_h = pin(net.src), pin(net.dst), pin(net.joint), pin(net.beliefs)
         out_h = torch.empty((V, S), dtype=torch.float32).pin_memory()
 
-        def e2e_step():
+        phases = {"create_ms": 0.0, "solve_ms": 0.0, "read_ms": 0.0, "destroy_ms": 0.0}
+
+        def e2e_step(record=False):
+            t0 = time.perf_counter()
             g2 = BPGraph(V, src_h, dst_h, joint_h, uniform_states=2, stream=handle, reorder=bool(a.reorder))
             g2.set_beliefs(bel_h)
+            t1 = time.perf_counter()
             g2.init_messages()
             g2.loopy(0.0, a.iterations, delta="f64")
+            t2 = time.perf_counter()
             g2.beliefs(out=out_h)
+            t3 = time.perf_counter()
             g2.close()
+            t4 = time.perf_counter()
+            if record:
+                for k, dt in zip(phases, (t1 - t0, t2 - t1, t3 - t2, t4 - t3)):
+                    phases[k] += 1e3 * dt / a.e2e_steps
 
         e2e_step()
         barrier()
@@ -621,7 +631,7 @@ def main():
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(a.e2e_steps):
-            e2e_step()
+            e2e_step(record=True)
         e1.record(stream)
         barrier()
         ems = e0.elapsed_time(e1) / a.e2e_steps
@@ -633,7 +643,7 @@ def main():
             ems = float(t.item())
         e2e = {"value": float(E) * a.iterations * world / (ems / 1e3), "unit": UNIT,
                "h2d_bytes_per_step": int(E * (4 + 4 + 4 * S * S) + V * 4 * S), "d2h_bytes_per_step": int(V * 4 * S),
-               "ms_per_step": ems}
+               "ms_per_step": ems, "phases_wall_ms": {k: round(v, 2) for k, v in phases.items()}}
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:

