@@ -13,6 +13,8 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
+#include <chrono>
 #include <vector>
 
 #include "bp_device.cuh"
@@ -37,22 +39,66 @@ int cuda_fail(cudaError_t e, const char *what, const char *file, int line) {
     return set_error(st, "%s failed: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
 }
 
+// Graph buffers come from the device's stream-ordered memory pool, whose
+// release threshold is raised once per device: memory freed by one graph
+// stays cached for the next instead of going back to the driver, so
+// creating and destroying graphs of similar size costs no cudaMalloc /
+// cudaFree round trips.  bp_release_cached_memory() trims the pool.
+static std::mutex g_pool_mutex;
+static bool g_pool_ready[64];
+
+static void ensure_pool(int dev) {
+    if (dev < 0 || dev >= 64) return;
+    std::lock_guard<std::mutex> lock(g_pool_mutex);
+    if (g_pool_ready[dev]) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t threshold = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+    }
+    g_pool_ready[dev] = true;
+}
+
 int dev_alloc(bp_graph *g, void **p, size_t bytes) {
     *p = nullptr;
     if (bytes == 0) bytes = 16;
-    cudaError_t e = cudaMalloc(p, bytes);
+    cudaError_t e = cudaMallocAsync(p, bytes, g->stream);
     if (e != cudaSuccess) {
         *p = nullptr;
-        return cuda_fail(e, "cudaMalloc", __FILE__, __LINE__);
+        return cuda_fail(e, "cudaMallocAsync", __FILE__, __LINE__);
     }
     g->device_bytes += bytes;
     return BP_OK;
 }
 
+// the pinned control blocks of loopy runs, reused across graphs
+static std::mutex g_pinned_mutex;
+static std::vector<LoopyCtl *> g_pinned_free;
+
+static LoopyCtl *pinned_ctl() {
+    {
+        std::lock_guard<std::mutex> lock(g_pinned_mutex);
+        if (!g_pinned_free.empty()) {
+            LoopyCtl *c = g_pinned_free.back();
+            g_pinned_free.pop_back();
+            return c;
+        }
+    }
+    LoopyCtl *c = nullptr;
+    if (cudaMallocHost((void **)&c, sizeof(LoopyCtl)) != cudaSuccess) return nullptr;
+    return c;
+}
+
+static void release_pinned_ctl(LoopyCtl *c) {
+    if (!c) return;
+    std::lock_guard<std::mutex> lock(g_pinned_mutex);
+    g_pinned_free.push_back(c);
+}
+
 int ensure_staging(bp_graph *g, size_t bytes) {
     if (g->staging_bytes >= bytes) return BP_OK;
     if (g->staging) {
-        cudaFree(g->staging);
+        cudaFreeAsync(g->staging, g->stream);
         g->device_bytes -= g->staging_bytes;
         g->staging = nullptr;
         g->staging_bytes = 0;
@@ -342,12 +388,16 @@ static void free_graph(bp_graph *g) {
     void *ptrs[] = {g->new_to_old, g->in_ptr, g->in_src, g->pos_edge, g->edge_pos, g->pos_dims, g->node_s, g->joint,
                     g->belief, g->msg[0], g->msg[1], g->q[0], g->q[1], g->out_ptr, g->out_pos,
                     g->out_dst, g->pos_dst, g->partials, g->absdiff, g->ctl, g->visited, g->staging,
-                    g->run_len, g->run_s, g->tree.d_node_level, g->tree.d_node_lidx, g->tree.d_wave_nodes};
+                    g->run_len, g->run_s};
     for (void *p : ptrs)
+        if (p) cudaFreeAsync(p, g->stream);
+    void *tree_ptrs[] = {g->tree.d_node_level, g->tree.d_node_lidx, g->tree.d_wave_nodes};
+    for (void *p : tree_ptrs)
         if (p) cudaFree(p);
     for (auto &c : g->loop_graph)
         if (c.exec) cudaGraphExecDestroy(c.exec);
-    if (g->ctl_host) cudaFreeHost(g->ctl_host);
+    if (g->stream) cudaStreamSynchronize(g->stream);
+    release_pinned_ctl(g->ctl_host);
     if (g->ev0) cudaEventDestroy(g->ev0);
     if (g->ev1) cudaEventDestroy(g->ev1);
     if (g->own_stream && g->stream) cudaStreamDestroy(g->stream);
@@ -359,9 +409,27 @@ static void free_graph(bp_graph *g) {
     delete g;
 }
 
+// BP_TRACE=1: wall time of each stage of bp_graph_create on stderr (each
+// mark waits for the graph's stream, so tracing serialises the stages)
+struct StageTrace {
+    bool on;
+    cudaStream_t s;
+    std::chrono::steady_clock::time_point t;
+    explicit StageTrace(cudaStream_t s_) : on(getenv("BP_TRACE") != nullptr), s(s_), t(std::chrono::steady_clock::now()) {}
+    void mark(const char *what) {
+        if (!on) return;
+        cudaStreamSynchronize(s);
+        const auto n = std::chrono::steady_clock::now();
+        fprintf(stderr, "bp_trace create %-22s %9.3f ms\n", what,
+                std::chrono::duration<double, std::milli>(n - t).count());
+        t = n;
+    }
+};
+
 static int create_impl(bp_graph *g, const bp_graph_desc *d) {
     const uint32_t V = d->num_nodes, E = d->num_edges;
     int st;
+    StageTrace trace(g->stream);
     // ---- state counts (validated on the host when they are host memory)
     std::vector<uint32_t> s32;
     const uint32_t *states = d->node_num_states;
@@ -387,7 +455,12 @@ static int create_impl(bp_graph *g, const bp_graph_desc *d) {
     g->ms = smax;
     g->uniform = (smax == smin) ? smax : 0;
     g->node_s_host = (uint8_t *)malloc(V ? V : 1);
-    for (uint32_t v = 0; v < V; ++v) g->node_s_host[v] = (uint8_t)(states ? states[v] : d->uniform_states);
+    if (!g->node_s_host) return set_error(BP_ERR_NOMEM, "host allocation failed");
+    if (states)
+        for (uint32_t v = 0; v < V; ++v) g->node_s_host[v] = (uint8_t)states[v];
+    else
+        memset(g->node_s_host, (int)d->uniform_states, V);
+    trace.mark("state counts");
 
     // ---- device arrays
     const size_t ms = g->ms;
@@ -407,9 +480,11 @@ static int create_impl(bp_graph *g, const bp_graph_desc *d) {
     }
     BP_CUDA(cudaMemsetAsync(g->belief, 0, sizeof(float) * ms * (size_t)V, g->stream));
     if ((st = dev_alloc(g, (void **)&g->ctl, sizeof(bpx::LoopyCtl)))) return st;
-    BP_CUDA(cudaMallocHost((void **)&g->ctl_host, sizeof(bpx::LoopyCtl)));
+    g->ctl_host = pinned_ctl();
+    if (!g->ctl_host) return set_error(BP_ERR_NOMEM, "pinned host allocation failed");
     if ((st = dev_alloc(g, (void **)&g->visited, (size_t)V))) return st;
     BP_CUDA(cudaMemsetAsync(g->visited, 0, (size_t)V, g->stream));
+    trace.mark("allocate + clear");
 
     // state counts -> u8
     {
@@ -424,6 +499,32 @@ static int create_impl(bp_graph *g, const bp_graph_desc *d) {
             BP_CUDA(cudaGetLastError());
         }
         if (owned) cudaFreeAsync(s_dev, g->stream);
+    }
+
+    // ---- joint tables of a host graph: upload on a side stream while the
+    // edges are sorted on the graph's stream
+    void *jd = nullptr;
+    bool own_j = false;
+    cudaStream_t side = nullptr;
+    cudaEvent_t joint_ready = nullptr;
+    size_t jbytes = 0;
+    if (E) {
+        const uint32_t rs = d->joint_row_stride;
+        const uint64_t es = d->joint_edge_stride;
+        if (rs < g->ms || es < (uint64_t)rs * (g->ms - 1) + g->ms)
+            return set_error(BP_ERR_SHAPE, "joint strides (%u, %llu) too small for %u states", rs,
+                             (unsigned long long)es, g->ms);
+        jbytes = sizeof(float) * (es * (uint64_t)(E - 1) + (uint64_t)rs * (g->ms - 1) + g->ms);
+        if (d->memory == BP_MEM_HOST) {
+            BP_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+            BP_CUDA(cudaEventCreateWithFlags(&joint_ready, cudaEventDisableTiming));
+            BP_CUDA(cudaMallocAsync(&jd, jbytes, side));
+            BP_CUDA(cudaMemcpyAsync(jd, d->edge_joint, jbytes, cudaMemcpyHostToDevice, side));
+            BP_CUDA(cudaEventRecord(joint_ready, side));
+            own_j = true;
+        } else {
+            jd = const_cast<float *>(d->edge_joint);
+        }
     }
 
     // ---- edges
@@ -448,6 +549,7 @@ static int create_impl(bp_graph *g, const bp_graph_desc *d) {
             return set_error(BP_ERR_INVALID, "an edge endpoint is >= num_nodes (%u)", V);
         }
     }
+    trace.mark("edges in + validate");
 
 
     if (d->flags & BP_GRAPH_REORDER_BY_OUT_DEGREE) {
@@ -488,12 +590,10 @@ static int create_impl(bp_graph *g, const bp_graph_desc *d) {
             k_permute_u8<<<grid_for(V, 256), 256, 0, g->stream>>>(g->node_s, g->new_to_old, V, s8);
             BP_CUDA(cudaMemcpyAsync(g->node_s, s8, V, cudaMemcpyDeviceToDevice, g->stream));
             cudaFreeAsync(s8, g->stream);
-            std::vector<uint32_t> perm(V);
-            BP_CUDA(cudaMemcpyAsync(perm.data(), g->new_to_old, sizeof(uint32_t) * V, cudaMemcpyDeviceToHost,
-                                    g->stream));
-            BP_CUDA(cudaStreamSynchronize(g->stream));
-            std::vector<uint8_t> s_old(g->node_s_host, g->node_s_host + V);
-            for (uint32_t i = 0; i < V; ++i) g->node_s_host[i] = s_old[perm[i]];
+            if (!g->uniform) {
+                BP_CUDA(cudaMemcpyAsync(g->node_s_host, g->node_s, V, cudaMemcpyDeviceToHost, g->stream));
+                BP_CUDA(cudaStreamSynchronize(g->stream));
+            }
         }
         BP_CUDA(cudaGetLastError());
         cudaFreeAsync(deg, g->stream);
@@ -505,6 +605,7 @@ static int create_impl(bp_graph *g, const bp_graph_desc *d) {
         src = src2;
         dst = dst2;
         own_src = own_dst = true;
+        trace.mark("renumber");
     }
 
     if (d->dest_node_list && d->dest_edge_list) {
@@ -535,6 +636,7 @@ static int create_impl(bp_graph *g, const bp_graph_desc *d) {
         cudaFreeAsync(iota, g->stream);
         cudaFreeAsync(keys, g->stream);
     }
+    trace.mark("dest sort");
     if (E) {
         k_positions<<<grid_for(E, 256), 256, 0, g->stream>>>(g->pos_edge, (const uint32_t *)src,
                                                              (const uint32_t *)dst, E, g->node_s, g->in_src,
@@ -542,25 +644,23 @@ static int create_impl(bp_graph *g, const bp_graph_desc *d) {
         BP_CUDA(cudaGetLastError());
     }
 
-    // ---- joint tables: stage host tables in edge-id order, then gather
+    // ---- joint tables: edge-id order with the caller's strides -> position order
     if (E) {
-        const uint32_t rs = d->joint_row_stride;
-        const uint64_t es = d->joint_edge_stride;
-        if (rs < g->ms || es < (uint64_t)rs * (g->ms - 1) + g->ms)
-            return set_error(BP_ERR_SHAPE, "joint strides (%u, %llu) too small for %u states", rs,
-                             (unsigned long long)es, g->ms);
-        const size_t jbytes = sizeof(float) * (es * (uint64_t)(E - 1) + (uint64_t)rs * (g->ms - 1) + g->ms);
-        void *jd = nullptr;
-        bool own_j = false;
-        if ((st = to_device(g, d->edge_joint, jbytes, d->memory, &jd, &own_j))) return st;
-        if ((st = gather_joint(g, (const float *)jd, rs, es, (const uint32_t *)dst))) return st;
+        if (joint_ready) BP_CUDA(cudaStreamWaitEvent(g->stream, joint_ready, 0));
+        if ((st = gather_joint(g, (const float *)jd, d->joint_row_stride, d->joint_edge_stride,
+                               (const uint32_t *)dst)))
+            return st;
         if (own_j) cudaFreeAsync(jd, g->stream);
     }
+    trace.mark("positions + joint");
+    if (joint_ready) cudaEventDestroy(joint_ready);
+    if (side) cudaStreamDestroy(side);
     if (own_src) cudaFreeAsync(src, g->stream);
     if (own_dst) cudaFreeAsync(dst, g->stream);
     BP_CUDA(cudaEventCreate(&g->ev0));
     BP_CUDA(cudaEventCreate(&g->ev1));
     BP_CUDA(cudaStreamSynchronize(g->stream));
+    trace.mark("finish");
     return BP_OK;
 }
 
@@ -601,6 +701,7 @@ int bp_graph_create(bp_graph **out, const bp_graph_desc *d, void *stream) {
     if (e != cudaSuccess || ndev == 0) return set_error(BP_ERR_NO_DEVICE, "no CUDA device available");
     bp_graph *g = new bp_graph();
     cudaGetDevice(&g->device);
+    ensure_pool(g->device);
     g->V = d->num_nodes;
     g->E = d->num_edges;
     if (stream) {
@@ -628,6 +729,16 @@ void bp_graph_destroy(bp_graph *g) {
     if (!g) return;
     if (g->stream) cudaStreamSynchronize(g->stream);
     free_graph(g);
+}
+
+int bp_release_cached_memory(void) {
+    int dev = 0;
+    BP_CUDA(cudaGetDevice(&dev));
+    cudaMemPool_t pool;
+    BP_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
+    BP_CUDA(cudaDeviceSynchronize());
+    BP_CUDA(cudaMemPoolTrimTo(pool, 0));
+    return BP_OK;
 }
 
 int bp_graph_info(const bp_graph *g, uint32_t *V, uint32_t *E, uint32_t *ms, uint32_t *uni) {

@@ -37,6 +37,10 @@ namespace bpx {
 
 template <int MS> constexpr int flood_nt() { return MS <= 4 ? 256 : 128; }
 template <int MS> constexpr int flood_smem_floats() { return MS <= 2 ? 4096 : 8192; }
+// in-edges per thread per phase-1 round of k_flood (tables held in registers)
+template <int MS> constexpr int flood_unroll() { return MS <= 2 ? 4 : (MS <= 4 ? 2 : 1); }
+// resident blocks per SM the register allocation must allow
+template <int MS, int FU> constexpr int flood_min_blocks() { return MS <= 2 && FU >= 4 ? 4 : 1; }
 
 struct FloodArgs {
     uint32_t V;
@@ -124,8 +128,8 @@ __device__ __forceinline__ void reduce_and_finalize(LoopyCtl *ctl, double *parti
     }
 }
 
-template <int MS, bool UNI>
-__global__ void __launch_bounds__(flood_nt<MS>()) k_flood(const FloodArgs a) {
+template <int MS, bool UNI, int FU>
+__global__ void __launch_bounds__(flood_nt<MS>(), flood_min_blocks<MS, FU>()) k_flood(const FloodArgs a) {
     constexpr int NT = flood_nt<MS>();
     constexpr uint32_t EMAX = flood_smem_floats<MS>() / MS;
     __shared__ __align__(16) float sm[EMAX * MS];
@@ -162,36 +166,58 @@ __global__ void __launch_bounds__(flood_nt<MS>()) k_flood(const FloodArgs a) {
 
     for (uint32_t c0 = e0; c0 < e1; c0 += EMAX) {
         const uint32_t c1 = min(e1, c0 + EMAX);
-        // phase 1: messages of this chunk of in-edges
-        for (uint32_t p = c0 + tid; p < c1; p += NT) {
-            const uint32_t s = __ldcs(a.in_src + p);
-            int x = MS, y = MS;
-            if (!UNI) {
-                const uint8_t d = a.pos_dims[p];
-                x = d & 15;
-                y = d >> 4;
-            }
-            float q[MS], m[MS];
-            ldv<MS>(q_in + (size_t)s * MS, q);
-            send_msg<MS, UNI>(a.joint + (size_t)p * (MS * MS), q, x, y, m);
-            if (want) {
-                float o[MS], ad[MS];
-                ldv<MS, kStream>(m_old + (size_t)p * MS, o);
+        // phase 1: messages of this chunk of in-edges, FU edges per thread per
+        // round with every load of the round issued before the first use, so
+        // a thread keeps FU gathers in flight instead of one
+        for (uint32_t pb = c0 + tid; pb < c1; pb += NT * FU) {
+            uint32_t src[FU];
+            int x[FU], y[FU];
+            float jt[FU][FU > 1 ? MS * MS : 1], o[FU][MS], q[FU][MS];
 #pragma unroll
-                for (int k = 0; k < MS; ++k) {
-                    float d = 0.0f;
-                    if (UNI || k < x) {
-                        d = FSUB(o[k], m[k]);
-                        if (d != d) d = 0.0f;
-                        d = fabsf(d);
+            for (int u = 0; u < FU; ++u) {
+                const uint32_t p = pb + u * NT;
+                src[u] = 0;
+                x[u] = MS;
+                y[u] = MS;
+                if (p < c1) {
+                    src[u] = __ldcs(a.in_src + p);
+                    if (!UNI) {
+                        const uint8_t d = a.pos_dims[p];
+                        x[u] = d & 15;
+                        y[u] = d >> 4;
                     }
-                    ad[k] = d;
-                    dsum += (double)d;
+                    if constexpr (FU > 1) ldv<MS * MS, kStream>(a.joint + (size_t)p * (MS * MS), jt[u]);
+                    if (want) ldv<MS, kStream>(m_old + (size_t)p * MS, o[u]);
                 }
-                if (serial) stv<MS>(a.absdiff + (size_t)__ldg(a.pos_edge + p) * MS, ad);
             }
-            stv<MS, kStream>(m_new + (size_t)p * MS, m);
-            stv<MS>(sm + (size_t)(p - c0) * MS, m);
+#pragma unroll
+            for (int u = 0; u < FU; ++u)
+                if (pb + u * NT < c1) ldv<MS>(q_in + (size_t)src[u] * MS, q[u]);
+#pragma unroll
+            for (int u = 0; u < FU; ++u) {
+                const uint32_t p = pb + u * NT;
+                if (p >= c1) break;
+                float m[MS];
+                if constexpr (FU > 1) send_msg_regs<MS, UNI>(jt[u], q[u], x[u], y[u], m);
+                else send_msg<MS, UNI>(a.joint + (size_t)p * (MS * MS), q[u], x[u], y[u], m);
+                if (want) {
+                    float ad[MS];
+#pragma unroll
+                    for (int k = 0; k < MS; ++k) {
+                        float d = 0.0f;
+                        if (UNI || k < x[u]) {
+                            d = FSUB(o[u][k], m[k]);
+                            if (d != d) d = 0.0f;
+                            d = fabsf(d);
+                        }
+                        ad[k] = d;
+                        dsum += (double)d;
+                    }
+                    if (serial) stv<MS>(a.absdiff + (size_t)__ldg(a.pos_edge + p) * MS, ad);
+                }
+                stv<MS, kStream>(m_new + (size_t)p * MS, m);
+                stv<MS>(sm + (size_t)(p - c0) * MS, m);
+            }
         }
         __syncthreads();
         // phase 2a: this node's product over its in-edges inside the chunk
@@ -640,7 +666,7 @@ __global__ void __launch_bounds__(256) k_edge_delta(const EdgeArgs a) {
 static int ensure_partials(bp_graph *g, uint32_t n) {
     if (g->partials_cap >= n) return BP_OK;
     if (g->partials) {
-        cudaFree(g->partials);
+        cudaFreeAsync(g->partials, g->stream);
         g->partials = nullptr;
     }
     for (auto &c : g->loop_graph)
@@ -759,14 +785,20 @@ static int enqueue_node_iterations(bp_graph *g, uint32_t k, bool serial, int var
     const uint64_t n = (uint64_t)g->E * MS;
     // edges in flight per lane: BP_FLOOD_UNROLL=1|2|4 overrides the default
     // for 1- and 2-state graphs (all variants give identical results)
-    int unroll = wflood_unroll<MS>();
+    int unroll = warp_tiled ? wflood_unroll<MS>() : flood_unroll<MS>();
     if constexpr (MS <= 2) {
         const char *env = getenv("BP_FLOOD_UNROLL");
         if (env && (env[0] == '1' || env[0] == '2' || env[0] == '4')) unroll = env[0] - '0';
     }
     for (uint32_t i = 0; i < k; ++i) {
         if (!warp_tiled) {
-            k_flood<MS, UNI><<<grid, NT, 0, g->stream>>>(a);
+            if constexpr (MS <= 2) {
+                if (unroll == 1) k_flood<MS, UNI, 1><<<grid, NT, 0, g->stream>>>(a);
+                else if (unroll == 2) k_flood<MS, UNI, 2><<<grid, NT, 0, g->stream>>>(a);
+                else k_flood<MS, UNI, 4><<<grid, NT, 0, g->stream>>>(a);
+            } else {
+                k_flood<MS, UNI, flood_unroll<MS>()><<<grid, NT, 0, g->stream>>>(a);
+            }
         } else if constexpr (MS <= 2) {
             if (unroll == 1) k_flood_w<MS, UNI, 1><<<grid, 256, 0, g->stream>>>(a);
             else if (unroll == 2) k_flood_w<MS, UNI, 2><<<grid, 256, 0, g->stream>>>(a);
@@ -1087,7 +1119,7 @@ static int noalloc_run(uint32_t V, uint32_t E, const uint32_t *in_ptr, const uin
     uint32_t done = 0;
     for (uint32_t launched = 0; launched < max_it && !done; launched += 32) {
         const uint32_t n = std::min<uint32_t>(32, max_it - launched);
-        for (uint32_t i = 0; i < n; ++i) k_flood<MS, true><<<grid, NT, 0, stream>>>(a);
+        for (uint32_t i = 0; i < n; ++i) k_flood<MS, true, flood_unroll<MS>()><<<grid, NT, 0, stream>>>(a);
         BP_CUDA(cudaGetLastError());
         BP_CUDA(cudaMemcpyAsync(&done, &ctl->done, sizeof(done), cudaMemcpyDeviceToHost, stream));
         BP_CUDA(cudaStreamSynchronize(stream));

@@ -40,6 +40,10 @@ namespace bpx {
 
 constexpr int kUThreads = 256;
 constexpr uint32_t kUMaxTables = 16;
+// the adjoint kernel keeps S*S table-adjoint accumulators per thread: in
+// registers for S <= 4, else in a shared-memory slice per thread (entry-major,
+// so a warp's adds hit 32 different banks) with smaller blocks
+template <int S> constexpr int bwd_threads() { return S <= 4 ? 256 : 64; }
 
 struct UGraph {
     uint32_t V, K;
@@ -206,20 +210,27 @@ __device__ __forceinline__ void gather_xbar(const UGraph &g, const float *sm, ui
 // Writes lbbar_out (mode 1: lbbar_0 without its own send term), this
 // iteration's rbar, and adds the block's log-table adjoint into epart.
 template <int S>
-__global__ void __launch_bounds__(kUThreads) k_u_bwd(const UGraph g, int mode, const float *__restrict__ send,
-                                                     const float *__restrict__ lb_t,
-                                                     const float *__restrict__ lbbar_t,
-                                                     const float *__restrict__ send_next,
-                                                     const float *__restrict__ rbar_next,
-                                                     float *__restrict__ lbbar_out, float *__restrict__ rbar,
-                                                     double *__restrict__ epart) {
+__global__ void __launch_bounds__(bwd_threads<S>()) k_u_bwd(const UGraph g, int mode, const float *__restrict__ send,
+                                                           const float *__restrict__ lb_t,
+                                                           const float *__restrict__ lbbar_t,
+                                                           const float *__restrict__ send_next,
+                                                           const float *__restrict__ rbar_next,
+                                                           float *__restrict__ lbbar_out, float *__restrict__ rbar,
+                                                           double *__restrict__ epart) {
+    constexpr int NT = bwd_threads<S>();
+    constexpr bool REG = S <= 4;
     __shared__ float sm[2 * kUMaxTables * S * S];
-    __shared__ float wred[kUThreads / 32][S * S];
+    __shared__ float sacc[REG ? 1 : S * S * NT];
+    __shared__ float wred[NT / 32][REG ? S * S : 1];
     load_tables_smem<S>(g, sm);
     const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-    float acc[S * S];
+    float acc[REG ? S * S : 1];
+    if constexpr (REG) {
 #pragma unroll
-    for (int k = 0; k < S * S; ++k) acc[k] = 0.0f;
+        for (int k = 0; k < S * S; ++k) acc[k] = 0.0f;
+    } else {
+        for (int k = 0; k < S * S; ++k) sacc[k * NT + threadIdx.x] = 0.0f;
+    }
     if (v < g.V) {
         float gb[S], gq[S], Pbar[S];
 #pragma unroll
@@ -267,32 +278,44 @@ __global__ void __launch_bounds__(kUThreads) k_u_bwd(const UGraph g, int mode, c
 #pragma unroll
             for (int i = 0; i < S; ++i) rb[i] = Pbar[i] - expf(lm[i]) * ps;
             stv<S>(rbar + (size_t)p * S, rb);
+            const bool tr = (tab & 0x80u) != 0;
 #pragma unroll
             for (int i = 0; i < S; ++i) {
                 const float c = rb[i] / sr[i];
 #pragma unroll
                 for (int j = 0; j < S; ++j) {
                     const float w = c * J[i * S + j] * e[j];
-                    if (tab & 0x80u) acc[j * S + i] += w;
-                    else acc[i * S + j] += w;
+                    const int k = tr ? j * S + i : i * S + j;
+                    if constexpr (REG) acc[k] += w;
+                    else sacc[k * NT + threadIdx.x] += w;
                 }
             }
         }
     }
-    // block sum of acc (fixed order), added to this block's running partial
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    // block sum of the accumulators (fixed order), added to this block's
+    // running partial
+    if constexpr (REG) {
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
-    for (int k = 0; k < S * S; ++k) {
-        float x = acc[k];
+        for (int k = 0; k < S * S; ++k) {
+            float x = acc[k];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-        if (lane == 0) wred[w][k] = x;
-    }
-    __syncthreads();
-    for (int k = threadIdx.x; k < S * S; k += blockDim.x) {
-        double t = 0.0;
-        for (int ww = 0; ww < (int)(blockDim.x >> 5); ++ww) t += (double)wred[ww][k];
-        epart[(size_t)blockIdx.x * S * S + k] += t;
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+            if (lane == 0) wred[w][k] = x;
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < S * S; k += blockDim.x) {
+            double t = 0.0;
+            for (int ww = 0; ww < NT / 32; ++ww) t += (double)wred[ww][k];
+            epart[(size_t)blockIdx.x * S * S + k] += t;
+        }
+    } else {
+        __syncthreads();
+        for (int k = threadIdx.x; k < S * S; k += blockDim.x) {
+            double t = 0.0;
+            for (int tt = 0; tt < NT; ++tt) t += (double)sacc[k * NT + tt];
+            epart[(size_t)blockIdx.x * S * S + k] += t;
+        }
     }
 }
 
@@ -327,21 +350,19 @@ __global__ void k_u_logsoftmax_bwd(uint32_t V, const float *__restrict__ lb0, co
     stv<S>(theta_bar + (size_t)v * S, gb);
 }
 
-// log_pair_bar[k] = sum of the block partials (fixed order)
+// log_pair_bar[k] = sum of the block partials (fixed order): one block per k
 __global__ void k_u_reduce_pair(const double *__restrict__ epart, uint32_t nblk, uint32_t n, float *__restrict__ out) {
     __shared__ double red[32];
-    for (uint32_t k = 0; k < n; ++k) {
-        double t = 0.0;
-        for (uint32_t b = threadIdx.x; b < nblk; b += blockDim.x) t += epart[(size_t)b * n + k];
-        t = warp_sum(t);
-        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double s = 0.0;
-            for (uint32_t w = 0; w < (blockDim.x >> 5); ++w) s += red[w];
-            out[k] = (float)s;
-        }
-        __syncthreads();
+    const uint32_t k = blockIdx.x;
+    double t = 0.0;
+    for (uint32_t b = threadIdx.x; b < nblk; b += blockDim.x) t += epart[(size_t)b * n + k];
+    t = warp_sum(t);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (uint32_t w = 0; w < (blockDim.x >> 5); ++w) s += red[w];
+        out[k] = (float)s;
     }
 }
 
@@ -401,8 +422,10 @@ static int u_backward(bp_unrolled *u) {
     const UGraph g{u->V, u->K, u->in_ptr, u->in_src, u->out_ptr, u->out_pos, u->pos_tab, u->tables};
     const size_t VS = (size_t)u->V * S;
     const unsigned gv = grid_for(u->V, kUThreads);
+    constexpr int BT = bwd_threads<S>();
+    const unsigned gb = grid_for(u->V, BT);
     cudaStream_t st = u->stream;
-    BP_CUDA(cudaMemsetAsync(u->epart, 0, sizeof(double) * u->nblk * S * S, st));
+    BP_CUDA(cudaMemsetAsync(u->epart, 0, sizeof(double) * gb * S * S, st));
     int bc = 0, rn = 0;
     const float *rb_next = nullptr;   // rbar of iteration t+1 (none at t = T)
     const uint32_t nseg = (u->T + u->ck - 1) / u->ck;
@@ -424,8 +447,8 @@ static int u_backward(bp_unrolled *u) {
             const float *q_next = (t == u->T) ? nullptr
                                   : (t == t_end) ? u->ck_q + (size_t)(s + 1) * VS
                                                  : u->seg_q + (j + 1) * VS;  // lQ_{t+1}
-            k_u_bwd<S><<<gv, kUThreads, 0, st>>>(g, 0, q_t, b_t, u->bbar[bc], q_next, rb_next, u->bbar[bc ^ 1],
-                                                 u->rbar[rn], u->epart);
+            k_u_bwd<S><<<gb, BT, 0, st>>>(g, 0, q_t, b_t, u->bbar[bc], q_next, rb_next, u->bbar[bc ^ 1],
+                                          u->rbar[rn], u->epart);
             bc ^= 1;
             rb_next = u->rbar[rn];
             rn ^= 1;
@@ -434,11 +457,11 @@ static int u_backward(bp_unrolled *u) {
     BP_CUDA(cudaGetLastError());
     // initial step: lQ_1 = lb_0 + sum lm(lb_0); its own x adjoint goes to lb_0
     const float *b0 = u->ck_b, *q1 = u->ck_q;
-    k_u_bwd<S><<<gv, kUThreads, 0, st>>>(g, 1, b0, nullptr, u->bbar[bc], q1, rb_next, u->bbar[bc ^ 1], u->rbar[rn],
-                                         u->epart);
+    k_u_bwd<S><<<gb, BT, 0, st>>>(g, 1, b0, nullptr, u->bbar[bc], q1, rb_next, u->bbar[bc ^ 1], u->rbar[rn],
+                                  u->epart);
     k_u_bwd_src<S><<<gv, kUThreads, 0, st>>>(g, b0, u->rbar[rn], u->bbar[bc ^ 1], u->bbar[bc]);
     k_u_logsoftmax_bwd<S><<<gv, kUThreads, 0, st>>>(u->V, b0, u->bbar[bc], u->gtheta_buf);
-    k_u_reduce_pair<<<1, 256, 0, st>>>(u->epart, u->nblk, u->K * S * S, u->glogp_buf);
+    k_u_reduce_pair<<<u->K * S * S, 256, 0, st>>>(u->epart, gb, u->K * S * S, u->glogp_buf);
     BP_CUDA(cudaGetLastError());
     return BP_OK;
 }
@@ -522,7 +545,7 @@ int bp_unrolled_create(bp_unrolled **out, uint32_t V, uint32_t E, uint32_t S, ui
     std::vector<uint32_t> ofill(out_ptr.begin(), out_ptr.end() - 1);
     for (uint32_t e = 0; e < E; ++e) out_pos[ofill[src[e]]++] = pos_of[e];
     const size_t VS = (size_t)V * S;
-    u->nblk = grid_for(V, kUThreads);
+    u->nblk = grid_for(V, 64);   // partial slots for the smallest backward block
     auto alloc = [&](void **p, size_t bytes) {
         return cudaMalloc(p, bytes ? bytes : 16) == cudaSuccess;
     };

@@ -137,6 +137,11 @@ int bp_set_stream(bp_graph *g, void *stream);
 int bp_synchronize(bp_graph *g);
 /* bytes of device memory the graph holds */
 int bp_graph_device_bytes(const bp_graph *g, uint64_t *bytes);
+/* Graph buffers come from the current device's stream-ordered memory pool,
+ * which this library sets to keep freed memory cached (so graph after graph
+ * reuses it without cudaMalloc/cudaFree); this returns the cached memory to
+ * the driver. */
+int bp_release_cached_memory(void);
 
 /* ---- state ----------------------------------------------------------- */
 int bp_set_beliefs(bp_graph *g, const float *beliefs, uint32_t ld, int memory);
