@@ -79,6 +79,120 @@ __device__ __forceinline__ void stv(float *__restrict__ p, const float *v) {
     }
 }
 
+// ---- loads / stores with an L2 eviction-priority policy ------------------
+// A policy from createpolicy rides on each access (ld/st .L2::cache_hint);
+// it sets the priority of the touched lines only and changes no cache
+// configuration.
+__device__ __forceinline__ uint64_t l2_evict_last_policy() {
+    uint64_t p;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
+template <int N>
+__device__ __forceinline__ void ldv_pol(const float *p, float *o, uint64_t pol) {
+    if constexpr (N % 4 == 0) {
+#pragma unroll
+        for (int k = 0; k < N / 4; ++k)
+            asm("ld.global.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+                         : "=f"(o[4 * k]), "=f"(o[4 * k + 1]), "=f"(o[4 * k + 2]), "=f"(o[4 * k + 3])
+                         : "l"(p + 4 * k), "l"(pol));
+    } else if constexpr (N % 2 == 0) {
+#pragma unroll
+        for (int k = 0; k < N / 2; ++k)
+            asm("ld.global.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;"
+                         : "=f"(o[2 * k]), "=f"(o[2 * k + 1])
+                         : "l"(p + 2 * k), "l"(pol));
+    } else {
+#pragma unroll
+        for (int k = 0; k < N; ++k)
+            asm("ld.global.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(o[k]) : "l"(p + k), "l"(pol));
+    }
+}
+
+template <int N>
+__device__ __forceinline__ void stv_pol(float *p, const float *v, uint64_t pol) {
+    if constexpr (N % 4 == 0) {
+#pragma unroll
+        for (int k = 0; k < N / 4; ++k)
+            asm volatile("st.global.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;"
+                         :: "l"(p + 4 * k), "f"(v[4 * k]), "f"(v[4 * k + 1]), "f"(v[4 * k + 2]),
+                            "f"(v[4 * k + 3]), "l"(pol) : "memory");
+    } else if constexpr (N % 2 == 0) {
+#pragma unroll
+        for (int k = 0; k < N / 2; ++k)
+            asm volatile("st.global.L2::cache_hint.v2.f32 [%0], {%1, %2}, %3;"
+                         :: "l"(p + 2 * k), "f"(v[2 * k]), "f"(v[2 * k + 1]), "l"(pol) : "memory");
+    } else {
+#pragma unroll
+        for (int k = 0; k < N; ++k)
+            asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" :: "l"(p + k), "f"(v[k]), "l"(pol) : "memory");
+    }
+}
+
+// ---- bulk asynchronous copies (global -> shared) and mbarriers -----------
+// cp.async.bulk without multicast: the copy engine moves a contiguous range
+// into this CTA's shared memory and signals the bytes on an mbarrier.
+// Addresses 16-byte aligned, sizes a positive multiple of 16.
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+// make initialised mbarriers visible to the async proxy
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// order this thread's generic-proxy shared-memory accesses before later
+// async-proxy (bulk copy) accesses
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+// one probe of the phase with the given parity (true once it has completed)
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+// bounded wait: false when the phase has not completed within `limit_ns`
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, uint64_t limit_ns) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    while (!mbar_try_wait(bar, parity))
+        if (global_ns() - t0 > limit_ns) return false;
+    return true;
+}
+
 // ---- the send step ---------------------------------------------------------
 // m[i] = sum_j J[i][j] * buf[j] for i < x, j < y (partial sums from 0 in j
 // order), normalised by their sum over i (sum <= 0 replaced by 1):

@@ -28,6 +28,11 @@
 namespace bpx {
 
 constexpr int kMaxStates = BP_MAX_STATES;
+// allocated entries past the ends of in_ptr and belief (nodes) and of in_src
+// and msg (edges): the staged iteration kernel copies whole node tiles and
+// 16-byte-rounded edge ranges
+constexpr uint32_t kArrayPadNodes = 264;
+constexpr uint32_t kArrayPadEdges = 8;
 
 // Control block of one loopy run, resident in device memory.  Kernels read it
 // at entry (iteration index, buffer parities, stop flag) and the last block
@@ -35,7 +40,7 @@ constexpr int kMaxStates = BP_MAX_STATES;
 // the whole loop with the reference's stopping rule evaluated on the device.
 struct LoopyCtl {
     uint32_t it;           // iterations executed so far in this run
-    uint32_t done;         // 0 running, 1 stopping rule fired, 2 ran out of iterations
+    uint32_t done;         // 0 running, 1 stopping rule fired, 2 ran out of iterations, 3 a device wait timed out
     uint32_t ret;          // the reference's return value
     uint32_t counter;      // last-block-done ticket
     uint32_t num_iter;     // _acc variants: completed batches * check_every
@@ -79,6 +84,8 @@ struct bp_graph {
     // node renumbering (BP_GRAPH_REORDER_BY_OUT_DEGREE): internal id i holds the
     // caller's node new_to_old[i]; null when ids are the caller's
     uint32_t *new_to_old = nullptr;
+    // renumbered graphs: internal ids below this have two or more out-edges
+    uint32_t reuse_nodes = 0;
     uint8_t *pos_dims = nullptr, *node_s = nullptr;
     float *joint = nullptr;
     float *belief = nullptr;
@@ -131,6 +138,10 @@ int cuda_fail(cudaError_t e, const char *what, const char *file, int line);
     } while (0)
 
 int dev_alloc(bp_graph *g, void **p, size_t bytes);
+// tree schedule (tree.cu, levels_gpu.cu)
+void tree_clear(bp_graph *g);
+int tree_prepare_host(bp_graph *g, const uint32_t *levels, uint32_t num_levels);
+int tree_build_levels_gpu(bp_graph *g, uint32_t *levels, uint32_t *num_levels);
 int ensure_staging(bp_graph *g, size_t bytes);
 int ensure_out_csr(bp_graph *g);
 int ensure_host_in_ptr(bp_graph *g);

@@ -208,6 +208,18 @@ __global__ void k_degree_keys(uint32_t *__restrict__ deg, uint32_t V, uint32_t *
     iota[v] = (uint32_t)v;
 }
 
+// number of sorted keys (0xffffffff - out-degree, ascending) of nodes with
+// out-degree >= 2
+__global__ void k_count_reused(const uint32_t *__restrict__ keys, uint32_t V, uint32_t *__restrict__ out) {
+    uint32_t lo = 0, hi = V;
+    while (lo < hi) {
+        const uint32_t mid = lo + (hi - lo) / 2;
+        if (keys[mid] <= 0xffffffffu - 2u) lo = mid + 1;
+        else hi = mid;
+    }
+    *out = lo;
+}
+
 __global__ void k_invert_perm(const uint32_t *__restrict__ new_to_old, uint32_t V, uint32_t *__restrict__ old_to_new) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < V) old_to_new[new_to_old[i]] = (uint32_t)i;
@@ -464,16 +476,18 @@ static int create_impl(bp_graph *g, const bp_graph_desc *d) {
 
     // ---- device arrays
     const size_t ms = g->ms;
-    if ((st = dev_alloc(g, (void **)&g->in_ptr, sizeof(uint32_t) * ((size_t)V + 1)))) return st;
-    if ((st = dev_alloc(g, (void **)&g->in_src, sizeof(uint32_t) * (size_t)E))) return st;
+    // padding past the ends: the staged iteration kernel copies whole
+    // 16-byte-aligned ranges and whole node tiles (loopy.cu, k_flood_staged)
+    if ((st = dev_alloc(g, (void **)&g->in_ptr, sizeof(uint32_t) * ((size_t)V + 1 + kArrayPadNodes)))) return st;
+    if ((st = dev_alloc(g, (void **)&g->in_src, sizeof(uint32_t) * ((size_t)E + kArrayPadEdges)))) return st;
     if ((st = dev_alloc(g, (void **)&g->pos_edge, sizeof(uint32_t) * (size_t)E))) return st;
     if ((st = dev_alloc(g, (void **)&g->edge_pos, sizeof(uint32_t) * (size_t)E))) return st;
     if ((st = dev_alloc(g, (void **)&g->node_s, (size_t)V))) return st;
     if (!g->uniform && (st = dev_alloc(g, (void **)&g->pos_dims, (size_t)E))) return st;
     if ((st = dev_alloc(g, (void **)&g->joint, sizeof(float) * ms * ms * (size_t)E))) return st;
-    if ((st = dev_alloc(g, (void **)&g->belief, sizeof(float) * ms * (size_t)V))) return st;
+    if ((st = dev_alloc(g, (void **)&g->belief, sizeof(float) * ms * ((size_t)V + kArrayPadNodes)))) return st;
     for (int k = 0; k < 2; ++k) {
-        if ((st = dev_alloc(g, (void **)&g->msg[k], sizeof(float) * ms * (size_t)E))) return st;
+        if ((st = dev_alloc(g, (void **)&g->msg[k], sizeof(float) * ms * ((size_t)E + kArrayPadEdges)))) return st;
         if ((st = dev_alloc(g, (void **)&g->q[k], sizeof(float) * ms * (size_t)V))) return st;
         BP_CUDA(cudaMemsetAsync(g->msg[k], 0, sizeof(float) * ms * (size_t)E, g->stream));
         BP_CUDA(cudaMemsetAsync(g->q[k], 0, sizeof(float) * ms * (size_t)V, g->stream));
@@ -576,6 +590,8 @@ static int create_impl(bp_graph *g, const bp_graph_desc *d) {
             cudaFreeAsync(tmp, g->stream);
             if (se != cudaSuccess) return cuda_fail(se, "DeviceRadixSort::SortPairs", __FILE__, __LINE__);
             k_invert_perm<<<grid_for(V, 256), 256, 0, g->stream>>>(g->new_to_old, V, old_to_new);
+            k_count_reused<<<1, 1, 0, g->stream>>>(keys, V, deg);
+            BP_CUDA(cudaMemcpyAsync(&g->reuse_nodes, deg, sizeof(uint32_t), cudaMemcpyDeviceToHost, g->stream));
         }
         uint32_t *src2 = nullptr, *dst2 = nullptr;
         BP_CUDA(cudaMallocAsync((void **)&src2, sizeof(uint32_t) * (E ? E : 1), g->stream));

@@ -44,6 +44,10 @@ template <int MS, int FU> constexpr int flood_min_blocks() { return MS <= 2 && F
 
 struct FloodArgs {
     uint32_t V;
+    // send-buffer entries of nodes below this id are gathered and written
+    // with an L2 evict-last policy (renumbered graphs: the nodes with the
+    // most out-edges, i.e. the most re-read entries); 0 = none
+    uint32_t hot;
     const uint32_t *in_ptr, *in_src, *pos_edge;
     const uint8_t *node_s, *pos_dims;
     const float *joint;
@@ -146,6 +150,7 @@ __global__ void __launch_bounds__(flood_nt<MS>(), flood_min_blocks<MS, FU>()) k_
     float *__restrict__ m_new = mp ? a.msg0 : a.msg1;
     const float *__restrict__ q_in = qp ? a.q1 : a.q0;
     float *__restrict__ q_out = qp ? a.q0 : a.q1;
+    const uint64_t keep = l2_evict_last_policy();
 
     const uint32_t V = a.V, tid = threadIdx.x, v0 = blockIdx.x * NT;
     const uint32_t vend = min(v0 + NT, V);
@@ -192,7 +197,10 @@ __global__ void __launch_bounds__(flood_nt<MS>(), flood_min_blocks<MS, FU>()) k_
             }
 #pragma unroll
             for (int u = 0; u < FU; ++u)
-                if (pb + u * NT < c1) ldv<MS>(q_in + (size_t)src[u] * MS, q[u]);
+                if (pb + u * NT < c1) {
+                    if (src[u] < a.hot) ldv_pol<MS>(q_in + (size_t)src[u] * MS, q[u], keep);
+                    else ldv<MS>(q_in + (size_t)src[u] * MS, q[u]);
+                }
 #pragma unroll
             for (int u = 0; u < FU; ++u) {
                 const uint32_t p = pb + u * NT;
@@ -260,10 +268,268 @@ __global__ void __launch_bounds__(flood_nt<MS>(), flood_min_blocks<MS, FU>()) k_
                 combine<MS, UNI>(qo, mm, S);
             }
         }
-        stv<MS>(q_out + (size_t)v * MS, qo);
+        if (v < a.hot) stv_pol<MS>(q_out + (size_t)v * MS, qo, keep);
+        else stv<MS>(q_out + (size_t)v * MS, qo);
     }
 
     if (!serial) reduce_and_finalize<NT>(ctl, a.partials, dsum, want, red, &s_last);
+}
+
+// Staged form of k_flood for uniform 2-state graphs (the layout is written
+// for 2 or 4 states; 4-state tables do not leave room for two stages of a
+// 256-node tile).  A persistent
+// grid walks the 256-node tiles round-robin (tile = blockIdx.x + k*gridDim.x,
+// a fixed assignment, so the delta sums in a fixed order).  For each tile one
+// thread issues bulk asynchronous copies (cp.async.bulk, no multicast) of the
+// tile's contiguous streams -- row pointers, beliefs, source ids, tables and
+// the previous messages -- into a ring of shared-memory stages, ST tiles
+// ahead of the tile being computed, each stage completing on its mbarrier.
+// The threads then only gather Q[src] (the one random access) and do the
+// arithmetic, in the order and rounding of k_flood.  A tile whose in-edges
+// do not fit a stage (more than CAP) is computed from global memory in
+// CAP-edge chunks, as k_flood does.
+//
+// Bulk copies need 16-byte aligned ranges: each stream is copied from its
+// first element rounded down to a 16-byte boundary and for a length rounded
+// up, so the graph's arrays carry padding past their ends (engine.cu,
+// kArrayPadNodes / kArrayPadEdges).
+constexpr uint32_t kStagedTN = 256;      // nodes per tile = threads per CTA
+constexpr uint64_t kWaitNs = 2000000000ull;  // bound on one stage wait: 2 s
+
+__host__ __device__ constexpr uint32_t round16(uint32_t b) { return (b + 15u) & ~15u; }
+
+template <int MS>
+struct Staged {
+    static constexpr uint32_t TN = kStagedTN;
+    static constexpr uint32_t CAP = MS <= 2 ? 1536 : 768;   // in-edges per stage
+    static constexpr int ST = 2;                            // stages
+    static constexpr int FU = MS <= 2 ? 4 : 2;              // gathers in flight per thread
+    static constexpr uint32_t EPM = 16 / (MS * 4);          // edges per 16 B of messages
+    // stage layout (byte offsets, each a multiple of 16)
+    static constexpr uint32_t SRC = 0;                                  // CAP + 8 u32
+    static constexpr uint32_t JNT = SRC + (CAP + 8) * 4;                // CAP tables
+    static constexpr uint32_t MOLD = JNT + CAP * MS * MS * 4;           // CAP + 2*EPM messages
+    static constexpr uint32_t PTR = MOLD + round16((CAP + 2 * EPM) * MS * 4);  // TN + 4 u32
+    static constexpr uint32_t BEL = PTR + (TN + 4) * 4;                 // TN beliefs
+    static constexpr uint32_t STAGE = round16(BEL + TN * MS * 4);
+    // after the stages: the tile's new messages, then the mbarriers
+    static constexpr uint32_t MSG = ST * STAGE;
+    static constexpr uint32_t BAR = MSG + round16(CAP * MS * 4);
+    static constexpr uint32_t SMEM = BAR + 16 * ST;
+    static_assert(MS == 2 || MS == 4, "staged tiles: 2 or 4 states");
+    static_assert(CAP % 4 == 0 && TN % 4 == 0, "16-byte aligned stage sections");
+};
+
+// issue the copies of `tile` into stage `st` (one thread); the byte count the
+// mbarrier expects is the sum of exactly the copies issued
+template <int MS>
+__device__ void staged_issue(const FloodArgs &a, const float *m_old, bool want, uint32_t tile, unsigned char *st,
+                             uint64_t *bar) {
+    using C = Staged<MS>;
+    const uint32_t v0 = tile * C::TN, v1 = min(v0 + C::TN, a.V);
+    const uint32_t e0 = a.in_ptr[v0], e1 = a.in_ptr[v1];
+    const uint32_t b_ptr = (C::TN + 4) * 4, b_bel = C::TN * MS * 4;
+    uint32_t b_src = 0, b_j = 0, b_m = 0, a4 = 0, am = 0;
+    if (e1 > e0 && e1 - e0 <= C::CAP) {
+        a4 = e0 & ~3u;
+        b_src = ((e1 - a4 + 3u) & ~3u) * 4;
+        b_j = (e1 - e0) * MS * MS * 4;
+        if (want) {
+            am = e0 & ~(C::EPM - 1);
+            b_m = ((e1 - am + C::EPM - 1) & ~(C::EPM - 1)) * MS * 4;
+        }
+    }
+    mbar_arrive_expect_tx(bar, b_ptr + b_bel + b_src + b_j + b_m);
+    bulk_g2s(st + C::PTR, a.in_ptr + v0, b_ptr, bar);
+    bulk_g2s(st + C::BEL, a.belief + (size_t)v0 * MS, b_bel, bar);
+    if (b_src) bulk_g2s(st + C::SRC, a.in_src + a4, b_src, bar);
+    if (b_j) bulk_g2s(st + C::JNT, a.joint + (size_t)e0 * (MS * MS), b_j, bar);
+    if (b_m) bulk_g2s(st + C::MOLD, m_old + (size_t)am * MS, b_m, bar);
+}
+
+template <int MS>
+__global__ void __launch_bounds__(kStagedTN) k_flood_staged(const FloodArgs a, uint32_t ntiles) {
+    using C = Staged<MS>;
+    constexpr uint32_t NT = C::TN;
+    constexpr int FU = C::FU;
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ double red[NT / 32];
+    __shared__ bool s_last;
+    __shared__ uint32_t s_err;
+
+    LoopyCtl *ctl = a.ctl;
+    if (*(volatile uint32_t *)&ctl->done) return;
+    const uint32_t it = ctl->it, ce = ctl->check_every;
+    const bool want = (ce <= 1) || ((it + 1) % ce == 0);
+    const int mp = (int)((ctl->msg_parity0 + it) & 1u), qp = (int)((ctl->q_parity0 + it) & 1u);
+    const float *__restrict__ m_old = mp ? a.msg1 : a.msg0;
+    float *__restrict__ m_new = mp ? a.msg0 : a.msg1;
+    const float *__restrict__ q_in = qp ? a.q1 : a.q0;
+    float *__restrict__ q_out = qp ? a.q0 : a.q1;
+    const uint64_t keep = l2_evict_last_policy();
+    const uint32_t tid = threadIdx.x;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + C::BAR);
+    float *msg_s = reinterpret_cast<float *>(smem + C::MSG);
+
+    if (tid == 0) {
+        s_err = 0;
+        for (int i = 0; i < C::ST; ++i) mbar_init(bars + i, 1);
+        fence_mbar_init();
+        for (int i = 0; i < C::ST; ++i) {
+            const uint32_t t = blockIdx.x + (uint32_t)i * gridDim.x;
+            if (t < ntiles) staged_issue<MS>(a, m_old, want, t, smem + i * C::STAGE, bars + i);
+        }
+    }
+    __syncthreads();
+
+    double dsum = 0.0;
+    uint32_t k = 0;
+    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++k) {
+        const int si = (int)(k % C::ST);
+        const uint32_t par = (k / C::ST) & 1u;
+        unsigned char *st = smem + si * C::STAGE;
+        if (tid == 0 && !mbar_wait_bounded(bars + si, par, kWaitNs)) s_err = 1;
+        __syncthreads();
+        if (s_err) break;
+        mbar_try_wait(bars + si, par);   // completed: orders this thread's reads after the copies
+
+        const uint32_t *ptr_s = reinterpret_cast<const uint32_t *>(st + C::PTR);
+        const uint32_t v0 = tile * NT, n = min(NT, a.V - v0);
+        const uint32_t e0 = ptr_s[0], e1 = ptr_s[n];
+        const bool staged = e1 - e0 <= C::CAP;
+        const uint32_t v = v0 + tid;
+        const bool has = tid < n;
+        uint32_t r0 = 0, r1 = 0;
+        if (has) {
+            r0 = ptr_s[tid];
+            r1 = ptr_s[tid + 1];
+        }
+        float prod[MS];
+#pragma unroll
+        for (int i = 0; i < MS; ++i) prod[i] = 1.0f;
+
+        for (uint32_t c0 = e0; c0 < e1; c0 += C::CAP) {
+            const uint32_t c1 = min(e1, c0 + C::CAP);
+            if (staged) {
+                const uint32_t *src_s = reinterpret_cast<const uint32_t *>(st + C::SRC) - (e0 & ~3u);
+                const float *j_s = reinterpret_cast<const float *>(st + C::JNT) - (size_t)e0 * (MS * MS);
+                const float *mo_s = reinterpret_cast<const float *>(st + C::MOLD) - (size_t)(e0 & ~(C::EPM - 1)) * MS;
+                for (uint32_t pb = c0 + tid; pb < c1; pb += NT * FU) {
+                    float q[FU][MS];
+#pragma unroll
+                    for (int u = 0; u < FU; ++u) {
+                        const uint32_t p = pb + u * NT;
+                        if (p < c1) {
+                            const uint32_t sv = src_s[p];
+                            if (sv < a.hot) ldv_pol<MS>(q_in + (size_t)sv * MS, q[u], keep);
+                            else ldv<MS>(q_in + (size_t)sv * MS, q[u]);
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < FU; ++u) {
+                        const uint32_t p = pb + u * NT;
+                        if (p >= c1) break;
+                        float jt[MS * MS], m[MS];
+                        ldv<MS * MS>(j_s + (size_t)p * (MS * MS), jt);
+                        send_msg_regs<MS, true>(jt, q[u], MS, MS, m);
+                        if (want) {
+                            float o[MS];
+                            ldv<MS>(mo_s + (size_t)p * MS, o);
+#pragma unroll
+                            for (int kk = 0; kk < MS; ++kk) {
+                                float d = FSUB(o[kk], m[kk]);
+                                if (d != d) d = 0.0f;
+                                dsum += (double)fabsf(d);
+                            }
+                        }
+                        stv<MS, kStream>(m_new + (size_t)p * MS, m);
+                        stv<MS>(msg_s + (size_t)(p - c0) * MS, m);
+                    }
+                }
+            } else {
+                for (uint32_t p = c0 + tid; p < c1; p += NT) {
+                    const uint32_t sv = __ldcs(a.in_src + p);
+                    float q[MS], m[MS];
+                    if (sv < a.hot) ldv_pol<MS>(q_in + (size_t)sv * MS, q, keep);
+                    else ldv<MS>(q_in + (size_t)sv * MS, q);
+                    send_msg<MS, true>(a.joint + (size_t)p * (MS * MS), q, MS, MS, m);
+                    if (want) {
+                        float o[MS];
+                        ldv<MS, kStream>(m_old + (size_t)p * MS, o);
+#pragma unroll
+                        for (int kk = 0; kk < MS; ++kk) {
+                            float d = FSUB(o[kk], m[kk]);
+                            if (d != d) d = 0.0f;
+                            dsum += (double)fabsf(d);
+                        }
+                    }
+                    stv<MS, kStream>(m_new + (size_t)p * MS, m);
+                    stv<MS>(msg_s + (size_t)(p - c0) * MS, m);
+                }
+            }
+            __syncthreads();
+            if (has) {
+                const uint32_t lo = max(r0, c0), hi = min(r1, c1);
+                for (uint32_t p = lo; p < hi; ++p) {
+                    float mm[MS];
+                    ldv<MS>(msg_s + (size_t)(p - c0) * MS, mm);
+                    combine<MS, true>(prod, mm, MS);
+                }
+            }
+            __syncthreads();
+        }
+
+        if (has) {
+            float b[MS];
+            ldv<MS>(reinterpret_cast<const float *>(st + C::BEL) + (size_t)tid * MS, b);
+            if (r1 > r0) {
+#pragma unroll
+                for (int i = 0; i < MS; ++i) b[i] = FMUL(b[i], prod[i]);
+            }
+            normalise<MS, true>(b, MS);
+            stv<MS, kStream>(a.belief + (size_t)v * MS, b);
+            float qo[MS];
+#pragma unroll
+            for (int i = 0; i < MS; ++i) qo[i] = b[i];
+            if (staged) {
+                for (uint32_t p = r0; p < r1; ++p) {
+                    float mm[MS];
+                    ldv<MS>(msg_s + (size_t)(p - e0) * MS, mm);
+                    combine<MS, true>(qo, mm, MS);
+                }
+            } else {
+                for (uint32_t p = r0; p < r1; ++p) {
+                    float mm[MS];
+                    ldv<MS>(m_new + (size_t)p * MS, mm);
+                    combine<MS, true>(qo, mm, MS);
+                }
+            }
+            if (v < a.hot) stv_pol<MS>(q_out + (size_t)v * MS, qo, keep);
+            else stv<MS>(q_out + (size_t)v * MS, qo);
+        }
+        // every thread is done with the stage and the message buffer; the
+        // stage takes the tile ST ahead
+        fence_proxy_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            const uint32_t nt = tile + (uint32_t)C::ST * gridDim.x;
+            if (nt < ntiles) staged_issue<MS>(a, m_old, want, nt, st, bars + si);
+        }
+    }
+
+    if (s_err) {
+        // a stage never completed: report it, wait (bounded) for the copies
+        // still in flight into this CTA's stages, and leave the grid
+        if (tid == 0) {
+            atomicExch(&ctl->done, 3u);
+            for (uint32_t j = 0; j < (uint32_t)C::ST; ++j) {
+                const uint32_t kk = k + j, t = blockIdx.x + kk * gridDim.x;
+                if (t < ntiles) mbar_wait_bounded(bars + (kk % C::ST), (kk / C::ST) & 1u, kWaitNs);
+            }
+        }
+        return;
+    }
+    reduce_and_finalize<NT>(ctl, a.partials, dsum, want, red, &s_last);
 }
 
 // Warp-tiled form of k_flood: each warp owns 32 consecutive destination
@@ -733,9 +999,20 @@ static int launch_gather(bp_graph *g) {
     return BP_OK;
 }
 
+// nodes whose send-buffer entries get the evict-last policy: the renumbered
+// nodes with two or more out-edges, at most BP_FLOOD_HOT_MB (default 48) MB
+// of send buffer
+static uint32_t flood_hot_nodes(const bp_graph *g) {
+    size_t mb = 48;
+    if (const char *env = getenv("BP_FLOOD_HOT_MB")) mb = (size_t)atol(env);
+    const size_t cap = (mb << 20) / (sizeof(float) * g->ms);
+    return (uint32_t)std::min<size_t>(g->reuse_nodes, cap);
+}
+
 static FloodArgs flood_args(bp_graph *g) {
     FloodArgs a;
     a.V = g->V;
+    a.hot = flood_hot_nodes(g);
     a.in_ptr = g->in_ptr;
     a.in_src = g->in_src;
     a.pos_edge = g->pos_edge;
@@ -776,9 +1053,48 @@ static EdgeArgs edge_args(bp_graph *g) {
     return a;
 }
 
+// staged kernel: dynamic shared memory opt-in (once per process) and the
+// persistent grid (resident CTAs per SM x SMs, at most one CTA per tile)
+template <int MS>
+static int staged_grid(const bp_graph *g, unsigned *grid, uint32_t *ntiles) {
+    using C = Staged<MS>;
+    static int bps = 0;
+    static std::mutex mu;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (bps == 0) {
+            BP_CUDA(cudaFuncSetAttribute(k_flood_staged<MS>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM));
+            BP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_flood_staged<MS>, C::TN, C::SMEM));
+            if (bps < 1) return set_error(BP_ERR_CUDA, "staged iteration kernel does not fit an SM");
+        }
+    }
+    int dev = 0, sms = 0;
+    BP_CUDA(cudaGetDevice(&dev));
+    BP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    *ntiles = (g->V + C::TN - 1) / C::TN;
+    *grid = (unsigned)std::min<uint64_t>(*ntiles, (uint64_t)bps * sms);
+    return BP_OK;
+}
+
 template <int MS, bool UNI>
 static int enqueue_node_iterations(bp_graph *g, uint32_t k, bool serial, int variant) {
     constexpr int NT = flood_nt<MS>();
+    if (variant == BP_KERNEL_STAGED_TILE) {
+        if constexpr (UNI && MS == 2) {
+            unsigned grid = 0;
+            uint32_t ntiles = 0;
+            int st = staged_grid<MS>(g, &grid, &ntiles);
+            if (st) return st;
+            const FloodArgs a = flood_args(g);
+            for (uint32_t i = 0; i < k; ++i) {
+                k_flood_staged<MS><<<grid, Staged<MS>::TN, Staged<MS>::SMEM, g->stream>>>(a, ntiles);
+                BP_CUDA(cudaGetLastError());
+            }
+            return BP_OK;
+        } else {
+            return set_error(BP_ERR_INVALID, "staged tiles need a uniform 2-state graph");
+        }
+    }
     const bool warp_tiled = variant != BP_KERNEL_BLOCK_TILE;
     const unsigned grid = warp_tiled ? grid_for(g->V, 256) : grid_for(g->V, NT);
     const FloodArgs a = flood_args(g);
@@ -840,9 +1156,28 @@ static int enqueue_iterations(bp_graph *g, int schedule, uint32_t k, bool serial
     BP_DISPATCH_MS(g->ms, g->uniform != 0, enqueue_edge_iterations, g, k, serial, variant);
 }
 
-static int flood_grid(bp_graph *g, int variant) {
+static int flood_grid(bp_graph *g, int variant, uint32_t *grid) {
+    if (variant == BP_KERNEL_STAGED_TILE) {
+        uint32_t ntiles = 0;
+        unsigned gr = 0;
+        int st = staged_grid<2>(g, &gr, &ntiles);
+        *grid = gr;
+        return st;
+    }
     const int nt = (variant != BP_KERNEL_BLOCK_TILE || g->ms <= 4) ? 256 : 128;
-    return (int)grid_for(g->V, nt);
+    *grid = grid_for(g->V, nt);
+    return BP_OK;
+}
+
+// the staged kernel applies to uniform 2-state graphs on the node schedule
+// with the f64 delta, whose arrays are 16-byte aligned and whose mean
+// in-degree leaves the typical tile inside a stage (<= 3/4 of CAP edges)
+static bool staged_applies(const bp_graph *g, int schedule, bool serial) {
+    if (schedule != BP_SCHEDULE_NODE || serial || g->uniform != 2) return false;
+    if ((uint64_t)g->E * Staged<2>::TN > (uint64_t)g->V * (Staged<2>::CAP * 3 / 4)) return false;
+    const uintptr_t any = (uintptr_t)g->in_ptr | (uintptr_t)g->in_src | (uintptr_t)g->joint |
+                          (uintptr_t)g->belief | (uintptr_t)g->msg[0] | (uintptr_t)g->msg[1];
+    return (any & 15u) == 0;
 }
 
 }  // namespace bpx
@@ -920,12 +1255,16 @@ int bp_loopy(bp_graph *g, const bp_loopy_options *opt, bp_loopy_result *res) {
     int variant = opt->kernel_variant;
     if (variant == BP_KERNEL_AUTO) {
         const char *env = getenv("BP_FLOOD_KERNEL");
-        variant = (env && env[0] == 'w') ? BP_KERNEL_WARP_TILE : BP_KERNEL_BLOCK_TILE;
+        if (env && env[0] == 'w') variant = BP_KERNEL_WARP_TILE;
+        else if (env && env[0] == 'b') variant = BP_KERNEL_BLOCK_TILE;
+        else variant = staged_applies(g, opt->schedule, serial) ? BP_KERNEL_STAGED_TILE : BP_KERNEL_BLOCK_TILE;
     }
-    if (variant != BP_KERNEL_BLOCK_TILE && variant != BP_KERNEL_WARP_TILE)
+    if (variant != BP_KERNEL_BLOCK_TILE && variant != BP_KERNEL_WARP_TILE && variant != BP_KERNEL_STAGED_TILE)
         return set_error(BP_ERR_INVALID, "unknown kernel variant %d", opt->kernel_variant);
-    const uint32_t grid_blocks = opt->schedule == BP_SCHEDULE_NODE ? (uint32_t)flood_grid(g, variant)
-                                                                   : grid_for(g->E, 256);
+    if (variant == BP_KERNEL_STAGED_TILE && opt->schedule == BP_SCHEDULE_NODE && !staged_applies(g, opt->schedule, serial))
+        return set_error(BP_ERR_INVALID, "staged tiles need a uniform 2-state graph of mean in-degree <= 4.5 and the f64 delta");
+    uint32_t grid_blocks = grid_for(g->E, 256);
+    if (opt->schedule == BP_SCHEDULE_NODE && (st = flood_grid(g, variant, &grid_blocks))) return st;
     if ((st = ensure_partials(g, grid_blocks))) return st;
     if (serial && (st = ensure_absdiff(g))) return st;
     if (opt->schedule == BP_SCHEDULE_EDGE && (st = ensure_runs(g))) return st;
@@ -998,6 +1337,7 @@ int bp_loopy(bp_graph *g, const bp_loopy_options *opt, bp_loopy_result *res) {
     BP_CUDA(cudaMemcpyAsync(g->ctl_host, g->ctl, sizeof(LoopyCtl), cudaMemcpyDeviceToHost, g->stream));
     BP_CUDA(cudaStreamSynchronize(g->stream));
     c = *g->ctl_host;
+    if (c.done == 3) return set_error(BP_ERR_TIMEOUT, "a bounded device wait of the iteration kernel timed out");
     if (!c.done) return set_error(BP_ERR_STATE, "loop ended without a stop decision (it=%u)", c.it);
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, g->ev0, g->ev1);

@@ -111,7 +111,7 @@ __global__ void k_tree_marginalize(uint32_t V, const uint32_t *__restrict__ in_p
     stv<MS>(belief + (size_t)v * MS, b);
 }
 
-static void tree_clear(bp_graph *g) {
+void tree_clear(bp_graph *g) {
     TreeData &t = g->tree;
     if (t.d_node_level) cudaFree(t.d_node_level);
     if (t.d_node_lidx) cudaFree(t.d_node_lidx);
@@ -122,12 +122,13 @@ static void tree_clear(bp_graph *g) {
     t = TreeData();
 }
 
-static int tree_prepare(bp_graph *g, const uint32_t *levels, uint32_t num_levels) {
+// waves of caller-given (or host-built) level lists, split on the host
+int tree_prepare_host(bp_graph *g, const uint32_t *levels, uint32_t num_levels) {
     const uint32_t V = g->V;
     if (g->new_to_old) return set_error(BP_ERR_STATE, "tree BP on a renumbered graph (BP_GRAPH_REORDER_BY_OUT_DEGREE)");
     TreeData &t = g->tree;
     if (t.ready && t.num_levels == num_levels &&
-        (V == 0 || memcmp(t.levels_host, levels, sizeof(uint32_t) * 2 * (size_t)V) == 0))
+        (V == 0 || (t.levels_host && memcmp(t.levels_host, levels, sizeof(uint32_t) * 2 * (size_t)V) == 0)))
         return BP_OK;
     tree_clear(g);
     if (num_levels == 0) return set_error(BP_ERR_STATE, "no levels (call init_levels_to_nodes first)");
@@ -222,6 +223,11 @@ int bp_tree_build_levels(bp_graph *g, uint32_t *levels, uint32_t *num_levels) {
     if (!g || !num_levels) return set_error(BP_ERR_INVALID, "null argument");
     if (g->new_to_old) return set_error(BP_ERR_STATE, "tree BP on a renumbered graph (BP_GRAPH_REORDER_BY_OUT_DEGREE)");
     int st;
+    // the device build; BP_TREE_LEVELS=host, or a caller's non-zero level
+    // count to continue from (the reference never resets num_levels), takes
+    // the host build
+    const char *env = getenv("BP_TREE_LEVELS");
+    if (*num_levels == 0 && !(env && env[0] == 'h')) return tree_build_levels_gpu(g, levels, num_levels);
     if ((st = ensure_out_csr(g))) return st;
     if ((st = ensure_host_in_ptr(g))) return st;
     const uint32_t V = g->V, E = g->E;
@@ -235,12 +241,12 @@ int bp_tree_build_levels(bp_graph *g, uint32_t *levels, uint32_t *num_levels) {
     if (rc == -1) return set_error(BP_ERR_GRAPH, "a node is unreachable from the in-degree<=2 seed set");
     *num_levels = nl;
     if (levels) memcpy(levels, lv.data(), sizeof(uint32_t) * 2 * (size_t)V);
-    return tree_prepare(g, lv.data(), nl);
+    return tree_prepare_host(g, lv.data(), nl);
 }
 
 int bp_tree_set_levels(bp_graph *g, const uint32_t *levels, uint32_t num_levels) {
     if (!g || (!levels && g->V)) return set_error(BP_ERR_INVALID, "null argument");
-    return tree_prepare(g, levels, num_levels);
+    return tree_prepare_host(g, levels, num_levels);
 }
 
 int bp_tree_start(bp_graph *g) {

@@ -21,10 +21,14 @@
 //   lbbar_{t-1} = abar;  lPbar = abar + lQbar_{t+1};  lmbar_e = lPbar (every in-edge)
 //   rbar = lmbar - m * sum(lmbar)  (m = exp lm);   w_ij = exp(logJ_ij + x_j - r_i)
 //   xbar_src[j] += sum_i rbar_i w_ij;   logJbar_ij += rbar_i w_ij
-// and finally theta_bar = lbbar_0 - softmax(theta) * sum(lbbar_0).  The
-// x_src adjoint is a gather over the source-sorted edge list (w recomputed
-// from the source's own state), so no atomics and the result is
-// deterministic.
+// and finally theta_bar = lbbar_0 - softmax(theta) * sum(lbbar_0).
+// With e_j = exp(x_j - mx) and s_i = sum_j J_ij e_j (J = exp logJ), the max
+// cancels: lm_i = log s_i - log sum_k s_k, m_i = s_i / sum_k s_k and
+// w_ij = J_ij e_j / s_i, so an edge costs S exponentials in either pass.
+// The destination's in-edge loop, which holds e and s of the edge's
+// source, writes the edge's x_src adjoint term c_j = sum_i rbar_i w_ij into
+// the edge's slot of the source-sorted order; the source then sums its
+// contiguous slots.  No atomics, and the result is deterministic.
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -44,13 +48,19 @@ constexpr uint32_t kUMaxTables = 16;
 // registers for S <= 4, else in a shared-memory slice per thread (entry-major,
 // so a warp's adds hit 32 different banks) with smaller blocks
 template <int S> constexpr int bwd_threads() { return S <= 4 ? 256 : 64; }
+// resident blocks per SM the adjoint kernel's register allocation must allow
+template <int S> constexpr int bwd_min_blocks() { return S <= 4 ? 3 : (S <= 8 ? 8 : 4); }
 
 struct UGraph {
     uint32_t V, K;
-    const uint32_t *in_ptr, *in_src, *out_ptr, *out_pos;
+    const uint32_t *in_ptr, *in_src, *out_ptr;
+    const uint32_t *pos_out;   // slot in the source-sorted order of the edge at position p
     const uint8_t *pos_tab;
     const float *tables;   // [K][S][S] = log_pair (log joint tables)
 };
+
+// in-edges whose loads one thread issues together
+template <int S> constexpr int u_batch() { return S <= 4 ? 4 : 2; }
 
 template <int S>
 __device__ __forceinline__ void load_tables_smem(const UGraph &g, float *sm) {
@@ -104,17 +114,57 @@ __device__ __forceinline__ void row_sums(const float *J, const float *e, float *
     }
 }
 
-// log-message: r_i = LSE_j(logJ_ij + x_j) = mx + log s_i, lm = r - LSE(r)
+// message of one edge in linear form: e = exp(x - max x), row sums s of
+// J e (s_i > 0); returns sum_i s_i.  lm_i = log s_i - log sum, m_i = s_i / sum.
 template <int S>
-__device__ __forceinline__ void log_msg(const float *J, const float *x, float *e, float *sr, float *lm) {
-    const float mx = shifted_exp<S>(x, e);
+__device__ __forceinline__ float msg_sums(const float *J, const float *x, float *e, float *sr) {
+    shifted_exp<S>(x, e);
     row_sums<S>(J, e, sr);
-    float r[S];
+    float z = 0.0f;
 #pragma unroll
-    for (int i = 0; i < S; ++i) r[i] = mx + logf(sr[i]);
-    const float z = lse<S>(r);
+    for (int i = 0; i < S; ++i) z += sr[i];
+    return z;
+}
+
+// P += lm over the in-edges [r0, r1) of a node, messages from the log-states
+// `send`; loads of a batch of edges are issued before the first use
+template <int S>
+__device__ __forceinline__ void sum_log_msgs(const UGraph &g, const float *sm, const float *__restrict__ send,
+                                             uint32_t r0, uint32_t r1, float *P) {
+    constexpr int B = u_batch<S>();
+    for (uint32_t p0 = r0; p0 < r1; p0 += B) {
+        uint32_t src[B];
+        uint8_t tb[B];
+        float x[B][S];
 #pragma unroll
-    for (int i = 0; i < S; ++i) lm[i] = r[i] - z;
+        for (int b = 0; b < B; ++b)
+            if (p0 + b < r1) {
+                src[b] = g.in_src[p0 + b];
+                tb[b] = g.pos_tab[p0 + b];
+            }
+#pragma unroll
+        for (int b = 0; b < B; ++b)
+            if (p0 + b < r1) ldv<S>(send + (size_t)src[b] * S, x[b]);
+#pragma unroll
+        for (int b = 0; b < B; ++b) {
+            if (p0 + b >= r1) break;
+            float e[S], sr[S];
+            const float z = logf(msg_sums<S>(edge_table<S>(sm, tb[b]), x[b], e, sr));
+#pragma unroll
+            for (int i = 0; i < S; ++i) P[i] += logf(sr[i]) - z;
+        }
+    }
+}
+
+// sum of the x adjoint terms in the source-sorted slots [q0, q1)
+template <int S>
+__device__ __forceinline__ void sum_slots(const float *__restrict__ xc, uint32_t q0, uint32_t q1, float *acc) {
+    for (uint32_t q = q0; q < q1; ++q) {
+        float c[S];
+        ldv<S>(xc + (size_t)q * S, c);
+#pragma unroll
+        for (int j = 0; j < S; ++j) acc[j] += c[j];
+    }
 }
 
 template <int S>
@@ -139,13 +189,7 @@ __global__ void __launch_bounds__(kUThreads) k_u_gather_q(const UGraph g, const 
     if (v >= g.V) return;
     float qo[S];
     ldv<S>(lb + (size_t)v * S, qo);
-    for (uint32_t p = g.in_ptr[v]; p < g.in_ptr[v + 1]; ++p) {
-        float x[S], e[S], sr[S], m[S];
-        ldv<S>(send + (size_t)g.in_src[p] * S, x);
-        log_msg<S>(edge_table<S>(sm, g.pos_tab[p]), x, e, sr, m);
-#pragma unroll
-        for (int i = 0; i < S; ++i) qo[i] += m[i];
-    }
+    sum_log_msgs<S>(g, sm, send, g.in_ptr[v], g.in_ptr[v + 1], qo);
     stv<S>(lq + (size_t)v * S, qo);
 }
 
@@ -161,13 +205,7 @@ __global__ void __launch_bounds__(kUThreads) k_u_iter(const UGraph g, const floa
     float P[S], a[S];
 #pragma unroll
     for (int i = 0; i < S; ++i) P[i] = 0.0f;
-    for (uint32_t p = g.in_ptr[v]; p < g.in_ptr[v + 1]; ++p) {
-        float x[S], e[S], sr[S], m[S];
-        ldv<S>(lq_in + (size_t)g.in_src[p] * S, x);
-        log_msg<S>(edge_table<S>(sm, g.pos_tab[p]), x, e, sr, m);
-#pragma unroll
-        for (int i = 0; i < S; ++i) P[i] += m[i];
-    }
+    sum_log_msgs<S>(g, sm, lq_in, g.in_ptr[v], g.in_ptr[v + 1], P);
     ldv<S>(lb_in + (size_t)v * S, a);
 #pragma unroll
     for (int i = 0; i < S; ++i) a[i] += P[i];
@@ -182,43 +220,22 @@ __global__ void __launch_bounds__(kUThreads) k_u_iter(const UGraph g, const floa
     stv<S>(lq_out + (size_t)v * S, qo);
 }
 
-// x adjoint of node s through its out-edges: sum_e sum_i rbar_e,i w_e,ij,
-// w recomputed from s's own log-state x
-template <int S>
-__device__ __forceinline__ void gather_xbar(const UGraph &g, const float *sm, uint32_t s, const float *x,
-                                            const float *__restrict__ rbar, float *acc) {
-    float e[S];
-    shifted_exp<S>(x, e);
-    for (uint32_t qq = g.out_ptr[s]; qq < g.out_ptr[s + 1]; ++qq) {
-        const uint32_t p = g.out_pos[qq];
-        const float *J = edge_table<S>(sm, g.pos_tab[p]);
-        float rb[S], sr[S];
-        ldv<S>(rbar + (size_t)p * S, rb);
-        row_sums<S>(J, e, sr);
-#pragma unroll
-        for (int i = 0; i < S; ++i) {
-            const float c = rb[i] / sr[i];
-#pragma unroll
-            for (int j = 0; j < S; ++j) acc[j] += c * J[i * S + j] * e[j];
-        }
-    }
-}
-
 // adjoint of iteration t at node v (mode 0), or of the initial step
 // (mode 1: lQ_1 = lb_0 + lP, messages from send = lb_0), fused with the
-// gather of lQbar_{t+1}(v) from iteration t+1's rbar (rbar_next, null at t=T).
-// Writes lbbar_out (mode 1: lbbar_0 without its own send term), this
-// iteration's rbar, and adds the block's log-table adjoint into epart.
+// gather of lQbar_{t+1}(v) from iteration t+1's x adjoint terms (xc_next, in
+// source-sorted slots; null at t = T).  Writes lbbar_out (mode 1: lbbar_0
+// without its own send term), this iteration's x adjoint terms xc, and adds
+// the block's log-table adjoint into epart.
 template <int S>
-__global__ void __launch_bounds__(bwd_threads<S>()) k_u_bwd(const UGraph g, int mode, const float *__restrict__ send,
+__global__ void __launch_bounds__(bwd_threads<S>(), bwd_min_blocks<S>()) k_u_bwd(const UGraph g, int mode, const float *__restrict__ send,
                                                            const float *__restrict__ lb_t,
                                                            const float *__restrict__ lbbar_t,
-                                                           const float *__restrict__ send_next,
-                                                           const float *__restrict__ rbar_next,
-                                                           float *__restrict__ lbbar_out, float *__restrict__ rbar,
+                                                           const float *__restrict__ xc_next,
+                                                           float *__restrict__ lbbar_out, float *__restrict__ xc,
                                                            double *__restrict__ epart) {
     constexpr int NT = bwd_threads<S>();
     constexpr bool REG = S <= 4;
+    constexpr int B = 2;
     __shared__ float sm[2 * kUMaxTables * S * S];
     __shared__ float sacc[REG ? 1 : S * S * NT];
     __shared__ float wred[NT / 32][REG ? S * S : 1];
@@ -239,11 +256,7 @@ __global__ void __launch_bounds__(bwd_threads<S>()) k_u_bwd(const UGraph g, int 
             gq[i] = 0.0f;
         }
         if (lbbar_t) ldv<S>(lbbar_t + (size_t)v * S, gb);
-        if (rbar_next) {
-            float xn[S];
-            ldv<S>(send_next + (size_t)v * S, xn);
-            gather_xbar<S>(g, sm, v, xn, rbar_next, gq);
-        }
+        if (xc_next) sum_slots<S>(xc_next, g.out_ptr[v], g.out_ptr[v + 1], gq);
         float out[S];
         if (mode == 0) {
             float lb[S], gs = 0.0f;
@@ -269,26 +282,68 @@ __global__ void __launch_bounds__(bwd_threads<S>()) k_u_bwd(const UGraph g, int 
         float ps = 0.0f;
 #pragma unroll
         for (int i = 0; i < S; ++i) ps += Pbar[i];
-        for (uint32_t p = g.in_ptr[v]; p < g.in_ptr[v + 1]; ++p) {
-            const uint8_t tab = g.pos_tab[p];
-            const float *J = edge_table<S>(sm, tab);
-            float x[S], e[S], sr[S], lm[S], rb[S];
-            ldv<S>(send + (size_t)g.in_src[p] * S, x);
-            log_msg<S>(J, x, e, sr, lm);
+        const uint32_t r0 = g.in_ptr[v], r1 = g.in_ptr[v + 1];
+        for (uint32_t p0 = r0; p0 < r1; p0 += B) {
+            uint32_t src[B], slot[B];
+            uint8_t tb[B];
+            float x[B][S];
 #pragma unroll
-            for (int i = 0; i < S; ++i) rb[i] = Pbar[i] - expf(lm[i]) * ps;
-            stv<S>(rbar + (size_t)p * S, rb);
-            const bool tr = (tab & 0x80u) != 0;
-#pragma unroll
-            for (int i = 0; i < S; ++i) {
-                const float c = rb[i] / sr[i];
-#pragma unroll
-                for (int j = 0; j < S; ++j) {
-                    const float w = c * J[i * S + j] * e[j];
-                    const int k = tr ? j * S + i : i * S + j;
-                    if constexpr (REG) acc[k] += w;
-                    else sacc[k * NT + threadIdx.x] += w;
+            for (int b = 0; b < B; ++b)
+                if (p0 + b < r1) {
+                    src[b] = g.in_src[p0 + b];
+                    tb[b] = g.pos_tab[p0 + b];
+                    slot[b] = g.pos_out[p0 + b];
                 }
+#pragma unroll
+            for (int b = 0; b < B; ++b)
+                if (p0 + b < r1) ldv<S>(send + (size_t)src[b] * S, x[b]);
+#pragma unroll
+            for (int b = 0; b < B; ++b) {
+                if (p0 + b >= r1) break;
+                const float *J = edge_table<S>(sm, tb[b]);
+                float e[S], sr[S], c[S];
+                const float z = msg_sums<S>(J, x[b], e, sr);
+#pragma unroll
+                for (int j = 0; j < S; ++j) c[j] = 0.0f;
+                // rbar_i / s_i = (Pbar_i - (s_i / z) sum(Pbar)) / s_i = Pbar_i / s_i - sum(Pbar) / z
+                const float psz = ps / z;
+                float ci[S];
+#pragma unroll
+                for (int i = 0; i < S; ++i) ci[i] = Pbar[i] / sr[i] - psz;
+                // the table adjoint lands transposed for a transposed table
+                const bool tr = (tb[b] & 0x80u) != 0;
+                if constexpr (REG) {
+                    if (tr) {
+#pragma unroll
+                        for (int i = 0; i < S; ++i)
+#pragma unroll
+                            for (int j = 0; j < S; ++j) {
+                                const float w = ci[i] * J[i * S + j] * e[j];
+                                c[j] += w;
+                                acc[j * S + i] += w;
+                            }
+                    } else {
+#pragma unroll
+                        for (int i = 0; i < S; ++i)
+#pragma unroll
+                            for (int j = 0; j < S; ++j) {
+                                const float w = ci[i] * J[i * S + j] * e[j];
+                                c[j] += w;
+                                acc[i * S + j] += w;
+                            }
+                    }
+                } else {
+                    const int si = tr ? 1 : S, sj = tr ? S : 1;   // entry (i, j) -> i*si + j*sj
+#pragma unroll
+                    for (int i = 0; i < S; ++i)
+#pragma unroll
+                        for (int j = 0; j < S; ++j) {
+                            const float w = ci[i] * J[i * S + j] * e[j];
+                            c[j] += w;
+                            sacc[(i * si + j * sj) * NT + threadIdx.x] += w;
+                        }
+                }
+                stv<S>(xc + (size_t)slot[b] * S, c);
             }
         }
     }
@@ -319,19 +374,15 @@ __global__ void __launch_bounds__(bwd_threads<S>()) k_u_bwd(const UGraph g, int 
     }
 }
 
-// out(s) = add(s) + x adjoint of s through its out-edges (initial step)
+// out(s) = add(s) + the x adjoint terms of s's out-edges (initial step)
 template <int S>
-__global__ void __launch_bounds__(kUThreads) k_u_bwd_src(const UGraph g, const float *__restrict__ send,
-                                                         const float *__restrict__ rbar,
+__global__ void __launch_bounds__(kUThreads) k_u_bwd_src(const UGraph g, const float *__restrict__ xc,
                                                          const float *__restrict__ add, float *__restrict__ out) {
-    __shared__ float sm[2 * kUMaxTables * S * S];
-    load_tables_smem<S>(g, sm);
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= g.V) return;
-    float acc[S], x[S];
+    float acc[S];
     ldv<S>(add + (size_t)s * S, acc);
-    ldv<S>(send + (size_t)s * S, x);
-    gather_xbar<S>(g, sm, s, x, rbar, acc);
+    sum_slots<S>(xc, g.out_ptr[s], g.out_ptr[s + 1], acc);
     stv<S>(out + (size_t)s * S, acc);
 }
 
@@ -372,7 +423,7 @@ struct bp_unrolled {
     uint32_t V = 0, E = 0, S = 0, K = 0, T = 0, ck = 1, nck = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
-    uint32_t *in_ptr = nullptr, *in_src = nullptr, *out_ptr = nullptr, *out_pos = nullptr;
+    uint32_t *in_ptr = nullptr, *in_src = nullptr, *out_ptr = nullptr, *pos_out = nullptr;
     uint8_t *pos_tab = nullptr;
     float *tables = nullptr;
     float *ck_b = nullptr, *ck_q = nullptr;    // [nck][V][S]
@@ -380,7 +431,7 @@ struct bp_unrolled {
     float *pp_b = nullptr, *pp_q = nullptr;    // [2][V][S]
     float *bT = nullptr;
     float *bbar[2] = {nullptr, nullptr};
-    float *rbar[2] = {nullptr, nullptr};
+    float *xc[2] = {nullptr, nullptr};       // [E][S] x adjoint terms, source-sorted slots
     double *epart = nullptr;
     float *theta_buf = nullptr, *gtheta_buf = nullptr, *glogp_buf = nullptr;
     cudaGraphExec_t fwd_exec = nullptr, bwd_exec = nullptr;
@@ -396,7 +447,7 @@ namespace bpx {
 // into a CUDA graph, replayed on every call
 template <int S>
 static int u_forward(bp_unrolled *u) {
-    const UGraph g{u->V, u->K, u->in_ptr, u->in_src, u->out_ptr, u->out_pos, u->pos_tab, u->tables};
+    const UGraph g{u->V, u->K, u->in_ptr, u->in_src, u->out_ptr, u->pos_out, u->pos_tab, u->tables};
     const size_t VS = (size_t)u->V * S;
     const unsigned gv = grid_for(u->V, kUThreads);
     cudaStream_t st = u->stream;
@@ -419,7 +470,7 @@ static int u_forward(bp_unrolled *u) {
 // entry; gtheta_buf, glogp_buf receive the gradients)
 template <int S>
 static int u_backward(bp_unrolled *u) {
-    const UGraph g{u->V, u->K, u->in_ptr, u->in_src, u->out_ptr, u->out_pos, u->pos_tab, u->tables};
+    const UGraph g{u->V, u->K, u->in_ptr, u->in_src, u->out_ptr, u->pos_out, u->pos_tab, u->tables};
     const size_t VS = (size_t)u->V * S;
     const unsigned gv = grid_for(u->V, kUThreads);
     constexpr int BT = bwd_threads<S>();
@@ -427,7 +478,7 @@ static int u_backward(bp_unrolled *u) {
     cudaStream_t st = u->stream;
     BP_CUDA(cudaMemsetAsync(u->epart, 0, sizeof(double) * gb * S * S, st));
     int bc = 0, rn = 0;
-    const float *rb_next = nullptr;   // rbar of iteration t+1 (none at t = T)
+    const float *xc_next = nullptr;   // x adjoint terms of iteration t+1 (none at t = T)
     const uint32_t nseg = (u->T + u->ck - 1) / u->ck;
     for (int s = (int)nseg - 1; s >= 0; --s) {
         const uint32_t t0 = (uint32_t)s * u->ck, t_end = std::min(t0 + u->ck, u->T);
@@ -444,22 +495,18 @@ static int u_backward(bp_unrolled *u) {
             const float *b_t = (t == u->T) ? u->bT
                                : (t == t_end) ? u->ck_b + (size_t)(s + 1) * VS
                                               : u->seg_b + (j + 1) * VS;     // lb_t
-            const float *q_next = (t == u->T) ? nullptr
-                                  : (t == t_end) ? u->ck_q + (size_t)(s + 1) * VS
-                                                 : u->seg_q + (j + 1) * VS;  // lQ_{t+1}
-            k_u_bwd<S><<<gb, BT, 0, st>>>(g, 0, q_t, b_t, u->bbar[bc], q_next, rb_next, u->bbar[bc ^ 1],
-                                          u->rbar[rn], u->epart);
+            k_u_bwd<S><<<gb, BT, 0, st>>>(g, 0, q_t, b_t, u->bbar[bc], xc_next, u->bbar[bc ^ 1], u->xc[rn],
+                                          u->epart);
             bc ^= 1;
-            rb_next = u->rbar[rn];
+            xc_next = u->xc[rn];
             rn ^= 1;
         }
     }
     BP_CUDA(cudaGetLastError());
     // initial step: lQ_1 = lb_0 + sum lm(lb_0); its own x adjoint goes to lb_0
-    const float *b0 = u->ck_b, *q1 = u->ck_q;
-    k_u_bwd<S><<<gb, BT, 0, st>>>(g, 1, b0, nullptr, u->bbar[bc], q1, rb_next, u->bbar[bc ^ 1], u->rbar[rn],
-                                  u->epart);
-    k_u_bwd_src<S><<<gv, kUThreads, 0, st>>>(g, b0, u->rbar[rn], u->bbar[bc ^ 1], u->bbar[bc]);
+    const float *b0 = u->ck_b;
+    k_u_bwd<S><<<gb, BT, 0, st>>>(g, 1, b0, nullptr, u->bbar[bc], xc_next, u->bbar[bc ^ 1], u->xc[rn], u->epart);
+    k_u_bwd_src<S><<<gv, kUThreads, 0, st>>>(g, u->xc[rn], u->bbar[bc ^ 1], u->bbar[bc]);
     k_u_logsoftmax_bwd<S><<<gv, kUThreads, 0, st>>>(u->V, b0, u->bbar[bc], u->gtheta_buf);
     k_u_reduce_pair<<<u->K * S * S, 256, 0, st>>>(u->epart, gb, u->K * S * S, u->glogp_buf);
     BP_CUDA(cudaGetLastError());
@@ -468,9 +515,9 @@ static int u_backward(bp_unrolled *u) {
 
 static void u_free(bp_unrolled *u) {
     if (!u) return;
-    void *ptrs[] = {u->in_ptr, u->in_src, u->out_ptr, u->out_pos, u->pos_tab, u->tables, u->ck_b, u->ck_q,
-                    u->seg_b, u->seg_q, u->pp_b, u->pp_q, u->bT, u->bbar[0], u->bbar[1], u->rbar[0],
-                    u->rbar[1], u->epart, u->theta_buf, u->gtheta_buf, u->glogp_buf};
+    void *ptrs[] = {u->in_ptr, u->in_src, u->out_ptr, u->pos_out, u->pos_tab, u->tables, u->ck_b, u->ck_q,
+                    u->seg_b, u->seg_q, u->pp_b, u->pp_q, u->bT, u->bbar[0], u->bbar[1], u->xc[0],
+                    u->xc[1], u->epart, u->theta_buf, u->gtheta_buf, u->glogp_buf};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (u->fwd_exec) cudaGraphExecDestroy(u->fwd_exec);
@@ -525,7 +572,7 @@ int bp_unrolled_create(bp_unrolled **out, uint32_t V, uint32_t E, uint32_t S, ui
         u->own_stream = true;
     }
     // destination-sorted (stable) and source-sorted edge orders, on the host
-    std::vector<uint32_t> in_ptr(V + 1, 0), out_ptr(V + 1, 0), perm(E), in_src(E), out_pos(E);
+    std::vector<uint32_t> in_ptr(V + 1, 0), out_ptr(V + 1, 0), in_src(E), pos_out(E);
     std::vector<uint8_t> ptab(E);
     for (uint32_t e = 0; e < E; ++e) {
         in_ptr[dst[e] + 1]++;
@@ -543,14 +590,14 @@ int bp_unrolled_create(bp_unrolled **out, uint32_t V, uint32_t E, uint32_t S, ui
         ptab[p] = tab[e];
     }
     std::vector<uint32_t> ofill(out_ptr.begin(), out_ptr.end() - 1);
-    for (uint32_t e = 0; e < E; ++e) out_pos[ofill[src[e]]++] = pos_of[e];
+    for (uint32_t e = 0; e < E; ++e) pos_out[pos_of[e]] = ofill[src[e]]++;
     const size_t VS = (size_t)V * S;
     u->nblk = grid_for(V, 64);   // partial slots for the smallest backward block
     auto alloc = [&](void **p, size_t bytes) {
         return cudaMalloc(p, bytes ? bytes : 16) == cudaSuccess;
     };
     bool ok = alloc((void **)&u->in_ptr, sizeof(uint32_t) * (V + 1)) && alloc((void **)&u->in_src, 4 * (size_t)E) &&
-              alloc((void **)&u->out_ptr, sizeof(uint32_t) * (V + 1)) && alloc((void **)&u->out_pos, 4 * (size_t)E) &&
+              alloc((void **)&u->out_ptr, sizeof(uint32_t) * (V + 1)) && alloc((void **)&u->pos_out, 4 * (size_t)E) &&
               alloc((void **)&u->pos_tab, (size_t)E) && alloc((void **)&u->tables, sizeof(float) * K * S * S) &&
               alloc((void **)&u->ck_b, sizeof(float) * VS * u->nck) &&
               alloc((void **)&u->ck_q, sizeof(float) * VS * u->nck) &&
@@ -558,8 +605,8 @@ int bp_unrolled_create(bp_unrolled **out, uint32_t V, uint32_t E, uint32_t S, ui
               alloc((void **)&u->pp_b, sizeof(float) * VS * 2) && alloc((void **)&u->pp_q, sizeof(float) * VS * 2) &&
               alloc((void **)&u->bT, sizeof(float) * VS) && alloc((void **)&u->bbar[0], sizeof(float) * VS) &&
               alloc((void **)&u->bbar[1], sizeof(float) * VS) &&
-              alloc((void **)&u->rbar[0], sizeof(float) * S * (size_t)E) &&
-              alloc((void **)&u->rbar[1], sizeof(float) * S * (size_t)E) &&
+              alloc((void **)&u->xc[0], sizeof(float) * S * (size_t)E) &&
+              alloc((void **)&u->xc[1], sizeof(float) * S * (size_t)E) &&
               alloc((void **)&u->epart, sizeof(double) * u->nblk * S * S) &&
               alloc((void **)&u->theta_buf, sizeof(float) * VS) && alloc((void **)&u->gtheta_buf, sizeof(float) * VS) &&
               alloc((void **)&u->glogp_buf, sizeof(float) * K * S * S);
@@ -571,7 +618,7 @@ int bp_unrolled_create(bp_unrolled **out, uint32_t V, uint32_t E, uint32_t S, ui
     cudaMemcpyAsync(u->out_ptr, out_ptr.data(), 4 * (V + 1), cudaMemcpyHostToDevice, u->stream);
     if (E) {
         cudaMemcpyAsync(u->in_src, in_src.data(), 4 * (size_t)E, cudaMemcpyHostToDevice, u->stream);
-        cudaMemcpyAsync(u->out_pos, out_pos.data(), 4 * (size_t)E, cudaMemcpyHostToDevice, u->stream);
+        cudaMemcpyAsync(u->pos_out, pos_out.data(), 4 * (size_t)E, cudaMemcpyHostToDevice, u->stream);
         cudaMemcpyAsync(u->pos_tab, ptab.data(), (size_t)E, cudaMemcpyHostToDevice, u->stream);
     }
     cudaEventCreate(&u->ev0);

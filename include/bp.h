@@ -62,9 +62,12 @@ typedef enum { BP_SYNC_EAGER = 0, BP_SYNC_LAZY = 1 } bp_sync_mode;
 
 /* the node-schedule iteration kernel: same results, different tiling */
 typedef enum {
-    BP_KERNEL_AUTO = 0,        /* block tiles (BP_FLOOD_KERNEL=warp in the environment selects warp tiles) */
+    BP_KERNEL_AUTO = 0,        /* staged tiles where they apply, else block tiles (BP_FLOOD_KERNEL=block|warp|staged
+                                  in the environment overrides) */
     BP_KERNEL_BLOCK_TILE = 1,  /* 256-node block tiles, block-wide barriers between phases */
-    BP_KERNEL_WARP_TILE = 2    /* 32-node warp tiles, unrolled edge loads */
+    BP_KERNEL_WARP_TILE = 2,   /* 32-node warp tiles, unrolled edge loads */
+    BP_KERNEL_STAGED_TILE = 3  /* persistent CTAs, bulk-copy staged tiles; uniform 2-state graphs of mean in-degree
+                                  <= 4.5, f64 delta */
 } bp_kernel_variant;
 
 typedef struct bp_graph bp_graph;

@@ -14,7 +14,7 @@ pytestmark = pytest.mark.gpu
 
 
 def gpu_loopy(bp, net, tol, max_it, check_every=1, schedule="node", delta="serial", init=True,
-              msgs=None, graph_chunk=0, reorder=False):
+              msgs=None, graph_chunk=0, reorder=False, kernel="auto"):
     from belief_propagation_b200.engine import BPGraph
     g = BPGraph.from_network(net, reorder=reorder)
     try:
@@ -25,7 +25,7 @@ def gpu_loopy(bp, net, tol, max_it, check_every=1, schedule="node", delta="seria
         if init:
             g.init_messages()
         r = g.loopy(tol, max_it, check_every=check_every, schedule=schedule, delta=delta,
-                    graph_chunk=graph_chunk)
+                    graph_chunk=graph_chunk, kernel=kernel)
         out = dict(r, beliefs=g.beliefs(), slot1=g.messages(1), slot0=g.messages(0), latest=g.latest_slot)
     finally:
         g.close()
@@ -233,3 +233,73 @@ def test_loopy_power_law_scale(bp, synth, restatement, O):
     d = np.abs(ora["prev_arr"][:, :2].astype(np.float64) - ora["cur_arr"][:, :2].astype(np.float64))
     d64 = float(np.nan_to_num(d).sum())
     assert abs(gpu["delta_f64"] - d64) <= 1e-9 * max(1.0, d64)
+
+
+def _staged_cases(synth):
+    rng = np.random.default_rng(17)
+    out = {"power_law": synth.power_law_loopy(1 << 16, 1 << 18, 2, 0.1, seed=5),
+           "ragged_tail": synth.random_loopy(257, 1000, 2, 0.1, seed=6),
+           "one_tile": synth.random_loopy(40, 150, 2, 0.1, seed=7)}
+    V = 300
+    out["no_edges"] = synth.Network(np.full(V, 2, np.uint32), rng.random((V, 2), dtype=np.float32),
+                                    np.zeros(V, np.uint8), np.zeros(0, np.uint32), np.zeros(0, np.uint32),
+                                    np.zeros((0, 2, 2), np.float32))
+    # a hub whose in-edges overflow a stage, beside ordinary tiles
+    V = 6000
+    src = np.arange(1, 3001, dtype=np.uint32)
+    dst = np.zeros(3000, np.uint32)
+    es = rng.integers(0, V, 12000).astype(np.uint32)
+    ed = rng.integers(1, V, 12000).astype(np.uint32)
+    keep = es != ed
+    src = np.concatenate([src, es[keep]])
+    dst = np.concatenate([dst, ed[keep]])
+    key = src.astype(np.int64) * V + dst
+    _, first = np.unique(key, return_index=True)
+    first.sort()
+    src, dst = src[first], dst[first]
+    j = rng.random((len(src), 2, 2), dtype=np.float32)
+    j /= j.sum(axis=2, keepdims=True)
+    out["hub"] = synth.Network(np.full(V, 2, np.uint32), rng.random((V, 2), dtype=np.float32) + 0.5,
+                               np.zeros(V, np.uint8), src, dst, j)
+    return out
+
+
+@pytest.mark.parametrize("name", ["power_law", "ragged_tail", "one_tile", "no_edges", "hub"])
+def test_loopy_staged_kernel_parity(bp, synth, restatement, O, name):
+    """The bulk-copy staged kernel (explicitly selected): the same beliefs and
+    messages, bit for bit, as the reference; fixed iterations, the _acc
+    variant's every-10 check (stages without the old messages), renumbered
+    ids, a partial last tile, a graph without edges and a hub tile that
+    overflows a stage."""
+    net = _staged_cases(synth)[name]
+    for tol, max_it, check, reorder in ((0.0, 7, 1, False), (0.0, 25, 10, False), (0.0, 6, 1, True)):
+        ora = restatement.loopy(O.OracleGraph(net), tol, max_it, check_every=check)
+        gpu = gpu_loopy(bp, net, tol, max_it, check_every=check, delta="f64", kernel="staged", reorder=reorder)
+        assert_same(gpu, ora, 2)
+
+
+def test_loopy_staged_matches_block_kernel_with_tolerance(bp, synth):
+    """Stopping on a tolerance: the staged and block kernels stop at the same
+    iteration with identical beliefs (their f64 deltas differ only in
+    summation order)."""
+    net = synth.power_law_loopy(1 << 15, 1 << 17, 2, 0.1, seed=9)
+    a = gpu_loopy(bp, net, 1e-3, 100, delta="f64", kernel="block")
+    b = gpu_loopy(bp, net, 1e-3, 100, delta="f64", kernel="staged")
+    assert a["iterations"] == b["iterations"] and a["executed"] == b["executed"]
+    np.testing.assert_array_equal(a["beliefs"], b["beliefs"])
+    np.testing.assert_array_equal(a["slot0"], b["slot0"])
+    assert abs(a["delta_f64"] - b["delta_f64"]) <= 1e-12 * max(1.0, abs(a["delta_f64"]))
+
+
+def test_loopy_staged_refuses_inapplicable_graphs(bp, synth):
+    from belief_propagation_b200.engine import BPGraph
+    from belief_propagation_b200.native import BPError
+    for net, delta in ((synth.random_loopy(300, 1200, 3, 0.1, seed=1), "f64"),
+                       (synth.random_loopy(300, 1200, 2, 0.1, seed=1), "serial"),
+                       (synth.random_loopy(300, 3000, 2, 0.1, seed=1), "f64")):
+        g = BPGraph.from_network(net)
+        try:
+            with pytest.raises(BPError):
+                g.loopy(0.0, 3, delta=delta, kernel="staged")
+        finally:
+            g.close()

@@ -99,3 +99,67 @@ def test_tree_unreachable_reports_error(bp, synth):
             g.build_levels()
     finally:
         g.close()
+
+
+def _path_network(synth, V, seed):
+    """A path 0-1-2-...: every node has in-degree <= 2, so the whole path is
+    level 0 and each node waits on its predecessor (V waves)."""
+    rng = np.random.default_rng(seed)
+    a = np.arange(V - 1, dtype=np.uint32)
+    src = np.empty(2 * (V - 1), np.uint32)
+    dst = np.empty(2 * (V - 1), np.uint32)
+    src[0::2], dst[0::2] = a, a + 1
+    src[1::2], dst[1::2] = a + 1, a
+    j = rng.random((len(src), 2, 2), dtype=np.float32)
+    j /= j.sum(axis=2, keepdims=True)
+    b = rng.random((V, 2), dtype=np.float32)
+    b /= b.sum(axis=1, keepdims=True)
+    return synth.Network(np.full(V, 2, np.uint32), b, np.zeros(V, np.uint8), src, dst, j)
+
+
+@pytest.mark.parametrize("V", [40, 700])
+def test_tree_long_wave_chains(bp, synth, restatement, O, V):
+    """Waves as long as the level (the device split hands chains longer than
+    its round cap to the host split): same results as the reference."""
+    net = _path_network(synth, V, seed=V)
+    ora = restatement.tree(O.OracleGraph(net))
+    r = gpu_tree(net)
+    assert r["num_levels"] == ora["num_levels"]
+    np.testing.assert_array_equal(r["levels"][net.V:], ora["levels"][net.V:])
+    np.testing.assert_array_equal(r["beliefs"][:, :2], ora["beliefs"][:, :2])
+    np.testing.assert_array_equal(r["messages"][:, :2], ora["messages"][:, :2])
+
+
+def test_tree_device_and_host_level_builds_agree(bp, synth, monkeypatch):
+    """The device level build gives the host build's lists, level count and
+    wave count, on trees and on graphs with cycles."""
+    nets = [synth.random_tree(30000, (2, 3), 0.05, seed=11)]
+    for seed in range(50, 80):
+        net = synth.random_loopy(500, 1200, 2, 0.1, seed=seed)
+        if (np.bincount(net.dst, minlength=net.V) <= 2).any():
+            nets.append(net)
+        if len(nets) == 4:
+            break
+    from belief_propagation_b200.native import BPError
+    compared = 0
+    for net in nets:
+        try:
+            dev = gpu_tree(net)
+        except BPError:
+            dev = None
+        monkeypatch.setenv("BP_TREE_LEVELS", "host")
+        try:
+            host = gpu_tree(net)
+        except BPError:
+            host = None
+        monkeypatch.delenv("BP_TREE_LEVELS")
+        assert (dev is None) == (host is None)
+        if dev is None:
+            continue
+        compared += 1
+        assert dev["num_levels"] == host["num_levels"]
+        assert dev["num_waves"] == host["num_waves"]
+        np.testing.assert_array_equal(dev["levels"][: dev["num_levels"]], host["levels"][: host["num_levels"]])
+        np.testing.assert_array_equal(dev["levels"][net.V:], host["levels"][net.V:])
+        np.testing.assert_array_equal(dev["beliefs"], host["beliefs"])
+    assert compared >= 2
