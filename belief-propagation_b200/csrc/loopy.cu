@@ -1256,8 +1256,8 @@ int bp_loopy(bp_graph *g, const bp_loopy_options *opt, bp_loopy_result *res) {
     if (variant == BP_KERNEL_AUTO) {
         const char *env = getenv("BP_FLOOD_KERNEL");
         if (env && env[0] == 'w') variant = BP_KERNEL_WARP_TILE;
-        else if (env && env[0] == 'b') variant = BP_KERNEL_BLOCK_TILE;
-        else variant = staged_applies(g, opt->schedule, serial) ? BP_KERNEL_STAGED_TILE : BP_KERNEL_BLOCK_TILE;
+        else if (env && env[0] == 's' && staged_applies(g, opt->schedule, serial)) variant = BP_KERNEL_STAGED_TILE;
+        else variant = BP_KERNEL_BLOCK_TILE;
     }
     if (variant != BP_KERNEL_BLOCK_TILE && variant != BP_KERNEL_WARP_TILE && variant != BP_KERNEL_STAGED_TILE)
         return set_error(BP_ERR_INVALID, "unknown kernel variant %d", opt->kernel_variant);

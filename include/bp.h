@@ -62,8 +62,8 @@ typedef enum { BP_SYNC_EAGER = 0, BP_SYNC_LAZY = 1 } bp_sync_mode;
 
 /* the node-schedule iteration kernel: same results, different tiling */
 typedef enum {
-    BP_KERNEL_AUTO = 0,        /* staged tiles where they apply, else block tiles (BP_FLOOD_KERNEL=block|warp|staged
-                                  in the environment overrides) */
+    BP_KERNEL_AUTO = 0,        /* block tiles (BP_FLOOD_KERNEL=warp|staged in the environment selects warp tiles,
+                                  or staged tiles where they apply) */
     BP_KERNEL_BLOCK_TILE = 1,  /* 256-node block tiles, block-wide barriers between phases */
     BP_KERNEL_WARP_TILE = 2,   /* 32-node warp tiles, unrolled edge loads */
     BP_KERNEL_STAGED_TILE = 3  /* persistent CTAs, bulk-copy staged tiles; uniform 2-state graphs of mean in-degree
