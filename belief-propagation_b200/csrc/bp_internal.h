@@ -22,6 +22,10 @@
 
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+
+#include <chrono>
 
 #include "bp.h"
 
@@ -145,6 +149,25 @@ int tree_build_levels_gpu(bp_graph *g, uint32_t *levels, uint32_t *num_levels);
 int ensure_staging(bp_graph *g, size_t bytes);
 int ensure_out_csr(bp_graph *g);
 int ensure_host_in_ptr(bp_graph *g);
+
+// BP_TRACE=1: wall time of each stage of a multi-stage call on stderr (each
+// mark waits for the graph's stream, so tracing serialises the stages)
+struct StageTrace {
+    bool on;
+    cudaStream_t s;
+    const char *what;
+    std::chrono::steady_clock::time_point t;
+    StageTrace(cudaStream_t s_, const char *what_)
+        : on(getenv("BP_TRACE") != nullptr), s(s_), what(what_), t(std::chrono::steady_clock::now()) {}
+    void mark(const char *stage) {
+        if (!on) return;
+        cudaStreamSynchronize(s);
+        const auto n = std::chrono::steady_clock::now();
+        fprintf(stderr, "bp_trace %s %-22s %9.3f ms\n", what, stage,
+                std::chrono::duration<double, std::milli>(n - t).count());
+        t = n;
+    }
+};
 
 inline unsigned grid_for(uint64_t n, unsigned block) {
     uint64_t b = (n + block - 1) / block;

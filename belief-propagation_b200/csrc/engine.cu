@@ -421,27 +421,10 @@ static void free_graph(bp_graph *g) {
     delete g;
 }
 
-// BP_TRACE=1: wall time of each stage of bp_graph_create on stderr (each
-// mark waits for the graph's stream, so tracing serialises the stages)
-struct StageTrace {
-    bool on;
-    cudaStream_t s;
-    std::chrono::steady_clock::time_point t;
-    explicit StageTrace(cudaStream_t s_) : on(getenv("BP_TRACE") != nullptr), s(s_), t(std::chrono::steady_clock::now()) {}
-    void mark(const char *what) {
-        if (!on) return;
-        cudaStreamSynchronize(s);
-        const auto n = std::chrono::steady_clock::now();
-        fprintf(stderr, "bp_trace create %-22s %9.3f ms\n", what,
-                std::chrono::duration<double, std::milli>(n - t).count());
-        t = n;
-    }
-};
-
 static int create_impl(bp_graph *g, const bp_graph_desc *d) {
     const uint32_t V = d->num_nodes, E = d->num_edges;
     int st;
-    StageTrace trace(g->stream);
+    StageTrace trace(g->stream, "create");
     // ---- state counts (validated on the host when they are host memory)
     std::vector<uint32_t> s32;
     const uint32_t *states = d->node_num_states;

@@ -151,7 +151,9 @@ int tree_build_levels_gpu(bp_graph *g, uint32_t *levels_out, uint32_t *num_level
     const uint32_t V = g->V;
     cudaStream_t st = g->stream;
     int rc;
+    StageTrace trace(st, "levels");
     if ((rc = ensure_out_csr(g))) return rc;
+    trace.mark("source-sorted csr");
     tree_clear(g);
     TreeData &t = g->tree;
     PoolBufs pb(st);
@@ -179,6 +181,7 @@ int tree_build_levels_gpu(bp_graph *g, uint32_t *levels_out, uint32_t *num_level
     uint32_t hc = 0;
     uint32_t *h_count = &hc;
 
+    trace.mark("buffers");
     // ---- level 0: ascending ids with in-degree <= 2
     const unsigned gv = grid_for(V, 256);
     k_leaf_flags<<<gv, 256, 0, st>>>(V, g->in_ptr, listed, iota);
@@ -229,6 +232,7 @@ int tree_build_levels_gpu(bp_graph *g, uint32_t *levels_out, uint32_t *num_level
         end += c;
     }
     const uint32_t L = (uint32_t)off.size();
+    trace.mark("level lists");
 
     // ---- waves: relaxation rounds to the longest-path fixed point
     bool converged = V == 0;
@@ -247,6 +251,7 @@ int tree_build_levels_gpu(bp_graph *g, uint32_t *levels_out, uint32_t *num_level
         }
     }
 
+    trace.mark("wave rounds");
     // the reference's levels_to_nodes layout: offsets, then the list at [V, 2V)
     std::vector<uint32_t> host_levels;
     const bool want_host = levels_out != nullptr || !converged;
@@ -257,6 +262,7 @@ int tree_build_levels_gpu(bp_graph *g, uint32_t *levels_out, uint32_t *num_level
         BP_CUDA(cudaStreamSynchronize(st));
         if (levels_out) memcpy(levels_out, host_levels.data(), sizeof(uint32_t) * 2 * (size_t)V);
     }
+    trace.mark("list to host");
     *num_levels_out = L;
     if (!converged) {
         // chains longer than the round cap: the host split on the same list
@@ -286,6 +292,7 @@ int tree_build_levels_gpu(bp_graph *g, uint32_t *levels_out, uint32_t *num_level
         BP_CUDA(cudaMemcpyAsync(run_lvl.data(), run_level, sizeof(uint32_t) * nruns, cudaMemcpyDeviceToHost, st));
         BP_CUDA(cudaStreamSynchronize(st));
     }
+    trace.mark("wave layout");
     t.wave_off = (uint32_t *)malloc(sizeof(uint32_t) * ((size_t)nruns + 1));
     t.level_wave_begin = (uint32_t *)malloc(sizeof(uint32_t) * ((size_t)L + 1));
     if (!t.wave_off || !t.level_wave_begin) {

@@ -115,8 +115,9 @@ __device__ __forceinline__ void reduce_and_finalize(LoopyCtl *ctl, double *parti
     double t = block_sum<NT>(dsum, red);
     if (threadIdx.x == 0) {
         partials[blockIdx.x] = t;
-        __threadfence();
-        unsigned ticket = atomicAdd(&ctl->counter, 1u);
+        // release: the partial is visible before the ticket is
+        unsigned ticket;
+        asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(ticket) : "l"(&ctl->counter) : "memory");
         *s_last = (ticket == gridDim.x - 1);
     }
     __syncthreads();
@@ -141,6 +142,22 @@ __global__ void __launch_bounds__(flood_nt<MS>(), flood_min_blocks<MS, FU>()) k_
     __shared__ bool s_last;
 
     LoopyCtl *ctl = a.ctl;
+    // the tile's row pointers and this node's belief do not depend on the
+    // control block, so their loads go out together with its read
+    const uint32_t V = a.V, tid = threadIdx.x, v0 = blockIdx.x * NT;
+    const uint32_t vend = min(v0 + NT, V);
+    const uint32_t e0 = a.in_ptr[v0], e1 = a.in_ptr[vend];
+    const uint32_t v = v0 + tid;
+    const bool has = v < V;
+    uint32_t r0 = 0, r1 = 0;
+    int S = MS;
+    float b[MS];
+    if (has) {
+        r0 = a.in_ptr[v];
+        r1 = a.in_ptr[v + 1];
+        if (!UNI) S = a.node_s[v];
+        ldv<MS, kStream>(a.belief + (size_t)v * MS, b);
+    }
     if (*(volatile uint32_t *)&ctl->done) return;
     const uint32_t it = ctl->it, ce = ctl->check_every;
     const bool serial = ctl->serial != 0;
@@ -151,19 +168,6 @@ __global__ void __launch_bounds__(flood_nt<MS>(), flood_min_blocks<MS, FU>()) k_
     const float *__restrict__ q_in = qp ? a.q1 : a.q0;
     float *__restrict__ q_out = qp ? a.q0 : a.q1;
     const uint64_t keep = l2_evict_last_policy();
-
-    const uint32_t V = a.V, tid = threadIdx.x, v0 = blockIdx.x * NT;
-    const uint32_t vend = min(v0 + NT, V);
-    const uint32_t e0 = a.in_ptr[v0], e1 = a.in_ptr[vend];
-    const uint32_t v = v0 + tid;
-    const bool has = v < V;
-    uint32_t r0 = 0, r1 = 0;
-    int S = MS;
-    if (has) {
-        r0 = a.in_ptr[v];
-        r1 = a.in_ptr[v + 1];
-        if (!UNI) S = a.node_s[v];
-    }
     float prod[MS];
 #pragma unroll
     for (int i = 0; i < MS; ++i) prod[i] = 1.0f;
@@ -243,8 +247,6 @@ __global__ void __launch_bounds__(flood_nt<MS>(), flood_min_blocks<MS, FU>()) k_
     // phase 2b: marginalise (graph.c:1003-1023), then the next send buffer
     // (graph.c:850-882) from the same messages
     if (has) {
-        float b[MS];
-        ldv<MS, kStream>(a.belief + (size_t)v * MS, b);
         if (r1 > r0) {
 #pragma unroll
             for (int i = 0; i < MS; ++i)

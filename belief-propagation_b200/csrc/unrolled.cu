@@ -49,7 +49,7 @@ constexpr uint32_t kUMaxTables = 16;
 // so a warp's adds hit 32 different banks) with smaller blocks
 template <int S> constexpr int bwd_threads() { return S <= 4 ? 256 : 64; }
 // resident blocks per SM the adjoint kernel's register allocation must allow
-template <int S> constexpr int bwd_min_blocks() { return S <= 4 ? 3 : (S <= 8 ? 8 : 4); }
+template <int S> constexpr int bwd_min_blocks() { return S <= 4 ? 4 : (S <= 8 ? 8 : 4); }
 
 struct UGraph {
     uint32_t V, K;
@@ -92,13 +92,15 @@ __device__ __forceinline__ float lse(const float *a) {
 }
 
 // shifted exponentials of a log-state: e_j = exp(x_j - mx)
-template <int S>
+// (FAST: the hardware exponential __expf, a few ulp from expf; the adjoint
+// uses it, the forward keeps expf)
+template <int S, bool FAST = false>
 __device__ __forceinline__ float shifted_exp(const float *x, float *e) {
     float mx = x[0];
 #pragma unroll
     for (int j = 1; j < S; ++j) mx = fmaxf(mx, x[j]);
 #pragma unroll
-    for (int j = 0; j < S; ++j) e[j] = expf(x[j] - mx);
+    for (int j = 0; j < S; ++j) e[j] = FAST ? __expf(x[j] - mx) : expf(x[j] - mx);
     return mx;
 }
 
@@ -116,9 +118,9 @@ __device__ __forceinline__ void row_sums(const float *J, const float *e, float *
 
 // message of one edge in linear form: e = exp(x - max x), row sums s of
 // J e (s_i > 0); returns sum_i s_i.  lm_i = log s_i - log sum, m_i = s_i / sum.
-template <int S>
+template <int S, bool FAST = false>
 __device__ __forceinline__ float msg_sums(const float *J, const float *x, float *e, float *sr) {
-    shifted_exp<S>(x, e);
+    shifted_exp<S, FAST>(x, e);
     row_sums<S>(J, e, sr);
     float z = 0.0f;
 #pragma unroll
@@ -302,14 +304,15 @@ __global__ void __launch_bounds__(bwd_threads<S>(), bwd_min_blocks<S>()) k_u_bwd
                 if (p0 + b >= r1) break;
                 const float *J = edge_table<S>(sm, tb[b]);
                 float e[S], sr[S], c[S];
-                const float z = msg_sums<S>(J, x[b], e, sr);
+                const float z = msg_sums<S, true>(J, x[b], e, sr);
 #pragma unroll
                 for (int j = 0; j < S; ++j) c[j] = 0.0f;
                 // rbar_i / s_i = (Pbar_i - (s_i / z) sum(Pbar)) / s_i = Pbar_i / s_i - sum(Pbar) / z
-                const float psz = ps / z;
+                // (fast division: s_i and z lie in [1e-37, S])
+                const float psz = __fdividef(ps, z);
                 float ci[S];
 #pragma unroll
-                for (int i = 0; i < S; ++i) ci[i] = Pbar[i] / sr[i] - psz;
+                for (int i = 0; i < S; ++i) ci[i] = __fdividef(Pbar[i], sr[i]) - psz;
                 // the table adjoint lands transposed for a transposed table
                 const bool tr = (tb[b] & 0x80u) != 0;
                 if constexpr (REG) {
