@@ -48,6 +48,8 @@ constexpr uint32_t kUMaxTables = 16;
 // registers for S <= 4, else in a shared-memory slice per thread (entry-major,
 // so a warp's adds hit 32 different banks) with smaller blocks
 template <int S> constexpr int bwd_threads() { return S <= 4 ? 256 : 64; }
+// nodes per thread of the adjoint kernel (grid-stride)
+constexpr uint32_t kBwdNodesPerThread = 2;
 // resident blocks per SM the adjoint kernel's register allocation must allow
 template <int S> constexpr int bwd_min_blocks() { return S <= 4 ? 4 : (S <= 8 ? 8 : 4); }
 
@@ -151,7 +153,14 @@ __device__ __forceinline__ void sum_log_msgs(const UGraph &g, const float *sm, c
         for (int b = 0; b < B; ++b) {
             if (p0 + b >= r1) break;
             float e[S], sr[S];
-            const float z = logf(msg_sums<S>(edge_table<S>(sm, tb[b]), x[b], e, sr));
+            float z;
+            if constexpr (S <= 4) {
+                float jr[S * S];   // the edge's table, vector loads from shared memory
+                ldv<S * S>(edge_table<S>(sm, tb[b]), jr);
+                z = logf(msg_sums<S>(jr, x[b], e, sr));
+            } else {
+                z = logf(msg_sums<S>(edge_table<S>(sm, tb[b]), x[b], e, sr));
+            }
 #pragma unroll
             for (int i = 0; i < S; ++i) P[i] += logf(sr[i]) - z;
         }
@@ -185,7 +194,7 @@ __global__ void k_u_logsoftmax(uint32_t V, const float *__restrict__ theta, floa
 template <int S>
 __global__ void __launch_bounds__(kUThreads) k_u_gather_q(const UGraph g, const float *__restrict__ lb,
                                                           const float *__restrict__ send, float *__restrict__ lq) {
-    __shared__ float sm[2 * kUMaxTables * S * S];
+    __shared__ __align__(16) float sm[2 * kUMaxTables * S * S];
     load_tables_smem<S>(g, sm);
     const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= g.V) return;
@@ -200,7 +209,7 @@ template <int S>
 __global__ void __launch_bounds__(kUThreads) k_u_iter(const UGraph g, const float *__restrict__ lb_in,
                                                       const float *__restrict__ lq_in, float *__restrict__ lb_out,
                                                       float *__restrict__ lq_out) {
-    __shared__ float sm[2 * kUMaxTables * S * S];
+    __shared__ __align__(16) float sm[2 * kUMaxTables * S * S];
     load_tables_smem<S>(g, sm);
     const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= g.V) return;
@@ -222,6 +231,104 @@ __global__ void __launch_bounds__(kUThreads) k_u_iter(const UGraph g, const floa
     stv<S>(lq_out + (size_t)v * S, qo);
 }
 
+// this block's sum of the per-thread table-adjoint accumulators (fixed
+// order), added to its running partial row (S*S doubles)
+template <int S, int NT, bool REG>
+__device__ __forceinline__ void block_partial_add(const float *acc, const float *sacc, float (*wred)[REG ? S * S : 1],
+                                                  double *__restrict__ row) {
+    if constexpr (REG) {
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+        for (int k = 0; k < S * S; ++k) {
+            float x = acc[k];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+            if (lane == 0) wred[w][k] = x;
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < S * S; k += blockDim.x) {
+            double t = 0.0;
+            for (int ww = 0; ww < NT / 32; ++ww) t += (double)wred[ww][k];
+            row[k] += t;
+        }
+    } else {
+        __syncthreads();
+        for (int k = threadIdx.x; k < S * S; k += blockDim.x) {
+            double t = 0.0;
+            for (int tt = 0; tt < NT; ++tt) t += (double)sacc[k * NT + tt];
+            row[k] += t;
+        }
+    }
+}
+
+// table adjoint of the edge with scaled adjoint ci (rbar_i / s_i), table J
+// and source exponentials e: += ci_i J_ij e_j at (i, j), or at (j, i) for a
+// transposed table
+template <int S, int NT, bool REG>
+__device__ __forceinline__ void add_table_adjoint(float *acc, float *sacc, const float *ci, const float *J,
+                                                  const float *e, bool tr) {
+    if constexpr (REG) {
+        if (tr) {
+#pragma unroll
+            for (int i = 0; i < S; ++i)
+#pragma unroll
+                for (int j = 0; j < S; ++j) acc[j * S + i] += ci[i] * J[i * S + j] * e[j];
+        } else {
+#pragma unroll
+            for (int i = 0; i < S; ++i)
+#pragma unroll
+                for (int j = 0; j < S; ++j) acc[i * S + j] += ci[i] * J[i * S + j] * e[j];
+        }
+    } else {
+        const int si = tr ? 1 : S, sj = tr ? S : 1;
+#pragma unroll
+        for (int i = 0; i < S; ++i)
+#pragma unroll
+            for (int j = 0; j < S; ++j) sacc[(i * si + j * sj) * NT + threadIdx.x] += ci[i] * J[i * S + j] * e[j];
+    }
+}
+
+// several tables (K > 1): table k's adjoint, from the per-node Pbar the
+// adjoint kernel stored; every in-edge with table k recomputes its message
+// sums.  One launch per table keeps the accumulators per thread.
+template <int S>
+__global__ void __launch_bounds__(bwd_threads<S>()) k_u_pair_grad(const UGraph g, const float *__restrict__ send,
+                                                                  const float *__restrict__ pbar, uint32_t k,
+                                                                  double *__restrict__ epart_k) {
+    constexpr int NT = bwd_threads<S>();
+    constexpr bool REG = S <= 4;
+    __shared__ __align__(16) float sm[2 * kUMaxTables * S * S];
+    __shared__ float sacc[REG ? 1 : S * S * NT];
+    __shared__ float wred[NT / 32][REG ? S * S : 1];
+    load_tables_smem<S>(g, sm);
+    float acc[REG ? S * S : 1];
+    if constexpr (REG) {
+#pragma unroll
+        for (int q = 0; q < S * S; ++q) acc[q] = 0.0f;
+    } else {
+        for (int q = 0; q < S * S; ++q) sacc[q * NT + threadIdx.x] = 0.0f;
+    }
+    for (uint32_t v = blockIdx.x * NT + threadIdx.x; v < g.V; v += gridDim.x * NT) {
+        float Pb[S], ps = 0.0f;
+        ldv<S>(pbar + (size_t)v * S, Pb);
+#pragma unroll
+        for (int i = 0; i < S; ++i) ps += Pb[i];
+        for (uint32_t p = g.in_ptr[v]; p < g.in_ptr[v + 1]; ++p) {
+            const uint8_t tab = g.pos_tab[p];
+            if ((tab & 0x7fu) != k) continue;
+            float x[S], e[S], sr[S], ci[S];
+            ldv<S>(send + (size_t)g.in_src[p] * S, x);
+            const float *J = edge_table<S>(sm, tab);
+            const float z = msg_sums<S, true>(J, x, e, sr);
+            const float psz = __fdividef(ps, z);
+#pragma unroll
+            for (int i = 0; i < S; ++i) ci[i] = __fdividef(Pb[i], sr[i]) - psz;
+            add_table_adjoint<S, NT, REG>(acc, sacc, ci, J, e, (tab & 0x80u) != 0);
+        }
+    }
+    block_partial_add<S, NT, REG>(acc, sacc, wred, epart_k + (size_t)blockIdx.x * S * S);
+}
+
 // adjoint of iteration t at node v (mode 0), or of the initial step
 // (mode 1: lQ_1 = lb_0 + lP, messages from send = lb_0), fused with the
 // gather of lQbar_{t+1}(v) from iteration t+1's x adjoint terms (xc_next, in
@@ -234,15 +341,14 @@ __global__ void __launch_bounds__(bwd_threads<S>(), bwd_min_blocks<S>()) k_u_bwd
                                                            const float *__restrict__ lbbar_t,
                                                            const float *__restrict__ xc_next,
                                                            float *__restrict__ lbbar_out, float *__restrict__ xc,
-                                                           double *__restrict__ epart) {
+                                                           double *__restrict__ epart, float *__restrict__ pbar_out) {
     constexpr int NT = bwd_threads<S>();
     constexpr bool REG = S <= 4;
     constexpr int B = 2;
-    __shared__ float sm[2 * kUMaxTables * S * S];
+    __shared__ __align__(16) float sm[2 * kUMaxTables * S * S];
     __shared__ float sacc[REG ? 1 : S * S * NT];
     __shared__ float wred[NT / 32][REG ? S * S : 1];
     load_tables_smem<S>(g, sm);
-    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     float acc[REG ? S * S : 1];
     if constexpr (REG) {
 #pragma unroll
@@ -250,7 +356,9 @@ __global__ void __launch_bounds__(bwd_threads<S>(), bwd_min_blocks<S>()) k_u_bwd
     } else {
         for (int k = 0; k < S * S; ++k) sacc[k * NT + threadIdx.x] = 0.0f;
     }
-    if (v < g.V) {
+    // grid-stride over nodes: several nodes per thread share one block
+    // reduction of the table adjoint
+    for (uint32_t v = blockIdx.x * NT + threadIdx.x; v < g.V; v += gridDim.x * NT) {
         float gb[S], gq[S], Pbar[S];
 #pragma unroll
         for (int i = 0; i < S; ++i) {
@@ -281,6 +389,8 @@ __global__ void __launch_bounds__(bwd_threads<S>(), bwd_min_blocks<S>()) k_u_bwd
             }
         }
         stv<S>(lbbar_out + (size_t)v * S, out);
+        if (pbar_out) stv<S>(pbar_out + (size_t)v * S, Pbar);   // several tables: k_u_pair_grad's input
+        const bool one_table = pbar_out == nullptr;
         float ps = 0.0f;
 #pragma unroll
         for (int i = 0; i < S; ++i) ps += Pbar[i];
@@ -302,7 +412,10 @@ __global__ void __launch_bounds__(bwd_threads<S>(), bwd_min_blocks<S>()) k_u_bwd
 #pragma unroll
             for (int b = 0; b < B; ++b) {
                 if (p0 + b >= r1) break;
-                const float *J = edge_table<S>(sm, tb[b]);
+                const float *Js = edge_table<S>(sm, tb[b]);
+                float jr[S <= 4 ? S * S : 1];
+                if constexpr (S <= 4) ldv<S * S>(Js, jr);   // the edge's table in registers
+                const float *J = S <= 4 ? jr : Js;
                 float e[S], sr[S], c[S];
                 const float z = msg_sums<S, true>(J, x[b], e, sr);
 #pragma unroll
@@ -313,103 +426,52 @@ __global__ void __launch_bounds__(bwd_threads<S>(), bwd_min_blocks<S>()) k_u_bwd
                 float ci[S];
 #pragma unroll
                 for (int i = 0; i < S; ++i) ci[i] = __fdividef(Pbar[i], sr[i]) - psz;
-                // the table adjoint lands transposed for a transposed table
-                const bool tr = (tb[b] & 0x80u) != 0;
-                if constexpr (REG) {
-                    if (tr) {
+                // x adjoint terms c_j = e_j sum_i ci_i J_ij, and (one table) the
+                // table adjoint ci_i J_ij e_j, transposed for a transposed table
 #pragma unroll
-                        for (int i = 0; i < S; ++i)
+                for (int i = 0; i < S; ++i)
 #pragma unroll
-                            for (int j = 0; j < S; ++j) {
-                                const float w = ci[i] * J[i * S + j] * e[j];
-                                c[j] += w;
-                                acc[j * S + i] += w;
-                            }
-                    } else {
+                    for (int j = 0; j < S; ++j) c[j] += ci[i] * J[i * S + j];
 #pragma unroll
-                        for (int i = 0; i < S; ++i)
-#pragma unroll
-                            for (int j = 0; j < S; ++j) {
-                                const float w = ci[i] * J[i * S + j] * e[j];
-                                c[j] += w;
-                                acc[i * S + j] += w;
-                            }
-                    }
-                } else {
-                    const int si = tr ? 1 : S, sj = tr ? S : 1;   // entry (i, j) -> i*si + j*sj
-#pragma unroll
-                    for (int i = 0; i < S; ++i)
-#pragma unroll
-                        for (int j = 0; j < S; ++j) {
-                            const float w = ci[i] * J[i * S + j] * e[j];
-                            c[j] += w;
-                            sacc[(i * si + j * sj) * NT + threadIdx.x] += w;
-                        }
-                }
+                for (int j = 0; j < S; ++j) c[j] *= e[j];
+                if (one_table) add_table_adjoint<S, NT, REG>(acc, sacc, ci, J, e, (tb[b] & 0x80u) != 0);
                 stv<S>(xc + (size_t)slot[b] * S, c);
             }
         }
     }
-    // block sum of the accumulators (fixed order), added to this block's
-    // running partial
-    if constexpr (REG) {
-        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-#pragma unroll
-        for (int k = 0; k < S * S; ++k) {
-            float x = acc[k];
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-            if (lane == 0) wred[w][k] = x;
-        }
-        __syncthreads();
-        for (int k = threadIdx.x; k < S * S; k += blockDim.x) {
-            double t = 0.0;
-            for (int ww = 0; ww < NT / 32; ++ww) t += (double)wred[ww][k];
-            epart[(size_t)blockIdx.x * S * S + k] += t;
-        }
-    } else {
-        __syncthreads();
-        for (int k = threadIdx.x; k < S * S; k += blockDim.x) {
-            double t = 0.0;
-            for (int tt = 0; tt < NT; ++tt) t += (double)sacc[k * NT + tt];
-            epart[(size_t)blockIdx.x * S * S + k] += t;
-        }
-    }
+    // several tables: k_u_pair_grad adds the table adjoint
+    if (pbar_out) return;
+    block_partial_add<S, NT, REG>(acc, sacc, wred, epart + (size_t)blockIdx.x * S * S);
 }
 
-// out(s) = add(s) + the x adjoint terms of s's out-edges (initial step)
+// the initial step's end: lbbar_0(s) = add(s) + the x adjoint terms of s's
+// out-edges, then through the log-softmax of the priors:
+// theta_bar = lbbar_0 - softmax(theta) * sum(lbbar_0)
 template <int S>
 __global__ void __launch_bounds__(kUThreads) k_u_bwd_src(const UGraph g, const float *__restrict__ xc,
-                                                         const float *__restrict__ add, float *__restrict__ out) {
+                                                         const float *__restrict__ add, const float *__restrict__ lb0,
+                                                         float *__restrict__ theta_bar) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= g.V) return;
-    float acc[S];
+    float acc[S], lb[S], sum = 0.0f;
     ldv<S>(add + (size_t)s * S, acc);
     sum_slots<S>(xc, g.out_ptr[s], g.out_ptr[s + 1], acc);
-    stv<S>(out + (size_t)s * S, acc);
+    ldv<S>(lb0 + (size_t)s * S, lb);
+#pragma unroll
+    for (int i = 0; i < S; ++i) sum += acc[i];
+#pragma unroll
+    for (int i = 0; i < S; ++i) acc[i] = acc[i] - expf(lb[i]) * sum;
+    stv<S>(theta_bar + (size_t)s * S, acc);
 }
 
-template <int S>
-__global__ void k_u_logsoftmax_bwd(uint32_t V, const float *__restrict__ lb0, const float *__restrict__ gbar,
-                                   float *__restrict__ theta_bar) {
-    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= V) return;
-    float lb[S], gb[S], s = 0.0f;
-    ldv<S>(lb0 + (size_t)v * S, lb);
-    ldv<S>(gbar + (size_t)v * S, gb);
-#pragma unroll
-    for (int i = 0; i < S; ++i) s += gb[i];
-#pragma unroll
-    for (int i = 0; i < S; ++i) gb[i] = gb[i] - expf(lb[i]) * s;
-    stv<S>(theta_bar + (size_t)v * S, gb);
-}
-
-// log_pair_bar[k] = sum of the block partials (fixed order): one block per k
-__global__ void k_u_reduce_pair(const double *__restrict__ epart, uint32_t nblk, uint32_t n, float *__restrict__ out) {
+// log_pair_bar[k] = sum of the block partials (fixed order): one block per
+// entry; partials laid out [table][block][S*S]
+__global__ void k_u_reduce_pair(const double *__restrict__ epart, uint32_t nblk, uint32_t ss, float *__restrict__ out) {
     __shared__ double red[32];
-    const uint32_t k = blockIdx.x;
+    const uint32_t k = blockIdx.x, kt = k / ss, idx = k % ss;
+    const double *base = epart + (size_t)kt * nblk * ss + idx;
     double t = 0.0;
-    for (uint32_t b = threadIdx.x; b < nblk; b += blockDim.x) t += epart[(size_t)b * n + k];
+    for (uint32_t b = threadIdx.x; b < nblk; b += blockDim.x) t += base[(size_t)b * ss];
     t = warp_sum(t);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
     __syncthreads();
@@ -430,11 +492,14 @@ struct bp_unrolled {
     uint8_t *pos_tab = nullptr;
     float *tables = nullptr;
     float *ck_b = nullptr, *ck_q = nullptr;    // [nck][V][S]
-    float *seg_b = nullptr, *seg_q = nullptr;  // [ck][V][S] (slot 0 unused)
+    float *seg_b = nullptr, *seg_q = nullptr;  // [2][ck][V][S] (slot 0 unused), by segment parity
+    cudaStream_t side = nullptr;                // the backward's recompute stream
+    cudaEvent_t ev_fork = nullptr, ev_rec[2] = {nullptr, nullptr}, ev_bwd[2] = {nullptr, nullptr};
     float *pp_b = nullptr, *pp_q = nullptr;    // [2][V][S]
     float *bT = nullptr;
     float *bbar[2] = {nullptr, nullptr};
     float *xc[2] = {nullptr, nullptr};       // [E][S] x adjoint terms, source-sorted slots
+    float *pbar = nullptr;                   // [V][S] node-step adjoint Pbar (several tables only)
     double *epart = nullptr;
     float *theta_buf = nullptr, *gtheta_buf = nullptr, *glogp_buf = nullptr;
     cudaGraphExec_t fwd_exec = nullptr, bwd_exec = nullptr;
@@ -457,9 +522,21 @@ static int u_forward(bp_unrolled *u) {
     k_u_logsoftmax<S><<<gv, kUThreads, 0, st>>>(u->V, u->theta_buf, u->ck_b);
     k_u_gather_q<S><<<gv, kUThreads, 0, st>>>(g, u->ck_b, u->ck_b, u->ck_q);
     BP_CUDA(cudaGetLastError());
-    // state t lives in checkpoint slot t/ck when t % ck == 0, else in pp[t&1]
-    auto loc_b = [&](uint32_t t) { return (t % u->ck == 0) ? u->ck_b + (t / u->ck) * VS : u->pp_b + (t & 1) * VS; };
-    auto loc_q = [&](uint32_t t) { return (t % u->ck == 0) ? u->ck_q + (t / u->ck) * VS : u->pp_q + (t & 1) * VS; };
+    // state t (lb_t, lQ_{t+1}) lives in checkpoint slot t/ck when t % ck == 0;
+    // inside the last segment in its slot of the segment buffer, where the
+    // backward reads it without recomputing; else in pp[t&1]
+    const uint32_t nseg = (u->T + u->ck - 1) / u->ck, t0_last = (nseg - 1) * u->ck;
+    const size_t last_buf = (size_t)((nseg - 1) & 1u) * u->ck;
+    auto loc_b = [&](uint32_t t) {
+        if (t % u->ck == 0) return u->ck_b + (t / u->ck) * VS;
+        if (t > t0_last) return u->seg_b + (last_buf + (t - t0_last)) * VS;
+        return u->pp_b + (t & 1) * VS;
+    };
+    auto loc_q = [&](uint32_t t) {
+        if (t % u->ck == 0) return u->ck_q + (t / u->ck) * VS;
+        if (t > t0_last) return u->seg_q + (last_buf + (t - t0_last)) * VS;
+        return u->pp_q + (t & 1) * VS;
+    };
     for (uint32_t t = 1; t <= u->T; ++t) {
         float *bo = (t == u->T) ? u->bT : loc_b(t);
         float *qo = (t == u->T) ? u->pp_q + (t & 1) * VS : loc_q(t);
@@ -477,41 +554,69 @@ static int u_backward(bp_unrolled *u) {
     const size_t VS = (size_t)u->V * S;
     const unsigned gv = grid_for(u->V, kUThreads);
     constexpr int BT = bwd_threads<S>();
-    const unsigned gb = grid_for(u->V, BT);
+    const unsigned gb = grid_for(u->V, BT * kBwdNodesPerThread);
     cudaStream_t st = u->stream;
-    BP_CUDA(cudaMemsetAsync(u->epart, 0, sizeof(double) * gb * S * S, st));
+    BP_CUDA(cudaMemsetAsync(u->epart, 0, sizeof(double) * u->K * gb * S * S, st));
+    // several tables: the table adjoint of each backward step, one pass per table
+    auto pair_grads = [&](const float *send) {
+        for (uint32_t k = 0; u->K > 1 && k < u->K; ++k)
+            k_u_pair_grad<S><<<gb, BT, 0, st>>>(g, send, u->pbar, k, u->epart + (size_t)k * gb * S * S);
+    };
+    float *pbar = u->K > 1 ? u->pbar : nullptr;
     int bc = 0, rn = 0;
     const float *xc_next = nullptr;   // x adjoint terms of iteration t+1 (none at t = T)
     const uint32_t nseg = (u->T + u->ck - 1) / u->ck;
-    for (int s = (int)nseg - 1; s >= 0; --s) {
-        const uint32_t t0 = (uint32_t)s * u->ck, t_end = std::min(t0 + u->ck, u->T);
+    // Segment s's recompute needs only its checkpoint, so it runs on the side
+    // stream while the adjoint of segment s+1 runs on the main stream; the
+    // two share nothing but the double-buffered segment states (buffer s & 1)
+    auto seg_b = [&](uint32_t s, uint32_t j) { return u->seg_b + ((size_t)(s & 1u) * u->ck + j) * VS; };
+    auto seg_q = [&](uint32_t s, uint32_t j) { return u->seg_q + ((size_t)(s & 1u) * u->ck + j) * VS; };
+    auto recompute = [&](uint32_t s) {
+        const uint32_t t0 = s * u->ck, t_end = std::min(t0 + u->ck, u->T);
         const float *ckb = u->ck_b + (size_t)s * VS, *ckq = u->ck_q + (size_t)s * VS;
-        // recompute states t0+1 .. t_end-1 into seg slots 1..
         for (uint32_t j = 1; j + t0 < t_end; ++j) {
-            const float *bi = (j == 1) ? ckb : u->seg_b + (j - 1) * VS;
-            const float *qi = (j == 1) ? ckq : u->seg_q + (j - 1) * VS;
-            k_u_iter<S><<<gv, kUThreads, 0, st>>>(g, bi, qi, u->seg_b + j * VS, u->seg_q + j * VS);
+            const float *bi = (j == 1) ? ckb : seg_b(s, j - 1);
+            const float *qi = (j == 1) ? ckq : seg_q(s, j - 1);
+            k_u_iter<S><<<gv, kUThreads, 0, u->side>>>(g, bi, qi, seg_b(s, j), seg_q(s, j));
         }
+    };
+    // the last segment's states are the forward's own (u_forward)
+    BP_CUDA(cudaEventRecord(u->ev_fork, st));
+    BP_CUDA(cudaStreamWaitEvent(u->side, u->ev_fork, 0));
+    BP_CUDA(cudaEventRecord(u->ev_rec[(nseg - 1) & 1u], u->side));
+    for (int s = (int)nseg - 1; s >= 0; --s) {
+        if (s >= 1) {
+            // buffer (s-1)&1 was last read by the adjoint of segment s+1
+            if ((uint32_t)s + 1 < nseg) BP_CUDA(cudaStreamWaitEvent(u->side, u->ev_bwd[(s + 1) & 1], 0));
+            recompute((uint32_t)s - 1);
+            BP_CUDA(cudaEventRecord(u->ev_rec[(s - 1) & 1], u->side));
+        }
+        BP_CUDA(cudaStreamWaitEvent(st, u->ev_rec[s & 1], 0));
+        const uint32_t t0 = (uint32_t)s * u->ck, t_end = std::min(t0 + u->ck, u->T);
+        const float *ckq = u->ck_q + (size_t)s * VS;
         for (uint32_t t = t_end; t > t0; --t) {
             const uint32_t j = t - t0 - 1;
-            const float *q_t = (j == 0) ? ckq : u->seg_q + j * VS;           // lQ_t
+            const float *q_t = (j == 0) ? ckq : seg_q((uint32_t)s, j);       // lQ_t
             const float *b_t = (t == u->T) ? u->bT
                                : (t == t_end) ? u->ck_b + (size_t)(s + 1) * VS
-                                              : u->seg_b + (j + 1) * VS;     // lb_t
+                                              : seg_b((uint32_t)s, j + 1);  // lb_t
             k_u_bwd<S><<<gb, BT, 0, st>>>(g, 0, q_t, b_t, u->bbar[bc], xc_next, u->bbar[bc ^ 1], u->xc[rn],
-                                          u->epart);
+                                          u->epart, pbar);
+            pair_grads(q_t);
             bc ^= 1;
             xc_next = u->xc[rn];
             rn ^= 1;
         }
+        BP_CUDA(cudaEventRecord(u->ev_bwd[s & 1], st));
     }
     BP_CUDA(cudaGetLastError());
     // initial step: lQ_1 = lb_0 + sum lm(lb_0); its own x adjoint goes to lb_0
     const float *b0 = u->ck_b;
-    k_u_bwd<S><<<gb, BT, 0, st>>>(g, 1, b0, nullptr, u->bbar[bc], xc_next, u->bbar[bc ^ 1], u->xc[rn], u->epart);
-    k_u_bwd_src<S><<<gv, kUThreads, 0, st>>>(g, u->xc[rn], u->bbar[bc ^ 1], u->bbar[bc]);
-    k_u_logsoftmax_bwd<S><<<gv, kUThreads, 0, st>>>(u->V, b0, u->bbar[bc], u->gtheta_buf);
-    k_u_reduce_pair<<<u->K * S * S, 256, 0, st>>>(u->epart, gb, u->K * S * S, u->glogp_buf);
+    k_u_bwd<S><<<gb, BT, 0, st>>>(g, 1, b0, nullptr, u->bbar[bc], xc_next, u->bbar[bc ^ 1], u->xc[rn], u->epart,
+                                  pbar);
+    pair_grads(b0);
+    k_u_bwd_src<S><<<gv, kUThreads, 0, st>>>(g, u->xc[rn], u->bbar[bc ^ 1], b0, u->gtheta_buf);
+    k_u_reduce_pair<<<u->K * S * S, 256, 0, st>>>(u->epart, gb, S * S, u->glogp_buf);
     BP_CUDA(cudaGetLastError());
     return BP_OK;
 }
@@ -520,13 +625,17 @@ static void u_free(bp_unrolled *u) {
     if (!u) return;
     void *ptrs[] = {u->in_ptr, u->in_src, u->out_ptr, u->pos_out, u->pos_tab, u->tables, u->ck_b, u->ck_q,
                     u->seg_b, u->seg_q, u->pp_b, u->pp_q, u->bT, u->bbar[0], u->bbar[1], u->xc[0],
-                    u->xc[1], u->epart, u->theta_buf, u->gtheta_buf, u->glogp_buf};
+                    u->xc[1], u->epart, u->theta_buf, u->gtheta_buf, u->glogp_buf, u->pbar};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (u->fwd_exec) cudaGraphExecDestroy(u->fwd_exec);
     if (u->bwd_exec) cudaGraphExecDestroy(u->bwd_exec);
     if (u->ev0) cudaEventDestroy(u->ev0);
     if (u->ev1) cudaEventDestroy(u->ev1);
+    cudaEvent_t evs[] = {u->ev_fork, u->ev_rec[0], u->ev_rec[1], u->ev_bwd[0], u->ev_bwd[1]};
+    for (cudaEvent_t e : evs)
+        if (e) cudaEventDestroy(e);
+    if (u->side) cudaStreamDestroy(u->side);
     if (u->own_stream && u->stream) cudaStreamDestroy(u->stream);
     delete u;
 }
@@ -604,13 +713,15 @@ int bp_unrolled_create(bp_unrolled **out, uint32_t V, uint32_t E, uint32_t S, ui
               alloc((void **)&u->pos_tab, (size_t)E) && alloc((void **)&u->tables, sizeof(float) * K * S * S) &&
               alloc((void **)&u->ck_b, sizeof(float) * VS * u->nck) &&
               alloc((void **)&u->ck_q, sizeof(float) * VS * u->nck) &&
-              alloc((void **)&u->seg_b, sizeof(float) * VS * ck) && alloc((void **)&u->seg_q, sizeof(float) * VS * ck) &&
+              alloc((void **)&u->seg_b, sizeof(float) * VS * 2 * ck) &&
+              alloc((void **)&u->seg_q, sizeof(float) * VS * 2 * ck) &&
               alloc((void **)&u->pp_b, sizeof(float) * VS * 2) && alloc((void **)&u->pp_q, sizeof(float) * VS * 2) &&
               alloc((void **)&u->bT, sizeof(float) * VS) && alloc((void **)&u->bbar[0], sizeof(float) * VS) &&
               alloc((void **)&u->bbar[1], sizeof(float) * VS) &&
               alloc((void **)&u->xc[0], sizeof(float) * S * (size_t)E) &&
               alloc((void **)&u->xc[1], sizeof(float) * S * (size_t)E) &&
-              alloc((void **)&u->epart, sizeof(double) * u->nblk * S * S) &&
+              alloc((void **)&u->epart, sizeof(double) * K * u->nblk * S * S) &&
+              (K == 1 || alloc((void **)&u->pbar, sizeof(float) * VS)) &&
               alloc((void **)&u->theta_buf, sizeof(float) * VS) && alloc((void **)&u->gtheta_buf, sizeof(float) * VS) &&
               alloc((void **)&u->glogp_buf, sizeof(float) * K * S * S);
     if (!ok) {
@@ -626,6 +737,15 @@ int bp_unrolled_create(bp_unrolled **out, uint32_t V, uint32_t E, uint32_t S, ui
     }
     cudaEventCreate(&u->ev0);
     cudaEventCreate(&u->ev1);
+    bool evok = cudaStreamCreateWithFlags(&u->side, cudaStreamNonBlocking) == cudaSuccess &&
+                cudaEventCreateWithFlags(&u->ev_fork, cudaEventDisableTiming) == cudaSuccess;
+    for (int i = 0; i < 2 && evok; ++i)
+        evok = cudaEventCreateWithFlags(&u->ev_rec[i], cudaEventDisableTiming) == cudaSuccess &&
+               cudaEventCreateWithFlags(&u->ev_bwd[i], cudaEventDisableTiming) == cudaSuccess;
+    if (!evok) {
+        u_free(u);
+        return set_error(BP_ERR_CUDA, "stream or event creation failed");
+    }
     if (cudaStreamSynchronize(u->stream) != cudaSuccess) {
         u_free(u);
         return set_error(BP_ERR_CUDA, "upload of the unrolled graph failed");

@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--reorder", type=int, default=1,
                     help="1: renumber nodes by out-degree inside the engine (results unchanged)")
     ap.add_argument("--networks", type=int, default=4096)
+    ap.add_argument("--grids", type=int, default=256,
+                    help="unrolled_batch: the first N of the 256 grids (smaller profiling cases)")
     ap.add_argument("--solo-sample", type=int, default=256,
                     help="batched: networks solved one launch sequence each, for the comparison")
     return ap.parse_args()
@@ -518,7 +520,7 @@ def run_unrolled(a, rank, world, batch):
     synth = W.bp.synth
     if batch:
         rng = np.random.default_rng(4)
-        sides = rng.integers(32, 257, size=256)
+        sides = rng.integers(32, 257, size=256)[: a.grids]
         S, T = 8, 20
     else:
         rng = np.random.default_rng(3)

@@ -136,3 +136,32 @@ def test_unrolled_repeated_calls_are_deterministic(bp):
         for x, y in zip(o, out[0]):
             assert torch.equal(x, y)
     eng.close()
+
+
+@pytest.mark.parametrize("S,K", [(4, 3), (8, 2)])
+def test_unrolled_several_tables(bp, S, K):
+    """Several shared tables (edge e uses table tab[e] & 0x7f): forward and
+    both gradients against the fp64 torch reference."""
+    import torch
+    from belief_propagation_b200.unrolled import UnrolledBP, grid_tables, torch_unrolled
+    side, T = 20, 9
+    src, dst, tab = grid_tables(side)
+    rng = np.random.default_rng(S * 10 + K)
+    tab = (tab & 0x80) | rng.integers(0, K, len(tab)).astype(np.uint8)
+    V = side * side
+    theta = torch.tensor(rng.normal(0, 1, (V, S)), dtype=torch.float32, device="cuda", requires_grad=True)
+    W = torch.tensor(rng.normal(0, 0.5, (K, S, S)), dtype=torch.float32, device="cuda", requires_grad=True)
+    labels = torch.tensor(rng.integers(0, S, V), device="cuda")
+    eng = UnrolledBP(V, src, dst, tab, S, T, checkpoint_every=4, num_tables=K)
+    _loss(eng(theta, W), labels).backward()
+    th64 = theta.detach().double().requires_grad_(True)
+    W64 = W.detach().double().requires_grad_(True)
+    b64 = torch_unrolled(th64, W64, src, dst, tab, T)
+    _loss(b64, labels).backward()
+    np.testing.assert_allclose(np.exp(eng(theta, W).detach().cpu().numpy()), np.exp(b64.detach().cpu().numpy()),
+                               atol=1e-4)
+    scale_t = th64.grad.abs().max().item()
+    scale_w = W64.grad.abs().max().item()
+    np.testing.assert_allclose(theta.grad.cpu().numpy(), th64.grad.cpu().numpy(), atol=1e-3 * scale_t + 1e-7)
+    np.testing.assert_allclose(W.grad.cpu().numpy(), W64.grad.cpu().numpy(), rtol=1e-3, atol=1e-3 * scale_w + 1e-7)
+    eng.close()
