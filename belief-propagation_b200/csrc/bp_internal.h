@@ -32,9 +32,9 @@
 namespace bpx {
 
 constexpr int kMaxStates = BP_MAX_STATES;
-// allocated entries past the ends of in_ptr and belief (nodes) and of in_src
-// and msg (edges): the staged iteration kernel copies whole node tiles and
-// 16-byte-rounded edge ranges
+// allocated entries past the ends of in_ptr and belief (nodes) and of
+// in_src, joint and msg (edges): the staged iteration kernel copies whole
+// node tiles and 16-byte-rounded ranges
 constexpr uint32_t kArrayPadNodes = 264;
 constexpr uint32_t kArrayPadEdges = 8;
 

@@ -459,15 +459,15 @@ static int create_impl(bp_graph *g, const bp_graph_desc *d) {
 
     // ---- device arrays
     const size_t ms = g->ms;
-    // padding past the ends: the staged iteration kernel copies whole
-    // 16-byte-aligned ranges and whole node tiles (loopy.cu, k_flood_staged)
+    // padding past the ends: the staged iteration kernel copies whole node
+    // tiles and 16-byte-aligned ranges (loopy.cu)
     if ((st = dev_alloc(g, (void **)&g->in_ptr, sizeof(uint32_t) * ((size_t)V + 1 + kArrayPadNodes)))) return st;
     if ((st = dev_alloc(g, (void **)&g->in_src, sizeof(uint32_t) * ((size_t)E + kArrayPadEdges)))) return st;
     if ((st = dev_alloc(g, (void **)&g->pos_edge, sizeof(uint32_t) * (size_t)E))) return st;
     if ((st = dev_alloc(g, (void **)&g->edge_pos, sizeof(uint32_t) * (size_t)E))) return st;
     if ((st = dev_alloc(g, (void **)&g->node_s, (size_t)V))) return st;
     if (!g->uniform && (st = dev_alloc(g, (void **)&g->pos_dims, (size_t)E))) return st;
-    if ((st = dev_alloc(g, (void **)&g->joint, sizeof(float) * ms * ms * (size_t)E))) return st;
+    if ((st = dev_alloc(g, (void **)&g->joint, sizeof(float) * ms * ms * ((size_t)E + kArrayPadEdges)))) return st;
     if ((st = dev_alloc(g, (void **)&g->belief, sizeof(float) * ms * ((size_t)V + kArrayPadNodes)))) return st;
     for (int k = 0; k < 2; ++k) {
         if ((st = dev_alloc(g, (void **)&g->msg[k], sizeof(float) * ms * ((size_t)E + kArrayPadEdges)))) return st;

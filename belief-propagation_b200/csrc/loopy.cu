@@ -133,18 +133,15 @@ __device__ __forceinline__ void reduce_and_finalize(LoopyCtl *ctl, double *parti
     }
 }
 
+// one 256-node tile of the flooding iteration (see the file header)
 template <int MS, bool UNI, int FU>
-__global__ void __launch_bounds__(flood_nt<MS>(), flood_min_blocks<MS, FU>()) k_flood(const FloodArgs a) {
+__device__ __forceinline__ void flood_tile(const FloodArgs &a, uint32_t tile, bool want, bool serial,
+                                           const float *__restrict__ m_old, float *__restrict__ m_new,
+                                           const float *__restrict__ q_in, float *__restrict__ q_out, uint64_t keep,
+                                           float *sm, double &dsum) {
     constexpr int NT = flood_nt<MS>();
     constexpr uint32_t EMAX = flood_smem_floats<MS>() / MS;
-    __shared__ __align__(16) float sm[EMAX * MS];
-    __shared__ double red[NT / 32];
-    __shared__ bool s_last;
-
-    LoopyCtl *ctl = a.ctl;
-    // the tile's row pointers and this node's belief do not depend on the
-    // control block, so their loads go out together with its read
-    const uint32_t V = a.V, tid = threadIdx.x, v0 = blockIdx.x * NT;
+    const uint32_t V = a.V, tid = threadIdx.x, v0 = tile * NT;
     const uint32_t vend = min(v0 + NT, V);
     const uint32_t e0 = a.in_ptr[v0], e1 = a.in_ptr[vend];
     const uint32_t v = v0 + tid;
@@ -158,20 +155,9 @@ __global__ void __launch_bounds__(flood_nt<MS>(), flood_min_blocks<MS, FU>()) k_
         if (!UNI) S = a.node_s[v];
         ldv<MS, kStream>(a.belief + (size_t)v * MS, b);
     }
-    if (*(volatile uint32_t *)&ctl->done) return;
-    const uint32_t it = ctl->it, ce = ctl->check_every;
-    const bool serial = ctl->serial != 0;
-    const bool want = (ce <= 1) || ((it + 1) % ce == 0);
-    const int mp = (int)((ctl->msg_parity0 + it) & 1u), qp = (int)((ctl->q_parity0 + it) & 1u);
-    const float *__restrict__ m_old = mp ? a.msg1 : a.msg0;
-    float *__restrict__ m_new = mp ? a.msg0 : a.msg1;
-    const float *__restrict__ q_in = qp ? a.q1 : a.q0;
-    float *__restrict__ q_out = qp ? a.q0 : a.q1;
-    const uint64_t keep = l2_evict_last_policy();
     float prod[MS];
 #pragma unroll
     for (int i = 0; i < MS; ++i) prod[i] = 1.0f;
-    double dsum = 0.0;
 
     for (uint32_t c0 = e0; c0 < e1; c0 += EMAX) {
         const uint32_t c1 = min(e1, c0 + EMAX);
@@ -274,6 +260,37 @@ __global__ void __launch_bounds__(flood_nt<MS>(), flood_min_blocks<MS, FU>()) k_
         else stv<MS>(q_out + (size_t)v * MS, qo);
     }
 
+}
+
+// Tiles are taken round-robin (tile = blockIdx.x + k * gridDim.x, a fixed
+// assignment, so the delta sums in a fixed order); with ntiles == gridDim.x
+// each block takes one tile.  A persistent grid (resident blocks per SM x SMs)
+// pays the block's delta reduction and ticket once instead of per tile.
+template <int MS, bool UNI, int FU>
+__global__ void __launch_bounds__(flood_nt<MS>(), flood_min_blocks<MS, FU>()) k_flood(const FloodArgs a,
+                                                                                     uint32_t ntiles) {
+    constexpr int NT = flood_nt<MS>();
+    constexpr uint32_t EMAX = flood_smem_floats<MS>() / MS;
+    __shared__ __align__(16) float sm[EMAX * MS];
+    __shared__ double red[NT / 32];
+    __shared__ bool s_last;
+
+    LoopyCtl *ctl = a.ctl;
+    if (*(volatile uint32_t *)&ctl->done) return;
+    const uint32_t it = ctl->it, ce = ctl->check_every;
+    const bool serial = ctl->serial != 0;
+    const bool want = (ce <= 1) || ((it + 1) % ce == 0);
+    const int mp = (int)((ctl->msg_parity0 + it) & 1u), qp = (int)((ctl->q_parity0 + it) & 1u);
+    const float *__restrict__ m_old = mp ? a.msg1 : a.msg0;
+    float *__restrict__ m_new = mp ? a.msg0 : a.msg1;
+    const float *__restrict__ q_in = qp ? a.q1 : a.q0;
+    float *__restrict__ q_out = qp ? a.q0 : a.q1;
+    const uint64_t keep = l2_evict_last_policy();
+    double dsum = 0.0;
+    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        flood_tile<MS, UNI, FU>(a, tile, want, serial, m_old, m_new, q_in, q_out, keep, sm, dsum);
+        __syncthreads();   // the tile's messages in shared memory are consumed
+    }
     if (!serial) reduce_and_finalize<NT>(ctl, a.partials, dsum, want, red, &s_last);
 }
 
@@ -1078,6 +1095,51 @@ static int staged_grid(const bp_graph *g, unsigned *grid, uint32_t *ntiles) {
     return BP_OK;
 }
 
+// edges in flight per thread of the block-tile kernel: BP_FLOOD_UNROLL=1|2|4
+// overrides the default for 1- and 2-state graphs (every choice gives the
+// same results)
+template <int MS>
+static int block_unroll() {
+    int unroll = flood_unroll<MS>();
+    if constexpr (MS <= 2) {
+        const char *env = getenv("BP_FLOOD_UNROLL");
+        if (env && (env[0] == '1' || env[0] == '2' || env[0] == '4')) unroll = env[0] - '0';
+    }
+    return unroll;
+}
+
+template <int MS, bool UNI, int FU>
+static int resident_blocks(int *bps) {
+    static int cached = 0;
+    if (!cached) BP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cached, k_flood<MS, UNI, FU>, flood_nt<MS>(), 0));
+    *bps = cached;
+    return BP_OK;
+}
+
+// block-tile grid: one block per tile, or (default; BP_FLOOD_PERSIST=0
+// turns it off) a persistent grid of resident blocks x SMs walking the tiles
+template <int MS, bool UNI>
+static int block_tiles(const bp_graph *g, unsigned *grid, uint32_t *ntiles) {
+    *ntiles = grid_for(g->V, flood_nt<MS>());
+    *grid = *ntiles;
+    const char *env = getenv("BP_FLOOD_PERSIST");
+    if (env && env[0] == '0') return BP_OK;
+    int bps = 0, st;
+    if constexpr (MS <= 2) {
+        const int fu = block_unroll<MS>();
+        st = fu == 1 ? resident_blocks<MS, UNI, 1>(&bps)
+                     : (fu == 2 ? resident_blocks<MS, UNI, 2>(&bps) : resident_blocks<MS, UNI, 4>(&bps));
+    } else {
+        st = resident_blocks<MS, UNI, flood_unroll<MS>()>(&bps);
+    }
+    if (st) return st;
+    int dev = 0, sms = 0;
+    BP_CUDA(cudaGetDevice(&dev));
+    BP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    if (bps > 0) *grid = (unsigned)std::min<uint64_t>(*ntiles, (uint64_t)bps * sms);
+    return BP_OK;
+}
+
 template <int MS, bool UNI>
 static int enqueue_node_iterations(bp_graph *g, uint32_t k, bool serial, int variant) {
     constexpr int NT = flood_nt<MS>();
@@ -1098,24 +1160,23 @@ static int enqueue_node_iterations(bp_graph *g, uint32_t k, bool serial, int var
         }
     }
     const bool warp_tiled = variant != BP_KERNEL_BLOCK_TILE;
-    const unsigned grid = warp_tiled ? grid_for(g->V, 256) : grid_for(g->V, NT);
+    unsigned grid = grid_for(g->V, 256);
+    uint32_t ntiles = 0;
+    if (!warp_tiled) {
+        int st = block_tiles<MS, UNI>(g, &grid, &ntiles);
+        if (st) return st;
+    }
     const FloodArgs a = flood_args(g);
     const uint64_t n = (uint64_t)g->E * MS;
-    // edges in flight per lane: BP_FLOOD_UNROLL=1|2|4 overrides the default
-    // for 1- and 2-state graphs (all variants give identical results)
-    int unroll = warp_tiled ? wflood_unroll<MS>() : flood_unroll<MS>();
-    if constexpr (MS <= 2) {
-        const char *env = getenv("BP_FLOOD_UNROLL");
-        if (env && (env[0] == '1' || env[0] == '2' || env[0] == '4')) unroll = env[0] - '0';
-    }
+    const int unroll = warp_tiled ? wflood_unroll<MS>() : block_unroll<MS>();
     for (uint32_t i = 0; i < k; ++i) {
         if (!warp_tiled) {
             if constexpr (MS <= 2) {
-                if (unroll == 1) k_flood<MS, UNI, 1><<<grid, NT, 0, g->stream>>>(a);
-                else if (unroll == 2) k_flood<MS, UNI, 2><<<grid, NT, 0, g->stream>>>(a);
-                else k_flood<MS, UNI, 4><<<grid, NT, 0, g->stream>>>(a);
+                if (unroll == 1) k_flood<MS, UNI, 1><<<grid, NT, 0, g->stream>>>(a, ntiles);
+                else if (unroll == 2) k_flood<MS, UNI, 2><<<grid, NT, 0, g->stream>>>(a, ntiles);
+                else k_flood<MS, UNI, 4><<<grid, NT, 0, g->stream>>>(a, ntiles);
             } else {
-                k_flood<MS, UNI, flood_unroll<MS>()><<<grid, NT, 0, g->stream>>>(a);
+                k_flood<MS, UNI, flood_unroll<MS>()><<<grid, NT, 0, g->stream>>>(a, ntiles);
             }
         } else if constexpr (MS <= 2) {
             if (unroll == 1) k_flood_w<MS, UNI, 1><<<grid, 256, 0, g->stream>>>(a);
@@ -1166,8 +1227,12 @@ static int flood_grid(bp_graph *g, int variant, uint32_t *grid) {
         *grid = gr;
         return st;
     }
-    const int nt = (variant != BP_KERNEL_BLOCK_TILE || g->ms <= 4) ? 256 : 128;
-    *grid = grid_for(g->V, nt);
+    if (variant == BP_KERNEL_BLOCK_TILE) {
+        uint32_t ntiles = 0;
+        auto tiles = [&]() -> int { BP_DISPATCH_MS(g->ms, g->uniform != 0, block_tiles, g, grid, &ntiles); };
+        return tiles();
+    }
+    *grid = grid_for(g->V, 256);
     return BP_OK;
 }
 
@@ -1461,7 +1526,7 @@ static int noalloc_run(uint32_t V, uint32_t E, const uint32_t *in_ptr, const uin
     uint32_t done = 0;
     for (uint32_t launched = 0; launched < max_it && !done; launched += 32) {
         const uint32_t n = std::min<uint32_t>(32, max_it - launched);
-        for (uint32_t i = 0; i < n; ++i) k_flood<MS, true, flood_unroll<MS>()><<<grid, NT, 0, stream>>>(a);
+        for (uint32_t i = 0; i < n; ++i) k_flood<MS, true, flood_unroll<MS>()><<<grid, NT, 0, stream>>>(a, grid);
         BP_CUDA(cudaGetLastError());
         BP_CUDA(cudaMemcpyAsync(&done, &ctl->done, sizeof(done), cudaMemcpyDeviceToHost, stream));
         BP_CUDA(cudaStreamSynchronize(stream));
