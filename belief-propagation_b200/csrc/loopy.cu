@@ -38,9 +38,13 @@ namespace bpx {
 template <int MS> constexpr int flood_nt() { return MS <= 4 ? 256 : 128; }
 template <int MS> constexpr int flood_smem_floats() { return MS <= 2 ? 4096 : 8192; }
 // in-edges per thread per phase-1 round of k_flood (tables held in registers)
-template <int MS> constexpr int flood_unroll() { return MS <= 2 ? 4 : (MS <= 4 ? 2 : 1); }
-// resident blocks per SM the register allocation must allow
-template <int MS, int FU> constexpr int flood_min_blocks() { return MS <= 2 && FU >= 4 ? 4 : 1; }
+template <int MS> constexpr int flood_unroll() { return MS <= 2 ? 1 : (MS <= 4 ? 2 : 1); }
+// resident blocks per SM the register allocation must allow.  With 1-2
+// states, 6 blocks (40 registers, 48 warps) of one edge per thread measured
+// fastest on the 16M-node graph: 0.93 ms against 1.07 ms for 4 blocks of 4
+// edges per thread (64 registers); more warps hide the gather better than
+// more gathers per warp.
+template <int MS, int FU> constexpr int flood_min_blocks() { return MS <= 2 ? (FU >= 4 ? 4 : 6) : 1; }
 
 struct FloodArgs {
     uint32_t V;
@@ -227,7 +231,9 @@ __device__ __forceinline__ void flood_tile(const FloodArgs &a, uint32_t tile, bo
                 combine<MS, UNI>(prod, mm, S);
             }
         }
-        __syncthreads();
+        // the next chunk overwrites the messages; after the last chunk the
+        // caller's barrier at the end of the tile does
+        if (c1 < e1) __syncthreads();
     }
 
     // phase 2b: marginalise (graph.c:1003-1023), then the next send buffer
@@ -266,9 +272,8 @@ __device__ __forceinline__ void flood_tile(const FloodArgs &a, uint32_t tile, bo
 // assignment, so the delta sums in a fixed order); with ntiles == gridDim.x
 // each block takes one tile.  A persistent grid (resident blocks per SM x SMs)
 // pays the block's delta reduction and ticket once instead of per tile.
-template <int MS, bool UNI, int FU>
-__global__ void __launch_bounds__(flood_nt<MS>(), flood_min_blocks<MS, FU>()) k_flood(const FloodArgs a,
-                                                                                     uint32_t ntiles) {
+template <int MS, bool UNI, int FU, int MB = flood_min_blocks<MS, FU>()>
+__global__ void __launch_bounds__(flood_nt<MS>(), MB) k_flood(const FloodArgs a, uint32_t ntiles) {
     constexpr int NT = flood_nt<MS>();
     constexpr uint32_t EMAX = flood_smem_floats<MS>() / MS;
     __shared__ __align__(16) float sm[EMAX * MS];
@@ -1108,12 +1113,46 @@ static int block_unroll() {
     return unroll;
 }
 
-template <int MS, bool UNI, int FU>
-static int resident_blocks(int *bps) {
+// resident blocks per SM the block-tile kernel's registers are capped for:
+// BP_FLOOD_MINB=5|6|8 overrides flood_min_blocks for 1- and 2-state graphs
+// (0 = the default)
+static int block_min_blocks() {
+    const char *env = getenv("BP_FLOOD_MINB");
+    if (env && (env[0] == '5' || env[0] == '6' || env[0] == '8')) return env[0] - '0';
+    return 0;
+}
+
+template <int MS, bool UNI, int FU, int MB>
+static int resident_blocks_mb(int *bps) {
     static int cached = 0;
-    if (!cached) BP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cached, k_flood<MS, UNI, FU>, flood_nt<MS>(), 0));
+    if (!cached)
+        BP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cached, k_flood<MS, UNI, FU, MB>, flood_nt<MS>(), 0));
     *bps = cached;
     return BP_OK;
+}
+
+template <int MS, bool UNI, int FU>
+static int resident_blocks(int *bps) {
+    if constexpr (MS <= 2) {
+        const int mb = block_min_blocks();
+        if (mb == 5) return resident_blocks_mb<MS, UNI, FU, 5>(bps);
+        if (mb == 6) return resident_blocks_mb<MS, UNI, FU, 6>(bps);
+        if (mb == 8) return resident_blocks_mb<MS, UNI, FU, 8>(bps);
+    }
+    return resident_blocks_mb<MS, UNI, FU, flood_min_blocks<MS, FU>()>(bps);
+}
+
+// launch of the block-tile kernel with the register cap block_min_blocks()
+template <int MS, bool UNI, int FU>
+static void launch_block_tiles(unsigned grid, cudaStream_t st, const FloodArgs &a, uint32_t ntiles) {
+    constexpr int NT = flood_nt<MS>();
+    if constexpr (MS <= 2) {
+        const int mb = block_min_blocks();
+        if (mb == 5) return k_flood<MS, UNI, FU, 5><<<grid, NT, 0, st>>>(a, ntiles);
+        if (mb == 6) return k_flood<MS, UNI, FU, 6><<<grid, NT, 0, st>>>(a, ntiles);
+        if (mb == 8) return k_flood<MS, UNI, FU, 8><<<grid, NT, 0, st>>>(a, ntiles);
+    }
+    k_flood<MS, UNI, FU><<<grid, NT, 0, st>>>(a, ntiles);
 }
 
 // block-tile grid: one block per tile, or (default; BP_FLOOD_PERSIST=0
@@ -1172,9 +1211,9 @@ static int enqueue_node_iterations(bp_graph *g, uint32_t k, bool serial, int var
     for (uint32_t i = 0; i < k; ++i) {
         if (!warp_tiled) {
             if constexpr (MS <= 2) {
-                if (unroll == 1) k_flood<MS, UNI, 1><<<grid, NT, 0, g->stream>>>(a, ntiles);
-                else if (unroll == 2) k_flood<MS, UNI, 2><<<grid, NT, 0, g->stream>>>(a, ntiles);
-                else k_flood<MS, UNI, 4><<<grid, NT, 0, g->stream>>>(a, ntiles);
+                if (unroll == 1) launch_block_tiles<MS, UNI, 1>(grid, g->stream, a, ntiles);
+                else if (unroll == 2) launch_block_tiles<MS, UNI, 2>(grid, g->stream, a, ntiles);
+                else launch_block_tiles<MS, UNI, 4>(grid, g->stream, a, ntiles);
             } else {
                 k_flood<MS, UNI, flood_unroll<MS>()><<<grid, NT, 0, g->stream>>>(a, ntiles);
             }
