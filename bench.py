@@ -40,6 +40,17 @@ UNIT = "edge-msg updates/s"
 FALLBACK_HBM_GBS = 6650.0
 
 
+def max_over_ranks(value, dist, device="cuda"):
+    """The largest `value` over all ranks (every rank calls this at the same
+    point); `value` itself when running alone."""
+    if dist is None:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -164,10 +175,21 @@ def reference_sample(iterations=None, target_s=10.0):
     def run(iters):
         if ref is not None:
             g = ref.build_graph(net)
-            t0 = time.perf_counter()
-            ref.lib.init_previous_edge(g)
-            ref.lib.loopy_propagate_until(g, 0.0, iters)
-            dt = time.perf_counter() - t0
+            # graph.c prints "No Convergence" on stdout when the fixed
+            # iteration count runs out; keep stdout for the JSON line
+            sys.stdout.flush()
+            saved = os.dup(1)
+            devnull = os.open(os.devnull, os.O_WRONLY)
+            os.dup2(devnull, 1)
+            try:
+                t0 = time.perf_counter()
+                ref.lib.init_previous_edge(g)
+                ref.lib.loopy_propagate_until(g, 0.0, iters)
+                dt = time.perf_counter() - t0
+            finally:
+                os.dup2(saved, 1)
+                os.close(saved)
+                os.close(devnull)
             ref.lib.graph_destroy(g)
             return dt
         R = O.Restatement()
@@ -263,10 +285,7 @@ def run_batched(a, rank, world):
     torch.cuda.synchronize()
     clk = clocks.stop()
     ms = e0.elapsed_time(e1) / a.steps
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist)
     res = b.results()
     edges = sum(n.E for n in nets)
     updates = float(res["executed"].astype(np.float64) @ np.array([n.E for n in nets], np.float64))
@@ -683,10 +702,7 @@ def main():
     barrier()
     clk = clocks.stop()
     ms = ev0.elapsed_time(ev1)
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist)
     ms_per_step = ms / a.steps
     updates = float(E) * a.iterations * world
     value = updates / (ms_per_step / 1e3)
@@ -742,10 +758,7 @@ def main():
         ems = e0.elapsed_time(e1) / a.e2e_steps
         wall = (time.perf_counter() - t0) / a.e2e_steps * 1e3
         ems = max(ems, wall)
-        if dist is not None:
-            t = torch.tensor([ems], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
+        ems = max_over_ranks(ems, dist)
         e2e = {"value": float(E) * a.iterations * world / (ems / 1e3), "unit": UNIT,
                "h2d_bytes_per_step": int(E * (4 + 4 + 4 * S * S) + V * 4 * S), "d2h_bytes_per_step": int(V * 4 * S),
                "ms_per_step": ems, "phases_wall_ms": {k: round(v, 2) for k, v in phases.items()}}
