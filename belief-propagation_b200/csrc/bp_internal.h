@@ -72,6 +72,7 @@ struct TreeData {
     uint32_t *wave_off = nullptr;      // host [num_waves_total + 1]
     uint32_t *level_wave_begin = nullptr; // host [num_levels + 1] index into waves
     uint32_t total_waves = 0;
+    cudaGraphExec_t exec = nullptr;    // bp_tree's launch sequence, captured once
 };
 
 }  // namespace bpx

@@ -408,6 +408,7 @@ static void free_graph(bp_graph *g) {
         if (p) cudaFree(p);
     for (auto &c : g->loop_graph)
         if (c.exec) cudaGraphExecDestroy(c.exec);
+    if (g->tree.exec) cudaGraphExecDestroy(g->tree.exec);
     if (g->stream) cudaStreamSynchronize(g->stream);
     release_pinned_ctl(g->ctl_host);
     if (g->ev0) cudaEventDestroy(g->ev0);

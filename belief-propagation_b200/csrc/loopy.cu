@@ -745,20 +745,41 @@ __global__ void k_send_from_beliefs(uint32_t E, const uint32_t *__restrict__ in_
 // the reference's own delta: fp32, serial, edge-id order (graph.c:1300-1309).
 // The |diff| values were written in edge-id order by the iteration kernel;
 // zero entries (slots past an edge's x_dim) leave a non-negative sum unchanged.
+// The reference's serial fp32 sum of the |m_old - m_new| terms in edge-id
+// order (graph.c:1300-1309): one dependent chain of adds, so its speed is the
+// add latency.  Thread 0 runs the chain out of shared memory while warps 1-7
+// stage the next 4096 terms into the other buffer.
 __global__ void __launch_bounds__(256) k_delta_serial(LoopyCtl *ctl, const float *__restrict__ absdiff, uint64_t n) {
-    __shared__ __align__(16) float buf[4096];
+    constexpr uint32_t CH = 4096;
+    __shared__ __align__(16) float buf[2][CH];
     if (*(volatile uint32_t *)&ctl->done) return;
     const uint32_t it = ctl->it, ce = ctl->check_every;
     const bool want = (ce <= 1) || ((it + 1) % ce == 0);
     float s = 0.0f;
     if (want) {
-        for (uint64_t base = 0; base < n; base += 4096) {
-            const uint32_t cnt = (uint32_t)min((uint64_t)4096, n - base);
-            for (uint32_t k = threadIdx.x; k < cnt; k += blockDim.x) buf[k] = absdiff[base + k];
-            __syncthreads();
-            if (threadIdx.x == 0) {
-#pragma unroll 8
-                for (uint32_t k = 0; k < cnt; ++k) s = FADD(s, buf[k]);
+        const uint64_t nch = (n + CH - 1) / CH;
+        auto stage = [&](uint64_t c) {   // warps 1-7
+            const uint64_t base = c * CH;
+            const uint32_t cnt = (uint32_t)min((uint64_t)CH, n - base);
+            for (uint32_t k = threadIdx.x - 32; k < cnt; k += blockDim.x - 32) buf[c & 1][k] = __ldcs(absdiff + base + k);
+        };
+        if (threadIdx.x >= 32 && nch) stage(0);
+        __syncthreads();
+        for (uint64_t c = 0; c < nch; ++c) {
+            if (threadIdx.x >= 32) {
+                if (c + 1 < nch) stage(c + 1);
+            } else if (threadIdx.x == 0) {
+                const uint32_t cnt = (uint32_t)min((uint64_t)CH, n - c * CH);
+                const float *b = buf[c & 1];
+                uint32_t k = 0;
+                for (; k + 4 <= cnt; k += 4) {
+                    const float4 v = *reinterpret_cast<const float4 *>(b + k);
+                    s = FADD(s, v.x);
+                    s = FADD(s, v.y);
+                    s = FADD(s, v.z);
+                    s = FADD(s, v.w);
+                }
+                for (; k < cnt; ++k) s = FADD(s, b[k]);
             }
             __syncthreads();
         }

@@ -113,6 +113,7 @@ __global__ void k_tree_marginalize(uint32_t V, const uint32_t *__restrict__ in_p
 
 void tree_clear(bp_graph *g) {
     TreeData &t = g->tree;
+    if (t.exec) cudaGraphExecDestroy(t.exec);
     if (t.d_node_level) cudaFree(t.d_node_level);
     if (t.d_node_lidx) cudaFree(t.d_node_lidx);
     if (t.d_wave_nodes) cudaFree(t.d_wave_nodes);
@@ -274,6 +275,20 @@ int bp_tree_marginalize(bp_graph *g) {
     return dispatch_marginalize(g);
 }
 
+// the whole schedule of c_benchmark/main.c:224-236 on the graph's stream
+static int tree_enqueue(bp_graph *g) {
+    int st;
+    const uint32_t L = g->tree.num_levels;
+    if ((st = bp_tree_reset_visited(g))) return st;
+    if ((st = dispatch_start(g))) return st;
+    for (uint32_t l = 1; l + 1 < L; ++l)
+        if ((st = dispatch_level(g, l))) return st;
+    if ((st = bp_tree_reset_visited(g))) return st;
+    for (uint32_t l = L - 1; l > 0; --l)
+        if ((st = dispatch_level(g, l))) return st;
+    return dispatch_marginalize(g);
+}
+
 int bp_tree(bp_graph *g, bp_tree_result *res) {
     if (!g) return set_error(BP_ERR_INVALID, "null graph");
     int st;
@@ -281,21 +296,32 @@ int bp_tree(bp_graph *g, bp_tree_result *res) {
         uint32_t nl = 0;
         if ((st = bp_tree_build_levels(g, nullptr, &nl))) return st;
     }
-    const uint32_t L = g->tree.num_levels;
+    TreeData &t = g->tree;
+    const uint32_t L = t.num_levels;
+    uint32_t waves = t.level_wave_begin[1] - t.level_wave_begin[0] ? 1 : 0;
+    for (uint32_t l = 1; l + 1 < L; ++l) waves += t.level_wave_begin[l + 1] - t.level_wave_begin[l];
+    for (uint32_t l = L - 1; l > 0; --l) waves += t.level_wave_begin[l + 1] - t.level_wave_begin[l];
+    // one launch per wave: the sequence is fixed for the levels, so it is
+    // captured once into a CUDA graph and replayed
+    if (!t.exec) {
+        cudaGraph_t graph = nullptr;
+        BP_CUDA(cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal));
+        st = tree_enqueue(g);
+        cudaError_t ce = cudaStreamEndCapture(g->stream, &graph);
+        if (st) {
+            if (graph) cudaGraphDestroy(graph);
+            return st;
+        }
+        if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture", __FILE__, __LINE__);
+        cudaError_t ie = cudaGraphInstantiate(&t.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ie != cudaSuccess) {
+            t.exec = nullptr;
+            return cuda_fail(ie, "cudaGraphInstantiate", __FILE__, __LINE__);
+        }
+    }
     BP_CUDA(cudaEventRecord(g->ev0, g->stream));
-    if ((st = bp_tree_reset_visited(g))) return st;
-    if ((st = dispatch_start(g))) return st;
-    uint32_t waves = g->tree.level_wave_begin[1] - g->tree.level_wave_begin[0] ? 1 : 0;
-    for (uint32_t l = 1; l + 1 < L; ++l) {
-        if ((st = dispatch_level(g, l))) return st;
-        waves += g->tree.level_wave_begin[l + 1] - g->tree.level_wave_begin[l];
-    }
-    if ((st = bp_tree_reset_visited(g))) return st;
-    for (uint32_t l = L - 1; l > 0; --l) {
-        if ((st = dispatch_level(g, l))) return st;
-        waves += g->tree.level_wave_begin[l + 1] - g->tree.level_wave_begin[l];
-    }
-    if ((st = dispatch_marginalize(g))) return st;
+    BP_CUDA(cudaGraphLaunch(t.exec, g->stream));
     BP_CUDA(cudaEventRecord(g->ev1, g->stream));
     BP_CUDA(cudaStreamSynchronize(g->stream));
     if (res) {
