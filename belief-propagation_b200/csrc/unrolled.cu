@@ -329,6 +329,71 @@ __global__ void __launch_bounds__(bwd_threads<S>()) k_u_pair_grad(const UGraph g
     block_partial_add<S, NT, REG>(acc, sacc, wred, epart_k + (size_t)blockIdx.x * S * S);
 }
 
+// node step of the adjoint at node v: lbbar_{t-1}(v) (to lbbar_out) and
+// Pbar = the adjoint of the node's summed log-messages, from lbbar_t(v) and
+// lQbar_{t+1}(v) (the gather of iteration t+1's x adjoint terms in v's
+// source-sorted slots); mode 1 is the initial step lQ_1 = lb_0 + lP
+template <int S>
+__device__ __forceinline__ void bwd_node_step(const UGraph &g, int mode, uint32_t v, const float *__restrict__ lb_t,
+                                              const float *__restrict__ lbbar_t, const float *__restrict__ xc_next,
+                                              float *__restrict__ lbbar_out, float *__restrict__ pbar_out,
+                                              float *Pbar) {
+    float gb[S], gq[S];
+#pragma unroll
+    for (int i = 0; i < S; ++i) {
+        gb[i] = 0.0f;
+        gq[i] = 0.0f;
+    }
+    if (lbbar_t) ldv<S>(lbbar_t + (size_t)v * S, gb);
+    if (xc_next) sum_slots<S>(xc_next, g.out_ptr[v], g.out_ptr[v + 1], gq);
+    float out[S];
+    if (mode == 0) {
+        float lb[S], gs = 0.0f;
+        ldv<S>(lb_t + (size_t)v * S, lb);
+#pragma unroll
+        for (int i = 0; i < S; ++i) {
+            gb[i] += gq[i];
+            gs += gb[i];
+        }
+#pragma unroll
+        for (int i = 0; i < S; ++i) {
+            out[i] = gb[i] - expf(lb[i]) * gs;
+            Pbar[i] = out[i] + gq[i];
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < S; ++i) {
+            out[i] = gb[i] + gq[i];
+            Pbar[i] = gq[i];
+        }
+    }
+    stv<S>(lbbar_out + (size_t)v * S, out);
+    if (pbar_out) stv<S>(pbar_out + (size_t)v * S, Pbar);   // several tables: k_u_pair_grad's input
+}
+
+// one in-edge's adjoint quantities: e (source exponentials), ci = rbar_i / s_i
+// and the x adjoint terms c_j = e_j sum_i ci_i J_ij, for table J (the edge's,
+// transposed when the edge says so) and log-state x of the source
+template <int S>
+__device__ __forceinline__ void bwd_edge(const float *J, const float *x, const float *Pbar, float ps, float *e,
+                                         float *ci, float *c) {
+    float sr[S];
+    const float z = msg_sums<S, true>(J, x, e, sr);
+    // rbar_i / s_i = (Pbar_i - (s_i / z) sum(Pbar)) / s_i = Pbar_i / s_i - sum(Pbar) / z
+    // (fast division: s_i and z lie in [1e-37, S max J])
+    const float psz = __fdividef(ps, z);
+#pragma unroll
+    for (int i = 0; i < S; ++i) ci[i] = __fdividef(Pbar[i], sr[i]) - psz;
+#pragma unroll
+    for (int j = 0; j < S; ++j) c[j] = 0.0f;
+#pragma unroll
+    for (int i = 0; i < S; ++i)
+#pragma unroll
+        for (int j = 0; j < S; ++j) c[j] += ci[i] * J[i * S + j];
+#pragma unroll
+    for (int j = 0; j < S; ++j) c[j] *= e[j];
+}
+
 // adjoint of iteration t at node v (mode 0), or of the initial step
 // (mode 1: lQ_1 = lb_0 + lP, messages from send = lb_0), fused with the
 // gather of lQbar_{t+1}(v) from iteration t+1's x adjoint terms (xc_next, in
@@ -359,37 +424,8 @@ __global__ void __launch_bounds__(bwd_threads<S>(), bwd_min_blocks<S>()) k_u_bwd
     // grid-stride over nodes: several nodes per thread share one block
     // reduction of the table adjoint
     for (uint32_t v = blockIdx.x * NT + threadIdx.x; v < g.V; v += gridDim.x * NT) {
-        float gb[S], gq[S], Pbar[S];
-#pragma unroll
-        for (int i = 0; i < S; ++i) {
-            gb[i] = 0.0f;
-            gq[i] = 0.0f;
-        }
-        if (lbbar_t) ldv<S>(lbbar_t + (size_t)v * S, gb);
-        if (xc_next) sum_slots<S>(xc_next, g.out_ptr[v], g.out_ptr[v + 1], gq);
-        float out[S];
-        if (mode == 0) {
-            float lb[S], gs = 0.0f;
-            ldv<S>(lb_t + (size_t)v * S, lb);
-#pragma unroll
-            for (int i = 0; i < S; ++i) {
-                gb[i] += gq[i];
-                gs += gb[i];
-            }
-#pragma unroll
-            for (int i = 0; i < S; ++i) {
-                out[i] = gb[i] - expf(lb[i]) * gs;
-                Pbar[i] = out[i] + gq[i];
-            }
-        } else {
-#pragma unroll
-            for (int i = 0; i < S; ++i) {
-                out[i] = gb[i] + gq[i];
-                Pbar[i] = gq[i];
-            }
-        }
-        stv<S>(lbbar_out + (size_t)v * S, out);
-        if (pbar_out) stv<S>(pbar_out + (size_t)v * S, Pbar);   // several tables: k_u_pair_grad's input
+        float Pbar[S];
+        bwd_node_step<S>(g, mode, v, lb_t, lbbar_t, xc_next, lbbar_out, pbar_out, Pbar);
         const bool one_table = pbar_out == nullptr;
         float ps = 0.0f;
 #pragma unroll
@@ -416,24 +452,8 @@ __global__ void __launch_bounds__(bwd_threads<S>(), bwd_min_blocks<S>()) k_u_bwd
                 float jr[S <= 4 ? S * S : 1];
                 if constexpr (S <= 4) ldv<S * S>(Js, jr);   // the edge's table in registers
                 const float *J = S <= 4 ? jr : Js;
-                float e[S], sr[S], c[S];
-                const float z = msg_sums<S, true>(J, x[b], e, sr);
-#pragma unroll
-                for (int j = 0; j < S; ++j) c[j] = 0.0f;
-                // rbar_i / s_i = (Pbar_i - (s_i / z) sum(Pbar)) / s_i = Pbar_i / s_i - sum(Pbar) / z
-                // (fast division: s_i and z lie in [1e-37, S])
-                const float psz = __fdividef(ps, z);
-                float ci[S];
-#pragma unroll
-                for (int i = 0; i < S; ++i) ci[i] = __fdividef(Pbar[i], sr[i]) - psz;
-                // x adjoint terms c_j = e_j sum_i ci_i J_ij, and (one table) the
-                // table adjoint ci_i J_ij e_j, transposed for a transposed table
-#pragma unroll
-                for (int i = 0; i < S; ++i)
-#pragma unroll
-                    for (int j = 0; j < S; ++j) c[j] += ci[i] * J[i * S + j];
-#pragma unroll
-                for (int j = 0; j < S; ++j) c[j] *= e[j];
+                float e[S], ci[S], c[S];
+                bwd_edge<S>(J, x[b], Pbar, ps, e, ci, c);
                 if (one_table) add_table_adjoint<S, NT, REG>(acc, sacc, ci, J, e, (tb[b] & 0x80u) != 0);
                 stv<S>(xc + (size_t)slot[b] * S, c);
             }
@@ -442,6 +462,133 @@ __global__ void __launch_bounds__(bwd_threads<S>(), bwd_min_blocks<S>()) k_u_bwd
     // several tables: k_u_pair_grad adds the table adjoint
     if (pbar_out) return;
     block_partial_add<S, NT, REG>(acc, sacc, wred, epart + (size_t)blockIdx.x * S * S);
+}
+
+// ---- the one-table adjoint on the tensor cores (5 <= S <= 8) ------------
+// With one shared table J, the table adjoint is J (.) sum over edges of
+// ci (x) e (transposed edges into the transposed entry), i.e. C^T E for the
+// edges' ci and e rows: a GEMM with K = the number of edges.  Each warp stages
+// 32 edges (one per lane) per round in shared memory and accumulates
+// D (16 x 8) += A (16 x 32) B (32 x 8) with four mma.sync m16n8k8 TF32 steps;
+// rows 0-7 of A hold ci of the non-transposed edges, rows 8-15 ci of the
+// transposed ones, B holds e (both zero-padded to 8 states).  Each product
+// is split into TF32 high and low parts (3 MMAs: hi*hi + hi*lo + lo*hi), which
+// keeps it to about fp32 accuracy; accumulation is fp32.  The order of every
+// sum is fixed, so the result is deterministic.
+constexpr int kMmaThreads = 128;
+
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+
+__device__ __forceinline__ void split_tf32(float x, uint32_t &hi, uint32_t &lo) {
+    hi = to_tf32(x);
+    lo = to_tf32(x - __uint_as_float(hi));
+}
+
+__device__ __forceinline__ void mma_tf32_16x8x8(float *d, const uint32_t *a, const uint32_t *b) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+        "{%0, %1, %2, %3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+template <int S>
+__global__ void __launch_bounds__(kMmaThreads, 4) k_u_bwd_mma(const UGraph g, int mode, const float *__restrict__ send,
+                                                             const float *__restrict__ lb_t,
+                                                             const float *__restrict__ lbbar_t,
+                                                             const float *__restrict__ xc_next,
+                                                             float *__restrict__ lbbar_out, float *__restrict__ xc,
+                                                             double *__restrict__ epart) {
+    static_assert(S >= 1 && S <= 8, "states padded to 8");
+    constexpr int NW = kMmaThreads / 32;
+    __shared__ __align__(16) float sm[2 * kUMaxTables * S * S];
+    __shared__ __align__(16) float st_c[NW][32][8];
+    __shared__ __align__(16) float st_e[NW][32][8];
+    __shared__ float st_tr[NW][32];
+    __shared__ float dred[NW][16][8];
+    load_tables_smem<S>(g, sm);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gq = lane >> 2, tq = lane & 3;
+    float d[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    for (uint32_t base = (blockIdx.x * NW + warp) * 32u;; base += gridDim.x * (uint32_t)kMmaThreads) {
+        const uint32_t v = base + lane;
+        const bool active = v < g.V;
+        if (!__any_sync(0xffffffffu, active)) break;
+        float Pbar[S], ps = 0.0f;
+        uint32_t r0 = 0, r1 = 0;
+        if (active) {
+            bwd_node_step<S>(g, mode, v, lb_t, lbbar_t, xc_next, lbbar_out, nullptr, Pbar);
+#pragma unroll
+            for (int i = 0; i < S; ++i) ps += Pbar[i];
+            r0 = g.in_ptr[v];
+            r1 = g.in_ptr[v + 1];
+        }
+        for (uint32_t j = 0;; ++j) {
+            const bool has = r0 + j < r1;
+            if (!__any_sync(0xffffffffu, has)) break;
+            float cs[8], es[8], tr = 0.0f;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                cs[i] = 0.0f;
+                es[i] = 0.0f;
+            }
+            if (has) {
+                const uint32_t p = r0 + j;
+                const uint8_t tab = g.pos_tab[p];
+                float x[S], e[S], ci[S], c[S];
+                ldv<S>(send + (size_t)g.in_src[p] * S, x);
+                bwd_edge<S>(edge_table<S>(sm, tab), x, Pbar, ps, e, ci, c);
+                stv<S>(xc + (size_t)g.pos_out[p] * S, c);
+#pragma unroll
+                for (int i = 0; i < S; ++i) {
+                    cs[i] = ci[i];
+                    es[i] = e[i];
+                }
+                tr = (tab & 0x80u) ? 1.0f : 0.0f;
+            }
+            reinterpret_cast<float4 *>(st_c[warp][lane])[0] = make_float4(cs[0], cs[1], cs[2], cs[3]);
+            reinterpret_cast<float4 *>(st_c[warp][lane])[1] = make_float4(cs[4], cs[5], cs[6], cs[7]);
+            reinterpret_cast<float4 *>(st_e[warp][lane])[0] = make_float4(es[0], es[1], es[2], es[3]);
+            reinterpret_cast<float4 *>(st_e[warp][lane])[1] = make_float4(es[4], es[5], es[6], es[7]);
+            st_tr[warp][lane] = tr;
+            __syncwarp();
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                // A (16 x 8, row-major): a0 (g, t), a1 (g+8, t), a2 (g, t+4), a3 (g+8, t+4)
+                // B (8 x 8, column-major): b0 (t, g), b1 (t+4, g); k indexes the round's edges
+                const int k0 = q * 8 + tq, k1 = k0 + 4;
+                const float c0 = st_c[warp][k0][gq], c1 = st_c[warp][k1][gq];
+                const bool t0 = st_tr[warp][k0] != 0.0f, t1 = st_tr[warp][k1] != 0.0f;
+                const float af[4] = {t0 ? 0.0f : c0, t0 ? c0 : 0.0f, t1 ? 0.0f : c1, t1 ? c1 : 0.0f};
+                const float bf[2] = {st_e[warp][k0][gq], st_e[warp][k1][gq]};
+                uint32_t ah[4], al[4], bh[2], bl[2];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) split_tf32(af[i], ah[i], al[i]);
+#pragma unroll
+                for (int i = 0; i < 2; ++i) split_tf32(bf[i], bh[i], bl[i]);
+                mma_tf32_16x8x8(d, ah, bh);
+                mma_tf32_16x8x8(d, ah, bl);
+                mma_tf32_16x8x8(d, al, bh);
+            }
+            __syncwarp();
+        }
+    }
+    // D (16 x 8): d0 (g, 2t), d1 (g, 2t+1), d2 (g+8, 2t), d3 (g+8, 2t+1)
+    dred[warp][gq][2 * tq] = d[0];
+    dred[warp][gq][2 * tq + 1] = d[1];
+    dred[warp][gq + 8][2 * tq] = d[2];
+    dred[warp][gq + 8][2 * tq + 1] = d[3];
+    __syncthreads();
+    // logJbar[a][b] += J[a][b] * (N[a][b] + T[b][a]), J = exp(table 0)
+    for (int k = threadIdx.x; k < S * S; k += blockDim.x) {
+        const int ra = k / S, cb = k % S;
+        double t = 0.0;
+        for (int w = 0; w < NW; ++w) t += (double)dred[w][ra][cb] + (double)dred[w][8 + cb][ra];
+        epart[(size_t)blockIdx.x * S * S + k] += (double)sm[ra * S + cb] * t;
+    }
 }
 
 // the initial step's end: lbbar_0(s) = add(s) + the x adjoint terms of s's
@@ -554,8 +701,20 @@ static int u_backward(bp_unrolled *u) {
     const size_t VS = (size_t)u->V * S;
     const unsigned gv = grid_for(u->V, kUThreads);
     constexpr int BT = bwd_threads<S>();
-    const unsigned gb = grid_for(u->V, BT * kBwdNodesPerThread);
+    // one table and 5..8 states: the table adjoint on the tensor cores
+    const bool mma = S >= 5 && S <= 8 && u->K == 1;
+    const unsigned gb = mma ? grid_for(u->V, kMmaThreads * 2) : grid_for(u->V, BT * kBwdNodesPerThread);
     cudaStream_t st = u->stream;
+    auto adjoint = [&](int mode, const float *send, const float *b_t, const float *gbar, const float *xn, float *out,
+                       float *xo, float *pb) {
+        if constexpr (S >= 5 && S <= 8) {
+            if (mma) {
+                k_u_bwd_mma<S><<<gb, kMmaThreads, 0, st>>>(g, mode, send, b_t, gbar, xn, out, xo, u->epart);
+                return;
+            }
+        }
+        k_u_bwd<S><<<gb, BT, 0, st>>>(g, mode, send, b_t, gbar, xn, out, xo, u->epart, pb);
+    };
     BP_CUDA(cudaMemsetAsync(u->epart, 0, sizeof(double) * u->K * gb * S * S, st));
     // several tables: the table adjoint of each backward step, one pass per table
     auto pair_grads = [&](const float *send) {
@@ -600,8 +759,7 @@ static int u_backward(bp_unrolled *u) {
             const float *b_t = (t == u->T) ? u->bT
                                : (t == t_end) ? u->ck_b + (size_t)(s + 1) * VS
                                               : seg_b((uint32_t)s, j + 1);  // lb_t
-            k_u_bwd<S><<<gb, BT, 0, st>>>(g, 0, q_t, b_t, u->bbar[bc], xc_next, u->bbar[bc ^ 1], u->xc[rn],
-                                          u->epart, pbar);
+            adjoint(0, q_t, b_t, u->bbar[bc], xc_next, u->bbar[bc ^ 1], u->xc[rn], pbar);
             pair_grads(q_t);
             bc ^= 1;
             xc_next = u->xc[rn];
@@ -612,8 +770,7 @@ static int u_backward(bp_unrolled *u) {
     BP_CUDA(cudaGetLastError());
     // initial step: lQ_1 = lb_0 + sum lm(lb_0); its own x adjoint goes to lb_0
     const float *b0 = u->ck_b;
-    k_u_bwd<S><<<gb, BT, 0, st>>>(g, 1, b0, nullptr, u->bbar[bc], xc_next, u->bbar[bc ^ 1], u->xc[rn], u->epart,
-                                  pbar);
+    adjoint(1, b0, nullptr, u->bbar[bc], xc_next, u->bbar[bc ^ 1], u->xc[rn], pbar);
     pair_grads(b0);
     k_u_bwd_src<S><<<gv, kUThreads, 0, st>>>(g, u->xc[rn], u->bbar[bc ^ 1], b0, u->gtheta_buf);
     k_u_reduce_pair<<<u->K * S * S, 256, 0, st>>>(u->epart, gb, S * S, u->glogp_buf);

@@ -26,7 +26,7 @@ def _loss(lb, labels):
 
 
 @pytest.mark.parametrize("side,S,T,ck", [(16, 4, 30, 5), (32, 8, 20, 5), (24, 3, 7, 3), (16, 4, 30, 1),
-                                         (16, 2, 6, 100)])
+                                         (16, 2, 6, 100), (20, 5, 8, 3), (18, 7, 6, 2), (12, 10, 5, 2)])
 def test_unrolled_matches_torch_reference(bp, side, S, T, ck):
     import torch
     from belief_propagation_b200.unrolled import torch_unrolled
