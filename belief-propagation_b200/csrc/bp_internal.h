@@ -59,6 +59,9 @@ struct LoopyCtl {
     float delta_f, prev_f;
     uint32_t pad0;
     double delta_d, prev_d;
+    // grid barrier of the fused (one-launch) loop: arrivals, generation, and
+    // a flag a block sets when its bounded wait ran out
+    uint32_t bar_count, bar_gen, bar_fail, pad1;
 };
 
 struct TreeData {

@@ -299,6 +299,101 @@ __global__ void __launch_bounds__(flood_nt<MS>(), MB) k_flood(const FloodArgs a,
     if (!serial) reduce_and_finalize<NT>(ctl, a.partials, dsum, want, red, &s_last);
 }
 
+// Small graphs: every iteration in one cooperative launch.  When each tile
+// has a block of its own on the GPU at once (a cooperative launch guarantees
+// co-residency), the per-iteration launch costs more than the iteration, so
+// the blocks loop over the iterations themselves and meet at a grid barrier
+// after each one (its wait bounded by kWaitNs; a block that gives up sets
+// bar_fail, and the others then give up at the next barrier).  Each block
+// keeps a copy of the control block and, after the barrier, sums the
+// per-block delta partials in the same fixed order as k_flood's last block
+// does, so every block takes the same stopping decision and the results equal
+// the one-launch-per-iteration loop's.  Partials are double-buffered by
+// iteration parity: a block writes the next iteration's while others may
+// still read this one's.
+constexpr uint64_t kBarrierWaitNs = 2000000000ull;   // 2 s
+
+__device__ __forceinline__ bool grid_barrier(LoopyCtl *c, uint32_t &gen, uint32_t *s_fail) {
+    __syncthreads();
+    if (threadIdx.x == 0 && !*s_fail) {
+        const uint32_t g0 = gen;
+        __threadfence();
+        if (atomicAdd(&c->bar_count, 1u) == gridDim.x - 1) {
+            c->bar_count = 0;   // untouched until the generation moves
+            __threadfence();
+            atomicExch(&c->bar_gen, g0 + 1u);
+        } else {
+            const uint64_t t0 = global_ns();
+            while (*(volatile uint32_t *)&c->bar_gen == g0) {
+                if (global_ns() - t0 > kBarrierWaitNs) {
+                    *s_fail = 1;
+                    atomicExch(&c->bar_fail, 1u);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    gen += 1;
+    return *s_fail == 0;
+}
+
+template <int MS, bool UNI, int FU, int MB = flood_min_blocks<MS, FU>()>
+__global__ void __launch_bounds__(flood_nt<MS>(), MB) k_flood_fused(const FloodArgs a, uint32_t ntiles) {
+    constexpr int NT = flood_nt<MS>();
+    constexpr uint32_t EMAX = flood_smem_floats<MS>() / MS;
+    __shared__ __align__(16) float sm[EMAX * MS];
+    __shared__ double red[NT / 32];
+    __shared__ LoopyCtl s_ctl;
+    __shared__ uint32_t s_fail;
+
+    LoopyCtl *ctl = a.ctl;
+    if (threadIdx.x == 0) {
+        s_ctl = *ctl;
+        s_fail = 0;
+    }
+    __syncthreads();
+    const uint64_t keep = l2_evict_last_policy();
+    uint32_t gen = 0;
+    while (!s_ctl.done) {
+        const uint32_t it = s_ctl.it, ce = s_ctl.check_every;
+        const bool want = (ce <= 1) || ((it + 1) % ce == 0);
+        const int mp = (int)((s_ctl.msg_parity0 + it) & 1u), qp = (int)((s_ctl.q_parity0 + it) & 1u);
+        const float *__restrict__ m_old = mp ? a.msg1 : a.msg0;
+        float *__restrict__ m_new = mp ? a.msg0 : a.msg1;
+        const float *__restrict__ q_in = qp ? a.q1 : a.q0;
+        float *__restrict__ q_out = qp ? a.q0 : a.q1;
+        double dsum = 0.0;
+        for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+            flood_tile<MS, UNI, FU>(a, tile, want, false, m_old, m_new, q_in, q_out, keep, sm, dsum);
+            __syncthreads();
+        }
+        const double t = block_sum<NT>(dsum, red);
+        double *part = a.partials + (size_t)(it & 1u) * gridDim.x;
+        if (threadIdx.x == 0) part[blockIdx.x] = t;
+        if (!grid_barrier(ctl, gen, &s_fail)) break;
+        double acc = 0.0;
+        for (uint32_t k = threadIdx.x; k < gridDim.x; k += NT) acc += __ldcg(part + k);
+        const double tot = block_sum<NT>(acc, red);
+        if (threadIdx.x == 0) finalize(&s_ctl, want, (float)tot, tot);
+        __syncthreads();
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && !s_fail) {
+        ctl->it = s_ctl.it;
+        ctl->ret = s_ctl.ret;
+        ctl->num_iter = s_ctl.num_iter;
+        ctl->final_i = s_ctl.final_i;
+        ctl->delta_f = s_ctl.delta_f;
+        ctl->prev_f = s_ctl.prev_f;
+        ctl->delta_d = s_ctl.delta_d;
+        ctl->prev_d = s_ctl.prev_d;
+        __threadfence();
+        ctl->done = s_ctl.done;
+    }
+}
+
 // Staged form of k_flood for uniform 2-state graphs (the layout is written
 // for 2 or 4 states; 4-state tables do not leave room for two stages of a
 // 256-node tile).  A persistent
@@ -1307,6 +1402,32 @@ static bool staged_applies(const bp_graph *g, int schedule, bool serial) {
     return (any & 15u) == 0;
 }
 
+// the fused loop: its grid (at most one co-resident block per tile), or 0
+// when the graph has more tiles than the GPU holds blocks at once
+template <int MS, bool UNI>
+static int fused_grid(const bp_graph *g, unsigned *grid, uint32_t *ntiles) {
+    constexpr int FU = flood_unroll<MS>();
+    static int bps = -1;
+    if (bps < 0)
+        BP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_flood_fused<MS, UNI, FU>, flood_nt<MS>(), 0));
+    int dev = 0, sms = 0;
+    BP_CUDA(cudaGetDevice(&dev));
+    BP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    *ntiles = grid_for(g->V, flood_nt<MS>());
+    *grid = (bps > 0 && (uint64_t)*ntiles <= (uint64_t)bps * sms) ? *ntiles : 0u;
+    return BP_OK;
+}
+
+template <int MS, bool UNI>
+static int launch_fused(bp_graph *g, unsigned grid, uint32_t ntiles) {
+    constexpr int FU = flood_unroll<MS>();
+    FloodArgs a = flood_args(g);
+    void *args[] = {(void *)&a, (void *)&ntiles};
+    BP_CUDA(cudaLaunchCooperativeKernel((const void *)k_flood_fused<MS, UNI, FU>, dim3(grid), dim3(flood_nt<MS>()),
+                                        args, 0, g->stream));
+    return BP_OK;
+}
+
 }  // namespace bpx
 
 using namespace bpx;
@@ -1392,6 +1513,20 @@ int bp_loopy(bp_graph *g, const bp_loopy_options *opt, bp_loopy_result *res) {
         return set_error(BP_ERR_INVALID, "staged tiles need a uniform 2-state graph of mean in-degree <= 4.5 and the f64 delta");
     uint32_t grid_blocks = grid_for(g->E, 256);
     if (opt->schedule == BP_SCHEDULE_NODE && (st = flood_grid(g, variant, &grid_blocks))) return st;
+    // small graphs (a co-resident block per tile), node schedule, f64 delta,
+    // block tiles: every iteration in one cooperative launch
+    // (BP_FLOOD_FUSED=0 keeps the launch-per-iteration loop)
+    unsigned fgrid = 0;
+    uint32_t fntiles = 0;
+    {
+        const char *env = getenv("BP_FLOOD_FUSED");
+        if (opt->schedule == BP_SCHEDULE_NODE && !serial && variant == BP_KERNEL_BLOCK_TILE &&
+            !(env && env[0] == '0')) {
+            auto fg = [&]() -> int { BP_DISPATCH_MS(g->ms, g->uniform != 0, fused_grid, g, &fgrid, &fntiles); };
+            if ((st = fg())) return st;
+        }
+    }
+    if (fgrid) grid_blocks = std::max(grid_blocks, 2 * fgrid);   // double-buffered partials
     if ((st = ensure_partials(g, grid_blocks))) return st;
     if (serial && (st = ensure_absdiff(g))) return st;
     if (opt->schedule == BP_SCHEDULE_EDGE && (st = ensure_runs(g))) return st;
@@ -1418,53 +1553,60 @@ int bp_loopy(bp_graph *g, const bp_loopy_options *opt, bp_loopy_result *res) {
         if ((st = gather())) return st;
     }
 
-    // CUDA graph of `chunk` iterations, cached per (schedule, delta, chunk)
-    const uint64_t key = 1ull | ((uint64_t)opt->schedule << 1) | ((uint64_t)serial << 2) |
-                         ((uint64_t)variant << 4) | ((uint64_t)chunk << 8);
-    bp_graph::CachedGraph *slot = nullptr;
-    for (auto &cg : g->loop_graph)
-        if (cg.exec && cg.key == key) slot = &cg;
-    if (!slot) {
-        slot = &g->loop_graph[0];
+    if (fgrid) {
+        BP_CUDA(cudaEventRecord(g->ev0, g->stream));
+        auto lf = [&]() -> int { BP_DISPATCH_MS(g->ms, g->uniform != 0, launch_fused, g, fgrid, fntiles); };
+        if ((st = lf())) return st;
+    } else {
+        // CUDA graph of `chunk` iterations, cached per (schedule, delta, chunk)
+        const uint64_t key = 1ull | ((uint64_t)opt->schedule << 1) | ((uint64_t)serial << 2) |
+                             ((uint64_t)variant << 4) | ((uint64_t)chunk << 8);
+        bp_graph::CachedGraph *slot = nullptr;
         for (auto &cg : g->loop_graph)
-            if (!cg.exec) {
-                slot = &cg;
-                break;
+            if (cg.exec && cg.key == key) slot = &cg;
+        if (!slot) {
+            slot = &g->loop_graph[0];
+            for (auto &cg : g->loop_graph)
+                if (!cg.exec) {
+                    slot = &cg;
+                    break;
+                }
+            if (slot->exec) {
+                cudaGraphExecDestroy(slot->exec);
+                slot->exec = nullptr;
             }
-        if (slot->exec) {
-            cudaGraphExecDestroy(slot->exec);
-            slot->exec = nullptr;
+            cudaGraph_t graph = nullptr;
+            BP_CUDA(cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal));
+            st = enqueue_iterations(g, opt->schedule, chunk, serial, variant);
+            cudaError_t ce2 = cudaStreamEndCapture(g->stream, &graph);
+            if (st) {
+                if (graph) cudaGraphDestroy(graph);
+                return st;
+            }
+            if (ce2 != cudaSuccess) return cuda_fail(ce2, "cudaStreamEndCapture", __FILE__, __LINE__);
+            cudaError_t ie = cudaGraphInstantiate(&slot->exec, graph, 0);
+            cudaGraphDestroy(graph);
+            if (ie != cudaSuccess) return cuda_fail(ie, "cudaGraphInstantiate", __FILE__, __LINE__);
+            slot->key = key;
         }
-        cudaGraph_t graph = nullptr;
-        BP_CUDA(cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal));
-        st = enqueue_iterations(g, opt->schedule, chunk, serial, variant);
-        cudaError_t ce2 = cudaStreamEndCapture(g->stream, &graph);
-        if (st) {
-            if (graph) cudaGraphDestroy(graph);
-            return st;
-        }
-        if (ce2 != cudaSuccess) return cuda_fail(ce2, "cudaStreamEndCapture", __FILE__, __LINE__);
-        cudaError_t ie = cudaGraphInstantiate(&slot->exec, graph, 0);
-        cudaGraphDestroy(graph);
-        if (ie != cudaSuccess) return cuda_fail(ie, "cudaGraphInstantiate", __FILE__, __LINE__);
-        slot->key = key;
-    }
 
-    BP_CUDA(cudaEventRecord(g->ev0, g->stream));
-    for (uint32_t launched = 0; launched < n_launch; launched += chunk) {
-        BP_CUDA(cudaGraphLaunch(slot->exec, g->stream));
-        if (launched + chunk < n_launch) {
-            BP_CUDA(cudaMemcpyAsync(&g->ctl_host->done, &g->ctl->done, sizeof(uint32_t), cudaMemcpyDeviceToHost,
-                                    g->stream));
-            BP_CUDA(cudaStreamSynchronize(g->stream));
-            if (g->ctl_host->done) break;
+        BP_CUDA(cudaEventRecord(g->ev0, g->stream));
+        for (uint32_t launched = 0; launched < n_launch; launched += chunk) {
+            BP_CUDA(cudaGraphLaunch(slot->exec, g->stream));
+            if (launched + chunk < n_launch) {
+                BP_CUDA(cudaMemcpyAsync(&g->ctl_host->done, &g->ctl->done, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                        g->stream));
+                BP_CUDA(cudaStreamSynchronize(g->stream));
+                if (g->ctl_host->done) break;
+            }
         }
     }
     BP_CUDA(cudaEventRecord(g->ev1, g->stream));
     BP_CUDA(cudaMemcpyAsync(g->ctl_host, g->ctl, sizeof(LoopyCtl), cudaMemcpyDeviceToHost, g->stream));
     BP_CUDA(cudaStreamSynchronize(g->stream));
     c = *g->ctl_host;
-    if (c.done == 3) return set_error(BP_ERR_TIMEOUT, "a bounded device wait of the iteration kernel timed out");
+    if (c.done == 3 || c.bar_fail)
+        return set_error(BP_ERR_TIMEOUT, "a bounded device wait of the iteration kernel timed out");
     if (!c.done) return set_error(BP_ERR_STATE, "loop ended without a stop decision (it=%u)", c.it);
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, g->ev0, g->ev1);

@@ -303,3 +303,26 @@ def test_loopy_staged_refuses_inapplicable_graphs(bp, synth):
                 g.loopy(0.0, 3, delta=delta, kernel="staged")
         finally:
             g.close()
+
+
+@pytest.mark.parametrize("case", CASES, ids=lambda c: f"S{c['S']}")
+def test_loopy_fused_loop_matches_launch_loop(bp, synth, restatement, O, monkeypatch, case):
+    """Small graphs run every iteration in one cooperative launch (grid
+    barrier between iterations); the launch-per-iteration loop
+    (BP_FLOOD_FUSED=0) gives the same beliefs, messages, iteration count and
+    f64 delta bit for bit, and the beliefs match the reference's."""
+    net = synth.random_loopy(case["V"], case["E"], case["S"], 0.1, seed=case["seed"] + 100)
+    S = case["S"]
+    for tol, max_it, check, reorder in ((1e-3, 60, 1, False), (0.0, 12, 1, True), (1e-3, 45, 10, False)):
+        fused = gpu_loopy(bp, net, tol, max_it, check_every=check, delta="f64", reorder=reorder)
+        monkeypatch.setenv("BP_FLOOD_FUSED", "0")
+        loop = gpu_loopy(bp, net, tol, max_it, check_every=check, delta="f64", reorder=reorder)
+        monkeypatch.delenv("BP_FLOOD_FUSED")
+        for k in ("iterations", "executed", "delta_f64", "latest"):
+            assert fused[k] == loop[k], k
+        for k in ("beliefs", "slot0", "slot1"):
+            np.testing.assert_array_equal(fused[k], loop[k])
+        if tol == 0.0:
+            ora = restatement.loopy(O.OracleGraph(net), tol, max_it, check_every=check)
+            np.testing.assert_array_equal(fused["beliefs"][:, :S], ora["beliefs"][:, :S])
+            assert fused["iterations"] == ora["ret"]
