@@ -559,6 +559,7 @@ static int create_impl(bp_graph *g, const bp_graph_desc *d) {
         BP_CUDA(cudaMallocAsync((void **)&keys, sizeof(uint32_t) * (V ? V : 1), g->stream));
         BP_CUDA(cudaMallocAsync((void **)&old_to_new, sizeof(uint32_t) * (V ? V : 1), g->stream));
         if ((st = dev_alloc(g, (void **)&g->new_to_old, sizeof(uint32_t) * (size_t)V))) return st;
+        trace.mark("renumber: allocate");
         BP_CUDA(cudaMemsetAsync(deg, 0, sizeof(uint32_t) * V, g->stream));
         if (E) k_out_degree<<<grid_for(E, 256), 256, 0, g->stream>>>((const uint32_t *)src, E, deg);
         if (V) k_degree_keys<<<grid_for(V, 256), 256, 0, g->stream>>>(deg, V, iota);
@@ -577,6 +578,7 @@ static int create_impl(bp_graph *g, const bp_graph_desc *d) {
             k_count_reused<<<1, 1, 0, g->stream>>>(keys, V, deg);
             BP_CUDA(cudaMemcpyAsync(&g->reuse_nodes, deg, sizeof(uint32_t), cudaMemcpyDeviceToHost, g->stream));
         }
+        trace.mark("renumber: degree sort");
         uint32_t *src2 = nullptr, *dst2 = nullptr;
         BP_CUDA(cudaMallocAsync((void **)&src2, sizeof(uint32_t) * (E ? E : 1), g->stream));
         BP_CUDA(cudaMallocAsync((void **)&dst2, sizeof(uint32_t) * (E ? E : 1), g->stream));
