@@ -81,6 +81,54 @@ __global__ void k_tree_wave(const uint32_t *__restrict__ nodes, uint32_t n, uint
     }
 }
 
+// the same step with a warp per node, for waves too small to fill the GPU
+// with a thread per node (their time is one node's chain of dependent
+// loads): the lanes load 32 incoming messages at a time and every lane
+// multiplies them into the buffer in edge order (shuffled from the loading
+// lane), so the product is the thread-per-node one bit for bit; the sends to
+// the out-neighbours go out in parallel, one per lane
+template <int MS, bool UNI>
+__global__ void k_tree_wave_warp(const uint32_t *__restrict__ nodes, uint32_t n, uint32_t level,
+                                 const uint32_t *__restrict__ in_ptr, const uint32_t *__restrict__ out_ptr,
+                                 const uint32_t *__restrict__ out_pos, const uint32_t *__restrict__ out_dst,
+                                 const uint32_t *__restrict__ node_level, const uint32_t *__restrict__ node_lidx,
+                                 const uint8_t *__restrict__ node_s, const float *__restrict__ joint,
+                                 float *__restrict__ msg, const uint8_t *__restrict__ visited) {
+    const uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31;
+    if (k >= n) return;   // the whole warp
+    const uint32_t u = nodes[k];
+    const int S = UNI ? MS : node_s[u];
+    const uint32_t my_idx = node_lidx[u];
+    float buf[MS];
+#pragma unroll
+    for (int i = 0; i < MS; ++i) buf[i] = (UNI || i < S) ? 1.0f : 0.0f;
+    const uint32_t r0 = in_ptr[u], r1 = in_ptr[u + 1];
+    for (uint32_t p0 = r0; p0 < r1; p0 += 32) {
+        float mm[MS];
+#pragma unroll
+        for (int i = 0; i < MS; ++i) mm[i] = 0.0f;
+        if (p0 + lane < r1) ldv<MS>(msg + (size_t)(p0 + lane) * MS, mm);
+        const uint32_t cnt = min(32u, r1 - p0);
+        for (uint32_t j = 0; j < cnt; ++j) {
+            float mj[MS];
+#pragma unroll
+            for (int i = 0; i < MS; ++i) mj[i] = __shfl_sync(0xffffffffu, mm[i], (int)j);
+            combine<MS, UNI>(buf, mj, S);
+        }
+    }
+    for (uint32_t q = out_ptr[u] + lane; q < out_ptr[u + 1]; q += 32) {
+        const uint32_t w = out_dst[q];
+        const bool seen = visited[w] || (node_level[w] == level && node_lidx[w] <= my_idx);
+        if (seen) continue;
+        const uint32_t p = out_pos[q];
+        const int y = UNI ? MS : node_s[w];
+        float m[MS];
+        send_msg<MS, UNI>(joint + (size_t)p * (MS * MS), buf, S, y, m);
+        stv<MS>(msg + (size_t)p * MS, m);
+    }
+}
+
 __global__ void k_mark_visited(const uint32_t *__restrict__ nodes, uint32_t n, uint8_t *__restrict__ visited) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k < n) visited[nodes[k]] = 1;
@@ -181,6 +229,10 @@ static int launch_start(bp_graph *g) {
     return BP_OK;
 }
 
+// waves of at most this many nodes x 32 run a warp per node (148 SMs x 2048
+// threads: the GPU holds them all at once)
+constexpr uint64_t kWarpWaveThreads = 148ull * 2048ull;
+
 template <int MS, bool UNI>
 static int launch_level(bp_graph *g, uint32_t level) {
     TreeData &t = g->tree;
@@ -188,9 +240,14 @@ static int launch_level(bp_graph *g, uint32_t level) {
     for (uint32_t w = w0; w < w1; ++w) {
         const uint32_t lo = t.wave_off[w], n = t.wave_off[w + 1] - lo;
         if (!n) continue;
-        k_tree_wave<MS, UNI><<<grid_for(n, 128), 128, 0, g->stream>>>(
-            t.d_wave_nodes + lo, n, level, g->in_ptr, g->out_ptr, g->out_pos, g->out_dst, t.d_node_level,
-            t.d_node_lidx, g->node_s, g->joint, g->msg[0], g->visited);
+        if ((uint64_t)n * 32 <= kWarpWaveThreads)
+            k_tree_wave_warp<MS, UNI><<<grid_for((uint64_t)n * 32, 128), 128, 0, g->stream>>>(
+                t.d_wave_nodes + lo, n, level, g->in_ptr, g->out_ptr, g->out_pos, g->out_dst, t.d_node_level,
+                t.d_node_lidx, g->node_s, g->joint, g->msg[0], g->visited);
+        else
+            k_tree_wave<MS, UNI><<<grid_for(n, 128), 128, 0, g->stream>>>(
+                t.d_wave_nodes + lo, n, level, g->in_ptr, g->out_ptr, g->out_pos, g->out_dst, t.d_node_level,
+                t.d_node_lidx, g->node_s, g->joint, g->msg[0], g->visited);
         BP_CUDA(cudaGetLastError());
     }
     if (w1 > w0) {
