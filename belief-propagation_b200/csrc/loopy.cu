@@ -52,6 +52,9 @@ struct FloodArgs {
     // with an L2 evict-last policy (renumbered graphs: the nodes with the
     // most out-edges, i.e. the most re-read entries); 0 = none
     uint32_t hot;
+    // one in-edge per thread: 1 = the next round's source id is loaded one
+    // round ahead, 2 = its table and old message too
+    uint32_t pipe;
     const uint32_t *in_ptr, *in_src, *pos_edge;
     const uint8_t *node_s, *pos_dims;
     const float *joint;
@@ -168,6 +171,65 @@ __device__ __forceinline__ void flood_tile(const FloodArgs &a, uint32_t tile, bo
         // phase 1: messages of this chunk of in-edges, FU edges per thread per
         // round with every load of the round issued before the first use, so
         // a thread keeps FU gathers in flight instead of one
+        if (FU == 1 && a.pipe) {
+            // software pipeline, one in-edge per thread per round: the next
+            // round's source id (and with pipe 2 its table and old message)
+            // is in flight while this round's gather completes
+            uint32_t p = c0 + tid;
+            uint32_t s_cur = p < c1 ? __ldcs(a.in_src + p) : 0u;
+            float j_cur[MS * MS], o_cur[MS];
+            const bool deep = a.pipe >= 2 && MS <= 2;
+            if (deep && p < c1) {
+                ldv<MS * MS, kStream>(a.joint + (size_t)p * (MS * MS), j_cur);
+                if (want) ldv<MS, kStream>(m_old + (size_t)p * MS, o_cur);
+            }
+            for (; p < c1; p += NT) {
+                const uint32_t pn = p + NT;
+                const uint32_t s_nxt = pn < c1 ? __ldcs(a.in_src + pn) : 0u;
+                int x = MS, y = MS;
+                if (!UNI) {
+                    const uint8_t d = a.pos_dims[p];
+                    x = d & 15;
+                    y = d >> 4;
+                }
+                float q[MS], m[MS], o[MS];
+                if (s_cur < a.hot) ldv_pol<MS>(q_in + (size_t)s_cur * MS, q, keep);
+                else ldv<MS>(q_in + (size_t)s_cur * MS, q);
+                if (deep) {
+#pragma unroll
+                    for (int k = 0; k < MS; ++k) o[k] = o_cur[k];
+                    float jt[MS * MS];
+#pragma unroll
+                    for (int k = 0; k < MS * MS; ++k) jt[k] = j_cur[k];
+                    if (pn < c1) {
+                        ldv<MS * MS, kStream>(a.joint + (size_t)pn * (MS * MS), j_cur);
+                        if (want) ldv<MS, kStream>(m_old + (size_t)pn * MS, o_cur);
+                    }
+                    send_msg_regs<MS, UNI>(jt, q, x, y, m);
+                } else {
+                    if (want) ldv<MS, kStream>(m_old + (size_t)p * MS, o);
+                    send_msg<MS, UNI>(a.joint + (size_t)p * (MS * MS), q, x, y, m);
+                }
+                if (want) {
+                    float ad[MS];
+#pragma unroll
+                    for (int k = 0; k < MS; ++k) {
+                        float d = 0.0f;
+                        if (UNI || k < x) {
+                            d = FSUB(o[k], m[k]);
+                            if (d != d) d = 0.0f;
+                            d = fabsf(d);
+                        }
+                        ad[k] = d;
+                        dsum += (double)d;
+                    }
+                    if (serial) stv<MS>(a.absdiff + (size_t)__ldg(a.pos_edge + p) * MS, ad);
+                }
+                stv<MS, kStream>(m_new + (size_t)p * MS, m);
+                stv<MS>(sm + (size_t)(p - c0) * MS, m);
+                s_cur = s_nxt;
+            }
+        } else
         for (uint32_t pb = c0 + tid; pb < c1; pb += NT * FU) {
             uint32_t src[FU];
             int x[FU], y[FU];
@@ -1153,6 +1215,12 @@ static FloodArgs flood_args(bp_graph *g) {
     FloodArgs a;
     a.V = g->V;
     a.hot = flood_hot_nodes(g);
+    {
+        // default 1: on the 16M-node graph 0.974 -> 0.932 ms per iteration
+        // (2 spills registers and is slower); BP_FLOOD_PIPE overrides
+        const char *env = getenv("BP_FLOOD_PIPE");
+        a.pipe = env ? (uint32_t)atoi(env) : 1u;
+    }
     a.in_ptr = g->in_ptr;
     a.in_src = g->in_src;
     a.pos_edge = g->pos_edge;
