@@ -35,16 +35,19 @@
 
 namespace bpx {
 
-template <int MS> constexpr int flood_nt() { return MS <= 4 ? 256 : 128; }
-template <int MS> constexpr int flood_smem_floats() { return MS <= 2 ? 4096 : 8192; }
+// nodes per tile (= threads per block) and the shared-memory message buffer;
+// with 1-2 states 128-node tiles (12 blocks per SM) measured 2 % faster than
+// 256-node tiles on the 16M-node graph, 512-node tiles 4 % slower
+template <int MS> constexpr int flood_nt() { return MS <= 2 ? 128 : (MS <= 4 ? 256 : 128); }
+template <int MS> constexpr int flood_smem_floats() { return MS <= 2 ? 2048 : 8192; }
 // in-edges per thread per phase-1 round of k_flood (tables held in registers)
 template <int MS> constexpr int flood_unroll() { return MS <= 2 ? 1 : (MS <= 4 ? 2 : 1); }
 // resident blocks per SM the register allocation must allow.  With 1-2
-// states, 6 blocks (40 registers, 48 warps) of one edge per thread measured
-// fastest on the 16M-node graph: 0.93 ms against 1.07 ms for 4 blocks of 4
-// edges per thread (64 registers); more warps hide the gather better than
-// more gathers per warp.
-template <int MS, int FU> constexpr int flood_min_blocks() { return MS <= 2 ? (FU >= 4 ? 4 : 6) : 1; }
+// states, 48 warps of one edge per thread at 40 registers measured fastest on
+// the 16M-node graph: 0.93 ms against 1.07 ms for 32 warps of 4 edges per
+// thread at 64 registers; more warps hide the gather better than more
+// gathers per warp.
+template <int MS, int FU> constexpr int flood_min_blocks() { return MS <= 2 ? (FU >= 4 ? 8 : 12) : 1; }
 
 struct FloodArgs {
     uint32_t V;
@@ -1298,12 +1301,12 @@ static int block_unroll() {
 }
 
 // resident blocks per SM the block-tile kernel's registers are capped for:
-// BP_FLOOD_MINB=5|6|8 overrides flood_min_blocks for 1- and 2-state graphs
-// (0 = the default)
+// BP_FLOOD_MINB=10|16 overrides flood_min_blocks (12) for 1- and 2-state
+// graphs (resident 128-thread blocks per SM), for sweeps; 0 = the default
 static int block_min_blocks() {
     const char *env = getenv("BP_FLOOD_MINB");
-    if (env && (env[0] == '5' || env[0] == '6' || env[0] == '8')) return env[0] - '0';
-    return 0;
+    const int v = env ? atoi(env) : 0;
+    return (v == 10 || v == 16) ? v : 0;
 }
 
 template <int MS, bool UNI, int FU, int MB>
@@ -1319,9 +1322,8 @@ template <int MS, bool UNI, int FU>
 static int resident_blocks(int *bps) {
     if constexpr (MS <= 2) {
         const int mb = block_min_blocks();
-        if (mb == 5) return resident_blocks_mb<MS, UNI, FU, 5>(bps);
-        if (mb == 6) return resident_blocks_mb<MS, UNI, FU, 6>(bps);
-        if (mb == 8) return resident_blocks_mb<MS, UNI, FU, 8>(bps);
+        if (mb == 10) return resident_blocks_mb<MS, UNI, FU, 10>(bps);
+        if (mb == 16) return resident_blocks_mb<MS, UNI, FU, 16>(bps);
     }
     return resident_blocks_mb<MS, UNI, FU, flood_min_blocks<MS, FU>()>(bps);
 }
@@ -1332,9 +1334,8 @@ static void launch_block_tiles(unsigned grid, cudaStream_t st, const FloodArgs &
     constexpr int NT = flood_nt<MS>();
     if constexpr (MS <= 2) {
         const int mb = block_min_blocks();
-        if (mb == 5) return k_flood<MS, UNI, FU, 5><<<grid, NT, 0, st>>>(a, ntiles);
-        if (mb == 6) return k_flood<MS, UNI, FU, 6><<<grid, NT, 0, st>>>(a, ntiles);
-        if (mb == 8) return k_flood<MS, UNI, FU, 8><<<grid, NT, 0, st>>>(a, ntiles);
+        if (mb == 10) return k_flood<MS, UNI, FU, 10><<<grid, NT, 0, st>>>(a, ntiles);
+        if (mb == 16) return k_flood<MS, UNI, FU, 16><<<grid, NT, 0, st>>>(a, ntiles);
     }
     k_flood<MS, UNI, FU><<<grid, NT, 0, st>>>(a, ntiles);
 }
