@@ -326,3 +326,26 @@ def test_loopy_fused_loop_matches_launch_loop(bp, synth, restatement, O, monkeyp
             ora = restatement.loopy(O.OracleGraph(net), tol, max_it, check_every=check)
             np.testing.assert_array_equal(fused["beliefs"][:, :S], ora["beliefs"][:, :S])
             assert fused["iterations"] == ora["ret"]
+
+
+def test_loopy_fused_loop_mixed_states(bp, synth, restatement, O, monkeypatch):
+    """Mixed state counts through the fused (one-launch) loop: the same
+    results as the launch-per-iteration loop, and the reference's beliefs."""
+    base = synth.random_loopy(700, 2800, 2, 0.1, seed=77)
+    rng = np.random.default_rng(12)
+    S = 6
+    ns = rng.choice(np.array([2, 3, 6], np.uint32), size=base.V)
+    b = rng.random((base.V, S), dtype=np.float32) * (np.arange(S)[None] < ns[:, None])
+    j = rng.random((base.E, S, S), dtype=np.float32)
+    j *= (np.arange(S)[None, :, None] < ns[base.src][:, None, None])
+    j *= (np.arange(S)[None, None, :] < ns[base.dst][:, None, None])
+    net = synth.Network(ns, b.astype(np.float32), base.observed, base.src, base.dst, j.astype(np.float32))
+    fused = gpu_loopy(bp, net, 0.0, 9, delta="f64")
+    monkeypatch.setenv("BP_FLOOD_FUSED", "0")
+    loop = gpu_loopy(bp, net, 0.0, 9, delta="f64")
+    monkeypatch.delenv("BP_FLOOD_FUSED")
+    assert fused["delta_f64"] == loop["delta_f64"] and fused["executed"] == loop["executed"]
+    np.testing.assert_array_equal(fused["beliefs"], loop["beliefs"])
+    np.testing.assert_array_equal(fused["slot0"], loop["slot0"])
+    ora = restatement.loopy(O.OracleGraph(net), 0.0, 9)
+    np.testing.assert_array_equal(fused["beliefs"][:, :S], ora["beliefs"][:, :S])
