@@ -81,22 +81,25 @@ __global__ void k_tree_wave(const uint32_t *__restrict__ nodes, uint32_t n, uint
     }
 }
 
-// the same step with a warp per node, for waves too small to fill the GPU
-// with a thread per node (their time is one node's chain of dependent
-// loads): the lanes load 32 incoming messages at a time and every lane
-// multiplies them into the buffer in edge order (shuffled from the loading
-// lane), so the product is the thread-per-node one bit for bit; the sends to
-// the out-neighbours go out in parallel, one per lane
-template <int MS, bool UNI>
-__global__ void k_tree_wave_warp(const uint32_t *__restrict__ nodes, uint32_t n, uint32_t level,
-                                 const uint32_t *__restrict__ in_ptr, const uint32_t *__restrict__ out_ptr,
-                                 const uint32_t *__restrict__ out_pos, const uint32_t *__restrict__ out_dst,
-                                 const uint32_t *__restrict__ node_level, const uint32_t *__restrict__ node_lidx,
-                                 const uint8_t *__restrict__ node_s, const float *__restrict__ joint,
-                                 float *__restrict__ msg, const uint8_t *__restrict__ visited) {
-    const uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t lane = threadIdx.x & 31;
-    if (k >= n) return;   // the whole warp
+// the same step with a group of G lanes (2 .. 32) per node, for waves too
+// small to fill the GPU with a thread per node (their time is one node's chain
+// of dependent loads): the lanes load G incoming messages at a time and every
+// lane multiplies them into the buffer in edge order (shuffled from the
+// loading lane), so the product is the thread-per-node one bit for bit; the
+// sends to the out-neighbours go out in parallel, one per lane.  A group's
+// lanes share the node, hence its trip counts, so the group mask is converged.
+template <int MS, bool UNI, int G>
+__global__ void k_tree_wave_group(const uint32_t *__restrict__ nodes, uint32_t n, uint32_t level,
+                                  const uint32_t *__restrict__ in_ptr, const uint32_t *__restrict__ out_ptr,
+                                  const uint32_t *__restrict__ out_pos, const uint32_t *__restrict__ out_dst,
+                                  const uint32_t *__restrict__ node_level, const uint32_t *__restrict__ node_lidx,
+                                  const uint8_t *__restrict__ node_s, const float *__restrict__ joint,
+                                  float *__restrict__ msg, const uint8_t *__restrict__ visited) {
+    static_assert(G >= 2 && G <= 32 && (G & (G - 1)) == 0, "group of 2..32 lanes");
+    const uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+    const uint32_t lane = threadIdx.x & (G - 1);
+    const uint32_t gmask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));
+    if (k >= n) return;   // the whole group
     const uint32_t u = nodes[k];
     const int S = UNI ? MS : node_s[u];
     const uint32_t my_idx = node_lidx[u];
@@ -104,20 +107,20 @@ __global__ void k_tree_wave_warp(const uint32_t *__restrict__ nodes, uint32_t n,
 #pragma unroll
     for (int i = 0; i < MS; ++i) buf[i] = (UNI || i < S) ? 1.0f : 0.0f;
     const uint32_t r0 = in_ptr[u], r1 = in_ptr[u + 1];
-    for (uint32_t p0 = r0; p0 < r1; p0 += 32) {
+    for (uint32_t p0 = r0; p0 < r1; p0 += G) {
         float mm[MS];
 #pragma unroll
         for (int i = 0; i < MS; ++i) mm[i] = 0.0f;
         if (p0 + lane < r1) ldv<MS>(msg + (size_t)(p0 + lane) * MS, mm);
-        const uint32_t cnt = min(32u, r1 - p0);
+        const uint32_t cnt = min((uint32_t)G, r1 - p0);
         for (uint32_t j = 0; j < cnt; ++j) {
             float mj[MS];
 #pragma unroll
-            for (int i = 0; i < MS; ++i) mj[i] = __shfl_sync(0xffffffffu, mm[i], (int)j);
+            for (int i = 0; i < MS; ++i) mj[i] = __shfl_sync(gmask, mm[i], (int)j, G);
             combine<MS, UNI>(buf, mj, S);
         }
     }
-    for (uint32_t q = out_ptr[u] + lane; q < out_ptr[u + 1]; q += 32) {
+    for (uint32_t q = out_ptr[u] + lane; q < out_ptr[u + 1]; q += G) {
         const uint32_t w = out_dst[q];
         const bool seen = visited[w] || (node_level[w] == level && node_lidx[w] <= my_idx);
         if (seen) continue;
@@ -229,9 +232,36 @@ static int launch_start(bp_graph *g) {
     return BP_OK;
 }
 
-// waves of at most this many nodes x 32 run a warp per node (148 SMs x 2048
-// threads: the GPU holds them all at once)
-constexpr uint64_t kWarpWaveThreads = 148ull * 2048ull;
+// lanes per node of a wave: the widest group (1, 2, 4, 8, 16 or 32 lanes)
+// that keeps the wave within three residencies of the GPU (148 SMs x 2048
+// threads x 3), so small waves spread each node's chain of dependent loads
+// over a group and big ones keep a thread per node (on a 2M-node random tree
+// budgets from 0.6M to 0.96M threads were equally fast, 2.56M lost 23 %);
+// BP_TREE_GROUP_THREADS overrides the budget (sweeps)
+constexpr uint64_t kGroupWaveThreads = 148ull * 2048ull * 3ull;
+static uint64_t group_wave_threads() {
+    static uint64_t t = 0;
+    if (!t) {
+        const char *env = getenv("BP_TREE_GROUP_THREADS");
+        t = env ? (uint64_t)atoll(env) : kGroupWaveThreads;
+        if (!t) t = 1;
+    }
+    return t;
+}
+static int wave_group(uint64_t n) {
+    const uint64_t t = group_wave_threads();
+    for (int gsz = 32; gsz >= 2; gsz >>= 1)
+        if (n * gsz <= t) return gsz;
+    return 1;
+}
+
+template <int MS, bool UNI, int G>
+static void launch_wave_group(bp_graph *g, const uint32_t *nodes, uint32_t n, uint32_t level) {
+    TreeData &t = g->tree;
+    k_tree_wave_group<MS, UNI, G><<<grid_for((uint64_t)n * G, 128), 128, 0, g->stream>>>(
+        nodes, n, level, g->in_ptr, g->out_ptr, g->out_pos, g->out_dst, t.d_node_level, t.d_node_lidx, g->node_s,
+        g->joint, g->msg[0], g->visited);
+}
 
 template <int MS, bool UNI>
 static int launch_level(bp_graph *g, uint32_t level) {
@@ -240,14 +270,18 @@ static int launch_level(bp_graph *g, uint32_t level) {
     for (uint32_t w = w0; w < w1; ++w) {
         const uint32_t lo = t.wave_off[w], n = t.wave_off[w + 1] - lo;
         if (!n) continue;
-        if ((uint64_t)n * 32 <= kWarpWaveThreads)
-            k_tree_wave_warp<MS, UNI><<<grid_for((uint64_t)n * 32, 128), 128, 0, g->stream>>>(
-                t.d_wave_nodes + lo, n, level, g->in_ptr, g->out_ptr, g->out_pos, g->out_dst, t.d_node_level,
-                t.d_node_lidx, g->node_s, g->joint, g->msg[0], g->visited);
-        else
+        const uint32_t *nodes = t.d_wave_nodes + lo;
+        switch (wave_group(n)) {
+        case 32: launch_wave_group<MS, UNI, 32>(g, nodes, n, level); break;
+        case 16: launch_wave_group<MS, UNI, 16>(g, nodes, n, level); break;
+        case 8: launch_wave_group<MS, UNI, 8>(g, nodes, n, level); break;
+        case 4: launch_wave_group<MS, UNI, 4>(g, nodes, n, level); break;
+        case 2: launch_wave_group<MS, UNI, 2>(g, nodes, n, level); break;
+        default:
             k_tree_wave<MS, UNI><<<grid_for(n, 128), 128, 0, g->stream>>>(
-                t.d_wave_nodes + lo, n, level, g->in_ptr, g->out_ptr, g->out_pos, g->out_dst, t.d_node_level,
-                t.d_node_lidx, g->node_s, g->joint, g->msg[0], g->visited);
+                nodes, n, level, g->in_ptr, g->out_ptr, g->out_pos, g->out_dst, t.d_node_level, t.d_node_lidx,
+                g->node_s, g->joint, g->msg[0], g->visited);
+        }
         BP_CUDA(cudaGetLastError());
     }
     if (w1 > w0) {
