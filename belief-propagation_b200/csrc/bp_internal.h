@@ -62,6 +62,19 @@ struct LoopyCtl {
     // grid barrier of the fused (one-launch) loop: arrivals, generation, and
     // a flag a block sets when its bounded wait ran out
     uint32_t bar_count, bar_gen, bar_fail, pad1;
+    // serial mode: the reference's fp32 sum of a check's |diff| terms lies
+    // in [dlo, dhi] (f64 sum of the terms +- the serial sum's rounding bound),
+    // and in [plo, phi] for the previous check; *_exact = the serial sum
+    // itself was formed (lo == hi == the float).  The terms of each check go
+    // to buffer (check index % 3) of absdiff, ad_stride floats apart.
+    uint64_t n_terms, ad_stride;
+    double dlo, dhi, plo, phi;
+    uint32_t delta_exact, prev_exact, cur_buf, prev_buf;
+    uint32_t serial_sums;  // serial sums formed because the bound could not decide
+    // the one-launch loop: block 0's serial sums for the other blocks
+    uint32_t fb_pform;     // the previous delta was formed too
+    float fb_s, fb_p;
+    uint32_t pad2;
 };
 
 struct TreeData {

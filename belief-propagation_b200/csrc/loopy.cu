@@ -68,16 +68,21 @@ struct FloodArgs {
     LoopyCtl *ctl;
 };
 
-// the reference's stopping rule (graph.c:1313-1318; _acc: :1410-1414) and
-// loop bookkeeping, evaluated by one thread after the iteration's delta
-__device__ void finalize(LoopyCtl *c, bool has_delta, float df, double dd) {
+// the previous check's delta takes the current one's value and bounds
+__device__ __forceinline__ void keep_prev(LoopyCtl *c, float df, double dd) {
+    c->prev_f = df;
+    c->prev_d = dd;
+    c->plo = c->dlo;
+    c->phi = c->dhi;
+    c->prev_exact = c->delta_exact;
+    c->prev_buf = c->cur_buf;
+}
+
+// the reference's loop bookkeeping (graph.c:1313-1318; _acc: :1410-1414)
+// once the stopping rule's outcome `stop` is known; one thread
+__device__ void finalize_with(LoopyCtl *c, bool has_delta, bool stop, float df, double dd) {
     const uint32_t it = c->it, ce = c->check_every, max_it = c->max_it;
-    bool stop = false;
     if (has_delta) {
-        if (c->serial)
-            stop = (df < c->tol) || (fabsf(FSUB(df, c->prev_f)) < c->tol);
-        else
-            stop = (dd < (double)c->tol) || (fabs(dd - c->prev_d) < (double)c->tol);
         c->delta_f = df;
         c->delta_d = dd;
     }
@@ -87,10 +92,7 @@ __device__ void finalize(LoopyCtl *c, bool has_delta, float df, double dd) {
             c->ret = it;
             c->final_i = it;
         } else {
-            if (it < max_it - 1) {
-                c->prev_f = df;
-                c->prev_d = dd;
-            }
+            if (it < max_it - 1) keep_prev(c, df, dd);
             if (it + 1 >= max_it) {
                 c->done = 2;
                 c->ret = max_it;
@@ -104,8 +106,7 @@ __device__ void finalize(LoopyCtl *c, bool has_delta, float df, double dd) {
             c->ret = c->num_iter;
             c->final_i = i_ref;
         } else {
-            c->prev_f = df;
-            c->prev_d = dd;
+            keep_prev(c, df, dd);
             c->num_iter += ce;
             if (i_ref + ce >= max_it) {
                 c->done = 2;
@@ -117,11 +118,207 @@ __device__ void finalize(LoopyCtl *c, bool has_delta, float df, double dd) {
     c->it = it + 1;
 }
 
+// the f64 delta's stopping rule (the reference's, on the f64 sum); one thread
+__device__ void finalize(LoopyCtl *c, bool has_delta, float df, double dd) {
+    const bool stop = has_delta && ((dd < (double)c->tol) || (fabs(dd - c->prev_d) < (double)c->tol));
+    finalize_with(c, has_delta, stop, df, dd);
+}
+
+// ---- the reference's serial fp32 delta, decided from bounds -------------
+//
+// The reference sums the n = E * stride terms t_i = |m_old - m_new| >= 0 in
+// fp32, one add after another in edge-id order (graph.c:1300-1309), and
+// stops when  delta < tol  or  |delta - previous_delta| < tol  (:1313).
+// Each of the n - 1 rounded adds errs by at most u = 2^-24 (+ 2^-52 for the
+// reference's add through double) of its exact result, which is at most
+// (1 + gamma) S, S = sum t_i; so the serial sum s lies within
+// gamma_(n-1) = (n-1)u / (1 - (n-1)u) of S (Higham, Accuracy and Stability of
+// Numerical Algorithms, 2nd ed., section 4.2), plus 2^-149 per add for a
+// subnormal result.  S itself comes from the iteration kernel's f64 sum of
+// the same floats, within 2^-20 relative for n < 2^22.  With directed
+// rounding these give an interval [lo, hi] that contains s.  When the
+// intervals of s and of the previous check's delta decide both comparisons,
+// the outcome is the reference's without forming s; otherwise the serial
+// sum is formed (the previous one too if its interval still straddles), and
+// the decision is exact.  The iteration count, messages and beliefs are
+// therefore the reference's in every case.
+
+__device__ __forceinline__ uint32_t check_index(uint32_t it, uint32_t ce) { return ce <= 1 ? it : (it + 1) / ce - 1; }
+
+__device__ void serial_interval(double T, uint64_t n, double &lo, double &hi) {
+    const double nd = (double)n;
+    const double a = __dmul_ru(nd, 0x1p-24 + 0x1p-52);   // >= (n - 1) u
+    if (!(T <= 1.0e300) || a >= 0.25) {
+        lo = 0.0;
+        hi = __longlong_as_double(0x7ff0000000000000ll);   // +inf: undecided
+        return;
+    }
+    const double gam = __ddiv_ru(a, __dsub_rd(1.0, a));
+    const double dT = __dmul_ru(T, 0x1p-20);
+    const double S_hi = __dadd_ru(T, dT), S_lo = __dsub_rd(T, dT);
+    const double B = __dadd_ru(__dmul_ru(S_hi, gam), __dmul_ru(nd, 0x1p-149));
+    lo = fmax(0.0, __dsub_rd(S_lo, B));
+    hi = __dadd_ru(S_hi, B);
+}
+
+// 1 stop, 0 go on, -1 undecided: s in [lo, hi], previous delta in [plo, phi];
+// when both are exact the reference's own float expression decides
+__device__ int serial_decide(double lo, double hi, bool s_exact, double plo, double phi, bool p_exact, float tol) {
+    if (s_exact && p_exact) {
+        const float s = (float)lo, p = (float)plo;
+        return ((s < tol) || (fabsf(FSUB(s, p)) < tol)) ? 1 : 0;
+    }
+    const double t = (double)tol;
+    if (hi < t) return 1;
+    // |fl(s - p)| < tol, with s - p in [dlo, dhi] and fl() monotone
+    const double dlo = __dsub_rd(lo, phi), dhi = __dsub_ru(hi, plo);
+    const double amax = fmax(fabs(dlo), fabs(dhi));
+    const double amin = (dlo <= 0.0 && dhi >= 0.0) ? 0.0 : fmin(fabs(dlo), fabs(dhi));
+    if (__dadd_ru(__dmul_ru(amax, 1.0 + 0x1p-23), 0x1p-149) < t) return 1;   // fl(x) <= x (1 + 2^-24)
+    if (lo >= t && amin >= t) return 0;                                       // tol is a float
+    return -1;
+}
+
+// the reference's serial fp32 sum of x[0, n) in index order (graph.c:1300-1309):
+// one dependent chain of adds, so its speed is the add latency.  Thread 0 runs
+// the chain out of shared memory while threads 32.. stage the next `ch` terms
+// into the other half of buf (2 * ch floats, 16-byte aligned, ch % 4 == 0).
+// Every thread of the block calls it and gets the sum.
+template <int NT>
+__device__ float block_serial_sum(const float *__restrict__ x, uint64_t n, float *buf, uint32_t ch) {
+    static_assert(NT >= 64, "a staging warp besides the chain's");
+    __shared__ float s_res;
+    const uint64_t nch = (n + ch - 1) / ch;
+    auto stage = [&](uint64_t c) {
+        const uint64_t base = c * ch;
+        const uint32_t cnt = (uint32_t)min((uint64_t)ch, n - base);
+        float *dst = buf + (c & 1) * ch;
+        for (uint32_t k = threadIdx.x - 32; k < cnt; k += NT - 32) dst[k] = __ldcg(x + base + k);
+    };
+    __syncthreads();   // buf is free
+    if (threadIdx.x >= 32 && nch) stage(0);
+    __syncthreads();
+    float s = 0.0f;
+    for (uint64_t c = 0; c < nch; ++c) {
+        if (threadIdx.x >= 32) {
+            if (c + 1 < nch) stage(c + 1);
+        } else if (threadIdx.x == 0) {
+            const uint32_t cnt = (uint32_t)min((uint64_t)ch, n - c * ch);
+            const float *b = buf + (c & 1) * ch;
+            uint32_t k = 0;
+            for (; k + 4 <= cnt; k += 4) {
+                const float4 v = *reinterpret_cast<const float4 *>(b + k);
+                s = FADD(s, v.x);
+                s = FADD(s, v.y);
+                s = FADD(s, v.z);
+                s = FADD(s, v.w);
+            }
+            for (; k < cnt; ++k) s = FADD(s, b[k]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) s_res = s;
+    __syncthreads();
+    return s_res;
+}
+
+// one serial-mode check: s (the reference's delta) in [lo, hi], the
+// previous delta in [plo, phi], d = serial_decide's outcome
+struct SerialCheck {
+    double T, lo, hi, plo, phi;
+    float s;   // (float)T until the serial sum is formed
+    bool s_exact, p_exact;
+    int d;
+    uint32_t sums, cb;
+};
+
+// the decision from the bounds alone; every thread, the same T
+__device__ SerialCheck serial_check(const LoopyCtl *c, double T) {
+    SerialCheck x;
+    x.T = T;
+    x.plo = c->plo;
+    x.phi = c->phi;
+    x.p_exact = c->prev_exact != 0;
+    x.s_exact = false;
+    x.sums = 0;
+    x.cb = check_index(c->it, c->check_every) % 3u;
+    x.s = (float)T;
+    serial_interval(T, c->n_terms, x.lo, x.hi);
+    x.d = serial_decide(x.lo, x.hi, false, x.plo, x.phi, x.p_exact, c->tol);
+    return x;
+}
+
+// an undecided check: form the serial sum, and the previous one if the
+// comparison with it still straddles; every thread of the block
+template <int NT>
+__device__ void serial_form(SerialCheck &x, const LoopyCtl *c, const float *absdiff, float *buf, uint32_t ch) {
+    const uint64_t n = c->n_terms, stride = c->ad_stride;
+    const uint32_t pb = c->prev_buf;
+    x.s = block_serial_sum<NT>(absdiff + (size_t)x.cb * stride, n, buf, ch);
+    x.lo = x.hi = (double)x.s;
+    x.s_exact = true;
+    ++x.sums;
+    x.d = serial_decide(x.lo, x.hi, true, x.plo, x.phi, x.p_exact, c->tol);
+    if (x.d < 0) {
+        const float p = block_serial_sum<NT>(absdiff + (size_t)pb * stride, n, buf, ch);
+        x.plo = x.phi = (double)p;
+        x.p_exact = true;
+        ++x.sums;
+        x.d = serial_decide(x.lo, x.hi, true, x.plo, x.phi, true, c->tol);
+    }
+}
+
+// record the check and run the loop bookkeeping; one thread
+__device__ void serial_commit(LoopyCtl *c, const SerialCheck &x) {
+    if (x.p_exact && !c->prev_exact) {
+        c->prev_f = (float)x.plo;
+        c->plo = c->phi = x.plo;
+        c->prev_exact = 1;
+    }
+    c->dlo = x.lo;
+    c->dhi = x.hi;
+    c->delta_exact = x.s_exact ? 1u : 0u;
+    c->cur_buf = x.cb;
+    c->serial_sums += x.sums;
+    finalize_with(c, true, x.d == 1, x.s, x.T);
+}
+
+// T (valid in thread 0, as block_sum leaves it) to every thread
+__device__ __forceinline__ double broadcast_sum(double T) {
+    __shared__ double s_T;
+    if (threadIdx.x == 0) s_T = T;
+    __syncthreads();
+    T = s_T;
+    __syncthreads();
+    return T;
+}
+
+// serial-mode decision and bookkeeping by one block after a check whose f64
+// term sum is T; every thread of the block calls it and takes the same
+// branches, thread 0 writes c
+template <int NT>
+__device__ void finalize_serial(LoopyCtl *c, bool want, double T, const float *absdiff, float *buf, uint32_t ch) {
+    if (!want) {
+        if (threadIdx.x == 0) finalize_with(c, false, false, 0.0f, 0.0);
+        return;
+    }
+    SerialCheck x = serial_check(c, broadcast_sum(T));
+    if (x.d < 0) serial_form<NT>(x, c, absdiff, buf, ch);
+    __syncthreads();   // every thread has read c
+    if (threadIdx.x == 0) serial_commit(c, x);
+}
+
 // grid-wide deterministic delta: per-block partial, last block sums the
-// partials in a fixed order and finalizes
+// partials in a fixed order and finalizes.  In serial mode the last block
+// decides from the f64 sum and, when the bound cannot, sums the terms every
+// block wrote to absdiff (a fence per writer makes them visible before the
+// ticket); buf/ch: the block's shared staging buffer for that sum.
 template <int NT>
 __device__ __forceinline__ void reduce_and_finalize(LoopyCtl *ctl, double *partials, double dsum, bool want,
-                                                    double *red, bool *s_last) {
+                                                    double *red, bool *s_last, bool serial = false,
+                                                    const float *absdiff = nullptr, float *buf = nullptr,
+                                                    uint32_t ch = 0) {
+    if (serial && want) __threadfence();
     double t = block_sum<NT>(dsum, red);
     if (threadIdx.x == 0) {
         partials[blockIdx.x] = t;
@@ -136,16 +333,25 @@ __device__ __forceinline__ void reduce_and_finalize(LoopyCtl *ctl, double *parti
         double acc = 0.0;
         for (uint32_t k = threadIdx.x; k < gridDim.x; k += NT) acc += __ldcg(partials + k);
         double tot = block_sum<NT>(acc, red);
-        if (threadIdx.x == 0) {
+        if (serial) {
+            finalize_serial<NT>(ctl, want, tot, absdiff, buf, ch);
+            if (threadIdx.x == 0) ctl->counter = 0;
+        } else if (threadIdx.x == 0) {
             ctl->counter = 0;
             finalize(ctl, want, (float)tot, tot);
         }
     }
 }
 
+// this check's |diff| buffer (serial mode), else nullptr
+__device__ __forceinline__ float *check_buffer(const LoopyCtl *c, float *absdiff, uint32_t it, bool want) {
+    if (!c->serial || !want) return nullptr;
+    return absdiff + (size_t)(check_index(it, c->check_every) % 3u) * c->ad_stride;
+}
+
 // one 256-node tile of the flooding iteration (see the file header)
 template <int MS, bool UNI, int FU>
-__device__ __forceinline__ void flood_tile(const FloodArgs &a, uint32_t tile, bool want, bool serial,
+__device__ __forceinline__ void flood_tile(const FloodArgs &a, uint32_t tile, bool want, float *__restrict__ absd,
                                            const float *__restrict__ m_old, float *__restrict__ m_new,
                                            const float *__restrict__ q_in, float *__restrict__ q_out, uint64_t keep,
                                            float *sm, double &dsum) {
@@ -226,7 +432,7 @@ __device__ __forceinline__ void flood_tile(const FloodArgs &a, uint32_t tile, bo
                         ad[k] = d;
                         dsum += (double)d;
                     }
-                    if (serial) stv<MS>(a.absdiff + (size_t)__ldg(a.pos_edge + p) * MS, ad);
+                    if (absd) stv<MS>(absd + (size_t)__ldg(a.pos_edge + p) * MS, ad);
                 }
                 stv<MS, kStream>(m_new + (size_t)p * MS, m);
                 stv<MS>(sm + (size_t)(p - c0) * MS, m);
@@ -280,7 +486,7 @@ __device__ __forceinline__ void flood_tile(const FloodArgs &a, uint32_t tile, bo
                         ad[k] = d;
                         dsum += (double)d;
                     }
-                    if (serial) stv<MS>(a.absdiff + (size_t)__ldg(a.pos_edge + p) * MS, ad);
+                    if (absd) stv<MS>(absd + (size_t)__ldg(a.pos_edge + p) * MS, ad);
                 }
                 stv<MS, kStream>(m_new + (size_t)p * MS, m);
                 stv<MS>(sm + (size_t)(p - c0) * MS, m);
@@ -356,12 +562,14 @@ __global__ void __launch_bounds__(flood_nt<MS>(), MB) k_flood(const FloodArgs a,
     const float *__restrict__ q_in = qp ? a.q1 : a.q0;
     float *__restrict__ q_out = qp ? a.q0 : a.q1;
     const uint64_t keep = l2_evict_last_policy();
+    float *absd = check_buffer(ctl, a.absdiff, it, want);
     double dsum = 0.0;
     for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        flood_tile<MS, UNI, FU>(a, tile, want, serial, m_old, m_new, q_in, q_out, keep, sm, dsum);
+        flood_tile<MS, UNI, FU>(a, tile, want, absd, m_old, m_new, q_in, q_out, keep, sm, dsum);
         __syncthreads();   // the tile's messages in shared memory are consumed
     }
-    if (!serial) reduce_and_finalize<NT>(ctl, a.partials, dsum, want, red, &s_last);
+    reduce_and_finalize<NT>(ctl, a.partials, dsum, want, red, &s_last, serial, a.absdiff, sm,
+                            ((EMAX * MS) / 2) & ~3u);
 }
 
 // Small graphs: every iteration in one cooperative launch.  When each tile
@@ -430,9 +638,10 @@ __global__ void __launch_bounds__(flood_nt<MS>(), MB) k_flood_fused(const FloodA
         float *__restrict__ m_new = mp ? a.msg0 : a.msg1;
         const float *__restrict__ q_in = qp ? a.q1 : a.q0;
         float *__restrict__ q_out = qp ? a.q0 : a.q1;
+        float *absd = check_buffer(&s_ctl, a.absdiff, it, want);
         double dsum = 0.0;
         for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-            flood_tile<MS, UNI, FU>(a, tile, want, false, m_old, m_new, q_in, q_out, keep, sm, dsum);
+            flood_tile<MS, UNI, FU>(a, tile, want, absd, m_old, m_new, q_in, q_out, keep, sm, dsum);
             __syncthreads();
         }
         const double t = block_sum<NT>(dsum, red);
@@ -442,7 +651,41 @@ __global__ void __launch_bounds__(flood_nt<MS>(), MB) k_flood_fused(const FloodA
         double acc = 0.0;
         for (uint32_t k = threadIdx.x; k < gridDim.x; k += NT) acc += __ldcg(part + k);
         const double tot = block_sum<NT>(acc, red);
-        if (threadIdx.x == 0) finalize(&s_ctl, want, (float)tot, tot);
+        if (s_ctl.serial && want) {
+            // every block reaches the same decision from the same sum; when
+            // the bound cannot decide, block 0 forms the serial sums and the
+            // blocks meet once more to read them.  The terms are
+            // triple-buffered by check, so no block overwrites them while
+            // block 0 reads.
+            SerialCheck x = serial_check(&s_ctl, broadcast_sum(tot));
+            if (x.d < 0) {
+                if (blockIdx.x == 0) {
+                    serial_form<NT>(x, &s_ctl, a.absdiff, sm, ((EMAX * MS) / 2) & ~3u);
+                    if (threadIdx.x == 0) {
+                        ctl->fb_s = x.s;
+                        ctl->fb_p = (float)x.plo;
+                        ctl->fb_pform = x.p_exact && !s_ctl.prev_exact;
+                    }
+                }
+                if (!grid_barrier(ctl, gen, &s_fail)) break;
+                if (blockIdx.x != 0) {
+                    x.s = *(volatile float *)&ctl->fb_s;
+                    x.lo = x.hi = (double)x.s;
+                    x.s_exact = true;
+                    x.sums = 1;
+                    if (*(volatile uint32_t *)&ctl->fb_pform) {
+                        x.plo = x.phi = (double)*(volatile float *)&ctl->fb_p;
+                        x.p_exact = true;
+                        x.sums = 2;
+                    }
+                    x.d = serial_decide(x.lo, x.hi, true, x.plo, x.phi, x.p_exact, s_ctl.tol);
+                }
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) serial_commit(&s_ctl, x);
+        } else if (threadIdx.x == 0) {
+            finalize(&s_ctl, want, (float)tot, tot);
+        }
         __syncthreads();
     }
     if (blockIdx.x == 0 && threadIdx.x == 0 && !s_fail) {
@@ -454,6 +697,15 @@ __global__ void __launch_bounds__(flood_nt<MS>(), MB) k_flood_fused(const FloodA
         ctl->prev_f = s_ctl.prev_f;
         ctl->delta_d = s_ctl.delta_d;
         ctl->prev_d = s_ctl.prev_d;
+        ctl->dlo = s_ctl.dlo;
+        ctl->dhi = s_ctl.dhi;
+        ctl->plo = s_ctl.plo;
+        ctl->phi = s_ctl.phi;
+        ctl->delta_exact = s_ctl.delta_exact;
+        ctl->prev_exact = s_ctl.prev_exact;
+        ctl->cur_buf = s_ctl.cur_buf;
+        ctl->prev_buf = s_ctl.prev_buf;
+        ctl->serial_sums = s_ctl.serial_sums;
         __threadfence();
         ctl->done = s_ctl.done;
     }
@@ -740,6 +992,7 @@ __global__ void __launch_bounds__(256) k_flood_w(const FloodArgs a) {
     const uint32_t it = ctl->it, ce = ctl->check_every;
     const bool serial = ctl->serial != 0;
     const bool want = (ce <= 1) || ((it + 1) % ce == 0);
+    float *absd = check_buffer(ctl, a.absdiff, it, want);
     const int mp = (int)((ctl->msg_parity0 + it) & 1u), qp = (int)((ctl->q_parity0 + it) & 1u);
     const float *__restrict__ m_old = mp ? a.msg1 : a.msg0;
     float *__restrict__ m_new = mp ? a.msg0 : a.msg1;
@@ -817,7 +1070,7 @@ __global__ void __launch_bounds__(256) k_flood_w(const FloodArgs a) {
                             ad[k] = d;
                             dsum += (double)d;
                         }
-                        if (serial) stv<MS>(a.absdiff + (size_t)__ldg(a.pos_edge + p) * MS, ad);
+                        if (absd) stv<MS>(absd + (size_t)__ldg(a.pos_edge + p) * MS, ad);
                     }
                     stv<MS, kStream>(m_new + (size_t)p * MS, m);
                     stv<MS>(wsm + (size_t)(p - c0) * MS, m);
@@ -861,7 +1114,8 @@ __global__ void __launch_bounds__(256) k_flood_w(const FloodArgs a) {
             stv<MS>(q_out + (size_t)v * MS, qo);
         }
     }
-    if (!serial) reduce_and_finalize<NT>(ctl, a.partials, dsum, want, red, &s_last);
+    reduce_and_finalize<NT>(ctl, a.partials, dsum, want, red, &s_last, serial, a.absdiff, sm,
+                            ((NW * WE * MS) / 2) & ~3u);
 }
 
 // prologue: Q_1 = b * prod of the latest messages (read_incoming_messages,
@@ -902,49 +1156,21 @@ __global__ void k_send_from_beliefs(uint32_t E, const uint32_t *__restrict__ in_
     stv<MS>(msg + p * MS, m);
 }
 
-// the reference's own delta: fp32, serial, edge-id order (graph.c:1300-1309).
-// The |diff| values were written in edge-id order by the iteration kernel;
-// zero entries (slots past an edge's x_dim) leave a non-negative sum unchanged.
-// The reference's serial fp32 sum of the |m_old - m_new| terms in edge-id
-// order (graph.c:1300-1309): one dependent chain of adds, so its speed is the
-// add latency.  Thread 0 runs the chain out of shared memory while warps 1-7
-// stage the next 4096 terms into the other buffer.
-__global__ void __launch_bounds__(256) k_delta_serial(LoopyCtl *ctl, const float *__restrict__ absdiff, uint64_t n) {
-    constexpr uint32_t CH = 4096;
-    __shared__ __align__(16) float buf[2][CH];
-    if (*(volatile uint32_t *)&ctl->done) return;
-    const uint32_t it = ctl->it, ce = ctl->check_every;
-    const bool want = (ce <= 1) || ((it + 1) % ce == 0);
-    float s = 0.0f;
-    if (want) {
-        const uint64_t nch = (n + CH - 1) / CH;
-        auto stage = [&](uint64_t c) {   // warps 1-7
-            const uint64_t base = c * CH;
-            const uint32_t cnt = (uint32_t)min((uint64_t)CH, n - base);
-            for (uint32_t k = threadIdx.x - 32; k < cnt; k += blockDim.x - 32) buf[c & 1][k] = __ldcs(absdiff + base + k);
-        };
-        if (threadIdx.x >= 32 && nch) stage(0);
-        __syncthreads();
-        for (uint64_t c = 0; c < nch; ++c) {
-            if (threadIdx.x >= 32) {
-                if (c + 1 < nch) stage(c + 1);
-            } else if (threadIdx.x == 0) {
-                const uint32_t cnt = (uint32_t)min((uint64_t)CH, n - c * CH);
-                const float *b = buf[c & 1];
-                uint32_t k = 0;
-                for (; k + 4 <= cnt; k += 4) {
-                    const float4 v = *reinterpret_cast<const float4 *>(b + k);
-                    s = FADD(s, v.x);
-                    s = FADD(s, v.y);
-                    s = FADD(s, v.z);
-                    s = FADD(s, v.w);
-                }
-                for (; k < cnt; ++k) s = FADD(s, b[k]);
-            }
-            __syncthreads();
-        }
+// the reference's `delta` and `previous_delta` at return (graph.c:1300-1318)
+// where the loop decided from bounds without forming them: block 0 sums the
+// last check's terms, block 1 the check's before (serial fp32, edge-id order)
+__global__ void __launch_bounds__(256) k_delta_final(LoopyCtl *ctl, const float *__restrict__ absdiff) {
+    __shared__ __align__(16) float buf[2 * 4096];
+    const LoopyCtl c = *ctl;
+    if (!c.serial || c.done == 0 || c.done == 3 || c.bar_fail) return;
+    const bool prev = blockIdx.x == 1;
+    if (prev ? c.prev_exact : c.delta_exact) return;
+    const uint32_t b = prev ? c.prev_buf : c.cur_buf;
+    const float s = block_serial_sum<256>(absdiff + (size_t)b * c.ad_stride, c.n_terms, buf, 4096);
+    if (threadIdx.x == 0) {
+        if (prev) ctl->prev_f = s;
+        else ctl->delta_f = s;
     }
-    if (threadIdx.x == 0) finalize(ctl, want, s, (double)s);
 }
 
 // ------------------------------------------------------------------------
@@ -1100,11 +1326,13 @@ template <int MS, bool UNI>
 __global__ void __launch_bounds__(256) k_edge_delta(const EdgeArgs a) {
     __shared__ double red[8];
     __shared__ bool s_last;
+    __shared__ __align__(16) float buf[2 * 1024];
     LoopyCtl *ctl = a.ctl;
     if (*(volatile uint32_t *)&ctl->done) return;
     const uint32_t it = ctl->it, ce = ctl->check_every;
     const bool want = (ce <= 1) || ((it + 1) % ce == 0);
     const bool serial = ctl->serial != 0;
+    float *absd = check_buffer(ctl, a.absdiff, it, want);
     // the delta reads the local prev/curr AFTER this iteration's swap (_acc)
     float *prev, *curr;
     edge_roles(a, ctl->acc_edge ? it + 1 : it, prev, curr);
@@ -1127,9 +1355,9 @@ __global__ void __launch_bounds__(256) k_edge_delta(const EdgeArgs a) {
             ad[k] = d;
             dsum += (double)d;
         }
-        if (serial) stv<MS>(a.absdiff + (size_t)a.pos_edge[p] * MS, ad);
+        if (absd) stv<MS>(absd + (size_t)a.pos_edge[p] * MS, ad);
     }
-    if (!serial) reduce_and_finalize<256>(ctl, a.partials, dsum, want, red, &s_last);
+    reduce_and_finalize<256>(ctl, a.partials, dsum, want, red, &s_last, serial, a.absdiff, buf, 1024);
 }
 
 // ---------------------------------------------------------------- driver --
@@ -1151,6 +1379,10 @@ static int ensure_partials(bp_graph *g, uint32_t n) {
     return st;
 }
 
+// floats between the three |diff| buffers of the serial delta (16-byte
+// aligned starts for the serial sum's float4 reads)
+static uint64_t absdiff_stride(const bp_graph *g) { return ((uint64_t)g->E * g->ms + 3u) & ~3ull; }
+
 static int ensure_absdiff(bp_graph *g) {
     if (g->absdiff) return BP_OK;
     for (auto &c : g->loop_graph)
@@ -1159,9 +1391,10 @@ static int ensure_absdiff(bp_graph *g) {
             c.exec = nullptr;
             c.key = 0;
         }
-    int st = dev_alloc(g, (void **)&g->absdiff, sizeof(float) * (size_t)g->ms * ((size_t)g->E + 1));
+    const size_t bytes = sizeof(float) * (3 * (size_t)absdiff_stride(g) + 4);
+    int st = dev_alloc(g, (void **)&g->absdiff, bytes);
     if (st) return st;
-    BP_CUDA(cudaMemsetAsync(g->absdiff, 0, sizeof(float) * (size_t)g->ms * ((size_t)g->E + 1), g->stream));
+    BP_CUDA(cudaMemsetAsync(g->absdiff, 0, bytes, g->stream));
     return BP_OK;
 }
 
@@ -1365,7 +1598,7 @@ static int block_tiles(const bp_graph *g, unsigned *grid, uint32_t *ntiles) {
 }
 
 template <int MS, bool UNI>
-static int enqueue_node_iterations(bp_graph *g, uint32_t k, bool serial, int variant) {
+static int enqueue_node_iterations(bp_graph *g, uint32_t k, bool, int variant) {
     constexpr int NT = flood_nt<MS>();
     if (variant == BP_KERNEL_STAGED_TILE) {
         if constexpr (UNI && MS == 2) {
@@ -1391,7 +1624,6 @@ static int enqueue_node_iterations(bp_graph *g, uint32_t k, bool serial, int var
         if (st) return st;
     }
     const FloodArgs a = flood_args(g);
-    const uint64_t n = (uint64_t)g->E * MS;
     const int unroll = warp_tiled ? wflood_unroll<MS>() : block_unroll<MS>();
     for (uint32_t i = 0; i < k; ++i) {
         if (!warp_tiled) {
@@ -1410,16 +1642,12 @@ static int enqueue_node_iterations(bp_graph *g, uint32_t k, bool serial, int var
             k_flood_w<MS, UNI, wflood_unroll<MS>()><<<grid, 256, 0, g->stream>>>(a);
         }
         BP_CUDA(cudaGetLastError());
-        if (serial) {
-            k_delta_serial<<<1, 256, 0, g->stream>>>(g->ctl, g->absdiff, n);
-            BP_CUDA(cudaGetLastError());
-        }
     }
     return BP_OK;
 }
 
 template <int MS, bool UNI>
-static int enqueue_edge_iterations(bp_graph *g, uint32_t k, bool serial, int) {
+static int enqueue_edge_iterations(bp_graph *g, uint32_t k, bool, int) {
     const EdgeArgs a = edge_args(g);
     const uint64_t n = (uint64_t)g->E * MS;
     for (uint32_t i = 0; i < k; ++i) {
@@ -1429,10 +1657,6 @@ static int enqueue_edge_iterations(bp_graph *g, uint32_t k, bool serial, int) {
         k_edge_normalise_node0<MS><<<1, 32, 0, g->stream>>>(a);
         k_edge_delta<MS, UNI><<<grid_for(g->E, 256), 256, 0, g->stream>>>(a);
         BP_CUDA(cudaGetLastError());
-        if (serial) {
-            k_delta_serial<<<1, 256, 0, g->stream>>>(g->ctl, g->absdiff, n);
-            BP_CUDA(cudaGetLastError());
-        }
     }
     return BP_OK;
 }
@@ -1589,7 +1813,7 @@ int bp_loopy(bp_graph *g, const bp_loopy_options *opt, bp_loopy_result *res) {
     uint32_t fntiles = 0;
     {
         const char *env = getenv("BP_FLOOD_FUSED");
-        if (opt->schedule == BP_SCHEDULE_NODE && !serial && variant == BP_KERNEL_BLOCK_TILE &&
+        if (opt->schedule == BP_SCHEDULE_NODE && variant == BP_KERNEL_BLOCK_TILE &&
             !(env && env[0] == '0')) {
             auto fg = [&]() -> int { BP_DISPATCH_MS(g->ms, g->uniform != 0, fused_grid, g, &fgrid, &fntiles); };
             if ((st = fg())) return st;
@@ -1615,6 +1839,11 @@ int bp_loopy(bp_graph *g, const bp_loopy_options *opt, bp_loopy_result *res) {
     c.tol = opt->tolerance;
     c.prev_f = -1.0f;
     c.prev_d = -1.0;
+    c.n_terms = (uint64_t)g->E * g->ms;
+    c.ad_stride = serial ? absdiff_stride(g) : 0;
+    c.plo = c.phi = -1.0;
+    c.prev_exact = 1;
+    c.delta_exact = 1;
     *g->ctl_host = c;
     BP_CUDA(cudaMemcpyAsync(g->ctl, g->ctl_host, sizeof(LoopyCtl), cudaMemcpyHostToDevice, g->stream));
     if (opt->schedule == BP_SCHEDULE_NODE) {
@@ -1670,6 +1899,12 @@ int bp_loopy(bp_graph *g, const bp_loopy_options *opt, bp_loopy_result *res) {
             }
         }
     }
+    if (serial) {
+        // the returned delta and previous delta where the loop decided
+        // without forming them
+        k_delta_final<<<2, 256, 0, g->stream>>>(g->ctl, g->absdiff);
+        BP_CUDA(cudaGetLastError());
+    }
     BP_CUDA(cudaEventRecord(g->ev1, g->stream));
     BP_CUDA(cudaMemcpyAsync(g->ctl_host, g->ctl, sizeof(LoopyCtl), cudaMemcpyDeviceToHost, g->stream));
     BP_CUDA(cudaStreamSynchronize(g->stream));
@@ -1686,6 +1921,7 @@ int bp_loopy(bp_graph *g, const bp_loopy_options *opt, bp_loopy_result *res) {
     r.previous_delta = serial ? c.prev_f : (float)c.prev_d;
     r.delta_f64 = c.delta_d;
     r.elapsed_ms = ms;
+    r.serial_sums = c.serial_sums;
     if (opt->schedule == BP_SCHEDULE_NODE) g->latest = (int)((c.msg_parity0 + c.it) & 1u);
     if (c.done == 2 && c.final_i == max_it && opt->verbose)
         printf("No Convergence: previous: %f vs current: %f\n", (double)r.previous_delta, (double)r.delta);

@@ -354,7 +354,9 @@ def run_random10k(a, rank, world):
     """The reference-runnable workload: 10,000 nodes, 40,000 uniform random
     edges, 2 states, 10% evidence, tol 1e-3, max 100 iterations, seed 0.  One
     step = init_previous_edge + loopy_propagate_until from the priors with the
-    reference's own serial fp32 delta (same iteration count by construction),
+    reference's own serial fp32 delta stopping rule (decided from the f64 sum
+    and the serial sum's rounding bound, the serial sum formed only where the
+    bound straddles the tolerance; the same iteration count by construction),
     through the drop-in-equivalent device API.  The reference's graph.c runs
     the same full workload on one host core beside it."""
     import torch
@@ -382,7 +384,7 @@ def run_random10k(a, rank, world):
         for _ in range(a.warmup):
             r = step(delta)
         ms = _time_cuda(lambda: step(delta), stream, max(a.steps, 10))
-        res[delta] = (ms, r["iterations"], r["executed"])
+        res[delta] = (ms, r["iterations"], r["executed"], r["serial_sums"])
     b_gpu = g.beliefs()
     g.close()
     cpu = None
@@ -401,13 +403,14 @@ def run_random10k(a, rank, world):
                          f"bit-identical: {bool(np.array_equal(b_ref[:, :2], b_gpu))}"}
     if rank != 0:
         return 0
-    ms, it, ex = res["serial"]
+    ms, it, ex, sums = res["serial"]
     line = {"metric": "loopy BP ms per solve (reference-runnable workload)", "value": ms, "unit": "ms",
             "n_gpus": 1, "steps": max(a.steps, 10), "warmup": a.warmup, "ms_per_step": ms,
             "higher_is_better": False, "scaling": "replicas", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
             "config": {"workload": "10,000 nodes, 40,000 edges, 2 states, 10% evidence, tol 1e-3, max 100, seed 0",
-                       "iterations_returned": it, "iterations_run": ex},
+                       "iterations_returned": it, "iterations_run": ex,
+                       "serial_sums_formed": sums},
             "us_per_iteration": 1e3 * ms / max(ex, 1), "edge_msg_updates_per_s": 40_000 * ex / (ms / 1e3),
             "f64_delta_ms_per_solve": res["f64"][0], "cpu_baseline": cpu}
     print(json.dumps(line), flush=True)

@@ -117,8 +117,11 @@ typedef struct {
     int32_t converged;        /* 1 when the stopping rule fired */
     float delta;              /* the reference's `delta` at return */
     float previous_delta;     /* the reference's `previous_delta` at return */
-    double delta_f64;
+    double delta_f64;         /* f64 sum of the last check's |diff| terms */
     float elapsed_ms;         /* device time of the iteration loop */
+    uint32_t serial_sums;     /* serial fp32 delta: checks whose stopping decision
+                               * needed the serial sum formed (the error bound of
+                               * the f64 sum could not decide) */
 } bp_loopy_result;
 
 typedef struct {

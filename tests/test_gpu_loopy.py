@@ -32,12 +32,19 @@ def gpu_loopy(bp, net, tol, max_it, check_every=1, schedule="node", delta="seria
     return out
 
 
-def assert_same(gpu, ora, S):
+def assert_same(gpu, ora, S, deltas=True):
+    """Bit-exact beliefs and messages, the same return value and iterations;
+    with the serial delta (gpu_loopy's default) also the reference's returned
+    fp32 delta and previous delta."""
     np.testing.assert_array_equal(gpu["beliefs"][:, :S], ora["beliefs"][:, :S])
     np.testing.assert_array_equal(gpu["slot1"][:, :S], ora["prev_arr"][:, :S])
     np.testing.assert_array_equal(gpu["slot0"][:, :S], ora["cur_arr"][:, :S])
     assert gpu["iterations"] == ora["ret"]
     assert gpu["executed"] == ora["executed"]
+    if deltas:
+        assert np.float32(gpu["delta"]) == np.float32(ora["delta"]), (gpu["delta"], ora["delta"])
+        assert np.float32(gpu["previous_delta"]) == np.float32(ora["prev_delta"]), \
+            (gpu["previous_delta"], ora["prev_delta"])
 
 
 def test_loopy_random_10k_matches_reference_fixture(bp):
@@ -275,7 +282,7 @@ def test_loopy_staged_kernel_parity(bp, synth, restatement, O, name):
     for tol, max_it, check, reorder in ((0.0, 7, 1, False), (0.0, 25, 10, False), (0.0, 6, 1, True)):
         ora = restatement.loopy(O.OracleGraph(net), tol, max_it, check_every=check)
         gpu = gpu_loopy(bp, net, tol, max_it, check_every=check, delta="f64", kernel="staged", reorder=reorder)
-        assert_same(gpu, ora, 2)
+        assert_same(gpu, ora, 2, deltas=False)
 
 
 def test_loopy_staged_matches_block_kernel_with_tolerance(bp, synth):
@@ -349,3 +356,72 @@ def test_loopy_fused_loop_mixed_states(bp, synth, restatement, O, monkeypatch):
     np.testing.assert_array_equal(fused["slot0"], loop["slot0"])
     ora = restatement.loopy(O.OracleGraph(net), 0.0, 9)
     np.testing.assert_array_equal(fused["beliefs"][:, :S], ora["beliefs"][:, :S])
+
+
+def _oracle_deltas(restatement, O, net, n, schedule="node", check=1):
+    """The reference's fp32 delta after each of the first n checks."""
+    og = O.OracleGraph(net)
+    return [np.float32(restatement.loopy(og, 0.0, k * check, check_every=check, schedule=schedule)["delta"])
+            for k in range(1, n + 1)]
+
+
+def _straddling_tolerances(restatement, O, net, deltas, sched, check):
+    """Tolerances whose stopping decision at some check k is certain to need
+    the serial sum: the serial sum's rounding bound (about 0.1 % of the delta
+    here) straddles the tolerance in one comparison while the other is decided
+    by a wide margin, and the reference's loop does reach check k."""
+    out = []
+    for k in range(1, len(deltas)):
+        dk, dp = deltas[k], deltas[k - 1]
+        diff = np.float32(abs(np.float32(dk - dp)))
+        cands = []
+        if diff > np.float32(1.05) * dk:      # delta < tol straddles, |delta - prev| >= tol surely
+            cands = [dk, np.nextafter(dk, np.float32(np.inf))]
+        elif dk > np.float32(1.05) * diff:    # |delta - prev| < tol straddles, delta >= tol surely
+            cands = [diff, np.nextafter(diff, np.float32(np.inf))]
+        for tol in cands:
+            ora = restatement.loopy(O.OracleGraph(net), float(tol), 200, check_every=check, schedule=sched)
+            if ora["executed"] >= (k + 1) * check:
+                out.append((float(tol), ora))
+        if len(out) >= 4:
+            break
+    return out
+
+
+@pytest.mark.parametrize("path", ["fused", "launch_loop", "warp", "edge", "node_acc"])
+def test_serial_delta_bound_straddling_tolerance(bp, synth, restatement, O, monkeypatch, path):
+    """The serial fp32 delta is decided from the f64 sum and the serial sum's
+    rounding bound, and formed only when that interval straddles the
+    tolerance.  Tolerances at the reference's own delta (or its step) at a
+    check make the interval straddle on purpose: the stop, iteration count,
+    beliefs, messages and returned deltas are still the reference's, and
+    those decisions formed the serial sum."""
+    net = synth.random_loopy(2000, 8000, 2, 0.1, seed=71)
+    sched = "edge" if path == "edge" else "node"
+    check = 10 if path == "node_acc" else 1
+    kernel = "warp" if path == "warp" else "auto"
+    if path == "launch_loop":
+        monkeypatch.setenv("BP_FLOOD_FUSED", "0")
+    d = _oracle_deltas(restatement, O, net, 12, sched, check)
+    cases = _straddling_tolerances(restatement, O, net, d, sched, check)
+    assert cases, d
+    for tol, ora in cases:
+        gpu = gpu_loopy(bp, net, tol, 200, check_every=check, schedule=sched, kernel=kernel)
+        assert_same(gpu, ora, 2)
+        assert gpu["serial_sums"] >= 1, (tol, d)
+
+
+@pytest.mark.parametrize("case", CASES[:2] + CASES[4:5], ids=lambda c: f"S{c['S']}")
+def test_serial_delta_fused_matches_launch_loop(bp, synth, restatement, O, monkeypatch, case):
+    """The serial delta through the one-launch (fused) loop and the
+    launch-per-iteration loop: identical results, equal to the reference's."""
+    net = synth.random_loopy(case["V"], case["E"], case["S"], 0.1, seed=case["seed"] + 200)
+    S = case["S"]
+    for tol, max_it, check in ((1e-3, 60, 1), (1e-3, 45, 10)):
+        ora = restatement.loopy(O.OracleGraph(net), tol, max_it, check_every=check)
+        fused = gpu_loopy(bp, net, tol, max_it, check_every=check)
+        monkeypatch.setenv("BP_FLOOD_FUSED", "0")
+        loop = gpu_loopy(bp, net, tol, max_it, check_every=check)
+        monkeypatch.delenv("BP_FLOOD_FUSED")
+        assert_same(fused, ora, S)
+        assert_same(loop, ora, S)
