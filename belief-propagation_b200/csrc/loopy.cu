@@ -179,13 +179,14 @@ __device__ int serial_decide(double lo, double hi, bool s_exact, double plo, dou
     return -1;
 }
 
-// the reference's serial fp32 sum of x[0, n) in index order (graph.c:1300-1309):
-// one dependent chain of adds, so its speed is the add latency.  Thread 0 runs
-// the chain out of shared memory while threads 32.. stage the next `ch` terms
-// into the other half of buf (2 * ch floats, 16-byte aligned, ch % 4 == 0).
-// Every thread of the block calls it and gets the sum.
+// the reference's serial fp32 sum of x[0, n) in index order (graph.c:1300-1309)
+// as one dependent chain of adds: thread 0 runs the chain out of shared
+// memory while threads 32.. stage the next `ch` terms into the other half of
+// buf (2 * ch floats, 16-byte aligned, ch % 4 == 0).  Every thread of the
+// block calls it and gets the sum.  Kept as the plain form the parallel one
+// below is checked against.
 template <int NT>
-__device__ float block_serial_sum(const float *__restrict__ x, uint64_t n, float *buf, uint32_t ch) {
+__device__ float block_serial_sum_chain(const float *__restrict__ x, uint64_t n, float *buf, uint32_t ch) {
     static_assert(NT >= 64, "a staging warp besides the chain's");
     __shared__ float s_res;
     const uint64_t nch = (n + ch - 1) / ch;
@@ -222,6 +223,197 @@ __device__ float block_serial_sum(const float *__restrict__ x, uint64_t n, float
     return s_res;
 }
 
+// ---- the same serial sum, formed in parallel -----------------------------
+//
+// For non-negative terms the running sum s never decreases.  While s stays
+// in one binade [2^e, 2^(e+1)) -- subnormals: [0, 2^-126) -- the floats
+// there are the multiples m U of one unit U, and rounding s + t to nearest
+// moves s by t rounded to a multiple of U: by floor(t/U) or floor(t/U) + 1,
+// the choice fixed by t alone except at an exact tie, where it goes to the
+// even m and so depends on the parity of m.  Each term is therefore a map
+// m -> m + c(m mod 2), a pair (c_even, c_odd); pairs compose associatively
+// (the parity of m after the first map is that of its increment, plus one
+// from an odd start), so a block scan of the pairs gives m before every
+// term, exactly.  The binade holds while m + floor(t/U) < 2^24 (2^23 for
+// subnormals; the sum may round up onto the binade's top, 2^(e+1), and the
+// next term then leaves).  The first term that leaves the binade, or is inf,
+// is added by one thread, and the scan resumes in the new binade: the sum
+// crosses O(log(n)) binades.  The result is bit for bit the one-by-one sum.
+struct SumStep {
+    uint32_t e, o;   // increment of m from an even / odd m
+};
+constexpr uint32_t kSumSat = 1u << 30;   // saturation: above every binade top
+
+__device__ __forceinline__ uint32_t sum_sat(uint32_t a, uint32_t b) { return min(a + b, kSumSat); }
+
+// a, then b
+__device__ __forceinline__ SumStep sum_compose(SumStep a, SumStep b) {
+    SumStep c;
+    c.e = sum_sat(a.e, (a.e & 1u) ? b.o : b.e);
+    c.o = sum_sat(a.o, (a.o & 1u) ? b.e : b.o);
+    return c;
+}
+
+// term t against the binade with unit 2^eu: fl = floor(t / U) (saturated),
+// the step's pair, and whether t is inf or NaN (added one by one)
+__device__ __forceinline__ SumStep sum_term(float t, int eu, uint32_t &fl, bool &special) {
+    const uint32_t tb = __float_as_uint(t);
+    const uint32_t Et = (tb >> 23) & 0xffu;
+    special = Et == 0xffu;
+    const uint32_t Mt = Et ? ((tb & 0x7fffffu) | 0x800000u) : (tb & 0x7fffffu);
+    const int shift = (Et ? (int)Et - 150 : -149) - eu;
+    SumStep st;
+    if (Mt == 0u) {
+        fl = 0u;
+        st.e = st.o = 0u;
+    } else if (shift >= 0) {
+        fl = shift >= 7 ? kSumSat : min(Mt << shift, kSumSat);
+        st.e = st.o = fl;
+    } else if (shift <= -26) {   // t < U / 4
+        fl = 0u;
+        st.e = st.o = 0u;
+    } else {
+        const uint32_t sh = (uint32_t)(-shift);
+        fl = Mt >> sh;
+        const uint32_t rem = Mt & ((1u << sh) - 1u), half = 1u << (sh - 1u);
+        if (rem == half) {   // tie: to the even m
+            st.e = fl + (fl & 1u);
+            st.o = fl + ((fl + 1u) & 1u);
+        } else {
+            st.e = st.o = fl + (rem > half ? 1u : 0u);
+        }
+    }
+    return st;
+}
+
+__device__ __forceinline__ uint32_t sum_apply(uint32_t m, SumStep st) { return sum_sat(m, (m & 1u) ? st.o : st.e); }
+
+// the reference's serial fp32 sum of x[0, n) (graph.c:1300-1309), exactly, for
+// non-negative terms; every thread of the block calls it and gets the sum.
+// buf: cap floats of shared memory, cap >= 3 * NT.
+template <int NT>
+__device__ float block_serial_sum(const float *__restrict__ x, uint64_t n, float *buf, uint32_t cap) {
+    static_assert(NT % 32 == 0 && NT <= 1024, "whole warps");
+    constexpr int NW = NT / 32;
+    constexpr uint32_t kHead = 32;   // terms added one by one at the start
+    __shared__ uint32_t s_we[NW], s_wo[NW];
+    __shared__ uint32_t s_first, s_m;
+    __shared__ float s_val;
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, w = tid >> 5;
+    uint32_t K = cap / NT;
+    K = (K > 1u ? K - 1u : 1u) & ~1u;   // terms per thread; row stride K + 1 is odd
+    K = min(max(K, 2u), 30u);
+    const uint32_t KS = K + 1u, P = NT * K;
+    float s = 0.0f;
+    __syncthreads();   // buf is free
+    for (uint64_t i = 0; i < n;) {
+        const uint32_t cnt = (uint32_t)min((uint64_t)P, n - i);
+        for (uint32_t k = tid; k < cnt; k += NT) buf[(k / K) * KS + k % K] = __ldcg(x + i + k);
+        __syncthreads();
+        uint32_t pos = 0;
+        if (i == 0) {   // the start: the sum crosses binades every few terms
+            if (tid == 0) {
+                const uint32_t h = min(kHead, cnt);
+                for (uint32_t k = 0; k < h; ++k) s = FADD(s, buf[(k / K) * KS + k % K]);
+                s_val = s;
+            }
+            __syncthreads();
+            s = s_val;
+            pos = min(kHead, cnt);
+        }
+        while (pos < cnt) {
+            const uint32_t sb = __float_as_uint(s);
+            const uint32_t Es = sb >> 23;
+            if (Es >= 0xffu) break;   // inf (or NaN): it stays
+            const int eu = Es ? (int)Es - 150 : -149;
+            const uint32_t m0 = Es ? ((sb & 0x7fffffu) | 0x800000u) : sb;
+            const uint32_t top = Es ? 0x1000000u : 0x800000u;
+            const uint32_t a0 = max(tid * K, pos), a1 = min(tid * K + K, cnt);
+            const float *row = buf + tid * KS - tid * K;   // row[k] for k in [tid K, tid K + K)
+            SumStep acc{0u, 0u};
+            for (uint32_t k = a0; k < a1; ++k) {
+                uint32_t fl;
+                bool sp;
+                acc = sum_compose(acc, sum_term(row[k], eu, fl, sp));
+            }
+            // block exclusive scan of the threads' maps
+            SumStep inc = acc;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                SumStep o;
+                o.e = __shfl_up_sync(0xffffffffu, inc.e, d);
+                o.o = __shfl_up_sync(0xffffffffu, inc.o, d);
+                if ((int)lane >= d) inc = sum_compose(o, inc);
+            }
+            if (lane == 31u) {
+                s_we[w] = inc.e;
+                s_wo[w] = inc.o;
+            }
+            if (tid == 0) s_first = cnt;
+            __syncthreads();
+            SumStep pre{0u, 0u};
+            for (uint32_t ww = 0; ww < w; ++ww) pre = sum_compose(pre, SumStep{s_we[ww], s_wo[ww]});
+            SumStep ex;
+            ex.e = __shfl_up_sync(0xffffffffu, inc.e, 1);
+            ex.o = __shfl_up_sync(0xffffffffu, inc.o, 1);
+            if (lane == 0u) ex = SumStep{0u, 0u};
+            pre = sum_compose(pre, ex);
+            // m before each of this thread's terms; the first that leaves
+            // the binade (or is inf) ends the run
+            uint32_t m = sum_apply(m0, pre), bad = cnt;
+            for (uint32_t k = a0; k < a1; ++k) {
+                uint32_t fl;
+                bool sp;
+                const SumStep st = sum_term(row[k], eu, fl, sp);
+                if (sp || sum_sat(m, fl) >= top) {
+                    bad = k;
+                    break;
+                }
+                m = sum_apply(m, st);
+            }
+            if (bad < cnt) atomicMin(&s_first, bad);
+            __syncthreads();
+            const uint32_t j = s_first;
+            // m just before term j (after the last term when j == cnt)
+            const uint32_t owner = (j < cnt ? j : cnt - 1u) / K;
+            if (tid == owner) s_m = m;
+            __syncthreads();
+            if (tid == 0) {
+                uint32_t mm = s_m;
+                s = __uint_as_float((Es << 23) + mm - (Es ? 0x800000u : 0u));
+                if (j < cnt) {
+                    // the leaving term, then (when the run was short) a few
+                    // more one by one
+                    const uint32_t stop = (j - pos < 32u) ? min(cnt, j + 1u + 64u) : j + 1u;
+                    for (uint32_t k = j; k < stop; ++k) s = FADD(s, buf[(k / K) * KS + k % K]);
+                    s_first = stop;
+                } else {
+                    s_first = cnt;
+                }
+                s_val = s;
+            }
+            __syncthreads();
+            s = s_val;
+            pos = s_first;
+            __syncthreads();   // s_first is rewritten next round
+        }
+        i += cnt;
+        __syncthreads();   // buf is rewritten next pass
+        if (__float_as_uint(s) >> 23 >= 0xffu) break;
+    }
+    return s;
+}
+
+// the serial sum by whichever form is faster for the block: the parallel
+// scan needs many threads and terms per thread to beat the chain (measured
+// on 80k terms: 256 threads with 8192 floats of staging 190 us, the chain
+// 224 us, 128 threads with 2048 floats 257 us)
+template <int NT>
+__device__ __forceinline__ float exact_serial_sum(const float *x, uint64_t n, float *buf, uint32_t cap) {
+    if (NT >= 256 && cap >= 24u * NT) return block_serial_sum<NT>(x, n, buf, cap);
+    return block_serial_sum_chain<NT>(x, n, buf, (cap / 2u) & ~3u);
+}
+
 // one serial-mode check: s (the reference's delta) in [lo, hi], the
 // previous delta in [plo, phi], d = serial_decide's outcome
 struct SerialCheck {
@@ -249,18 +441,20 @@ __device__ SerialCheck serial_check(const LoopyCtl *c, double T) {
 }
 
 // an undecided check: form the serial sum, and the previous one if the
-// comparison with it still straddles; every thread of the block
+// comparison with it still straddles; every thread of the block (out of
+// line: the iteration kernels' register allocation is not shaped by it)
 template <int NT>
-__device__ void serial_form(SerialCheck &x, const LoopyCtl *c, const float *absdiff, float *buf, uint32_t ch) {
+__device__ __noinline__ void serial_form(SerialCheck &x, const LoopyCtl *c, const float *absdiff, float *buf,
+                                         uint32_t cap) {
     const uint64_t n = c->n_terms, stride = c->ad_stride;
     const uint32_t pb = c->prev_buf;
-    x.s = block_serial_sum<NT>(absdiff + (size_t)x.cb * stride, n, buf, ch);
+    x.s = exact_serial_sum<NT>(absdiff + (size_t)x.cb * stride, n, buf, cap);
     x.lo = x.hi = (double)x.s;
     x.s_exact = true;
     ++x.sums;
     x.d = serial_decide(x.lo, x.hi, true, x.plo, x.phi, x.p_exact, c->tol);
     if (x.d < 0) {
-        const float p = block_serial_sum<NT>(absdiff + (size_t)pb * stride, n, buf, ch);
+        const float p = exact_serial_sum<NT>(absdiff + (size_t)pb * stride, n, buf, cap);
         x.plo = x.phi = (double)p;
         x.p_exact = true;
         ++x.sums;
@@ -297,13 +491,14 @@ __device__ __forceinline__ double broadcast_sum(double T) {
 // term sum is T; every thread of the block calls it and takes the same
 // branches, thread 0 writes c
 template <int NT>
-__device__ void finalize_serial(LoopyCtl *c, bool want, double T, const float *absdiff, float *buf, uint32_t ch) {
+__device__ __noinline__ void finalize_serial(LoopyCtl *c, bool want, double T, const float *absdiff, float *buf,
+                                             uint32_t cap) {
     if (!want) {
         if (threadIdx.x == 0) finalize_with(c, false, false, 0.0f, 0.0);
         return;
     }
     SerialCheck x = serial_check(c, broadcast_sum(T));
-    if (x.d < 0) serial_form<NT>(x, c, absdiff, buf, ch);
+    if (x.d < 0) serial_form<NT>(x, c, absdiff, buf, cap);
     __syncthreads();   // every thread has read c
     if (threadIdx.x == 0) serial_commit(c, x);
 }
@@ -312,13 +507,12 @@ __device__ void finalize_serial(LoopyCtl *c, bool want, double T, const float *a
 // partials in a fixed order and finalizes.  In serial mode the last block
 // decides from the f64 sum and, when the bound cannot, sums the terms every
 // block wrote to absdiff (a fence per writer makes them visible before the
-// ticket); buf/ch: the block's shared staging buffer for that sum.
-template <int NT>
+// ticket); buf/cap: the block's shared staging buffer for that sum (floats).
+template <int NT, bool SER = false>
 __device__ __forceinline__ void reduce_and_finalize(LoopyCtl *ctl, double *partials, double dsum, bool want,
-                                                    double *red, bool *s_last, bool serial = false,
-                                                    const float *absdiff = nullptr, float *buf = nullptr,
-                                                    uint32_t ch = 0) {
-    if (serial && want) __threadfence();
+                                                    double *red, bool *s_last, const float *absdiff = nullptr,
+                                                    float *buf = nullptr, uint32_t cap = 0) {
+    if (SER && want) __threadfence();
     double t = block_sum<NT>(dsum, red);
     if (threadIdx.x == 0) {
         partials[blockIdx.x] = t;
@@ -333,8 +527,8 @@ __device__ __forceinline__ void reduce_and_finalize(LoopyCtl *ctl, double *parti
         double acc = 0.0;
         for (uint32_t k = threadIdx.x; k < gridDim.x; k += NT) acc += __ldcg(partials + k);
         double tot = block_sum<NT>(acc, red);
-        if (serial) {
-            finalize_serial<NT>(ctl, want, tot, absdiff, buf, ch);
+        if constexpr (SER) {
+            finalize_serial<NT>(ctl, want, tot, absdiff, buf, cap);
             if (threadIdx.x == 0) ctl->counter = 0;
         } else if (threadIdx.x == 0) {
             ctl->counter = 0;
@@ -543,7 +737,7 @@ __device__ __forceinline__ void flood_tile(const FloodArgs &a, uint32_t tile, bo
 // assignment, so the delta sums in a fixed order); with ntiles == gridDim.x
 // each block takes one tile.  A persistent grid (resident blocks per SM x SMs)
 // pays the block's delta reduction and ticket once instead of per tile.
-template <int MS, bool UNI, int FU, int MB = flood_min_blocks<MS, FU>()>
+template <int MS, bool UNI, int FU, int MB = flood_min_blocks<MS, FU>(), bool SER = false>
 __global__ void __launch_bounds__(flood_nt<MS>(), MB) k_flood(const FloodArgs a, uint32_t ntiles) {
     constexpr int NT = flood_nt<MS>();
     constexpr uint32_t EMAX = flood_smem_floats<MS>() / MS;
@@ -554,7 +748,6 @@ __global__ void __launch_bounds__(flood_nt<MS>(), MB) k_flood(const FloodArgs a,
     LoopyCtl *ctl = a.ctl;
     if (*(volatile uint32_t *)&ctl->done) return;
     const uint32_t it = ctl->it, ce = ctl->check_every;
-    const bool serial = ctl->serial != 0;
     const bool want = (ce <= 1) || ((it + 1) % ce == 0);
     const int mp = (int)((ctl->msg_parity0 + it) & 1u), qp = (int)((ctl->q_parity0 + it) & 1u);
     const float *__restrict__ m_old = mp ? a.msg1 : a.msg0;
@@ -562,14 +755,14 @@ __global__ void __launch_bounds__(flood_nt<MS>(), MB) k_flood(const FloodArgs a,
     const float *__restrict__ q_in = qp ? a.q1 : a.q0;
     float *__restrict__ q_out = qp ? a.q0 : a.q1;
     const uint64_t keep = l2_evict_last_policy();
-    float *absd = check_buffer(ctl, a.absdiff, it, want);
+    // serial delta (SER): the |diff| terms go to this check's buffer
+    float *absd = SER ? check_buffer(ctl, a.absdiff, it, want) : nullptr;
     double dsum = 0.0;
     for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         flood_tile<MS, UNI, FU>(a, tile, want, absd, m_old, m_new, q_in, q_out, keep, sm, dsum);
         __syncthreads();   // the tile's messages in shared memory are consumed
     }
-    reduce_and_finalize<NT>(ctl, a.partials, dsum, want, red, &s_last, serial, a.absdiff, sm,
-                            ((EMAX * MS) / 2) & ~3u);
+    reduce_and_finalize<NT, SER>(ctl, a.partials, dsum, want, red, &s_last, a.absdiff, sm, EMAX * MS);
 }
 
 // Small graphs: every iteration in one cooperative launch.  When each tile
@@ -613,7 +806,7 @@ __device__ __forceinline__ bool grid_barrier(LoopyCtl *c, uint32_t &gen, uint32_
     return *s_fail == 0;
 }
 
-template <int MS, bool UNI, int FU, int MB = flood_min_blocks<MS, FU>()>
+template <int MS, bool UNI, int FU, bool SER = false, int MB = flood_min_blocks<MS, FU>()>
 __global__ void __launch_bounds__(flood_nt<MS>(), MB) k_flood_fused(const FloodArgs a, uint32_t ntiles) {
     constexpr int NT = flood_nt<MS>();
     constexpr uint32_t EMAX = flood_smem_floats<MS>() / MS;
@@ -638,7 +831,7 @@ __global__ void __launch_bounds__(flood_nt<MS>(), MB) k_flood_fused(const FloodA
         float *__restrict__ m_new = mp ? a.msg0 : a.msg1;
         const float *__restrict__ q_in = qp ? a.q1 : a.q0;
         float *__restrict__ q_out = qp ? a.q0 : a.q1;
-        float *absd = check_buffer(&s_ctl, a.absdiff, it, want);
+        float *absd = SER ? check_buffer(&s_ctl, a.absdiff, it, want) : nullptr;
         double dsum = 0.0;
         for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
             flood_tile<MS, UNI, FU>(a, tile, want, absd, m_old, m_new, q_in, q_out, keep, sm, dsum);
@@ -651,7 +844,7 @@ __global__ void __launch_bounds__(flood_nt<MS>(), MB) k_flood_fused(const FloodA
         double acc = 0.0;
         for (uint32_t k = threadIdx.x; k < gridDim.x; k += NT) acc += __ldcg(part + k);
         const double tot = block_sum<NT>(acc, red);
-        if (s_ctl.serial && want) {
+        if (SER && want) {
             // every block reaches the same decision from the same sum; when
             // the bound cannot decide, block 0 forms the serial sums and the
             // blocks meet once more to read them.  The terms are
@@ -660,7 +853,7 @@ __global__ void __launch_bounds__(flood_nt<MS>(), MB) k_flood_fused(const FloodA
             SerialCheck x = serial_check(&s_ctl, broadcast_sum(tot));
             if (x.d < 0) {
                 if (blockIdx.x == 0) {
-                    serial_form<NT>(x, &s_ctl, a.absdiff, sm, ((EMAX * MS) / 2) & ~3u);
+                    serial_form<NT>(x, &s_ctl, a.absdiff, sm, EMAX * MS);
                     if (threadIdx.x == 0) {
                         ctl->fb_s = x.s;
                         ctl->fb_p = (float)x.plo;
@@ -1114,8 +1307,8 @@ __global__ void __launch_bounds__(256) k_flood_w(const FloodArgs a) {
             stv<MS>(q_out + (size_t)v * MS, qo);
         }
     }
-    reduce_and_finalize<NT>(ctl, a.partials, dsum, want, red, &s_last, serial, a.absdiff, sm,
-                            ((NW * WE * MS) / 2) & ~3u);
+    if (serial) reduce_and_finalize<NT, true>(ctl, a.partials, dsum, want, red, &s_last, a.absdiff, sm, NW * WE * MS);
+    else reduce_and_finalize<NT>(ctl, a.partials, dsum, want, red, &s_last);
 }
 
 // prologue: Q_1 = b * prod of the latest messages (read_incoming_messages,
@@ -1156,6 +1349,16 @@ __global__ void k_send_from_beliefs(uint32_t E, const uint32_t *__restrict__ in_
     stv<MS>(msg + p * MS, m);
 }
 
+// one block forms the serial fp32 sum of x[0, n): the parallel form with NT
+// threads and cap floats of staging, or the one-thread chain
+template <int NT>
+__global__ void __launch_bounds__(NT) k_serial_sum(const float *__restrict__ x, uint64_t n, float *out, int chain,
+                                                  uint32_t cap) {
+    __shared__ __align__(16) float buf[8192];
+    const float s = chain ? block_serial_sum_chain<NT>(x, n, buf, 4096) : block_serial_sum<NT>(x, n, buf, cap);
+    if (threadIdx.x == 0) *out = s;
+}
+
 // the reference's `delta` and `previous_delta` at return (graph.c:1300-1318)
 // where the loop decided from bounds without forming them: block 0 sums the
 // last check's terms, block 1 the check's before (serial fp32, edge-id order)
@@ -1166,7 +1369,7 @@ __global__ void __launch_bounds__(256) k_delta_final(LoopyCtl *ctl, const float 
     const bool prev = blockIdx.x == 1;
     if (prev ? c.prev_exact : c.delta_exact) return;
     const uint32_t b = prev ? c.prev_buf : c.cur_buf;
-    const float s = block_serial_sum<256>(absdiff + (size_t)b * c.ad_stride, c.n_terms, buf, 4096);
+    const float s = exact_serial_sum<256>(absdiff + (size_t)b * c.ad_stride, c.n_terms, buf, 2 * 4096);
     if (threadIdx.x == 0) {
         if (prev) ctl->prev_f = s;
         else ctl->delta_f = s;
@@ -1357,7 +1560,8 @@ __global__ void __launch_bounds__(256) k_edge_delta(const EdgeArgs a) {
         }
         if (absd) stv<MS>(absd + (size_t)a.pos_edge[p] * MS, ad);
     }
-    reduce_and_finalize<256>(ctl, a.partials, dsum, want, red, &s_last, serial, a.absdiff, buf, 1024);
+    if (serial) reduce_and_finalize<256, true>(ctl, a.partials, dsum, want, red, &s_last, a.absdiff, buf, 2 * 1024);
+    else reduce_and_finalize<256>(ctl, a.partials, dsum, want, red, &s_last);
 }
 
 // ---------------------------------------------------------------- driver --
@@ -1563,8 +1767,10 @@ static int resident_blocks(int *bps) {
 
 // launch of the block-tile kernel with the register cap block_min_blocks()
 template <int MS, bool UNI, int FU>
-static void launch_block_tiles(unsigned grid, cudaStream_t st, const FloodArgs &a, uint32_t ntiles) {
+static void launch_block_tiles(unsigned grid, cudaStream_t st, const FloodArgs &a, uint32_t ntiles, bool serial) {
     constexpr int NT = flood_nt<MS>();
+    constexpr int MB = flood_min_blocks<MS, FU>();
+    if (serial) return k_flood<MS, UNI, FU, MB, true><<<grid, NT, 0, st>>>(a, ntiles);
     if constexpr (MS <= 2) {
         const int mb = block_min_blocks();
         if (mb == 10) return k_flood<MS, UNI, FU, 10><<<grid, NT, 0, st>>>(a, ntiles);
@@ -1598,7 +1804,7 @@ static int block_tiles(const bp_graph *g, unsigned *grid, uint32_t *ntiles) {
 }
 
 template <int MS, bool UNI>
-static int enqueue_node_iterations(bp_graph *g, uint32_t k, bool, int variant) {
+static int enqueue_node_iterations(bp_graph *g, uint32_t k, bool serial, int variant) {
     constexpr int NT = flood_nt<MS>();
     if (variant == BP_KERNEL_STAGED_TILE) {
         if constexpr (UNI && MS == 2) {
@@ -1628,11 +1834,13 @@ static int enqueue_node_iterations(bp_graph *g, uint32_t k, bool, int variant) {
     for (uint32_t i = 0; i < k; ++i) {
         if (!warp_tiled) {
             if constexpr (MS <= 2) {
-                if (unroll == 1) launch_block_tiles<MS, UNI, 1>(grid, g->stream, a, ntiles);
-                else if (unroll == 2) launch_block_tiles<MS, UNI, 2>(grid, g->stream, a, ntiles);
-                else launch_block_tiles<MS, UNI, 4>(grid, g->stream, a, ntiles);
+                if (unroll == 1) launch_block_tiles<MS, UNI, 1>(grid, g->stream, a, ntiles, serial);
+                else if (unroll == 2) launch_block_tiles<MS, UNI, 2>(grid, g->stream, a, ntiles, serial);
+                else launch_block_tiles<MS, UNI, 4>(grid, g->stream, a, ntiles, serial);
             } else {
-                k_flood<MS, UNI, flood_unroll<MS>()><<<grid, NT, 0, g->stream>>>(a, ntiles);
+                constexpr int FU = flood_unroll<MS>();
+                if (serial) k_flood<MS, UNI, FU, flood_min_blocks<MS, FU>(), true><<<grid, NT, 0, g->stream>>>(a, ntiles);
+                else k_flood<MS, UNI, FU><<<grid, NT, 0, g->stream>>>(a, ntiles);
             }
         } else if constexpr (MS <= 2) {
             if (unroll == 1) k_flood_w<MS, UNI, 1><<<grid, 256, 0, g->stream>>>(a);
@@ -1698,11 +1906,17 @@ static bool staged_applies(const bp_graph *g, int schedule, bool serial) {
 // the fused loop: its grid (at most one co-resident block per tile), or 0
 // when the graph has more tiles than the GPU holds blocks at once
 template <int MS, bool UNI>
-static int fused_grid(const bp_graph *g, unsigned *grid, uint32_t *ntiles) {
+static int fused_grid(const bp_graph *g, unsigned *grid, uint32_t *ntiles, bool serial) {
     constexpr int FU = flood_unroll<MS>();
-    static int bps = -1;
-    if (bps < 0)
-        BP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_flood_fused<MS, UNI, FU>, flood_nt<MS>(), 0));
+    static int bps_f64 = -1, bps_ser = -1;
+    int &bps = serial ? bps_ser : bps_f64;
+    if (bps < 0) {
+        if (serial)
+            BP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_flood_fused<MS, UNI, FU, true>,
+                                                                  flood_nt<MS>(), 0));
+        else
+            BP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_flood_fused<MS, UNI, FU>, flood_nt<MS>(), 0));
+    }
     int dev = 0, sms = 0;
     BP_CUDA(cudaGetDevice(&dev));
     BP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -1712,12 +1926,12 @@ static int fused_grid(const bp_graph *g, unsigned *grid, uint32_t *ntiles) {
 }
 
 template <int MS, bool UNI>
-static int launch_fused(bp_graph *g, unsigned grid, uint32_t ntiles) {
+static int launch_fused(bp_graph *g, unsigned grid, uint32_t ntiles, bool serial) {
     constexpr int FU = flood_unroll<MS>();
     FloodArgs a = flood_args(g);
     void *args[] = {(void *)&a, (void *)&ntiles};
-    BP_CUDA(cudaLaunchCooperativeKernel((const void *)k_flood_fused<MS, UNI, FU>, dim3(grid), dim3(flood_nt<MS>()),
-                                        args, 0, g->stream));
+    const void *fn = serial ? (const void *)k_flood_fused<MS, UNI, FU, true> : (const void *)k_flood_fused<MS, UNI, FU>;
+    BP_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(flood_nt<MS>()), args, 0, g->stream));
     return BP_OK;
 }
 
@@ -1742,6 +1956,20 @@ void bp_loopy_default_options(bp_loopy_options *o) {
 int bp_init_messages(bp_graph *g) {
     if (!g) return set_error(BP_ERR_INVALID, "null graph");
     BP_DISPATCH_MS(g->ms, g->uniform != 0, launch_init, g);
+}
+
+int bp_serial_sum_f32(const float *x, uint64_t n, float *out, int method, void *stream) {
+    if (!out || (n && !x)) return set_error(BP_ERR_INVALID, "null argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    switch (method) {
+    case 0: k_serial_sum<256><<<1, 256, 0, st>>>(x, n, out, 0, 8192); break;
+    case 1: k_serial_sum<128><<<1, 128, 0, st>>>(x, n, out, 0, 2048); break;
+    case 2: k_serial_sum<256><<<1, 256, 0, st>>>(x, n, out, 0, 2048); break;
+    case 3: k_serial_sum<256><<<1, 256, 0, st>>>(x, n, out, 1, 8192); break;
+    default: return set_error(BP_ERR_INVALID, "unknown method %d", method);
+    }
+    BP_CUDA(cudaGetLastError());
+    return BP_OK;
 }
 
 int bp_loopy(bp_graph *g, const bp_loopy_options *opt, bp_loopy_result *res) {
@@ -1815,7 +2043,7 @@ int bp_loopy(bp_graph *g, const bp_loopy_options *opt, bp_loopy_result *res) {
         const char *env = getenv("BP_FLOOD_FUSED");
         if (opt->schedule == BP_SCHEDULE_NODE && variant == BP_KERNEL_BLOCK_TILE &&
             !(env && env[0] == '0')) {
-            auto fg = [&]() -> int { BP_DISPATCH_MS(g->ms, g->uniform != 0, fused_grid, g, &fgrid, &fntiles); };
+            auto fg = [&]() -> int { BP_DISPATCH_MS(g->ms, g->uniform != 0, fused_grid, g, &fgrid, &fntiles, serial); };
             if ((st = fg())) return st;
         }
     }
@@ -1853,7 +2081,7 @@ int bp_loopy(bp_graph *g, const bp_loopy_options *opt, bp_loopy_result *res) {
 
     if (fgrid) {
         BP_CUDA(cudaEventRecord(g->ev0, g->stream));
-        auto lf = [&]() -> int { BP_DISPATCH_MS(g->ms, g->uniform != 0, launch_fused, g, fgrid, fntiles); };
+        auto lf = [&]() -> int { BP_DISPATCH_MS(g->ms, g->uniform != 0, launch_fused, g, fgrid, fntiles, serial); };
         if ((st = lf())) return st;
     } else {
         // CUDA graph of `chunk` iterations, cached per (schedule, delta, chunk)

@@ -167,6 +167,18 @@ int bp_init_messages(bp_graph *g);
 /* loopy_propagate_until / _edge / _acc / _edge_acc (graph.c:1186-1547) */
 int bp_loopy(bp_graph *g, const bp_loopy_options *opt, bp_loopy_result *res);
 
+/* The reference's serial fp32 delta sum (graph.c:1300-1309): *out = the sum
+ * of the n non-negative DEVICE floats x[0..n) added one at a time in index
+ * order in fp32, bit for bit, written to the DEVICE float *out on `stream`
+ * (asynchronous).  Formed in parallel: inside one binade of the running sum
+ * every add is the term rounded to that binade's unit, so a scan of
+ * per-term increments gives the running sum exactly; a term that moves the
+ * sum to the next binade is added alone.  method: 0 = 256 threads (the
+ * form bp_loopy's final delta uses), 1 = 128 threads with 2048 floats of
+ * staging (the iteration kernel's), 2 = 256 threads with 2048 floats,
+ * 3 = the one-add-at-a-time chain. */
+int bp_serial_sum_f32(const float *x, uint64_t n, float *out, int method, void *stream);
+
 /* ---- loopy BP without allocating ------------------------------------- */
 /* No counterpart in the reference: an addition of this library.
  *

@@ -425,3 +425,58 @@ def test_serial_delta_fused_matches_launch_loop(bp, synth, restatement, O, monke
         monkeypatch.delenv("BP_FLOOD_FUSED")
         assert_same(fused, ora, S)
         assert_same(loop, ora, S)
+
+
+def _serial_sum_cases():
+    rng = np.random.default_rng(123)
+    f32 = np.float32
+    out = {
+        "empty": np.zeros(0, f32),
+        "one": np.array([3.5], f32),
+        "zeros": np.zeros(5000, f32),
+        "uniform_80k": rng.random(80_000, dtype=f32),
+        "tiny_terms": (rng.random(200_000, dtype=f32) * f32(1e-4)),
+        "wide_exponents": (rng.random(50_000) * 10.0 ** rng.uniform(-40, 30, 50_000)).astype(f32),
+        "subnormals": (rng.integers(0, 1 << 20, 30_000).astype(np.uint32)).view(f32),
+        # powers of two: every add an exact tie or exact, ties to even
+        "ties": np.ldexp(f32(1.0), rng.integers(-30, -10, 100_000)).astype(f32),
+        "half_ulp_runs": np.concatenate([np.array([1.0], f32), np.full(70_000, np.ldexp(f32(1.0), -24), f32),
+                                         np.full(3000, np.ldexp(f32(1.0), -23), f32)]),
+        "large_then_small": np.concatenate([np.full(10, 1e30, f32), rng.random(20_000, dtype=f32)]),
+        "growing": (np.arange(1, 60_001, dtype=np.float64) ** 2).astype(f32),
+        "with_inf": np.concatenate([rng.random(9000, dtype=f32), np.array([np.inf], f32),
+                                    rng.random(9000, dtype=f32)]),
+        "overflow": np.full(40, 3.0e38, f32),
+        "ragged_1793": rng.random(1793, dtype=f32),
+        "max_float_mix": np.concatenate([rng.random(4000, dtype=f32),
+                                         np.full(4, np.finfo(f32).max / f32(8), f32)]),
+    }
+    # |diff| terms as the iteration kernels write them: messages of 2 states
+    a = rng.random((40_000, 2), dtype=f32)
+    b = a + (rng.standard_normal((40_000, 2)) * 1e-3).astype(f32)
+    out["message_diffs"] = np.abs(a - b).ravel()
+    return out
+
+
+@pytest.mark.parametrize("name", list(_serial_sum_cases()))
+def test_serial_sum_parallel_is_the_one_by_one_sum(bp, name):
+    """The parallel serial fp32 sum (a scan of per-term increments inside each
+    binade of the running sum) equals the one-add-at-a-time fp32 sum bit for
+    bit -- the device chain and numpy's sequential accumulate -- for every
+    block shape, on ties, subnormals, exponent ranges, inf and overflow."""
+    import ctypes as C
+    import torch
+    from belief_propagation_b200 import native as N
+    x = _serial_sum_cases()[name]
+    ref = np.add.accumulate(x, dtype=np.float32)[-1] if len(x) else np.float32(0.0)
+    xd = torch.from_numpy(x.copy()).cuda() if len(x) else torch.zeros(1, device="cuda")
+    out = torch.full((4,), -7.0, device="cuda")
+    lib = N.load()
+    for method in range(4):
+        rc = lib.bp_serial_sum_f32(C.c_void_p(xd.data_ptr()), C.c_uint64(len(x)),
+                                   C.c_void_p(out.data_ptr() + 4 * method), method, None)
+        assert rc == 0
+    torch.cuda.synchronize()
+    got = out.cpu().numpy()
+    for method in range(4):
+        assert got[method].tobytes() == np.float32(ref).tobytes(), (name, method, got[method], ref)
