@@ -74,6 +74,9 @@ struct LoopyCtl {
     // the one-launch loop: block 0's serial sums for the other blocks
     uint32_t fb_pform;     // the previous delta was formed too
     float fb_s, fb_p;
+    // [dlo, dhi] / [plo, phi] narrowed from the terms' own rounding errors
+    uint32_t delta_ref, prev_ref;
+    uint32_t serial_refines;   // checks that needed the narrowed interval
     uint32_t pad2;
 };
 

@@ -75,6 +75,7 @@ __device__ __forceinline__ void keep_prev(LoopyCtl *c, float df, double dd) {
     c->plo = c->dlo;
     c->phi = c->dhi;
     c->prev_exact = c->delta_exact;
+    c->prev_ref = c->delta_ref;
     c->prev_buf = c->cur_buf;
 }
 
@@ -404,6 +405,208 @@ __device__ float block_serial_sum(const float *__restrict__ x, uint64_t n, float
     return s;
 }
 
+// ---- a narrow interval for the serial sum, from the terms' own errors ---
+//
+// s_n = S + sum_k d_k, S = sum t_k exactly, d_k = the rounding error of add k.
+// Where the running sum is certainly inside one binade with unit U both
+// before and after add k -- judged from the exact prefix P_k and the bound
+// |s_k - P_k| <= k u' P_k / (1 - n u') (plus 2^-149 per add) -- the add rounds
+// t_k to a multiple of U, so d_k = RN_U(t_k) - t_k is known exactly from t_k
+// alone (an exact tie: |d_k| = U / 2, sign unknown).  Elsewhere (the few
+// adds next to a binade crossing) |d_k| <= half an ulp of the largest
+// possible s_k.  Summing the known d_k and the bounds of the others gives an
+// interval about as wide as those few bounds, instead of n u S.
+
+// a block's exclusive scan of doubles (every thread's v); total to all
+template <int NT>
+__device__ __forceinline__ double block_excl_scan_f64(double v, double *wsum, double &total) {
+    constexpr int NW = NT / 32;
+    const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+    double inc = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const double o = __shfl_up_sync(0xffffffffu, inc, d);
+        if ((int)lane >= d) inc += o;
+    }
+    if (lane == 31u) wsum[w] = inc;
+    __syncthreads();
+    double pre = 0.0, tot = 0.0;
+#pragma unroll
+    for (int k = 0; k < NW; ++k) {
+        const double x = wsum[k];
+        if (k < (int)w) pre += x;
+        tot += x;
+    }
+    __syncthreads();   // wsum is free again
+    total = tot;
+    return pre + inc - v;
+}
+
+struct Refine {
+    double E;   // sum of the known errors
+    double A;   // sum of their magnitudes (for the f64 rounding of E)
+    double B;   // sum of the bounds of the unknown ones
+    bool bad;   // an inf/NaN term or an overflowing sum: no interval
+};
+
+// per-add bound factor: |s_k - P_k| <= P_k k c0 + k 2^-149 (c0 covers
+// u' / (1 - n u') and the f64 rounding of P); 0 when n u' is too large
+__device__ __forceinline__ double refine_c0(uint64_t n) {
+    const double a = __dmul_ru((double)n, 0x1p-24 + 0x1p-52);
+    if (a >= 0.25) return 0.0;
+    return __dadd_ru(__dmul_ru(__ddiv_ru(0x1p-24 + 0x1p-52, __dsub_rd(1.0, a)), 1.0 + 0x1p-20), 0x1p-51);
+}
+
+// one add's contribution: running prefix P before it, t the term, k its
+// 1-based index
+__device__ __forceinline__ void refine_term(float t, double P, double Pn, uint64_t k, double c0, Refine &r) {
+    const uint32_t tb = __float_as_uint(t);
+    const uint32_t Et = (tb >> 23) & 0xffu;
+    if (Et == 0xffu) {
+        r.bad = true;
+        return;
+    }
+    if ((tb & 0x7fffffffu) == 0u || P == 0.0) return;   // adding 0, or onto 0: exact
+    const double kd = (double)k;
+    const double G = __dadd_ru(__dmul_ru(__dmul_ru(Pn, kd), c0), __dmul_ru(kd, 0x1p-149));
+    const double lo = __dsub_rd(P, G), hi = __dadd_ru(Pn, G);
+    if (hi >= 0x1p127) {
+        r.bad = true;
+        return;
+    }
+    int eu;   // unit exponent of the binade, when certain
+    if (hi < 0x1p-126) eu = -149;
+    else if (lo >= 0x1p-126 && ilogb(lo) == ilogb(hi)) eu = ilogb(hi) - 23;
+    else {
+        r.B = __dadd_ru(r.B, hi < 0x1p-126 ? 0x1p-150 : ldexp(1.0, ilogb(hi) - 24));
+        return;
+    }
+    const uint32_t Mt = Et ? ((tb & 0x7fffffu) | 0x800000u) : (tb & 0x7fffffu);
+    const int et = Et ? (int)Et - 150 : -149;
+    const int shift = et - eu;
+    if (Mt == 0u || shift >= 0) return;   // a multiple of U: exact
+    const int sh = -shift;
+    double d;
+    if (sh >= 25) {
+        d = -(double)t;   // below U / 2: rounds away entirely
+    } else {
+        const uint32_t rem = Mt & ((1u << sh) - 1u), half = 1u << (sh - 1);
+        if (rem == half) {
+            r.B = __dadd_ru(r.B, ldexp(1.0, eu - 1));
+            return;
+        }
+        d = rem > half ? ldexp((double)((1u << sh) - rem), et) : -ldexp((double)rem, et);
+    }
+    r.E += d;
+    r.A += fabs(d);
+}
+
+// the terms x[lo, hi) of a sum whose exact prefix before x[lo] is P0, staged
+// through buf (cap floats, cap >= 3 NT) in passes of NT K terms; every thread
+// of the block calls it, and gets the block's totals and the end prefix
+template <int NT>
+__device__ Refine refine_segment(const float *__restrict__ x, uint64_t lo, uint64_t hi, double P0, double c0,
+                                 float *buf, uint32_t cap, double &P_end) {
+    __shared__ double s_w[NT / 32];
+    __shared__ double s_r[4];
+    const uint32_t tid = threadIdx.x;
+    uint32_t K = cap / NT;
+    K = (K > 1u ? K - 1u : 1u) & ~1u;
+    K = min(max(K, 2u), 30u);
+    const uint32_t KS = K + 1u, Pn = NT * K;
+    Refine r{0.0, 0.0, 0.0, false};
+    double P = P0;
+    __syncthreads();   // buf is free
+    for (uint64_t base = lo; base < hi; base += Pn) {
+        const uint32_t cnt = (uint32_t)min((uint64_t)Pn, hi - base);
+        for (uint32_t k = tid; k < cnt; k += NT) buf[(k / K) * KS + k % K] = __ldcg(x + base + k);
+        __syncthreads();
+        const uint32_t a0 = tid * K, a1 = min(a0 + K, cnt);
+        const float *row = buf + tid * KS;
+        double ls = 0.0;
+        for (uint32_t k = a0; k < a1; ++k) ls += (double)row[k - a0];
+        double tot;
+        double Pk = P + block_excl_scan_f64<NT>(ls, s_w, tot);
+        for (uint32_t k = a0; k < a1; ++k) {
+            const float t = row[k - a0];
+            const double Pn1 = Pk + (double)t;
+            refine_term(t, Pk, Pn1, base + k + 1, c0, r);
+            Pk = Pn1;
+        }
+        P += tot;
+        __syncthreads();   // buf is rewritten next pass
+    }
+    // block totals (E, A in any order: their f64 error is bounded by A;
+    // B rounded up)
+    double e = r.E, a = r.A, b = r.B;
+    uint32_t bad = r.bad ? 1u : 0u;
+    for (int d = 16; d > 0; d >>= 1) {
+        e += __shfl_xor_sync(0xffffffffu, e, d);
+        a += __shfl_xor_sync(0xffffffffu, a, d);
+        b = __dadd_ru(b, __shfl_xor_sync(0xffffffffu, b, d));
+        bad |= __shfl_xor_sync(0xffffffffu, bad, d);
+    }
+    __shared__ double s_e[NT / 32], s_a[NT / 32], s_b[NT / 32];
+    __shared__ uint32_t s_bad;
+    if (tid == 0) s_bad = 0u;
+    __syncthreads();
+    if ((tid & 31u) == 0u) {
+        s_e[tid >> 5] = e;
+        s_a[tid >> 5] = a;
+        s_b[tid >> 5] = b;
+        if (bad) s_bad = 1u;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double E = 0.0, A = 0.0, B = 0.0;
+        for (int w = 0; w < NT / 32; ++w) {
+            E += s_e[w];
+            A += s_a[w];
+            B = __dadd_ru(B, s_b[w]);
+        }
+        s_r[0] = E;
+        s_r[1] = A;
+        s_r[2] = B;
+        s_r[3] = s_bad ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    Refine out{s_r[0], s_r[1], s_r[2], s_r[3] != 0.0};
+    P_end = P;
+    __syncthreads();
+    return out;
+}
+
+// the interval of s from the exact-sum estimate T (an f64 sum of n terms),
+// the known errors E (magnitudes A) and the bounds B
+__device__ __forceinline__ void refine_interval(double T, const Refine &r, uint64_t n, double &lo, double &hi) {
+    const double m = (double)n + 0x1p21;   // adds in any f64 summation of the pieces
+    const double tS = __dmul_ru(__dmul_ru(T, m), 0x1p-52), tE = __dmul_ru(__dmul_ru(r.A, m), 0x1p-52);
+    const double w = __dadd_ru(__dadd_ru(tS, tE), __dmul_ru(r.B, 1.0 + 0x1p-40));
+    const double mid = T + r.E;
+    const double mw = __dmul_ru(fabs(mid), 0x1p-52);   // the rounding of mid
+    lo = fmax(0.0, __dsub_rd(__dsub_rd(mid, mw), w));
+    hi = __dadd_ru(__dadd_ru(mid, mw), w);
+}
+
+// a block's narrowed interval of the serial sum of x[0, n); false if none
+template <int NT>
+__device__ bool refine_block(const float *x, uint64_t n, float *buf, uint32_t cap, double &lo, double &hi) {
+    const double c0 = refine_c0(n);
+    if (c0 == 0.0) return false;
+    double T;
+    const Refine r = refine_segment<NT>(x, 0, n, 0.0, c0, buf, cap, T);
+    if (r.bad) return false;
+    refine_interval(T, r, n, lo, hi);
+    return true;
+}
+
+// [lo, hi] holding one float only: that float
+__device__ __forceinline__ bool interval_pins(double lo, double hi, float &f) {
+    const float a = __double2float_ru(lo), b = __double2float_rd(hi);
+    f = a;
+    return a == b;
+}
+
 // the serial sum by whichever form is faster for the block: the parallel
 // scan needs many threads and terms per thread to beat the chain (measured
 // on 80k terms: 256 threads with 8192 floats of staging 190 us, the chain
@@ -418,10 +621,12 @@ __device__ __forceinline__ float exact_serial_sum(const float *x, uint64_t n, fl
 // previous delta in [plo, phi], d = serial_decide's outcome
 struct SerialCheck {
     double T, lo, hi, plo, phi;
-    float s;   // (float)T until the serial sum is formed
+    float s;   // (float)T until the serial sum is known
     bool s_exact, p_exact;
+    bool s_ref, p_ref;   // narrowed from the terms' errors
+    bool p_new;          // [plo, phi] changed in this check
     int d;
-    uint32_t sums, cb;
+    uint32_t sums, refines, cb;
 };
 
 // the decision from the bounds alone; every thread, the same T
@@ -431,8 +636,9 @@ __device__ SerialCheck serial_check(const LoopyCtl *c, double T) {
     x.plo = c->plo;
     x.phi = c->phi;
     x.p_exact = c->prev_exact != 0;
-    x.s_exact = false;
-    x.sums = 0;
+    x.p_ref = c->prev_ref != 0;
+    x.s_exact = x.s_ref = x.p_new = false;
+    x.sums = x.refines = 0;
     x.cb = check_index(c->it, c->check_every) % 3u;
     x.s = (float)T;
     serial_interval(T, c->n_terms, x.lo, x.hi);
@@ -440,40 +646,78 @@ __device__ SerialCheck serial_check(const LoopyCtl *c, double T) {
     return x;
 }
 
-// an undecided check: form the serial sum, and the previous one if the
-// comparison with it still straddles; every thread of the block (out of
-// line: the iteration kernels' register allocation is not shaped by it)
+// a narrowed interval [lo, hi] of s (which == 0) or of the previous delta
+__device__ __forceinline__ void serial_narrow(SerialCheck &x, int which, double lo, double hi) {
+    double &L = which ? x.plo : x.lo, &H = which ? x.phi : x.hi;
+    L = fmax(L, lo);
+    H = fmin(H, hi);
+    float f;
+    const bool pinned = interval_pins(L, H, f);
+    if (pinned) L = H = (double)f;
+    if (which) {
+        x.p_ref = x.p_new = true;
+        x.p_exact = pinned;
+    } else {
+        x.s_ref = true;
+        x.s_exact = pinned;
+        if (pinned) x.s = f;
+    }
+}
+
+// an undecided check, one block: narrow the interval of s (and of the
+// previous delta when it straddles too), then form the serial sums where
+// that still does not decide; every thread of the block (out of line: the
+// iteration kernels' register allocation is not shaped by it)
 template <int NT>
 __device__ __noinline__ void serial_form(SerialCheck &x, const LoopyCtl *c, const float *absdiff, float *buf,
-                                         uint32_t cap) {
+                                         uint32_t cap, bool narrow) {
     const uint64_t n = c->n_terms, stride = c->ad_stride;
     const uint32_t pb = c->prev_buf;
-    x.s = exact_serial_sum<NT>(absdiff + (size_t)x.cb * stride, n, buf, cap);
-    x.lo = x.hi = (double)x.s;
-    x.s_exact = true;
-    ++x.sums;
-    x.d = serial_decide(x.lo, x.hi, true, x.plo, x.phi, x.p_exact, c->tol);
+    const float tol = c->tol;
+    double lo, hi;
+    if (narrow) {
+        ++x.refines;
+        if (refine_block<NT>(absdiff + (size_t)x.cb * stride, n, buf, cap, lo, hi)) serial_narrow(x, 0, lo, hi);
+        x.d = serial_decide(x.lo, x.hi, x.s_exact, x.plo, x.phi, x.p_exact, tol);
+        if (x.d < 0 && !x.p_exact && !x.p_ref) {
+            if (refine_block<NT>(absdiff + (size_t)pb * stride, n, buf, cap, lo, hi)) serial_narrow(x, 1, lo, hi);
+            x.d = serial_decide(x.lo, x.hi, x.s_exact, x.plo, x.phi, x.p_exact, tol);
+        }
+    }
+    if (x.d < 0 && !x.s_exact) {
+        x.s = exact_serial_sum<NT>(absdiff + (size_t)x.cb * stride, n, buf, cap);
+        x.lo = x.hi = (double)x.s;
+        x.s_exact = true;
+        ++x.sums;
+        x.d = serial_decide(x.lo, x.hi, true, x.plo, x.phi, x.p_exact, tol);
+    }
     if (x.d < 0) {
         const float p = exact_serial_sum<NT>(absdiff + (size_t)pb * stride, n, buf, cap);
         x.plo = x.phi = (double)p;
-        x.p_exact = true;
+        x.p_exact = x.p_new = true;
         ++x.sums;
-        x.d = serial_decide(x.lo, x.hi, true, x.plo, x.phi, true, c->tol);
+        x.d = serial_decide(x.lo, x.hi, true, x.plo, x.phi, true, tol);
     }
 }
 
 // record the check and run the loop bookkeeping; one thread
 __device__ void serial_commit(LoopyCtl *c, const SerialCheck &x) {
-    if (x.p_exact && !c->prev_exact) {
-        c->prev_f = (float)x.plo;
-        c->plo = c->phi = x.plo;
-        c->prev_exact = 1;
+    if (x.p_new) {
+        c->plo = x.plo;
+        c->phi = x.phi;
+        c->prev_ref = x.p_ref ? 1u : 0u;
+        if (x.p_exact) {
+            c->prev_f = (float)x.plo;
+            c->prev_exact = 1;
+        }
     }
     c->dlo = x.lo;
     c->dhi = x.hi;
     c->delta_exact = x.s_exact ? 1u : 0u;
+    c->delta_ref = x.s_ref ? 1u : 0u;
     c->cur_buf = x.cb;
     c->serial_sums += x.sums;
+    c->serial_refines += x.refines;
     finalize_with(c, true, x.d == 1, x.s, x.T);
 }
 
@@ -498,7 +742,7 @@ __device__ __noinline__ void finalize_serial(LoopyCtl *c, bool want, double T, c
         return;
     }
     SerialCheck x = serial_check(c, broadcast_sum(T));
-    if (x.d < 0) serial_form<NT>(x, c, absdiff, buf, cap);
+    if (x.d < 0) serial_form<NT>(x, c, absdiff, buf, cap, true);
     __syncthreads();   // every thread has read c
     if (threadIdx.x == 0) serial_commit(c, x);
 }
@@ -806,6 +1050,125 @@ __device__ __forceinline__ bool grid_barrier(LoopyCtl *c, uint32_t &gen, uint32_
     return *s_fail == 0;
 }
 
+// the narrowed intervals of an undecided check in the one-launch loop,
+// grid-wide: each block takes one slice of the terms (of s, and of the
+// previous delta when that is neither exact nor narrowed yet); slice sums,
+// a barrier, each slice's errors from its exact prefix, a barrier, and
+// every block sums the same slices in the same order, so all blocks end with
+// the same intervals.  Scratch: 8 doubles per block after the partials.
+// false when a barrier gave up.
+template <int NT>
+__device__ bool grid_refine(const FloodArgs &a, LoopyCtl *ctl, uint32_t &gen, uint32_t *s_fail, SerialCheck &x,
+                            const LoopyCtl &sc, float *buf, uint32_t cap, double *red) {
+    __shared__ double s_b[4];
+    __shared__ double s_v[NT / 32][6];
+    __shared__ double s_t[6];
+    const uint64_t n = sc.n_terms, stride = sc.ad_stride;
+    const double c0 = refine_c0(n);
+    if (c0 == 0.0) return true;
+    const bool do_p = !x.p_exact && !x.p_ref;
+    ++x.refines;
+    const uint32_t G = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
+    double *scr = a.partials + 2 * (size_t)G;
+    const uint64_t L = ((n + G - 1) / G + 3) & ~3ull;
+    const uint64_t lo = min(n, (uint64_t)b * L), hi = min(n, lo + L);
+    const float *xs = a.absdiff + (size_t)x.cb * stride, *xp = a.absdiff + (size_t)sc.prev_buf * stride;
+    double ls = 0.0, lp = 0.0;
+    for (uint64_t k = lo + tid; k < hi; k += NT) {
+        ls += (double)__ldcg(xs + k);
+        if (do_p) lp += (double)__ldcg(xp + k);
+    }
+    ls = block_sum<NT>(ls, red);
+    lp = block_sum<NT>(lp, red);
+    if (tid == 0) {
+        scr[b] = ls;
+        scr[G + b] = lp;
+    }
+    if (!grid_barrier(ctl, gen, s_fail)) return false;
+    // prefixes before this slice, and the totals (the same in every block)
+    double ps = 0.0, ts = 0.0, pp = 0.0, tp = 0.0;
+    for (uint32_t k = tid; k < G; k += NT) {
+        const double vs = __ldcg(scr + k), vp = __ldcg(scr + G + k);
+        ts += vs;
+        tp += vp;
+        if (k < b) {
+            ps += vs;
+            pp += vp;
+        }
+    }
+    ps = block_sum<NT>(ps, red);
+    ts = block_sum<NT>(ts, red);
+    pp = block_sum<NT>(pp, red);
+    tp = block_sum<NT>(tp, red);
+    if (tid == 0) {
+        s_b[0] = ps;
+        s_b[1] = ts;
+        s_b[2] = pp;
+        s_b[3] = tp;
+    }
+    __syncthreads();
+    ps = s_b[0];
+    ts = s_b[1];
+    pp = s_b[2];
+    tp = s_b[3];
+    double pe;
+    const Refine rs = refine_segment<NT>(xs, lo, hi, ps, c0, buf, cap, pe);
+    Refine rp{0.0, 0.0, 0.0, false};
+    if (do_p) rp = refine_segment<NT>(xp, lo, hi, pp, c0, buf, cap, pe);
+    const double inf = __longlong_as_double(0x7ff0000000000000ll);
+    if (tid == 0) {
+        scr[2 * (size_t)G + b] = rs.E;
+        scr[3 * (size_t)G + b] = rs.A;
+        scr[4 * (size_t)G + b] = rs.bad ? inf : rs.B;
+        scr[5 * (size_t)G + b] = rp.E;
+        scr[6 * (size_t)G + b] = rp.A;
+        scr[7 * (size_t)G + b] = rp.bad ? inf : rp.B;
+    }
+    if (!grid_barrier(ctl, gen, s_fail)) return false;
+    // the same totals in every block: fixed per-thread slices, then a fixed
+    // reduction order; the bounds (j = 2, 5) rounded up
+    double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    for (uint32_t k = tid; k < G; k += NT) {
+#pragma unroll
+        for (int j = 0; j < 6; ++j) {
+            const double y = __ldcg(scr + (size_t)(2 + j) * G + k);
+            v[j] = (j == 2 || j == 5) ? __dadd_ru(v[j], y) : v[j] + y;
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 6; ++j)
+        for (int d = 16; d > 0; d >>= 1) {
+            const double y = __shfl_xor_sync(0xffffffffu, v[j], d);
+            v[j] = (j == 2 || j == 5) ? __dadd_ru(v[j], y) : v[j] + y;
+        }
+    if ((tid & 31u) == 0u)
+        for (int j = 0; j < 6; ++j) s_v[tid >> 5][j] = v[j];
+    __syncthreads();
+    if (tid == 0)
+        for (int j = 0; j < 6; ++j) {
+            double t = 0.0;
+            for (int w = 0; w < NT / 32; ++w) t = (j == 2 || j == 5) ? __dadd_ru(t, s_v[w][j]) : t + s_v[w][j];
+            s_t[j] = t;
+        }
+    __syncthreads();
+    double lo2, hi2;
+    const Refine Rs{s_t[0], s_t[1], s_t[2], !(s_t[2] < inf)};
+    if (!Rs.bad) {
+        refine_interval(ts, Rs, n, lo2, hi2);
+        serial_narrow(x, 0, lo2, hi2);
+    }
+    if (do_p) {
+        const Refine Rp{s_t[3], s_t[4], s_t[5], !(s_t[5] < inf)};
+        if (!Rp.bad) {
+            refine_interval(tp, Rp, n, lo2, hi2);
+            serial_narrow(x, 1, lo2, hi2);
+        }
+    }
+    x.d = serial_decide(x.lo, x.hi, x.s_exact, x.plo, x.phi, x.p_exact, sc.tol);
+    __syncthreads();   // s_t and s_b are free
+    return true;
+}
+
 template <int MS, bool UNI, int FU, bool SER = false, int MB = flood_min_blocks<MS, FU>()>
 __global__ void __launch_bounds__(flood_nt<MS>(), MB) k_flood_fused(const FloodArgs a, uint32_t ntiles) {
     constexpr int NT = flood_nt<MS>();
@@ -851,27 +1214,29 @@ __global__ void __launch_bounds__(flood_nt<MS>(), MB) k_flood_fused(const FloodA
             // triple-buffered by check, so no block overwrites them while
             // block 0 reads.
             SerialCheck x = serial_check(&s_ctl, broadcast_sum(tot));
+            if (x.d < 0 && !grid_refine<NT>(a, ctl, gen, &s_fail, x, s_ctl, sm, EMAX * MS, red)) break;
             if (x.d < 0) {
+                const bool s_ex0 = x.s_exact, p_ex0 = x.p_exact;
                 if (blockIdx.x == 0) {
-                    serial_form<NT>(x, &s_ctl, a.absdiff, sm, EMAX * MS);
+                    serial_form<NT>(x, &s_ctl, a.absdiff, sm, EMAX * MS, false);
                     if (threadIdx.x == 0) {
                         ctl->fb_s = x.s;
                         ctl->fb_p = (float)x.plo;
-                        ctl->fb_pform = x.p_exact && !s_ctl.prev_exact;
+                        ctl->fb_pform = x.p_exact && !p_ex0;
                     }
                 }
                 if (!grid_barrier(ctl, gen, &s_fail)) break;
                 if (blockIdx.x != 0) {
-                    x.s = *(volatile float *)&ctl->fb_s;
-                    x.lo = x.hi = (double)x.s;
-                    x.s_exact = true;
-                    x.sums = 1;
+                    if (!s_ex0) {
+                        x.s = *(volatile float *)&ctl->fb_s;
+                        x.lo = x.hi = (double)x.s;
+                        x.s_exact = true;
+                    }
                     if (*(volatile uint32_t *)&ctl->fb_pform) {
                         x.plo = x.phi = (double)*(volatile float *)&ctl->fb_p;
-                        x.p_exact = true;
-                        x.sums = 2;
+                        x.p_exact = x.p_new = true;
                     }
-                    x.d = serial_decide(x.lo, x.hi, true, x.plo, x.phi, x.p_exact, s_ctl.tol);
+                    x.d = serial_decide(x.lo, x.hi, x.s_exact, x.plo, x.phi, x.p_exact, s_ctl.tol);
                 }
             }
             __syncthreads();
@@ -899,6 +1264,9 @@ __global__ void __launch_bounds__(flood_nt<MS>(), MB) k_flood_fused(const FloodA
         ctl->cur_buf = s_ctl.cur_buf;
         ctl->prev_buf = s_ctl.prev_buf;
         ctl->serial_sums = s_ctl.serial_sums;
+        ctl->serial_refines = s_ctl.serial_refines;
+        ctl->delta_ref = s_ctl.delta_ref;
+        ctl->prev_ref = s_ctl.prev_ref;
         __threadfence();
         ctl->done = s_ctl.done;
     }
@@ -1351,6 +1719,16 @@ __global__ void k_send_from_beliefs(uint32_t E, const uint32_t *__restrict__ in_
 
 // one block forms the serial fp32 sum of x[0, n): the parallel form with NT
 // threads and cap floats of staging, or the one-thread chain
+__global__ void __launch_bounds__(256) k_serial_sum_bounds(const float *__restrict__ x, uint64_t n, double *lohi) {
+    __shared__ __align__(16) float buf[8192];
+    double lo = 0.0, hi = __longlong_as_double(0x7ff0000000000000ll);
+    refine_block<256>(x, n, buf, 8192, lo, hi);
+    if (threadIdx.x == 0) {
+        lohi[0] = lo;
+        lohi[1] = hi;
+    }
+}
+
 template <int NT>
 __global__ void __launch_bounds__(NT) k_serial_sum(const float *__restrict__ x, uint64_t n, float *out, int chain,
                                                   uint32_t cap) {
@@ -1958,6 +2336,13 @@ int bp_init_messages(bp_graph *g) {
     BP_DISPATCH_MS(g->ms, g->uniform != 0, launch_init, g);
 }
 
+int bp_serial_sum_bounds(const float *x, uint64_t n, double *lohi, void *stream) {
+    if (!lohi || (n && !x)) return set_error(BP_ERR_INVALID, "null argument");
+    k_serial_sum_bounds<<<1, 256, 0, (cudaStream_t)stream>>>(x, n, lohi);
+    BP_CUDA(cudaGetLastError());
+    return BP_OK;
+}
+
 int bp_serial_sum_f32(const float *x, uint64_t n, float *out, int method, void *stream) {
     if (!out || (n && !x)) return set_error(BP_ERR_INVALID, "null argument");
     cudaStream_t st = (cudaStream_t)stream;
@@ -2047,7 +2432,9 @@ int bp_loopy(bp_graph *g, const bp_loopy_options *opt, bp_loopy_result *res) {
             if ((st = fg())) return st;
         }
     }
-    if (fgrid) grid_blocks = std::max(grid_blocks, 2 * fgrid);   // double-buffered partials
+    // double-buffered partials, and in serial mode 8 more per block for the
+    // grid-wide narrowing
+    if (fgrid) grid_blocks = std::max(grid_blocks, (serial ? 10u : 2u) * fgrid);
     if ((st = ensure_partials(g, grid_blocks))) return st;
     if (serial && (st = ensure_absdiff(g))) return st;
     if (opt->schedule == BP_SCHEDULE_EDGE && (st = ensure_runs(g))) return st;
@@ -2150,6 +2537,7 @@ int bp_loopy(bp_graph *g, const bp_loopy_options *opt, bp_loopy_result *res) {
     r.delta_f64 = c.delta_d;
     r.elapsed_ms = ms;
     r.serial_sums = c.serial_sums;
+    r.serial_refines = c.serial_refines;
     if (opt->schedule == BP_SCHEDULE_NODE) g->latest = (int)((c.msg_parity0 + c.it) & 1u);
     if (c.done == 2 && c.final_i == max_it && opt->verbose)
         printf("No Convergence: previous: %f vs current: %f\n", (double)r.previous_delta, (double)r.delta);

@@ -49,7 +49,7 @@ class LoopyOptions(C.Structure):
 class LoopyResult(C.Structure):
     _fields_ = [("iterations", C.c_uint32), ("executed", C.c_uint32), ("converged", C.c_int32),
                 ("delta", C.c_float), ("previous_delta", C.c_float), ("delta_f64", C.c_double),
-                ("elapsed_ms", C.c_float), ("serial_sums", C.c_uint32)]
+                ("elapsed_ms", C.c_float), ("serial_sums", C.c_uint32), ("serial_refines", C.c_uint32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -172,6 +172,7 @@ def load(path=LIB_PATH):
         "bp_unrolled_destroy": ([vp], None), "bp_unrolled_set_stream": ([vp, vp], i32),
         "bp_unrolled_forward": ([vp, vp, vp, vp], i32), "bp_unrolled_backward": ([vp, vp, vp, vp], i32),
         "bp_serial_sum_f32": ([vp, C.c_uint64, vp, i32, vp], i32),
+        "bp_serial_sum_bounds": ([vp, C.c_uint64, vp, vp], i32),
         # graph.h
         "create_graph": ([C.c_uint, C.c_uint], C.POINTER(StructGraph)),
         "graph_add_node": ([vp, C.c_uint, C.c_char_p], None),

@@ -119,9 +119,10 @@ typedef struct {
     float previous_delta;     /* the reference's `previous_delta` at return */
     double delta_f64;         /* f64 sum of the last check's |diff| terms */
     float elapsed_ms;         /* device time of the iteration loop */
-    uint32_t serial_sums;     /* serial fp32 delta: checks whose stopping decision
-                               * needed the serial sum formed (the error bound of
-                               * the f64 sum could not decide) */
+    uint32_t serial_sums;     /* serial fp32 delta: serial sums formed because no
+                               * bound decided the stop */
+    uint32_t serial_refines;  /* serial fp32 delta: checks that needed the interval
+                               * narrowed from the terms' own rounding errors */
 } bp_loopy_result;
 
 typedef struct {
@@ -178,6 +179,12 @@ int bp_loopy(bp_graph *g, const bp_loopy_options *opt, bp_loopy_result *res);
  * staging (the iteration kernel's), 2 = 256 threads with 2048 floats,
  * 3 = the one-add-at-a-time chain. */
 int bp_serial_sum_f32(const float *x, uint64_t n, float *out, int method, void *stream);
+/* An interval [lohi[0], lohi[1]] (DEVICE doubles) holding that same serial
+ * sum, narrowed from the terms' own rounding errors: exact for every add where
+ * the running sum's binade is certain, half an ulp for the rest (binade
+ * crossings, exact ties).  [0, +inf] when there is none (an inf term, or n
+ * too large for the running bound). */
+int bp_serial_sum_bounds(const float *x, uint64_t n, double *lohi, void *stream);
 
 /* ---- loopy BP without allocating ------------------------------------- */
 /* No counterpart in the reference: an addition of this library.
