@@ -15,7 +15,10 @@ value  edge-msg updates/s over the whole job (E * iterations * N / max-rank time
        graph resident in HBM.
 e2e    the same metric through the public C-ABI with host (pinned) buffers:
        every step uploads the graph (edges, tables, priors), builds the
-       destination-sorted layout on the GPU, runs, and reads the beliefs back.
+       destination-sorted layout on the GPU, runs, and reads the beliefs back;
+       the steps are pipelined as a serving loop runs them (step k+1's upload
+       and build on a second stream and host thread during step k's solve),
+       timed by wall clock from the first upload to the last read.
 Multi-GPU: independent replicas, one per rank (weak scaling), no collective
 on the data path; the timing is the max over ranks.
 """
@@ -60,7 +63,7 @@ def parse():
     ap.add_argument("--iterations", type=int, default=100)
     ap.add_argument("--nodes", type=int, default=1 << 24)
     ap.add_argument("--edges", type=int, default=1 << 26)
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", choices=["power_law", "random10k", "batched", "tree", "unrolled",
@@ -750,21 +753,53 @@ def main():
 
         e2e_step()
         barrier()
+        # one step after another: the phases of a step
         t0 = time.perf_counter()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
         for _ in range(a.e2e_steps):
             e2e_step(record=True)
-        e1.record(stream)
         barrier()
-        ems = e0.elapsed_time(e1) / a.e2e_steps
-        wall = (time.perf_counter() - t0) / a.e2e_steps * 1e3
-        ems = max(ems, wall)
+        seq_ms = (time.perf_counter() - t0) / a.e2e_steps * 1e3
+
+        # pipelined, as a serving loop runs it: a second host thread builds
+        # graph k+1 (pinned-host upload, device CSR build, beliefs) on its own
+        # stream while this thread solves graph k and reads its beliefs back;
+        # every step's copies and work stay inside the timed region, which
+        # runs from before the first build to after the last read
+        from concurrent.futures import ThreadPoolExecutor
+        streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+        outs = [out_h, torch.empty((V, S), dtype=torch.float32).pin_memory()]
+
+        def build(k):
+            gk = BPGraph(V, src_h, dst_h, joint_h, uniform_states=2, stream=streams[k % 2].cuda_stream,
+                         reorder=bool(a.reorder))
+            gk.set_beliefs(bel_h)
+            return gk
+
+        def pipelined(n):
+            with ThreadPoolExecutor(max_workers=1) as ex:
+                fut = ex.submit(build, 0)
+                for k in range(n):
+                    gk = fut.result()
+                    if k + 1 < n:
+                        fut = ex.submit(build, k + 1)
+                    gk.init_messages()
+                    gk.loopy(0.0, a.iterations, delta="f64")
+                    gk.beliefs(out=outs[k % 2])
+                    gk.close()
+
+        pipelined(2)
+        barrier()
+        t0 = time.perf_counter()
+        pipelined(a.e2e_steps)
+        barrier()
+        ems = (time.perf_counter() - t0) / a.e2e_steps * 1e3
         ems = max_over_ranks(ems, dist)
         e2e = {"value": float(E) * a.iterations * world / (ems / 1e3), "unit": UNIT,
                "h2d_bytes_per_step": int(E * (4 + 4 + 4 * S * S) + V * 4 * S), "d2h_bytes_per_step": int(V * 4 * S),
-               "ms_per_step": ems, "phases_wall_ms": {k: round(v, 2) for k, v in phases.items()}}
+               "ms_per_step": ems, "steps": a.e2e_steps, "timing": "wall clock over all steps, first build included",
+               "pipelined": "the build of step k+1 (its H2D copies included) overlaps the solve of step k",
+               "sequential_ms_per_step": round(max_over_ranks(seq_ms, dist), 2),
+               "phases_wall_ms": {k: round(v, 2) for k, v in phases.items()}}
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
