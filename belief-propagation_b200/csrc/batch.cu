@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "bp_device.cuh"
+#include "bp_serial.cuh"
 #include "bp_internal.h"
 
 namespace bpx {
@@ -47,6 +48,8 @@ struct BatchArgs {
     const uint32_t *in_ptr, *in_src, *pos_edge;
     const float *joint;
     float *belief, *msg0, *msg1, *q0, *q1, *absdiff;
+    uint64_t ad_stride;   // floats between the two |diff| buffers (by iteration parity)
+    uint32_t sum_ch;      // serial mode: staging chunk of the block's serial sum (dynamic smem 2 sum_ch floats)
     NetResult *res;
     uint8_t *latest;
     float tol;
@@ -54,8 +57,70 @@ struct BatchArgs {
     int serial, init;
 };
 
+// the reference's serial fp32 sum of x[0, n) (graph.c:1300-1309), one thread
+__device__ __noinline__ float net_serial_sum(const float *x, uint64_t n) {
+    float s = 0.0f;
+    uint64_t k = 0;
+    for (; k + 4 <= n; k += 4) {
+        const float t0 = x[k], t1 = x[k + 1], t2 = x[k + 2], t3 = x[k + 3];
+        s = FADD(s, t0);
+        s = FADD(s, t1);
+        s = FADD(s, t2);
+        s = FADD(s, t3);
+    }
+    for (; k < n; ++k) s = FADD(s, x[k]);
+    return s;
+}
+
+// the same sum by the whole block: thread 0 adds in order out of shared
+// memory while threads 32.. stage the next ch terms (buf: 2 ch floats,
+// ch % 4 == 0); with fewer than 64 threads thread 0 reads global memory
+// itself.  Every thread calls it and gets the sum.
+__device__ float net_serial_sum_block(const float *x, uint64_t n, float *buf, uint32_t ch, float *s_res) {
+    const uint32_t T = blockDim.x, tid = threadIdx.x;
+    __syncthreads();   // buf and *s_res are free
+    if (T < 64 || ch == 0) {
+        if (tid == 0) *s_res = net_serial_sum(x, n);
+    } else {
+        const uint64_t nch = (n + ch - 1) / ch;
+        auto stage = [&](uint64_t c) {
+            const uint64_t base = c * ch;
+            const uint32_t cnt = (uint32_t)min((uint64_t)ch, n - base);
+            float *dst = buf + (c & 1) * ch;
+            for (uint32_t k = tid - 32; k < cnt; k += T - 32) dst[k] = x[base + k];
+        };
+        if (tid >= 32 && nch) stage(0);
+        __syncthreads();
+        float s = 0.0f;
+        for (uint64_t c = 0; c < nch; ++c) {
+            if (tid >= 32) {
+                if (c + 1 < nch) stage(c + 1);
+            } else if (tid == 0) {
+                const uint32_t cnt = (uint32_t)min((uint64_t)ch, n - c * ch);
+                const float *b = buf + (c & 1) * ch;
+                uint32_t k = 0;
+                for (; k + 4 <= cnt; k += 4) {
+                    const float4 v = *reinterpret_cast<const float4 *>(b + k);
+                    s = FADD(s, v.x);
+                    s = FADD(s, v.y);
+                    s = FADD(s, v.z);
+                    s = FADD(s, v.w);
+                }
+                for (; k < cnt; ++k) s = FADD(s, b[k]);
+            }
+            __syncthreads();
+        }
+        if (tid == 0) *s_res = s;
+    }
+    __syncthreads();
+    const float r = *s_res;
+    __syncthreads();
+    return r;
+}
+
 template <int S>
-__device__ void solve_network(const BatchArgs &a, uint32_t n, double *red, int *s_flag) {
+__device__ void solve_network(const BatchArgs &a, uint32_t n, double *red, int *s_flag, double *s_tot, float *s_res,
+                              float *sbuf) {
     const NetInfo ni = a.info[n];
     const uint32_t V = ni.V, E = ni.E;
     const uint32_t *ptr = a.in_ptr + ni.ptr_off;
@@ -91,6 +156,15 @@ __device__ void solve_network(const BatchArgs &a, uint32_t n, double *red, int *
 
     float prev_f = -1.0f, delta_f = 0.0f;
     double prev_d = -1.0, delta_d = 0.0;
+    // serial delta (thread 0): intervals of the serial sums of this check and
+    // of the previous one, whether each is the sum itself, and their buffers
+    double d_lo = 0.0, d_hi = 0.0, p_lo = -1.0, p_hi = -1.0;
+    bool d_ex = true, p_ex = true, d_ref = false, p_ref = false;
+    // the narrowed interval needs 3 floats of staging per thread
+    const bool refine_ok = blockDim.x <= 1024 && 3u * blockDim.x <= 2u * a.sum_ch;
+    uint32_t d_buf = 0, p_buf = 0;
+    const uint64_t nterms = (uint64_t)E * S;
+    const float *ad_base = a.serial ? a.absdiff + ni.msg_off : nullptr;
     uint32_t it = 0, ret = a.max_it, converged = 0;
     for (it = 0; it < a.max_it; ++it) {
         const float *m_old = msg[latest];
@@ -111,7 +185,10 @@ __device__ void solve_network(const BatchArgs &a, uint32_t n, double *red, int *
                 ad[k] = fabsf(d);
                 dsum += (double)ad[k];
             }
-            if (a.serial) stv<S>(a.absdiff + ni.msg_off + (size_t)a.pos_edge[ni.edge_off + p] * S, ad);
+            if (a.serial)
+                stv<S>(a.absdiff + (size_t)(it & 1u) * a.ad_stride + ni.msg_off +
+                           (size_t)a.pos_edge[ni.edge_off + p] * S,
+                       ad);
             stv<S>(m_new + (size_t)p * S, m);
         }
         __syncthreads();
@@ -154,20 +231,85 @@ __device__ void solve_network(const BatchArgs &a, uint32_t n, double *red, int *
                 tot = warp_sum(t);
             }
         }
-        if (tid == 0) {
-            bool stop;
-            if (a.serial) {
-                float s = 0.0f;
-                const float *ad = a.absdiff + ni.msg_off;
-                for (uint64_t k = 0; k < (uint64_t)E * S; ++k) s = FADD(s, ad[k]);
-                delta_f = s;
-                delta_d = s;
-                stop = (s < a.tol) || (fabsf(FSUB(s, prev_f)) < a.tol);
-            } else {
-                delta_d = tot;
-                delta_f = (float)tot;
-                stop = (tot < (double)a.tol) || (fabs(tot - prev_d) < (double)a.tol);
+        if (a.serial) {
+            // every thread takes the same decision: the f64 sum to all, the
+            // reference's serial fp32 decision from its interval, and the
+            // serial sums (formed by the whole block) only where it straddles
+            if (tid == 0) *s_tot = tot;
+            __syncthreads();
+            tot = *s_tot;
+            double lo, hi;
+            serial_interval(tot, nterms, lo, hi);
+            bool s_ex = false, s_ref = false;
+            float s = (float)tot;
+            int d = serial_decide(lo, hi, false, p_lo, p_hi, p_ex, a.tol);
+            const float *ad_cur = ad_base + (size_t)(it & 1u) * a.ad_stride;
+            const float *ad_prev = ad_base + (size_t)p_buf * a.ad_stride;
+            // narrowed from the terms' own rounding errors (intersected with
+            // the bound; an interval holding one float gives the sum)
+            auto narrow = [&](double &L, double &H, bool &ex, float &val, double l2, double h2) {
+                L = fmax(L, l2);
+                H = fmin(H, h2);
+                float f;
+                if (interval_pins(L, H, f)) {
+                    L = H = (double)f;
+                    ex = true;
+                    val = f;
+                }
+            };
+            if (d < 0 && refine_ok) {
+                double l2, h2;
+                if (refine_block<1024>(ad_cur, nterms, sbuf, 2 * a.sum_ch, l2, h2)) narrow(lo, hi, s_ex, s, l2, h2);
+                s_ref = true;
+                d = serial_decide(lo, hi, s_ex, p_lo, p_hi, p_ex, a.tol);
+                if (d < 0 && !p_ex && !p_ref) {
+                    if (refine_block<1024>(ad_prev, nterms, sbuf, 2 * a.sum_ch, l2, h2))
+                        narrow(p_lo, p_hi, p_ex, prev_f, l2, h2);
+                    p_ref = true;
+                    d = serial_decide(lo, hi, s_ex, p_lo, p_hi, p_ex, a.tol);
+                }
             }
+            if (d < 0 && !s_ex) {
+                s = net_serial_sum_block(ad_cur, nterms, sbuf, a.sum_ch, s_res);
+                lo = hi = (double)s;
+                s_ex = true;
+                d = serial_decide(lo, hi, true, p_lo, p_hi, p_ex, a.tol);
+            }
+            if (d < 0) {
+                prev_f = net_serial_sum_block(ad_prev, nterms, sbuf, a.sum_ch, s_res);
+                p_lo = p_hi = (double)prev_f;
+                p_ex = true;
+                d = serial_decide(lo, hi, true, p_lo, p_hi, true, a.tol);
+            }
+            delta_f = s;
+            delta_d = tot;
+            d_lo = lo;
+            d_hi = hi;
+            d_ex = s_ex;
+            d_ref = s_ref;
+            d_buf = it & 1u;
+            const bool stop = d == 1;
+            if (stop) {
+                ret = it;
+                converged = 1;
+            } else if (it < a.max_it - 1) {
+                prev_f = delta_f;
+                prev_d = delta_d;
+                p_lo = d_lo;
+                p_hi = d_hi;
+                p_ex = d_ex;
+                p_ref = d_ref;
+                p_buf = d_buf;
+            }
+            latest ^= 1;
+            __syncthreads();   // *s_tot is rewritten next iteration
+            if (stop) break;
+            continue;
+        }
+        if (tid == 0) {
+            delta_d = tot;
+            delta_f = (float)tot;
+            const bool stop = (tot < (double)a.tol) || (fabs(tot - prev_d) < (double)a.tol);
             if (stop) {
                 ret = it;
                 converged = 1;
@@ -183,6 +325,10 @@ __device__ void solve_network(const BatchArgs &a, uint32_t n, double *red, int *
         __syncthreads();
         if (stop) break;
     }
+    // the returned delta and previous delta where the loop decided without
+    // forming them (the whole block; every thread has the same flags)
+    if (a.serial && !d_ex) delta_f = net_serial_sum_block(ad_base + (size_t)d_buf * a.ad_stride, nterms, sbuf, a.sum_ch, s_res);
+    if (a.serial && !p_ex) prev_f = net_serial_sum_block(ad_base + (size_t)p_buf * a.ad_stride, nterms, sbuf, a.sum_ch, s_res);
     if (tid == 0) {
         NetResult r;
         r.iterations = converged ? ret : a.max_it;
@@ -204,13 +350,16 @@ __global__ void k_batch_solve(const BatchArgs a, const uint32_t *__restrict__ or
     __shared__ double red[32];
     __shared__ int s_flag;
     __shared__ uint32_t s_next;
+    __shared__ double s_tot;
+    __shared__ float s_res;
+    extern __shared__ __align__(16) float sbuf[];   // serial mode: 2 sum_ch floats
     for (;;) {
         if (threadIdx.x == 0) s_next = atomicAdd(queue, 1u);
         __syncthreads();
         const uint32_t k = s_next;
         __syncthreads();
         if (k >= count) break;
-        solve_network<S>(a, order[k], red, &s_flag);
+        solve_network<S>(a, order[k], red, &s_flag, &s_tot, &s_res, sbuf);
     }
 }
 
@@ -267,7 +416,8 @@ namespace bpx {
 template <int S>
 static int launch_group(bp_batch *bt, Group &gr, const BatchArgs &a, uint32_t gi, uint32_t block, uint32_t grid,
                         cudaStream_t s) {
-    k_batch_solve<S><<<grid, block, 0, s>>>(a, gr.d_order, (uint32_t)gr.order.size(), bt->queues + gi);
+    k_batch_solve<S><<<grid, block, sizeof(float) * 2 * a.sum_ch, s>>>(a, gr.d_order, (uint32_t)gr.order.size(),
+                                                                         bt->queues + gi);
     BP_CUDA(cudaGetLastError());
     return BP_OK;
 }
@@ -288,6 +438,8 @@ static int launch_group_s(bp_batch *bt, Group &gr, const BatchArgs &a, uint32_t 
     }
 }
 
+constexpr uint32_t kSumChunk = 1024;   // serial mode: 8 KB of dynamic shared memory per block
+
 static BatchArgs batch_args(bp_batch *bt, float tol, uint32_t max_it, int serial, int init) {
     BatchArgs a;
     a.info = bt->d_info;
@@ -301,6 +453,8 @@ static BatchArgs batch_args(bp_batch *bt, float tol, uint32_t max_it, int serial
     a.q0 = bt->q[0];
     a.q1 = bt->q[1];
     a.absdiff = bt->absdiff;
+    a.sum_ch = serial ? kSumChunk : 0u;
+    a.ad_stride = bt->totMsgF + 4;   // totMsgF % 4 == 0: buffer 1 keeps the 16-byte alignment of buffer 0
     a.res = bt->res;
     a.latest = bt->latest;
     a.tol = tol;
@@ -312,26 +466,26 @@ static BatchArgs batch_args(bp_batch *bt, float tol, uint32_t max_it, int serial
 
 // blocks that fit on the GPU at once for this group
 template <int S>
-static uint32_t occupancy_grid(bp_batch *bt, uint32_t block) {
+static uint32_t occupancy_grid(bp_batch *bt, uint32_t block, size_t dyn) {
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_solve<S>, (int)block, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_solve<S>, (int)block, dyn);
     if (per_sm < 1) per_sm = 1;
     return (uint32_t)per_sm * (uint32_t)bt->sm_count;
 }
 
-static uint32_t grid_for_group(bp_batch *bt, const Group &gr, uint32_t block) {
+static uint32_t grid_for_group(bp_batch *bt, const Group &gr, uint32_t block, size_t dyn = 0) {
     uint32_t g = 0;
     switch (gr.S) {
-    case 1: g = occupancy_grid<1>(bt, block); break;
-    case 2: g = occupancy_grid<2>(bt, block); break;
-    case 3: g = occupancy_grid<3>(bt, block); break;
-    case 4: g = occupancy_grid<4>(bt, block); break;
-    case 5: g = occupancy_grid<5>(bt, block); break;
-    case 6: g = occupancy_grid<6>(bt, block); break;
-    case 7: g = occupancy_grid<7>(bt, block); break;
-    case 8: g = occupancy_grid<8>(bt, block); break;
-    case 9: g = occupancy_grid<9>(bt, block); break;
-    default: g = occupancy_grid<10>(bt, block); break;
+    case 1: g = occupancy_grid<1>(bt, block, dyn); break;
+    case 2: g = occupancy_grid<2>(bt, block, dyn); break;
+    case 3: g = occupancy_grid<3>(bt, block, dyn); break;
+    case 4: g = occupancy_grid<4>(bt, block, dyn); break;
+    case 5: g = occupancy_grid<5>(bt, block, dyn); break;
+    case 6: g = occupancy_grid<6>(bt, block, dyn); break;
+    case 7: g = occupancy_grid<7>(bt, block, dyn); break;
+    case 8: g = occupancy_grid<8>(bt, block, dyn); break;
+    case 9: g = occupancy_grid<9>(bt, block, dyn); break;
+    default: g = occupancy_grid<10>(bt, block, dyn); break;
     }
     return std::min<uint32_t>(g, (uint32_t)gr.order.size());
 }
@@ -345,7 +499,9 @@ static int enqueue_batch(bp_batch *bt, const BatchArgs &a) {
         Group &gr = bt->groups[gi];
         cudaStream_t s = bt->side[gi];
         BP_CUDA(cudaStreamWaitEvent(s, bt->fork_ev, 0));
-        int st = launch_group_s(bt, gr, a, (uint32_t)gi, gr.block, gr.grid, s);
+        // serial mode holds 2 sum_ch floats of dynamic shared memory per block
+        const uint32_t grid = a.sum_ch ? grid_for_group(bt, gr, gr.block, sizeof(float) * 2 * a.sum_ch) : gr.grid;
+        int st = launch_group_s(bt, gr, a, (uint32_t)gi, gr.block, grid, s);
         if (st) return st;
         BP_CUDA(cudaEventRecord(bt->side_ev[gi], s));
         BP_CUDA(cudaStreamWaitEvent(bt->stream, bt->side_ev[gi], 0));
@@ -673,7 +829,7 @@ int bp_batch_autotune(bp_batch *bt, const bp_batch_options *o) {
     if (!bt || !o) return set_error(BP_ERR_INVALID, "null argument");
     static const uint32_t cand[] = {64, 128, 256, 512};
     const int serial = o->delta_mode == BP_DELTA_SERIAL_F32;
-    if (serial && !bt->absdiff) BP_CUDA(cudaMalloc((void **)&bt->absdiff, sizeof(float) * (bt->totMsgF + 1)));
+    if (serial && !bt->absdiff) BP_CUDA(cudaMalloc((void **)&bt->absdiff, sizeof(float) * 2 * (bt->totMsgF + 4)));
     // beliefs are overwritten by trial runs: keep them
     float *keep = nullptr;
     BP_CUDA(cudaMalloc((void **)&keep, sizeof(float) * (bt->totNodeF + 1)));
@@ -689,7 +845,7 @@ int bp_batch_autotune(bp_batch *bt, const bp_batch_options *o) {
         if (!best) {
             float best_ms = 1e30f;
             for (uint32_t c : cand) {
-                const uint32_t grid = grid_for_group(bt, gr, c);
+                const uint32_t grid = grid_for_group(bt, gr, c, sizeof(float) * 2 * a.sum_ch);
                 float tot = 0.0f;
                 for (int rep = 0; rep < 2; ++rep) {
                     BP_CUDA(cudaMemcpyAsync(bt->belief, keep, sizeof(float) * bt->totNodeF, cudaMemcpyDeviceToDevice,
@@ -746,7 +902,7 @@ int bp_batch_loopy(bp_batch *bt, const bp_batch_options *o, bp_batch_result *r) 
         return set_error(BP_ERR_INVALID, "unknown delta mode %d", o->delta_mode);
     const int serial = o->delta_mode == BP_DELTA_SERIAL_F32;
     if (serial && !bt->absdiff) {
-        BP_CUDA(cudaMalloc((void **)&bt->absdiff, sizeof(float) * (bt->totMsgF + 1)));
+        BP_CUDA(cudaMalloc((void **)&bt->absdiff, sizeof(float) * 2 * (bt->totMsgF + 4)));
         if (bt->exec) {
             cudaGraphExecDestroy(bt->exec);
             bt->exec = nullptr;

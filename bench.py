@@ -66,6 +66,9 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--batch-delta", choices=["serial", "f64"], default="f64",
+                    help="batched workload's stopping rule: the reference's serial fp32 delta (decided by "
+                         "bounds) or a deterministic fp64 sum")
     ap.add_argument("--workload", choices=["power_law", "random10k", "batched", "tree", "unrolled",
                                            "unrolled_batch"],
                     default="power_law",
@@ -266,11 +269,11 @@ def run_batched(a, rank, world):
     prior = torch.from_numpy(b.pack_beliefs()).cuda()
     b.set_beliefs(prior)
     os.environ.setdefault("BP_AUTOTUNE_CACHE", os.path.join(ROOT, "gpurun_out", "bp_autotune.txt"))
-    tuned = b.autotune(tol=1e-4, max_iterations=200)
+    tuned = b.autotune(tol=1e-4, max_iterations=200, delta=a.batch_delta)
 
     def step():
         b.set_beliefs(prior)
-        return b.loopy(tol=1e-4, max_iterations=200)
+        return b.loopy(tol=1e-4, max_iterations=200, delta=a.batch_delta)
 
     for _ in range(a.warmup):
         step()
@@ -305,7 +308,7 @@ def run_batched(a, rank, world):
             g.set_beliefs(p)
             g.latest_slot = 1
             g.init_messages()
-            g.loopy(1e-4, 200, delta="f64")
+            g.loopy(1e-4, 200, delta=a.batch_delta)
 
     solo_all()
     torch.cuda.synchronize()
@@ -342,6 +345,8 @@ def run_batched(a, rank, world):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"{a.networks} independent networks, V log-uniform [32,4096], E U(2,6)xV, "
                                    "S in {2,3,4,8}, tol 1e-4 per network, max 200 iterations, seed 2",
+                       "delta": a.batch_delta + (" (the reference's serial fp32 stopping rule, decided by bounds)"
+                                                 if a.batch_delta == "serial" else " (deterministic fp64 sum)"),
                        "nodes": int(sum(n.V for n in nets)), "edges": int(edges), "block_threads": tuned,
                        "generator_s": round(gen_s, 1), "l2": "batch working set larger than L2"},
             "converged": int(r["converged"]), "max_iterations_run": int(r["max_executed"]),

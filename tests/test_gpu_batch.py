@@ -39,6 +39,7 @@ def test_batch_matches_each_network_alone(bp, small_batch, restatement, O, delta
             if delta == "serial":
                 ora = restatement.loopy(O.OracleGraph(net), 1e-4, 120)
                 assert res["iterations"][k] == ora["ret"], k
+                assert np.float32(res["delta"][k]) == np.float32(ora["delta"]), k
                 np.testing.assert_array_equal(b.beliefs(k), ora["beliefs"][:, :S])
                 np.testing.assert_array_equal(b.messages(k), ora["latest"][:, :S])
             else:
