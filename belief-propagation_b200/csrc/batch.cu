@@ -118,7 +118,7 @@ __device__ float net_serial_sum_block(const float *x, uint64_t n, float *buf, ui
     return r;
 }
 
-template <int S>
+template <int S, bool SER>
 __device__ void solve_network(const BatchArgs &a, uint32_t n, double *red, int *s_flag, double *s_tot, float *s_res,
                               float *sbuf) {
     const NetInfo ni = a.info[n];
@@ -164,7 +164,7 @@ __device__ void solve_network(const BatchArgs &a, uint32_t n, double *red, int *
     const bool refine_ok = blockDim.x <= 1024 && 3u * blockDim.x <= 2u * a.sum_ch;
     uint32_t d_buf = 0, p_buf = 0;
     const uint64_t nterms = (uint64_t)E * S;
-    const float *ad_base = a.serial ? a.absdiff + ni.msg_off : nullptr;
+    const float *ad_base = SER ? a.absdiff + ni.msg_off : nullptr;
     uint32_t it = 0, ret = a.max_it, converged = 0;
     for (it = 0; it < a.max_it; ++it) {
         const float *m_old = msg[latest];
@@ -185,7 +185,7 @@ __device__ void solve_network(const BatchArgs &a, uint32_t n, double *red, int *
                 ad[k] = fabsf(d);
                 dsum += (double)ad[k];
             }
-            if (a.serial)
+            if constexpr (SER)
                 stv<S>(a.absdiff + (size_t)(it & 1u) * a.ad_stride + ni.msg_off +
                            (size_t)a.pos_edge[ni.edge_off + p] * S,
                        ad);
@@ -231,7 +231,7 @@ __device__ void solve_network(const BatchArgs &a, uint32_t n, double *red, int *
                 tot = warp_sum(t);
             }
         }
-        if (a.serial) {
+        if constexpr (SER) {
             // every thread takes the same decision: the f64 sum to all, the
             // reference's serial fp32 decision from its interval, and the
             // serial sums (formed by the whole block) only where it straddles
@@ -327,8 +327,8 @@ __device__ void solve_network(const BatchArgs &a, uint32_t n, double *red, int *
     }
     // the returned delta and previous delta where the loop decided without
     // forming them (the whole block; every thread has the same flags)
-    if (a.serial && !d_ex) delta_f = net_serial_sum_block(ad_base + (size_t)d_buf * a.ad_stride, nterms, sbuf, a.sum_ch, s_res);
-    if (a.serial && !p_ex) prev_f = net_serial_sum_block(ad_base + (size_t)p_buf * a.ad_stride, nterms, sbuf, a.sum_ch, s_res);
+    if (SER && !d_ex) delta_f = net_serial_sum_block(ad_base + (size_t)d_buf * a.ad_stride, nterms, sbuf, a.sum_ch, s_res);
+    if (SER && !p_ex) prev_f = net_serial_sum_block(ad_base + (size_t)p_buf * a.ad_stride, nterms, sbuf, a.sum_ch, s_res);
     if (tid == 0) {
         NetResult r;
         r.iterations = converged ? ret : a.max_it;
@@ -344,7 +344,7 @@ __device__ void solve_network(const BatchArgs &a, uint32_t n, double *red, int *
     __syncthreads();
 }
 
-template <int S>
+template <int S, bool SER>
 __global__ void k_batch_solve(const BatchArgs a, const uint32_t *__restrict__ order, uint32_t count,
                               uint32_t *queue) {
     __shared__ double red[32];
@@ -359,7 +359,7 @@ __global__ void k_batch_solve(const BatchArgs a, const uint32_t *__restrict__ or
         const uint32_t k = s_next;
         __syncthreads();
         if (k >= count) break;
-        solve_network<S>(a, order[k], red, &s_flag, &s_tot, &s_res, sbuf);
+        solve_network<S, SER>(a, order[k], red, &s_flag, &s_tot, &s_res, sbuf);
     }
 }
 
@@ -416,8 +416,11 @@ namespace bpx {
 template <int S>
 static int launch_group(bp_batch *bt, Group &gr, const BatchArgs &a, uint32_t gi, uint32_t block, uint32_t grid,
                         cudaStream_t s) {
-    k_batch_solve<S><<<grid, block, sizeof(float) * 2 * a.sum_ch, s>>>(a, gr.d_order, (uint32_t)gr.order.size(),
-                                                                         bt->queues + gi);
+    if (a.serial)
+        k_batch_solve<S, true><<<grid, block, sizeof(float) * 2 * a.sum_ch, s>>>(a, gr.d_order,
+                                                                               (uint32_t)gr.order.size(), bt->queues + gi);
+    else
+        k_batch_solve<S, false><<<grid, block, 0, s>>>(a, gr.d_order, (uint32_t)gr.order.size(), bt->queues + gi);
     BP_CUDA(cudaGetLastError());
     return BP_OK;
 }
@@ -468,7 +471,8 @@ static BatchArgs batch_args(bp_batch *bt, float tol, uint32_t max_it, int serial
 template <int S>
 static uint32_t occupancy_grid(bp_batch *bt, uint32_t block, size_t dyn) {
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_solve<S>, (int)block, dyn);
+    if (dyn) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_solve<S, true>, (int)block, dyn);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_solve<S, false>, (int)block, 0);
     if (per_sm < 1) per_sm = 1;
     return (uint32_t)per_sm * (uint32_t)bt->sm_count;
 }
@@ -500,7 +504,8 @@ static int enqueue_batch(bp_batch *bt, const BatchArgs &a) {
         cudaStream_t s = bt->side[gi];
         BP_CUDA(cudaStreamWaitEvent(s, bt->fork_ev, 0));
         // serial mode holds 2 sum_ch floats of dynamic shared memory per block
-        const uint32_t grid = a.sum_ch ? grid_for_group(bt, gr, gr.block, sizeof(float) * 2 * a.sum_ch) : gr.grid;
+        const uint32_t grid =
+            a.sum_ch ? std::min(gr.grid, grid_for_group(bt, gr, gr.block, sizeof(float) * 2 * a.sum_ch)) : gr.grid;
         int st = launch_group_s(bt, gr, a, (uint32_t)gi, gr.block, grid, s);
         if (st) return st;
         BP_CUDA(cudaEventRecord(bt->side_ev[gi], s));
@@ -672,7 +677,11 @@ static int batch_create_impl(bp_batch *bt, uint32_t N, const bp_graph_desc *desc
 }
 
 // ---- autotuning of threads per block, cached on disk ---------------------
-static std::string tune_key(bp_batch *bt, const Group &gr) {
+// kernel revision in the autotune key: a cached block size belongs to the
+// kernel it was timed on
+constexpr int kTuneRevision = 3;
+
+static std::string tune_key(bp_batch *bt, const Group &gr, int serial) {
     uint64_t V = 0, E = 0;
     for (uint32_t n : gr.order) {
         V += bt->info[n].V;
@@ -687,8 +696,8 @@ static std::string tune_key(bp_batch *bt, const Group &gr) {
     cudaGetDevice(&dev);
     cudaGetDeviceProperties(&prop, dev);
     char buf[256];
-    snprintf(buf, sizeof buf, "%s|S=%d|log2V=%u|deg10=%u|nets=%llu", prop.name, gr.S, lv, deg10,
-             (unsigned long long)(cnt >= 1024 ? 1024 : cnt));
+    snprintf(buf, sizeof buf, "%s|S=%d|log2V=%u|deg10=%u|nets=%llu|delta=%s|rev=%d", prop.name, gr.S, lv, deg10,
+             (unsigned long long)(cnt >= 1024 ? 1024 : cnt), serial ? "serial" : "f64", kTuneRevision);
     for (char *c = buf; *c; ++c)
         if (*c == ' ') *c = '_';
     return buf;
@@ -701,18 +710,23 @@ static std::string cache_path() {
     return std::string(home ? home : "/tmp") + "/.cache/bp_b200_autotune.txt";
 }
 
-static uint32_t cache_lookup(const std::string &key) {
+// a cached (block, grid) for the key, or block 0
+static uint32_t cache_lookup(const std::string &key, uint32_t *grid) {
     FILE *f = fopen(cache_path().c_str(), "r");
     if (!f) return 0;
-    char k[256];
-    unsigned b = 0, found = 0;
-    while (fscanf(f, "%255s %u", k, &b) == 2)
-        if (key == k) found = b;
+    char line[512], k[256];
+    unsigned b = 0, gsz = 0, found = 0, found_g = 0;
+    while (fgets(line, sizeof line, f))
+        if (sscanf(line, "%255s %u %u", k, &b, &gsz) == 3 && key == k) {
+            found = b;
+            found_g = gsz;
+        }
     fclose(f);
+    *grid = found_g;
     return found;
 }
 
-static void cache_store(const std::string &key, uint32_t block) {
+static void cache_store(const std::string &key, uint32_t block, uint32_t grid) {
     std::string path = cache_path();
     std::string dir = path.substr(0, path.find_last_of('/'));
     if (!dir.empty()) {
@@ -721,7 +735,7 @@ static void cache_store(const std::string &key, uint32_t block) {
     }
     FILE *f = fopen(path.c_str(), "a");
     if (!f) return;
-    fprintf(f, "%s %u\n", key.c_str(), block);
+    fprintf(f, "%s %u %u\n", key.c_str(), block, grid);
     fclose(f);
 }
 
@@ -840,12 +854,26 @@ int bp_batch_autotune(bp_batch *bt, const bp_batch_options *o) {
     const BatchArgs a = batch_args(bt, o->tolerance, o->max_iterations, serial, o->init_messages);
     for (size_t gi = 0; gi < bt->groups.size(); ++gi) {
         Group &gr = bt->groups[gi];
-        const std::string key = tune_key(bt, gr);
-        uint32_t best = cache_lookup(key);
+        const std::string key = tune_key(bt, gr, serial);
+        uint32_t best_grid = 0;
+        uint32_t best = cache_lookup(key, &best_grid);
         if (!best) {
             float best_ms = 1e30f;
+            // block sizes, and networks in flight: a block keeps its
+            // network's arrays in L2 across its iterations, so fewer blocks
+            // than the GPU holds can be faster once the networks in flight
+            // outgrow L2
+            std::vector<std::pair<uint32_t, uint32_t>> trials;
             for (uint32_t c : cand) {
-                const uint32_t grid = grid_for_group(bt, gr, c, sizeof(float) * 2 * a.sum_ch);
+                const uint32_t occ = grid_for_group(bt, gr, c, sizeof(float) * 2 * a.sum_ch);
+                trials.push_back({c, occ});
+                for (uint32_t per_sm : {1u, 2u, 4u, 8u}) {
+                    const uint32_t g = per_sm * (uint32_t)bt->sm_count;
+                    if (g < occ) trials.push_back({c, g});
+                }
+            }
+            for (const auto &tr : trials) {
+                const uint32_t c = tr.first, grid = tr.second;
                 float tot = 0.0f;
                 for (int rep = 0; rep < 2; ++rep) {
                     BP_CUDA(cudaMemcpyAsync(bt->belief, keep, sizeof(float) * bt->totNodeF, cudaMemcpyDeviceToDevice,
@@ -867,12 +895,14 @@ int bp_batch_autotune(bp_batch *bt, const bp_batch_options *o) {
                 if (tot < best_ms) {
                     best_ms = tot;
                     best = c;
+                    best_grid = grid;
                 }
             }
-            cache_store(key, best);
+            cache_store(key, best, best_grid);
         }
         gr.block = best;
-        gr.grid = grid_for_group(bt, gr, best);
+        const uint32_t occ = grid_for_group(bt, gr, best);
+        gr.grid = best_grid ? std::min(best_grid, occ) : occ;
     }
     BP_CUDA(cudaMemcpyAsync(bt->belief, keep, sizeof(float) * bt->totNodeF, cudaMemcpyDeviceToDevice, bt->stream));
     BP_CUDA(cudaMemcpyAsync(bt->latest, latest0.data(), bt->N, cudaMemcpyHostToDevice, bt->stream));
