@@ -75,6 +75,11 @@ class BPGraph:
             g.set_beliefs(net.beliefs)
         return g
 
+    def set_stream(self, stream):
+        """Run this graph's later work on `stream` (a cudaStream_t as int);
+        its pending work on the old stream is finished first."""
+        N.check(self.lib.bp_set_stream(self.h, stream))
+
     def close(self):
         if getattr(self, "h", None):
             self.lib.bp_graph_destroy(self.h)

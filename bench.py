@@ -771,7 +771,12 @@ def main():
         # every step's copies and work stay inside the timed region, which
         # runs from before the first build to after the last read
         from concurrent.futures import ThreadPoolExecutor
-        streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+        # the builds yield the SMs to the solve (stream priorities); their
+        # copies run on the copy engines either way
+        lo_prio, hi_prio = torch.cuda.Stream.priority_range() if hasattr(torch.cuda.Stream, "priority_range") \
+            else (0, -1)
+        streams = [torch.cuda.Stream(priority=lo_prio), torch.cuda.Stream(priority=lo_prio)]
+        solve_stream = torch.cuda.Stream(priority=hi_prio)
         outs = [out_h, torch.empty((V, S), dtype=torch.float32).pin_memory()]
 
         def build(k):
@@ -787,6 +792,7 @@ def main():
                     gk = fut.result()
                     if k + 1 < n:
                         fut = ex.submit(build, k + 1)
+                    gk.set_stream(solve_stream.cuda_stream)
                     gk.init_messages()
                     gk.loopy(0.0, a.iterations, delta="f64")
                     gk.beliefs(out=outs[k % 2])
