@@ -374,12 +374,12 @@ __device__ float block_serial_sum(const float *__restrict__ x, uint64_t n, float
 }
 
 // the serial sum by whichever form is faster for the block: the parallel
-// scan needs many threads and terms per thread to beat the chain (measured
-// on 80k terms: 256 threads with 8192 floats of staging 190 us, the chain
-// 224 us, 128 threads with 2048 floats 257 us)
+// scan needs at least 256 threads to beat the chain (measured on 80k terms:
+// 1024 threads with 8192 floats of staging 140 us, 256 threads 180-190 us,
+// the chain 224 us, 128 threads with 2048 floats 257 us)
 template <int NT>
 __device__ __forceinline__ float exact_serial_sum(const float *x, uint64_t n, float *buf, uint32_t cap) {
-    if (NT >= 256 && cap >= 24u * NT) return block_serial_sum<NT>(x, n, buf, cap);
+    if (NT >= 256 && cap >= 8u * NT) return block_serial_sum<NT>(x, n, buf, cap);
     return block_serial_sum_chain<NT>(x, n, buf, (cap / 2u) & ~3u);
 }
 
@@ -1506,14 +1506,14 @@ __global__ void __launch_bounds__(NT) k_serial_sum(const float *__restrict__ x, 
 // the reference's `delta` and `previous_delta` at return (graph.c:1300-1318)
 // where the loop decided from bounds without forming them: block 0 sums the
 // last check's terms, block 1 the check's before (serial fp32, edge-id order)
-__global__ void __launch_bounds__(256) k_delta_final(LoopyCtl *ctl, const float *__restrict__ absdiff) {
+__global__ void __launch_bounds__(1024) k_delta_final(LoopyCtl *ctl, const float *__restrict__ absdiff) {
     __shared__ __align__(16) float buf[2 * 4096];
     const LoopyCtl c = *ctl;
     if (!c.serial || c.done == 0 || c.done == 3 || c.bar_fail) return;
     const bool prev = blockIdx.x == 1;
     if (prev ? c.prev_exact : c.delta_exact) return;
     const uint32_t b = prev ? c.prev_buf : c.cur_buf;
-    const float s = exact_serial_sum<256>(absdiff + (size_t)b * c.ad_stride, c.n_terms, buf, 2 * 4096);
+    const float s = exact_serial_sum<1024>(absdiff + (size_t)b * c.ad_stride, c.n_terms, buf, 2 * 4096);
     if (threadIdx.x == 0) {
         if (prev) ctl->prev_f = s;
         else ctl->delta_f = s;
@@ -2117,6 +2117,7 @@ int bp_serial_sum_f32(const float *x, uint64_t n, float *out, int method, void *
     case 1: k_serial_sum<128><<<1, 128, 0, st>>>(x, n, out, 0, 2048); break;
     case 2: k_serial_sum<256><<<1, 256, 0, st>>>(x, n, out, 0, 2048); break;
     case 3: k_serial_sum<256><<<1, 256, 0, st>>>(x, n, out, 1, 8192); break;
+    case 4: k_serial_sum<1024><<<1, 1024, 0, st>>>(x, n, out, 0, 8192); break;
     default: return set_error(BP_ERR_INVALID, "unknown method %d", method);
     }
     BP_CUDA(cudaGetLastError());
@@ -2283,7 +2284,7 @@ int bp_loopy(bp_graph *g, const bp_loopy_options *opt, bp_loopy_result *res) {
     if (serial) {
         // the returned delta and previous delta where the loop decided
         // without forming them
-        k_delta_final<<<2, 256, 0, g->stream>>>(g->ctl, g->absdiff);
+        k_delta_final<<<2, 1024, 0, g->stream>>>(g->ctl, g->absdiff);
         BP_CUDA(cudaGetLastError());
     }
     BP_CUDA(cudaEventRecord(g->ev1, g->stream));

@@ -177,7 +177,7 @@ int bp_loopy(bp_graph *g, const bp_loopy_options *opt, bp_loopy_result *res);
  * sum to the next binade is added alone.  method: 0 = 256 threads (the
  * form bp_loopy's final delta uses), 1 = 128 threads with 2048 floats of
  * staging (the iteration kernel's), 2 = 256 threads with 2048 floats,
- * 3 = the one-add-at-a-time chain. */
+ * 3 = the one-add-at-a-time chain, 4 = 1024 threads with 8192 floats. */
 int bp_serial_sum_f32(const float *x, uint64_t n, float *out, int method, void *stream);
 /* An interval [lohi[0], lohi[1]] (DEVICE doubles) holding that same serial
  * sum, narrowed from the terms' own rounding errors: exact for every add where

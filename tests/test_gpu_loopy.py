@@ -470,15 +470,15 @@ def test_serial_sum_parallel_is_the_one_by_one_sum(bp, name):
     x = _serial_sum_cases()[name]
     ref = np.add.accumulate(x, dtype=np.float32)[-1] if len(x) else np.float32(0.0)
     xd = torch.from_numpy(x.copy()).cuda() if len(x) else torch.zeros(1, device="cuda")
-    out = torch.full((4,), -7.0, device="cuda")
+    out = torch.full((5,), -7.0, device="cuda")
     lib = N.load()
-    for method in range(4):
+    for method in range(5):
         rc = lib.bp_serial_sum_f32(C.c_void_p(xd.data_ptr()), C.c_uint64(len(x)),
                                    C.c_void_p(out.data_ptr() + 4 * method), method, None)
         assert rc == 0
     torch.cuda.synchronize()
     got = out.cpu().numpy()
-    for method in range(4):
+    for method in range(5):
         assert got[method].tobytes() == np.float32(ref).tobytes(), (name, method, got[method], ref)
 
 
