@@ -815,7 +815,73 @@ using namespace bpx;
     default: return FN<10>(__VA_ARGS__);                           \
     }
 
+// ---- the cross-entropy loss head: -mean_v log_beliefs[v][label_v] -------
+// one launch for the value (per-block partials in f64, the last block sums
+// them in block order, so the value is deterministic) and one for its
+// gradient (-g / V at each node's label, 0 elsewhere), instead of a gather,
+// a reduction and a scatter of generic tensor kernels
+constexpr int kNllThreads = 256;
+constexpr uint32_t kNllBlocks = 296;   // 2 per SM
+
+__global__ void __launch_bounds__(kNllThreads) k_nll(const float *__restrict__ lb, const int64_t *__restrict__ labels,
+                                                      uint32_t V, uint32_t S, double *partials, uint32_t *ticket,
+                                                      float *loss) {
+    __shared__ double red[kNllThreads / 32];
+    __shared__ bool last;
+    double acc = 0.0;
+    for (uint32_t v = blockIdx.x * kNllThreads + threadIdx.x; v < V; v += gridDim.x * kNllThreads) {
+        const uint64_t lab = (uint64_t)labels[v];   // a label outside [0, S) makes the loss NaN
+        acc -= lab < S ? (double)lb[(size_t)v * S + lab] : __longlong_as_double(0x7ff8000000000000ll);
+    }
+    double t = block_sum<kNllThreads>(acc, red);
+    if (threadIdx.x == 0) {
+        partials[blockIdx.x] = t;
+        unsigned k;
+        asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(k) : "l"(ticket) : "memory");
+        last = (k == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double a = 0.0;
+    for (uint32_t k = threadIdx.x; k < gridDim.x; k += kNllThreads) a += __ldcg(partials + k);
+    a = block_sum<kNllThreads>(a, red);
+    if (threadIdx.x == 0) {
+        *loss = (float)(a / (double)V);
+        *ticket = 0;
+    }
+}
+
+__global__ void k_nll_grad(const int64_t *__restrict__ labels, uint32_t V, uint32_t S, const float *__restrict__ g,
+                           float *__restrict__ grad) {
+    const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= (uint64_t)V * S) return;
+    const uint32_t v = (uint32_t)(k / S), st = (uint32_t)(k % S);
+    grad[k] = ((uint64_t)st == (uint64_t)labels[v]) ? -g[0] / (float)V : 0.0f;
+}
+
 extern "C" {
+
+int bp_nll_f32(const float *log_beliefs, const int64_t *labels, uint32_t V, uint32_t S, double *scratch,
+               float *loss, void *stream) {
+    if (!log_beliefs || !labels || !scratch || !loss) return set_error(BP_ERR_INVALID, "null argument");
+    if (V == 0 || S == 0) return set_error(BP_ERR_SHAPE, "empty log-beliefs");
+    // scratch: kNllBlocks partials, then the ticket (zero before the first call)
+    k_nll<<<kNllBlocks, kNllThreads, 0, (cudaStream_t)stream>>>(log_beliefs, labels, V, S, scratch,
+                                                               reinterpret_cast<uint32_t *>(scratch + kNllBlocks),
+                                                               loss);
+    BP_CUDA(cudaGetLastError());
+    return BP_OK;
+}
+
+int bp_nll_grad_f32(const int64_t *labels, uint32_t V, uint32_t S, const float *grad_loss, float *grad_log_beliefs,
+                    void *stream) {
+    if (!labels || !grad_loss || !grad_log_beliefs) return set_error(BP_ERR_INVALID, "null argument");
+    const uint64_t n = (uint64_t)V * S;
+    if (n) k_nll_grad<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(labels, V, S, grad_loss, grad_log_beliefs);
+    BP_CUDA(cudaGetLastError());
+    return BP_OK;
+}
 
 int bp_unrolled_create(bp_unrolled **out, uint32_t V, uint32_t E, uint32_t S, uint32_t K, const uint32_t *src,
                        const uint32_t *dst, const uint8_t *tab, uint32_t T, uint32_t ck, void *stream) {

@@ -172,6 +172,8 @@ def load(path=LIB_PATH):
         "bp_unrolled_destroy": ([vp], None), "bp_unrolled_set_stream": ([vp, vp], i32),
         "bp_unrolled_forward": ([vp, vp, vp, vp], i32), "bp_unrolled_backward": ([vp, vp, vp, vp], i32),
         "bp_serial_sum_f32": ([vp, C.c_uint64, vp, i32, vp], i32),
+        "bp_nll_f32": ([vp, vp, u32, u32, vp, vp, vp], i32),
+        "bp_nll_grad_f32": ([vp, u32, u32, vp, vp, vp], i32),
         "bp_serial_sum_bounds": ([vp, C.c_uint64, vp, vp], i32),
         # graph.h
         "create_graph": ([C.c_uint, C.c_uint], C.POINTER(StructGraph)),

@@ -3,7 +3,7 @@ behind torch.autograd.Function.
 
     bp = UnrolledBP(num_nodes, src, dst, edge_table, states=4, iterations=30)
     log_beliefs = bp(log_unary, log_pair)   # [V, S], differentiable
-    loss = torch.nn.functional.nll_loss(log_beliefs, labels)   # cross-entropy
+    loss = nll_loss(log_beliefs, labels)     # cross-entropy (fused)
     loss.backward()                          # log_unary.grad, log_pair.grad
 
 edge_table[e] names the shared table edge e uses (bit 0x80: transposed).
@@ -83,6 +83,45 @@ class UnrolledBP:
             self.close()
         except Exception:
             pass
+
+
+class _NLLFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, log_beliefs, labels, scratch):
+        lib = N.load()
+        V, S = log_beliefs.shape
+        loss = torch.empty((), device=log_beliefs.device, dtype=torch.float32)
+        st = torch.cuda.current_stream().cuda_stream
+        N.check(lib.bp_nll_f32(log_beliefs.data_ptr(), labels.data_ptr(), V, S, scratch.data_ptr(),
+                               loss.data_ptr(), st))
+        ctx.save_for_backward(labels)
+        ctx.VS = (V, S)
+        return loss
+
+    @staticmethod
+    def backward(ctx, g):
+        (labels,) = ctx.saved_tensors
+        V, S = ctx.VS
+        g = g.contiguous().float()
+        grad = torch.empty((V, S), device=g.device, dtype=torch.float32)
+        N.check(N.load().bp_nll_grad_f32(labels.data_ptr(), V, S, g.data_ptr(), grad.data_ptr(),
+                                         torch.cuda.current_stream().cuda_stream))
+        return grad, None, None
+
+
+_nll_scratch = {}
+
+
+def nll_loss(log_beliefs, labels):
+    """Cross-entropy of log-beliefs [V, S] against int64 labels [V]: the value
+    of torch.nn.functional.nll_loss(log_beliefs, labels) (mean over nodes),
+    in one launch forward and one backward."""
+    if log_beliefs.dtype != torch.float32 or labels.dtype != torch.int64:
+        raise TypeError("float32 log-beliefs and int64 labels")
+    dev = log_beliefs.device
+    if dev not in _nll_scratch:
+        _nll_scratch[dev] = torch.zeros(297, device=dev, dtype=torch.float64)
+    return _NLLFn.apply(log_beliefs.contiguous(), labels.contiguous(), _nll_scratch[dev])
 
 
 def grid_tables(side):

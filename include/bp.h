@@ -310,6 +310,18 @@ int bp_batch_network_results(bp_batch *b, uint32_t *iterations, uint32_t *execut
  * forward/backward are device memory, 16-byte aligned; the graph arrays of
  * create are host memory.  At most 16 tables. */
 typedef struct bp_unrolled bp_unrolled;
+/* Cross-entropy loss head for the unrolled engine's log-beliefs: on `stream`,
+ * *loss (a DEVICE float) = -(1/V) sum_v log_beliefs[v*S + labels[v]], summed
+ * in f64 in a fixed order; scratch: 297 DEVICE doubles, zeroed before the
+ * first call (the last block resets the ticket it keeps there).
+ * bp_nll_grad_f32 writes the gradient: grad_log_beliefs[v*S + s] =
+ * -grad_loss[0] / V at s == labels[v], else 0 (grad_loss a DEVICE float).
+ * A label outside [0, S) makes the loss NaN. */
+int bp_nll_f32(const float *log_beliefs, const int64_t *labels, uint32_t V, uint32_t S, double *scratch,
+               float *loss, void *stream);
+int bp_nll_grad_f32(const int64_t *labels, uint32_t V, uint32_t S, const float *grad_loss, float *grad_log_beliefs,
+                    void *stream);
+
 int bp_unrolled_create(bp_unrolled **out, uint32_t num_nodes, uint32_t num_edges, uint32_t num_states,
                        uint32_t num_tables, const uint32_t *edge_src, const uint32_t *edge_dst,
                        const uint8_t *edge_table, uint32_t iterations, uint32_t checkpoint_every,

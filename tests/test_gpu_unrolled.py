@@ -165,3 +165,23 @@ def test_unrolled_several_tables(bp, S, K):
     np.testing.assert_allclose(theta.grad.cpu().numpy(), th64.grad.cpu().numpy(), atol=1e-3 * scale_t + 1e-7)
     np.testing.assert_allclose(W.grad.cpu().numpy(), W64.grad.cpu().numpy(), rtol=1e-3, atol=1e-3 * scale_w + 1e-7)
     eng.close()
+
+
+def test_fused_nll_loss_matches_torch():
+    """The fused cross-entropy head: torch's nll_loss value (mean over nodes)
+    and its gradient, -1/V at each node's label."""
+    import torch
+    from belief_propagation_b200.unrolled import nll_loss
+    g = torch.Generator(device="cpu").manual_seed(5)
+    for V, S in ((1, 2), (1000, 4), (262_144, 4), (70_001, 8)):
+        lb = torch.log_softmax(torch.randn(V, S, generator=g), 1).cuda().requires_grad_(True)
+        labels = torch.randint(0, S, (V,), generator=g).cuda()
+        loss = nll_loss(lb, labels)
+        loss.backward()
+        ref = torch.nn.functional.nll_loss(lb.detach().double(), labels)
+        assert abs(float(loss) - float(ref)) <= 1e-6 * max(1.0, abs(float(ref)))
+        ref_lb = lb.detach().clone().requires_grad_(True)
+        torch.nn.functional.nll_loss(ref_lb, labels).backward()
+        torch.testing.assert_close(lb.grad, ref_lb.grad, rtol=1e-7, atol=0)
+    bad = torch.zeros(4, 3, device="cuda")
+    assert torch.isnan(nll_loss(bad, torch.tensor([0, 1, 3, 2], device="cuda")))
