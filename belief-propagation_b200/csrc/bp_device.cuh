@@ -300,6 +300,15 @@ __device__ __forceinline__ double block_sum(double v, double *red) {
     return t;  // valid in thread 0
 }
 
+// programmatic dependent launch: a kernel launched with the programmatic
+// stream-serialization attribute may start before the kernel ahead of it on
+// the stream has finished; it must call griddep_wait() before it reads
+// anything that kernel (or an earlier one) wrote.  launch_dependents lets the
+// next such kernel start once every block of this one has issued it.
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::); }
+__device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 }  // namespace bpx
 
 // dispatch on (max states, uniform): instantiates FN<1..10, true/false>

@@ -56,20 +56,25 @@ __global__ void k_tree_wave(const uint32_t *__restrict__ nodes, uint32_t n, uint
                             const uint32_t *__restrict__ node_level, const uint32_t *__restrict__ node_lidx,
                             const uint8_t *__restrict__ node_s, const float *__restrict__ joint,
                             float *__restrict__ msg, const uint8_t *__restrict__ visited) {
+    griddep_launch_dependents();
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
+    // the schedule's arrays first (no tree kernel writes them), then the wait
+    // for the kernels ahead, whose messages and visited flags follow
     const uint32_t u = nodes[k];
     const int S = UNI ? MS : node_s[u];
     const uint32_t my_idx = node_lidx[u];
+    const uint32_t r0 = in_ptr[u], r1 = in_ptr[u + 1], o0 = out_ptr[u], o1 = out_ptr[u + 1];
+    griddep_wait();
     float buf[MS];
 #pragma unroll
     for (int i = 0; i < MS; ++i) buf[i] = (UNI || i < S) ? 1.0f : 0.0f;
-    for (uint32_t p = in_ptr[u]; p < in_ptr[u + 1]; ++p) {
+    for (uint32_t p = r0; p < r1; ++p) {
         float mm[MS];
         ldv<MS>(msg + (size_t)p * MS, mm);
         combine<MS, UNI>(buf, mm, S);
     }
-    for (uint32_t q = out_ptr[u]; q < out_ptr[u + 1]; ++q) {
+    for (uint32_t q = o0; q < o1; ++q) {
         const uint32_t w = out_dst[q];
         const bool seen = visited[w] || (node_level[w] == level && node_lidx[w] <= my_idx);
         if (seen) continue;
@@ -99,14 +104,35 @@ __global__ void k_tree_wave_group(const uint32_t *__restrict__ nodes, uint32_t n
     const uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) / G;
     const uint32_t lane = threadIdx.x & (G - 1);
     const uint32_t gmask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));
+    griddep_launch_dependents();
     if (k >= n) return;   // the whole group
+    // the schedule's arrays first (no tree kernel writes them): the node, its
+    // edge ranges, and this lane's first out-edge with its neighbour's level
+    // (and, for the latency-bound small waves, its table into L2); then the
+    // wait for the kernels ahead, whose messages and visited flags follow
     const uint32_t u = nodes[k];
     const int S = UNI ? MS : node_s[u];
     const uint32_t my_idx = node_lidx[u];
+    const uint32_t r0 = in_ptr[u], r1 = in_ptr[u + 1], o0 = out_ptr[u], o1 = out_ptr[u + 1];
+    const uint32_t q0 = o0 + lane;
+    uint32_t w0 = 0, pp0 = 0, lv0 = 0, li0 = 0;
+    int y0 = MS;
+    if (q0 < o1) {
+        w0 = out_dst[q0];
+        pp0 = out_pos[q0];
+        lv0 = node_level[w0];
+        li0 = node_lidx[w0];
+        if (!UNI) y0 = node_s[w0];
+        if constexpr (G >= 16) {
+            const float *jt = joint + (size_t)pp0 * (MS * MS);
+            prefetch_l2(jt);
+            if constexpr (MS * MS > 32) prefetch_l2(jt + 32);
+        }
+    }
+    griddep_wait();
     float buf[MS];
 #pragma unroll
     for (int i = 0; i < MS; ++i) buf[i] = (UNI || i < S) ? 1.0f : 0.0f;
-    const uint32_t r0 = in_ptr[u], r1 = in_ptr[u + 1];
     for (uint32_t p0 = r0; p0 < r1; p0 += G) {
         float mm[MS];
 #pragma unroll
@@ -120,12 +146,14 @@ __global__ void k_tree_wave_group(const uint32_t *__restrict__ nodes, uint32_t n
             combine<MS, UNI>(buf, mj, S);
         }
     }
-    for (uint32_t q = out_ptr[u] + lane; q < out_ptr[u + 1]; q += G) {
-        const uint32_t w = out_dst[q];
-        const bool seen = visited[w] || (node_level[w] == level && node_lidx[w] <= my_idx);
+    for (uint32_t q = q0; q < o1; q += G) {
+        const bool first = q == q0;
+        const uint32_t w = first ? w0 : out_dst[q];
+        const uint32_t lv = first ? lv0 : node_level[w], li = first ? li0 : node_lidx[w];
+        const bool seen = visited[w] || (lv == level && li <= my_idx);
         if (seen) continue;
-        const uint32_t p = out_pos[q];
-        const int y = UNI ? MS : node_s[w];
+        const uint32_t p = first ? pp0 : out_pos[q];
+        const int y = UNI ? MS : (first ? y0 : (int)node_s[w]);
         float m[MS];
         send_msg<MS, UNI>(joint + (size_t)p * (MS * MS), buf, S, y, m);
         stv<MS>(msg + (size_t)p * MS, m);
@@ -255,12 +283,41 @@ static int wave_group(uint64_t n) {
     return 1;
 }
 
+// wave kernels may start while the kernel ahead drains (programmatic
+// dependent launch): they read the schedule first and wait before the
+// messages; BP_TREE_PDL=0 launches them one after another
+static bool tree_pdl() {
+    static int on = -1;
+    if (on < 0) {
+        const char *env = getenv("BP_TREE_PDL");
+        on = (env && env[0] == '0') ? 0 : 1;
+    }
+    return on != 0;
+}
+
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_wave(void (*kern)(KArgs...), unsigned grid, cudaStream_t st, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(128);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = tree_pdl() ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 template <int MS, bool UNI, int G>
-static void launch_wave_group(bp_graph *g, const uint32_t *nodes, uint32_t n, uint32_t level) {
+static cudaError_t launch_wave_group(bp_graph *g, const uint32_t *nodes, uint32_t n, uint32_t level) {
     TreeData &t = g->tree;
-    k_tree_wave_group<MS, UNI, G><<<grid_for((uint64_t)n * G, 128), 128, 0, g->stream>>>(
-        nodes, n, level, g->in_ptr, g->out_ptr, g->out_pos, g->out_dst, t.d_node_level, t.d_node_lidx, g->node_s,
-        g->joint, g->msg[0], g->visited);
+    return launch_wave(k_tree_wave_group<MS, UNI, G>, grid_for((uint64_t)n * G, 128), g->stream, nodes, n, level,
+                       (const uint32_t *)g->in_ptr, (const uint32_t *)g->out_ptr, (const uint32_t *)g->out_pos,
+                       (const uint32_t *)g->out_dst, (const uint32_t *)t.d_node_level,
+                       (const uint32_t *)t.d_node_lidx, (const uint8_t *)g->node_s, (const float *)g->joint,
+                       g->msg[0], (const uint8_t *)g->visited);
 }
 
 template <int MS, bool UNI>
@@ -271,17 +328,21 @@ static int launch_level(bp_graph *g, uint32_t level) {
         const uint32_t lo = t.wave_off[w], n = t.wave_off[w + 1] - lo;
         if (!n) continue;
         const uint32_t *nodes = t.d_wave_nodes + lo;
+        cudaError_t le;
         switch (wave_group(n)) {
-        case 32: launch_wave_group<MS, UNI, 32>(g, nodes, n, level); break;
-        case 16: launch_wave_group<MS, UNI, 16>(g, nodes, n, level); break;
-        case 8: launch_wave_group<MS, UNI, 8>(g, nodes, n, level); break;
-        case 4: launch_wave_group<MS, UNI, 4>(g, nodes, n, level); break;
-        case 2: launch_wave_group<MS, UNI, 2>(g, nodes, n, level); break;
+        case 32: le = launch_wave_group<MS, UNI, 32>(g, nodes, n, level); break;
+        case 16: le = launch_wave_group<MS, UNI, 16>(g, nodes, n, level); break;
+        case 8: le = launch_wave_group<MS, UNI, 8>(g, nodes, n, level); break;
+        case 4: le = launch_wave_group<MS, UNI, 4>(g, nodes, n, level); break;
+        case 2: le = launch_wave_group<MS, UNI, 2>(g, nodes, n, level); break;
         default:
-            k_tree_wave<MS, UNI><<<grid_for(n, 128), 128, 0, g->stream>>>(
-                nodes, n, level, g->in_ptr, g->out_ptr, g->out_pos, g->out_dst, t.d_node_level, t.d_node_lidx,
-                g->node_s, g->joint, g->msg[0], g->visited);
+            le = launch_wave(k_tree_wave<MS, UNI>, grid_for(n, 128), g->stream, nodes, n, level,
+                             (const uint32_t *)g->in_ptr, (const uint32_t *)g->out_ptr, (const uint32_t *)g->out_pos,
+                             (const uint32_t *)g->out_dst, (const uint32_t *)t.d_node_level,
+                             (const uint32_t *)t.d_node_lidx, (const uint8_t *)g->node_s, (const float *)g->joint,
+                             g->msg[0], (const uint8_t *)g->visited);
         }
+        if (le != cudaSuccess) return cuda_fail(le, "cudaLaunchKernelEx", __FILE__, __LINE__);
         BP_CUDA(cudaGetLastError());
     }
     if (w1 > w0) {
