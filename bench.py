@@ -772,12 +772,9 @@ def main():
         # every step's copies and work stay inside the timed region, which
         # runs from before the first build to after the last read
         from concurrent.futures import ThreadPoolExecutor
-        # the builds yield the SMs to the solve (stream priorities); their
-        # copies run on the copy engines either way
-        lo_prio, hi_prio = torch.cuda.Stream.priority_range() if hasattr(torch.cuda.Stream, "priority_range") \
-            else (0, -1)
-        streams = [torch.cuda.Stream(priority=lo_prio), torch.cuda.Stream(priority=lo_prio)]
-        solve_stream = torch.cuda.Stream(priority=hi_prio)
+        # equal stream priorities: a low-priority build starves for a whole
+        # CUDA-graph chunk of the solve at each of its host synchronisations
+        streams = [torch.cuda.Stream(), torch.cuda.Stream()]
         outs = [out_h, torch.empty((V, S), dtype=torch.float32).pin_memory()]
 
         def build(k):
@@ -793,7 +790,6 @@ def main():
                     gk = fut.result()
                     if k + 1 < n:
                         fut = ex.submit(build, k + 1)
-                    gk.set_stream(solve_stream.cuda_stream)
                     gk.init_messages()
                     gk.loopy(0.0, a.iterations, delta="f64")
                     gk.beliefs(out=outs[k % 2])
