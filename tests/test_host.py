@@ -190,3 +190,22 @@ def test_synth_tree_contract(synth):
     par = net.src[0::2]
     assert np.all(par < net.dst[0::2])
     np.testing.assert_array_equal(net.joint[1::2], np.transpose(net.joint[0::2], (0, 2, 1)))
+
+
+def test_bench_arguments_and_algorithmic_bytes(monkeypatch):
+    """bench.py's documented defaults (the headline workload, N=1, W>=3, the
+    e2e pipeline length, the batched delta) and the flooding kernel's
+    algorithmic bytes: 44 B per edge + 28 B per node at 2 states, 3.42 GB for
+    the 16.8M-node / 67.1M-edge graph."""
+    import sys
+    import bench
+    monkeypatch.setattr(sys, "argv", ["bench.py"])
+    a = bench.parse()
+    assert (a.gpus, a.impl, a.workload, a.iterations) == (1, "bp", "power_law", 100)
+    assert a.warmup >= 3 and a.e2e_steps == 6 and a.batch_delta == "f64"
+    assert (a.nodes, a.edges) == (1 << 24, 1 << 26)
+    for d in ("serial", "f64"):
+        monkeypatch.setattr(sys, "argv", ["bench.py", "--workload", "batched", "--batch-delta", d])
+        assert bench.parse().batch_delta == d
+    assert bench.flood_bytes_per_iteration(1, 1, 2) == 44 + 28
+    assert abs(bench.flood_bytes_per_iteration(1 << 24, 1 << 26, 2) - 3.42e9) < 0.01e9
