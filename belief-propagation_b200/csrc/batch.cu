@@ -927,6 +927,7 @@ int bp_batch_get_block_threads(const bp_batch *bt, uint32_t *states, uint32_t *b
 }
 
 int bp_batch_loopy(bp_batch *bt, const bp_batch_options *o, bp_batch_result *r) {
+    NvtxRange nvtx("bp_batch_loopy");
     if (!bt || !o) return set_error(BP_ERR_INVALID, "null argument");
     if (o->delta_mode < BP_DELTA_AUTO || o->delta_mode > BP_DELTA_F64)
         return set_error(BP_ERR_INVALID, "unknown delta mode %d", o->delta_mode);

@@ -27,6 +27,8 @@
 
 #include <chrono>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "bp.h"
 
 namespace bpx {
@@ -170,16 +172,28 @@ int ensure_staging(bp_graph *g, size_t bytes);
 int ensure_out_csr(bp_graph *g);
 int ensure_host_in_ptr(bp_graph *g);
 
+// an NVTX range for the lifetime of the object: the entry points show up
+// as named ranges on a profiler's timeline (no cost without a tool attached)
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
+
 // BP_TRACE=1: wall time of each stage of a multi-stage call on stderr (each
-// mark waits for the graph's stream, so tracing serialises the stages)
+// mark waits for the graph's stream, so tracing serialises the stages); the
+// call is an NVTX range and each stage an NVTX mark in any case
 struct StageTrace {
     bool on;
     cudaStream_t s;
     const char *what;
     std::chrono::steady_clock::time_point t;
+    NvtxRange range;
     StageTrace(cudaStream_t s_, const char *what_)
-        : on(getenv("BP_TRACE") != nullptr), s(s_), what(what_), t(std::chrono::steady_clock::now()) {}
+        : on(getenv("BP_TRACE") != nullptr), s(s_), what(what_), t(std::chrono::steady_clock::now()), range(what_) {}
     void mark(const char *stage) {
+        nvtxMarkA(stage);
         if (!on) return;
         cudaStreamSynchronize(s);
         const auto n = std::chrono::steady_clock::now();

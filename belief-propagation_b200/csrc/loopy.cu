@@ -2125,6 +2125,7 @@ int bp_serial_sum_f32(const float *x, uint64_t n, float *out, int method, void *
 }
 
 int bp_loopy(bp_graph *g, const bp_loopy_options *opt, bp_loopy_result *res) {
+    NvtxRange nvtx("bp_loopy");
     if (!g || !opt) return set_error(BP_ERR_INVALID, "null argument");
     if (opt->schedule != BP_SCHEDULE_NODE && opt->schedule != BP_SCHEDULE_EDGE)
         return set_error(BP_ERR_INVALID, "unknown schedule %d", opt->schedule);

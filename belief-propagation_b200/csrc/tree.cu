@@ -442,6 +442,7 @@ static int tree_enqueue(bp_graph *g) {
 }
 
 int bp_tree(bp_graph *g, bp_tree_result *res) {
+    NvtxRange nvtx("bp_tree");
     if (!g) return set_error(BP_ERR_INVALID, "null graph");
     int st;
     if (!g->tree.ready) {

@@ -1003,6 +1003,7 @@ static int fwd_body(bp_unrolled *u) { BP_DISPATCH_S(u->S, u_forward, u); }
 static int bwd_body(bp_unrolled *u) { BP_DISPATCH_S(u->S, u_backward, u); }
 
 int bp_unrolled_forward(bp_unrolled *u, const float *log_unary, const float *log_pair, float *log_beliefs) {
+    NvtxRange nvtx("bp_unrolled_forward");
     if (!u || !log_unary || !log_pair || !log_beliefs) return set_error(BP_ERR_INVALID, "null argument");
     if (((uintptr_t)log_unary | (uintptr_t)log_beliefs) & 15u)
         return set_error(BP_ERR_INVALID, "log_unary and log_beliefs must be 16-byte aligned");
@@ -1019,6 +1020,7 @@ int bp_unrolled_forward(bp_unrolled *u, const float *log_unary, const float *log
 }
 
 int bp_unrolled_backward(bp_unrolled *u, const float *grad_log_beliefs, float *grad_log_unary, float *grad_log_pair) {
+    NvtxRange nvtx("bp_unrolled_backward");
     if (!u || !grad_log_beliefs || !grad_log_unary || !grad_log_pair) return set_error(BP_ERR_INVALID, "null argument");
     if (((uintptr_t)grad_log_beliefs | (uintptr_t)grad_log_unary) & 15u)
         return set_error(BP_ERR_INVALID, "grad_log_beliefs and grad_log_unary must be 16-byte aligned");
