@@ -695,7 +695,7 @@ static std::string tune_key(bp_batch *bt, const Group &gr, int serial) {
     int dev = 0;
     cudaGetDevice(&dev);
     cudaGetDeviceProperties(&prop, dev);
-    char buf[256];
+    char buf[512];
     snprintf(buf, sizeof buf, "%s|S=%d|log2V=%u|deg10=%u|nets=%llu|delta=%s|rev=%d", prop.name, gr.S, lv, deg10,
              (unsigned long long)(cnt >= 1024 ? 1024 : cnt), serial ? "serial" : "f64", kTuneRevision);
     for (char *c = buf; *c; ++c)
@@ -714,10 +714,10 @@ static std::string cache_path() {
 static uint32_t cache_lookup(const std::string &key, uint32_t *grid) {
     FILE *f = fopen(cache_path().c_str(), "r");
     if (!f) return 0;
-    char line[512], k[256];
+    char line[1024], k[512];
     unsigned b = 0, gsz = 0, found = 0, found_g = 0;
     while (fgets(line, sizeof line, f))
-        if (sscanf(line, "%255s %u %u", k, &b, &gsz) == 3 && key == k) {
+        if (sscanf(line, "%511s %u %u", k, &b, &gsz) == 3 && key == k) {
             found = b;
             found_g = gsz;
         }
