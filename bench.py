@@ -268,7 +268,6 @@ def run_batched(a, rank, world):
     b = BPBatch(nets, stream=handle)
     prior = torch.from_numpy(b.pack_beliefs()).cuda()
     b.set_beliefs(prior)
-    os.environ.setdefault("BP_AUTOTUNE_CACHE", os.path.join(ROOT, "gpurun_out", "bp_autotune.txt"))
     tuned = b.autotune(tol=1e-4, max_iterations=200, delta=a.batch_delta)
 
     def step():
