@@ -209,3 +209,32 @@ def test_bench_arguments_and_algorithmic_bytes(monkeypatch):
         assert bench.parse().batch_delta == d
     assert bench.flood_bytes_per_iteration(1, 1, 2) == 44 + 28
     assert abs(bench.flood_bytes_per_iteration(1 << 24, 1 << 26, 2) - 3.42e9) < 0.01e9
+
+
+def test_status_codes_and_thread_local_errors():
+    """bp_status_string names every bp_status, argument errors come back as
+    statuses before any device work, and bp_last_error is per thread."""
+    import ctypes as C
+    import threading
+    from belief_propagation_b200 import native as N
+    lib = N.load()
+    names = [lib.bp_status_string(k) for k in range(9)]
+    assert names[0] == b"ok" and len(set(names)) == 9 and all(names)
+    assert lib.bp_status_string(99) == b"unknown status"
+    assert lib.bp_version() >= 1
+    dummy = (C.c_float * 4)()
+    BP_ERR_INVALID, BP_ERR_SHAPE = 1, 2
+    assert lib.bp_serial_sum_f32(None, C.c_uint64(5), C.addressof(dummy), 0, None) == BP_ERR_INVALID
+    assert lib.bp_serial_sum_f32(C.addressof(dummy), C.c_uint64(4), C.addressof(dummy), 9, None) == BP_ERR_INVALID
+    assert lib.bp_loopy(None, None, None) == BP_ERR_INVALID
+    seen = {}
+
+    def worker(name, call):
+        seen[name] = (call(), lib.bp_last_error())
+
+    t1 = threading.Thread(target=worker, args=("a", lambda: lib.bp_loopy(None, None, None)))
+    t2 = threading.Thread(target=worker, args=("b", lambda: lib.bp_nll_f32(
+        C.addressof(dummy), C.addressof(dummy), 0, 4, C.addressof(dummy), C.addressof(dummy), None)))
+    t1.start(); t1.join(); t2.start(); t2.join()
+    assert seen["a"] == (BP_ERR_INVALID, b"null argument")
+    assert seen["b"][0] == BP_ERR_SHAPE and b"empty" in seen["b"][1]
