@@ -238,3 +238,30 @@ def test_status_codes_and_thread_local_errors():
     t1.start(); t1.join(); t2.start(); t2.join()
     assert seen["a"] == (BP_ERR_INVALID, b"null argument")
     assert seen["b"][0] == BP_ERR_SHAPE and b"empty" in seen["b"][1]
+
+
+@pytest.mark.parametrize("rel,V,E,ret", [("dog.bif", 5, 5, 6)])
+def test_reference_parser_smoke_values(native, rel, V, E, ret):
+    """The reference's own parser smoke run (bnf-parser/main.c:230-242: build,
+    both CSRs, init_previous_edge, loopy_propagate_until(graph, 1e-3, 200)) on
+    the serial reference build: dog, 5 nodes / 5 edges, returns 6."""
+    on_ref = os.path.join(ROOT, "oracle", "_ref", "libref_bif.so")
+    path = os.path.join(BIF, rel)
+    if not (os.path.exists(on_ref) and os.path.exists(path)):
+        pytest.skip("reference parser or BIF files not available here")
+    L = C.CDLL(on_ref)
+    L.refbif_load.restype = C.c_void_p
+    L.refbif_load.argtypes = [C.c_char_p]
+    for f in ("init_previous_edge", "set_up_src_nodes_to_edges", "set_up_dest_nodes_to_edges"):
+        getattr(L, f).argtypes = [C.c_void_p]
+    L.loopy_propagate_until.argtypes = [C.c_void_p, C.c_float, C.c_uint]
+    L.loopy_propagate_until.restype = C.c_uint
+    L.graph_destroy.argtypes = [C.c_void_p]
+    g = L.refbif_load(path.encode())
+    s = C.cast(g, C.POINTER(native.StructGraph)).contents
+    assert (s.current_num_vertices, s.current_num_edges) == (V, E)
+    L.set_up_src_nodes_to_edges(g)
+    L.set_up_dest_nodes_to_edges(g)
+    L.init_previous_edge(g)
+    assert L.loopy_propagate_until(g, C.c_float(1e-3), 200) == ret
+    L.graph_destroy(g)
