@@ -265,3 +265,34 @@ def test_reference_parser_smoke_values(native, rel, V, E, ret):
     L.init_previous_edge(g)
     assert L.loopy_propagate_until(g, C.c_float(1e-3), 200) == ret
     L.graph_destroy(g)
+
+
+def test_synth_batch_contract(synth):
+    """Config 2's generator: node counts log-uniform in [32, 4096], edges
+    U(2, 6) x nodes, one state count per network from {2, 3, 4, 8}, no
+    self-loops or duplicate edges, normalised priors and tables."""
+    nets = synth.batch_of_networks(count=64, seed=2)
+    assert len(nets) == 64
+    for n in nets:
+        assert 32 <= n.V <= 4096 and 2 * n.V - 1 <= n.E <= 6 * n.V + 1
+        assert len(set(np.asarray(n.num_states).tolist())) == 1 and int(n.num_states[0]) in (2, 3, 4, 8)
+        assert not np.any(n.src == n.dst)
+        assert len(np.unique(n.src.astype(np.int64) * n.V + n.dst)) == n.E
+        np.testing.assert_allclose(n.beliefs[:, : n.s_max].sum(axis=1), 1.0, rtol=1e-5)
+    sizes = np.log([n.V for n in nets])
+    assert sizes.min() < np.log(128) and sizes.max() > np.log(1024)   # spread over the log range
+
+
+def test_synth_grid_edges_contract(synth):
+    """Configs 3-4's grid: side x side nodes, 4-neighbour, both directions
+    (512 x 512 gives 1,046,528 directed edges), each forward edge followed by
+    its reverse."""
+    for side in (2, 7, 512):
+        src, dst, fwd = synth.grid_edges(side)
+        assert len(src) == 4 * side * (side - 1)
+        np.testing.assert_array_equal(src[0::2], dst[1::2])
+        np.testing.assert_array_equal(dst[0::2], src[1::2])
+        assert fwd[0::2].all() and not fwd[1::2].any()
+        d = np.abs(src.astype(np.int64) - dst.astype(np.int64))
+        assert np.all((d == 1) | (d == side))
+    assert len(synth.grid_edges(512)[0]) == 1_046_528
