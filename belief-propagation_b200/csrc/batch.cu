@@ -13,7 +13,9 @@
 //
 // Layout: the networks' arrays are concatenated (network order); inside a
 // network the edges are destination-sorted exactly as in bp_graph.
+#include <errno.h>
 #include <stdio.h>
+#include <sys/stat.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -726,13 +728,21 @@ static uint32_t cache_lookup(const std::string &key, uint32_t *grid) {
     return found;
 }
 
+// every directory on the way to `dir` (mkdir -p without a shell); false if
+// one could not be made
+static bool make_dirs(const std::string &dir) {
+    for (size_t i = 1; i <= dir.size(); ++i) {
+        if (i < dir.size() && dir[i] != '/') continue;
+        const std::string part = dir.substr(0, i);
+        if (mkdir(part.c_str(), 0755) != 0 && errno != EEXIST) return false;
+    }
+    return true;
+}
+
 static void cache_store(const std::string &key, uint32_t block, uint32_t grid) {
     std::string path = cache_path();
-    std::string dir = path.substr(0, path.find_last_of('/'));
-    if (!dir.empty()) {
-        std::string cmd = "mkdir -p '" + dir + "' 2>/dev/null";
-        if (system(cmd.c_str()) != 0) return;
-    }
+    const size_t slash = path.find_last_of('/');
+    if (slash != std::string::npos && slash > 0 && !make_dirs(path.substr(0, slash))) return;
     FILE *f = fopen(path.c_str(), "a");
     if (!f) return;
     fprintf(f, "%s %u %u\n", key.c_str(), block, grid);
