@@ -63,7 +63,11 @@ struct LoopyCtl {
     double delta_d, prev_d;
     // grid barrier of the fused (one-launch) loop: arrivals, generation, and
     // a flag a block sets when its bounded wait ran out
-    uint32_t bar_count, bar_gen, bar_fail, pad1;
+    uint32_t bar_count, bar_gen, bar_fail;
+    // test hook of that bounded wait (BP_DEBUG_BARRIER_SKIP): block
+    // bar_skip - 1 does not arrive at the first barrier, so the others' waits
+    // run out; 0 = off
+    uint32_t bar_skip;
     // serial mode: the reference's fp32 sum of a check's |diff| terms lies
     // in [dlo, dhi] (f64 sum of the terms +- the serial sum's rounding bound),
     // and in [plo, phi] for the previous check; *_exact = the serial sum
@@ -79,7 +83,7 @@ struct LoopyCtl {
     // [dlo, dhi] / [plo, phi] narrowed from the terms' own rounding errors
     uint32_t delta_ref, prev_ref;
     uint32_t serial_refines;   // checks that needed the narrowed interval
-    uint32_t pad2;
+    uint32_t wait_ms;          // limit of the grid barrier's wait; 0 = 2000 ms
 };
 
 struct TreeData {

@@ -789,10 +789,16 @@ __global__ void __launch_bounds__(flood_nt<MS>(), MB) k_flood(const FloodArgs a,
 // still read this one's.
 constexpr uint64_t kBarrierWaitNs = 2000000000ull;   // 2 s
 
+// The wait is bounded by kBarrierWaitNs, or by c->wait_ms when the host set
+// one.  Test hook: with c->bar_skip == blockIdx.x + 1 this block does not
+// arrive at the first barrier (gen 0) and goes on, so the other blocks' waits
+// run out and the run ends with bar_fail; every later wait of this block is
+// bounded the same way, so the launch still ends.
 __device__ __forceinline__ bool grid_barrier(LoopyCtl *c, uint32_t &gen, uint32_t *s_fail) {
     __syncthreads();
-    if (threadIdx.x == 0 && !*s_fail) {
+    if (threadIdx.x == 0 && !*s_fail && !(gen == 0 && c->bar_skip == blockIdx.x + 1u)) {
         const uint32_t g0 = gen;
+        const uint64_t limit = c->wait_ms ? (uint64_t)c->wait_ms * 1000000ull : kBarrierWaitNs;
         __threadfence();
         if (atomicAdd(&c->bar_count, 1u) == gridDim.x - 1) {
             c->bar_count = 0;   // untouched until the generation moves
@@ -801,7 +807,7 @@ __device__ __forceinline__ bool grid_barrier(LoopyCtl *c, uint32_t &gen, uint32_
         } else {
             const uint64_t t0 = global_ns();
             while (*(volatile uint32_t *)&c->bar_gen == g0) {
-                if (global_ns() - t0 > kBarrierWaitNs) {
+                if (global_ns() - t0 > limit) {
                     *s_fail = 1;
                     atomicExch(&c->bar_fail, 1u);
                     break;
@@ -2227,6 +2233,10 @@ int bp_loopy(bp_graph *g, const bp_loopy_options *opt, bp_loopy_result *res) {
     c.plo = c.phi = -1.0;
     c.prev_exact = 1;
     c.delta_exact = 1;
+    // test hook of the one-launch loop's bounded grid barrier: a shorter
+    // wait limit, and a block that does not arrive at the first barrier
+    if (const char *env = getenv("BP_DEBUG_WAIT_MS")) c.wait_ms = (uint32_t)strtoul(env, nullptr, 10);
+    if (const char *env = getenv("BP_DEBUG_BARRIER_SKIP")) c.bar_skip = (uint32_t)strtoul(env, nullptr, 10) + 1u;
     *g->ctl_host = c;
     BP_CUDA(cudaMemcpyAsync(g->ctl, g->ctl_host, sizeof(LoopyCtl), cudaMemcpyHostToDevice, g->stream));
     if (opt->schedule == BP_SCHEDULE_NODE) {
@@ -2330,34 +2340,51 @@ int bp_loopy(bp_graph *g, const bp_loopy_options *opt, bp_loopy_result *res) {
 namespace bpx {
 
 constexpr size_t kNoAllocScratchBytes = BP_NOALLOC_SCRATCH_BYTES;
-constexpr int kNoAllocMaxDevices = 64;
 
 // Device-side working memory of bp_loopy_noalloc.  Every GPU that loads the
 // library holds these bytes until the process exits.  In host code the name
 // is only a stand-in for the symbol: the device address comes from
-// cudaGetSymbolAddress, once per device, below.
+// cudaGetSymbolAddress on the current device, on every call, below.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
-
-static void *g_noalloc_base[kNoAllocMaxDevices];
-static std::mutex g_noalloc_mutex;
 
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
-// device address of the scratch array on the current device (set up on the
-// first call made on that device)
+// device address of the scratch array on the current device.  Looked up on
+// every call (a host-side table lookup): a cached address would dangle after
+// a device reset reloads the module.
 static int noalloc_base(void **base) {
-    int dev = 0;
-    BP_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kNoAllocMaxDevices) return set_error(BP_ERR_INVALID, "device %d out of range", dev);
-    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_base[dev]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress", __FILE__, __LINE__);
-        g_noalloc_base[dev] = p;
-    }
-    *base = g_noalloc_base[dev];
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress", __FILE__, __LINE__);
+    *base = p;
     return BP_OK;
+}
+
+// The caller's destination-sorted layout is checked before any kernel reads
+// through it: in_ptr[0] == 0, rows non-decreasing, in_ptr[V] == E (bit 0 of
+// *bad), every source id < V (bit 1).
+__global__ void k_noalloc_validate(const uint32_t *__restrict__ in_ptr, const uint32_t *__restrict__ in_src,
+                                   uint32_t V, uint32_t E, uint32_t *__restrict__ bad) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i <= V) {
+        const uint32_t p = in_ptr[i];
+        bool ok = i == 0 ? p == 0u : p >= in_ptr[i - 1];
+        if (i == V) ok = ok && p == E;
+        if (!ok) atomicOr(bad, 1u);
+    }
+    if (i < E && in_src[i] >= V) atomicOr(bad, 2u);
+}
+
+// scratch layout: [LoopyCtl][validation flag][partials][Q0][Q1], 256-byte
+// aligned pieces
+template <int MS>
+static size_t noalloc_need(uint32_t V, size_t *off_bad, size_t *off_part, size_t *off_q0, size_t *qbytes) {
+    constexpr int NT = flood_nt<MS>();
+    *off_bad = align256(sizeof(LoopyCtl));
+    *off_part = *off_bad + 256;
+    *off_q0 = *off_part + align256(sizeof(double) * grid_for(V, NT));
+    *qbytes = align256(sizeof(float) * MS * (size_t)V);
+    return *off_q0 + 2 * *qbytes;
 }
 
 template <int MS>
@@ -2366,11 +2393,9 @@ static int noalloc_run(uint32_t V, uint32_t E, const uint32_t *in_ptr, const uin
                        cudaStream_t stream, bp_loopy_result *res, int *latest_out) {
     constexpr int NT = flood_nt<MS>();
     const uint32_t grid = grid_for(V, NT);
-    const size_t off_part = align256(sizeof(LoopyCtl));
-    const size_t off_q0 = off_part + align256(sizeof(double) * grid);
-    const size_t qbytes = align256(sizeof(float) * MS * (size_t)V);
-    const size_t need = off_q0 + 2 * qbytes;
-    if (need > kNoAllocScratchBytes)
+    size_t off_bad, off_part, off_q0, qbytes;
+    const size_t need = noalloc_need<MS>(V, &off_bad, &off_part, &off_q0, &qbytes);
+    if (max_it > 0 && need > kNoAllocScratchBytes)
         return set_error(BP_ERR_SHAPE,
                          "bp_loopy_noalloc: %u nodes x %d states need %zu bytes of working memory; its fixed "
                          "array holds %zu (BP_NOALLOC_SCRATCH_BYTES)",
@@ -2380,6 +2405,40 @@ static int noalloc_run(uint32_t V, uint32_t E, const uint32_t *in_ptr, const uin
     if (st) return st;
     unsigned char *b = (unsigned char *)base;
     LoopyCtl *ctl = (LoopyCtl *)b;
+    uint32_t *bad = (uint32_t *)(b + off_bad);
+
+    // the caller's arrays are validated first: a bad row pointer or source
+    // id would otherwise be read through on the device
+    BP_CUDA(cudaMemsetAsync(bad, 0, sizeof(uint32_t), stream));
+    k_noalloc_validate<<<grid_for(std::max<uint64_t>((uint64_t)V + 1, E), 256), 256, 0, stream>>>(in_ptr, in_src, V,
+                                                                                                 E, bad);
+    BP_CUDA(cudaGetLastError());
+    uint32_t hbad = 0;
+    BP_CUDA(cudaMemcpyAsync(&hbad, bad, sizeof(hbad), cudaMemcpyDeviceToHost, stream));
+    BP_CUDA(cudaStreamSynchronize(stream));
+    if (hbad & 1u)
+        return set_error(BP_ERR_INVALID, "bp_loopy_noalloc: in_ptr is not a row-pointer array of %u rows ending at "
+                                         "num_edges (%u)", V, E);
+    if (hbad & 2u) return set_error(BP_ERR_INVALID, "bp_loopy_noalloc: a source id in in_src is >= num_nodes (%u)", V);
+
+    float *msg_latest = messages + (size_t)latest * E * MS;
+    if (init && E) {
+        k_send_from_beliefs<MS, true><<<grid_for(E, 256), 256, 0, stream>>>(E, in_src, nullptr, joint, beliefs,
+                                                                            msg_latest);
+        BP_CUDA(cudaGetLastError());
+    }
+    if (max_it == 0) {
+        // the reference's loop body never runs (init_previous_edge above
+        // still does)
+        BP_CUDA(cudaStreamSynchronize(stream));
+        if (res) {
+            bp_loopy_result r = {};
+            r.previous_delta = -1.0f;
+            *res = r;
+        }
+        if (latest_out) *latest_out = latest;
+        return BP_OK;
+    }
 
     // every run starts from a fully written control block; the delta
     // partials and send buffers are written before they are read
@@ -2394,12 +2453,6 @@ static int noalloc_run(uint32_t V, uint32_t E, const uint32_t *in_ptr, const uin
     c.prev_d = -1.0;
     BP_CUDA(cudaMemcpyAsync(ctl, &c, sizeof(c), cudaMemcpyHostToDevice, stream));
 
-    float *msg_latest = messages + (size_t)latest * E * MS;
-    if (init && E) {
-        k_send_from_beliefs<MS, true><<<grid_for(E, 256), 256, 0, stream>>>(E, in_src, nullptr, joint, beliefs,
-                                                                            msg_latest);
-        BP_CUDA(cudaGetLastError());
-    }
     FloodArgs a = {};
     a.V = V;
     a.in_ptr = in_ptr;
@@ -2457,16 +2510,6 @@ extern "C" int bp_loopy_noalloc(uint32_t num_nodes, uint32_t num_edges, uint32_t
     // the kernels read S (and S*S) floats at a time as float2/float4
     if (((uintptr_t)joint | (uintptr_t)beliefs | (uintptr_t)messages) & 15u)
         return set_error(BP_ERR_INVALID, "joint, beliefs and messages must be 16-byte aligned");
-    if (max_iterations == 0) {
-        // the reference's loop body never runs: nothing to launch
-        if (result) {
-            bp_loopy_result r = {};
-            r.previous_delta = -1.0f;
-            *result = r;
-        }
-        if (latest_out) *latest_out = latest_slot;
-        return BP_OK;
-    }
     cudaStream_t s = (cudaStream_t)stream;
     switch (num_states) {
     case 1: return noalloc_run<1>(num_nodes, num_edges, in_ptr, in_src, joint, beliefs, messages, latest_slot, init_messages, tolerance, max_iterations, s, result, latest_out);

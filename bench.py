@@ -130,6 +130,11 @@ class ClockSampler:
                  "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # the timed region starts once the sampler reports (nvidia-smi
+            # takes a moment to start), so short regions still get samples
+            t0 = time.time()
+            while not self.rows and time.time() - t0 < 5.0 and self.proc.poll() is None:
+                time.sleep(0.02)
         except Exception:
             self.proc = None
 
@@ -153,6 +158,30 @@ class ClockSampler:
         reasons = sorted({names[i] for r in self.rows for i in range(4) if r[3 + i].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(self.rows)}
+
+
+def _restatement(openmp=True):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    return O, O.Restatement(openmp=openmp)
+
+
+def fp64_error_loopy(net, tol, max_it, gpu_beliefs, gpu_iterations, what):
+    """Accuracy of a GPU loopy run (the checker's leg, after the timed region):
+    max |b_gpu - b| against the oracle's fp32 run of the same schedule (the
+    reference's arithmetic; 0 means bit-identical) and against the oracle's
+    fp64 run of the same schedule, with each run's returned iteration count.
+    The oracle's OpenMP build runs the node loops on all host cores."""
+    O, R = _restatement()
+    og = O.OracleGraph(net)
+    S = int(net.s_max)
+    f32 = R.loopy(og, tol, max_it)
+    f64 = R.loopy(og, tol, max_it, dtype=np.float64)
+    b = np.asarray(gpu_beliefs, np.float64)[:, :S]
+    return {"max_abs_err_vs_oracle": float(np.abs(b - f32["beliefs"][:, :S]).max()) if net.V else 0.0,
+            "max_abs_err_vs_fp64": float(np.abs(b - f64["beliefs"][:, :S]).max()) if net.V else 0.0,
+            "iterations": int(gpu_iterations), "oracle_iterations": int(f32["ret"]),
+            "fp64_iterations": int(f64["ret"]), "fp64_delta": float(f64["delta"]), "sample": what}
 
 
 def flood_bytes_per_iteration(V, E, S):
@@ -213,6 +242,27 @@ def reference_sample(iterations=None, target_s=10.0):
             "sample": f"{net.V:,} nodes / {net.E:,} edges of the same generator, {iterations} fixed iterations, "
                       f"init_previous_edge + loopy_propagate_until timed ({dt:.2f} s)",
             "seconds": dt, "iterations": iterations}
+
+
+def power_law_accuracy(a, handle):
+    """The GPU's beliefs after the workload's fixed iterations on the
+    1,048,576-node sample of the same generator (the CPU baseline's sample,
+    small enough for the fp64 oracle), same code path as the timed run."""
+    import belief_network_wrapper as W
+    from belief_propagation_b200.engine import BPGraph
+    net = W.bp.synth.power_law_loopy(1 << 20, 1 << 22, 2, 0.10, seed=1)
+    g = BPGraph(net.V, net.src, net.dst, net.joint, uniform_states=2, stream=handle, reorder=bool(a.reorder))
+    try:
+        g.set_beliefs(net.beliefs)
+        g.latest_slot = 1
+        g.init_messages()
+        r = g.loopy(0.0, a.iterations, delta="f64")
+        b = g.beliefs()
+    finally:
+        g.close()
+    return fp64_error_loopy(net, 0.0, a.iterations, b, r["iterations"],
+                            f"{net.V:,} nodes / {net.E:,} edges of the same generator, {a.iterations} fixed "
+                            "iterations, same code path")
 
 
 def run_reference_arm(a, rank, world):
@@ -292,6 +342,7 @@ def run_batched(a, rank, world):
     ms = e0.elapsed_time(e1) / a.steps
     ms = max_over_ranks(ms, dist)
     res = b.results()
+    flat = b.beliefs()
     edges = sum(n.E for n in nets)
     updates = float(res["executed"].astype(np.float64) @ np.array([n.E for n in nets], np.float64))
 
@@ -319,6 +370,28 @@ def run_batched(a, rank, world):
         g.close()
     solo_nets_s = len(sample) / solo_s
     b.close()
+    accuracy = None
+    if rank == 0:
+        # the oracle's fp32 and fp64 runs of 64 sampled networks, each alone
+        try:
+            acc_sample = sorted(np.random.default_rng(1).choice(len(nets), size=min(64, len(nets)),
+                                                                replace=False).tolist())
+            errs = []
+            for k in acc_sample:
+                n = nets[k]
+                S = n.uniform_states
+                o = int(b.belief_off[k])
+                bk = flat[o:o + n.V * S].reshape(n.V, S)
+                errs.append(fp64_error_loopy(n, 1e-4, 200, bk, int(res["iterations"][k]), ""))
+            accuracy = {"max_abs_err_vs_oracle": max(e["max_abs_err_vs_oracle"] for e in errs),
+                        "max_abs_err_vs_fp64": max(e["max_abs_err_vs_fp64"] for e in errs),
+                        "fp64_iterations_equal": sum(e["fp64_iterations"] == e["iterations"] for e in errs),
+                        "oracle_iterations_equal": sum(e["oracle_iterations"] == e["iterations"] for e in errs),
+                        "sample": f"{len(acc_sample)} networks of the batch (seeded choice), each run alone by "
+                                  "the oracle in fp32 (the reference's serial stopping rule) and in fp64 (its own "
+                                  "stopping rule), tol 1e-4, max 200"}
+        except Exception as ex:  # reported, not fatal
+            accuracy = {"error": str(ex)[:200]}
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -334,11 +407,13 @@ def run_batched(a, rank, world):
         algo += n.E * (4 * S * S + 4 + 4 * S + 4 * S) + n.V * (4 + 4 * S + 4 * S)
     peak, peak_src = measured_hbm_peak()
     achieved = algo / (ms / 1e3) / 1e9
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": None, "kernel": "k_batch_solve", "peak_source": peak_src,
+    # no HBM roofline: a block iterates one network to convergence and the
+    # network's arrays (<= ~1 MB) stay in L2 across its iterations, so these
+    # bytes are mostly L2 traffic, and no measured L2 peak is at hand
+    roofline = {"bound": "l2 / latency", "achieved": achieved, "peak": None, "unit": "GB/s", "frac": None,
+                "traffic": None, "kernel": "k_batch_solve", "peak_source": None,
                 "algorithmic_bytes_per_step": algo,
-                "note": "one block iterates one network to convergence; a network's arrays (<= ~1 MB) stay in "
-                        "L2 across its iterations, so the algorithmic bytes are mostly L2 traffic"}
+                "note": "algorithmic bytes per second, mostly served from L2; not a fraction of the HBM peak"}
     line = {"metric": "batched nets/s", "value": value, "unit": "networks/s", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -353,6 +428,9 @@ def run_batched(a, rank, world):
             "per_network_launches": {"sample": len(sample), "networks_per_s": solo_nets_s,
                                      "speedup_of_batched": value / world / solo_nets_s},
             "roofline": roofline, "gpu_launches": len(tuned) * a.steps, "clocks": clk}
+    if accuracy is not None:
+        line.update({k: accuracy[k] for k in ("max_abs_err_vs_oracle", "max_abs_err_vs_fp64") if k in accuracy})
+        line["accuracy"] = accuracy
     print(json.dumps(line), flush=True)
     return 0
 
@@ -387,12 +465,17 @@ def run_random10k(a, rank, world):
         return g.loopy(1e-3, 100, delta=delta)
 
     res = {}
+    # about 1.5 s of solves per mode, so the clock sampler sees the region
+    reps = max(a.steps, 1000)
+    clocks = ClockSampler(local)
+    clocks.start()
     for delta in ("serial", "f64"):
         for _ in range(a.warmup):
             r = step(delta)
-        ms = _time_cuda(lambda: step(delta), stream, max(a.steps, 10))
-        res[delta] = (ms, r["iterations"], r["executed"], r["serial_sums"])
-    b_gpu = g.beliefs()
+        ms = _time_cuda(lambda: step(delta), stream, reps)
+        res[delta] = (ms, r["iterations"], r["executed"], r["serial_sums"], g.beliefs())
+    clk = clocks.stop()
+    b_gpu = res["serial"][4]
     g.close()
     cpu = None
     if O.reference_available():
@@ -408,9 +491,16 @@ def run_random10k(a, rank, world):
         cpu = {"value": 1e3 * cpu_s, "unit": "ms per solve", "cores": 1, "kind": "reference",
                "sample": f"the full workload on the reference's graph.c (serial), returned {it_ref}; GPU beliefs "
                          f"bit-identical: {bool(np.array_equal(b_ref[:, :2], b_gpu))}"}
+    accuracy = None
+    if rank == 0:
+        try:
+            accuracy = fp64_error_loopy(net, 1e-3, 100, b_gpu, res["serial"][1],
+                                        "the full workload, the reference's serial fp32 stopping rule")
+        except Exception as ex:  # reported, not fatal
+            accuracy = {"error": str(ex)[:200]}
     if rank != 0:
         return 0
-    ms, it, ex, sums = res["serial"]
+    ms, it, ex, sums, _ = res["serial"]
     line = {"metric": "loopy BP ms per solve (reference-runnable workload)", "value": ms, "unit": "ms",
             "n_gpus": 1, "steps": max(a.steps, 10), "warmup": a.warmup, "ms_per_step": ms,
             "higher_is_better": False, "scaling": "replicas", "vs_baseline": None, "dtype": "f32",
@@ -419,7 +509,11 @@ def run_random10k(a, rank, world):
                        "iterations_returned": it, "iterations_run": ex,
                        "serial_sums_formed": sums},
             "us_per_iteration": 1e3 * ms / max(ex, 1), "edge_msg_updates_per_s": 40_000 * ex / (ms / 1e3),
-            "f64_delta_ms_per_solve": res["f64"][0], "cpu_baseline": cpu}
+            "f64_delta_ms_per_solve": res["f64"][0], "cpu_baseline": cpu, "clocks": clk}
+    if accuracy is not None:
+        line.update({k: accuracy[k] for k in ("max_abs_err_vs_oracle", "max_abs_err_vs_fp64", "fp64_iterations")
+                     if k in accuracy})
+        line["accuracy"] = accuracy
     print(json.dumps(line), flush=True)
     return 0
 
@@ -456,29 +550,43 @@ def run_tree(a, rank, world):
     for _ in range(a.warmup):
         r = step()
     torch.cuda.synchronize()
+    # at least ~2 s of trees, so the clock sampler sees the timed region
+    t0 = time.perf_counter()
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    per = (time.perf_counter() - t0) / 3
+    steps = max(a.steps, int(2.0 / max(per, 1e-4)))
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     clocks = ClockSampler(local)
     clocks.start()
     e0.record(stream)
-    for _ in range(a.steps):
+    for _ in range(steps):
         r = step()
     e1.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
-    ms = e0.elapsed_time(e1) / a.steps
+    ms = e0.elapsed_time(e1) / steps
     b_gpu = g.beliefs()
     g.close()
     cpu = None
+    accuracy = None
     if rank == 0:
         R = O.Restatement()
         og = O.OracleGraph(net)
         t0 = time.perf_counter()
         ora = R.tree(og)
         cpu_s = time.perf_counter() - t0
-        same = bool(np.array_equal(b_gpu, ora["beliefs"][:, : net.s_max]))
+        S = net.s_max
+        same = bool(np.array_equal(b_gpu, ora["beliefs"][:, :S]))
         cpu = {"value": 1e3 * cpu_s, "unit": "ms per tree (levels + passes)", "cores": 1, "kind": "port",
                "sample": f"the full tree, oracle restatement (O(V+E) levels), bit-identical to the GPU: {same}"}
+        o64 = R.tree(og, dtype=np.float64)
+        bg = b_gpu.astype(np.float64)
+        accuracy = {"max_abs_err_vs_oracle": float(np.abs(bg - ora["beliefs"][:, :S]).max()),
+                    "max_abs_err_vs_fp64": float(np.abs(bg - o64["beliefs"][:, :S]).max()),
+                    "sample": "the full tree; tree BP runs a fixed schedule (no iteration count)"}
     if rank != 0:
         return 0
     # algorithmic bytes of one tree: two passes over the edges (tables
@@ -494,15 +602,18 @@ def run_tree(a, rank, world):
     roofline = {"bound": "latency (levels and waves)", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": None, "kernel": "k_tree_wave", "peak_source": peak_src,
                 "algorithmic_bytes_per_tree": algo}
-    line = {"metric": "tree BP ms per tree", "value": ms, "unit": "ms", "n_gpus": 1, "steps": a.steps,
+    line = {"metric": "tree BP ms per tree", "value": ms, "unit": "ms", "n_gpus": 1, "steps": steps,
             "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "replicas",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"tree BP, random recursive tree, {net.V:,} nodes, {net.E:,} edges, "
                                    "states {2,3,4,8}, 5% evidence, seed 1",
                        "levels": nl, "waves": r["num_waves"], "level_build_s": levels_s},
             "nodes_per_s": net.V / (ms / 1e3), "roofline": roofline, "cpu_baseline": cpu,
-            "gpu_launches": (r["num_waves"] + 5) * a.steps,
+            "gpu_launches": (r["num_waves"] + 5) * steps,
             "clocks": clk}
+    if accuracy is not None:
+        line.update({k: accuracy[k] for k in ("max_abs_err_vs_oracle", "max_abs_err_vs_fp64")})
+        line["accuracy"] = accuracy
     print(json.dumps(line), flush=True)
     return 0
 
@@ -527,6 +638,43 @@ def _time_cuda(fn, stream, reps):
     e1.record(stream)
     torch.cuda.synchronize()
     return e0.elapsed_time(e1) / reps
+
+
+def unrolled_fp64_error(eng, theta, Wp, labels, srcs, dsts, tabs, sides, S, T, batch):
+    """fp32 engine against the pure-torch unrolled reference in fp64
+    (autograd through every step): beliefs and both gradients of the
+    cross-entropy.  The whole grid for the single-grid workload; for the
+    batch, the first 8 grids through an engine of their own (the batch's
+    gradient of the shared table sums over every grid)."""
+    import torch
+    from belief_propagation_b200.unrolled import UnrolledBP, torch_unrolled
+    k = 8 if batch else 1
+    Vs = int(sum(int(s) * int(s) for s in sides[:k]))
+    src = np.concatenate(srcs[:k]).astype(np.uint32)
+    dst = np.concatenate(dsts[:k]).astype(np.uint32)
+    tab = np.concatenate(tabs[:k])
+    sub_eng = UnrolledBP(Vs, src, dst, tab, S, T, checkpoint_every=5) if batch else eng
+    th = theta.detach()[:Vs].clone().requires_grad_(True)
+    W = Wp.detach().clone().requires_grad_(True)
+    lab = labels[:Vs]
+    lb = sub_eng(th, W)
+    ce_loss(lb, lab).backward()
+    th64 = th.detach().double().requires_grad_(True)
+    W64 = W.detach().double().requires_grad_(True)
+    lb64 = torch_unrolled(th64, W64, src, dst, tab, T)
+    torch.nn.functional.nll_loss(lb64, lab).backward()
+    out = {"max_abs_err_vs_fp64": float((lb.detach().double().exp() - lb64.detach().exp()).abs().max()),
+           "grad_log_unary_max_rel_err_vs_fp64": float((th.grad.double() - th64.grad).abs().max()
+                                                        / th64.grad.abs().max()),
+           "grad_log_pair_max_rel_err_vs_fp64": float((W.grad.double() - W64.grad).abs().max()
+                                                       / W64.grad.abs().max()),
+           "sample": (f"the first {k} grids ({Vs:,} nodes), an engine of their own" if batch else "the whole grid")
+           + "; pure-torch unrolled reference in fp64, autograd"}
+    if batch:
+        sub_eng.close()
+    del lb64, th64, W64
+    torch.cuda.empty_cache()
+    return out
 
 
 def run_unrolled(a, rank, world, batch):
@@ -613,6 +761,7 @@ def run_unrolled(a, rank, world, batch):
     g.close()
     b_unrolled = np.exp(fwd().cpu().numpy())
     max_diff = float(np.abs(b_plain - b_unrolled).max())
+    accuracy = unrolled_fp64_error(eng, theta, Wp, labels, srcs, dsts, tabs, sides, S, T, batch)
     extra = {}
     if batch:
         losses = []
@@ -640,6 +789,7 @@ def run_unrolled(a, rank, world, batch):
                        "nodes": V, "edges": E},
             "forward_ms": f_ms, "fwd_bwd_over_fwd": fb_ms / f_ms, "plain_forward_ms": p_ms,
             "fwd_bwd_over_plain_forward": fb_ms / p_ms, "max_abs_belief_diff_vs_plain": max_diff,
+            "max_abs_err_vs_fp64": accuracy["max_abs_err_vs_fp64"], "accuracy": accuracy,
             "clocks": clk, **extra}
     print(json.dumps(line), flush=True)
     return 0
@@ -809,12 +959,17 @@ def main():
                "phases_wall_ms": {k: round(v, 2) for k, v in phases.items()}}
 
     cpu = None
+    accuracy = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         try:
             cpu = reference_sample()
             cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
         except Exception as ex:  # reported, not fatal
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "unavailable", "sample": str(ex)[:200]}
+        try:
+            accuracy = power_law_accuracy(a, handle)
+        except Exception as ex:  # reported, not fatal
+            accuracy = {"error": str(ex)[:200]}
 
     if dist is not None:
         dist.barrier()
@@ -831,6 +986,10 @@ def main():
                        "parallelism": f"replicas x{world}", "generator_s": round(gen_s, 1)},
             "hbm_gbs_algorithmic": achieved, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches_per_step * a.steps, "clocks": clk}
+    if accuracy is not None:
+        line.update({k: accuracy[k] for k in ("max_abs_err_vs_oracle", "max_abs_err_vs_fp64", "fp64_iterations")
+                     if k in accuracy})
+        line["accuracy"] = accuracy
     print(json.dumps(line), flush=True)
     return 0
 

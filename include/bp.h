@@ -194,9 +194,18 @@ int bp_serial_sum_bounds(const float *x, uint64_t n, double *lohi, void *stream)
  * forbids components from calling cudaMalloc, a real-time loop that cannot
  * afford an allocation or the device-wide synchronisation cudaFree implies,
  * or a process pinned right at its memory cap.  This call runs the same
- * kernels as bp_loopy (node schedule, loopy_propagate_until semantics,
- * deterministic fp64 delta) and allocates nothing: no cudaMalloc, no
- * cudaFree, no allocating library routine.
+ * kernels as bp_loopy (node schedule, loopy_propagate_until semantics) and
+ * allocates nothing: no cudaMalloc, no cudaFree, no allocating library
+ * routine.
+ *
+ * Stopping rule: the reference's test (delta < tol or |delta - previous| <
+ * tol, graph.c:1313) on a deterministic fp64 sum of the |diff| terms, i.e.
+ * bp_loopy with BP_DELTA_F64.  It is NOT the reference's serial fp32 sum that
+ * bp_loopy's default uses on small graphs: where delta or its step lies
+ * within about 1e-4 relative of tol, the iteration count can differ by one
+ * from the reference's.  Use bp_loopy with BP_DELTA_SERIAL_F32 when the
+ * reference's exact decision is needed.  delta and previous_delta in the
+ * result are that fp64 sum rounded to float.
  *
  * The caller passes every input and output as DEVICE memory, already in the
  * destination-sorted layout bp_graph_create builds internally:
@@ -206,23 +215,28 @@ int bp_serial_sum_bounds(const float *x, uint64_t n, double *lohi, void *stream)
  *   beliefs  [num_nodes][S]             read and updated in place
  *   messages [2][num_edges][S]          the two message arrays; slot
  *                                       latest_slot holds the latest ones
- * with S = num_states for every node.  init_messages != 0 first fills the
- * latest slot with normalise(J . belief_src) (init_previous_edge).  On
- * return *latest_out is the slot holding the newest messages.
+ * with S = num_states for every node.  in_ptr and in_src are checked on the
+ * device before anything reads through them (in_ptr[0] == 0, rows
+ * non-decreasing, in_ptr[num_nodes] == num_edges, sources < num_nodes);
+ * a violation returns BP_ERR_INVALID.  init_messages != 0 first fills the
+ * latest slot with normalise(J . belief_src) (init_previous_edge), also when
+ * max_iterations is 0.  On return *latest_out is the slot holding the newest
+ * messages.
  *
  * Working memory (two send buffers of num_nodes * S floats, one double per
- * 256-node tile, a control block) lives in one array of
- * BP_NOALLOC_SCRATCH_BYTES compiled into the library; every GPU that loads
- * the library holds it until the process exits.  Graphs whose working memory
- * does not fit (about 1M nodes at 2 states) are rejected with BP_ERR_SHAPE
- * and a message giving the size needed.
+ * node tile, a control block) lives in one array of BP_NOALLOC_SCRATCH_BYTES
+ * compiled into the library; every GPU that loads the library holds it until
+ * the process exits.  Graphs whose working memory does not fit (about 1M
+ * nodes at 2 states) are rejected with BP_ERR_SHAPE and a message giving the
+ * size needed.
  *
- * The first call on a device looks the array's device address up with that
- * device current (cudaGetSymbolAddress); make that first call before any
- * stream capture on the device.  All calls share the one array and leave
- * their contents in it; each call rewrites the control block and the buffers
- * before reading them.  Calls whose work overlaps on the GPU (other streams,
- * other threads) race on that array: serialise them. */
+ * Each call looks the array's device address up on the current device
+ * (cudaGetSymbolAddress); the first call on a device also loads the module
+ * there, so make that first call before any stream capture on the device.
+ * All calls share the one array and leave their contents in it; each call
+ * rewrites the control block and the buffers before reading them.  Calls
+ * whose work overlaps on the GPU (other streams, other threads) race on
+ * that array: serialise them. */
 #define BP_NOALLOC_SCRATCH_BYTES (16u << 20)
 int bp_loopy_noalloc(uint32_t num_nodes, uint32_t num_edges, uint32_t num_states,
                      const uint32_t *in_ptr, const uint32_t *in_src, const float *joint,

@@ -22,6 +22,9 @@ import subprocess
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+# Where the reference's sources lie (read-only); the same REF variable the
+# Makefile takes.  Only building the checker and writing fixtures read it.
+REF = os.environ.get("REF", "/root/reference")
 MS = 10
 _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
 _u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
@@ -32,13 +35,22 @@ _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
 def build(reference=True):
     """Build the restatement (and the reference checker when its sources exist)."""
     targets = ["restatement"]
-    if reference and os.path.isdir("/root/reference/src/graph"):
+    if reference and reference_sources_present():
         targets.append("reference")
-    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+    subprocess.run(["make", "-s", "-C", HERE, f"REF={REF}"] + targets, check=True)
 
 
-def restatement_path():
-    return os.path.join(HERE, "_build", "libbp_oracle.so")
+def reference_sources_present():
+    return os.path.isdir(os.path.join(REF, "src", "graph"))
+
+
+def reference_benchmark_files():
+    """The reference's bundled network files (BIF / XMLBIF)."""
+    return os.path.join(REF, "src", "benchmark_files")
+
+
+def restatement_path(openmp=False):
+    return os.path.join(HERE, "_build", "libbp_oracle_omp.so" if openmp else "libbp_oracle.so")
 
 
 def reference_path(openmp=False):
@@ -100,10 +112,12 @@ class OracleGraph:
 class Restatement:
     """ctypes front end of bp_oracle.c."""
 
-    def __init__(self):
-        if not os.path.exists(restatement_path()):
+    def __init__(self, openmp=False):
+        """openmp: the build whose node loops run on all host cores (same
+        results; the delta stays a serial sum)."""
+        if not os.path.exists(restatement_path(openmp)):
             build(reference=False)
-        self.lib = C.CDLL(restatement_path())
+        self.lib = C.CDLL(restatement_path(openmp))
         L = self.lib
         for sfx, fp, real in (("f32", _f32p, C.c_float), ("f64", _f64p, C.c_double)):
             f = getattr(L, f"bpo_init_messages_{sfx}")

@@ -1,7 +1,8 @@
 """Write the golden fixtures of tests/golden/ by running the REFERENCE ITSELF:
 its src/graph/graph.c compiled unmodified into oracle/_ref/libref_graph.so
 (oracle/Makefile), and its vendored BIF parser (libref_bif.so) for the
-bundled networks.  Needs /root/reference (run in the build container):
+bundled networks.  Needs the reference sources (REF, as oracle/oracle.py
+reads it; run in the build container):
 
     make -C oracle reference && python tests/golden/make_golden.py
 
@@ -24,7 +25,7 @@ sys.path.insert(0, HERE)
 import golden_nets as GN  # noqa: E402
 import oracle as O  # noqa: E402
 
-BENCH = "/root/reference/src/benchmark_files"
+BENCH = O.reference_benchmark_files()
 
 
 def _pack(net):

@@ -242,6 +242,44 @@ def test_loopy_power_law_scale(bp, synth, restatement, O):
     assert abs(gpu["delta_f64"] - d64) <= 1e-9 * max(1.0, d64)
 
 
+@pytest.fixture(scope="module")
+def headline_sample(synth, O):
+    """The headline workload's generator at 1,048,576 nodes / 4,194,304 edges
+    (power-law out-degree, 2 states, seed 1) and the oracle's beliefs and
+    latest messages after 10 and 100 fixed iterations from the priors.  The
+    100-iteration run uses the reference's own graph.c (OpenMP build: with a
+    fixed iteration count its thread-scaled delta changes nothing) where it
+    was built, else the restatement."""
+    net = synth.power_law_loopy(1 << 20, 1 << 22, 2, 0.1, seed=1)
+    R = O.Restatement()
+    og = O.OracleGraph(net)
+    out = {10: R.loopy(og, 0.0, 10)}
+    if O.reference_available(openmp=True):
+        r = O.Reference(openmp=True).loopy(net, 0.0, 100)
+        out[100] = dict(beliefs=r["beliefs"], latest=r["latest"])
+    else:
+        out[100] = R.loopy(og, 0.0, 100)
+    return net, out
+
+
+@pytest.mark.parametrize("iterations", [10, 100])
+def test_loopy_headline_path_bit_exact(bp, headline_sample, monkeypatch, iterations):
+    """The benchmark's exact code path -- nodes renumbered by out-degree, the
+    persistent-grid block-tile kernel with the source id loaded one round
+    ahead, fp64 delta, tolerance 0 -- on a graph large enough that the
+    evict-last send-buffer prefix (cut to 1 MB here) leaves most sources on
+    the plain-load side: bit-exact beliefs and latest messages against the
+    oracle after 10 and 100 iterations."""
+    net, ora = headline_sample
+    monkeypatch.setenv("BP_FLOOD_HOT_MB", "1")
+    monkeypatch.setenv("BP_FLOOD_PIPE", "1")
+    gpu = gpu_loopy(bp, net, 0.0, iterations, delta="f64", reorder=True)
+    assert gpu["executed"] == iterations
+    latest = gpu["slot1"] if gpu["latest"] == 1 else gpu["slot0"]
+    np.testing.assert_array_equal(gpu["beliefs"][:, :2], ora[iterations]["beliefs"][:, :2])
+    np.testing.assert_array_equal(latest[:, :2], ora[iterations]["latest"][:, :2])
+
+
 def _staged_cases(synth):
     rng = np.random.default_rng(17)
     out = {"power_law": synth.power_law_loopy(1 << 16, 1 << 18, 2, 0.1, seed=5),
@@ -356,6 +394,38 @@ def test_loopy_fused_loop_mixed_states(bp, synth, restatement, O, monkeypatch):
     np.testing.assert_array_equal(fused["slot0"], loop["slot0"])
     ora = restatement.loopy(O.OracleGraph(net), 0.0, 9)
     np.testing.assert_array_equal(fused["beliefs"][:, :S], ora["beliefs"][:, :S])
+
+
+@pytest.mark.parametrize("delta", ["f64", "serial"])
+def test_fused_loop_barrier_wait_runs_out_and_graph_stays_usable(bp, synth, restatement, O, monkeypatch, delta):
+    """The one-launch loop's grid barrier waits a bounded time.  With block 1
+    held back from the first barrier (BP_DEBUG_BARRIER_SKIP) and the limit cut
+    to 50 ms (BP_DEBUG_WAIT_MS), every other block's wait runs out and so does
+    block 1's next one: bp_loopy returns BP_ERR_TIMEOUT instead of hanging,
+    the context stays usable, and the same graph then solves bit-exactly."""
+    from belief_propagation_b200.engine import BPGraph
+    from belief_propagation_b200.native import BPError
+    net = synth.random_loopy(3000, 12000, 2, 0.1, seed=91)   # 24 tiles: the fused loop runs
+    g = BPGraph.from_network(net)
+    try:
+        monkeypatch.setenv("BP_DEBUG_WAIT_MS", "50")
+        monkeypatch.setenv("BP_DEBUG_BARRIER_SKIP", "1")
+        g.latest_slot = 1
+        g.init_messages()
+        with pytest.raises(BPError) as err:
+            g.loopy(1e-3, 40, delta=delta)
+        assert err.value.status == 8, err.value    # BP_ERR_TIMEOUT
+        monkeypatch.delenv("BP_DEBUG_WAIT_MS")
+        monkeypatch.delenv("BP_DEBUG_BARRIER_SKIP")
+        g.set_beliefs(net.beliefs)
+        g.set_messages(0, np.zeros((net.E, 2), np.float32))
+        g.latest_slot = 1
+        g.init_messages()
+        r = g.loopy(1e-3, 40, delta="serial")
+        gpu = dict(r, beliefs=g.beliefs(), slot1=g.messages(1), slot0=g.messages(0), latest=g.latest_slot)
+    finally:
+        g.close()
+    assert_same(gpu, restatement.loopy(O.OracleGraph(net), 1e-3, 40), 2)
 
 
 def _oracle_deltas(restatement, O, net, n, schedule="node", check=1):

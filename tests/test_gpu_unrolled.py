@@ -185,3 +185,56 @@ def test_fused_nll_loss_matches_torch():
         torch.testing.assert_close(lb.grad, ref_lb.grad, rtol=1e-7, atol=0)
     bad = torch.zeros(4, 3, device="cuda")
     assert torch.isnan(nll_loss(bad, torch.tensor([0, 1, 3, 2], device="cuda")))
+
+
+def test_unrolled_batch_of_grids_of_different_sides(bp):
+    """The batched + differentiable workload's shape: a disjoint union of
+    grids of sides 9, 16 and 23 (one engine, one launch sequence forward and
+    one backward), 8 states, one shared 8x8 table, T = 20, checkpoints every
+    5.  Forward and both gradients against the fp64 torch reference, and one
+    coordinate of the shared table against an fp64 central difference."""
+    import torch
+    from belief_propagation_b200.unrolled import UnrolledBP, torch_unrolled
+    from belief_propagation_b200.synth import grid_edges
+    S, T = 8, 20
+    srcs, dsts, tabs, off = [], [], [], 0
+    for side in (9, 16, 23):
+        s_, d_, fwd = grid_edges(side)
+        srcs.append(s_.astype(np.int64) + off)
+        dsts.append(d_.astype(np.int64) + off)
+        tabs.append(np.where(fwd, 0, 0x80).astype(np.uint8))
+        off += side * side
+    V = off
+    src = np.concatenate(srcs).astype(np.uint32)
+    dst = np.concatenate(dsts).astype(np.uint32)
+    tab = np.concatenate(tabs)
+    rng = np.random.default_rng(4)
+    theta = torch.tensor(rng.normal(0, 1, (V, S)), dtype=torch.float32, device="cuda", requires_grad=True)
+    W = torch.tensor(rng.normal(0, 0.5, (1, S, S)), dtype=torch.float32, device="cuda", requires_grad=True)
+    labels = torch.tensor(rng.integers(0, S, V), device="cuda")
+    eng = UnrolledBP(V, src, dst, tab, S, T, checkpoint_every=5)
+    lb = eng(theta, W)
+    _loss(lb, labels).backward()
+    th64 = theta.detach().double().requires_grad_(True)
+    W64 = W.detach().double().requires_grad_(True)
+    lb64 = torch_unrolled(th64, W64, src, dst, tab, T)
+    _loss(lb64, labels).backward()
+    np.testing.assert_allclose(np.exp(lb.detach().cpu().numpy()), np.exp(lb64.detach().cpu().numpy()), atol=1e-4)
+    scale_t = th64.grad.abs().max().item()
+    scale_w = W64.grad.abs().max().item()
+    np.testing.assert_allclose(theta.grad.cpu().numpy(), th64.grad.cpu().numpy(), atol=1e-3 * scale_t + 1e-7)
+    np.testing.assert_allclose(W.grad.cpu().numpy(), W64.grad.cpu().numpy(), rtol=1e-3, atol=1e-3 * scale_w + 1e-7)
+    th0, W0 = theta.detach().double(), W.detach().double()
+
+    def f(w):
+        with torch.no_grad():
+            return _loss(torch_unrolled(th0, w, src, dst, tab, T), labels).item()
+
+    h = 1e-5
+    i, j = 2, 5
+    wp, wm = W0.clone(), W0.clone()
+    wp[0, i, j] += h
+    wm[0, i, j] -= h
+    fd = (f(wp) - f(wm)) / (2 * h)
+    assert abs(W.grad[0, i, j].item() - fd) <= 2e-4 * max(1e-3, abs(fd)) + 2e-6, (W.grad[0, i, j].item(), fd)
+    eng.close()

@@ -15,7 +15,10 @@ import pytest
 
 from conftest import ROOT
 
-BENCH = "/root/reference/src/benchmark_files"
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+import oracle as _O  # noqa: E402  (the checker: where the reference files lie)
+
+BENCH = _O.reference_benchmark_files()
 
 
 def test_dog_xml_matches_dog_bif_counts(bp):
