@@ -28,7 +28,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = ["engine.cu", "loopy.cu", "tree.cu", "levels_gpu.cu", "batch.cu", "unrolled.cu"]
 C_SOURCES = ["graph_api.c", "levels.c"]
-HEADERS = ["bp_internal.h", "bp_device.cuh", "bp_levels.h"]
+HEADERS = ["bp_internal.h", "bp_device.cuh", "bp_levels.h", "bp_serial.cuh", "flood_split.cuh"]
 
 
 def _newer(target, deps):

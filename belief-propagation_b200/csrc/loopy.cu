@@ -1301,6 +1301,8 @@ __global__ void __launch_bounds__(kStagedTN) k_flood_staged(const FloodArgs a, u
     reduce_and_finalize<NT>(ctl, a.partials, dsum, want, red, &s_last);
 }
 
+#include "flood_split.cuh"
+
 // Warp-tiled form of k_flood: each warp owns 32 consecutive destination
 // nodes and their in-edges, so the two phases synchronise a warp instead of
 // the block (the block meets once, for the delta).  Phase 1 issues the loads
@@ -1953,6 +1955,179 @@ static int block_tiles(const bp_graph *g, unsigned *grid, uint32_t *ntiles) {
     return BP_OK;
 }
 
+// ---- the split schedule (flood_split.cuh) ----------------------------------
+
+// send buffers per source range: BP_FLOOD_RANGE_MB (default 32) MB, and at
+// most NodeCfg::RMAX ranges
+static uint32_t split_range_nodes(const bp_graph *g) {
+    size_t mb = 32;
+    if (const char *env = getenv("BP_FLOOD_RANGE_MB")) mb = std::max<size_t>(1, (size_t)atol(env));
+    uint64_t rn = std::max<uint64_t>(1, (mb << 20) / (sizeof(float) * g->ms));
+    const uint64_t min_rn = ((uint64_t)g->V + NodeCfg<2>::RMAX - 1) / NodeCfg<2>::RMAX;
+    return (uint32_t)std::min<uint64_t>(std::max(rn, min_rn), 0xffffffffu);
+}
+
+// BP_FLOOD_SPLIT=0 never, =1 whenever the layout fits; default: when the
+// send buffers exceed BP_FLOOD_SPLIT_MIN_MB (default 64) MB, i.e. when they
+// no longer stay in L2 across an iteration
+static bool split_wanted(const bp_graph *g) {
+    const char *env = getenv("BP_FLOOD_SPLIT");
+    if (env && env[0] == '0') return false;
+    if (env && env[0] == '1') return true;
+    size_t mb = 64;
+    if (const char *e2 = getenv("BP_FLOOD_SPLIT_MIN_MB")) mb = (size_t)atol(e2);
+    return (uint64_t)g->V * g->ms * sizeof(float) > ((uint64_t)mb << 20);
+}
+
+template <int MS>
+static int split_prepare_ms(bp_graph *g) {
+    return split_build(g, NodeCfg<MS>::NT, NodeCfg<MS>::EB, split_range_nodes(g));
+}
+
+static int split_prepare(bp_graph *g) {
+    switch (g->ms) {
+    case 1: return split_prepare_ms<1>(g);
+    case 2: return split_prepare_ms<2>(g);
+    case 3: return split_prepare_ms<3>(g);
+    default: return split_prepare_ms<4>(g);
+    }
+}
+
+// build the split layout of a graph the default loop would run it on (the
+// graph build calls this, so a serving loop's next graph is prepared beside
+// the current solve); a no-op for graphs it does not apply to
+int flood_split_prepare(bp_graph *g) {
+    if (g->split.state || !g->uniform || g->ms > 4 || g->E == 0 || !split_wanted(g)) return BP_OK;
+    return split_prepare(g);
+}
+
+template <int MS, bool SER>
+static int split_grid(unsigned *grid_a, unsigned *grid_b) {
+    static int bps_a = 0, bps_b = 0;
+    static std::mutex mu;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (bps_a == 0) {
+            BP_CUDA(cudaFuncSetAttribute(k_flood_send<MS, SER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         SendCfg<MS>::SMEM));
+            BP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps_a, k_flood_send<MS, SER>, SendCfg<MS>::NT,
+                                                                  SendCfg<MS>::SMEM));
+            BP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps_b, k_flood_nodes<MS, SER>, NodeCfg<MS>::NT, 0));
+            if (bps_a < 1 || bps_b < 1) return set_error(BP_ERR_CUDA, "split iteration kernels do not fit an SM");
+        }
+    }
+    int dev = 0, sms = 0;
+    BP_CUDA(cudaGetDevice(&dev));
+    BP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    *grid_a = (unsigned)(bps_a * sms);
+    *grid_b = (unsigned)(bps_b * sms);
+    return BP_OK;
+}
+
+template <int MS>
+static SplitArgs split_args(bp_graph *g, unsigned grid_a) {
+    SplitArgs a;
+    const auto &s = g->split;
+    a.V = g->V;
+    a.E = g->E;
+    a.nchunks = (g->E + SendCfg<MS>::CH - 1) / SendCfg<MS>::CH;
+    a.ntiles = s.ntiles;
+    a.R = s.R;
+    a.nparts = std::min<unsigned>(grid_a, a.nchunks);
+    a.in_ptr = g->in_ptr;
+    a.s_src = s.s_src;
+    a.s_edge = s.s_edge;
+    a.seg = s.seg;
+    a.s_off = s.s_off;
+    a.s_joint = s.s_joint;
+    a.s_msg0 = s.s_msg[0];
+    a.s_msg1 = s.s_msg[1];
+    a.q0 = g->q[0];
+    a.q1 = g->q[1];
+    a.belief = g->belief;
+    a.partials = g->partials;
+    a.absdiff = g->absdiff;
+    a.ctl = g->ctl;
+    return a;
+}
+
+template <int MS, bool UNI>
+static int enqueue_split_iterations(bp_graph *g, uint32_t k, bool serial) {
+    if constexpr (!UNI || MS > 4) {
+        return set_error(BP_ERR_INVALID, "split schedule: uniform graphs of at most 4 states");
+    } else {
+        unsigned ga = 0, gb = 0;
+        int st = serial ? split_grid<MS, true>(&ga, &gb) : split_grid<MS, false>(&ga, &gb);
+        if (st) return st;
+        const SplitArgs a = split_args<MS>(g, ga);
+        ga = a.nparts;
+        gb = std::min<unsigned>(gb, a.ntiles);
+        for (uint32_t i = 0; i < k; ++i) {
+            if (serial) {
+                k_flood_send<MS, true><<<ga, SendCfg<MS>::NT, SendCfg<MS>::SMEM, g->stream>>>(a);
+                k_flood_nodes<MS, true><<<gb, NodeCfg<MS>::NT, 0, g->stream>>>(a);
+            } else {
+                k_flood_send<MS, false><<<ga, SendCfg<MS>::NT, SendCfg<MS>::SMEM, g->stream>>>(a);
+                k_flood_nodes<MS, false><<<gb, NodeCfg<MS>::NT, 0, g->stream>>>(a);
+            }
+            BP_CUDA(cudaGetLastError());
+        }
+        return BP_OK;
+    }
+}
+
+// the send pass's grid (the delta partials it writes)
+template <int MS, bool UNI>
+static int split_send_blocks(bp_graph *g, bool serial, uint32_t *n) {
+    if constexpr (!UNI || MS > 4) {
+        return set_error(BP_ERR_INVALID, "split schedule: uniform graphs of at most 4 states");
+    } else {
+        unsigned ga = 0, gb = 0;
+        int st = serial ? split_grid<MS, true>(&ga, &gb) : split_grid<MS, false>(&ga, &gb);
+        if (st) return st;
+        *n = split_args<MS>(g, ga).nparts;
+        return BP_OK;
+    }
+}
+
+// messages between position order and send order (dir 0: the latest slot
+// into send order; dir 1: both slots back)
+template <int MS, bool UNI>
+static int split_convert(bp_graph *g, int dir) {
+    if constexpr (!UNI || MS > 4) {
+        return set_error(BP_ERR_INVALID, "split schedule: uniform graphs of at most 4 states");
+    } else {
+        const auto &s = g->split;
+        if (dir == 0) {
+            k_to_send_order<MS><<<grid_for(g->E, 256), 256, 0, g->stream>>>(s.s_pos, g->E, g->msg[g->latest],
+                                                                             s.s_msg[g->latest]);
+        } else {
+            for (int k = 0; k < 2; ++k)
+                k_from_send_order<MS><<<grid_for(g->E, 256), 256, 0, g->stream>>>(s.s_pos, g->E, s.s_msg[k],
+                                                                                  g->msg[k]);
+        }
+        BP_CUDA(cudaGetLastError());
+        return BP_OK;
+    }
+}
+
+// whether the node schedule's loop runs split (*use): uniform graphs of at
+// most 4 states, the default loop (kernel variant AUTO: when split_wanted) or
+// BP_KERNEL_SPLIT asked for; the layout is built here if the graph build did
+// not; a graph whose node tiles hold too many in-edges keeps k_flood
+static int split_applies(bp_graph *g, int schedule, int variant, bool *use) {
+    *use = false;
+    if (schedule != BP_SCHEDULE_NODE || !g->uniform || g->ms > 4 || g->E == 0 || g->V == 0) return BP_OK;
+    if (variant != BP_KERNEL_AUTO && variant != BP_KERNEL_SPLIT) return BP_OK;
+    if (variant == BP_KERNEL_AUTO && !split_wanted(g)) return BP_OK;
+    if (g->split.state == 0) {
+        int st = split_prepare(g);
+        if (st) return st;
+    }
+    *use = g->split.state == 1;
+    return BP_OK;
+}
+
 template <int MS, bool UNI>
 static int enqueue_node_iterations(bp_graph *g, uint32_t k, bool serial, int variant) {
     constexpr int NT = flood_nt<MS>();
@@ -2020,12 +2195,18 @@ static int enqueue_edge_iterations(bp_graph *g, uint32_t k, bool, int) {
 }
 
 static int enqueue_iterations(bp_graph *g, int schedule, uint32_t k, bool serial, int variant) {
+    if (schedule == BP_SCHEDULE_NODE && variant == BP_KERNEL_SPLIT)
+        BP_DISPATCH_MS(g->ms, g->uniform != 0, enqueue_split_iterations, g, k, serial);
     if (schedule == BP_SCHEDULE_NODE)
         BP_DISPATCH_MS(g->ms, g->uniform != 0, enqueue_node_iterations, g, k, serial, variant);
     BP_DISPATCH_MS(g->ms, g->uniform != 0, enqueue_edge_iterations, g, k, serial, variant);
 }
 
-static int flood_grid(bp_graph *g, int variant, uint32_t *grid) {
+static int flood_grid(bp_graph *g, int variant, uint32_t *grid, bool serial) {
+    if (variant == BP_KERNEL_SPLIT) {
+        auto f = [&]() -> int { BP_DISPATCH_MS(g->ms, g->uniform != 0, split_send_blocks, g, serial, grid); };
+        return f();
+    }
     if (variant == BP_KERNEL_STAGED_TILE) {
         uint32_t ntiles = 0;
         unsigned gr = 0;
@@ -2181,18 +2362,31 @@ int bp_loopy(bp_graph *g, const bp_loopy_options *opt, bp_loopy_result *res) {
     }
     int st;
     int variant = opt->kernel_variant;
+    if (variant == BP_KERNEL_SPLIT) variant = BP_KERNEL_BLOCK_TILE;   // resolved below
     if (variant == BP_KERNEL_AUTO) {
         const char *env = getenv("BP_FLOOD_KERNEL");
         if (env && env[0] == 'w') variant = BP_KERNEL_WARP_TILE;
         else if (env && env[0] == 's' && staged_applies(g, opt->schedule, serial)) variant = BP_KERNEL_STAGED_TILE;
         else variant = BP_KERNEL_BLOCK_TILE;
     }
-    if (variant != BP_KERNEL_BLOCK_TILE && variant != BP_KERNEL_WARP_TILE && variant != BP_KERNEL_STAGED_TILE)
+    if (variant == BP_KERNEL_BLOCK_TILE && (opt->kernel_variant == BP_KERNEL_AUTO || opt->kernel_variant == BP_KERNEL_SPLIT)) {
+        // large uniform graphs: the split schedule (send pass in source-range
+        // order + node pass)
+        bool use = false;
+        if ((st = split_applies(g, opt->schedule, opt->kernel_variant, &use))) return st;
+        if (use) variant = BP_KERNEL_SPLIT;
+        else if (opt->kernel_variant == BP_KERNEL_SPLIT)
+            return set_error(BP_ERR_INVALID, "split tiles need the node schedule on a uniform graph of at most 4 "
+                                             "states whose 128-node tiles hold at most %u in-edges",
+                                             g->ms <= 2 ? 4096u / g->ms : 8192u / g->ms);
+    }
+    if (variant != BP_KERNEL_BLOCK_TILE && variant != BP_KERNEL_WARP_TILE && variant != BP_KERNEL_STAGED_TILE &&
+        variant != BP_KERNEL_SPLIT)
         return set_error(BP_ERR_INVALID, "unknown kernel variant %d", opt->kernel_variant);
     if (variant == BP_KERNEL_STAGED_TILE && opt->schedule == BP_SCHEDULE_NODE && !staged_applies(g, opt->schedule, serial))
         return set_error(BP_ERR_INVALID, "staged tiles need a uniform 2-state graph of mean in-degree <= 4.5 and the f64 delta");
     uint32_t grid_blocks = grid_for(g->E, 256);
-    if (opt->schedule == BP_SCHEDULE_NODE && (st = flood_grid(g, variant, &grid_blocks))) return st;
+    if (opt->schedule == BP_SCHEDULE_NODE && (st = flood_grid(g, variant, &grid_blocks, serial))) return st;
     // small graphs (a co-resident block per tile), node schedule, f64 delta,
     // block tiles: every iteration in one cooperative launch
     // (BP_FLOOD_FUSED=0 keeps the launch-per-iteration loop)
@@ -2242,6 +2436,10 @@ int bp_loopy(bp_graph *g, const bp_loopy_options *opt, bp_loopy_result *res) {
     if (opt->schedule == BP_SCHEDULE_NODE) {
         auto gather = [&]() -> int { BP_DISPATCH_MS(g->ms, g->uniform != 0, launch_gather, g); };
         if ((st = gather())) return st;
+    }
+    if (variant == BP_KERNEL_SPLIT) {
+        auto conv = [&]() -> int { BP_DISPATCH_MS(g->ms, g->uniform != 0, split_convert, g, 0); };
+        if ((st = conv())) return st;
     }
 
     if (fgrid) {
@@ -2299,6 +2497,12 @@ int bp_loopy(bp_graph *g, const bp_loopy_options *opt, bp_loopy_result *res) {
         BP_CUDA(cudaGetLastError());
     }
     BP_CUDA(cudaEventRecord(g->ev1, g->stream));
+    if (variant == BP_KERNEL_SPLIT) {
+        // both message arrays back to position order (every run executes at
+        // least one iteration, so both send-order arrays are defined)
+        auto conv = [&]() -> int { BP_DISPATCH_MS(g->ms, g->uniform != 0, split_convert, g, 1); };
+        if ((st = conv())) return st;
+    }
     BP_CUDA(cudaMemcpyAsync(g->ctl_host, g->ctl, sizeof(LoopyCtl), cudaMemcpyDeviceToHost, g->stream));
     BP_CUDA(cudaStreamSynchronize(g->stream));
     c = *g->ctl_host;

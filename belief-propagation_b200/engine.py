@@ -157,7 +157,7 @@ class BPGraph:
         o.delta_mode = _DELTA[delta]
         o.verbose = int(bool(verbose))
         o.graph_chunk = int(graph_chunk)
-        o.kernel_variant = {"auto": 0, "block": 1, "warp": 2, "staged": 3}[kernel]
+        o.kernel_variant = {"auto": 0, "block": 1, "warp": 2, "staged": 3, "split": 4}[kernel]
         r = N.LoopyResult()
         N.check(self.lib.bp_loopy(self.h, C.byref(o), C.byref(r)))
         return r.as_dict()

@@ -184,6 +184,45 @@ def fp64_error_loopy(net, tol, max_it, gpu_beliefs, gpu_iterations, what):
             "fp64_iterations": int(f64["ret"]), "fp64_delta": float(f64["delta"]), "sample": what}
 
 
+def fp64_error_curve(net, graph, checkpoints=(1, 2, 5, 10, 20, 50, 100)):
+    """How far the fp32 schedule (the reference's arithmetic, which the GPU
+    reproduces bit for bit) drifts from the same schedule in fp64, iteration
+    by iteration, tolerance 0: the GPU graph `graph` and the oracle's fp32 and
+    fp64 runs are continued from checkpoint to checkpoint (each continuation
+    recomputes the send buffers from the beliefs and latest messages, as the
+    next iteration would).  The reference's update multiplies each belief
+    into itself every iteration, so beliefs saturate towards 0/1 and a node
+    whose fp32 and fp64 runs tip opposite ways shows an error near 1."""
+    O, R = _restatement()
+    og = O.OracleGraph(net)
+    S = int(net.s_max)
+    graph.set_beliefs(net.beliefs)
+    graph.latest_slot = 1
+    graph.init_messages()
+    st = {}
+    done = 0
+    out = []
+    for k in checkpoints:
+        graph.loopy(0.0, k - done, delta="f64")
+        b_gpu = graph.beliefs().astype(np.float64)[:, :S]
+        row = {"iterations": k}
+        for dt, name in ((np.float32, "oracle"), (np.float64, "fp64")):
+            prev = st.get(name)
+            if prev is None:
+                r = R.loopy(og, 0.0, k, dtype=dt)
+            else:
+                r = R.loopy(og, 0.0, k - done, dtype=dt, init=False, beliefs=prev["beliefs"],
+                            msgs=(prev["latest"], prev["older"]))
+            st[name] = r
+            row[f"max_abs_err_vs_{name}"] = float(np.abs(b_gpu - r["beliefs"][:, :S]).max())
+        ref64 = st["fp64"]["beliefs"][:, :S]
+        row["argmax_differs_vs_fp64"] = float(np.mean(b_gpu.argmax(1) != ref64.argmax(1)))
+        row["nodes_off_by_1e-5_vs_fp64"] = float(np.mean(np.abs(b_gpu - ref64).max(1) > 1e-5))
+        out.append(row)
+        done = k
+    return out
+
+
 def flood_bytes_per_iteration(V, E, S):
     """Compulsory HBM bytes of one fused flooding iteration (loopy.cu header)."""
     return E * (4 * S * S + 4 + 4 * S * 3) + V * (4 + 4 * S * 3)
@@ -258,11 +297,14 @@ def power_law_accuracy(a, handle):
         g.init_messages()
         r = g.loopy(0.0, a.iterations, delta="f64")
         b = g.beliefs()
+        out = fp64_error_loopy(net, 0.0, a.iterations, b, r["iterations"],
+                               f"{net.V:,} nodes / {net.E:,} edges of the same generator, {a.iterations} fixed "
+                               "iterations, same code path")
+        out["by_iteration"] = fp64_error_curve(net, g, tuple(k for k in (1, 2, 5, 10, 20, 50, 100)
+                                                             if k <= a.iterations))
     finally:
         g.close()
-    return fp64_error_loopy(net, 0.0, a.iterations, b, r["iterations"],
-                            f"{net.V:,} nodes / {net.E:,} edges of the same generator, {a.iterations} fixed "
-                            "iterations, same code path")
+    return out
 
 
 def run_reference_arm(a, rank, world):
@@ -476,6 +518,12 @@ def run_random10k(a, rank, world):
         res[delta] = (ms, r["iterations"], r["executed"], r["serial_sums"], g.beliefs())
     clk = clocks.stop()
     b_gpu = res["serial"][4]
+    curve = None
+    if rank == 0:
+        try:
+            curve = fp64_error_curve(net, g)
+        except Exception as ex:  # reported, not fatal
+            curve = [{"error": str(ex)[:200]}]
     g.close()
     cpu = None
     if O.reference_available():
@@ -496,6 +544,7 @@ def run_random10k(a, rank, world):
         try:
             accuracy = fp64_error_loopy(net, 1e-3, 100, b_gpu, res["serial"][1],
                                         "the full workload, the reference's serial fp32 stopping rule")
+            accuracy["by_iteration"] = curve
         except Exception as ex:  # reported, not fatal
             accuracy = {"error": str(ex)[:200]}
     if rank != 0:

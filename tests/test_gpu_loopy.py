@@ -262,22 +262,110 @@ def headline_sample(synth, O):
     return net, out
 
 
+@pytest.mark.parametrize("path", ["block", "split"])
 @pytest.mark.parametrize("iterations", [10, 100])
-def test_loopy_headline_path_bit_exact(bp, headline_sample, monkeypatch, iterations):
-    """The benchmark's exact code path -- nodes renumbered by out-degree, the
-    persistent-grid block-tile kernel with the source id loaded one round
-    ahead, fp64 delta, tolerance 0 -- on a graph large enough that the
-    evict-last send-buffer prefix (cut to 1 MB here) leaves most sources on
-    the plain-load side: bit-exact beliefs and latest messages against the
-    oracle after 10 and 100 iterations."""
+def test_loopy_headline_path_bit_exact(bp, headline_sample, monkeypatch, iterations, path):
+    """The benchmark's code paths -- nodes renumbered by out-degree, fp64
+    delta, tolerance 0 -- on the headline generator at 1M nodes / 4M edges:
+    block: the persistent-grid block-tile kernel with the source id loaded
+    one round ahead and the evict-last send-buffer prefix cut to 1 MB, so
+    most sources take the plain-load side;
+    split: the send pass over source ranges (cut to 2 MB of send buffers
+    here, 4 ranges) + node pass, the schedule the full-size graph runs.
+    Bit-exact beliefs and latest messages against the oracle after 10 and
+    100 iterations."""
     net, ora = headline_sample
-    monkeypatch.setenv("BP_FLOOD_HOT_MB", "1")
-    monkeypatch.setenv("BP_FLOOD_PIPE", "1")
-    gpu = gpu_loopy(bp, net, 0.0, iterations, delta="f64", reorder=True)
+    if path == "block":
+        monkeypatch.setenv("BP_FLOOD_SPLIT", "0")
+        monkeypatch.setenv("BP_FLOOD_HOT_MB", "1")
+        monkeypatch.setenv("BP_FLOOD_PIPE", "1")
+    else:
+        monkeypatch.setenv("BP_FLOOD_SPLIT", "1")
+        monkeypatch.setenv("BP_FLOOD_RANGE_MB", "2")
+    gpu = gpu_loopy(bp, net, 0.0, iterations, delta="f64", reorder=True, kernel="auto" if path == "block" else "split")
     assert gpu["executed"] == iterations
     latest = gpu["slot1"] if gpu["latest"] == 1 else gpu["slot0"]
     np.testing.assert_array_equal(gpu["beliefs"][:, :2], ora[iterations]["beliefs"][:, :2])
     np.testing.assert_array_equal(latest[:, :2], ora[iterations]["latest"][:, :2])
+
+
+SPLIT_CASES = [
+    dict(V=3000, E=12000, S=2, seed=41),
+    dict(V=1000, E=5000, S=3, seed=42),
+    dict(V=800, E=4000, S=4, seed=43),
+    dict(V=2500, E=9000, S=1, seed=44),
+]
+
+
+@pytest.mark.parametrize("reorder", [False, True], ids=["ids", "renumbered"])
+@pytest.mark.parametrize("case", SPLIT_CASES, ids=lambda c: f"S{c['S']}")
+@pytest.mark.parametrize("range_mb", ["0", "32"], ids=["many_ranges", "one_range"])
+def test_loopy_split_schedule_parity(bp, synth, restatement, O, monkeypatch, case, reorder, range_mb):
+    """The split schedule (send pass over source ranges + node pass) forced
+    on small graphs: with one range, and with the range cut to one node's
+    send buffer (BP_FLOOD_RANGE_MB=0 rounds up to the 32-range limit); the
+    reference's serial delta and the fp64 delta, check every iteration and
+    every 10 (_acc): beliefs, both message arrays, iteration count and
+    returned deltas equal the oracle's."""
+    monkeypatch.setenv("BP_FLOOD_SPLIT", "1")
+    monkeypatch.setenv("BP_FLOOD_RANGE_MB", range_mb)
+    net = synth.random_loopy(case["V"], case["E"], case["S"], 0.1, seed=case["seed"])
+    S = case["S"]
+    for tol, max_it, check in ((1e-3, 40, 1), (0.0, 15, 1), (1e-3, 45, 10)):
+        ora = restatement.loopy(O.OracleGraph(net), tol, max_it, check_every=check)
+        gpu = gpu_loopy(bp, net, tol, max_it, check_every=check, reorder=reorder, kernel="split")
+        assert_same(gpu, ora, S)
+        f64 = gpu_loopy(bp, net, tol, max_it, check_every=check, reorder=reorder, kernel="split", delta="f64")
+        blk = gpu_loopy(bp, net, tol, max_it, check_every=check, reorder=reorder, kernel="block", delta="f64")
+        for k in ("iterations", "executed", "latest"):
+            assert f64[k] == blk[k], k
+        for k in ("beliefs", "slot0", "slot1"):
+            np.testing.assert_array_equal(f64[k], blk[k])
+
+
+def test_loopy_split_schedule_power_law_serial_delta(bp, synth, restatement, O, monkeypatch):
+    """A power-law graph through the split schedule with four source ranges
+    and the reference's serial delta at a tolerance it converges under."""
+    monkeypatch.setenv("BP_FLOOD_SPLIT", "1")
+    monkeypatch.setenv("BP_FLOOD_RANGE_MB", "0")
+    net = synth.power_law_loopy(1 << 14, 1 << 16, 2, 0.1, seed=9)
+    ora = restatement.loopy(O.OracleGraph(net), 1e-2, 60)
+    assert_same(gpu_loopy(bp, net, 1e-2, 60, reorder=True, kernel="split"), ora, 2)
+
+
+def test_loopy_split_schedule_refuses_or_falls_back(bp, synth, restatement, O, monkeypatch):
+    """Graphs the split layout does not hold: mixed state counts, more than 4
+    states, and a hub whose 128-node tile holds more in-edges than the node
+    pass stages.  kernel="split" refuses them; the default loop (split
+    wanted) runs k_flood on them with the oracle's results."""
+    from belief_propagation_b200.native import BPError
+    from belief_propagation_b200.engine import BPGraph
+    rng = np.random.default_rng(3)
+    base = synth.random_loopy(400, 1600, 2, 0.1, seed=8)
+    ns = rng.choice(np.array([2, 3], np.uint32), size=base.V)
+    S = 3
+    b = rng.random((base.V, S), dtype=np.float32) * (np.arange(S)[None] < ns[:, None])
+    j = rng.random((base.E, S, S), dtype=np.float32)
+    j *= (np.arange(S)[None, :, None] < ns[base.src][:, None, None])
+    j *= (np.arange(S)[None, None, :] < ns[base.dst][:, None, None])
+    mixed = synth.Network(ns, b.astype(np.float32), base.observed, base.src, base.dst, j.astype(np.float32))
+    five = synth.random_loopy(300, 1200, 5, 0.1, seed=2)
+    V = 3000
+    src = rng.integers(1, V, 5000).astype(np.uint32)
+    dst = np.zeros(5000, np.uint32)          # node 0's tile: 5000 in-edges > 2048
+    hub = synth.Network(np.full(V, 2, np.uint32), rng.random((V, 2), dtype=np.float32), np.zeros(V, np.uint8),
+                        src, dst, rng.random((5000, 2, 2), dtype=np.float32))
+    monkeypatch.setenv("BP_FLOOD_SPLIT", "1")
+    for net in (mixed, five, hub):
+        g = BPGraph.from_network(net)
+        try:
+            with pytest.raises(BPError):
+                g.loopy(0.0, 3, delta="f64", kernel="split")
+        finally:
+            g.close()
+        ora = restatement.loopy(O.OracleGraph(net), 1e-3, 20)
+        gpu = gpu_loopy(bp, net, 1e-3, 20)
+        assert_same(gpu, ora, int(net.s_max))
 
 
 def _staged_cases(synth):
