@@ -27,7 +27,7 @@ LIB = os.path.join(LIB_DIR, "libbp.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = ["engine.cu", "loopy.cu", "tree.cu", "levels_gpu.cu", "batch.cu", "unrolled.cu"]
-C_SOURCES = ["graph_api.c", "levels.c"]
+C_SOURCES = ["graph_api.c", "levels.c", "xmlbif.c"]
 HEADERS = ["bp_internal.h", "bp_device.cuh", "bp_levels.h", "bp_serial.cuh", "flood_split.cuh"]
 
 
@@ -50,7 +50,7 @@ def build(force=False, verbose_ptxas=False, jobs=None):
     os.makedirs(OBJ, exist_ok=True)
     os.makedirs(LIB_DIR, exist_ok=True)
     common_deps = [os.path.join(CSRC, h) for h in HEADERS] + [
-        os.path.join(INCLUDE, h) for h in ("bp.h", "graph.h", "constants.h")]
+        os.path.join(INCLUDE, h) for h in ("bp.h", "graph.h", "constants.h", "xml-expression.h")]
     steps = []
     objs = []
     for s in CU_SOURCES:

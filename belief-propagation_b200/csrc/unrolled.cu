@@ -180,6 +180,8 @@ __device__ __forceinline__ void sum_slots(const float *__restrict__ xc, uint32_t
 
 template <int S>
 __global__ void k_u_logsoftmax(uint32_t V, const float *__restrict__ theta, float *__restrict__ lb0) {
+    griddep_launch_dependents();
+    griddep_wait();
     const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= V) return;
     float t[S];
@@ -195,7 +197,9 @@ template <int S>
 __global__ void __launch_bounds__(kUThreads) k_u_gather_q(const UGraph g, const float *__restrict__ lb,
                                                           const float *__restrict__ send, float *__restrict__ lq) {
     __shared__ __align__(16) float sm[2 * kUMaxTables * S * S];
-    load_tables_smem<S>(g, sm);
+    griddep_launch_dependents();
+    load_tables_smem<S>(g, sm);   // the tables do not change inside a pass
+    griddep_wait();               // the kernel ahead's states
     const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= g.V) return;
     float qo[S];
@@ -210,7 +214,9 @@ __global__ void __launch_bounds__(kUThreads) k_u_iter(const UGraph g, const floa
                                                       const float *__restrict__ lq_in, float *__restrict__ lb_out,
                                                       float *__restrict__ lq_out) {
     __shared__ __align__(16) float sm[2 * kUMaxTables * S * S];
+    griddep_launch_dependents();
     load_tables_smem<S>(g, sm);
+    griddep_wait();
     const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= g.V) return;
     float P[S], a[S];
@@ -300,7 +306,9 @@ __global__ void __launch_bounds__(bwd_threads<S>()) k_u_pair_grad(const UGraph g
     __shared__ __align__(16) float sm[2 * kUMaxTables * S * S];
     __shared__ float sacc[REG ? 1 : S * S * NT];
     __shared__ float wred[NT / 32][REG ? S * S : 1];
+    griddep_launch_dependents();
     load_tables_smem<S>(g, sm);
+    griddep_wait();
     float acc[REG ? S * S : 1];
     if constexpr (REG) {
 #pragma unroll
@@ -400,7 +408,7 @@ __device__ __forceinline__ void bwd_edge(const float *J, const float *x, const f
 // source-sorted slots; null at t = T).  Writes lbbar_out (mode 1: lbbar_0
 // without its own send term), this iteration's x adjoint terms xc, and adds
 // the block's log-table adjoint into epart.
-template <int S>
+template <int S, int B = 2>
 __global__ void __launch_bounds__(bwd_threads<S>(), bwd_min_blocks<S>()) k_u_bwd(const UGraph g, int mode, const float *__restrict__ send,
                                                            const float *__restrict__ lb_t,
                                                            const float *__restrict__ lbbar_t,
@@ -409,11 +417,12 @@ __global__ void __launch_bounds__(bwd_threads<S>(), bwd_min_blocks<S>()) k_u_bwd
                                                            double *__restrict__ epart, float *__restrict__ pbar_out) {
     constexpr int NT = bwd_threads<S>();
     constexpr bool REG = S <= 4;
-    constexpr int B = 2;
     __shared__ __align__(16) float sm[2 * kUMaxTables * S * S];
     __shared__ float sacc[REG ? 1 : S * S * NT];
     __shared__ float wred[NT / 32][REG ? S * S : 1];
+    griddep_launch_dependents();
     load_tables_smem<S>(g, sm);
+    griddep_wait();
     float acc[REG ? S * S : 1];
     if constexpr (REG) {
 #pragma unroll
@@ -510,7 +519,9 @@ __global__ void __launch_bounds__(kMmaThreads, 4) k_u_bwd_mma(const UGraph g, in
     __shared__ __align__(16) float st_e[NW][32][8];
     __shared__ float st_tr[NW][32];
     __shared__ float dred[NW][16][8];
+    griddep_launch_dependents();
     load_tables_smem<S>(g, sm);
+    griddep_wait();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gq = lane >> 2, tq = lane & 3;
     float d[4] = {0.0f, 0.0f, 0.0f, 0.0f};
     for (uint32_t base = (blockIdx.x * NW + warp) * 32u;; base += gridDim.x * (uint32_t)kMmaThreads) {
@@ -598,6 +609,8 @@ template <int S>
 __global__ void __launch_bounds__(kUThreads) k_u_bwd_src(const UGraph g, const float *__restrict__ xc,
                                                          const float *__restrict__ add, const float *__restrict__ lb0,
                                                          float *__restrict__ theta_bar) {
+    griddep_launch_dependents();
+    griddep_wait();
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= g.V) return;
     float acc[S], lb[S], sum = 0.0f;
@@ -615,6 +628,8 @@ __global__ void __launch_bounds__(kUThreads) k_u_bwd_src(const UGraph g, const f
 // entry; partials laid out [table][block][S*S]
 __global__ void k_u_reduce_pair(const double *__restrict__ epart, uint32_t nblk, uint32_t ss, float *__restrict__ out) {
     __shared__ double red[32];
+    griddep_launch_dependents();
+    griddep_wait();
     const uint32_t k = blockIdx.x, kt = k / ss, idx = k % ss;
     const double *base = epart + (size_t)kt * nblk * ss + idx;
     double t = 0.0;
@@ -658,6 +673,44 @@ struct bp_unrolled {
 
 namespace bpx {
 
+// Launches of the forward and backward passes use programmatic dependent
+// launch: each kernel lets the next one start once all its blocks run; the
+// next kernel loads and exponentiates the tables (which no kernel of a pass
+// writes) and then waits (griddepcontrol.wait) for the whole grid ahead and
+// its memory before it reads any state.  BP_UNROLLED_PDL=0 turns it off.
+static bool u_pdl() {
+    static int on = -1;
+    if (on < 0) {
+        const char *env = getenv("BP_UNROLLED_PDL");
+        on = (env && env[0] == '0') ? 0 : 1;
+    }
+    return on != 0;
+}
+
+template <typename... KArgs, typename... Args>
+static int u_launch(void (*kern)(KArgs...), unsigned grid, unsigned block, cudaStream_t st, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = u_pdl() ? 1 : 0;
+    cudaError_t e = cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaLaunchKernelEx", __FILE__, __LINE__);
+    return BP_OK;
+}
+
+// in-edges per batch of the adjoint kernel (BP_UBWD_BATCH=2|4, 1-4 states)
+// and nodes per thread (BP_UBWD_NPT=1|2); every choice gives the same results
+static int ubwd_env(const char *name, int dflt, int alt) {
+    const char *env = getenv(name);
+    return (env && atoi(env) == alt) ? alt : dflt;
+}
+
 // the forward on the engine's own buffers (theta_buf, tables): captured once
 // into a CUDA graph, replayed on every call
 template <int S>
@@ -666,9 +719,11 @@ static int u_forward(bp_unrolled *u) {
     const size_t VS = (size_t)u->V * S;
     const unsigned gv = grid_for(u->V, kUThreads);
     cudaStream_t st = u->stream;
-    k_u_logsoftmax<S><<<gv, kUThreads, 0, st>>>(u->V, u->theta_buf, u->ck_b);
-    k_u_gather_q<S><<<gv, kUThreads, 0, st>>>(g, u->ck_b, u->ck_b, u->ck_q);
-    BP_CUDA(cudaGetLastError());
+    int rc;
+    if ((rc = u_launch(k_u_logsoftmax<S>, gv, kUThreads, st, u->V, (const float *)u->theta_buf, u->ck_b))) return rc;
+    if ((rc = u_launch(k_u_gather_q<S>, gv, kUThreads, st, g, (const float *)u->ck_b, (const float *)u->ck_b,
+                       u->ck_q)))
+        return rc;
     // state t (lb_t, lQ_{t+1}) lives in checkpoint slot t/ck when t % ck == 0;
     // inside the last segment in its slot of the segment buffer, where the
     // backward reads it without recomputing; else in pp[t&1]
@@ -687,9 +742,10 @@ static int u_forward(bp_unrolled *u) {
     for (uint32_t t = 1; t <= u->T; ++t) {
         float *bo = (t == u->T) ? u->bT : loc_b(t);
         float *qo = (t == u->T) ? u->pp_q + (t & 1) * VS : loc_q(t);
-        k_u_iter<S><<<gv, kUThreads, 0, st>>>(g, loc_b(t - 1), loc_q(t - 1), bo, qo);
+        if ((rc = u_launch(k_u_iter<S>, gv, kUThreads, st, g, (const float *)loc_b(t - 1), (const float *)loc_q(t - 1),
+                           bo, qo)))
+            return rc;
     }
-    BP_CUDA(cudaGetLastError());
     return BP_OK;
 }
 
@@ -703,23 +759,32 @@ static int u_backward(bp_unrolled *u) {
     constexpr int BT = bwd_threads<S>();
     // one table and 5..8 states: the table adjoint on the tensor cores
     const bool mma = S >= 5 && S <= 8 && u->K == 1;
-    const unsigned gb = mma ? grid_for(u->V, kMmaThreads * 2) : grid_for(u->V, BT * kBwdNodesPerThread);
+    const int batch = S <= 4 ? ubwd_env("BP_UBWD_BATCH", 2, 4) : 2;
+    const uint32_t npt = (uint32_t)ubwd_env("BP_UBWD_NPT", (int)kBwdNodesPerThread, 1);
+    const unsigned gb = mma ? grid_for(u->V, kMmaThreads * 2) : grid_for(u->V, BT * npt);
     cudaStream_t st = u->stream;
+    int rc = BP_OK;
     auto adjoint = [&](int mode, const float *send, const float *b_t, const float *gbar, const float *xn, float *out,
-                       float *xo, float *pb) {
+                       float *xo, float *pb) -> int {
         if constexpr (S >= 5 && S <= 8) {
-            if (mma) {
-                k_u_bwd_mma<S><<<gb, kMmaThreads, 0, st>>>(g, mode, send, b_t, gbar, xn, out, xo, u->epart);
-                return;
-            }
+            if (mma) return u_launch(k_u_bwd_mma<S>, gb, kMmaThreads, st, g, mode, send, b_t, gbar, xn, out, xo,
+                                     u->epart);
         }
-        k_u_bwd<S><<<gb, BT, 0, st>>>(g, mode, send, b_t, gbar, xn, out, xo, u->epart, pb);
+        if constexpr (S <= 4) {
+            if (batch == 4)
+                return u_launch(k_u_bwd<S, 4>, gb, BT, st, g, mode, send, b_t, gbar, xn, out, xo, u->epart, pb);
+        }
+        return u_launch(k_u_bwd<S, 2>, gb, BT, st, g, mode, send, b_t, gbar, xn, out, xo, u->epart, pb);
     };
     BP_CUDA(cudaMemsetAsync(u->epart, 0, sizeof(double) * u->K * gb * S * S, st));
     // several tables: the table adjoint of each backward step, one pass per table
-    auto pair_grads = [&](const float *send) {
-        for (uint32_t k = 0; u->K > 1 && k < u->K; ++k)
-            k_u_pair_grad<S><<<gb, BT, 0, st>>>(g, send, u->pbar, k, u->epart + (size_t)k * gb * S * S);
+    auto pair_grads = [&](const float *send) -> int {
+        for (uint32_t k = 0; u->K > 1 && k < u->K; ++k) {
+            int r = u_launch(k_u_pair_grad<S>, gb, BT, st, g, send, (const float *)u->pbar, k,
+                             u->epart + (size_t)k * gb * S * S);
+            if (r) return r;
+        }
+        return BP_OK;
     };
     float *pbar = u->K > 1 ? u->pbar : nullptr;
     int bc = 0, rn = 0;
@@ -730,14 +795,16 @@ static int u_backward(bp_unrolled *u) {
     // two share nothing but the double-buffered segment states (buffer s & 1)
     auto seg_b = [&](uint32_t s, uint32_t j) { return u->seg_b + ((size_t)(s & 1u) * u->ck + j) * VS; };
     auto seg_q = [&](uint32_t s, uint32_t j) { return u->seg_q + ((size_t)(s & 1u) * u->ck + j) * VS; };
-    auto recompute = [&](uint32_t s) {
+    auto recompute = [&](uint32_t s) -> int {
         const uint32_t t0 = s * u->ck, t_end = std::min(t0 + u->ck, u->T);
         const float *ckb = u->ck_b + (size_t)s * VS, *ckq = u->ck_q + (size_t)s * VS;
         for (uint32_t j = 1; j + t0 < t_end; ++j) {
             const float *bi = (j == 1) ? ckb : seg_b(s, j - 1);
             const float *qi = (j == 1) ? ckq : seg_q(s, j - 1);
-            k_u_iter<S><<<gv, kUThreads, 0, u->side>>>(g, bi, qi, seg_b(s, j), seg_q(s, j));
+            int r = u_launch(k_u_iter<S>, gv, kUThreads, u->side, g, bi, qi, seg_b(s, j), seg_q(s, j));
+            if (r) return r;
         }
+        return BP_OK;
     };
     // the last segment's states are the forward's own (u_forward)
     BP_CUDA(cudaEventRecord(u->ev_fork, st));
@@ -747,7 +814,7 @@ static int u_backward(bp_unrolled *u) {
         if (s >= 1) {
             // buffer (s-1)&1 was last read by the adjoint of segment s+1
             if ((uint32_t)s + 1 < nseg) BP_CUDA(cudaStreamWaitEvent(u->side, u->ev_bwd[(s + 1) & 1], 0));
-            recompute((uint32_t)s - 1);
+            if ((rc = recompute((uint32_t)s - 1))) return rc;
             BP_CUDA(cudaEventRecord(u->ev_rec[(s - 1) & 1], u->side));
         }
         BP_CUDA(cudaStreamWaitEvent(st, u->ev_rec[s & 1], 0));
@@ -759,8 +826,8 @@ static int u_backward(bp_unrolled *u) {
             const float *b_t = (t == u->T) ? u->bT
                                : (t == t_end) ? u->ck_b + (size_t)(s + 1) * VS
                                               : seg_b((uint32_t)s, j + 1);  // lb_t
-            adjoint(0, q_t, b_t, u->bbar[bc], xc_next, u->bbar[bc ^ 1], u->xc[rn], pbar);
-            pair_grads(q_t);
+            if ((rc = adjoint(0, q_t, b_t, u->bbar[bc], xc_next, u->bbar[bc ^ 1], u->xc[rn], pbar))) return rc;
+            if ((rc = pair_grads(q_t))) return rc;
             bc ^= 1;
             xc_next = u->xc[rn];
             rn ^= 1;
@@ -770,12 +837,13 @@ static int u_backward(bp_unrolled *u) {
     BP_CUDA(cudaGetLastError());
     // initial step: lQ_1 = lb_0 + sum lm(lb_0); its own x adjoint goes to lb_0
     const float *b0 = u->ck_b;
-    adjoint(1, b0, nullptr, u->bbar[bc], xc_next, u->bbar[bc ^ 1], u->xc[rn], pbar);
-    pair_grads(b0);
-    k_u_bwd_src<S><<<gv, kUThreads, 0, st>>>(g, u->xc[rn], u->bbar[bc ^ 1], b0, u->gtheta_buf);
-    k_u_reduce_pair<<<u->K * S * S, 256, 0, st>>>(u->epart, gb, S * S, u->glogp_buf);
-    BP_CUDA(cudaGetLastError());
-    return BP_OK;
+    if ((rc = adjoint(1, b0, nullptr, u->bbar[bc], xc_next, u->bbar[bc ^ 1], u->xc[rn], pbar))) return rc;
+    if ((rc = pair_grads(b0))) return rc;
+    if ((rc = u_launch(k_u_bwd_src<S>, gv, kUThreads, st, g, (const float *)u->xc[rn], (const float *)u->bbar[bc ^ 1],
+                       b0, u->gtheta_buf)))
+        return rc;
+    return u_launch(k_u_reduce_pair, u->K * S * S, 256u, st, (const double *)u->epart, gb, (uint32_t)(S * S),
+                    u->glogp_buf);
 }
 
 static void u_free(bp_unrolled *u) {

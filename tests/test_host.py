@@ -26,7 +26,9 @@ def _declared(header):
 def test_library_exports_every_declared_symbol(native):
     lib = native.load()
     missing = []
-    for header in ("graph.h", "bp.h"):
+    headers = sorted(h for h in os.listdir(os.path.join(ROOT, "include")) if h.endswith(".h"))
+    assert {"graph.h", "bp.h", "constants.h", "xml-expression.h"} <= set(headers)
+    for header in headers:
         for name in _declared(header):
             try:
                 getattr(lib, name)
