@@ -257,6 +257,35 @@ __device__ __forceinline__ void send_msg(const float *__restrict__ J, const floa
     for (int i = 0; i < MS; ++i) m[i] = (UNI || i < x) ? FDIV(m[i], sum) : 0.0f;
 }
 
+// the same send step on a dense x-by-y table (row stride y; for uniform
+// graphs y = MS): the operations and their order are send_msg's
+template <int MS, bool UNI>
+__device__ __forceinline__ void send_msg_dense(const float *__restrict__ J, const float *buf, int x, int y,
+                                               float *m) {
+    float sum = 0.0f;
+#pragma unroll
+    for (int i = 0; i < MS; ++i) {
+        float partial = 0.0f;
+        if (UNI || i < x) {
+            float row[MS];
+            if constexpr (UNI && MS % 2 == 0) {
+                ldv<MS, kReadOnly>(J + i * MS, row);
+            } else {
+#pragma unroll
+                for (int c = 0; c < MS; ++c) row[c] = (UNI || c < y) ? __ldg(J + i * (UNI ? MS : y) + c) : 0.0f;
+            }
+#pragma unroll
+            for (int c = 0; c < MS; ++c)
+                if (UNI || c < y) partial = FADD(partial, FMUL(row[c], buf[c]));
+            sum = FADD(sum, partial);
+        }
+        m[i] = partial;
+    }
+    if (sum <= 0.0f) sum = 1.0f;
+#pragma unroll
+    for (int i = 0; i < MS; ++i) m[i] = (UNI || i < x) ? FDIV(m[i], sum) : 0.0f;
+}
+
 // buf[i] *= m[i] for i < s unless m[i] is NaN: graph.c:450-459 (combine_message)
 template <int MS, bool UNI>
 __device__ __forceinline__ void combine(float *buf, const float *m, int s) {

@@ -98,6 +98,13 @@ struct TreeData {
     uint32_t *level_wave_begin = nullptr; // host [num_levels + 1] index into waves
     uint32_t total_waves = 0;
     cudaGraphExec_t exec = nullptr;    // bp_tree's launch sequence, captured once
+    // out-edge order (q, the source-sorted CSR) arrays of the tree kernels, so
+    // a sending node reads its out-edges' tables and the destinations' level
+    // data as contiguous runs instead of at random positions:
+    float *q_joint = nullptr;          // x-by-y tables (row stride y), each padded to 4 floats
+    uint32_t *q_joff = nullptr;        // [E] float offset of out-edge q's table
+    uint2 *q_lvidx = nullptr;          // [E] (level, index in level) of out-edge q's destination
+    uint8_t *q_y = nullptr;            // [E] state count of out-edge q's destination
 };
 
 }  // namespace bpx

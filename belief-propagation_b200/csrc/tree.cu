@@ -14,6 +14,7 @@
 // which is what the sequential loop sees, so any call order the reference
 // accepts gives the reference's messages.  All messages live in slot 0
 // (struct graph's edges_messages), position order.
+#include <cub/device/device_scan.cuh>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -26,12 +27,18 @@
 
 namespace bpx {
 
+// Out-edges are walked in the source-sorted (q) order, whose per-edge arrays
+// (TreeData::q_*) put a node's out-edge tables, destination state counts and
+// destination level data next to each other; only the destination's visited
+// flag and the message store (at the edge's position) are random accesses.
+
 // propagate_using_levels_start (graph.c:376-424)
 template <int MS, bool UNI>
 __global__ void k_tree_start(const uint32_t *__restrict__ nodes, uint32_t n, const uint32_t *__restrict__ out_ptr,
-                             const uint32_t *__restrict__ out_pos, const uint32_t *__restrict__ out_dst,
-                             const uint8_t *__restrict__ node_s, const float *__restrict__ joint,
-                             const float *__restrict__ belief, float *__restrict__ msg, uint8_t *__restrict__ visited) {
+                             const uint32_t *__restrict__ out_pos, const uint8_t *__restrict__ node_s,
+                             const uint8_t *__restrict__ q_y, const uint32_t *__restrict__ q_joff,
+                             const float *__restrict__ q_joint, const float *__restrict__ belief,
+                             float *__restrict__ msg, uint8_t *__restrict__ visited) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const uint32_t u = nodes[k];
@@ -41,9 +48,9 @@ __global__ void k_tree_start(const uint32_t *__restrict__ nodes, uint32_t n, con
     ldv<MS>(belief + (size_t)u * MS, buf);
     for (uint32_t q = out_ptr[u]; q < out_ptr[u + 1]; ++q) {
         const uint32_t p = out_pos[q];
-        const int y = UNI ? MS : node_s[out_dst[q]];
+        const int y = UNI ? MS : q_y[q];
         float m[MS];
-        send_msg<MS, UNI>(joint + (size_t)p * (MS * MS), buf, x, y, m);
+        send_msg_dense<MS, UNI>(q_joint + q_joff[q], buf, x, y, m);
         stv<MS>(msg + (size_t)p * MS, m);
     }
 }
@@ -53,8 +60,9 @@ template <int MS, bool UNI>
 __global__ void k_tree_wave(const uint32_t *__restrict__ nodes, uint32_t n, uint32_t level,
                             const uint32_t *__restrict__ in_ptr, const uint32_t *__restrict__ out_ptr,
                             const uint32_t *__restrict__ out_pos, const uint32_t *__restrict__ out_dst,
-                            const uint32_t *__restrict__ node_level, const uint32_t *__restrict__ node_lidx,
-                            const uint8_t *__restrict__ node_s, const float *__restrict__ joint,
+                            const uint2 *__restrict__ q_lvidx, const uint32_t *__restrict__ node_lidx,
+                            const uint8_t *__restrict__ node_s, const uint8_t *__restrict__ q_y,
+                            const uint32_t *__restrict__ q_joff, const float *__restrict__ q_joint,
                             float *__restrict__ msg, const uint8_t *__restrict__ visited) {
     griddep_launch_dependents();
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -76,12 +84,13 @@ __global__ void k_tree_wave(const uint32_t *__restrict__ nodes, uint32_t n, uint
     }
     for (uint32_t q = o0; q < o1; ++q) {
         const uint32_t w = out_dst[q];
-        const bool seen = visited[w] || (node_level[w] == level && node_lidx[w] <= my_idx);
+        const uint2 li = q_lvidx[q];
+        const bool seen = visited[w] || (li.x == level && li.y <= my_idx);
         if (seen) continue;
         const uint32_t p = out_pos[q];
-        const int y = UNI ? MS : node_s[w];
+        const int y = UNI ? MS : q_y[q];
         float m[MS];
-        send_msg<MS, UNI>(joint + (size_t)p * (MS * MS), buf, S, y, m);
+        send_msg_dense<MS, UNI>(q_joint + q_joff[q], buf, S, y, m);
         stv<MS>(msg + (size_t)p * MS, m);
     }
 }
@@ -97,8 +106,9 @@ template <int MS, bool UNI, int G>
 __global__ void k_tree_wave_group(const uint32_t *__restrict__ nodes, uint32_t n, uint32_t level,
                                   const uint32_t *__restrict__ in_ptr, const uint32_t *__restrict__ out_ptr,
                                   const uint32_t *__restrict__ out_pos, const uint32_t *__restrict__ out_dst,
-                                  const uint32_t *__restrict__ node_level, const uint32_t *__restrict__ node_lidx,
-                                  const uint8_t *__restrict__ node_s, const float *__restrict__ joint,
+                                  const uint2 *__restrict__ q_lvidx, const uint32_t *__restrict__ node_lidx,
+                                  const uint8_t *__restrict__ node_s, const uint8_t *__restrict__ q_y,
+                                  const uint32_t *__restrict__ q_joff, const float *__restrict__ q_joint,
                                   float *__restrict__ msg, const uint8_t *__restrict__ visited) {
     static_assert(G >= 2 && G <= 32 && (G & (G - 1)) == 0, "group of 2..32 lanes");
     const uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) / G;
@@ -107,24 +117,25 @@ __global__ void k_tree_wave_group(const uint32_t *__restrict__ nodes, uint32_t n
     griddep_launch_dependents();
     if (k >= n) return;   // the whole group
     // the schedule's arrays first (no tree kernel writes them): the node, its
-    // edge ranges, and this lane's first out-edge with its neighbour's level
-    // (and, for the latency-bound small waves, its table into L2); then the
-    // wait for the kernels ahead, whose messages and visited flags follow
+    // edge ranges, and this lane's first out-edge with its destination's
+    // level data and table (into L2 for the latency-bound small waves); then
+    // the wait for the kernels ahead, whose messages and visited flags follow
     const uint32_t u = nodes[k];
     const int S = UNI ? MS : node_s[u];
     const uint32_t my_idx = node_lidx[u];
     const uint32_t r0 = in_ptr[u], r1 = in_ptr[u + 1], o0 = out_ptr[u], o1 = out_ptr[u + 1];
     const uint32_t q0 = o0 + lane;
-    uint32_t w0 = 0, pp0 = 0, lv0 = 0, li0 = 0;
+    uint32_t w0 = 0, pp0 = 0, jo0 = 0;
+    uint2 li0 = make_uint2(0u, 0u);
     int y0 = MS;
     if (q0 < o1) {
         w0 = out_dst[q0];
         pp0 = out_pos[q0];
-        lv0 = node_level[w0];
-        li0 = node_lidx[w0];
-        if (!UNI) y0 = node_s[w0];
+        li0 = q_lvidx[q0];
+        jo0 = q_joff[q0];
+        if (!UNI) y0 = q_y[q0];
         if constexpr (G >= 16) {
-            const float *jt = joint + (size_t)pp0 * (MS * MS);
+            const float *jt = q_joint + jo0;
             prefetch_l2(jt);
             if constexpr (MS * MS > 32) prefetch_l2(jt + 32);
         }
@@ -149,14 +160,51 @@ __global__ void k_tree_wave_group(const uint32_t *__restrict__ nodes, uint32_t n
     for (uint32_t q = q0; q < o1; q += G) {
         const bool first = q == q0;
         const uint32_t w = first ? w0 : out_dst[q];
-        const uint32_t lv = first ? lv0 : node_level[w], li = first ? li0 : node_lidx[w];
-        const bool seen = visited[w] || (lv == level && li <= my_idx);
+        const uint2 li = first ? li0 : q_lvidx[q];
+        const bool seen = visited[w] || (li.x == level && li.y <= my_idx);
         if (seen) continue;
         const uint32_t p = first ? pp0 : out_pos[q];
-        const int y = UNI ? MS : (first ? y0 : (int)node_s[w]);
+        const int y = UNI ? MS : (first ? y0 : (int)q_y[q]);
         float m[MS];
-        send_msg<MS, UNI>(joint + (size_t)p * (MS * MS), buf, S, y, m);
+        send_msg_dense<MS, UNI>(q_joint + (first ? jo0 : q_joff[q]), buf, S, y, m);
         stv<MS>(msg + (size_t)p * MS, m);
+    }
+}
+
+// ---- the out-edge order arrays (TreeData::q_*) ---------------------------
+// per out-edge: the destination's state count and the padded table size
+__global__ void k_tq_sizes(uint32_t V, const uint32_t *__restrict__ out_ptr, const uint32_t *__restrict__ out_dst,
+                           const uint8_t *__restrict__ node_s, uint8_t *__restrict__ q_y, uint32_t *__restrict__ size) {
+    const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= V) return;
+    const uint32_t x = node_s[u];
+    for (uint32_t q = out_ptr[u]; q < out_ptr[u + 1]; ++q) {
+        const uint32_t y = node_s[out_dst[q]];
+        q_y[q] = (uint8_t)y;
+        size[q] = (x * y + 3u) & ~3u;
+    }
+}
+
+// the dense tables (rows of y floats, zero padding) and the destinations'
+// (level, index in level)
+template <int MS>
+__global__ void k_tq_fill(uint32_t V, const uint32_t *__restrict__ out_ptr, const uint32_t *__restrict__ out_pos,
+                          const uint32_t *__restrict__ out_dst, const uint8_t *__restrict__ node_s,
+                          const uint8_t *__restrict__ q_y, const uint32_t *__restrict__ q_joff,
+                          const float *__restrict__ joint, const uint32_t *__restrict__ node_level,
+                          const uint32_t *__restrict__ node_lidx, float *__restrict__ q_joint,
+                          uint2 *__restrict__ q_lvidx) {
+    const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= V) return;
+    const uint32_t x = node_s[u];
+    for (uint32_t q = out_ptr[u]; q < out_ptr[u + 1]; ++q) {
+        const uint32_t y = q_y[q], p = out_pos[q], w = out_dst[q];
+        float *dst = q_joint + q_joff[q];
+        const float *src = joint + (size_t)p * (MS * MS);
+        for (uint32_t i = 0; i < x; ++i)
+            for (uint32_t j = 0; j < y; ++j) dst[i * y + j] = src[i * MS + j];
+        for (uint32_t k = x * y; k < ((x * y + 3u) & ~3u); ++k) dst[k] = 0.0f;
+        q_lvidx[q] = make_uint2(node_level[w], node_lidx[w]);
     }
 }
 
@@ -193,6 +241,10 @@ __global__ void k_tree_marginalize(uint32_t V, const uint32_t *__restrict__ in_p
 void tree_clear(bp_graph *g) {
     TreeData &t = g->tree;
     if (t.exec) cudaGraphExecDestroy(t.exec);
+    if (t.q_joint) cudaFree(t.q_joint);
+    if (t.q_joff) cudaFree(t.q_joff);
+    if (t.q_lvidx) cudaFree(t.q_lvidx);
+    if (t.q_y) cudaFree(t.q_y);
     if (t.d_node_level) cudaFree(t.d_node_level);
     if (t.d_node_lidx) cudaFree(t.d_node_lidx);
     if (t.d_wave_nodes) cudaFree(t.d_wave_nodes);
@@ -246,6 +298,47 @@ int tree_prepare_host(bp_graph *g, const uint32_t *levels, uint32_t num_levels) 
     return BP_OK;
 }
 
+// the out-edge order arrays for the current levels (built once per level
+// lists, before any capture)
+template <int MS, bool UNI>
+static int tree_q_build(bp_graph *g) {
+    TreeData &t = g->tree;
+    if (t.q_joint) return BP_OK;
+    const uint32_t V = g->V, E = g->E;
+    int st;
+    if ((st = ensure_out_csr(g))) return st;
+    const size_t ne = E ? E : 1;
+    BP_CUDA(cudaMalloc((void **)&t.q_y, ne));
+    BP_CUDA(cudaMalloc((void **)&t.q_joff, sizeof(uint32_t) * (ne + 1)));
+    BP_CUDA(cudaMalloc((void **)&t.q_lvidx, sizeof(uint2) * ne));
+    uint32_t *size = nullptr;
+    BP_CUDA(cudaMallocAsync((void **)&size, sizeof(uint32_t) * (ne + 1), g->stream));
+    BP_CUDA(cudaMemsetAsync(size, 0, sizeof(uint32_t) * (ne + 1), g->stream));
+    if (V) k_tq_sizes<<<grid_for(V, 256), 256, 0, g->stream>>>(V, g->out_ptr, g->out_dst, g->node_s, t.q_y, size);
+    BP_CUDA(cudaGetLastError());
+    {
+        size_t temp = 0;
+        BP_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, temp, size, t.q_joff, (int64_t)E + 1, g->stream));
+        void *tmp = nullptr;
+        BP_CUDA(cudaMallocAsync(&tmp, temp, g->stream));
+        cudaError_t e = cub::DeviceScan::ExclusiveSum(tmp, temp, size, t.q_joff, (int64_t)E + 1, g->stream);
+        cudaFreeAsync(tmp, g->stream);
+        if (e != cudaSuccess) return cuda_fail(e, "DeviceScan::ExclusiveSum", __FILE__, __LINE__);
+    }
+    uint32_t total = 0;
+    BP_CUDA(cudaMemcpyAsync(&total, t.q_joff + E, sizeof(uint32_t), cudaMemcpyDeviceToHost, g->stream));
+    BP_CUDA(cudaStreamSynchronize(g->stream));
+    cudaFreeAsync(size, g->stream);
+    BP_CUDA(cudaMalloc((void **)&t.q_joint, sizeof(float) * ((size_t)total + 4)));
+    if (V)
+        k_tq_fill<MS><<<grid_for(V, 256), 256, 0, g->stream>>>(V, g->out_ptr, g->out_pos, g->out_dst, g->node_s,
+                                                               t.q_y, t.q_joff, g->joint, t.d_node_level,
+                                                               t.d_node_lidx, t.q_joint, t.q_lvidx);
+    BP_CUDA(cudaGetLastError());
+    BP_CUDA(cudaStreamSynchronize(g->stream));
+    return BP_OK;
+}
+
 template <int MS, bool UNI>
 static int launch_start(bp_graph *g) {
     TreeData &t = g->tree;
@@ -254,8 +347,8 @@ static int launch_start(bp_graph *g) {
     const uint32_t lo = t.wave_off[w0], hi = t.wave_off[w1];
     const uint32_t n = hi - lo;
     k_tree_start<MS, UNI><<<grid_for(n, 128), 128, 0, g->stream>>>(t.d_wave_nodes + lo, n, g->out_ptr, g->out_pos,
-                                                                    g->out_dst, g->node_s, g->joint, g->belief,
-                                                                    g->msg[0], g->visited);
+                                                                    g->node_s, t.q_y, t.q_joff, t.q_joint,
+                                                                    g->belief, g->msg[0], g->visited);
     BP_CUDA(cudaGetLastError());
     return BP_OK;
 }
@@ -315,9 +408,9 @@ static cudaError_t launch_wave_group(bp_graph *g, const uint32_t *nodes, uint32_
     TreeData &t = g->tree;
     return launch_wave(k_tree_wave_group<MS, UNI, G>, grid_for((uint64_t)n * G, 128), g->stream, nodes, n, level,
                        (const uint32_t *)g->in_ptr, (const uint32_t *)g->out_ptr, (const uint32_t *)g->out_pos,
-                       (const uint32_t *)g->out_dst, (const uint32_t *)t.d_node_level,
-                       (const uint32_t *)t.d_node_lidx, (const uint8_t *)g->node_s, (const float *)g->joint,
-                       g->msg[0], (const uint8_t *)g->visited);
+                       (const uint32_t *)g->out_dst, (const uint2 *)t.q_lvidx, (const uint32_t *)t.d_node_lidx,
+                       (const uint8_t *)g->node_s, (const uint8_t *)t.q_y, (const uint32_t *)t.q_joff,
+                       (const float *)t.q_joint, g->msg[0], (const uint8_t *)g->visited);
 }
 
 template <int MS, bool UNI>
@@ -338,9 +431,9 @@ static int launch_level(bp_graph *g, uint32_t level) {
         default:
             le = launch_wave(k_tree_wave<MS, UNI>, grid_for(n, 128), g->stream, nodes, n, level,
                              (const uint32_t *)g->in_ptr, (const uint32_t *)g->out_ptr, (const uint32_t *)g->out_pos,
-                             (const uint32_t *)g->out_dst, (const uint32_t *)t.d_node_level,
-                             (const uint32_t *)t.d_node_lidx, (const uint8_t *)g->node_s, (const float *)g->joint,
-                             g->msg[0], (const uint8_t *)g->visited);
+                             (const uint32_t *)g->out_dst, (const uint2 *)t.q_lvidx, (const uint32_t *)t.d_node_lidx,
+                             (const uint8_t *)g->node_s, (const uint8_t *)t.q_y, (const uint32_t *)t.q_joff,
+                             (const float *)t.q_joint, g->msg[0], (const uint8_t *)g->visited);
         }
         if (le != cudaSuccess) return cuda_fail(le, "cudaLaunchKernelEx", __FILE__, __LINE__);
         BP_CUDA(cudaGetLastError());
@@ -362,6 +455,7 @@ static int launch_marginalize(bp_graph *g) {
     return BP_OK;
 }
 
+static int dispatch_q_build(bp_graph *g) { BP_DISPATCH_MS(g->ms, g->uniform != 0, tree_q_build, g); }
 static int dispatch_start(bp_graph *g) { BP_DISPATCH_MS(g->ms, g->uniform != 0, launch_start, g); }
 static int dispatch_level(bp_graph *g, uint32_t l) { BP_DISPATCH_MS(g->ms, g->uniform != 0, launch_level, g, l); }
 static int dispatch_marginalize(bp_graph *g) { BP_DISPATCH_MS(g->ms, g->uniform != 0, launch_marginalize, g); }
@@ -405,7 +499,8 @@ int bp_tree_set_levels(bp_graph *g, const uint32_t *levels, uint32_t num_levels)
 int bp_tree_start(bp_graph *g) {
     if (!g) return set_error(BP_ERR_INVALID, "null graph");
     if (!g->tree.ready) return set_error(BP_ERR_STATE, "tree levels not set");
-    return dispatch_start(g);
+    int st = dispatch_q_build(g);
+    return st ? st : dispatch_start(g);
 }
 
 int bp_tree_level(bp_graph *g, uint32_t level) {
@@ -413,7 +508,8 @@ int bp_tree_level(bp_graph *g, uint32_t level) {
     if (!g->tree.ready) return set_error(BP_ERR_STATE, "tree levels not set");
     if (level >= g->tree.num_levels) return set_error(BP_ERR_INVALID, "level %u >= num_levels %u", level,
                                                       g->tree.num_levels);
-    return dispatch_level(g, level);
+    int st = dispatch_q_build(g);
+    return st ? st : dispatch_level(g, level);
 }
 
 int bp_tree_reset_visited(bp_graph *g) {
@@ -449,6 +545,7 @@ int bp_tree(bp_graph *g, bp_tree_result *res) {
         uint32_t nl = 0;
         if ((st = bp_tree_build_levels(g, nullptr, &nl))) return st;
     }
+    if ((st = dispatch_q_build(g))) return st;
     TreeData &t = g->tree;
     const uint32_t L = t.num_levels;
     uint32_t waves = t.level_wave_begin[1] - t.level_wave_begin[0] ? 1 : 0;
