@@ -51,7 +51,8 @@ template <int MS> constexpr int flood_unroll() { return MS <= 2 ? 1 : (MS <= 4 ?
 template <int MS, int FU> constexpr int flood_min_blocks() { return MS <= 2 ? (FU >= 4 ? 8 : 12) : 1; }
 
 struct FloodArgs {
-    uint32_t V;
+    uint32_t V;          // tiles cover nodes [v_base, V)
+    uint32_t v_base;     // first node of tile 0 (a node range of a sharded run; else 0)
     // send-buffer entries of nodes below this id are gathered and written
     // with an L2 evict-last policy (renumbered graphs: the nodes with the
     // most out-edges, i.e. the most re-read entries); 0 = none
@@ -561,7 +562,7 @@ __device__ __forceinline__ void flood_tile(const FloodArgs &a, uint32_t tile, bo
                                            float *sm, double &dsum) {
     constexpr int NT = flood_nt<MS>();
     constexpr uint32_t EMAX = flood_smem_floats<MS>() / MS;
-    const uint32_t V = a.V, tid = threadIdx.x, v0 = tile * NT;
+    const uint32_t V = a.V, tid = threadIdx.x, v0 = a.v_base + tile * NT;
     const uint32_t vend = min(v0 + NT, V);
     const uint32_t e0 = a.in_ptr[v0], e1 = a.in_ptr[vend];
     const uint32_t v = v0 + tid;
@@ -1453,6 +1454,39 @@ __global__ void __launch_bounds__(256) k_flood_w(const FloodArgs a) {
     else reduce_and_finalize<NT>(ctl, a.partials, dsum, want, red, &s_last);
 }
 
+// One iteration for the destination nodes [a.v_base, a.V) only: a rank of a
+// sharded run (one process per GPU, each owning a node range) computes its
+// nodes' incoming messages from the full send buffers q_in, their beliefs
+// and their next send buffers in q_out; the ranks then exchange q_out.  The
+// per-tile work is k_flood's (flood_tile); the |diff| terms of the range are
+// summed per block into `partials` and, by k_sum_partials, in a fixed order.
+template <int MS, bool UNI, int FU>
+__global__ void __launch_bounds__(flood_nt<MS>()) k_flood_range(const FloodArgs a, uint32_t ntiles,
+                                                                const float *__restrict__ m_old,
+                                                                float *__restrict__ m_new,
+                                                                const float *__restrict__ q_in,
+                                                                float *__restrict__ q_out, double *partials) {
+    constexpr int NT = flood_nt<MS>();
+    constexpr uint32_t EMAX = flood_smem_floats<MS>() / MS;
+    __shared__ __align__(16) float sm[EMAX * MS];
+    __shared__ double red[NT / 32];
+    double dsum = 0.0;
+    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        flood_tile<MS, UNI, FU>(a, tile, true, nullptr, m_old, m_new, q_in, q_out, 0, sm, dsum);
+        __syncthreads();
+    }
+    const double t = block_sum<NT>(dsum, red);
+    if (threadIdx.x == 0) partials[blockIdx.x] = t;
+}
+
+__global__ void k_sum_partials(const double *__restrict__ partials, uint32_t n, double *__restrict__ out) {
+    __shared__ double red[8];
+    double acc = 0.0;
+    for (uint32_t k = threadIdx.x; k < n; k += 256) acc += partials[k];
+    const double t = block_sum<256>(acc, red);
+    if (threadIdx.x == 0) *out = t;
+}
+
 // prologue: Q_1 = b * prod of the latest messages (read_incoming_messages,
 // graph.c:860-882, on the messages init_previous_edge left)
 template <int MS, bool UNI>
@@ -1806,6 +1840,7 @@ static uint32_t flood_hot_nodes(const bp_graph *g) {
 static FloodArgs flood_args(bp_graph *g) {
     FloodArgs a;
     a.V = g->V;
+    a.v_base = 0;
     a.hot = flood_hot_nodes(g);
     {
         // default 1: on the 16M-node graph 0.974 -> 0.932 ms per iteration
@@ -2266,11 +2301,77 @@ static int launch_fused(bp_graph *g, unsigned grid, uint32_t ntiles, bool serial
     return BP_OK;
 }
 
+// ---- one rank's node range of a sharded run ----------------------------
+
+template <int MS, bool UNI>
+static int launch_gather_range(bp_graph *g, uint32_t v0, uint32_t v1, float *q_out, cudaStream_t st) {
+    if (v1 > v0)
+        k_gather_q<MS, UNI><<<grid_for(v1 - v0, 256), 256, 0, st>>>(v1 - v0, g->in_ptr + v0, g->node_s + v0,
+                                                                    g->belief + (size_t)v0 * MS, g->msg[g->latest],
+                                                                    q_out + (size_t)v0 * MS);
+    BP_CUDA(cudaGetLastError());
+    return BP_OK;
+}
+
+template <int MS, bool UNI>
+static int launch_flood_range(bp_graph *g, uint32_t v0, uint32_t v1, const float *q_in, float *q_out,
+                              double *delta, cudaStream_t st) {
+    constexpr int NT = flood_nt<MS>();
+    constexpr int FU = flood_unroll<MS>();
+    static int bps = 0;
+    if (!bps) BP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_flood_range<MS, UNI, FU>, NT, 0));
+    int dev = 0, sms = 0;
+    BP_CUDA(cudaGetDevice(&dev));
+    BP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const uint32_t ntiles = (v1 - v0 + NT - 1) / NT;
+    const uint32_t grid = std::min<uint32_t>(ntiles, (uint32_t)std::max(1, bps * sms));
+    int rc;
+    if ((rc = ensure_partials(g, std::max(grid, 1u)))) return rc;
+    FloodArgs a = flood_args(g);
+    a.V = v1;
+    a.v_base = v0;
+    a.hot = 0;
+    if (ntiles)
+        k_flood_range<MS, UNI, FU><<<grid, NT, 0, st>>>(a, ntiles, g->msg[g->latest], g->msg[g->latest ^ 1], q_in,
+                                                        q_out, g->partials);
+    k_sum_partials<<<1, 256, 0, st>>>(g->partials, ntiles ? grid : 0u, delta);
+    BP_CUDA(cudaGetLastError());
+    g->latest ^= 1;
+    return BP_OK;
+}
+
+static int range_check(const bp_graph *g, uint32_t v0, uint32_t v1) {
+    if (!g) return set_error(BP_ERR_INVALID, "null graph");
+    if (v0 > v1 || v1 > g->V) return set_error(BP_ERR_INVALID, "node range [%u, %u) not inside [0, %u)", v0, v1, g->V);
+    if (g->new_to_old)
+        return set_error(BP_ERR_STATE, "node ranges of a renumbered graph (BP_GRAPH_REORDER_BY_OUT_DEGREE)");
+    return BP_OK;
+}
+
 }  // namespace bpx
 
 using namespace bpx;
 
 extern "C" {
+
+int bp_send_buffers_range(bp_graph *g, uint32_t node_begin, uint32_t node_end, float *q_out, void *stream) {
+    int st = range_check(g, node_begin, node_end);
+    if (st) return st;
+    if (!q_out) return set_error(BP_ERR_INVALID, "null send buffers");
+    cudaStream_t s = stream ? (cudaStream_t)stream : g->stream;
+    BP_DISPATCH_MS(g->ms, g->uniform != 0, launch_gather_range, g, node_begin, node_end, q_out, s);
+}
+
+int bp_flood_range(bp_graph *g, uint32_t node_begin, uint32_t node_end, const float *q_in, float *q_out,
+                   double *delta, void *stream) {
+    NvtxRange nvtx("bp_flood_range");
+    int st = range_check(g, node_begin, node_end);
+    if (st) return st;
+    if (!q_in || !q_out || !delta) return set_error(BP_ERR_INVALID, "null argument");
+    if (q_in == q_out) return set_error(BP_ERR_INVALID, "q_in and q_out must be different buffers");
+    cudaStream_t s = stream ? (cudaStream_t)stream : g->stream;
+    BP_DISPATCH_MS(g->ms, g->uniform != 0, launch_flood_range, g, node_begin, node_end, q_in, q_out, delta, s);
+}
 
 void bp_loopy_default_options(bp_loopy_options *o) {
     if (!o) return;

@@ -190,6 +190,29 @@ int bp_serial_sum_f32(const float *x, uint64_t n, float *out, int method, void *
  * too large for the running bound). */
 int bp_serial_sum_bounds(const float *x, uint64_t n, double *lohi, void *stream);
 
+/* ---- one rank of a sharded loopy run --------------------------------- */
+/* SURVEY's multi-GPU split of the node schedule (no counterpart in the
+ * reference, which runs on one device): each rank (one process per GPU)
+ * owns the destination nodes [node_begin, node_end) and holds their
+ * in-edges (a bp_graph of all V nodes whose edges are those in-edges, built
+ * from the full edge list filtered by destination, in edge order), every
+ * node's beliefs, and two DEVICE send-buffer arrays of [V][max states]
+ * floats.  Per iteration of loopy_propagate_until (graph.c:1278-1324):
+ *   bp_flood_range reads every node's send buffer from q_in, writes the
+ *     owned nodes' messages (into the slot after the latest one, which then
+ *     becomes the latest), beliefs and next send buffers (q_out[node_begin,
+ *     node_end)), and the f64 sum of the owned in-edges' |diff| terms to the
+ *     DEVICE double *delta;
+ *   the ranks then all-gather q_out and sum the deltas (every rank the same
+ *     sum, in rank order) for the reference's stopping rule.
+ * bp_send_buffers_range writes the first send buffers (read_incoming_messages,
+ * graph.c:850-882, after init_previous_edge) of the owned nodes.  Results
+ * are the single-GPU node schedule's bit for bit.  stream NULL = the graph's
+ * stream.  Renumbered graphs return BP_ERR_STATE. */
+int bp_send_buffers_range(bp_graph *g, uint32_t node_begin, uint32_t node_end, float *q_out, void *stream);
+int bp_flood_range(bp_graph *g, uint32_t node_begin, uint32_t node_end, const float *q_in, float *q_out,
+                   double *delta, void *stream);
+
 /* ---- loopy BP without allocating ------------------------------------- */
 /* No counterpart in the reference: an addition of this library.
  *
