@@ -2002,13 +2002,16 @@ static uint32_t split_range_nodes(const bp_graph *g) {
     return (uint32_t)std::min<uint64_t>(std::max(rn, min_rn), 0xffffffffu);
 }
 
-// BP_FLOOD_SPLIT=0 never, =1 whenever the layout fits; default: when the
-// send buffers exceed BP_FLOOD_SPLIT_MIN_MB (default 64) MB, i.e. when they
-// no longer stay in L2 across an iteration
+// BP_FLOOD_SPLIT=1: whenever the layout fits; =auto: when the send buffers
+// exceed BP_FLOOD_SPLIT_MIN_MB (default 64) MB, i.e. when they no longer stay
+// in L2 across an iteration; default (or 0): never.  On the 16.8M-node graph
+// the split schedule moves 3.7 GB per iteration against k_flood's 4.8 GB,
+// but its two kernels run at 3.9 and 2.5 TB/s (1.11 ms against 0.87 ms), so
+// the default loop keeps k_flood.
 static bool split_wanted(const bp_graph *g) {
     const char *env = getenv("BP_FLOOD_SPLIT");
-    if (env && env[0] == '0') return false;
-    if (env && env[0] == '1') return true;
+    if (!env || env[0] == '0') return false;
+    if (env[0] == '1') return true;
     size_t mb = 64;
     if (const char *e2 = getenv("BP_FLOOD_SPLIT_MIN_MB")) mb = (size_t)atol(e2);
     return (uint64_t)g->V * g->ms * sizeof(float) > ((uint64_t)mb << 20);
