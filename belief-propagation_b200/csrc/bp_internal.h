@@ -142,6 +142,7 @@ struct bp_graph {
         uint32_t R = 0;                  // source ranges
         uint32_t range_nodes = 0;
         uint32_t ntiles = 0;             // node tiles of the node pass
+        uint32_t tile_nodes = 0;         // nodes per node tile
         uint32_t *s_src = nullptr;       // [E] source node (send order)
         uint32_t *s_edge = nullptr;      // [E] edge id (serial delta terms)
         uint32_t *s_pos = nullptr;       // [E] position of send index k

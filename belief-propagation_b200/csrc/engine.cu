@@ -484,6 +484,7 @@ int split_build(bp_graph *g, uint32_t tn, uint32_t te, uint32_t range_nodes) {
     s.R = R;
     s.range_nodes = range_nodes;
     s.ntiles = ntiles;
+    s.tile_nodes = tn;
     int st;
     const size_t nseg = (size_t)R * ntiles + 1;
     if ((st = dev_alloc(g, (void **)&s.s_src, sizeof(uint32_t) * ((size_t)E + kArrayPadEdges)))) return st;

@@ -47,14 +47,14 @@ struct SplitArgs {
     LoopyCtl *ctl;
 };
 
-// send pass: CH edges per chunk, three stages of (source ids, tables, old
-// messages) per CTA, under 29 KB each
-template <int MS>
-struct SendCfg {
-    static constexpr uint32_t NT = 256;
-    static constexpr uint32_t CH = MS == 1 ? 2048 : (MS == 2 ? 1024 : (MS == 3 ? 512 : 256));
+// send pass: CH edges per chunk, ST stages of (source ids, tables, old
+// messages) per CTA of NT threads
+template <int MS, uint32_t CH_, int ST_, uint32_t NT_>
+struct SendCfgT {
+    static constexpr uint32_t NT = NT_;
+    static constexpr uint32_t CH = CH_;
     static constexpr uint32_t U = CH / NT;   // edges per thread per chunk
-    static constexpr int ST = 3;
+    static constexpr int ST = ST_;
     static constexpr uint32_t SRC = 0;
     static constexpr uint32_t JNT = SRC + CH * 4;
     static constexpr uint32_t MOLD = JNT + CH * MS * MS * 4;
@@ -64,12 +64,17 @@ struct SendCfg {
     static_assert(MS >= 1 && MS <= 4, "split schedule: 1 to 4 states");
     static_assert(CH % NT == 0 && (CH * 4) % 16 == 0, "whole rounds, 16-byte aligned sections");
 };
-
-// node pass: 128-node tiles holding at most EB in-edges
+// the default shape: stages under 29 KB, three of them
 template <int MS>
+using SendCfg = SendCfgT<MS, (MS == 1 ? 2048u : (MS == 2 ? 1024u : (MS == 3 ? 512u : 256u))), 3, 256u>;
+
+// node pass: tiles of NT nodes holding at most EB in-edges (8 in-edges per
+// node on average with 1-2 states, 16 with 3-4: a tile's messages take 8 or
+// 32 KB of shared memory per 128 nodes)
+template <int MS, uint32_t NT_ = 128>
 struct NodeCfg {
-    static constexpr uint32_t NT = 128;
-    static constexpr uint32_t EB = (MS <= 2 ? 4096u : 8192u) / MS;
+    static constexpr uint32_t NT = NT_;
+    static constexpr uint32_t EB = (MS <= 2 ? 2048u : 8192u) / MS * (NT_ / 128u);
     static constexpr uint32_t RMAX = 32;   // source ranges at most
 };
 
@@ -93,10 +98,9 @@ __device__ __forceinline__ void bulk_g2s_hint(void *dst, const void *src, uint32
 // CH, so every source address is 16-byte aligned; lengths are rounded up to
 // 16 bytes and the send-order arrays carry padding past their ends.  The
 // mbarrier expects exactly the bytes issued.
-template <int MS>
+template <int MS, typename C>
 __device__ void send_issue(const SplitArgs &a, const float *m_old, bool want, uint32_t c, unsigned char *st,
                            uint64_t *bar, uint64_t pol) {
-    using C = SendCfg<MS>;
     const uint32_t k0 = c * C::CH, n = min(C::CH, a.E - k0);
     const uint32_t b_src = round16(n * 4), b_j = round16(n * MS * MS * 4), b_m = want ? round16(n * MS * 4) : 0u;
     mbar_arrive_expect_tx(bar, b_src + b_j + b_m);
@@ -105,9 +109,24 @@ __device__ void send_issue(const SplitArgs &a, const float *m_old, bool want, ui
     if (b_m) bulk_g2s_hint(st + C::MOLD, m_old + (size_t)k0 * MS, b_m, bar, pol);
 }
 
-template <int MS, bool SER>
-__global__ void __launch_bounds__(256) k_flood_send(const SplitArgs a) {
-    using C = SendCfg<MS>;
+// the gathers Q_t[src] of chunk c's edges (thread's U edges) into registers
+template <int MS, typename C>
+__device__ __forceinline__ void send_gather(const SplitArgs &a, const unsigned char *st, uint32_t c,
+                                            const float *__restrict__ q_in, float (*q)[MS]) {
+    const uint32_t k0 = c * C::CH, n = min(C::CH, a.E - k0);
+    const uint32_t *src_s = reinterpret_cast<const uint32_t *>(st + C::SRC);
+#pragma unroll
+    for (uint32_t u = 0; u < C::U; ++u) {
+        const uint32_t j = threadIdx.x + u * C::NT;
+        if (j < n) ldv<MS>(q_in + (size_t)src_s[j] * MS, q[u]);
+    }
+}
+
+// The chunks of a CTA form a pipeline: chunk i+ST-1's bulk copies are in
+// flight, chunk i+1's gathers are in flight (issued from its landed source
+// ids), and chunk i is computed from its stage and its gathered values.
+template <int MS, bool SER, typename C>
+__global__ void __launch_bounds__(C::NT) k_flood_send(const SplitArgs a) {
     constexpr uint32_t NT = C::NT;
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ double red[NT / 32];
@@ -132,32 +151,44 @@ __global__ void __launch_bounds__(256) k_flood_send(const SplitArgs a) {
         fence_mbar_init();
         for (int i = 0; i < C::ST; ++i) {
             const uint32_t c = blockIdx.x + (uint32_t)i * gridDim.x;
-            if (c < a.nchunks) send_issue<MS>(a, m_old, want, c, smem + i * C::STAGE, bars + i, pol);
+            if (c < a.nchunks) send_issue<MS, C>(a, m_old, want, c, smem + i * C::STAGE, bars + i, pol);
         }
     }
     __syncthreads();
 
-    double dsum = 0.0;
-    uint32_t i = 0;
-    for (uint32_t c = blockIdx.x; c < a.nchunks; c += gridDim.x, ++i) {
+    // stage of chunk number i of this CTA landed: every thread may read it
+    auto wait_stage = [&](uint32_t i) -> bool {
         const int si = (int)(i % C::ST);
         const uint32_t par = (i / C::ST) & 1u;
-        unsigned char *st = smem + si * C::STAGE;
         if (tid == 0 && !mbar_wait_bounded(bars + si, par, kWaitNs)) s_err = 1;
         __syncthreads();
-        if (s_err) break;
+        if (s_err) return false;
         mbar_try_wait(bars + si, par);   // completed: orders this thread's reads after the copies
+        return true;
+    };
+
+    double dsum = 0.0;
+    float q[C::U][MS], qn[C::U][MS];
+    uint32_t i = 0;
+    bool ok = blockIdx.x >= a.nchunks || wait_stage(0);
+    if (ok && blockIdx.x < a.nchunks) send_gather<MS, C>(a, smem, blockIdx.x, q_in, qn);
+    for (uint32_t c = blockIdx.x; ok && c < a.nchunks; c += gridDim.x, ++i) {
+#pragma unroll
+        for (uint32_t u = 0; u < C::U; ++u)
+#pragma unroll
+            for (int s = 0; s < MS; ++s) q[u][s] = qn[u][s];
+        const uint32_t cn = c + gridDim.x;
+        if (cn < a.nchunks) {
+            if (!wait_stage(i + 1)) {
+                ok = false;
+                break;
+            }
+            send_gather<MS, C>(a, smem + ((i + 1) % C::ST) * C::STAGE, cn, q_in, qn);
+        }
+        unsigned char *st = smem + (i % C::ST) * C::STAGE;
         const uint32_t k0 = c * C::CH, n = min(C::CH, a.E - k0);
-        const uint32_t *src_s = reinterpret_cast<const uint32_t *>(st + C::SRC);
         const float *j_s = reinterpret_cast<const float *>(st + C::JNT);
         const float *mo_s = reinterpret_cast<const float *>(st + C::MOLD);
-        // every gather of the chunk in flight before the first use
-        float q[C::U][MS];
-#pragma unroll
-        for (uint32_t u = 0; u < C::U; ++u) {
-            const uint32_t j = tid + u * NT;
-            if (j < n) ldv<MS>(q_in + (size_t)src_s[j] * MS, q[u]);
-        }
 #pragma unroll
         for (uint32_t u = 0; u < C::U; ++u) {
             const uint32_t j = tid + u * NT;
@@ -186,11 +217,11 @@ __global__ void __launch_bounds__(256) k_flood_send(const SplitArgs a) {
         __syncthreads();
         if (tid == 0) {
             const uint32_t nc = c + (uint32_t)C::ST * gridDim.x;
-            if (nc < a.nchunks) send_issue<MS>(a, m_old, want, nc, st, bars + si, pol);
+            if (nc < a.nchunks) send_issue<MS, C>(a, m_old, want, nc, st, bars + (i % C::ST), pol);
         }
     }
 
-    if (s_err) {
+    if (!ok) {
         // a stage never completed: report it, wait (bounded) for the copies
         // still in flight into this CTA's stages, and leave
         if (tid == 0) {
@@ -233,10 +264,10 @@ __device__ __forceinline__ void split_finalize(const SplitArgs &a, bool want, do
     }
 }
 
-template <int MS, bool SER>
-__global__ void __launch_bounds__(128) k_flood_nodes(const SplitArgs a) {
-    using C = NodeCfg<MS>;
+template <int MS, bool SER, typename C>
+__global__ void __launch_bounds__(C::NT) k_flood_nodes(const SplitArgs a) {
     constexpr uint32_t NT = C::NT;
+    constexpr uint32_t UB = 4;   // messages per thread in flight while they go to shared memory
     __shared__ __align__(16) float sm[C::EB * MS];
     __shared__ uint32_t s_beg[C::RMAX], s_pre[C::RMAX + 1];
     __shared__ double red[NT / 32];
@@ -275,16 +306,25 @@ __global__ void __launch_bounds__(128) k_flood_nodes(const SplitArgs a) {
         }
         __syncthreads();
         const uint32_t total = s_pre[R];
-        // messages back to position order in shared memory
-#pragma unroll 4
-        for (uint32_t j = tid; j < total; j += NT) {
-            uint32_t r = 0;
-            while (j >= s_pre[r + 1]) ++r;
-            const size_t k = (size_t)s_beg[r] + (j - s_pre[r]);
-            float m[MS];
-            ldv<MS, kStream>(m_new + k * MS, m);
-            const uint32_t o = __ldcs(a.s_off + k);
-            stv<MS>(sm + (size_t)o * MS, m);
+        // messages back to position order in shared memory: UB of them
+        // per thread loaded before the first is stored
+        for (uint32_t j0 = tid; j0 < total; j0 += NT * UB) {
+            float m[UB][MS];
+            uint32_t o[UB];
+#pragma unroll
+            for (uint32_t u = 0; u < UB; ++u) {
+                const uint32_t j = j0 + u * NT;
+                if (j < total) {
+                    uint32_t r = 0;
+                    while (j >= s_pre[r + 1]) ++r;
+                    const size_t k = (size_t)s_beg[r] + (j - s_pre[r]);
+                    ldv<MS, kStream>(m_new + k * MS, m[u]);
+                    o[u] = __ldcs(a.s_off + k);
+                }
+            }
+#pragma unroll
+            for (uint32_t u = 0; u < UB; ++u)
+                if (j0 + u * NT < total) stv<MS>(sm + (size_t)o[u] * MS, m[u]);
         }
         __syncthreads();
         // marginalise (graph.c:1003-1023), then the next send buffer

@@ -2017,8 +2017,18 @@ static bool split_wanted(const bp_graph *g) {
     return (uint64_t)g->V * g->ms * sizeof(float) > ((uint64_t)mb << 20);
 }
 
+// node-pass tiles: BP_SPLIT_NODE_NT=256 builds 256-node tiles (1-2 states),
+// else 128; fixed when the layout is built
+static uint32_t split_tile_nodes(const bp_graph *g) {
+    const char *env = getenv("BP_SPLIT_NODE_NT");
+    return (g->ms <= 2 && env && atoi(env) == 256) ? 256u : 128u;
+}
+
 template <int MS>
 static int split_prepare_ms(bp_graph *g) {
+    if (split_tile_nodes(g) == 256) {
+        if constexpr (MS <= 2) return split_build(g, 256, NodeCfg<MS, 256>::EB, split_range_nodes(g));
+    }
     return split_build(g, NodeCfg<MS>::NT, NodeCfg<MS>::EB, split_range_nodes(g));
 }
 
@@ -2039,36 +2049,26 @@ int flood_split_prepare(bp_graph *g) {
     return split_prepare(g);
 }
 
-template <int MS, bool SER>
-static int split_grid(unsigned *grid_a, unsigned *grid_b) {
-    static int bps_a = 0, bps_b = 0;
-    static std::mutex mu;
-    {
-        std::lock_guard<std::mutex> lock(mu);
-        if (bps_a == 0) {
-            BP_CUDA(cudaFuncSetAttribute(k_flood_send<MS, SER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         SendCfg<MS>::SMEM));
-            BP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps_a, k_flood_send<MS, SER>, SendCfg<MS>::NT,
-                                                                  SendCfg<MS>::SMEM));
-            BP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps_b, k_flood_nodes<MS, SER>, NodeCfg<MS>::NT, 0));
-            if (bps_a < 1 || bps_b < 1) return set_error(BP_ERR_CUDA, "split iteration kernels do not fit an SM");
-        }
-    }
-    int dev = 0, sms = 0;
-    BP_CUDA(cudaGetDevice(&dev));
-    BP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    *grid_a = (unsigned)(bps_a * sms);
-    *grid_b = (unsigned)(bps_b * sms);
-    return BP_OK;
+// send-pass shapes of 2-state graphs, BP_SPLIT_SEND=0..3 (sweeps; every
+// shape gives the same results): 0 = 1024-edge chunks x 3 stages, 256
+// threads; 1 = 512 x 3, 256; 2 = 1024 x 4, 512; 3 = 2048 x 3, 512
+template <int MS, int SV> struct SendShape { using C = SendCfg<MS>; };
+template <> struct SendShape<2, 1> { using C = SendCfgT<2, 512u, 3, 256u>; };
+template <> struct SendShape<2, 2> { using C = SendCfgT<2, 1024u, 4, 512u>; };
+template <> struct SendShape<2, 3> { using C = SendCfgT<2, 2048u, 3, 512u>; };
+
+static int split_send_shape(const bp_graph *g) {
+    const char *env = getenv("BP_SPLIT_SEND");
+    const int v = env ? atoi(env) : 0;
+    return (g->ms == 2 && v >= 0 && v <= 3) ? v : 0;
 }
 
-template <int MS>
-static SplitArgs split_args(bp_graph *g, unsigned grid_a) {
+static SplitArgs split_args(bp_graph *g, uint32_t ch, unsigned grid_a) {
     SplitArgs a;
     const auto &s = g->split;
     a.V = g->V;
     a.E = g->E;
-    a.nchunks = (g->E + SendCfg<MS>::CH - 1) / SendCfg<MS>::CH;
+    a.nchunks = (g->E + ch - 1) / ch;
     a.ntiles = s.ntiles;
     a.R = s.R;
     a.nparts = std::min<unsigned>(grid_a, a.nchunks);
@@ -2089,28 +2089,63 @@ static SplitArgs split_args(bp_graph *g, unsigned grid_a) {
     return a;
 }
 
+// k launches of (send pass, node pass) with shapes SC / NC, or (k == 0) the
+// send pass's block count only (the delta partials it writes)
+template <int MS, bool SER, typename SC, typename NC>
+static int split_run(bp_graph *g, uint32_t k, uint32_t *nparts) {
+    static int bps_a = 0, bps_b = 0;
+    static std::mutex mu;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (bps_a == 0) {
+            BP_CUDA(cudaFuncSetAttribute(k_flood_send<MS, SER, SC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         SC::SMEM));
+            BP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps_a, k_flood_send<MS, SER, SC>, SC::NT, SC::SMEM));
+            BP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps_b, k_flood_nodes<MS, SER, NC>, NC::NT, 0));
+            if (bps_a < 1 || bps_b < 1) return set_error(BP_ERR_CUDA, "split iteration kernels do not fit an SM");
+        }
+    }
+    int dev = 0, sms = 0;
+    BP_CUDA(cudaGetDevice(&dev));
+    BP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const SplitArgs a = split_args(g, SC::CH, (unsigned)(bps_a * sms));
+    if (nparts) *nparts = a.nparts;
+    const unsigned ga = a.nparts, gb = std::min<unsigned>((unsigned)(bps_b * sms), a.ntiles);
+    for (uint32_t i = 0; i < k; ++i) {
+        k_flood_send<MS, SER, SC><<<ga, SC::NT, SC::SMEM, g->stream>>>(a);
+        k_flood_nodes<MS, SER, NC><<<gb, NC::NT, 0, g->stream>>>(a);
+        BP_CUDA(cudaGetLastError());
+    }
+    return BP_OK;
+}
+
+template <int MS, bool SER, typename NC>
+static int split_dispatch_send(bp_graph *g, uint32_t k, uint32_t *nparts) {
+    if constexpr (MS == 2 && !SER) {
+        switch (split_send_shape(g)) {
+        case 1: return split_run<MS, SER, SendShape<2, 1>::C, NC>(g, k, nparts);
+        case 2: return split_run<MS, SER, SendShape<2, 2>::C, NC>(g, k, nparts);
+        case 3: return split_run<MS, SER, SendShape<2, 3>::C, NC>(g, k, nparts);
+        default: break;
+        }
+    }
+    return split_run<MS, SER, SendCfg<MS>, NC>(g, k, nparts);
+}
+
+template <int MS, bool SER>
+static int split_dispatch(bp_graph *g, uint32_t k, uint32_t *nparts) {
+    if constexpr (MS <= 2) {
+        if (g->split.tile_nodes == 256) return split_dispatch_send<MS, SER, NodeCfg<MS, 256>>(g, k, nparts);
+    }
+    return split_dispatch_send<MS, SER, NodeCfg<MS>>(g, k, nparts);
+}
+
 template <int MS, bool UNI>
 static int enqueue_split_iterations(bp_graph *g, uint32_t k, bool serial) {
     if constexpr (!UNI || MS > 4) {
         return set_error(BP_ERR_INVALID, "split schedule: uniform graphs of at most 4 states");
     } else {
-        unsigned ga = 0, gb = 0;
-        int st = serial ? split_grid<MS, true>(&ga, &gb) : split_grid<MS, false>(&ga, &gb);
-        if (st) return st;
-        const SplitArgs a = split_args<MS>(g, ga);
-        ga = a.nparts;
-        gb = std::min<unsigned>(gb, a.ntiles);
-        for (uint32_t i = 0; i < k; ++i) {
-            if (serial) {
-                k_flood_send<MS, true><<<ga, SendCfg<MS>::NT, SendCfg<MS>::SMEM, g->stream>>>(a);
-                k_flood_nodes<MS, true><<<gb, NodeCfg<MS>::NT, 0, g->stream>>>(a);
-            } else {
-                k_flood_send<MS, false><<<ga, SendCfg<MS>::NT, SendCfg<MS>::SMEM, g->stream>>>(a);
-                k_flood_nodes<MS, false><<<gb, NodeCfg<MS>::NT, 0, g->stream>>>(a);
-            }
-            BP_CUDA(cudaGetLastError());
-        }
-        return BP_OK;
+        return serial ? split_dispatch<MS, true>(g, k, nullptr) : split_dispatch<MS, false>(g, k, nullptr);
     }
 }
 
@@ -2120,11 +2155,7 @@ static int split_send_blocks(bp_graph *g, bool serial, uint32_t *n) {
     if constexpr (!UNI || MS > 4) {
         return set_error(BP_ERR_INVALID, "split schedule: uniform graphs of at most 4 states");
     } else {
-        unsigned ga = 0, gb = 0;
-        int st = serial ? split_grid<MS, true>(&ga, &gb) : split_grid<MS, false>(&ga, &gb);
-        if (st) return st;
-        *n = split_args<MS>(g, ga).nparts;
-        return BP_OK;
+        return serial ? split_dispatch<MS, true>(g, 0, n) : split_dispatch<MS, false>(g, 0, n);
     }
 }
 

@@ -323,6 +323,21 @@ def test_loopy_split_schedule_parity(bp, synth, restatement, O, monkeypatch, cas
             np.testing.assert_array_equal(f64[k], blk[k])
 
 
+@pytest.mark.parametrize("send_shape", ["0", "1", "2", "3"])
+@pytest.mark.parametrize("node_tile", ["128", "256"])
+def test_loopy_split_schedule_shapes(bp, synth, restatement, O, monkeypatch, send_shape, node_tile):
+    """Every send-pass shape (chunk, stages, threads) and node-tile size of
+    the split schedule gives the oracle's results on a 2-state power-law
+    graph with a ragged last chunk and many ranges."""
+    monkeypatch.setenv("BP_FLOOD_SPLIT", "1")
+    monkeypatch.setenv("BP_FLOOD_RANGE_MB", "0")
+    monkeypatch.setenv("BP_SPLIT_SEND", send_shape)
+    monkeypatch.setenv("BP_SPLIT_NODE_NT", node_tile)
+    net = synth.power_law_loopy(20_011, 80_021, 2, 0.1, seed=13)
+    ora = restatement.loopy(O.OracleGraph(net), 0.0, 12)
+    assert_same(gpu_loopy(bp, net, 0.0, 12, reorder=True, kernel="split", delta="f64"), ora, 2, deltas=False)
+
+
 def test_loopy_split_schedule_power_law_serial_delta(bp, synth, restatement, O, monkeypatch):
     """A power-law graph through the split schedule with four source ranges
     and the reference's serial delta at a tolerance it converges under."""
