@@ -238,10 +238,12 @@ __global__ void __launch_bounds__(kUThreads) k_u_iter(const UGraph g, const floa
 }
 
 // this block's sum of the per-thread table-adjoint accumulators (fixed
-// order), added to its running partial row (S*S doubles)
+// order), added to its running partial row (S*S doubles); with `scale`, each
+// entry k is multiplied by scale[k] first (the one-table adjoint accumulates
+// ci (x) e and takes the table's factor J once per block)
 template <int S, int NT, bool REG>
 __device__ __forceinline__ void block_partial_add(const float *acc, const float *sacc, float (*wred)[REG ? S * S : 1],
-                                                  double *__restrict__ row) {
+                                                  double *__restrict__ row, const float *scale = nullptr) {
     if constexpr (REG) {
         const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
@@ -255,15 +257,41 @@ __device__ __forceinline__ void block_partial_add(const float *acc, const float 
         for (int k = threadIdx.x; k < S * S; k += blockDim.x) {
             double t = 0.0;
             for (int ww = 0; ww < NT / 32; ++ww) t += (double)wred[ww][k];
-            row[k] += t;
+            row[k] += scale ? (double)scale[k] * t : t;
         }
     } else {
         __syncthreads();
         for (int k = threadIdx.x; k < S * S; k += blockDim.x) {
             double t = 0.0;
             for (int tt = 0; tt < NT; ++tt) t += (double)sacc[k * NT + tt];
-            row[k] += t;
+            row[k] += scale ? (double)scale[k] * t : t;
         }
+    }
+}
+
+// the one-table form: += ci_i e_j at (i, j), or at (j, i) for a transposed
+// table; the factor J at that entry is the same for every edge and is
+// applied per block (block_partial_add's scale)
+template <int S, int NT, bool REG>
+__device__ __forceinline__ void add_table_outer(float *acc, float *sacc, const float *ci, const float *e, bool tr) {
+    if constexpr (REG) {
+        if (tr) {
+#pragma unroll
+            for (int i = 0; i < S; ++i)
+#pragma unroll
+                for (int j = 0; j < S; ++j) acc[j * S + i] += ci[i] * e[j];
+        } else {
+#pragma unroll
+            for (int i = 0; i < S; ++i)
+#pragma unroll
+                for (int j = 0; j < S; ++j) acc[i * S + j] += ci[i] * e[j];
+        }
+    } else {
+        const int si = tr ? 1 : S, sj = tr ? S : 1;
+#pragma unroll
+        for (int i = 0; i < S; ++i)
+#pragma unroll
+            for (int j = 0; j < S; ++j) sacc[(i * si + j * sj) * NT + threadIdx.x] += ci[i] * e[j];
     }
 }
 
@@ -408,8 +436,8 @@ __device__ __forceinline__ void bwd_edge(const float *J, const float *x, const f
 // source-sorted slots; null at t = T).  Writes lbbar_out (mode 1: lbbar_0
 // without its own send term), this iteration's x adjoint terms xc, and adds
 // the block's log-table adjoint into epart.
-template <int S, int B = 2>
-__global__ void __launch_bounds__(bwd_threads<S>(), bwd_min_blocks<S>()) k_u_bwd(const UGraph g, int mode, const float *__restrict__ send,
+template <int S, int B = 2, int MB = bwd_min_blocks<S>()>
+__global__ void __launch_bounds__(bwd_threads<S>(), MB) k_u_bwd(const UGraph g, int mode, const float *__restrict__ send,
                                                            const float *__restrict__ lb_t,
                                                            const float *__restrict__ lbbar_t,
                                                            const float *__restrict__ xc_next,
@@ -463,14 +491,14 @@ __global__ void __launch_bounds__(bwd_threads<S>(), bwd_min_blocks<S>()) k_u_bwd
                 const float *J = S <= 4 ? jr : Js;
                 float e[S], ci[S], c[S];
                 bwd_edge<S>(J, x[b], Pbar, ps, e, ci, c);
-                if (one_table) add_table_adjoint<S, NT, REG>(acc, sacc, ci, J, e, (tb[b] & 0x80u) != 0);
+                if (one_table) add_table_outer<S, NT, REG>(acc, sacc, ci, e, (tb[b] & 0x80u) != 0);
                 stv<S>(xc + (size_t)slot[b] * S, c);
             }
         }
     }
     // several tables: k_u_pair_grad adds the table adjoint
     if (pbar_out) return;
-    block_partial_add<S, NT, REG>(acc, sacc, wred, epart + (size_t)blockIdx.x * S * S);
+    block_partial_add<S, NT, REG>(acc, sacc, wred, epart + (size_t)blockIdx.x * S * S, sm);
 }
 
 // ---- the one-table adjoint on the tensor cores (5 <= S <= 8) ------------
@@ -761,6 +789,9 @@ static int u_backward(bp_unrolled *u) {
     const bool mma = S >= 5 && S <= 8 && u->K == 1;
     const int batch = S <= 4 ? ubwd_env("BP_UBWD_BATCH", 2, 4) : 2;
     const uint32_t npt = (uint32_t)ubwd_env("BP_UBWD_NPT", (int)kBwdNodesPerThread, 1);
+    // register cap of the adjoint kernel, 1-4 states: BP_UBWD_MINB=3 allows
+    // 85 registers (3 blocks per SM) instead of 64 (4 blocks)
+    const int minb = ubwd_env("BP_UBWD_MINB", 4, 3);
     const unsigned gb = mma ? grid_for(u->V, kMmaThreads * 2) : grid_for(u->V, BT * npt);
     cudaStream_t st = u->stream;
     int rc = BP_OK;
@@ -773,6 +804,8 @@ static int u_backward(bp_unrolled *u) {
         if constexpr (S <= 4) {
             if (batch == 4)
                 return u_launch(k_u_bwd<S, 4>, gb, BT, st, g, mode, send, b_t, gbar, xn, out, xo, u->epart, pb);
+            if (minb == 3)
+                return u_launch(k_u_bwd<S, 2, 3>, gb, BT, st, g, mode, send, b_t, gbar, xn, out, xo, u->epart, pb);
         }
         return u_launch(k_u_bwd<S, 2>, gb, BT, st, g, mode, send, b_t, gbar, xn, out, xo, u->epart, pb);
     };
