@@ -135,19 +135,15 @@ struct bp_graph {
     // node (range_nodes consecutive ids per range, so one range's send
     // buffers fit L2), in position order inside a range.  The send pass reads
     // these streams contiguously and gathers Q from one range at a time; the
-    // node pass reads each node tile's messages as one segment per range and
-    // puts them back in position order through s_off.
+    // node pass reads each in-edge's message through s_inv.
     struct Split {
         int state = 0;                   // 0 not built, 1 ready, -1 not applicable to this graph
         uint32_t R = 0;                  // source ranges
         uint32_t range_nodes = 0;
-        uint32_t ntiles = 0;             // node tiles of the node pass
-        uint32_t tile_nodes = 0;         // nodes per node tile
         uint32_t *s_src = nullptr;       // [E] source node (send order)
         uint32_t *s_edge = nullptr;      // [E] edge id (serial delta terms)
         uint32_t *s_pos = nullptr;       // [E] position of send index k
-        uint16_t *s_off = nullptr;       // [E] position - first position of its node tile
-        uint32_t *seg = nullptr;         // [R * ntiles + 1] first send index of (range, tile), range-major
+        uint32_t *s_inv = nullptr;       // [E] send index of position p
         float *s_joint = nullptr;        // [E][MS][MS]
         float *s_msg[2] = {nullptr, nullptr};   // the two message arrays in send order
     } split;
@@ -204,11 +200,10 @@ int tree_build_levels_gpu(bp_graph *g, uint32_t *levels, uint32_t *num_levels);
 int ensure_staging(bp_graph *g, size_t bytes);
 int ensure_out_csr(bp_graph *g);
 int ensure_host_in_ptr(bp_graph *g);
-// split flooding schedule: build g->split for node tiles of `tile_nodes`
-// nodes holding at most `tile_edges` in-edges each and source ranges of
-// `range_nodes` ids; state -1 (and nothing allocated) when a tile holds more
+// split flooding schedule: build g->split with source ranges of
+// `range_nodes` ids (uniform graphs of at most 4 states; else state -1)
 void split_free(bp_graph *g);
-int split_build(bp_graph *g, uint32_t tile_nodes, uint32_t tile_edges, uint32_t range_nodes);
+int split_build(bp_graph *g, uint32_t range_nodes);
 // the split layout for a graph the default loop runs split (loopy.cu)
 int flood_split_prepare(bp_graph *g);
 

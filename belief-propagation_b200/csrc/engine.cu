@@ -398,150 +398,87 @@ int ensure_out_csr(bp_graph *g) {
 
 // ---- split flooding schedule layout (used by loopy.cu) ---------------------
 
-// largest in-edge count of any node tile of tn nodes
-__global__ void k_split_tile_edges(const uint32_t *__restrict__ in_ptr, uint32_t V, uint32_t tn, uint32_t ntiles,
-                                   uint32_t *__restrict__ maxe) {
-    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= ntiles) return;
-    const uint64_t v0 = t * tn, v1 = (uint64_t)V < v0 + tn ? (uint64_t)V : v0 + tn;
-    atomicMax(maxe, in_ptr[v1] - in_ptr[v0]);
+// per position: the range of its source (the sort key)
+__global__ void k_split_keys(const uint32_t *__restrict__ in_src, uint32_t E, uint32_t range_nodes,
+                             uint32_t *__restrict__ key) {
+    const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < E) key[p] = in_src[p] / range_nodes;
 }
 
-// per position: the range of its source (sort key), its node tile, and its
-// offset from the tile's first position
-__global__ void k_split_keys(const uint32_t *__restrict__ in_ptr, const uint32_t *__restrict__ in_src, uint32_t V,
-                             uint32_t tn, uint32_t range_nodes, uint32_t *__restrict__ key,
-                             uint32_t *__restrict__ tile_of, uint16_t *__restrict__ off) {
-    const uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= V) return;
-    const uint32_t t = (uint32_t)(v / tn), base = in_ptr[(size_t)t * tn];
-    for (uint32_t p = in_ptr[v]; p < in_ptr[v + 1]; ++p) {
-        key[p] = in_src[p] / range_nodes;
-        tile_of[p] = t;
-        off[p] = (uint16_t)(p - base);
-    }
-}
-
-// the send-order streams, and the (range, tile) histogram the segment table
-// is scanned from
+// the send-order streams and the inverse permutation
 template <int MS>
 __global__ void k_split_gather(const uint32_t *__restrict__ s_pos, uint32_t E, const uint32_t *__restrict__ in_src,
-                               const uint32_t *__restrict__ pos_edge, const uint32_t *__restrict__ tile_of,
-                               const uint16_t *__restrict__ off, const float *__restrict__ joint,
-                               uint32_t range_nodes, uint32_t ntiles, uint32_t *__restrict__ s_src,
-                               uint32_t *__restrict__ s_edge, uint16_t *__restrict__ s_off,
-                               float *__restrict__ s_joint, uint32_t *__restrict__ hist) {
+                               const uint32_t *__restrict__ pos_edge, const float *__restrict__ joint,
+                               uint32_t *__restrict__ s_src, uint32_t *__restrict__ s_edge,
+                               uint32_t *__restrict__ s_inv, float *__restrict__ s_joint) {
     const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= E) return;
-    const uint32_t p = s_pos[k], s = in_src[p];
-    s_src[k] = s;
+    const uint32_t p = s_pos[k];
+    s_src[k] = in_src[p];
     s_edge[k] = pos_edge[p];
-    s_off[k] = off[p];
+    s_inv[p] = (uint32_t)k;
     float j[MS * MS];
     ldv<MS * MS>(joint + (size_t)p * (MS * MS), j);
     stv<MS * MS>(s_joint + (size_t)k * (MS * MS), j);
-    atomicAdd(hist + (size_t)(s / range_nodes) * ntiles + tile_of[p], 1u);
 }
 
 void split_free(bp_graph *g) {
     auto &s = g->split;
-    void *ptrs[] = {s.s_src, s.s_edge, s.s_pos, s.s_off, s.seg, s.s_joint, s.s_msg[0], s.s_msg[1]};
+    void *ptrs[] = {s.s_src, s.s_edge, s.s_pos, s.s_inv, s.s_joint, s.s_msg[0], s.s_msg[1]};
     for (void *p : ptrs)
         if (p) cudaFreeAsync(p, g->stream);
     s = bp_graph::Split{};
 }
 
 template <int MS>
-static int split_gather(bp_graph *g, const uint32_t *tile_of, const uint16_t *off, uint32_t *hist) {
+static int split_gather(bp_graph *g) {
     auto &s = g->split;
-    k_split_gather<MS><<<grid_for(g->E, 256), 256, 0, g->stream>>>(s.s_pos, g->E, g->in_src, g->pos_edge, tile_of,
-                                                                   off, g->joint, s.range_nodes, s.ntiles, s.s_src,
-                                                                   s.s_edge, s.s_off, s.s_joint, hist);
+    k_split_gather<MS><<<grid_for(g->E, 256), 256, 0, g->stream>>>(s.s_pos, g->E, g->in_src, g->pos_edge, g->joint,
+                                                                   s.s_src, s.s_edge, s.s_inv, s.s_joint);
     BP_CUDA(cudaGetLastError());
     return BP_OK;
 }
 
-int split_build(bp_graph *g, uint32_t tn, uint32_t te, uint32_t range_nodes) {
+int split_build(bp_graph *g, uint32_t range_nodes) {
     auto &s = g->split;
     if (s.state) return BP_OK;
     const uint32_t V = g->V, E = g->E, ms = g->ms;
     s.state = -1;
-    if (!g->uniform || ms > 4 || V == 0 || E == 0 || te > 65536u || range_nodes == 0) return BP_OK;
+    if (!g->uniform || ms > 4 || V == 0 || E == 0 || range_nodes == 0) return BP_OK;
     StageTrace trace(g->stream, "split layout");
-    const uint32_t ntiles = (uint32_t)(((uint64_t)V + tn - 1) / tn);
-    uint32_t *maxe = nullptr;
-    BP_CUDA(cudaMallocAsync((void **)&maxe, sizeof(uint32_t), g->stream));
-    BP_CUDA(cudaMemsetAsync(maxe, 0, sizeof(uint32_t), g->stream));
-    k_split_tile_edges<<<grid_for(ntiles, 256), 256, 0, g->stream>>>(g->in_ptr, V, tn, ntiles, maxe);
-    BP_CUDA(cudaGetLastError());
-    uint32_t hmax = 0;
-    BP_CUDA(cudaMemcpyAsync(&hmax, maxe, sizeof(uint32_t), cudaMemcpyDeviceToHost, g->stream));
-    BP_CUDA(cudaStreamSynchronize(g->stream));
-    cudaFreeAsync(maxe, g->stream);
-    if (hmax > te) return BP_OK;   // a node tile's in-edges do not fit the node pass
-
     const uint32_t R = (uint32_t)(((uint64_t)V + range_nodes - 1) / range_nodes);
     s.R = R;
     s.range_nodes = range_nodes;
-    s.ntiles = ntiles;
-    s.tile_nodes = tn;
     int st;
-    const size_t nseg = (size_t)R * ntiles + 1;
-    if ((st = dev_alloc(g, (void **)&s.s_src, sizeof(uint32_t) * ((size_t)E + kArrayPadEdges)))) return st;
+    if ((st = dev_alloc(g, (void **)&s.s_src, sizeof(uint32_t) * (size_t)E))) return st;
     if ((st = dev_alloc(g, (void **)&s.s_edge, sizeof(uint32_t) * (size_t)E))) return st;
     if ((st = dev_alloc(g, (void **)&s.s_pos, sizeof(uint32_t) * (size_t)E))) return st;
-    if ((st = dev_alloc(g, (void **)&s.s_off, sizeof(uint16_t) * ((size_t)E + kArrayPadEdges)))) return st;
-    if ((st = dev_alloc(g, (void **)&s.seg, sizeof(uint32_t) * nseg))) return st;
-    if ((st = dev_alloc(g, (void **)&s.s_joint, sizeof(float) * ms * ms * ((size_t)E + kArrayPadEdges)))) return st;
-    for (int k = 0; k < 2; ++k) {
-        if ((st = dev_alloc(g, (void **)&s.s_msg[k], sizeof(float) * ms * ((size_t)E + kArrayPadEdges)))) return st;
-        // the bulk copies read the padding past the last edge: keep it defined
-        BP_CUDA(cudaMemsetAsync(s.s_msg[k], 0, sizeof(float) * ms * ((size_t)E + kArrayPadEdges), g->stream));
-    }
-    BP_CUDA(cudaMemsetAsync(s.s_src + E, 0, sizeof(uint32_t) * kArrayPadEdges, g->stream));
-    BP_CUDA(cudaMemsetAsync(s.s_joint + (size_t)E * ms * ms, 0, sizeof(float) * ms * ms * kArrayPadEdges, g->stream));
+    if ((st = dev_alloc(g, (void **)&s.s_inv, sizeof(uint32_t) * (size_t)E))) return st;
+    if ((st = dev_alloc(g, (void **)&s.s_joint, sizeof(float) * ms * ms * (size_t)E))) return st;
+    for (int k = 0; k < 2; ++k)
+        if ((st = dev_alloc(g, (void **)&s.s_msg[k], sizeof(float) * ms * (size_t)E))) return st;
     trace.mark("allocate");
-
-    uint32_t *key = nullptr, *key_sorted = nullptr, *iota = nullptr, *tile_of = nullptr;
-    uint16_t *off = nullptr;
+    uint32_t *key = nullptr, *key_sorted = nullptr, *iota = nullptr;
     BP_CUDA(cudaMallocAsync((void **)&key, sizeof(uint32_t) * E, g->stream));
     BP_CUDA(cudaMallocAsync((void **)&key_sorted, sizeof(uint32_t) * E, g->stream));
     BP_CUDA(cudaMallocAsync((void **)&iota, sizeof(uint32_t) * E, g->stream));
-    BP_CUDA(cudaMallocAsync((void **)&tile_of, sizeof(uint32_t) * E, g->stream));
-    BP_CUDA(cudaMallocAsync((void **)&off, sizeof(uint16_t) * E, g->stream));
-    k_split_keys<<<grid_for(V, 256), 256, 0, g->stream>>>(g->in_ptr, g->in_src, V, tn, range_nodes, key, tile_of, off);
+    k_split_keys<<<grid_for(E, 256), 256, 0, g->stream>>>(g->in_src, E, range_nodes, key);
     k_iota<<<grid_for(E, 256), 256, 0, g->stream>>>(iota, E);
     BP_CUDA(cudaGetLastError());
     // stable: inside a range the positions stay in order
     if ((st = radix_sort_pairs(g, key, key_sorted, iota, s.s_pos, E, R - 1))) return st;
     trace.mark("range sort");
-    uint32_t *hist = nullptr;
-    BP_CUDA(cudaMallocAsync((void **)&hist, sizeof(uint32_t) * nseg, g->stream));
-    BP_CUDA(cudaMemsetAsync(hist, 0, sizeof(uint32_t) * nseg, g->stream));
     switch (ms) {
-    case 1: st = split_gather<1>(g, tile_of, off, hist); break;
-    case 2: st = split_gather<2>(g, tile_of, off, hist); break;
-    case 3: st = split_gather<3>(g, tile_of, off, hist); break;
-    default: st = split_gather<4>(g, tile_of, off, hist); break;
+    case 1: st = split_gather<1>(g); break;
+    case 2: st = split_gather<2>(g); break;
+    case 3: st = split_gather<3>(g); break;
+    default: st = split_gather<4>(g); break;
     }
     if (st) return st;
-    {
-        size_t temp = 0;
-        BP_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, temp, hist, s.seg, (int64_t)nseg, g->stream));
-        void *tmp = nullptr;
-        BP_CUDA(cudaMallocAsync(&tmp, temp, g->stream));
-        cudaError_t e = cub::DeviceScan::ExclusiveSum(tmp, temp, hist, s.seg, (int64_t)nseg, g->stream);
-        cudaFreeAsync(tmp, g->stream);
-        if (e != cudaSuccess) return cuda_fail(e, "DeviceScan::ExclusiveSum", __FILE__, __LINE__);
-    }
-    cudaFreeAsync(hist, g->stream);
     cudaFreeAsync(key, g->stream);
     cudaFreeAsync(key_sorted, g->stream);
     cudaFreeAsync(iota, g->stream);
-    cudaFreeAsync(tile_of, g->stream);
-    cudaFreeAsync(off, g->stream);
-    BP_CUDA(cudaStreamSynchronize(g->stream));
-    trace.mark("gather + segments");
+    trace.mark("gather");
     s.state = 1;
     return BP_OK;
 }

@@ -1992,22 +1992,19 @@ static int block_tiles(const bp_graph *g, unsigned *grid, uint32_t *ntiles) {
 
 // ---- the split schedule (flood_split.cuh) ----------------------------------
 
-// send buffers per source range: BP_FLOOD_RANGE_MB (default 32) MB, and at
-// most NodeCfg::RMAX ranges
+// send buffers per source range: BP_FLOOD_RANGE_MB (default 32) MB, or
+// BP_FLOOD_RANGE_NODES nodes
 static uint32_t split_range_nodes(const bp_graph *g) {
+    if (const char *env = getenv("BP_FLOOD_RANGE_NODES")) return std::max<uint32_t>(1, (uint32_t)atol(env));
     size_t mb = 32;
     if (const char *env = getenv("BP_FLOOD_RANGE_MB")) mb = std::max<size_t>(1, (size_t)atol(env));
-    uint64_t rn = std::max<uint64_t>(1, (mb << 20) / (sizeof(float) * g->ms));
-    const uint64_t min_rn = ((uint64_t)g->V + NodeCfg<2>::RMAX - 1) / NodeCfg<2>::RMAX;
-    return (uint32_t)std::min<uint64_t>(std::max(rn, min_rn), 0xffffffffu);
+    const uint64_t rn = std::max<uint64_t>(1, (mb << 20) / (sizeof(float) * g->ms));
+    return (uint32_t)std::min<uint64_t>(rn, 0xffffffffu);
 }
 
-// BP_FLOOD_SPLIT=1: whenever the layout fits; =auto: when the send buffers
+// BP_FLOOD_SPLIT=1: whenever the layout applies; =auto: when the send buffers
 // exceed BP_FLOOD_SPLIT_MIN_MB (default 64) MB, i.e. when they no longer stay
-// in L2 across an iteration; default (or 0): never.  On the 16.8M-node graph
-// the split schedule moves 3.7 GB per iteration against k_flood's 4.8 GB,
-// but its two kernels run at 3.9 and 2.5 TB/s (1.11 ms against 0.87 ms), so
-// the default loop keeps k_flood.
+// in L2 across an iteration; default (or 0): never.
 static bool split_wanted(const bp_graph *g) {
     const char *env = getenv("BP_FLOOD_SPLIT");
     if (!env || env[0] == '0') return false;
@@ -2017,29 +2014,7 @@ static bool split_wanted(const bp_graph *g) {
     return (uint64_t)g->V * g->ms * sizeof(float) > ((uint64_t)mb << 20);
 }
 
-// node-pass tiles: BP_SPLIT_NODE_NT=256 builds 256-node tiles (1-2 states),
-// else 128; fixed when the layout is built
-static uint32_t split_tile_nodes(const bp_graph *g) {
-    const char *env = getenv("BP_SPLIT_NODE_NT");
-    return (g->ms <= 2 && env && atoi(env) == 256) ? 256u : 128u;
-}
-
-template <int MS>
-static int split_prepare_ms(bp_graph *g) {
-    if (split_tile_nodes(g) == 256) {
-        if constexpr (MS <= 2) return split_build(g, 256, NodeCfg<MS, 256>::EB, split_range_nodes(g));
-    }
-    return split_build(g, NodeCfg<MS>::NT, NodeCfg<MS>::EB, split_range_nodes(g));
-}
-
-static int split_prepare(bp_graph *g) {
-    switch (g->ms) {
-    case 1: return split_prepare_ms<1>(g);
-    case 2: return split_prepare_ms<2>(g);
-    case 3: return split_prepare_ms<3>(g);
-    default: return split_prepare_ms<4>(g);
-    }
-}
+static int split_prepare(bp_graph *g) { return split_build(g, split_range_nodes(g)); }
 
 // build the split layout of a graph the default loop would run it on (the
 // graph build calls this, so a serving loop's next graph is prepared beside
@@ -2049,34 +2024,15 @@ int flood_split_prepare(bp_graph *g) {
     return split_prepare(g);
 }
 
-// send-pass shapes of 2-state graphs, BP_SPLIT_SEND=0..3 (sweeps; every
-// shape gives the same results): 0 = 1024-edge chunks x 3 stages, 256
-// threads; 1 = 512 x 3, 256; 2 = 1024 x 4, 512; 3 = 2048 x 3, 512
-template <int MS, int SV> struct SendShape { using C = SendCfg<MS>; };
-template <> struct SendShape<2, 1> { using C = SendCfgT<2, 512u, 3, 256u>; };
-template <> struct SendShape<2, 2> { using C = SendCfgT<2, 1024u, 4, 512u>; };
-template <> struct SendShape<2, 3> { using C = SendCfgT<2, 2048u, 3, 512u>; };
-
-static int split_send_shape(const bp_graph *g) {
-    const char *env = getenv("BP_SPLIT_SEND");
-    const int v = env ? atoi(env) : 0;
-    return (g->ms == 2 && v >= 0 && v <= 3) ? v : 0;
-}
-
-static SplitArgs split_args(bp_graph *g, uint32_t ch, unsigned grid_a) {
+static SplitArgs split_args(bp_graph *g, uint32_t nparts) {
     SplitArgs a;
     const auto &s = g->split;
     a.V = g->V;
     a.E = g->E;
-    a.nchunks = (g->E + ch - 1) / ch;
-    a.ntiles = s.ntiles;
-    a.R = s.R;
-    a.nparts = std::min<unsigned>(grid_a, a.nchunks);
     a.in_ptr = g->in_ptr;
     a.s_src = s.s_src;
     a.s_edge = s.s_edge;
-    a.seg = s.seg;
-    a.s_off = s.s_off;
+    a.s_inv = s.s_inv;
     a.s_joint = s.s_joint;
     a.s_msg0 = s.s_msg[0];
     a.s_msg1 = s.s_msg[1];
@@ -2084,60 +2040,40 @@ static SplitArgs split_args(bp_graph *g, uint32_t ch, unsigned grid_a) {
     a.q1 = g->q[1];
     a.belief = g->belief;
     a.partials = g->partials;
+    a.nparts = nparts;
     a.absdiff = g->absdiff;
     a.ctl = g->ctl;
     return a;
 }
 
-// k launches of (send pass, node pass) with shapes SC / NC, or (k == 0) the
-// send pass's block count only (the delta partials it writes)
-template <int MS, bool SER, typename SC, typename NC>
+// k launches of (send pass, node pass), or (k == 0) the send pass's block
+// count only (the delta partials it writes): resident blocks x SMs, at most
+// one block per 256 edges
+template <int MS, bool SER>
 static int split_run(bp_graph *g, uint32_t k, uint32_t *nparts) {
     static int bps_a = 0, bps_b = 0;
     static std::mutex mu;
     {
         std::lock_guard<std::mutex> lock(mu);
         if (bps_a == 0) {
-            BP_CUDA(cudaFuncSetAttribute(k_flood_send<MS, SER, SC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         SC::SMEM));
-            BP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps_a, k_flood_send<MS, SER, SC>, SC::NT, SC::SMEM));
-            BP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps_b, k_flood_nodes<MS, SER, NC>, NC::NT, 0));
+            BP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps_a, k_flood_send<MS, SER>, kSendThreads, 0));
+            BP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps_b, k_flood_nodes<MS, SER>, kNodeThreads, 0));
             if (bps_a < 1 || bps_b < 1) return set_error(BP_ERR_CUDA, "split iteration kernels do not fit an SM");
         }
     }
     int dev = 0, sms = 0;
     BP_CUDA(cudaGetDevice(&dev));
     BP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const SplitArgs a = split_args(g, SC::CH, (unsigned)(bps_a * sms));
-    if (nparts) *nparts = a.nparts;
-    const unsigned ga = a.nparts, gb = std::min<unsigned>((unsigned)(bps_b * sms), a.ntiles);
+    const unsigned ga = std::min<unsigned>((unsigned)(bps_a * sms), grid_for(g->E, kSendThreads));
+    const unsigned gb = std::min<unsigned>((unsigned)(bps_b * sms), grid_for(g->V, kNodeThreads));
+    if (nparts) *nparts = ga;
+    const SplitArgs a = split_args(g, ga);
     for (uint32_t i = 0; i < k; ++i) {
-        k_flood_send<MS, SER, SC><<<ga, SC::NT, SC::SMEM, g->stream>>>(a);
-        k_flood_nodes<MS, SER, NC><<<gb, NC::NT, 0, g->stream>>>(a);
+        k_flood_send<MS, SER><<<ga, kSendThreads, 0, g->stream>>>(a);
+        k_flood_nodes<MS, SER><<<gb, kNodeThreads, 0, g->stream>>>(a);
         BP_CUDA(cudaGetLastError());
     }
     return BP_OK;
-}
-
-template <int MS, bool SER, typename NC>
-static int split_dispatch_send(bp_graph *g, uint32_t k, uint32_t *nparts) {
-    if constexpr (MS == 2 && !SER) {
-        switch (split_send_shape(g)) {
-        case 1: return split_run<MS, SER, SendShape<2, 1>::C, NC>(g, k, nparts);
-        case 2: return split_run<MS, SER, SendShape<2, 2>::C, NC>(g, k, nparts);
-        case 3: return split_run<MS, SER, SendShape<2, 3>::C, NC>(g, k, nparts);
-        default: break;
-        }
-    }
-    return split_run<MS, SER, SendCfg<MS>, NC>(g, k, nparts);
-}
-
-template <int MS, bool SER>
-static int split_dispatch(bp_graph *g, uint32_t k, uint32_t *nparts) {
-    if constexpr (MS <= 2) {
-        if (g->split.tile_nodes == 256) return split_dispatch_send<MS, SER, NodeCfg<MS, 256>>(g, k, nparts);
-    }
-    return split_dispatch_send<MS, SER, NodeCfg<MS>>(g, k, nparts);
 }
 
 template <int MS, bool UNI>
@@ -2145,7 +2081,7 @@ static int enqueue_split_iterations(bp_graph *g, uint32_t k, bool serial) {
     if constexpr (!UNI || MS > 4) {
         return set_error(BP_ERR_INVALID, "split schedule: uniform graphs of at most 4 states");
     } else {
-        return serial ? split_dispatch<MS, true>(g, k, nullptr) : split_dispatch<MS, false>(g, k, nullptr);
+        return serial ? split_run<MS, true>(g, k, nullptr) : split_run<MS, false>(g, k, nullptr);
     }
 }
 
@@ -2155,7 +2091,7 @@ static int split_send_blocks(bp_graph *g, bool serial, uint32_t *n) {
     if constexpr (!UNI || MS > 4) {
         return set_error(BP_ERR_INVALID, "split schedule: uniform graphs of at most 4 states");
     } else {
-        return serial ? split_dispatch<MS, true>(g, 0, n) : split_dispatch<MS, false>(g, 0, n);
+        return serial ? split_run<MS, true>(g, 0, n) : split_run<MS, false>(g, 0, n);
     }
 }
 
@@ -2512,8 +2448,7 @@ int bp_loopy(bp_graph *g, const bp_loopy_options *opt, bp_loopy_result *res) {
         if (use) variant = BP_KERNEL_SPLIT;
         else if (opt->kernel_variant == BP_KERNEL_SPLIT)
             return set_error(BP_ERR_INVALID, "split tiles need the node schedule on a uniform graph of at most 4 "
-                                             "states whose 128-node tiles hold at most %u in-edges",
-                                             g->ms <= 2 ? 4096u / g->ms : 8192u / g->ms);
+                                             "states");
     }
     if (variant != BP_KERNEL_BLOCK_TILE && variant != BP_KERNEL_WARP_TILE && variant != BP_KERNEL_STAGED_TILE &&
         variant != BP_KERNEL_SPLIT)

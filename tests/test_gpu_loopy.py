@@ -299,16 +299,15 @@ SPLIT_CASES = [
 
 @pytest.mark.parametrize("reorder", [False, True], ids=["ids", "renumbered"])
 @pytest.mark.parametrize("case", SPLIT_CASES, ids=lambda c: f"S{c['S']}")
-@pytest.mark.parametrize("range_mb", ["0", "32"], ids=["many_ranges", "one_range"])
-def test_loopy_split_schedule_parity(bp, synth, restatement, O, monkeypatch, case, reorder, range_mb):
+@pytest.mark.parametrize("range_nodes", ["97", "100000"], ids=["many_ranges", "one_range"])
+def test_loopy_split_schedule_parity(bp, synth, restatement, O, monkeypatch, case, reorder, range_nodes):
     """The split schedule (send pass over source ranges + node pass) forced
-    on small graphs: with one range, and with the range cut to one node's
-    send buffer (BP_FLOOD_RANGE_MB=0 rounds up to the 32-range limit); the
-    reference's serial delta and the fp64 delta, check every iteration and
+    on small graphs: with one range, and with ranges of 97 nodes
+    (BP_FLOOD_RANGE_NODES); the reference's serial delta and the fp64 delta, check every iteration and
     every 10 (_acc): beliefs, both message arrays, iteration count and
     returned deltas equal the oracle's."""
     monkeypatch.setenv("BP_FLOOD_SPLIT", "1")
-    monkeypatch.setenv("BP_FLOOD_RANGE_MB", range_mb)
+    monkeypatch.setenv("BP_FLOOD_RANGE_NODES", range_nodes)
     net = synth.random_loopy(case["V"], case["E"], case["S"], 0.1, seed=case["seed"])
     S = case["S"]
     for tol, max_it, check in ((1e-3, 40, 1), (0.0, 15, 1), (1e-3, 45, 10)):
@@ -323,16 +322,13 @@ def test_loopy_split_schedule_parity(bp, synth, restatement, O, monkeypatch, cas
             np.testing.assert_array_equal(f64[k], blk[k])
 
 
-@pytest.mark.parametrize("send_shape", ["0", "1", "2", "3"])
-@pytest.mark.parametrize("node_tile", ["128", "256"])
-def test_loopy_split_schedule_shapes(bp, synth, restatement, O, monkeypatch, send_shape, node_tile):
-    """Every send-pass shape (chunk, stages, threads) and node-tile size of
-    the split schedule gives the oracle's results on a 2-state power-law
-    graph with a ragged last chunk and many ranges."""
+@pytest.mark.parametrize("range_nodes", ["1", "4096"])
+def test_loopy_split_schedule_ragged_power_law(bp, synth, restatement, O, monkeypatch, range_nodes):
+    """The split schedule on a 2-state power-law graph whose edge count fills
+    no whole round of the send pass, with one node per range and with ranges
+    of 4096 nodes (BP_FLOOD_RANGE_NODES): the oracle's results."""
     monkeypatch.setenv("BP_FLOOD_SPLIT", "1")
-    monkeypatch.setenv("BP_FLOOD_RANGE_MB", "0")
-    monkeypatch.setenv("BP_SPLIT_SEND", send_shape)
-    monkeypatch.setenv("BP_SPLIT_NODE_NT", node_tile)
+    monkeypatch.setenv("BP_FLOOD_RANGE_NODES", range_nodes)
     net = synth.power_law_loopy(20_011, 80_021, 2, 0.1, seed=13)
     ora = restatement.loopy(O.OracleGraph(net), 0.0, 12)
     assert_same(gpu_loopy(bp, net, 0.0, 12, reorder=True, kernel="split", delta="f64"), ora, 2, deltas=False)
@@ -342,17 +338,17 @@ def test_loopy_split_schedule_power_law_serial_delta(bp, synth, restatement, O, 
     """A power-law graph through the split schedule with four source ranges
     and the reference's serial delta at a tolerance it converges under."""
     monkeypatch.setenv("BP_FLOOD_SPLIT", "1")
-    monkeypatch.setenv("BP_FLOOD_RANGE_MB", "0")
+    monkeypatch.setenv("BP_FLOOD_RANGE_NODES", "4096")
     net = synth.power_law_loopy(1 << 14, 1 << 16, 2, 0.1, seed=9)
     ora = restatement.loopy(O.OracleGraph(net), 1e-2, 60)
     assert_same(gpu_loopy(bp, net, 1e-2, 60, reorder=True, kernel="split"), ora, 2)
 
 
 def test_loopy_split_schedule_refuses_or_falls_back(bp, synth, restatement, O, monkeypatch):
-    """Graphs the split layout does not hold: mixed state counts, more than 4
-    states, and a hub whose 128-node tile holds more in-edges than the node
-    pass stages.  kernel="split" refuses them; the default loop (split
-    wanted) runs k_flood on them with the oracle's results."""
+    """Graphs the split layout does not hold -- mixed state counts, more than
+    4 states -- are refused by kernel="split" and run k_flood in the default
+    loop (split wanted), with the oracle's results; a hub with 5000 in-edges
+    runs split, with the oracle's results."""
     from belief_propagation_b200.native import BPError
     from belief_propagation_b200.engine import BPGraph
     rng = np.random.default_rng(3)
@@ -371,7 +367,7 @@ def test_loopy_split_schedule_refuses_or_falls_back(bp, synth, restatement, O, m
     hub = synth.Network(np.full(V, 2, np.uint32), rng.random((V, 2), dtype=np.float32), np.zeros(V, np.uint8),
                         src, dst, rng.random((5000, 2, 2), dtype=np.float32))
     monkeypatch.setenv("BP_FLOOD_SPLIT", "1")
-    for net in (mixed, five, hub):
+    for net in (mixed, five):
         g = BPGraph.from_network(net)
         try:
             with pytest.raises(BPError):
@@ -381,6 +377,8 @@ def test_loopy_split_schedule_refuses_or_falls_back(bp, synth, restatement, O, m
         ora = restatement.loopy(O.OracleGraph(net), 1e-3, 20)
         gpu = gpu_loopy(bp, net, 1e-3, 20)
         assert_same(gpu, ora, int(net.s_max))
+    ora = restatement.loopy(O.OracleGraph(hub), 1e-3, 20)
+    assert_same(gpu_loopy(bp, hub, 1e-3, 20, kernel="split"), ora, 2)
 
 
 def _staged_cases(synth):
