@@ -105,6 +105,8 @@ struct TreeData {
     uint32_t *q_joff = nullptr;        // [E] float offset of out-edge q's table
     uint2 *q_lvidx = nullptr;          // [E] (level, index in level) of out-edge q's destination
     uint8_t *q_y = nullptr;            // [E] state count of out-edge q's destination
+    uint32_t *d_wave_off = nullptr;    // device copy of wave_off (the cooperative tail launches)
+    uint32_t *d_bar = nullptr;         // grid barrier of a tail launch: arrivals, generation, failure
 };
 
 }  // namespace bpx

@@ -171,6 +171,112 @@ __global__ void k_tree_wave_group(const uint32_t *__restrict__ nodes, uint32_t n
     }
 }
 
+// ---- the small waves of a level in one cooperative launch ---------------
+// A level's run of consecutive small waves (a warp per node) is one launch
+// whose blocks meet at a grid barrier between waves, instead of one launch
+// per wave: each such wave is a chain of a few dependent loads, so the
+// launch between two waves cost as much as the wave.  Messages written by a
+// wave are read by the next ones through L2 (ld.cg), since another SM may
+// hold a stale line in L1.  The barrier's wait is bounded (2 s); a block
+// whose wait runs out sets bar[2] and leaves, and the others leave at their
+// next barrier; bp_tree then returns BP_ERR_TIMEOUT.
+struct TreeTailArgs {
+    const uint32_t *wave_nodes, *wave_off;
+    uint32_t w0, w1, level;
+    const uint32_t *in_ptr, *out_ptr, *out_pos, *out_dst;
+    const uint2 *q_lvidx;
+    const uint32_t *node_lidx;
+    const uint8_t *node_s, *q_y;
+    const uint32_t *q_joff;
+    const float *q_joint;
+    float *msg;
+    const uint8_t *visited;
+    uint32_t *bar;   // arrivals, generation, failure flag (zeroed before the launch)
+};
+
+constexpr uint64_t kTailWaitNs = 2000000000ull;
+
+__device__ __forceinline__ bool tail_barrier(uint32_t *bar, uint32_t &gen, uint32_t *s_fail) {
+    __syncthreads();
+    if (threadIdx.x == 0 && !*s_fail) {
+        const uint32_t g0 = gen;
+        __threadfence();
+        if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+            bar[0] = 0;
+            __threadfence();
+            atomicExch(bar + 1, g0 + 1u);
+        } else {
+            const uint64_t t0 = global_ns();
+            while (*(volatile uint32_t *)(bar + 1) == g0) {
+                if (global_ns() - t0 > kTailWaitNs || *(volatile uint32_t *)(bar + 2)) {
+                    *s_fail = 1;
+                    atomicExch(bar + 2, 1u);
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    gen += 1;
+    return *s_fail == 0;
+}
+
+// one node of a wave with a warp (k_tree_wave_group's step, G = 32, the
+// incoming messages read through L2)
+template <int MS, bool UNI>
+__device__ __forceinline__ void tail_node(const TreeTailArgs &a, uint32_t u, uint32_t lane) {
+    const int S = UNI ? MS : a.node_s[u];
+    const uint32_t my_idx = a.node_lidx[u];
+    const uint32_t r0 = a.in_ptr[u], r1 = a.in_ptr[u + 1], o0 = a.out_ptr[u], o1 = a.out_ptr[u + 1];
+    float buf[MS];
+#pragma unroll
+    for (int i = 0; i < MS; ++i) buf[i] = (UNI || i < S) ? 1.0f : 0.0f;
+    for (uint32_t p0 = r0; p0 < r1; p0 += 32) {
+        float mm[MS];
+#pragma unroll
+        for (int i = 0; i < MS; ++i) mm[i] = 0.0f;
+        if (p0 + lane < r1) {
+#pragma unroll
+            for (int i = 0; i < MS; ++i) mm[i] = __ldcg(a.msg + (size_t)(p0 + lane) * MS + i);
+        }
+        const uint32_t cnt = min(32u, r1 - p0);
+        for (uint32_t j = 0; j < cnt; ++j) {
+            float mj[MS];
+#pragma unroll
+            for (int i = 0; i < MS; ++i) mj[i] = __shfl_sync(0xffffffffu, mm[i], (int)j);
+            combine<MS, UNI>(buf, mj, S);
+        }
+    }
+    for (uint32_t q = o0 + lane; q < o1; q += 32) {
+        const uint32_t w = a.out_dst[q];
+        const uint2 li = a.q_lvidx[q];
+        const bool seen = a.visited[w] || (li.x == a.level && li.y <= my_idx);
+        if (seen) continue;
+        const uint32_t p = a.out_pos[q];
+        const int y = UNI ? MS : (int)a.q_y[q];
+        float m[MS];
+        send_msg_dense<MS, UNI>(a.q_joint + a.q_joff[q], buf, S, y, m);
+        stv<MS>(a.msg + (size_t)p * MS, m);
+    }
+}
+
+template <int MS, bool UNI>
+__global__ void __launch_bounds__(256) k_tree_tail(const TreeTailArgs a) {
+    __shared__ uint32_t s_fail;
+    if (threadIdx.x == 0) s_fail = 0;
+    __syncthreads();
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+    uint32_t gen = 0;
+    for (uint32_t w = a.w0; w < a.w1; ++w) {
+        const uint32_t lo = a.wave_off[w], n = a.wave_off[w + 1] - lo;
+        for (uint32_t k = warp; k < n; k += nwarps) tail_node<MS, UNI>(a, a.wave_nodes[lo + k], lane);
+        if (w + 1 < a.w1 && !tail_barrier(a.bar, gen, &s_fail)) return;
+    }
+}
+
 // ---- the out-edge order arrays (TreeData::q_*) ---------------------------
 // per out-edge: the destination's state count and the padded table size
 __global__ void k_tq_sizes(uint32_t V, const uint32_t *__restrict__ out_ptr, const uint32_t *__restrict__ out_dst,
@@ -245,6 +351,8 @@ void tree_clear(bp_graph *g) {
     if (t.q_joff) cudaFree(t.q_joff);
     if (t.q_lvidx) cudaFree(t.q_lvidx);
     if (t.q_y) cudaFree(t.q_y);
+    if (t.d_wave_off) cudaFree(t.d_wave_off);
+    if (t.d_bar) cudaFree(t.d_bar);
     if (t.d_node_level) cudaFree(t.d_node_level);
     if (t.d_node_lidx) cudaFree(t.d_node_lidx);
     if (t.d_wave_nodes) cudaFree(t.d_wave_nodes);
@@ -330,6 +438,11 @@ static int tree_q_build(bp_graph *g) {
     BP_CUDA(cudaStreamSynchronize(g->stream));
     cudaFreeAsync(size, g->stream);
     BP_CUDA(cudaMalloc((void **)&t.q_joint, sizeof(float) * ((size_t)total + 4)));
+    BP_CUDA(cudaMalloc((void **)&t.d_wave_off, sizeof(uint32_t) * ((size_t)t.total_waves + 1)));
+    BP_CUDA(cudaMemcpy(t.d_wave_off, t.wave_off, sizeof(uint32_t) * ((size_t)t.total_waves + 1),
+                       cudaMemcpyHostToDevice));
+    BP_CUDA(cudaMalloc((void **)&t.d_bar, 4 * sizeof(uint32_t)));
+    BP_CUDA(cudaMemset(t.d_bar, 0, 4 * sizeof(uint32_t)));
     if (V)
         k_tq_fill<MS><<<grid_for(V, 256), 256, 0, g->stream>>>(V, g->out_ptr, g->out_pos, g->out_dst, g->node_s,
                                                                t.q_y, t.q_joff, g->joint, t.d_node_level,
@@ -413,6 +526,62 @@ static cudaError_t launch_wave_group(bp_graph *g, const uint32_t *nodes, uint32_
                        (const float *)t.q_joint, g->msg[0], (const uint8_t *)g->visited);
 }
 
+// BP_TREE_TAIL=0 launches every wave on its own (read when the launch
+// sequence is built)
+static bool tree_tail_on() {
+    const char *env = getenv("BP_TREE_TAIL");
+    return !(env && env[0] == '0');
+}
+
+// waves [wa, wb) of `level` (every one a warp per node) as one cooperative
+// launch of k_tree_tail
+template <int MS, bool UNI>
+static int launch_tail(bp_graph *g, uint32_t level, uint32_t wa, uint32_t wb) {
+    TreeData &t = g->tree;
+    static int bps = 0;
+    if (!bps) BP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_tree_tail<MS, UNI>, 256, 0));
+    int dev = 0, sms = 0;
+    BP_CUDA(cudaGetDevice(&dev));
+    BP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    uint32_t nmax = 0;
+    for (uint32_t w = wa; w < wb; ++w) nmax = std::max(nmax, t.wave_off[w + 1] - t.wave_off[w]);
+    const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)bps * sms,
+                                                                           ((uint64_t)nmax * 32 + 255) / 256));
+    TreeTailArgs a;
+    a.wave_nodes = t.d_wave_nodes;
+    a.wave_off = t.d_wave_off;
+    a.w0 = wa;
+    a.w1 = wb;
+    a.level = level;
+    a.in_ptr = g->in_ptr;
+    a.out_ptr = g->out_ptr;
+    a.out_pos = g->out_pos;
+    a.out_dst = g->out_dst;
+    a.q_lvidx = t.q_lvidx;
+    a.node_lidx = t.d_node_lidx;
+    a.node_s = g->node_s;
+    a.q_y = t.q_y;
+    a.q_joff = t.q_joff;
+    a.q_joint = t.q_joint;
+    a.msg = g->msg[0];
+    a.visited = g->visited;
+    a.bar = t.d_bar;
+    // arrivals and generation restart at zero; a failure flag set by an
+    // earlier launch stays set for bp_tree to report
+    BP_CUDA(cudaMemsetAsync(t.d_bar, 0, 2 * sizeof(uint32_t), g->stream));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(256);
+    cfg.stream = g->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    BP_CUDA(cudaLaunchKernelEx(&cfg, k_tree_tail<MS, UNI>, a));
+    return BP_OK;
+}
+
 template <int MS, bool UNI>
 static int launch_level(bp_graph *g, uint32_t level) {
     TreeData &t = g->tree;
@@ -420,6 +589,17 @@ static int launch_level(bp_graph *g, uint32_t level) {
     for (uint32_t w = w0; w < w1; ++w) {
         const uint32_t lo = t.wave_off[w], n = t.wave_off[w + 1] - lo;
         if (!n) continue;
+        if (tree_tail_on() && wave_group(n) == 32) {
+            // the run of warp-per-node waves that starts here
+            uint32_t we = w + 1;
+            while (we < w1 && wave_group(t.wave_off[we + 1] - t.wave_off[we]) == 32) ++we;
+            if (we - w >= 2) {
+                int st = launch_tail<MS, UNI>(g, level, w, we);
+                if (st) return st;
+                w = we - 1;
+                continue;
+            }
+        }
         const uint32_t *nodes = t.d_wave_nodes + lo;
         cudaError_t le;
         switch (wave_group(n)) {
@@ -574,6 +754,14 @@ int bp_tree(bp_graph *g, bp_tree_result *res) {
     BP_CUDA(cudaGraphLaunch(t.exec, g->stream));
     BP_CUDA(cudaEventRecord(g->ev1, g->stream));
     BP_CUDA(cudaStreamSynchronize(g->stream));
+    if (t.d_bar) {
+        uint32_t fail = 0;
+        BP_CUDA(cudaMemcpy(&fail, t.d_bar + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+        if (fail) {
+            BP_CUDA(cudaMemset(t.d_bar + 2, 0, sizeof(uint32_t)));
+            return set_error(BP_ERR_TIMEOUT, "a bounded grid-barrier wait of the tree's small waves timed out");
+        }
+    }
     if (res) {
         res->num_levels = L;
         res->num_waves = waves;
