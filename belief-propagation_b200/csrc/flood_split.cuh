@@ -135,10 +135,23 @@ __device__ __forceinline__ void split_finalize(const SplitArgs &a, bool want, do
     }
 }
 
+// messages of in-edge positions [p, p + B) of a node, from send order: the B
+// send indices first, then the B message loads, so they are in flight
+// together
+template <int MS, int B>
+__device__ __forceinline__ void load_in_msgs(const SplitArgs &a, const float *__restrict__ m_new, uint32_t p,
+                                             float (*mm)[MS]) {
+    uint32_t k[B];
+#pragma unroll
+    for (int u = 0; u < B; ++u) k[u] = __ldg(a.s_inv + p + u);
+#pragma unroll
+    for (int u = 0; u < B; ++u) ldv<MS>(m_new + (size_t)k[u] * MS, mm[u]);
+}
+
 // marginalise (graph.c:1003-1023), then the next send buffer
 // (graph.c:850-882) from the same messages: k_flood's phase 2, the messages
-// read from send order (the second pass re-reads them, from L1).  Nodes
-// grid-stride.
+// read from send order four at a time (the second pass re-reads them, from
+// L1), multiplied in position order.  Nodes grid-stride.
 template <int MS, bool SER>
 __global__ void __launch_bounds__(kNodeThreads) k_flood_nodes(const SplitArgs a) {
     constexpr int NT = kNodeThreads;
@@ -159,10 +172,17 @@ __global__ void __launch_bounds__(kNodeThreads) k_flood_nodes(const SplitArgs a)
         ldv<MS, kStream>(a.belief + (size_t)v * MS, b);
 #pragma unroll
         for (int s = 0; s < MS; ++s) prod[s] = 1.0f;
-        for (uint32_t p = r0; p < r1; ++p) {
-            float mm[MS];
-            ldv<MS>(m_new + (size_t)__ldg(a.s_inv + p) * MS, mm);
-            combine<MS, true>(prod, mm, MS);
+        uint32_t p = r0;
+        for (; p + 4 <= r1; p += 4) {
+            float mm[4][MS];
+            load_in_msgs<MS, 4>(a, m_new, p, mm);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) combine<MS, true>(prod, mm[u], MS);
+        }
+        for (; p < r1; ++p) {
+            float mm[1][MS];
+            load_in_msgs<MS, 1>(a, m_new, p, mm);
+            combine<MS, true>(prod, mm[0], MS);
         }
         if (r1 > r0) {
 #pragma unroll
@@ -173,10 +193,16 @@ __global__ void __launch_bounds__(kNodeThreads) k_flood_nodes(const SplitArgs a)
         float qo[MS];
 #pragma unroll
         for (int s = 0; s < MS; ++s) qo[s] = b[s];
-        for (uint32_t p = r0; p < r1; ++p) {
-            float mm[MS];
-            ldv<MS>(m_new + (size_t)__ldg(a.s_inv + p) * MS, mm);
-            combine<MS, true>(qo, mm, MS);
+        for (p = r0; p + 4 <= r1; p += 4) {
+            float mm[4][MS];
+            load_in_msgs<MS, 4>(a, m_new, p, mm);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) combine<MS, true>(qo, mm[u], MS);
+        }
+        for (; p < r1; ++p) {
+            float mm[1][MS];
+            load_in_msgs<MS, 1>(a, m_new, p, mm);
+            combine<MS, true>(qo, mm[0], MS);
         }
         stv<MS>(q_out + (size_t)v * MS, qo);
     }
