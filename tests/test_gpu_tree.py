@@ -168,14 +168,14 @@ def test_tree_device_and_host_level_builds_agree(bp, synth, monkeypatch):
 @pytest.mark.parametrize("n,states,seed", [(60000, (2, 3, 4, 8), 5), (30000, (2,), 6)])
 def test_tree_small_waves_in_one_launch(bp, synth, restatement, O, monkeypatch, n, states, seed):
     """The runs of small waves go through one cooperative launch with a grid
-    barrier between waves (the default) or one launch per wave
-    (BP_TREE_TAIL=0): the same beliefs and messages, the oracle's."""
+    barrier between waves (BP_TREE_TAIL=1) or one launch per wave (the
+    default): the same beliefs and messages, the oracle's."""
     net = synth.random_tree(n, states, 0.05, seed=seed)
     ora = restatement.tree(O.OracleGraph(net))
     S = net.s_max
-    coop = gpu_tree(net)
-    monkeypatch.setenv("BP_TREE_TAIL", "0")
     sep = gpu_tree(net)
+    monkeypatch.setenv("BP_TREE_TAIL", "1")
+    coop = gpu_tree(net)
     for r in (coop, sep):
         np.testing.assert_array_equal(r["beliefs"], ora["beliefs"][:, :S])
         np.testing.assert_array_equal(r["messages"][:, :S], ora["messages"][:, :S])
