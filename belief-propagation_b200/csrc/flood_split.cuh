@@ -16,15 +16,14 @@
 //       contiguous streams; the grid walks send order front to back (round r
 //       of every block covers one window of it), so at any time the gathers
 //       hit one range whose send buffers stay in L2.
-//   node pass (k_flood_nodes, warp tiles of 32 nodes):
+//   node pass (k_flood_nodes, a thread per node):
 //       each in-edge's message is read from send order through s_inv (the
-//       send index of position p); a warp reads its tile's messages together
-//       (coalesced s_inv, and a tile's messages sit in a few contiguous runs
-//       of send order, one per range) into shared memory, and each lane
-//       multiplies its node's messages in position order, so the product is
-//       k_flood's phase 2 exactly; the node writes b_t and Q_{t+1}.  The last
-//       block to finish sums the send pass's delta partials in a fixed order
-//       and applies the stopping rule.
+//       send index of position p), in position order, so the product is
+//       k_flood's phase 2 exactly; the node writes b_t and Q_{t+1}.  A node
+//       tile's messages sit in a few contiguous runs of send order (one per
+//       range), so these reads share sectors.  The last block to finish sums
+//       the send pass's delta partials in a fixed order and applies the
+//       stopping rule.
 //
 // Every fp32 operation is k_flood's, on the same operands in the same order
 // (the product order inside a node is the position order), so beliefs and
@@ -136,47 +135,29 @@ __device__ __forceinline__ void split_finalize(const SplitArgs &a, bool want, do
     }
 }
 
-// Node pass in warp tiles of 32 consecutive nodes: the lanes read the
-// tile's in-edge messages cooperatively -- lane l takes positions c0 + l,
-// c0 + l + 32, ... of the tile's contiguous position range, so the s_inv
-// reads are coalesced and the message reads of a warp fall in the tile's few
-// contiguous runs of send order -- into the warp's slice of shared memory,
-// then each lane multiplies its own node's messages in position order
-// (k_flood's phase 2).  A tile with more than WE in-edges is taken in WE-edge
-// chunks; its next send buffers then re-read the messages from global memory.
-template <int MS> constexpr uint32_t nodes_we() { return MS <= 2 ? 256u : 128u; }
-
-template <int MS>
-__device__ __forceinline__ void stage_msgs(const SplitArgs &a, const float *__restrict__ m_new, uint32_t c0,
-                                           uint32_t c1, uint32_t lane, float *wsm) {
-    constexpr int U = 4;
-    for (uint32_t p0 = c0 + lane; p0 < c1; p0 += 32u * U) {
-        uint32_t k[U];
-        float m[U][MS];
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const uint32_t p = p0 + 32u * u;
-            k[u] = p < c1 ? __ldcs(a.s_inv + p) : 0u;
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u)
-            if (p0 + 32u * u < c1) ldv<MS, kStream>(m_new + (size_t)k[u] * MS, m[u]);
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const uint32_t p = p0 + 32u * u;
-            if (p < c1) stv<MS>(wsm + (size_t)(p - c0) * MS, m[u]);
-        }
-    }
+// marginalise (graph.c:1003-1023), then the next send buffer
+// (graph.c:850-882) from the same messages: k_flood's phase 2, a thread per
+// node, the messages read from send order through s_inv in position order
+// (the second pass re-reads them, from L1).  Nodes grid-stride.  NV selects
+// the form of the loads (sweeps; the same results): 0 plain, 1 the loop
+// unrolled by 4 by the compiler, 2 the send indices and messages through
+// the read-only path.  Measured forms that were slower: four messages loaded
+// before their use (0.43 ms against 0.34 ms per launch on the 16.8M-node
+// graph), and warp tiles staging a tile's messages through shared memory
+// (0.45 ms).
+template <int MS, int NV>
+__device__ __forceinline__ void node_msg(const SplitArgs &a, const float *__restrict__ m_new, uint32_t p, float *mm) {
+    if constexpr (NV == 2) ldv<MS, kReadOnly>(m_new + (size_t)__ldg(a.s_inv + p) * MS, mm);
+    else ldv<MS>(m_new + (size_t)a.s_inv[p] * MS, mm);
 }
 
-template <int MS, bool SER>
+template <int MS, bool SER, int NV = 0>
 __global__ void __launch_bounds__(kNodeThreads) k_flood_nodes(const SplitArgs a) {
-    constexpr int NT = kNodeThreads, NW = NT / 32;
-    constexpr uint32_t WE = nodes_we<MS>();
+    constexpr int NT = kNodeThreads;
     constexpr uint32_t CAP = SER ? 8u * NT : 1u;   // staging of the serial sum (serial mode only)
-    __shared__ __align__(16) float sm[NW * WE * MS > CAP ? NW * WE * MS : CAP];
     __shared__ double red[NT / 32];
     __shared__ bool s_last;
+    __shared__ __align__(16) float sbuf[CAP];
     LoopyCtl *ctl = a.ctl;
     if (*(volatile uint32_t *)&ctl->done) return;
     const uint32_t it = ctl->it, ce = ctl->check_every;
@@ -184,71 +165,43 @@ __global__ void __launch_bounds__(kNodeThreads) k_flood_nodes(const SplitArgs a)
     const int mp = (int)((ctl->msg_parity0 + it) & 1u), qp = (int)((ctl->q_parity0 + it) & 1u);
     const float *__restrict__ m_new = mp ? a.s_msg0 : a.s_msg1;
     float *__restrict__ q_out = qp ? a.q0 : a.q1;
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    float *wsm = sm + (size_t)warp * WE * MS;
-    const uint32_t ntiles = (a.V + 31u) / 32u;
-    for (uint32_t tile = blockIdx.x * NW + warp; tile < ntiles; tile += gridDim.x * NW) {
-        const uint32_t v0 = tile * 32u, v = v0 + lane;
-        const bool has = v < a.V;
-        const uint32_t last = min(v0 + 32u, a.V) - 1u - v0;
-        uint32_t r0 = 0, r1 = 0;
+    for (uint32_t v = blockIdx.x * NT + threadIdx.x; v < a.V; v += gridDim.x * NT) {
+        const uint32_t r0 = a.in_ptr[v], r1 = a.in_ptr[v + 1];
         float b[MS], prod[MS];
+        ldv<MS, kStream>(a.belief + (size_t)v * MS, b);
 #pragma unroll
-        for (int s = 0; s < MS; ++s) {
-            b[s] = 0.0f;
-            prod[s] = 1.0f;
-        }
-        if (has) {
-            r0 = a.in_ptr[v];
-            r1 = a.in_ptr[v + 1];
-            ldv<MS, kStream>(a.belief + (size_t)v * MS, b);
-        }
-        const uint32_t e0 = __shfl_sync(0xffffffffu, r0, 0), e1 = __shfl_sync(0xffffffffu, r1, last);
-        for (uint32_t c0 = e0; c0 < e1; c0 += WE) {
-            const uint32_t c1 = min(e1, c0 + WE);
-            stage_msgs<MS>(a, m_new, c0, c1, lane, wsm);
-            __syncwarp();
-            if (has) {
-                const uint32_t lo = max(r0, c0), hi = min(r1, c1);
-                for (uint32_t p = lo; p < hi; ++p) {
-                    float mm[MS];
-                    ldv<MS>(wsm + (size_t)(p - c0) * MS, mm);
-                    combine<MS, true>(prod, mm, MS);
-                }
+        for (int s = 0; s < MS; ++s) prod[s] = 1.0f;
+        if constexpr (NV == 1) {
+#pragma unroll 4
+            for (uint32_t p = r0; p < r1; ++p) {
+                float mm[MS];
+                node_msg<MS, NV>(a, m_new, p, mm);
+                combine<MS, true>(prod, mm, MS);
             }
-            __syncwarp();
+        } else {
+            for (uint32_t p = r0; p < r1; ++p) {
+                float mm[MS];
+                node_msg<MS, NV>(a, m_new, p, mm);
+                combine<MS, true>(prod, mm, MS);
+            }
         }
-        if (has) {
-            // marginalise (graph.c:1003-1023), then the next send buffer
-            // (graph.c:850-882) from the same messages
-            if (r1 > r0) {
+        if (r1 > r0) {
 #pragma unroll
-                for (int s = 0; s < MS; ++s) b[s] = FMUL(b[s], prod[s]);
-            }
-            normalise<MS, true>(b, MS);
-            stv<MS, kStream>(a.belief + (size_t)v * MS, b);
-            float qo[MS];
-#pragma unroll
-            for (int s = 0; s < MS; ++s) qo[s] = b[s];
-            if (e1 - e0 <= WE) {
-                for (uint32_t p = r0; p < r1; ++p) {
-                    float mm[MS];
-                    ldv<MS>(wsm + (size_t)(p - e0) * MS, mm);
-                    combine<MS, true>(qo, mm, MS);
-                }
-            } else {
-                for (uint32_t p = r0; p < r1; ++p) {
-                    float mm[MS];
-                    ldv<MS>(m_new + (size_t)__ldg(a.s_inv + p) * MS, mm);
-                    combine<MS, true>(qo, mm, MS);
-                }
-            }
-            stv<MS>(q_out + (size_t)v * MS, qo);
+            for (int s = 0; s < MS; ++s) b[s] = FMUL(b[s], prod[s]);
         }
-        __syncwarp();   // the slice is free for the next tile
+        normalise<MS, true>(b, MS);
+        stv<MS, kStream>(a.belief + (size_t)v * MS, b);
+        float qo[MS];
+#pragma unroll
+        for (int s = 0; s < MS; ++s) qo[s] = b[s];
+        for (uint32_t p = r0; p < r1; ++p) {
+            float mm[MS];
+            node_msg<MS, NV>(a, m_new, p, mm);
+            combine<MS, true>(qo, mm, MS);
+        }
+        stv<MS>(q_out + (size_t)v * MS, qo);
     }
-    __syncthreads();   // the block's shared memory is the serial sum's staging below
-    split_finalize<NT, SER>(a, want, red, &s_last, sm, CAP);
+    split_finalize<NT, SER>(a, want, red, &s_last, sbuf, CAP);
 }
 
 // the latest messages into send order before the loop, and both message

@@ -2049,15 +2049,15 @@ static SplitArgs split_args(bp_graph *g, uint32_t nparts) {
 // k launches of (send pass, node pass), or (k == 0) the send pass's block
 // count only (the delta partials it writes): resident blocks x SMs, at most
 // one block per 256 edges
-template <int MS, bool SER>
-static int split_run(bp_graph *g, uint32_t k, uint32_t *nparts) {
+template <int MS, bool SER, int NV>
+static int split_run_nv(bp_graph *g, uint32_t k, uint32_t *nparts) {
     static int bps_a = 0, bps_b = 0;
     static std::mutex mu;
     {
         std::lock_guard<std::mutex> lock(mu);
         if (bps_a == 0) {
             BP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps_a, k_flood_send<MS, SER>, kSendThreads, 0));
-            BP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps_b, k_flood_nodes<MS, SER>, kNodeThreads, 0));
+            BP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps_b, k_flood_nodes<MS, SER, NV>, kNodeThreads, 0));
             if (bps_a < 1 || bps_b < 1) return set_error(BP_ERR_CUDA, "split iteration kernels do not fit an SM");
         }
     }
@@ -2070,10 +2070,22 @@ static int split_run(bp_graph *g, uint32_t k, uint32_t *nparts) {
     const SplitArgs a = split_args(g, ga);
     for (uint32_t i = 0; i < k; ++i) {
         k_flood_send<MS, SER><<<ga, kSendThreads, 0, g->stream>>>(a);
-        k_flood_nodes<MS, SER><<<gb, kNodeThreads, 0, g->stream>>>(a);
+        k_flood_nodes<MS, SER, NV><<<gb, kNodeThreads, 0, g->stream>>>(a);
         BP_CUDA(cudaGetLastError());
     }
     return BP_OK;
+}
+
+// BP_SPLIT_NODES=0|1|2: the node pass's load form (sweeps, 2-state graphs)
+template <int MS, bool SER>
+static int split_run(bp_graph *g, uint32_t k, uint32_t *nparts) {
+    if constexpr (MS == 2) {
+        const char *env = getenv("BP_SPLIT_NODES");
+        const int nv = env ? atoi(env) : 0;
+        if (nv == 1) return split_run_nv<MS, SER, 1>(g, k, nparts);
+        if (nv == 2) return split_run_nv<MS, SER, 2>(g, k, nparts);
+    }
+    return split_run_nv<MS, SER, 0>(g, k, nparts);
 }
 
 template <int MS, bool UNI>

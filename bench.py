@@ -75,6 +75,9 @@ def parse():
                     help="power_law: the headline loopy workload; batched: 4096 independent networks; "
                          "tree: tree BP on a 2M-node random recursive tree")
     ap.add_argument("--tree-nodes", type=int, default=2_000_000)
+    ap.add_argument("--shard", action="store_true",
+                    help="split the one graph over the ranks by destination-node ranges (strong scaling: send "
+                         "buffers all-gathered every iteration) instead of one replica per rank")
     ap.add_argument("--reorder", type=int, default=1,
                     help="1: renumber nodes by out-degree inside the engine (results unchanged)")
     ap.add_argument("--networks", type=int, default=4096)
@@ -305,6 +308,56 @@ def power_law_accuracy(a, handle):
     finally:
         g.close()
     return out
+
+
+def run_sharded(a, rank, world, net, gen_s, dist, barrier, local):
+    """The headline graph split over the ranks by destination-node ranges
+    (belief_propagation_b200.sharded): each rank holds its nodes' in-edges and
+    runs bp_flood_range on them; the send buffers are all-gathered over NCCL
+    and the deltas summed in rank order after every iteration.  value = the
+    whole job's edge-msg updates/s (strong scaling: the graph is fixed)."""
+    import torch
+    from belief_propagation_b200.sharded import LocalComm, RangeEngine, TorchComm, node_ranges, sharded_loopy
+    ranges, chunk = node_ranges(net.V, world)
+    eng = RangeEngine(net, *ranges[rank], chunk, world)
+    comm = TorchComm(dist, rank, chunk) if dist is not None else LocalComm(chunk)
+    prior = torch.from_numpy(net.beliefs).cuda()
+
+    def step():
+        return sharded_loopy([eng], comm, prior, 0.0, a.iterations)
+
+    for _ in range(a.warmup):
+        step()
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    ev0.record()
+    for _ in range(a.steps):
+        r = step()
+    ev1.record()
+    barrier()
+    clk = clocks.stop()
+    ms = max_over_ranks(ev0.elapsed_time(ev1), dist) / a.steps
+    eng.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {"metric": METRIC, "value": float(net.E) * a.iterations / (ms / 1e3), "unit": UNIT, "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": workload_name(a), "nodes": net.V, "edges": net.E, "states": 2,
+                       "iterations": a.iterations, "parallelism": f"destination-range split x{world}",
+                       "node_order": "caller ids", "generator_s": round(gen_s, 1),
+                       "exchange": "send buffers all-gathered (NCCL) and deltas summed in rank order, every "
+                                   "iteration"},
+            "executed": r["executed"], "clocks": clk}
+    print(json.dumps(line), flush=True)
+    return 0
 
 
 def run_reference_arm(a, rank, world):
@@ -885,6 +938,9 @@ def main():
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     handle = stream.cuda_stream
+
+    if a.shard:
+        return run_sharded(a, rank, world, net, gen_s, dist, barrier, local)
 
     # ---- resident graph
     g = BPGraph(V, net.src, net.dst, net.joint, uniform_states=2, stream=handle, reorder=bool(a.reorder))
