@@ -204,91 +204,6 @@ __global__ void __launch_bounds__(kNodeThreads) k_flood_nodes(const SplitArgs a)
     split_finalize<NT, SER>(a, want, red, &s_last, sbuf, CAP);
 }
 
-// The node pass with a group of G lanes per node: lane j of a node loads the
-// node's in-edges j, j + G, ... (send index, then message: the chains of the
-// node's in-edges run side by side instead of one after another), and every
-// lane multiplies them in position order, shuffled from the loading lane, so
-// the product is the thread-per-node one bit for bit.  A group's lanes share
-// the node and its trip counts, so the group mask is converged.
-template <int MS, bool SER, int G>
-__global__ void __launch_bounds__(kNodeThreads) k_flood_nodes_group(const SplitArgs a) {
-    constexpr int NT = kNodeThreads;
-    constexpr uint32_t CAP = SER ? 8u * NT : 1u;
-    static_assert(G >= 2 && G <= 32 && (G & (G - 1)) == 0, "group of 2..32 lanes");
-    __shared__ double red[NT / 32];
-    __shared__ bool s_last;
-    __shared__ __align__(16) float sbuf[CAP];
-    LoopyCtl *ctl = a.ctl;
-    if (*(volatile uint32_t *)&ctl->done) return;
-    const uint32_t it = ctl->it, ce = ctl->check_every;
-    const bool want = (ce <= 1) || ((it + 1) % ce == 0);
-    const int mp = (int)((ctl->msg_parity0 + it) & 1u), qp = (int)((ctl->q_parity0 + it) & 1u);
-    const float *__restrict__ m_new = mp ? a.s_msg0 : a.s_msg1;
-    float *__restrict__ q_out = qp ? a.q0 : a.q1;
-    const uint32_t lane = threadIdx.x & (G - 1);
-    const uint32_t gmask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));
-    const uint32_t groups = gridDim.x * (NT / G);
-    for (uint32_t v = (blockIdx.x * NT + threadIdx.x) / G; v < a.V; v += groups) {
-        const uint32_t r0 = a.in_ptr[v], r1 = a.in_ptr[v + 1];
-        float b[MS], prod[MS];
-        ldv<MS, kStream>(a.belief + (size_t)v * MS, b);
-#pragma unroll
-        for (int s = 0; s < MS; ++s) prod[s] = 1.0f;
-        // the first G messages stay in the lanes for the second product
-        float first[MS];
-#pragma unroll
-        for (int s = 0; s < MS; ++s) first[s] = 1.0f;
-        for (uint32_t p0 = r0; p0 < r1; p0 += G) {
-            float mm[MS];
-#pragma unroll
-            for (int s = 0; s < MS; ++s) mm[s] = 1.0f;
-            if (p0 + lane < r1) ldv<MS>(m_new + (size_t)__ldg(a.s_inv + p0 + lane) * MS, mm);
-            if (p0 == r0) {
-#pragma unroll
-                for (int s = 0; s < MS; ++s) first[s] = mm[s];
-            }
-            const uint32_t cnt = min((uint32_t)G, r1 - p0);
-            for (uint32_t j = 0; j < cnt; ++j) {
-                float mj[MS];
-#pragma unroll
-                for (int s = 0; s < MS; ++s) mj[s] = __shfl_sync(gmask, mm[s], (int)j, G);
-                combine<MS, true>(prod, mj, MS);
-            }
-        }
-        if (r1 > r0) {
-#pragma unroll
-            for (int s = 0; s < MS; ++s) b[s] = FMUL(b[s], prod[s]);
-        }
-        normalise<MS, true>(b, MS);
-        float qo[MS];
-#pragma unroll
-        for (int s = 0; s < MS; ++s) qo[s] = b[s];
-        for (uint32_t p0 = r0; p0 < r1; p0 += G) {
-            float mm[MS];
-            if (p0 == r0) {
-#pragma unroll
-                for (int s = 0; s < MS; ++s) mm[s] = first[s];
-            } else {
-#pragma unroll
-                for (int s = 0; s < MS; ++s) mm[s] = 1.0f;
-                if (p0 + lane < r1) ldv<MS>(m_new + (size_t)__ldg(a.s_inv + p0 + lane) * MS, mm);
-            }
-            const uint32_t cnt = min((uint32_t)G, r1 - p0);
-            for (uint32_t j = 0; j < cnt; ++j) {
-                float mj[MS];
-#pragma unroll
-                for (int s = 0; s < MS; ++s) mj[s] = __shfl_sync(gmask, mm[s], (int)j, G);
-                combine<MS, true>(qo, mj, MS);
-            }
-        }
-        if (lane == 0) {
-            stv<MS, kStream>(a.belief + (size_t)v * MS, b);
-            stv<MS>(q_out + (size_t)v * MS, qo);
-        }
-    }
-    split_finalize<NT, SER>(a, want, red, &s_last, sbuf, CAP);
-}
-
 // the latest messages into send order before the loop, and both message
 // arrays back to position order after it
 template <int MS>

@@ -2056,20 +2056,14 @@ static SplitArgs split_args(bp_graph *g, uint32_t nparts) {
 // one block per 256 edges
 template <int MS, bool SER, int NV>
 static int split_run_nv(bp_graph *g, uint32_t k, uint32_t *nparts) {
-    // NV 4: the node pass with 4 lanes per node, else a thread per node
-    constexpr int G = NV == 4 ? 4 : 1;
     static int bps_a = 0, bps_b = 0;
     static std::mutex mu;
     {
         std::lock_guard<std::mutex> lock(mu);
         if (bps_a == 0) {
             BP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps_a, k_flood_send<MS, SER>, kSendThreads, 0));
-            if constexpr (G > 1)
-                BP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps_b, k_flood_nodes_group<MS, SER, G>,
-                                                                      kNodeThreads, 0));
-            else
-                BP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps_b, k_flood_nodes<MS, SER, NV>,
-                                                                      kNodeThreads, 0));
+            BP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps_b, k_flood_nodes<MS, SER, NV>,
+                                                                  kNodeThreads, 0));
             if (bps_a < 1 || bps_b < 1) return set_error(BP_ERR_CUDA, "split iteration kernels do not fit an SM");
         }
     }
@@ -2077,13 +2071,12 @@ static int split_run_nv(bp_graph *g, uint32_t k, uint32_t *nparts) {
     BP_CUDA(cudaGetDevice(&dev));
     BP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const unsigned ga = std::min<unsigned>((unsigned)(bps_a * sms), grid_for(g->E, kSendThreads));
-    const unsigned gb = std::min<unsigned>((unsigned)(bps_b * sms), grid_for((uint64_t)g->V * G, kNodeThreads));
+    const unsigned gb = std::min<unsigned>((unsigned)(bps_b * sms), grid_for(g->V, kNodeThreads));
     if (nparts) *nparts = ga;
     const SplitArgs a = split_args(g, ga);
     for (uint32_t i = 0; i < k; ++i) {
         k_flood_send<MS, SER><<<ga, kSendThreads, 0, g->stream>>>(a);
-        if constexpr (G > 1) k_flood_nodes_group<MS, SER, G><<<gb, kNodeThreads, 0, g->stream>>>(a);
-        else k_flood_nodes<MS, SER, NV><<<gb, kNodeThreads, 0, g->stream>>>(a);
+        k_flood_nodes<MS, SER, NV><<<gb, kNodeThreads, 0, g->stream>>>(a);
         BP_CUDA(cudaGetLastError());
     }
     return BP_OK;
@@ -2091,7 +2084,8 @@ static int split_run_nv(bp_graph *g, uint32_t k, uint32_t *nparts) {
 
 // BP_SPLIT_NODES=0|1|2: the node pass's load form (sweeps, 2-state graphs;
 // 1, the default, measured 0.859 ms per iteration against 0.876 for 0 and
-// 0.864 for 2 on the 16.8M-node graph)
+// 0.864 for 2 on the 16.8M-node graph; a group of 4 lanes per node, each
+// lane repeating the node's products, measured 2.06 ms and was removed)
 template <int MS, bool SER>
 static int split_run(bp_graph *g, uint32_t k, uint32_t *nparts) {
     if constexpr (MS == 2) {
@@ -2099,7 +2093,6 @@ static int split_run(bp_graph *g, uint32_t k, uint32_t *nparts) {
         const int nv = env ? atoi(env) : 1;
         if (nv == 0) return split_run_nv<MS, SER, 0>(g, k, nparts);
         if (nv == 2) return split_run_nv<MS, SER, 2>(g, k, nparts);
-        if (nv == 4) return split_run_nv<MS, SER, 4>(g, k, nparts);
         return split_run_nv<MS, SER, 1>(g, k, nparts);
     }
     return split_run_nv<MS, SER, 0>(g, k, nparts);

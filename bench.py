@@ -20,7 +20,11 @@ e2e    the same metric through the public C-ABI with host (pinned) buffers:
        and build on a second stream and host thread during step k's solve),
        timed by wall clock from the first upload to the last read.
 Multi-GPU: independent replicas, one per rank (weak scaling), no collective
-on the data path; the timing is the max over ranks.
+on the data path; the timing is the max over ranks.  --shard splits the one
+graph over the ranks by destination-node ranges instead.
+On one GPU the headline line also carries `other_configs`: the lines of the
+other workloads (random10k, tree, batched, unrolled, unrolled_batch), each
+run in a child process after the headline (--configs none skips them).
 """
 from __future__ import annotations
 
@@ -85,7 +89,41 @@ def parse():
                     help="unrolled_batch: the first N of the 256 grids (smaller profiling cases)")
     ap.add_argument("--solo-sample", type=int, default=256,
                     help="batched: networks solved one launch sequence each, for the comparison")
+    ap.add_argument("--configs", choices=["all", "none"], default="all",
+                    help="headline run on one GPU: also run every other workload (one child process each, "
+                         "after the headline's timed region) and attach their results under other_configs")
     return ap.parse_args()
+
+
+OTHER_WORKLOADS = ("random10k", "tree", "batched", "unrolled", "unrolled_batch")
+OTHER_KEYS = ("metric", "value", "unit", "ms_per_step", "steps", "warmup", "higher_is_better", "config", "clocks",
+              "max_abs_err_vs_oracle", "max_abs_err_vs_fp64", "fp64_iterations", "iterations", "roofline",
+              "cpu_baseline", "forward_ms", "fwd_bwd_over_fwd", "plain_forward_ms", "networks_per_s_fwd_bwd",
+              "gpu_launches")
+
+
+def run_other_configs(a):
+    """Every other workload, each as `bench.py --workload W` in a child
+    process on the same GPU (its own clock record), run after the headline's
+    timed region; returns {workload: the fields of its JSON line} (or the
+    error a workload ended with, which does not fail the headline)."""
+    out = {}
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "LOCAL_RANK", "WORLD_SIZE")}
+    for w in OTHER_WORKLOADS:
+        cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--workload", w, "--warmup", str(max(a.warmup, 3))]
+        t0 = time.time()
+        try:
+            r = subprocess.run(cmd, cwd=ROOT, env=env, capture_output=True, text=True, timeout=900)
+            lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+            if r.returncode != 0 or not lines:
+                out[w] = {"error": f"exit {r.returncode}: " + (r.stderr or r.stdout)[-300:]}
+            else:
+                d = json.loads(lines[-1])
+                out[w] = {k: d[k] for k in OTHER_KEYS if k in d}
+        except subprocess.TimeoutExpired:
+            out[w] = {"error": "did not finish in 900 s"}
+        out[w]["wall_s"] = round(time.time() - t0, 1)
+    return out
 
 
 def workload_name(a):
@@ -1076,6 +1114,10 @@ def main():
         except Exception as ex:  # reported, not fatal
             accuracy = {"error": str(ex)[:200]}
 
+    others = None
+    if rank == 0 and world == 1 and a.configs == "all":
+        others = run_other_configs(a)
+
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -1095,6 +1137,8 @@ def main():
         line.update({k: accuracy[k] for k in ("max_abs_err_vs_oracle", "max_abs_err_vs_fp64", "fp64_iterations")
                      if k in accuracy})
         line["accuracy"] = accuracy
+    if others is not None:
+        line["other_configs"] = others
     print(json.dumps(line), flush=True)
     return 0
 

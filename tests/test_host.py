@@ -212,6 +212,37 @@ def test_bench_arguments_and_algorithmic_bytes(monkeypatch):
         assert bench.parse().batch_delta == d
     assert bench.flood_bytes_per_iteration(1, 1, 2) == 44 + 28
     assert abs(bench.flood_bytes_per_iteration(1 << 24, 1 << 26, 2) - 3.42e9) < 0.01e9
+    assert a.configs == "all"
+
+
+def test_bench_other_configs_collects_each_workload_line(monkeypatch):
+    """The headline run's other_configs: one child `bench.py --workload W`
+    per other workload, the fields of its JSON line kept, a failed child
+    recorded as an error without failing the rest."""
+    import json
+    import subprocess
+    import sys
+    import bench
+    monkeypatch.setattr(sys, "argv", ["bench.py"])
+    a = bench.parse()
+    calls = []
+
+    def fake_run(cmd, **kw):
+        w = cmd[cmd.index("--workload") + 1]
+        calls.append((w, cmd[cmd.index("--warmup") + 1], kw["env"].get("RANK")))
+        if w == "tree":
+            return subprocess.CompletedProcess(cmd, 1, "", "boom")
+        line = {"metric": w, "value": 1.5, "unit": "u", "clocks": {"sm_mhz": 1965}, "noise": 0}
+        return subprocess.CompletedProcess(cmd, 0, "log line\n" + json.dumps(line) + "\n", "")
+
+    monkeypatch.setattr(subprocess, "run", fake_run)
+    monkeypatch.setenv("RANK", "0")
+    out = bench.run_other_configs(a)
+    assert [c[0] for c in calls] == list(bench.OTHER_WORKLOADS)
+    assert all(int(c[1]) >= 3 and c[2] is None for c in calls)
+    assert "boom" in out["tree"]["error"]
+    assert out["batched"]["value"] == 1.5 and out["batched"]["clocks"] == {"sm_mhz": 1965}
+    assert "noise" not in out["batched"] and "wall_s" in out["unrolled"]
 
 
 def test_status_codes_and_thread_local_errors():
