@@ -98,13 +98,20 @@ struct TreeData {
     uint32_t *level_wave_begin = nullptr; // host [num_levels + 1] index into waves
     uint32_t total_waves = 0;
     cudaGraphExec_t exec = nullptr;    // bp_tree's launch sequence, captured once
-    // out-edge order (q, the source-sorted CSR) arrays of the tree kernels, so
-    // a sending node reads its out-edges' tables and the destinations' level
-    // data as contiguous runs instead of at random positions:
+    // schedule order: k = a node's index in d_wave_nodes.  Per k (s_*), and
+    // per out-edge with the out-edges grouped by their source's k (q order,
+    // q_*), so the nodes of a wave read their records and out-edges as
+    // contiguous runs:
+    uint2 *s_in = nullptr;             // [V] in-edge range (positions) of node k
+    uint32_t *s_out = nullptr;         // [V + 1] out-edge range of node k in q order
+    uint32_t *s_lidx = nullptr;        // [V] index in its level
+    uint8_t *s_S = nullptr;            // [V] state count
     float *q_joint = nullptr;          // x-by-y tables (row stride y), each padded to 4 floats
     uint32_t *q_joff = nullptr;        // [E] float offset of out-edge q's table
     uint2 *q_lvidx = nullptr;          // [E] (level, index in level) of out-edge q's destination
     uint8_t *q_y = nullptr;            // [E] state count of out-edge q's destination
+    uint32_t *q_pos = nullptr;         // [E] message position of out-edge q
+    uint32_t *q_dst = nullptr;         // [E] destination of out-edge q
     uint32_t *d_wave_off = nullptr;    // device copy of wave_off (the cooperative tail launches)
     uint32_t *d_bar = nullptr;         // grid barrier of a tail launch: arrivals, generation, failure
 };

@@ -492,12 +492,9 @@ static void free_graph(bp_graph *g) {
     for (void *p : ptrs)
         if (p) cudaFreeAsync(p, g->stream);
     split_free(g);
-    void *tree_ptrs[] = {g->tree.d_node_level, g->tree.d_node_lidx, g->tree.d_wave_nodes};
-    for (void *p : tree_ptrs)
-        if (p) cudaFree(p);
+    tree_clear(g);
     for (auto &c : g->loop_graph)
         if (c.exec) cudaGraphExecDestroy(c.exec);
-    if (g->tree.exec) cudaGraphExecDestroy(g->tree.exec);
     if (g->stream) cudaStreamSynchronize(g->stream);
     release_pinned_ctl(g->ctl_host);
     if (g->ev0) cudaEventDestroy(g->ev0);
@@ -505,9 +502,6 @@ static void free_graph(bp_graph *g) {
     if (g->own_stream && g->stream) cudaStreamDestroy(g->stream);
     free(g->node_s_host);
     free(g->in_ptr_host);
-    free(g->tree.levels_host);
-    free(g->tree.wave_off);
-    free(g->tree.level_wave_begin);
     delete g;
 }
 

@@ -27,71 +27,101 @@
 
 namespace bpx {
 
-// Out-edges are walked in the source-sorted (q) order, whose per-edge arrays
-// (TreeData::q_*) put a node's out-edge tables, destination state counts and
-// destination level data next to each other; only the destination's visited
-// flag and the message store (at the edge's position) are random accesses.
+// Schedule order.  The nodes are listed wave by wave, level by level
+// (TreeData::d_wave_nodes); a node's index k in that list is its schedule
+// index, and a wave is a range of k.  Per node the kernels read records in
+// schedule order (TreeData::s_*: in-edge range, out-edge range, index in
+// level, state count), so the threads of a wave read them as contiguous
+// runs, and the out-edges are laid out by the source's schedule index
+// (TreeData::q_*: message position, destination, destination level data and
+// state count, dense table), so a wave's out-edge data is one contiguous
+// stream.  The random accesses left are the incoming messages, the message
+// stores (both in position order) and, at level 0, the beliefs.
+//
+// Who has been visited.  The graph.h calls keep the visited flags in
+// g->visited (mode 0).  bp_tree runs the whole schedule from cleared flags,
+// so the flags at node u's turn in level l are a function of the levels:
+// upward (mode 1) every node of a level below l, downward (mode 2) every node
+// of a level above l, and in both the nodes of l up to u's index; bp_tree
+// reads no flags and writes the final ones (levels >= 1) once at the end.
 
-// propagate_using_levels_start (graph.c:376-424)
+struct TreeArgs {
+    const uint32_t *nodes;            // schedule order -> node
+    const uint2 *s_in;                // [k] in-edge range (positions) of node k
+    const uint32_t *s_out;            // [k], [k + 1]: out-edge range (q order)
+    const uint32_t *s_lidx;           // [k] index in its level
+    const uint8_t *s_S;               // [k] state count
+    const uint32_t *q_pos, *q_dst;    // [q] message position, destination
+    const uint2 *q_lvidx;             // [q] destination (level, index in level)
+    const uint8_t *q_y;               // [q] destination state count
+    const uint32_t *q_joff;           // [q] offset of the dense table in q_joint
+    const float *q_joint;
+    const float *belief;
+    float *msg;
+    uint8_t *visited;
+};
+
+// has w (out-edge q, level data li) been visited at the turn of the node
+// with index my_idx in `level`?
+__device__ __forceinline__ bool tree_seen(const TreeArgs &a, int mode, uint32_t level, uint32_t my_idx, uint32_t q,
+                                          uint2 li) {
+    const bool earlier = li.x == level && li.y <= my_idx;
+    if (mode == 1) return li.x < level || earlier;
+    if (mode == 2) return li.x > level || earlier;
+    return a.visited[a.q_dst[q]] || earlier;
+}
+
+// propagate_using_levels_start (graph.c:376-424): level 0 is schedule
+// indices [k0, k0 + n); mark: set the visited flags (graph.h calls)
 template <int MS, bool UNI>
-__global__ void k_tree_start(const uint32_t *__restrict__ nodes, uint32_t n, const uint32_t *__restrict__ out_ptr,
-                             const uint32_t *__restrict__ out_pos, const uint8_t *__restrict__ node_s,
-                             const uint8_t *__restrict__ q_y, const uint32_t *__restrict__ q_joff,
-                             const float *__restrict__ q_joint, const float *__restrict__ belief,
-                             float *__restrict__ msg, uint8_t *__restrict__ visited) {
-    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    const uint32_t u = nodes[k];
-    visited[u] = 1;
-    const int x = UNI ? MS : node_s[u];
+__global__ void k_tree_start(const TreeArgs a, uint32_t k0, uint32_t n, int mark) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const uint32_t k = k0 + t;
+    const uint32_t u = a.nodes[k];
+    if (mark) a.visited[u] = 1;
+    const int x = UNI ? MS : a.s_S[k];
     float buf[MS];
-    ldv<MS>(belief + (size_t)u * MS, buf);
-    for (uint32_t q = out_ptr[u]; q < out_ptr[u + 1]; ++q) {
-        const uint32_t p = out_pos[q];
-        const int y = UNI ? MS : q_y[q];
+    ldv<MS>(a.belief + (size_t)u * MS, buf);
+    for (uint32_t q = a.s_out[k]; q < a.s_out[k + 1]; ++q) {
+        const uint32_t p = a.q_pos[q];
+        const int y = UNI ? MS : a.q_y[q];
         float m[MS];
-        send_msg_dense<MS, UNI>(q_joint + q_joff[q], buf, x, y, m);
-        stv<MS>(msg + (size_t)p * MS, m);
+        send_msg_dense<MS, UNI>(a.q_joint + a.q_joff[q], buf, x, y, m);
+        stv<MS>(a.msg + (size_t)p * MS, m);
     }
 }
 
-// one wave of propagate_node_using_levels (graph.c:461-522)
+// one wave of propagate_node_using_levels (graph.c:461-522): schedule
+// indices [k0, k0 + n) of `level`, a thread per node
 template <int MS, bool UNI>
-__global__ void k_tree_wave(const uint32_t *__restrict__ nodes, uint32_t n, uint32_t level,
-                            const uint32_t *__restrict__ in_ptr, const uint32_t *__restrict__ out_ptr,
-                            const uint32_t *__restrict__ out_pos, const uint32_t *__restrict__ out_dst,
-                            const uint2 *__restrict__ q_lvidx, const uint32_t *__restrict__ node_lidx,
-                            const uint8_t *__restrict__ node_s, const uint8_t *__restrict__ q_y,
-                            const uint32_t *__restrict__ q_joff, const float *__restrict__ q_joint,
-                            float *__restrict__ msg, const uint8_t *__restrict__ visited) {
+__global__ void k_tree_wave(const TreeArgs a, uint32_t k0, uint32_t n, uint32_t level, int mode) {
     griddep_launch_dependents();
-    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    // the schedule's arrays first (no tree kernel writes them), then the wait
-    // for the kernels ahead, whose messages and visited flags follow
-    const uint32_t u = nodes[k];
-    const int S = UNI ? MS : node_s[u];
-    const uint32_t my_idx = node_lidx[u];
-    const uint32_t r0 = in_ptr[u], r1 = in_ptr[u + 1], o0 = out_ptr[u], o1 = out_ptr[u + 1];
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    // the schedule's records first (no tree kernel writes them), then the
+    // wait for the kernels ahead, whose messages and visited flags follow
+    const uint32_t k = k0 + t;
+    const int S = UNI ? MS : a.s_S[k];
+    const uint32_t my_idx = a.s_lidx[k];
+    const uint2 r = a.s_in[k];
+    const uint32_t o0 = a.s_out[k], o1 = a.s_out[k + 1];
     griddep_wait();
     float buf[MS];
 #pragma unroll
     for (int i = 0; i < MS; ++i) buf[i] = (UNI || i < S) ? 1.0f : 0.0f;
-    for (uint32_t p = r0; p < r1; ++p) {
+    for (uint32_t p = r.x; p < r.y; ++p) {
         float mm[MS];
-        ldv<MS>(msg + (size_t)p * MS, mm);
+        ldv<MS>(a.msg + (size_t)p * MS, mm);
         combine<MS, UNI>(buf, mm, S);
     }
     for (uint32_t q = o0; q < o1; ++q) {
-        const uint32_t w = out_dst[q];
-        const uint2 li = q_lvidx[q];
-        const bool seen = visited[w] || (li.x == level && li.y <= my_idx);
-        if (seen) continue;
-        const uint32_t p = out_pos[q];
-        const int y = UNI ? MS : q_y[q];
+        if (tree_seen(a, mode, level, my_idx, q, a.q_lvidx[q])) continue;
+        const uint32_t p = a.q_pos[q];
+        const int y = UNI ? MS : a.q_y[q];
         float m[MS];
-        send_msg_dense<MS, UNI>(q_joint + q_joff[q], buf, S, y, m);
-        stv<MS>(msg + (size_t)p * MS, m);
+        send_msg_dense<MS, UNI>(a.q_joint + a.q_joff[q], buf, S, y, m);
+        stv<MS>(a.msg + (size_t)p * MS, m);
     }
 }
 
@@ -103,39 +133,33 @@ __global__ void k_tree_wave(const uint32_t *__restrict__ nodes, uint32_t n, uint
 // sends to the out-neighbours go out in parallel, one per lane.  A group's
 // lanes share the node, hence its trip counts, so the group mask is converged.
 template <int MS, bool UNI, int G>
-__global__ void k_tree_wave_group(const uint32_t *__restrict__ nodes, uint32_t n, uint32_t level,
-                                  const uint32_t *__restrict__ in_ptr, const uint32_t *__restrict__ out_ptr,
-                                  const uint32_t *__restrict__ out_pos, const uint32_t *__restrict__ out_dst,
-                                  const uint2 *__restrict__ q_lvidx, const uint32_t *__restrict__ node_lidx,
-                                  const uint8_t *__restrict__ node_s, const uint8_t *__restrict__ q_y,
-                                  const uint32_t *__restrict__ q_joff, const float *__restrict__ q_joint,
-                                  float *__restrict__ msg, const uint8_t *__restrict__ visited) {
+__global__ void k_tree_wave_group(const TreeArgs a, uint32_t k0, uint32_t n, uint32_t level, int mode) {
     static_assert(G >= 2 && G <= 32 && (G & (G - 1)) == 0, "group of 2..32 lanes");
-    const uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+    const uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) / G;
     const uint32_t lane = threadIdx.x & (G - 1);
     const uint32_t gmask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));
     griddep_launch_dependents();
-    if (k >= n) return;   // the whole group
-    // the schedule's arrays first (no tree kernel writes them): the node, its
-    // edge ranges, and this lane's first out-edge with its destination's
-    // level data and table (into L2 for the latency-bound small waves); then
-    // the wait for the kernels ahead, whose messages and visited flags follow
-    const uint32_t u = nodes[k];
-    const int S = UNI ? MS : node_s[u];
-    const uint32_t my_idx = node_lidx[u];
-    const uint32_t r0 = in_ptr[u], r1 = in_ptr[u + 1], o0 = out_ptr[u], o1 = out_ptr[u + 1];
+    if (t >= n) return;   // the whole group
+    // the schedule's records first (no tree kernel writes them): the node's
+    // ranges, and this lane's first out-edge with its destination's level data
+    // and table (into L2 for the latency-bound small waves); then the wait
+    // for the kernels ahead, whose messages and visited flags follow
+    const uint32_t k = k0 + t;
+    const int S = UNI ? MS : a.s_S[k];
+    const uint32_t my_idx = a.s_lidx[k];
+    const uint2 r = a.s_in[k];
+    const uint32_t o0 = a.s_out[k], o1 = a.s_out[k + 1];
     const uint32_t q0 = o0 + lane;
-    uint32_t w0 = 0, pp0 = 0, jo0 = 0;
+    uint32_t pp0 = 0, jo0 = 0;
     uint2 li0 = make_uint2(0u, 0u);
     int y0 = MS;
     if (q0 < o1) {
-        w0 = out_dst[q0];
-        pp0 = out_pos[q0];
-        li0 = q_lvidx[q0];
-        jo0 = q_joff[q0];
-        if (!UNI) y0 = q_y[q0];
+        pp0 = a.q_pos[q0];
+        li0 = a.q_lvidx[q0];
+        jo0 = a.q_joff[q0];
+        if (!UNI) y0 = a.q_y[q0];
         if constexpr (G >= 16) {
-            const float *jt = q_joint + jo0;
+            const float *jt = a.q_joint + jo0;
             prefetch_l2(jt);
             if constexpr (MS * MS > 32) prefetch_l2(jt + 32);
         }
@@ -144,12 +168,12 @@ __global__ void k_tree_wave_group(const uint32_t *__restrict__ nodes, uint32_t n
     float buf[MS];
 #pragma unroll
     for (int i = 0; i < MS; ++i) buf[i] = (UNI || i < S) ? 1.0f : 0.0f;
-    for (uint32_t p0 = r0; p0 < r1; p0 += G) {
+    for (uint32_t p0 = r.x; p0 < r.y; p0 += G) {
         float mm[MS];
 #pragma unroll
         for (int i = 0; i < MS; ++i) mm[i] = 0.0f;
-        if (p0 + lane < r1) ldv<MS>(msg + (size_t)(p0 + lane) * MS, mm);
-        const uint32_t cnt = min((uint32_t)G, r1 - p0);
+        if (p0 + lane < r.y) ldv<MS>(a.msg + (size_t)(p0 + lane) * MS, mm);
+        const uint32_t cnt = min((uint32_t)G, r.y - p0);
         for (uint32_t j = 0; j < cnt; ++j) {
             float mj[MS];
 #pragma unroll
@@ -159,15 +183,12 @@ __global__ void k_tree_wave_group(const uint32_t *__restrict__ nodes, uint32_t n
     }
     for (uint32_t q = q0; q < o1; q += G) {
         const bool first = q == q0;
-        const uint32_t w = first ? w0 : out_dst[q];
-        const uint2 li = first ? li0 : q_lvidx[q];
-        const bool seen = visited[w] || (li.x == level && li.y <= my_idx);
-        if (seen) continue;
-        const uint32_t p = first ? pp0 : out_pos[q];
-        const int y = UNI ? MS : (first ? y0 : (int)q_y[q]);
+        if (tree_seen(a, mode, level, my_idx, q, first ? li0 : a.q_lvidx[q])) continue;
+        const uint32_t p = first ? pp0 : a.q_pos[q];
+        const int y = UNI ? MS : (first ? y0 : (int)a.q_y[q]);
         float m[MS];
-        send_msg_dense<MS, UNI>(q_joint + (first ? jo0 : q_joff[q]), buf, S, y, m);
-        stv<MS>(msg + (size_t)p * MS, m);
+        send_msg_dense<MS, UNI>(a.q_joint + (first ? jo0 : a.q_joff[q]), buf, S, y, m);
+        stv<MS>(a.msg + (size_t)p * MS, m);
     }
 }
 
@@ -181,16 +202,10 @@ __global__ void k_tree_wave_group(const uint32_t *__restrict__ nodes, uint32_t n
 // whose wait runs out sets bar[2] and leaves, and the others leave at their
 // next barrier; bp_tree then returns BP_ERR_TIMEOUT.
 struct TreeTailArgs {
-    const uint32_t *wave_nodes, *wave_off;
+    TreeArgs t;
+    const uint32_t *wave_off;
     uint32_t w0, w1, level;
-    const uint32_t *in_ptr, *out_ptr, *out_pos, *out_dst;
-    const uint2 *q_lvidx;
-    const uint32_t *node_lidx;
-    const uint8_t *node_s, *q_y;
-    const uint32_t *q_joff;
-    const float *q_joint;
-    float *msg;
-    const uint8_t *visited;
+    int mode;
     uint32_t *bar;   // arrivals, generation, failure flag (zeroed before the launch)
 };
 
@@ -223,25 +238,27 @@ __device__ __forceinline__ bool tail_barrier(uint32_t *bar, uint32_t &gen, uint3
     return *s_fail == 0;
 }
 
-// one node of a wave with a warp (k_tree_wave_group's step, G = 32, the
-// incoming messages read through L2)
+// the node with schedule index k of a wave with a warp (k_tree_wave_group's
+// step, G = 32, the incoming messages read through L2)
 template <int MS, bool UNI>
-__device__ __forceinline__ void tail_node(const TreeTailArgs &a, uint32_t u, uint32_t lane) {
-    const int S = UNI ? MS : a.node_s[u];
-    const uint32_t my_idx = a.node_lidx[u];
-    const uint32_t r0 = a.in_ptr[u], r1 = a.in_ptr[u + 1], o0 = a.out_ptr[u], o1 = a.out_ptr[u + 1];
+__device__ __forceinline__ void tail_node(const TreeTailArgs &ta, uint32_t k, uint32_t lane) {
+    const TreeArgs &a = ta.t;
+    const int S = UNI ? MS : a.s_S[k];
+    const uint32_t my_idx = a.s_lidx[k];
+    const uint2 r = a.s_in[k];
+    const uint32_t o0 = a.s_out[k], o1 = a.s_out[k + 1];
     float buf[MS];
 #pragma unroll
     for (int i = 0; i < MS; ++i) buf[i] = (UNI || i < S) ? 1.0f : 0.0f;
-    for (uint32_t p0 = r0; p0 < r1; p0 += 32) {
+    for (uint32_t p0 = r.x; p0 < r.y; p0 += 32) {
         float mm[MS];
 #pragma unroll
         for (int i = 0; i < MS; ++i) mm[i] = 0.0f;
-        if (p0 + lane < r1) {
+        if (p0 + lane < r.y) {
 #pragma unroll
             for (int i = 0; i < MS; ++i) mm[i] = __ldcg(a.msg + (size_t)(p0 + lane) * MS + i);
         }
-        const uint32_t cnt = min(32u, r1 - p0);
+        const uint32_t cnt = min(32u, r.y - p0);
         for (uint32_t j = 0; j < cnt; ++j) {
             float mj[MS];
 #pragma unroll
@@ -250,11 +267,8 @@ __device__ __forceinline__ void tail_node(const TreeTailArgs &a, uint32_t u, uin
         }
     }
     for (uint32_t q = o0 + lane; q < o1; q += 32) {
-        const uint32_t w = a.out_dst[q];
-        const uint2 li = a.q_lvidx[q];
-        const bool seen = a.visited[w] || (li.x == a.level && li.y <= my_idx);
-        if (seen) continue;
-        const uint32_t p = a.out_pos[q];
+        if (tree_seen(a, ta.mode, ta.level, my_idx, q, a.q_lvidx[q])) continue;
+        const uint32_t p = a.q_pos[q];
         const int y = UNI ? MS : (int)a.q_y[q];
         float m[MS];
         send_msg_dense<MS, UNI>(a.q_joint + a.q_joff[q], buf, S, y, m);
@@ -272,51 +286,79 @@ __global__ void __launch_bounds__(256) k_tree_tail(const TreeTailArgs a) {
     uint32_t gen = 0;
     for (uint32_t w = a.w0; w < a.w1; ++w) {
         const uint32_t lo = a.wave_off[w], n = a.wave_off[w + 1] - lo;
-        for (uint32_t k = warp; k < n; k += nwarps) tail_node<MS, UNI>(a, a.wave_nodes[lo + k], lane);
+        for (uint32_t k = warp; k < n; k += nwarps) tail_node<MS, UNI>(a, lo + k, lane);
         if (w + 1 < a.w1 && !tail_barrier(a.bar, gen, &s_fail)) return;
     }
 }
 
-// ---- the out-edge order arrays (TreeData::q_*) ---------------------------
-// per out-edge: the destination's state count and the padded table size
-__global__ void k_tq_sizes(uint32_t V, const uint32_t *__restrict__ out_ptr, const uint32_t *__restrict__ out_dst,
-                           const uint8_t *__restrict__ node_s, uint8_t *__restrict__ q_y, uint32_t *__restrict__ size) {
-    const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
-    if (u >= V) return;
-    const uint32_t x = node_s[u];
-    for (uint32_t q = out_ptr[u]; q < out_ptr[u + 1]; ++q) {
-        const uint32_t y = node_s[out_dst[q]];
-        q_y[q] = (uint8_t)y;
-        size[q] = (x * y + 3u) & ~3u;
+// ---- the schedule-order arrays (TreeData::s_*, q_*) -----------------------
+// per schedule index: the node's in-edge range, index in level, state count
+// and out-degree (scanned into s_out)
+__global__ void k_ts_nodes(uint32_t V, const uint32_t *__restrict__ nodes, const uint32_t *__restrict__ in_ptr,
+                           const uint32_t *__restrict__ out_ptr, const uint32_t *__restrict__ node_lidx,
+                           const uint8_t *__restrict__ node_s, uint2 *__restrict__ s_in, uint32_t *__restrict__ s_lidx,
+                           uint8_t *__restrict__ s_S, uint32_t *__restrict__ deg) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= V) return;
+    const uint32_t u = nodes[k];
+    s_in[k] = make_uint2(in_ptr[u], in_ptr[u + 1]);
+    s_lidx[k] = node_lidx[u];
+    s_S[k] = node_s[u];
+    deg[k] = out_ptr[u + 1] - out_ptr[u];
+}
+
+// per out-edge in q order: the destination's state count and the padded
+// table size
+__global__ void k_tq_sizes(uint32_t V, const uint32_t *__restrict__ nodes, const uint32_t *__restrict__ s_out,
+                           const uint32_t *__restrict__ out_ptr, const uint32_t *__restrict__ out_dst,
+                           const uint8_t *__restrict__ node_s, uint8_t *__restrict__ q_y,
+                           uint32_t *__restrict__ size) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= V) return;
+    const uint32_t u = nodes[k], x = node_s[u], e0 = out_ptr[u], q0 = s_out[k], n = s_out[k + 1] - q0;
+    for (uint32_t j = 0; j < n; ++j) {
+        const uint32_t y = node_s[out_dst[e0 + j]];
+        q_y[q0 + j] = (uint8_t)y;
+        size[q0 + j] = (x * y + 3u) & ~3u;
     }
 }
 
-// the dense tables (rows of y floats, zero padding) and the destinations'
-// (level, index in level)
+// the dense tables (rows of y floats, zero padding), message positions,
+// destinations and the destinations' (level, index in level)
 template <int MS>
-__global__ void k_tq_fill(uint32_t V, const uint32_t *__restrict__ out_ptr, const uint32_t *__restrict__ out_pos,
+__global__ void k_tq_fill(uint32_t V, const uint32_t *__restrict__ nodes, const uint32_t *__restrict__ s_out,
+                          const uint32_t *__restrict__ out_ptr, const uint32_t *__restrict__ out_pos,
                           const uint32_t *__restrict__ out_dst, const uint8_t *__restrict__ node_s,
                           const uint8_t *__restrict__ q_y, const uint32_t *__restrict__ q_joff,
                           const float *__restrict__ joint, const uint32_t *__restrict__ node_level,
                           const uint32_t *__restrict__ node_lidx, float *__restrict__ q_joint,
-                          uint2 *__restrict__ q_lvidx) {
-    const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
-    if (u >= V) return;
-    const uint32_t x = node_s[u];
-    for (uint32_t q = out_ptr[u]; q < out_ptr[u + 1]; ++q) {
-        const uint32_t y = q_y[q], p = out_pos[q], w = out_dst[q];
+                          uint2 *__restrict__ q_lvidx, uint32_t *__restrict__ q_pos, uint32_t *__restrict__ q_dst) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= V) return;
+    const uint32_t u = nodes[k], x = node_s[u], e0 = out_ptr[u], q0 = s_out[k], n = s_out[k + 1] - q0;
+    for (uint32_t j = 0; j < n; ++j) {
+        const uint32_t q = q0 + j, y = q_y[q], p = out_pos[e0 + j], w = out_dst[e0 + j];
         float *dst = q_joint + q_joff[q];
         const float *src = joint + (size_t)p * (MS * MS);
         for (uint32_t i = 0; i < x; ++i)
-            for (uint32_t j = 0; j < y; ++j) dst[i * y + j] = src[i * MS + j];
-        for (uint32_t k = x * y; k < ((x * y + 3u) & ~3u); ++k) dst[k] = 0.0f;
+            for (uint32_t c = 0; c < y; ++c) dst[i * y + c] = src[i * MS + c];
+        for (uint32_t c = x * y; c < ((x * y + 3u) & ~3u); ++c) dst[c] = 0.0f;
         q_lvidx[q] = make_uint2(node_level[w], node_lidx[w]);
+        q_pos[q] = p;
+        q_dst[q] = w;
     }
 }
 
 __global__ void k_mark_visited(const uint32_t *__restrict__ nodes, uint32_t n, uint8_t *__restrict__ visited) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k < n) visited[nodes[k]] = 1;
+}
+
+// the flags the whole schedule leaves: cleared before the downward pass,
+// then set for every node of levels L-1 .. 1
+__global__ void k_final_visited(uint32_t V, const uint32_t *__restrict__ node_level, uint8_t *__restrict__ visited) {
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v < V) visited[v] = node_level[v] >= 1u ? 1 : 0;
 }
 
 // marginalize (graph.c:540-596): the belief is replaced by the product of
@@ -347,10 +389,9 @@ __global__ void k_tree_marginalize(uint32_t V, const uint32_t *__restrict__ in_p
 void tree_clear(bp_graph *g) {
     TreeData &t = g->tree;
     if (t.exec) cudaGraphExecDestroy(t.exec);
-    if (t.q_joint) cudaFree(t.q_joint);
-    if (t.q_joff) cudaFree(t.q_joff);
-    if (t.q_lvidx) cudaFree(t.q_lvidx);
-    if (t.q_y) cudaFree(t.q_y);
+    void *sched[] = {t.q_joint, t.q_joff, t.q_lvidx, t.q_y, t.q_pos, t.q_dst, t.s_in, t.s_out, t.s_lidx, t.s_S};
+    for (void *p : sched)
+        if (p) cudaFree(p);
     if (t.d_wave_off) cudaFree(t.d_wave_off);
     if (t.d_bar) cudaFree(t.d_bar);
     if (t.d_node_level) cudaFree(t.d_node_level);
@@ -406,7 +447,18 @@ int tree_prepare_host(bp_graph *g, const uint32_t *levels, uint32_t num_levels) 
     return BP_OK;
 }
 
-// the out-edge order arrays for the current levels (built once per level
+static int exclusive_scan(const uint32_t *in, uint32_t *out, int64_t n, cudaStream_t st) {
+    size_t temp = 0;
+    BP_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, temp, in, out, n, st));
+    void *tmp = nullptr;
+    BP_CUDA(cudaMallocAsync(&tmp, temp, st));
+    cudaError_t e = cub::DeviceScan::ExclusiveSum(tmp, temp, in, out, n, st);
+    cudaFreeAsync(tmp, st);
+    if (e != cudaSuccess) return cuda_fail(e, "DeviceScan::ExclusiveSum", __FILE__, __LINE__);
+    return BP_OK;
+}
+
+// the schedule-order arrays for the current levels (built once per level
 // lists, before any capture)
 template <int MS, bool UNI>
 static int tree_q_build(bp_graph *g) {
@@ -415,28 +467,34 @@ static int tree_q_build(bp_graph *g) {
     const uint32_t V = g->V, E = g->E;
     int st;
     if ((st = ensure_out_csr(g))) return st;
-    const size_t ne = E ? E : 1;
+    const size_t ne = E ? E : 1, nv = V ? V : 1;
+    BP_CUDA(cudaMalloc((void **)&t.s_in, sizeof(uint2) * nv));
+    BP_CUDA(cudaMalloc((void **)&t.s_out, sizeof(uint32_t) * (nv + 1)));
+    BP_CUDA(cudaMalloc((void **)&t.s_lidx, sizeof(uint32_t) * nv));
+    BP_CUDA(cudaMalloc((void **)&t.s_S, nv));
     BP_CUDA(cudaMalloc((void **)&t.q_y, ne));
     BP_CUDA(cudaMalloc((void **)&t.q_joff, sizeof(uint32_t) * (ne + 1)));
     BP_CUDA(cudaMalloc((void **)&t.q_lvidx, sizeof(uint2) * ne));
-    uint32_t *size = nullptr;
-    BP_CUDA(cudaMallocAsync((void **)&size, sizeof(uint32_t) * (ne + 1), g->stream));
-    BP_CUDA(cudaMemsetAsync(size, 0, sizeof(uint32_t) * (ne + 1), g->stream));
-    if (V) k_tq_sizes<<<grid_for(V, 256), 256, 0, g->stream>>>(V, g->out_ptr, g->out_dst, g->node_s, t.q_y, size);
+    BP_CUDA(cudaMalloc((void **)&t.q_pos, sizeof(uint32_t) * ne));
+    BP_CUDA(cudaMalloc((void **)&t.q_dst, sizeof(uint32_t) * ne));
+    uint32_t *cnt = nullptr;
+    BP_CUDA(cudaMallocAsync((void **)&cnt, sizeof(uint32_t) * (std::max(nv, ne) + 1), g->stream));
+    BP_CUDA(cudaMemsetAsync(cnt, 0, sizeof(uint32_t) * (std::max(nv, ne) + 1), g->stream));
+    if (V)
+        k_ts_nodes<<<grid_for(V, 256), 256, 0, g->stream>>>(V, t.d_wave_nodes, g->in_ptr, g->out_ptr, t.d_node_lidx,
+                                                            g->node_s, t.s_in, t.s_lidx, t.s_S, cnt);
     BP_CUDA(cudaGetLastError());
-    {
-        size_t temp = 0;
-        BP_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, temp, size, t.q_joff, (int64_t)E + 1, g->stream));
-        void *tmp = nullptr;
-        BP_CUDA(cudaMallocAsync(&tmp, temp, g->stream));
-        cudaError_t e = cub::DeviceScan::ExclusiveSum(tmp, temp, size, t.q_joff, (int64_t)E + 1, g->stream);
-        cudaFreeAsync(tmp, g->stream);
-        if (e != cudaSuccess) return cuda_fail(e, "DeviceScan::ExclusiveSum", __FILE__, __LINE__);
-    }
+    if ((st = exclusive_scan(cnt, t.s_out, (int64_t)V + 1, g->stream))) return st;
+    BP_CUDA(cudaMemsetAsync(cnt, 0, sizeof(uint32_t) * (ne + 1), g->stream));
+    if (V)
+        k_tq_sizes<<<grid_for(V, 256), 256, 0, g->stream>>>(V, t.d_wave_nodes, t.s_out, g->out_ptr, g->out_dst,
+                                                            g->node_s, t.q_y, cnt);
+    BP_CUDA(cudaGetLastError());
+    if ((st = exclusive_scan(cnt, t.q_joff, (int64_t)E + 1, g->stream))) return st;
     uint32_t total = 0;
     BP_CUDA(cudaMemcpyAsync(&total, t.q_joff + E, sizeof(uint32_t), cudaMemcpyDeviceToHost, g->stream));
     BP_CUDA(cudaStreamSynchronize(g->stream));
-    cudaFreeAsync(size, g->stream);
+    cudaFreeAsync(cnt, g->stream);
     BP_CUDA(cudaMalloc((void **)&t.q_joint, sizeof(float) * ((size_t)total + 4)));
     BP_CUDA(cudaMalloc((void **)&t.d_wave_off, sizeof(uint32_t) * ((size_t)t.total_waves + 1)));
     BP_CUDA(cudaMemcpy(t.d_wave_off, t.wave_off, sizeof(uint32_t) * ((size_t)t.total_waves + 1),
@@ -444,24 +502,43 @@ static int tree_q_build(bp_graph *g) {
     BP_CUDA(cudaMalloc((void **)&t.d_bar, 4 * sizeof(uint32_t)));
     BP_CUDA(cudaMemset(t.d_bar, 0, 4 * sizeof(uint32_t)));
     if (V)
-        k_tq_fill<MS><<<grid_for(V, 256), 256, 0, g->stream>>>(V, g->out_ptr, g->out_pos, g->out_dst, g->node_s,
-                                                               t.q_y, t.q_joff, g->joint, t.d_node_level,
-                                                               t.d_node_lidx, t.q_joint, t.q_lvidx);
+        k_tq_fill<MS><<<grid_for(V, 256), 256, 0, g->stream>>>(V, t.d_wave_nodes, t.s_out, g->out_ptr, g->out_pos,
+                                                               g->out_dst, g->node_s, t.q_y, t.q_joff, g->joint,
+                                                               t.d_node_level, t.d_node_lidx, t.q_joint, t.q_lvidx,
+                                                               t.q_pos, t.q_dst);
     BP_CUDA(cudaGetLastError());
     BP_CUDA(cudaStreamSynchronize(g->stream));
     return BP_OK;
 }
 
+static TreeArgs tree_args(bp_graph *g) {
+    TreeData &t = g->tree;
+    TreeArgs a;
+    a.nodes = t.d_wave_nodes;
+    a.s_in = t.s_in;
+    a.s_out = t.s_out;
+    a.s_lidx = t.s_lidx;
+    a.s_S = t.s_S;
+    a.q_pos = t.q_pos;
+    a.q_dst = t.q_dst;
+    a.q_lvidx = t.q_lvidx;
+    a.q_y = t.q_y;
+    a.q_joff = t.q_joff;
+    a.q_joint = t.q_joint;
+    a.belief = g->belief;
+    a.msg = g->msg[0];
+    a.visited = g->visited;
+    return a;
+}
+
+// mark: set the level-0 visited flags (graph.h calls; bp_tree derives them)
 template <int MS, bool UNI>
-static int launch_start(bp_graph *g) {
+static int launch_start(bp_graph *g, int mark) {
     TreeData &t = g->tree;
     const uint32_t w0 = t.level_wave_begin[0], w1 = t.level_wave_begin[1];
     if (w1 == w0) return BP_OK;
-    const uint32_t lo = t.wave_off[w0], hi = t.wave_off[w1];
-    const uint32_t n = hi - lo;
-    k_tree_start<MS, UNI><<<grid_for(n, 128), 128, 0, g->stream>>>(t.d_wave_nodes + lo, n, g->out_ptr, g->out_pos,
-                                                                    g->node_s, t.q_y, t.q_joff, t.q_joint,
-                                                                    g->belief, g->msg[0], g->visited);
+    const uint32_t lo = t.wave_off[w0], n = t.wave_off[w1] - lo;
+    k_tree_start<MS, UNI><<<grid_for(n, 128), 128, 0, g->stream>>>(tree_args(g), lo, n, mark);
     BP_CUDA(cudaGetLastError());
     return BP_OK;
 }
@@ -517,13 +594,9 @@ static cudaError_t launch_wave(void (*kern)(KArgs...), unsigned grid, cudaStream
 }
 
 template <int MS, bool UNI, int G>
-static cudaError_t launch_wave_group(bp_graph *g, const uint32_t *nodes, uint32_t n, uint32_t level) {
-    TreeData &t = g->tree;
-    return launch_wave(k_tree_wave_group<MS, UNI, G>, grid_for((uint64_t)n * G, 128), g->stream, nodes, n, level,
-                       (const uint32_t *)g->in_ptr, (const uint32_t *)g->out_ptr, (const uint32_t *)g->out_pos,
-                       (const uint32_t *)g->out_dst, (const uint2 *)t.q_lvidx, (const uint32_t *)t.d_node_lidx,
-                       (const uint8_t *)g->node_s, (const uint8_t *)t.q_y, (const uint32_t *)t.q_joff,
-                       (const float *)t.q_joint, g->msg[0], (const uint8_t *)g->visited);
+static cudaError_t launch_wave_group(bp_graph *g, uint32_t k0, uint32_t n, uint32_t level, int mode) {
+    return launch_wave(k_tree_wave_group<MS, UNI, G>, grid_for((uint64_t)n * G, 128), g->stream, tree_args(g), k0, n,
+                       level, mode);
 }
 
 // BP_TREE_TAIL=1 runs each run of warp-per-node waves as one cooperative
@@ -539,7 +612,7 @@ static bool tree_tail_on() {
 // waves [wa, wb) of `level` (every one a warp per node) as one cooperative
 // launch of k_tree_tail
 template <int MS, bool UNI>
-static int launch_tail(bp_graph *g, uint32_t level, uint32_t wa, uint32_t wb) {
+static int launch_tail(bp_graph *g, uint32_t level, uint32_t wa, uint32_t wb, int mode) {
     TreeData &t = g->tree;
     static int bps = 0;
     if (!bps) BP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_tree_tail<MS, UNI>, 256, 0));
@@ -551,23 +624,12 @@ static int launch_tail(bp_graph *g, uint32_t level, uint32_t wa, uint32_t wb) {
     const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)bps * sms,
                                                                            ((uint64_t)nmax * 32 + 255) / 256));
     TreeTailArgs a;
-    a.wave_nodes = t.d_wave_nodes;
+    a.t = tree_args(g);
     a.wave_off = t.d_wave_off;
     a.w0 = wa;
     a.w1 = wb;
     a.level = level;
-    a.in_ptr = g->in_ptr;
-    a.out_ptr = g->out_ptr;
-    a.out_pos = g->out_pos;
-    a.out_dst = g->out_dst;
-    a.q_lvidx = t.q_lvidx;
-    a.node_lidx = t.d_node_lidx;
-    a.node_s = g->node_s;
-    a.q_y = t.q_y;
-    a.q_joff = t.q_joff;
-    a.q_joint = t.q_joint;
-    a.msg = g->msg[0];
-    a.visited = g->visited;
+    a.mode = mode;
     a.bar = t.d_bar;
     // arrivals and generation restart at zero; a failure flag set by an
     // earlier launch stays set for bp_tree to report
@@ -585,8 +647,11 @@ static int launch_tail(bp_graph *g, uint32_t level, uint32_t wa, uint32_t wb) {
     return BP_OK;
 }
 
+// the waves of `level`; mode 0 (graph.h calls) reads and then sets the
+// visited flags, modes 1 and 2 (bp_tree's upward and downward passes) derive
+// them from the levels
 template <int MS, bool UNI>
-static int launch_level(bp_graph *g, uint32_t level) {
+static int launch_level(bp_graph *g, uint32_t level, int mode) {
     TreeData &t = g->tree;
     const uint32_t w0 = t.level_wave_begin[level], w1 = t.level_wave_begin[level + 1];
     for (uint32_t w = w0; w < w1; ++w) {
@@ -597,31 +662,25 @@ static int launch_level(bp_graph *g, uint32_t level) {
             uint32_t we = w + 1;
             while (we < w1 && wave_group(t.wave_off[we + 1] - t.wave_off[we]) == 32) ++we;
             if (we - w >= 2) {
-                int st = launch_tail<MS, UNI>(g, level, w, we);
+                int st = launch_tail<MS, UNI>(g, level, w, we, mode);
                 if (st) return st;
                 w = we - 1;
                 continue;
             }
         }
-        const uint32_t *nodes = t.d_wave_nodes + lo;
         cudaError_t le;
         switch (wave_group(n)) {
-        case 32: le = launch_wave_group<MS, UNI, 32>(g, nodes, n, level); break;
-        case 16: le = launch_wave_group<MS, UNI, 16>(g, nodes, n, level); break;
-        case 8: le = launch_wave_group<MS, UNI, 8>(g, nodes, n, level); break;
-        case 4: le = launch_wave_group<MS, UNI, 4>(g, nodes, n, level); break;
-        case 2: le = launch_wave_group<MS, UNI, 2>(g, nodes, n, level); break;
-        default:
-            le = launch_wave(k_tree_wave<MS, UNI>, grid_for(n, 128), g->stream, nodes, n, level,
-                             (const uint32_t *)g->in_ptr, (const uint32_t *)g->out_ptr, (const uint32_t *)g->out_pos,
-                             (const uint32_t *)g->out_dst, (const uint2 *)t.q_lvidx, (const uint32_t *)t.d_node_lidx,
-                             (const uint8_t *)g->node_s, (const uint8_t *)t.q_y, (const uint32_t *)t.q_joff,
-                             (const float *)t.q_joint, g->msg[0], (const uint8_t *)g->visited);
+        case 32: le = launch_wave_group<MS, UNI, 32>(g, lo, n, level, mode); break;
+        case 16: le = launch_wave_group<MS, UNI, 16>(g, lo, n, level, mode); break;
+        case 8: le = launch_wave_group<MS, UNI, 8>(g, lo, n, level, mode); break;
+        case 4: le = launch_wave_group<MS, UNI, 4>(g, lo, n, level, mode); break;
+        case 2: le = launch_wave_group<MS, UNI, 2>(g, lo, n, level, mode); break;
+        default: le = launch_wave(k_tree_wave<MS, UNI>, grid_for(n, 128), g->stream, tree_args(g), lo, n, level, mode);
         }
         if (le != cudaSuccess) return cuda_fail(le, "cudaLaunchKernelEx", __FILE__, __LINE__);
         BP_CUDA(cudaGetLastError());
     }
-    if (w1 > w0) {
+    if (w1 > w0 && mode == 0) {
         const uint32_t lo = t.wave_off[w0], n = t.wave_off[w1] - lo;
         k_mark_visited<<<grid_for(n, 256), 256, 0, g->stream>>>(t.d_wave_nodes + lo, n, g->visited);
         BP_CUDA(cudaGetLastError());
@@ -639,8 +698,10 @@ static int launch_marginalize(bp_graph *g) {
 }
 
 static int dispatch_q_build(bp_graph *g) { BP_DISPATCH_MS(g->ms, g->uniform != 0, tree_q_build, g); }
-static int dispatch_start(bp_graph *g) { BP_DISPATCH_MS(g->ms, g->uniform != 0, launch_start, g); }
-static int dispatch_level(bp_graph *g, uint32_t l) { BP_DISPATCH_MS(g->ms, g->uniform != 0, launch_level, g, l); }
+static int dispatch_start(bp_graph *g, int mark) { BP_DISPATCH_MS(g->ms, g->uniform != 0, launch_start, g, mark); }
+static int dispatch_level(bp_graph *g, uint32_t l, int mode) {
+    BP_DISPATCH_MS(g->ms, g->uniform != 0, launch_level, g, l, mode);
+}
 static int dispatch_marginalize(bp_graph *g) { BP_DISPATCH_MS(g->ms, g->uniform != 0, launch_marginalize, g); }
 
 }  // namespace bpx
@@ -683,7 +744,7 @@ int bp_tree_start(bp_graph *g) {
     if (!g) return set_error(BP_ERR_INVALID, "null graph");
     if (!g->tree.ready) return set_error(BP_ERR_STATE, "tree levels not set");
     int st = dispatch_q_build(g);
-    return st ? st : dispatch_start(g);
+    return st ? st : dispatch_start(g, 1);
 }
 
 int bp_tree_level(bp_graph *g, uint32_t level) {
@@ -692,7 +753,7 @@ int bp_tree_level(bp_graph *g, uint32_t level) {
     if (level >= g->tree.num_levels) return set_error(BP_ERR_INVALID, "level %u >= num_levels %u", level,
                                                       g->tree.num_levels);
     int st = dispatch_q_build(g);
-    return st ? st : dispatch_level(g, level);
+    return st ? st : dispatch_level(g, level, 0);
 }
 
 int bp_tree_reset_visited(bp_graph *g) {
@@ -706,18 +767,25 @@ int bp_tree_marginalize(bp_graph *g) {
     return dispatch_marginalize(g);
 }
 
-// the whole schedule of c_benchmark/main.c:224-236 on the graph's stream
+// the whole schedule of c_benchmark/main.c:224-236 on the graph's stream:
+// reset_visited, start, levels 1 .. L-2, reset_visited, levels L-1 .. 1,
+// marginalize.  The visited flags of each step follow from the levels
+// (modes 1 and 2 of launch_level); the flags the schedule leaves are written
+// at the end.
 static int tree_enqueue(bp_graph *g) {
     int st;
     const uint32_t L = g->tree.num_levels;
-    if ((st = bp_tree_reset_visited(g))) return st;
-    if ((st = dispatch_start(g))) return st;
+    if ((st = dispatch_start(g, 0))) return st;
     for (uint32_t l = 1; l + 1 < L; ++l)
-        if ((st = dispatch_level(g, l))) return st;
-    if ((st = bp_tree_reset_visited(g))) return st;
+        if ((st = dispatch_level(g, l, 1))) return st;
     for (uint32_t l = L - 1; l > 0; --l)
-        if ((st = dispatch_level(g, l))) return st;
-    return dispatch_marginalize(g);
+        if ((st = dispatch_level(g, l, 2))) return st;
+    if ((st = dispatch_marginalize(g))) return st;
+    if (g->V) {
+        k_final_visited<<<grid_for(g->V, 256), 256, 0, g->stream>>>(g->V, g->tree.d_node_level, g->visited);
+        BP_CUDA(cudaGetLastError());
+    }
+    return BP_OK;
 }
 
 int bp_tree(bp_graph *g, bp_tree_result *res) {

@@ -179,3 +179,64 @@ def test_tree_small_waves_in_one_launch(bp, synth, restatement, O, monkeypatch, 
     for r in (coop, sep):
         np.testing.assert_array_equal(r["beliefs"], ora["beliefs"][:, :S])
         np.testing.assert_array_equal(r["messages"][:, :S], ora["messages"][:, :S])
+
+
+def _visited(g):
+    import ctypes as C
+    from belief_propagation_b200 import native as N
+    out = np.zeros(g.V, np.uint8)
+    N.check(g.lib.bp_get_visited(g.h, C.c_void_p(out.ctypes.data)))
+    return out
+
+
+@pytest.mark.parametrize("case", ["mixed_tree", "cycles", "path"])
+def test_tree_whole_schedule_matches_step_calls(bp, synth, case):
+    """bp_tree derives each step's visited flags from the levels; the graph.h
+    steps (start, levels 1 .. L-2, reset_visited, levels L-1 .. 1,
+    marginalize) read and write the flags.  Both leave the same messages,
+    beliefs and visited flags, after stale flags were set beforehand."""
+    from belief_propagation_b200.engine import BPGraph
+    import ctypes as C
+    from belief_propagation_b200 import native as N
+    if case == "mixed_tree":
+        net = synth.random_tree(4000, (2, 3, 4, 8), 0.05, seed=21)
+    elif case == "path":
+        net = _path_network(synth, 300, seed=3)
+    else:
+        net = None
+        for seed in range(5, 40):
+            cand = synth.random_loopy(600, 1500, 2, 0.1, seed=seed)
+            g = BPGraph.from_network(cand)
+            try:
+                g.build_levels()
+                net = cand
+                break
+            except Exception:
+                continue
+            finally:
+                g.close()
+        assert net is not None
+    rng = np.random.default_rng(0)
+    stale = (rng.random(net.V) < 0.5).astype(np.uint8)
+    res = []
+    for whole in (True, False):
+        g = BPGraph.from_network(net)
+        try:
+            lv, L = g.build_levels()
+            N.check(g.lib.bp_set_visited(g.h, C.c_void_p(stale.ctypes.data)))
+            if whole:
+                g.tree()
+            else:
+                g.tree_reset_visited()
+                g.tree_start()
+                for l in range(1, L - 1):
+                    g.tree_level(l)
+                g.tree_reset_visited()
+                for l in range(L - 1, 0, -1):
+                    g.tree_level(l)
+                g.tree_marginalize()
+            res.append((g.messages(0), g.beliefs(), _visited(g)))
+        finally:
+            g.close()
+    for a, b in zip(*res):
+        np.testing.assert_array_equal(a, b)
