@@ -202,23 +202,33 @@ __global__ void k_out_degree(const uint32_t *__restrict__ src, uint32_t E, uint3
     if (e < E) atomicAdd(deg + src[e], 1u);
 }
 
-__global__ void k_degree_keys(uint32_t *__restrict__ deg, uint32_t V, uint32_t *__restrict__ iota) {
+// sort keys: decreasing out-degree; with indeg, then increasing in-degree
+// (both clamped to 16 bits), so the 32 nodes of a warp have similar in-degrees
+// and the node pass's per-node loops diverge less
+__global__ void k_degree_keys(uint32_t *__restrict__ deg, const uint32_t *__restrict__ indeg, uint32_t V,
+                              uint32_t *__restrict__ iota) {
     uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= V) return;
-    deg[v] = 0xffffffffu - deg[v];
+    if (indeg) deg[v] = ((0xffffu - min(deg[v], 0xffffu)) << 16) | min(indeg[v], 0xffffu);
+    else deg[v] = 0xffffffffu - deg[v];
     iota[v] = (uint32_t)v;
 }
 
-// number of sorted keys (0xffffffff - out-degree, ascending) of nodes with
-// out-degree >= 2
-__global__ void k_count_reused(const uint32_t *__restrict__ keys, uint32_t V, uint32_t *__restrict__ out) {
+// number of sorted keys below `limit` (the keys of out-degree >= 2 nodes)
+__global__ void k_count_reused(const uint32_t *__restrict__ keys, uint32_t V, uint32_t limit, uint32_t *__restrict__ out) {
     uint32_t lo = 0, hi = V;
     while (lo < hi) {
         const uint32_t mid = lo + (hi - lo) / 2;
-        if (keys[mid] <= 0xffffffffu - 2u) lo = mid + 1;
+        if (keys[mid] < limit) lo = mid + 1;
         else hi = mid;
     }
     *out = lo;
+}
+
+// BP_REORDER_INDEG=1: renumbering breaks out-degree ties by in-degree
+static bool reorder_by_indegree() {
+    const char *env = getenv("BP_REORDER_INDEG");
+    return env && env[0] == '1';
 }
 
 __global__ void k_invert_perm(const uint32_t *__restrict__ new_to_old, uint32_t V, uint32_t *__restrict__ old_to_new) {
@@ -645,7 +655,13 @@ static int create_impl(bp_graph *g, const bp_graph_desc *d) {
         trace.mark("renumber: allocate");
         BP_CUDA(cudaMemsetAsync(deg, 0, sizeof(uint32_t) * V, g->stream));
         if (E) k_out_degree<<<grid_for(E, 256), 256, 0, g->stream>>>((const uint32_t *)src, E, deg);
-        if (V) k_degree_keys<<<grid_for(V, 256), 256, 0, g->stream>>>(deg, V, iota);
+        const bool by_in = reorder_by_indegree();
+        if (by_in) {
+            // the in-degree histogram in old_to_new (filled later)
+            BP_CUDA(cudaMemsetAsync(old_to_new, 0, sizeof(uint32_t) * V, g->stream));
+            if (E) k_out_degree<<<grid_for(E, 256), 256, 0, g->stream>>>((const uint32_t *)dst, E, old_to_new);
+        }
+        if (V) k_degree_keys<<<grid_for(V, 256), 256, 0, g->stream>>>(deg, by_in ? old_to_new : nullptr, V, iota);
         BP_CUDA(cudaGetLastError());
         if (V) {
             size_t temp = 0;
@@ -658,7 +674,7 @@ static int create_impl(bp_graph *g, const bp_graph_desc *d) {
             cudaFreeAsync(tmp, g->stream);
             if (se != cudaSuccess) return cuda_fail(se, "DeviceRadixSort::SortPairs", __FILE__, __LINE__);
             k_invert_perm<<<grid_for(V, 256), 256, 0, g->stream>>>(g->new_to_old, V, old_to_new);
-            k_count_reused<<<1, 1, 0, g->stream>>>(keys, V, deg);
+            k_count_reused<<<1, 1, 0, g->stream>>>(keys, V, by_in ? 0xfffe0000u : 0xfffffffeu, deg);
             BP_CUDA(cudaMemcpyAsync(&g->reuse_nodes, deg, sizeof(uint32_t), cudaMemcpyDeviceToHost, g->stream));
         }
         trace.mark("renumber: degree sort");
@@ -825,6 +841,26 @@ int bp_release_cached_memory(void) {
     BP_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
     BP_CUDA(cudaDeviceSynchronize());
     BP_CUDA(cudaMemPoolTrimTo(pool, 0));
+    return BP_OK;
+}
+
+int bp_reserve_cached_memory(uint64_t bytes) {
+    int dev = 0;
+    BP_CUDA(cudaGetDevice(&dev));
+    ensure_pool(dev);
+    cudaMemPool_t pool;
+    BP_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
+    uint64_t held = 0;
+    BP_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &held));
+    if (held >= bytes) return BP_OK;
+    cudaStream_t st = nullptr;
+    BP_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    void *p = nullptr;
+    cudaError_t e = cudaMallocFromPoolAsync(&p, bytes - held, pool, st);
+    if (e == cudaSuccess) e = cudaFreeAsync(p, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+    if (e != cudaSuccess) return cuda_fail(e, "reserving pool memory", __FILE__, __LINE__);
     return BP_OK;
 }
 

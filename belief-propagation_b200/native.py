@@ -105,7 +105,7 @@ BP_SYMBOLS = [
     "bp_loopy_default_options", "bp_init_messages", "bp_loopy", "bp_tree_build_levels",
     "bp_tree_set_levels", "bp_tree_start", "bp_tree_level", "bp_tree_reset_visited",
     "bp_tree_marginalize", "bp_tree", "bp_set_visited", "bp_get_visited", "bp_set_sync_mode",
-    "bp_sync_host", "bp_graph_of", "bp_loopy_noalloc", "bp_release_cached_memory", "bp_batch_create", "bp_batch_destroy",
+    "bp_sync_host", "bp_graph_of", "bp_loopy_noalloc", "bp_release_cached_memory", "bp_reserve_cached_memory", "bp_batch_create", "bp_batch_destroy",
     "bp_batch_layout", "bp_batch_set_beliefs", "bp_batch_get_beliefs", "bp_batch_get_messages",
     "bp_batch_default_options", "bp_batch_autotune", "bp_batch_get_block_threads", "bp_batch_loopy",
     "bp_batch_network_results", "bp_unrolled_create", "bp_unrolled_destroy", "bp_unrolled_set_stream",
@@ -155,7 +155,7 @@ def load(path=LIB_PATH):
         "bp_tree_marginalize": ([vp], i32), "bp_tree": ([vp, C.POINTER(TreeResult)], i32),
         "bp_set_visited": ([vp, vp], i32), "bp_get_visited": ([vp, vp], i32),
         "bp_set_sync_mode": ([vp, i32], i32), "bp_sync_host": ([vp], i32),
-        "bp_graph_of": ([vp, C.POINTER(vp)], i32), "bp_release_cached_memory": ([], i32),
+        "bp_graph_of": ([vp, C.POINTER(vp)], i32), "bp_release_cached_memory": ([], i32), "bp_reserve_cached_memory": ([C.c_uint64], i32),
         "bp_loopy_noalloc": ([u32, u32, u32, vp, vp, vp, vp, vp, i32, i32, C.c_float, u32, vp,
                               C.POINTER(LoopyResult), C.POINTER(i32)], i32),
         "bp_batch_create": ([C.POINTER(vp), u32, C.POINTER(GraphDesc), vp], i32),

@@ -18,7 +18,9 @@ e2e    the same metric through the public C-ABI with host (pinned) buffers:
        destination-sorted layout on the GPU, runs, and reads the beliefs back;
        the steps are pipelined as a serving loop runs them (step k+1's upload
        and build on a second stream and host thread during step k's solve),
-       timed by wall clock from the first upload to the last read.
+       timed by wall clock from the first upload to the last read; the
+       median of three such runs.  The loop reserves its device memory once
+       at start-up (bp_reserve_cached_memory).
 Multi-GPU: independent replicas, one per rank (weak scaling), no collective
 on the data path; the timing is the max over ranks.  --shard splits the one
 graph over the ranks by destination-node ranges instead.
@@ -1020,6 +1022,7 @@ def main():
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic, "kernel": "k_flood<2,true>", "peak_source": peak_src,
                 "algorithmic_bytes_per_launch": algo, "launch_ms": it_ms}
+    graph_bytes = g.device_bytes()
     g.close()
     del prior
     torch.cuda.empty_cache()
@@ -1032,6 +1035,12 @@ def main():
         out_h = torch.empty((V, S), dtype=torch.float32).pin_memory()
 
         phases = {"create_ms": 0.0, "solve_ms": 0.0, "read_ms": 0.0, "destroy_ms": 0.0}
+        # the serving loop's memory reservation, made once at start-up: room
+        # for a graph solving, the next one building, its temporaries, and
+        # slack for the pool's fragmentation
+        from belief_propagation_b200 import native as N
+        reserve = 12 * int(graph_bytes)
+        N.check(N.load().bp_reserve_cached_memory(reserve))
 
         def e2e_step(record=False):
             t0 = time.perf_counter()
@@ -1089,16 +1098,22 @@ def main():
 
         pipelined(2)
         barrier()
-        t0 = time.perf_counter()
-        pipelined(a.e2e_steps)
-        barrier()
-        ems = (time.perf_counter() - t0) / a.e2e_steps * 1e3
-        ems = max_over_ranks(ems, dist)
+        # three timed runs of e2e_steps steps each; the median run is the number
+        runs = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            pipelined(a.e2e_steps)
+            barrier()
+            runs.append((time.perf_counter() - t0) / a.e2e_steps * 1e3)
+        ems = max_over_ranks(sorted(runs)[1], dist)
         e2e = {"value": float(E) * a.iterations * world / (ems / 1e3), "unit": UNIT,
                "h2d_bytes_per_step": int(E * (4 + 4 + 4 * S * S) + V * 4 * S), "d2h_bytes_per_step": int(V * 4 * S),
-               "ms_per_step": ems, "steps": a.e2e_steps, "timing": "wall clock over all steps, first build included",
+               "ms_per_step": ems, "steps": a.e2e_steps,
+               "timing": "wall clock over all steps, first build included; median of 3 runs",
+               "runs_ms_per_step": [round(r, 2) for r in runs],
                "pipelined": "the build of step k+1 (its H2D copies included) overlaps the solve of step k",
                "sequential_ms_per_step": round(max_over_ranks(seq_ms, dist), 2),
+               "pool_reserved_bytes": reserve,
                "phases_wall_ms": {k: round(v, 2) for k, v in phases.items()}}
 
     cpu = None

@@ -153,6 +153,14 @@ int bp_graph_device_bytes(const bp_graph *g, uint64_t *bytes);
  * reuses it without cudaMalloc/cudaFree); this returns the cached memory to
  * the driver. */
 int bp_release_cached_memory(void);
+/* Grows that pool, once, to hold at least `bytes` (one block allocated and
+ * freed at once), so that graphs built later carve their buffers out of the
+ * reservation.  For serving loops that build and destroy graphs while others
+ * solve: the pool otherwise grows in the middle of a build whenever no cached
+ * block fits, and on a B200 such growth stalled a build (and a solve on
+ * another stream) for up to a second.  No effect when the pool already holds
+ * `bytes`; bp_release_cached_memory() gives the memory back. */
+int bp_reserve_cached_memory(uint64_t bytes);
 
 /* ---- state ----------------------------------------------------------- */
 int bp_set_beliefs(bp_graph *g, const float *beliefs, uint32_t ld, int memory);

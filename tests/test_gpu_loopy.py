@@ -262,7 +262,7 @@ def headline_sample(synth, O):
     return net, out
 
 
-@pytest.mark.parametrize("path", ["block", "split"])
+@pytest.mark.parametrize("path", ["block", "block_indeg", "split"])
 @pytest.mark.parametrize("iterations", [10, 100])
 def test_loopy_headline_path_bit_exact(bp, headline_sample, monkeypatch, iterations, path):
     """The benchmark's code paths -- nodes renumbered by out-degree, fp64
@@ -270,19 +270,22 @@ def test_loopy_headline_path_bit_exact(bp, headline_sample, monkeypatch, iterati
     block: the persistent-grid block-tile kernel with the source id loaded
     one round ahead and the evict-last send-buffer prefix cut to 1 MB, so
     most sources take the plain-load side;
+    block_indeg: the same with out-degree ties broken by in-degree
+    (BP_REORDER_INDEG=1);
     split: the send pass over source ranges (cut to 2 MB of send buffers
-    here, 4 ranges) + node pass, the schedule the full-size graph runs.
+    here, 4 ranges) + node pass.
     Bit-exact beliefs and latest messages against the oracle after 10 and
     100 iterations."""
     net, ora = headline_sample
-    if path == "block":
+    monkeypatch.setenv("BP_REORDER_INDEG", "1" if path == "block_indeg" else "0")
+    if path in ("block", "block_indeg"):
         monkeypatch.setenv("BP_FLOOD_SPLIT", "0")
         monkeypatch.setenv("BP_FLOOD_HOT_MB", "1")
         monkeypatch.setenv("BP_FLOOD_PIPE", "1")
     else:
         monkeypatch.setenv("BP_FLOOD_SPLIT", "1")
         monkeypatch.setenv("BP_FLOOD_RANGE_MB", "2")
-    gpu = gpu_loopy(bp, net, 0.0, iterations, delta="f64", reorder=True, kernel="auto" if path == "block" else "split")
+    gpu = gpu_loopy(bp, net, 0.0, iterations, delta="f64", reorder=True, kernel="split" if path == "split" else "auto")
     assert gpu["executed"] == iterations
     latest = gpu["slot1"] if gpu["latest"] == 1 else gpu["slot0"]
     np.testing.assert_array_equal(gpu["beliefs"][:, :2], ora[iterations]["beliefs"][:, :2])
@@ -676,3 +679,17 @@ def test_serial_sum_bounds_hold_the_sum(bp, name):
     if name in ("uniform_80k", "message_diffs", "tiny_terms"):
         worst = len(x) * 2.0 ** -24 * float(np.sum(x, dtype=np.float64))
         assert hi - lo < 0.05 * worst, (name, hi - lo, worst)
+
+
+def test_reserve_cached_memory_then_build_and_solve(bp, synth, restatement, O):
+    """bp_reserve_cached_memory grows the stream-ordered pool once (a second
+    call with a smaller size does nothing); graphs built afterwards solve as
+    before, and bp_release_cached_memory hands the memory back."""
+    from belief_propagation_b200 import native as N
+    lib = N.load()
+    assert lib.bp_reserve_cached_memory(256 << 20) == 0
+    assert lib.bp_reserve_cached_memory(16 << 20) == 0
+    net = synth.random_loopy(2000, 8000, 2, 0.1, seed=4)
+    ora = restatement.loopy(O.OracleGraph(net), 1e-3, 30)
+    assert_same(gpu_loopy(bp, net, 1e-3, 30), ora, 2)
+    assert lib.bp_release_cached_memory() == 0
