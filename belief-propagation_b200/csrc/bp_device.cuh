@@ -294,24 +294,6 @@ __device__ __forceinline__ void combine(float *buf, const float *m, int s) {
         if ((UNI || i < s) && m[i] == m[i]) buf[i] = FMUL(buf[i], m[i]);
 }
 
-// combine for messages known to hold no NaN: the same products, without
-// the test
-template <int MS, bool UNI>
-__device__ __forceinline__ void combine_finite(float *buf, const float *m, int s) {
-#pragma unroll
-    for (int i = 0; i < MS; ++i)
-        if (UNI || i < s) buf[i] = FMUL(buf[i], m[i]);
-}
-
-// does any of the MS values hold a NaN?
-template <int MS>
-__device__ __forceinline__ bool has_nan(const float *m) {
-    bool n = false;
-#pragma unroll
-    for (int i = 0; i < MS; ++i) n |= m[i] != m[i];
-    return n;
-}
-
 // b /= sum(b) over i < s, sum <= 0 replaced by 1 (graph.c:1011-1023)
 template <int MS, bool UNI>
 __device__ __forceinline__ void normalise(float *b, int s) {

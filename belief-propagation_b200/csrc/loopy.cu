@@ -579,7 +579,6 @@ __device__ __forceinline__ void flood_tile(const FloodArgs &a, uint32_t tile, bo
     float prod[MS];
 #pragma unroll
     for (int i = 0; i < MS; ++i) prod[i] = 1.0f;
-    bool nan_seen = false, tile_nan = false;
 
     for (uint32_t c0 = e0; c0 < e1; c0 += EMAX) {
         const uint32_t c1 = min(e1, c0 + EMAX);
@@ -642,7 +641,6 @@ __device__ __forceinline__ void flood_tile(const FloodArgs &a, uint32_t tile, bo
                 }
                 stv<MS, kStream>(m_new + (size_t)p * MS, m);
                 stv<MS>(sm + (size_t)(p - c0) * MS, m);
-                nan_seen |= has_nan<MS>(m);
                 s_cur = s_nxt;
             }
         } else
@@ -697,29 +695,16 @@ __device__ __forceinline__ void flood_tile(const FloodArgs &a, uint32_t tile, bo
                 }
                 stv<MS, kStream>(m_new + (size_t)p * MS, m);
                 stv<MS>(sm + (size_t)(p - c0) * MS, m);
-                nan_seen |= has_nan<MS>(m);
             }
         }
-        // the barrier also tells every thread whether a message of this
-        // chunk is NaN; without one the products skip combine's NaN test
-        const bool chunk_nan = __syncthreads_or(nan_seen) != 0;
-        tile_nan |= chunk_nan;
-        nan_seen = false;
+        __syncthreads();
         // phase 2a: this node's product over its in-edges inside the chunk
         if (has) {
             const uint32_t lo = max(r0, c0), hi = min(r1, c1);
-            if (chunk_nan) {
-                for (uint32_t p = lo; p < hi; ++p) {
-                    float mm[MS];
-                    ldv<MS>(sm + (size_t)(p - c0) * MS, mm);
-                    combine<MS, UNI>(prod, mm, S);
-                }
-            } else {
-                for (uint32_t p = lo; p < hi; ++p) {
-                    float mm[MS];
-                    ldv<MS>(sm + (size_t)(p - c0) * MS, mm);
-                    combine_finite<MS, UNI>(prod, mm, S);
-                }
+            for (uint32_t p = lo; p < hi; ++p) {
+                float mm[MS];
+                ldv<MS>(sm + (size_t)(p - c0) * MS, mm);
+                combine<MS, UNI>(prod, mm, S);
             }
         }
         // the next chunk overwrites the messages; after the last chunk the
@@ -740,13 +725,7 @@ __device__ __forceinline__ void flood_tile(const FloodArgs &a, uint32_t tile, bo
         float qo[MS];
 #pragma unroll
         for (int i = 0; i < MS; ++i) qo[i] = b[i];
-        if (e1 - e0 <= EMAX && !tile_nan) {
-            for (uint32_t p = r0; p < r1; ++p) {
-                float mm[MS];
-                ldv<MS>(sm + (size_t)(p - e0) * MS, mm);
-                combine_finite<MS, UNI>(qo, mm, S);
-            }
-        } else if (e1 - e0 <= EMAX) {
+        if (e1 - e0 <= EMAX) {
             for (uint32_t p = r0; p < r1; ++p) {
                 float mm[MS];
                 ldv<MS>(sm + (size_t)(p - e0) * MS, mm);

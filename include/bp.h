@@ -96,8 +96,9 @@ typedef struct {
 } bp_graph_desc;
 
 typedef enum {
-    /* renumber nodes internally by decreasing out-degree (ties by id) so the
-     * send buffers of frequent sources share cache sectors; results are
+    /* renumber nodes internally by decreasing out-degree (ties by increasing
+     * in-degree, then id) so the send buffers of frequent sources share
+     * cache sectors and a warp's nodes have similar in-degrees; results are
      * unchanged (each node's in-edges keep their order), node ids at the API
      * stay the caller's.  Node-schedule loopy BP only: tree BP and the edge
      * schedule return BP_ERR_STATE on such a graph. */

@@ -262,7 +262,7 @@ def headline_sample(synth, O):
     return net, out
 
 
-@pytest.mark.parametrize("path", ["block", "block_indeg", "split"])
+@pytest.mark.parametrize("path", ["block", "block_outdeg", "split"])
 @pytest.mark.parametrize("iterations", [10, 100])
 def test_loopy_headline_path_bit_exact(bp, headline_sample, monkeypatch, iterations, path):
     """The benchmark's code paths -- nodes renumbered by out-degree, fp64
@@ -270,15 +270,15 @@ def test_loopy_headline_path_bit_exact(bp, headline_sample, monkeypatch, iterati
     block: the persistent-grid block-tile kernel with the source id loaded
     one round ahead and the evict-last send-buffer prefix cut to 1 MB, so
     most sources take the plain-load side;
-    block_indeg: the same with out-degree ties broken by in-degree
-    (BP_REORDER_INDEG=1);
+    block_outdeg: the same with out-degree ties broken by id only
+    (BP_REORDER_INDEG=0);
     split: the send pass over source ranges (cut to 2 MB of send buffers
     here, 4 ranges) + node pass.
     Bit-exact beliefs and latest messages against the oracle after 10 and
     100 iterations."""
     net, ora = headline_sample
-    monkeypatch.setenv("BP_REORDER_INDEG", "1" if path == "block_indeg" else "0")
-    if path in ("block", "block_indeg"):
+    monkeypatch.setenv("BP_REORDER_INDEG", "0" if path == "block_outdeg" else "1")
+    if path in ("block", "block_outdeg"):
         monkeypatch.setenv("BP_FLOOD_SPLIT", "0")
         monkeypatch.setenv("BP_FLOOD_HOT_MB", "1")
         monkeypatch.setenv("BP_FLOOD_PIPE", "1")
