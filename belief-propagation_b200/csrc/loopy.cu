@@ -2002,18 +2002,19 @@ static uint32_t split_range_nodes(const bp_graph *g) {
     return (uint32_t)std::min<uint64_t>(rn, 0xffffffffu);
 }
 
-// BP_FLOOD_SPLIT=1: whenever the layout applies; =auto: when the send buffers
-// exceed BP_FLOOD_SPLIT_MIN_MB (default 64) MB, i.e. when they no longer stay
-// in L2 across an iteration; default (or 0): never.  On the 16.8M-node graph
-// the split loop cuts DRAM traffic from 4.8 to 3.8 GB per iteration and runs
-// 0.86 ms against k_flood's 0.89 ms (the node pass, 1.25 GB in 0.34 ms, is
-// latency-bound), but its layout (a second edge order: a radix sort and a
-// 2.7 GB gather) lengthens a graph build from 44 to 58 ms, so a build-then-
-// solve-once serving loop is slower with it: the default keeps k_flood.
+// BP_FLOOD_SPLIT=1: whenever the layout applies; =0: never; default (auto):
+// when the send buffers exceed BP_FLOOD_SPLIT_MIN_MB (default 64) MB, i.e.
+// when they no longer stay in L2 across an iteration.  On the 16.8M-node
+// power-law graph (nodes renumbered, in-degree tie-break) the split loop cuts
+// DRAM traffic from 4.8 to 3.85 GB per iteration and runs 0.755-0.78 ms
+// against k_flood's 0.85-0.88 ms; its layout (a second edge order: a radix
+// sort and a 2.7 GB gather) adds about 2 ms of host time and 14 ms of device
+// work to a graph build, which a serving loop overlaps with the previous
+// solve (101 against 106 ms per build + 100-iteration solve).
 static bool split_wanted(const bp_graph *g) {
     const char *env = getenv("BP_FLOOD_SPLIT");
-    if (!env || env[0] == '0') return false;
-    if (env[0] == '1') return true;
+    if (env && env[0] == '0') return false;
+    if (env && env[0] == '1') return true;
     size_t mb = 64;
     if (const char *e2 = getenv("BP_FLOOD_SPLIT_MIN_MB")) mb = (size_t)atol(e2);
     return (uint64_t)g->V * g->ms * sizeof(float) > ((uint64_t)mb << 20);
@@ -2612,6 +2613,7 @@ int bp_loopy(bp_graph *g, const bp_loopy_options *opt, bp_loopy_result *res) {
     r.elapsed_ms = ms;
     r.serial_sums = c.serial_sums;
     r.serial_refines = c.serial_refines;
+    r.kernel_used = opt->schedule == BP_SCHEDULE_NODE ? (fgrid ? (int32_t)BP_KERNEL_BLOCK_TILE : (int32_t)variant) : 0;
     if (opt->schedule == BP_SCHEDULE_NODE) g->latest = (int)((c.msg_parity0 + c.it) & 1u);
     if (c.done == 2 && c.final_i == max_it && opt->verbose)
         printf("No Convergence: previous: %f vs current: %f\n", (double)r.previous_delta, (double)r.delta);

@@ -59,7 +59,6 @@ struct UGraph {
     const uint32_t *pos_out;   // slot in the source-sorted order of the edge at position p
     const uint8_t *pos_tab;
     const float *tables;   // [K][S][S] = log_pair (log joint tables)
-    const uint32_t *pos_dst;   // destination of the edge at position p
 };
 
 // in-edges whose loads one thread issues together
@@ -514,69 +513,6 @@ __global__ void __launch_bounds__(bwd_threads<S>(), MB) k_u_bwd(const UGraph g, 
     block_partial_add<S, NT, REG>(acc, sacc, wred, epart + (size_t)blockIdx.x * S * S, sm);
 }
 
-// The same step in node tiles (1 <= S <= 4): the block's threads first take
-// one node each (the node step: lbbar_out, Pbar into shared memory), then
-// the tile's in-edges, which are contiguous positions, one per thread per
-// round, with the destination's Pbar from shared memory.  The in-edge loads
-// are coalesced and no lane waits on another lane's longer in-edge list, in
-// place of k_u_bwd's sequential per-node edge loop.  Every quantity is
-// k_u_bwd's: the x adjoint terms are the same values; the table adjoint
-// adds the same per-edge terms in another order.
-template <int S>
-__global__ void __launch_bounds__(bwd_threads<S>(), bwd_min_blocks<S>())
-    k_u_bwd_tile(const UGraph g, int mode, const float *__restrict__ send, const float *__restrict__ lb_t,
-                 const float *__restrict__ lbbar_t, const float *__restrict__ xc_next, float *__restrict__ lbbar_out,
-                 float *__restrict__ xc, double *__restrict__ epart, float *__restrict__ pbar_out) {
-    static_assert(S <= 4, "register accumulators");
-    constexpr int NT = bwd_threads<S>();
-    constexpr int PS = S + 1;   // Pbar and its sum per node
-    __shared__ __align__(16) float sm[2 * kUMaxTables * S * S];
-    __shared__ float s_pb[NT * PS];
-    __shared__ float wred[NT / 32][S * S];
-    griddep_launch_dependents();
-    load_tables_smem<S>(g, sm);
-    griddep_wait();
-    float acc[S * S];
-#pragma unroll
-    for (int k = 0; k < S * S; ++k) acc[k] = 0.0f;
-    const bool one_table = pbar_out == nullptr;
-    const uint32_t ntiles = (g.V + NT - 1) / NT;
-    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const uint32_t v0 = tile * NT, v = v0 + threadIdx.x, vend = min(v0 + NT, g.V);
-        const uint32_t e0 = g.in_ptr[v0], e1 = g.in_ptr[vend];
-        if (v < g.V) {
-            float Pbar[S];
-            bwd_node_step<S>(g, mode, v, lb_t, lbbar_t, xc_next, lbbar_out, pbar_out, Pbar);
-            float ps = 0.0f;
-#pragma unroll
-            for (int i = 0; i < S; ++i) {
-                ps += Pbar[i];
-                s_pb[threadIdx.x * PS + i] = Pbar[i];
-            }
-            s_pb[threadIdx.x * PS + S] = ps;
-        }
-        __syncthreads();
-        for (uint32_t p = e0 + threadIdx.x; p < e1; p += NT) {
-            const uint32_t l = g.pos_dst[p] - v0, src = g.in_src[p], slot = g.pos_out[p];
-            const uint8_t tb = g.pos_tab[p];
-            float x[S], Pb[S], jr[S * S];
-            ldv<S>(send + (size_t)src * S, x);
-#pragma unroll
-            for (int i = 0; i < S; ++i) Pb[i] = s_pb[l * PS + i];
-            const float ps = s_pb[l * PS + S];
-            ldv<S * S>(edge_table<S>(sm, tb), jr);
-            float e[S], ci[S], c[S];
-            bwd_edge<S>(jr, x, Pb, ps, e, ci, c);
-            if (one_table) add_table_outer<S, NT, true>(acc, nullptr, ci, e, (tb & 0x80u) != 0);
-            stv<S>(xc + (size_t)slot * S, c);
-        }
-        __syncthreads();   // s_pb is rewritten by the next tile
-    }
-    // several tables: k_u_pair_grad adds the table adjoint
-    if (pbar_out) return;
-    block_partial_add<S, NT, true>(acc, nullptr, wred, epart + (size_t)blockIdx.x * S * S, sm);
-}
-
 // ---- the one-table adjoint on the tensor cores (5 <= S <= 8) ------------
 // With one shared table J, the table adjoint is J (.) sum over edges of
 // ci (x) e (transposed edges into the transposed entry), i.e. C^T E for the
@@ -754,7 +690,7 @@ struct bp_unrolled {
     uint32_t V = 0, E = 0, S = 0, K = 0, T = 0, ck = 1, nck = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
-    uint32_t *in_ptr = nullptr, *in_src = nullptr, *out_ptr = nullptr, *pos_out = nullptr, *pos_dst = nullptr;
+    uint32_t *in_ptr = nullptr, *in_src = nullptr, *out_ptr = nullptr, *pos_out = nullptr;
     uint8_t *pos_tab = nullptr;
     float *tables = nullptr;
     float *ck_b = nullptr, *ck_q = nullptr;    // [nck][V][S]
@@ -819,7 +755,7 @@ static int ubwd_env(const char *name, int dflt, int alt) {
 // into a CUDA graph, replayed on every call
 template <int S>
 static int u_forward(bp_unrolled *u) {
-    const UGraph g{u->V, u->K, u->in_ptr, u->in_src, u->out_ptr, u->pos_out, u->pos_tab, u->tables, u->pos_dst};
+    const UGraph g{u->V, u->K, u->in_ptr, u->in_src, u->out_ptr, u->pos_out, u->pos_tab, u->tables};
     const size_t VS = (size_t)u->V * S;
     const unsigned gv = grid_for(u->V, kUThreads);
     cudaStream_t st = u->stream;
@@ -857,7 +793,7 @@ static int u_forward(bp_unrolled *u) {
 // entry; gtheta_buf, glogp_buf receive the gradients)
 template <int S>
 static int u_backward(bp_unrolled *u) {
-    const UGraph g{u->V, u->K, u->in_ptr, u->in_src, u->out_ptr, u->pos_out, u->pos_tab, u->tables, u->pos_dst};
+    const UGraph g{u->V, u->K, u->in_ptr, u->in_src, u->out_ptr, u->pos_out, u->pos_tab, u->tables};
     const size_t VS = (size_t)u->V * S;
     const unsigned gv = grid_for(u->V, kUThreads);
     constexpr int BT = bwd_threads<S>();
@@ -868,9 +804,6 @@ static int u_backward(bp_unrolled *u) {
     // register cap of the adjoint kernel, 1-4 states: BP_UBWD_MINB=3 allows
     // 85 registers (3 blocks per SM) instead of 64 (4 blocks)
     const int minb = ubwd_env("BP_UBWD_MINB", 4, 3);
-    // 1-4 states: node tiles with edge-parallel rounds (BP_UBWD_TILE=0: a
-    // thread per node and its in-edge loop)
-    const bool tile = ubwd_env("BP_UBWD_TILE", 1, 0) == 1;
     const unsigned gb = mma ? grid_for(u->V, kMmaThreads * 2) : grid_for(u->V, BT * npt);
     cudaStream_t st = u->stream;
     int rc = BP_OK;
@@ -881,8 +814,6 @@ static int u_backward(bp_unrolled *u) {
                                      u->epart);
         }
         if constexpr (S <= 4) {
-            if (tile)
-                return u_launch(k_u_bwd_tile<S>, gb, BT, st, g, mode, send, b_t, gbar, xn, out, xo, u->epart, pb);
             if (batch == 4)
                 return u_launch(k_u_bwd<S, 4>, gb, BT, st, g, mode, send, b_t, gbar, xn, out, xo, u->epart, pb);
             if (minb == 3)
@@ -962,7 +893,7 @@ static int u_backward(bp_unrolled *u) {
 
 static void u_free(bp_unrolled *u) {
     if (!u) return;
-    void *ptrs[] = {u->in_ptr, u->in_src, u->out_ptr, u->pos_out, u->pos_dst, u->pos_tab, u->tables, u->ck_b, u->ck_q,
+    void *ptrs[] = {u->in_ptr, u->in_src, u->out_ptr, u->pos_out, u->pos_tab, u->tables, u->ck_b, u->ck_q,
                     u->seg_b, u->seg_q, u->pp_b, u->pp_q, u->bT, u->bbar[0], u->bbar[1], u->xc[0],
                     u->xc[1], u->epart, u->theta_buf, u->gtheta_buf, u->glogp_buf, u->pbar};
     for (void *p : ptrs)
@@ -1108,16 +1039,13 @@ int bp_unrolled_create(bp_unrolled **out, uint32_t V, uint32_t E, uint32_t S, ui
     }
     std::vector<uint32_t> ofill(out_ptr.begin(), out_ptr.end() - 1);
     for (uint32_t e = 0; e < E; ++e) pos_out[pos_of[e]] = ofill[src[e]]++;
-    std::vector<uint32_t> pos_dst(E);
-    for (uint32_t v = 0; v < V; ++v)
-        for (uint32_t p = in_ptr[v]; p < in_ptr[v + 1]; ++p) pos_dst[p] = v;
     const size_t VS = (size_t)V * S;
     u->nblk = grid_for(V, 64);   // partial slots for the smallest backward block
     auto alloc = [&](void **p, size_t bytes) {
         return cudaMalloc(p, bytes ? bytes : 16) == cudaSuccess;
     };
     bool ok = alloc((void **)&u->in_ptr, sizeof(uint32_t) * (V + 1)) && alloc((void **)&u->in_src, 4 * (size_t)E) &&
-              alloc((void **)&u->out_ptr, sizeof(uint32_t) * (V + 1)) && alloc((void **)&u->pos_out, 4 * (size_t)E) && alloc((void **)&u->pos_dst, 4 * (size_t)E) &&
+              alloc((void **)&u->out_ptr, sizeof(uint32_t) * (V + 1)) && alloc((void **)&u->pos_out, 4 * (size_t)E) &&
               alloc((void **)&u->pos_tab, (size_t)E) && alloc((void **)&u->tables, sizeof(float) * K * S * S) &&
               alloc((void **)&u->ck_b, sizeof(float) * VS * u->nck) &&
               alloc((void **)&u->ck_q, sizeof(float) * VS * u->nck) &&
@@ -1141,7 +1069,6 @@ int bp_unrolled_create(bp_unrolled **out, uint32_t V, uint32_t E, uint32_t S, ui
     if (E) {
         cudaMemcpyAsync(u->in_src, in_src.data(), 4 * (size_t)E, cudaMemcpyHostToDevice, u->stream);
         cudaMemcpyAsync(u->pos_out, pos_out.data(), 4 * (size_t)E, cudaMemcpyHostToDevice, u->stream);
-        cudaMemcpyAsync(u->pos_dst, pos_dst.data(), 4 * (size_t)E, cudaMemcpyHostToDevice, u->stream);
         cudaMemcpyAsync(u->pos_tab, ptab.data(), (size_t)E, cudaMemcpyHostToDevice, u->stream);
     }
     cudaEventCreate(&u->ev0);

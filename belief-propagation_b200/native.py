@@ -49,7 +49,8 @@ class LoopyOptions(C.Structure):
 class LoopyResult(C.Structure):
     _fields_ = [("iterations", C.c_uint32), ("executed", C.c_uint32), ("converged", C.c_int32),
                 ("delta", C.c_float), ("previous_delta", C.c_float), ("delta_f64", C.c_double),
-                ("elapsed_ms", C.c_float), ("serial_sums", C.c_uint32), ("serial_refines", C.c_uint32)]
+                ("elapsed_ms", C.c_float), ("serial_sums", C.c_uint32), ("serial_refines", C.c_uint32),
+                ("kernel_used", C.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

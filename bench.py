@@ -142,14 +142,15 @@ def measured_hbm_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def profiled_traffic(name):
-    """DRAM bytes per launch of the flooding kernel from the committed ncu
-    summary (profiles/<name>), or None."""
+def profiled_traffic(name, key="traffic_bytes_per_launch"):
+    """DRAM bytes per launch (or per iteration, with that key) of the
+    flooding kernels from the committed ncu summary (profiles/<name>), or
+    None."""
     p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return None
     for line in open(p):
-        if line.startswith("traffic_bytes_per_launch:"):
+        if line.startswith(key + ":"):
             return float(line.split(":", 1)[1])
     return None
 
@@ -1004,6 +1005,7 @@ def main():
     for _ in range(a.steps):
         r = step()
         kernel_ms.append(r["elapsed_ms"] / max(r["executed"], 1))
+    split = r["kernel_used"] == 4   # BP_KERNEL_SPLIT
     ev1.record(stream)
     barrier()
     clk = clocks.stop()
@@ -1013,15 +1015,23 @@ def main():
     updates = float(E) * a.iterations * world
     value = updates / (ms_per_step / 1e3)
 
-    # ---- roofline of the flooding kernel (one launch = one iteration)
+    # ---- roofline of one iteration: one k_flood launch, or the split
+    # schedule's send pass + node pass (the library's choice for send buffers
+    # larger than L2); its algorithmic bytes are the iteration's minimum
     it_ms = statistics.median(kernel_ms)
     algo = flood_bytes_per_iteration(V, E, S)
     achieved = algo / (it_ms / 1e3) / 1e9
     peak, peak_src = measured_hbm_peak()
-    traffic = profiled_traffic("k_flood_power_law_16M_dram.md")
+    if split:
+        traffic = profiled_traffic("k_flood_split_power_law_16M_dram.md", "traffic_bytes_per_iteration")
+        kernel = "k_flood_send<2,0> + k_flood_nodes<2,0,1> (one split iteration, 2 launches)"
+    else:
+        traffic = profiled_traffic("k_flood_power_law_16M_dram.md")
+        kernel = "k_flood<2,true>"
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "kernel": "k_flood<2,true>", "peak_source": peak_src,
-                "algorithmic_bytes_per_launch": algo, "launch_ms": it_ms}
+                "traffic": traffic, "kernel": kernel, "peak_source": peak_src,
+                "algorithmic_bytes_per_launch": algo, "algorithmic_bytes_per_iteration": algo, "launch_ms": it_ms,
+                "iteration_ms": it_ms, "launches_per_iteration": 2 if split else 1}
     graph_bytes = g.device_bytes()
     g.close()
     del prior
@@ -1138,7 +1148,9 @@ def main():
         dist.destroy_process_group()
     if rank != 0:
         return 0
-    launches_per_step = 1 + 1 + 1 + a.iterations   # set_beliefs, init, gather, flood x iterations
+    # set_beliefs, init, gather, then flood x iterations, or (split) the
+    # conversion to send order, 2 x iterations and the two conversions back
+    launches_per_step = 3 + (3 + 2 * a.iterations if split else a.iterations)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",

@@ -62,15 +62,16 @@ typedef enum { BP_SYNC_EAGER = 0, BP_SYNC_LAZY = 1 } bp_sync_mode;
 
 /* the node-schedule iteration kernel: same results, different tiling */
 typedef enum {
-    BP_KERNEL_AUTO = 0,        /* block tiles (BP_FLOOD_SPLIT=1|auto in the environment: split tiles whenever they
-                                  fit | when the send buffers exceed 64 MB; BP_FLOOD_KERNEL=warp|staged selects warp
-                                  tiles, or staged tiles where they apply) */
+    BP_KERNEL_AUTO = 0,        /* the split schedule for uniform graphs of <= 4 states whose send buffers exceed
+                                  64 MB (they no longer stay in L2), else block tiles.  BP_FLOOD_SPLIT=0|1 in the
+                                  environment: never | whenever it applies; BP_FLOOD_KERNEL=warp|staged selects warp
+                                  tiles, or staged tiles where they apply */
     BP_KERNEL_BLOCK_TILE = 1,  /* 256-node block tiles, block-wide barriers between phases */
     BP_KERNEL_WARP_TILE = 2,   /* 32-node warp tiles, unrolled edge loads */
     BP_KERNEL_STAGED_TILE = 3, /* persistent CTAs, bulk-copy staged tiles; uniform 2-state graphs of mean in-degree
                                   <= 4.5, f64 delta */
-    BP_KERNEL_SPLIT = 4        /* send pass over the edges grouped by source-node range (bulk-copy stages, gathers
-                                  from one L2-sized range of send buffers at a time) + node pass; uniform graphs of
+    BP_KERNEL_SPLIT = 4        /* send pass over the edges grouped by source-node range (gathers from one
+                                  L2-sized range of send buffers at a time) + node pass; uniform graphs of
                                   <= 4 states */
 } bp_kernel_variant;
 
@@ -128,6 +129,9 @@ typedef struct {
                                * bound decided the stop */
     uint32_t serial_refines;  /* serial fp32 delta: checks that needed the interval
                                * narrowed from the terms' own rounding errors */
+    int32_t kernel_used;      /* bp_kernel_variant that ran the node-schedule
+                               * iterations (block tiles for the one-launch loop
+                               * of small graphs); 0 for the edge schedule */
 } bp_loopy_result;
 
 typedef struct {
