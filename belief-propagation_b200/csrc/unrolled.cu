@@ -228,24 +228,26 @@ __global__ void __launch_bounds__(kUThreads) k_u_iter(const UGraph g, const floa
     griddep_launch_dependents();
     load_tables_smem<S>(g, sm);
     griddep_wait();
-    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= g.V) return;
-    float P[S], a[S];
+    // grid-stride: the backward's recompute runs on a smaller grid beside the
+    // adjoint (one node per thread on the forward's full grid)
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < g.V; v += gridDim.x * blockDim.x) {
+        float P[S], a[S];
 #pragma unroll
-    for (int i = 0; i < S; ++i) P[i] = 0.0f;
-    sum_log_msgs<S>(g, sm, lq_in, g.in_ptr[v], g.in_ptr[v + 1], P);
-    ldv<S>(lb_in + (size_t)v * S, a);
+        for (int i = 0; i < S; ++i) P[i] = 0.0f;
+        sum_log_msgs<S>(g, sm, lq_in, g.in_ptr[v], g.in_ptr[v + 1], P);
+        ldv<S>(lb_in + (size_t)v * S, a);
 #pragma unroll
-    for (int i = 0; i < S; ++i) a[i] += P[i];
-    const float z = lse<S>(a);
-    float qo[S];
+        for (int i = 0; i < S; ++i) a[i] += P[i];
+        const float z = lse<S>(a);
+        float qo[S];
 #pragma unroll
-    for (int i = 0; i < S; ++i) {
-        a[i] -= z;
-        qo[i] = a[i] + P[i];
+        for (int i = 0; i < S; ++i) {
+            a[i] -= z;
+            qo[i] = a[i] + P[i];
+        }
+        stv<S>(lb_out + (size_t)v * S, a);
+        stv<S>(lq_out + (size_t)v * S, qo);
     }
-    stv<S>(lb_out + (size_t)v * S, a);
-    stv<S>(lq_out + (size_t)v * S, qo);
 }
 
 // this block's sum of the per-thread table-adjoint accumulators (fixed
@@ -805,6 +807,10 @@ static int u_backward(bp_unrolled *u) {
     // 85 registers (3 blocks per SM) instead of 64 (4 blocks)
     const int minb = ubwd_env("BP_UBWD_MINB", 4, 3);
     const unsigned gb = mma ? grid_for(u->V, kMmaThreads * 2) : grid_for(u->V, BT * npt);
+    // the recompute's grid (BP_UREC_GRID=<blocks>, sweeps): by default the
+    // forward's, a thread per node
+    unsigned rgrid = gv;
+    if (const char *env = getenv("BP_UREC_GRID")) rgrid = std::max(1u, std::min(gv, (unsigned)atoi(env)));
     cudaStream_t st = u->stream;
     int rc = BP_OK;
     auto adjoint = [&](int mode, const float *send, const float *b_t, const float *gbar, const float *xn, float *out,
@@ -846,7 +852,7 @@ static int u_backward(bp_unrolled *u) {
         for (uint32_t j = 1; j + t0 < t_end; ++j) {
             const float *bi = (j == 1) ? ckb : seg_b(s, j - 1);
             const float *qi = (j == 1) ? ckq : seg_q(s, j - 1);
-            int r = u_launch(k_u_iter<S>, gv, kUThreads, u->side, g, bi, qi, seg_b(s, j), seg_q(s, j));
+            int r = u_launch(k_u_iter<S>, rgrid, kUThreads, u->side, g, bi, qi, seg_b(s, j), seg_q(s, j));
             if (r) return r;
         }
         return BP_OK;
