@@ -141,10 +141,12 @@ __device__ __forceinline__ void split_finalize(const SplitArgs &a, bool want, do
 // (the second pass re-reads them, from L1).  Nodes grid-stride.  NV selects
 // the form of the loads (sweeps; the same results): 0 plain, 1 the loop
 // unrolled by 4 by the compiler, 2 the send indices and messages through
-// the read-only path.  Measured forms that were slower: four messages loaded
-// before their use (0.43 ms against 0.34 ms per launch on the 16.8M-node
-// graph), and warp tiles staging a tile's messages through shared memory
-// (0.45 ms).
+// the read-only path.  Measured forms that were slower, on the 16.8M-node
+// graph with nodes renumbered by out-degree (ties by id): four messages
+// loaded before their use (0.43 ms against 0.34 ms per launch), warp tiles
+// staging a tile's messages through shared memory (0.45 ms), and a group of
+// 4 lanes per node (1.6 ms).  With ties broken by in-degree, so that a warp's
+// nodes have in-edge lists of similar length, this form takes 0.26 ms.
 template <int MS, int NV>
 __device__ __forceinline__ void node_msg(const SplitArgs &a, const float *__restrict__ m_new, uint32_t p, float *mm) {
     if constexpr (NV == 2) ldv<MS, kReadOnly>(m_new + (size_t)__ldg(a.s_inv + p) * MS, mm);

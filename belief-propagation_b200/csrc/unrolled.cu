@@ -228,8 +228,6 @@ __global__ void __launch_bounds__(kUThreads) k_u_iter(const UGraph g, const floa
     griddep_launch_dependents();
     load_tables_smem<S>(g, sm);
     griddep_wait();
-    // grid-stride: the backward's recompute runs on a smaller grid beside the
-    // adjoint (one node per thread on the forward's full grid)
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < g.V; v += gridDim.x * blockDim.x) {
         float P[S], a[S];
 #pragma unroll
@@ -807,10 +805,9 @@ static int u_backward(bp_unrolled *u) {
     // 85 registers (3 blocks per SM) instead of 64 (4 blocks)
     const int minb = ubwd_env("BP_UBWD_MINB", 4, 3);
     const unsigned gb = mma ? grid_for(u->V, kMmaThreads * 2) : grid_for(u->V, BT * npt);
-    // the recompute's grid (BP_UREC_GRID=<blocks>, sweeps): by default the
-    // forward's, a thread per node
-    unsigned rgrid = gv;
-    if (const char *env = getenv("BP_UREC_GRID")) rgrid = std::max(1u, std::min(gv, (unsigned)atoi(env)));
+    // the recompute keeps the forward's grid, a thread per node: on smaller
+    // grids beside the adjoint (80-296 blocks) it became the critical path
+    const unsigned rgrid = gv;
     cudaStream_t st = u->stream;
     int rc = BP_OK;
     auto adjoint = [&](int mode, const float *send, const float *b_t, const float *gbar, const float *xn, float *out,
