@@ -19,8 +19,6 @@
 #include <stdlib.h>
 #include <string.h>
 
-#include <cooperative_groups.h>
-
 #include <algorithm>
 #include <numeric>
 #include <string>
@@ -348,185 +346,6 @@ __device__ void solve_network(const BatchArgs &a, uint32_t n, double *red, int *
     __syncthreads();
 }
 
-// One network by a thread-block cluster (fp64 delta): solve_network's loops
-// stride over the cluster's threads, and a cluster barrier (hardware, across
-// the cluster's SMs) separates the phases.  Each block sums its |diff| terms,
-// rank 0 adds the blocks' sums in rank order, takes the stopping decision
-// and hands it to the other blocks through distributed shared memory.  Data
-// that another block of the cluster wrote (send buffers, this iteration's
-// messages) is read through L2.  Per-value arithmetic is solve_network's, so
-// beliefs and messages are bit-identical to it; the fp64 delta adds the same
-// terms in another order.
-template <int S>
-__device__ void solve_network_cluster(const BatchArgs &a, uint32_t n, double *red, double *s_part, int *s_flag) {
-    namespace cg = cooperative_groups;
-    cg::cluster_group cl = cg::this_cluster();
-    const uint32_t rank = cl.block_rank(), ncl = cl.num_blocks();
-    const NetInfo ni = a.info[n];
-    const uint32_t V = ni.V, E = ni.E;
-    const uint32_t *ptr = a.in_ptr + ni.ptr_off;
-    const uint32_t *src = a.in_src + ni.edge_off;
-    const float *J = a.joint + ni.joint_off;
-    float *b = a.belief + ni.node_off;
-    float *msg[2] = {a.msg0 + ni.msg_off, a.msg1 + ni.msg_off};
-    float *q[2] = {a.q0 + ni.node_off, a.q1 + ni.node_off};
-    const uint32_t T = blockDim.x, tid = threadIdx.x, gt = rank * T + tid, GT = ncl * T;
-    int latest = a.latest[n];
-
-    if (a.init) {  // init_previous_edge (graph.c:725-751)
-        for (uint32_t p = gt; p < E; p += GT) {
-            float buf[S], m[S];
-            ldv<S>(b + (size_t)src[p] * S, buf);
-            send_msg<S, true>(J + (size_t)p * S * S, buf, S, S, m);
-            stv<S>(msg[latest] + (size_t)p * S, m);
-        }
-        cl.sync();
-    }
-    // Q_1 = b * prod of the latest messages (graph.c:860-882)
-    for (uint32_t v = gt; v < V; v += GT) {
-        float bb[S];
-        ldv<S>(b + (size_t)v * S, bb);
-        for (uint32_t p = ptr[v]; p < ptr[v + 1]; ++p) {
-            float mm[S];
-            ldv<S, kL2>(msg[latest] + (size_t)p * S, mm);
-            combine<S, true>(bb, mm, S);
-        }
-        stv<S>(q[0] + (size_t)v * S, bb);
-    }
-    cl.sync();
-
-    float prev_f = -1.0f, delta_f = 0.0f;
-    double prev_d = -1.0, delta_d = 0.0;
-    uint32_t it = 0, ret = a.max_it, converged = 0;
-    for (it = 0; it < a.max_it; ++it) {
-        const float *m_old = msg[latest];
-        float *m_new = msg[latest ^ 1];
-        const float *q_in = q[it & 1];
-        float *q_out = q[(it + 1) & 1];
-        double dsum = 0.0;
-        for (uint32_t p = gt; p < E; p += GT) {
-            float qq[S], m[S], o[S];
-            ldv<S, kL2>(q_in + (size_t)src[p] * S, qq);
-            ldv<S>(m_old + (size_t)p * S, o);
-            send_msg<S, true>(J + (size_t)p * S * S, qq, S, S, m);
-#pragma unroll
-            for (int k = 0; k < S; ++k) {
-                float d = FSUB(o[k], m[k]);
-                if (d != d) d = 0.0f;
-                dsum += (double)fabsf(d);
-            }
-            stv<S>(m_new + (size_t)p * S, m);
-        }
-        cl.sync();
-        for (uint32_t v = gt; v < V; v += GT) {
-            const uint32_t r0 = ptr[v], r1 = ptr[v + 1];
-            float prod[S], bb[S];
-#pragma unroll
-            for (int i = 0; i < S; ++i) prod[i] = 1.0f;
-            for (uint32_t p = r0; p < r1; ++p) {
-                float mm[S];
-                ldv<S, kL2>(m_new + (size_t)p * S, mm);
-                combine<S, true>(prod, mm, S);
-            }
-            ldv<S>(b + (size_t)v * S, bb);
-            if (r1 > r0) {
-#pragma unroll
-                for (int i = 0; i < S; ++i) bb[i] = FMUL(bb[i], prod[i]);
-            }
-            normalise<S, true>(bb, S);
-            stv<S>(b + (size_t)v * S, bb);
-            float qo[S];
-#pragma unroll
-            for (int i = 0; i < S; ++i) qo[i] = bb[i];
-            for (uint32_t p = r0; p < r1; ++p) {
-                float mm[S];
-                ldv<S, kL2>(m_new + (size_t)p * S, mm);
-                combine<S, true>(qo, mm, S);
-            }
-            stv<S>(q_out + (size_t)v * S, qo);
-        }
-        {   // this block's sum
-            const double v = warp_sum(dsum);
-            const int lane = tid & 31, w = tid >> 5;
-            if (lane == 0) red[w] = v;
-            __syncthreads();
-            if (w == 0) {
-                const double t = warp_sum(lane < (int)(T >> 5) ? red[lane] : 0.0);
-                if (lane == 0) *s_part = t;
-            }
-        }
-        cl.sync();   // the blocks' sums, beliefs and send buffers
-        if (rank == 0 && tid == 0) {
-            double tot = 0.0;
-            for (uint32_t r = 0; r < ncl; ++r) tot += *cl.map_shared_rank(s_part, r);
-            delta_d = tot;
-            delta_f = (float)tot;
-            const bool stop = (tot < (double)a.tol) || (fabs(tot - prev_d) < (double)a.tol);
-            if (stop) {
-                ret = it;
-                converged = 1;
-            } else if (it < a.max_it - 1) {
-                prev_f = delta_f;
-                prev_d = delta_d;
-            }
-            *s_flag = stop ? 1 : 0;
-        }
-        cl.sync();
-        latest ^= 1;
-        // the flag is rewritten after at least one more cluster barrier, and
-        // every block reads it before that barrier
-        if (*cl.map_shared_rank(s_flag, 0)) break;
-    }
-    if (rank == 0 && tid == 0) {
-        NetResult r;
-        r.iterations = converged ? ret : a.max_it;
-        r.executed = converged ? it + 1 : a.max_it;
-        r.converged = converged;
-        r.latest = (uint32_t)latest;
-        r.delta = delta_f;
-        r.prev_delta = prev_f;
-        r.delta_d = delta_d;
-        a.res[n] = r;
-        a.latest[n] = (uint8_t)latest;
-    }
-    cl.sync();   // every block is done with this network and its shared state
-}
-
-// The fp64-delta solve with clusters for the largest networks: order[0,
-// n_large) (the largest work first) are taken a cluster at a time, each
-// solved by its whole cluster; once that queue is empty the cluster's blocks
-// take order[n_large, count) one block each (solve_network).  A network
-// solved by one block takes its whole time on one SM, so without clusters the
-// largest networks set the batch's time long after the other SMs finished.
-template <int S>
-__global__ void k_batch_solve_cl(const BatchArgs a, const uint32_t *__restrict__ order, uint32_t n_large,
-                                 uint32_t count, uint32_t *queues) {
-    namespace cg = cooperative_groups;
-    __shared__ double red[32];
-    __shared__ double s_part;
-    __shared__ int s_flag;
-    __shared__ uint32_t s_next;
-    __shared__ double s_tot;
-    __shared__ float s_res;
-    cg::cluster_group cl = cg::this_cluster();
-    for (;;) {
-        if (cl.block_rank() == 0 && threadIdx.x == 0) s_next = atomicAdd(queues, 1u);
-        cl.sync();
-        const uint32_t k = *cl.map_shared_rank(&s_next, 0);
-        cl.sync();   // rank 0 takes the next one only after every block read this one
-        if (k >= n_large) break;
-        solve_network_cluster<S>(a, order[k], red, &s_part, &s_flag);
-    }
-    for (;;) {
-        if (threadIdx.x == 0) s_next = atomicAdd(queues + 1, 1u);
-        __syncthreads();
-        const uint32_t k = n_large + s_next;
-        __syncthreads();
-        if (k >= count) break;
-        solve_network<S, false>(a, order[k], red, &s_flag, &s_tot, &s_res, nullptr);
-    }
-}
-
 template <int S, bool SER>
 __global__ void k_batch_solve(const BatchArgs a, const uint32_t *__restrict__ order, uint32_t count,
                               uint32_t *queue) {
@@ -583,7 +402,7 @@ struct bp_batch {
     float *absdiff = nullptr, *staging = nullptr;
     bpx::NetResult *res = nullptr;
     uint8_t *latest = nullptr;
-    uint32_t *queues = nullptr;   // two counters per group: clusters' and blocks' queue
+    uint32_t *queues = nullptr;   // one counter per group
     std::vector<bpx::Group> groups;
     cudaGraphExec_t exec = nullptr;
     uint64_t exec_key = 0;
@@ -596,54 +415,14 @@ struct bp_batch {
 
 namespace bpx {
 
-// blocks per cluster for the largest networks of the fp64-delta solve
-// (BP_BATCH_CLUSTER=1|2|4|8; 1 solves every network with one block), and
-// which networks count as largest: work (E S^2 + V S) at least the group's
-// largest over BP_BATCH_LARGE_DIV (default 4; 0: none)
-static uint32_t batch_cluster() {
-    const char *env = getenv("BP_BATCH_CLUSTER");
-    const int c = env ? atoi(env) : 8;
-    return (c == 1 || c == 2 || c == 4 || c == 8) ? (uint32_t)c : 8u;
-}
-
-static uint64_t net_work(const NetInfo &ni) { return (uint64_t)ni.E * ni.S * ni.S + (uint64_t)ni.V * ni.S; }
-
-static uint32_t large_count(const bp_batch *bt, const Group &gr) {
-    const char *env = getenv("BP_BATCH_LARGE_DIV");
-    const uint64_t div = env ? (uint64_t)atoll(env) : 4u;
-    if (!div || gr.order.empty()) return 0;
-    const uint64_t thr = (net_work(bt->info[gr.order[0]]) + div - 1) / div;
-    uint32_t k = 0;
-    while (k < gr.order.size() && net_work(bt->info[gr.order[k]]) >= thr) ++k;
-    return k;
-}
-
 template <int S>
 static int launch_group(bp_batch *bt, Group &gr, const BatchArgs &a, uint32_t gi, uint32_t block, uint32_t grid,
                         cudaStream_t s) {
-    uint32_t *queues = bt->queues + 2 * gi;
-    const uint32_t count = (uint32_t)gr.order.size();
-    const uint32_t cl = batch_cluster(), n_large = a.serial ? 0u : large_count(bt, gr);
-    if (a.serial) {
-        k_batch_solve<S, true><<<grid, block, sizeof(float) * 2 * a.sum_ch, s>>>(a, gr.d_order, count, queues);
-    } else if (cl > 1 && n_large > 0) {
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(std::max(cl, grid / cl * cl));
-        cfg.blockDim = dim3(block);
-        cfg.dynamicSmemBytes = 0;
-        cfg.stream = s;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeClusterDimension;
-        attr[0].val.clusterDim.x = cl;
-        attr[0].val.clusterDim.y = 1;
-        attr[0].val.clusterDim.z = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        BP_CUDA(cudaLaunchKernelEx(&cfg, k_batch_solve_cl<S>, a, (const uint32_t *)gr.d_order, n_large, count,
-                                   queues));
-    } else {
-        k_batch_solve<S, false><<<grid, block, 0, s>>>(a, gr.d_order, count, queues);
-    }
+    if (a.serial)
+        k_batch_solve<S, true><<<grid, block, sizeof(float) * 2 * a.sum_ch, s>>>(a, gr.d_order,
+                                                                               (uint32_t)gr.order.size(), bt->queues + gi);
+    else
+        k_batch_solve<S, false><<<grid, block, 0, s>>>(a, gr.d_order, (uint32_t)gr.order.size(), bt->queues + gi);
     BP_CUDA(cudaGetLastError());
     return BP_OK;
 }
@@ -720,7 +499,7 @@ static uint32_t grid_for_group(bp_batch *bt, const Group &gr, uint32_t block, si
 // the whole batched solve on bt->stream: reset queues, fork one stream per
 // state-count group, launch each group's persistent kernel, join
 static int enqueue_batch(bp_batch *bt, const BatchArgs &a) {
-    BP_CUDA(cudaMemsetAsync(bt->queues, 0, sizeof(uint32_t) * 2 * bt->groups.size(), bt->stream));
+    BP_CUDA(cudaMemsetAsync(bt->queues, 0, sizeof(uint32_t) * bt->groups.size(), bt->stream));
     BP_CUDA(cudaEventRecord(bt->fork_ev, bt->stream));
     for (size_t gi = 0; gi < bt->groups.size(); ++gi) {
         Group &gr = bt->groups[gi];
@@ -891,7 +670,7 @@ static int batch_create_impl(bp_batch *bt, uint32_t N, const bp_graph_desc *desc
         BP_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         bt->side_ev.push_back(e);
     }
-    if ((st = alloc((void **)&bt->queues, sizeof(uint32_t) * 2 * bt->groups.size()))) return st;
+    if ((st = alloc((void **)&bt->queues, sizeof(uint32_t) * bt->groups.size()))) return st;
     BP_CUDA(cudaEventCreateWithFlags(&bt->fork_ev, cudaEventDisableTiming));
     BP_CUDA(cudaEventCreate(&bt->ev0));
     BP_CUDA(cudaEventCreate(&bt->ev1));
@@ -902,7 +681,7 @@ static int batch_create_impl(bp_batch *bt, uint32_t N, const bp_graph_desc *desc
 // ---- autotuning of threads per block, cached on disk ---------------------
 // kernel revision in the autotune key: a cached block size belongs to the
 // kernel it was timed on
-constexpr int kTuneRevision = 4;
+constexpr int kTuneRevision = 3;
 
 static std::string tune_key(bp_batch *bt, const Group &gr, int serial) {
     uint64_t V = 0, E = 0;
@@ -1110,7 +889,7 @@ int bp_batch_autotune(bp_batch *bt, const bp_batch_options *o) {
                     BP_CUDA(cudaMemcpyAsync(bt->belief, keep, sizeof(float) * bt->totNodeF, cudaMemcpyDeviceToDevice,
                                             bt->stream));
                     BP_CUDA(cudaMemcpyAsync(bt->latest, latest0.data(), bt->N, cudaMemcpyHostToDevice, bt->stream));
-                    BP_CUDA(cudaMemsetAsync(bt->queues + 2 * gi, 0, 2 * sizeof(uint32_t), bt->stream));
+                    BP_CUDA(cudaMemsetAsync(bt->queues + gi, 0, sizeof(uint32_t), bt->stream));
                     BP_CUDA(cudaEventRecord(bt->ev0, bt->stream));
                     int st = launch_group_s(bt, gr, a, (uint32_t)gi, c, grid, bt->stream);
                     if (st) {

@@ -22,9 +22,7 @@ namespace bpx {
 // ---- vector loads / stores of N consecutive floats ------------------------
 // N*4 bytes at an address that is a multiple of N*4 bytes (every array here is
 // indexed by element * N), so float4 needs N % 4 == 0 and float2 N % 2 == 0.
-// kL2: through L2 only (ld.cg), for data another SM wrote since this SM may
-// have cached the line
-enum CacheHint { kDefault = 0, kStream = 1, kReadOnly = 2, kL2 = 3 };
+enum CacheHint { kDefault = 0, kStream = 1, kReadOnly = 2 };
 
 template <int N, int H = kDefault>
 __device__ __forceinline__ void ldv(const float *__restrict__ p, float *o) {
@@ -34,7 +32,6 @@ __device__ __forceinline__ void ldv(const float *__restrict__ p, float *o) {
             float4 v;
             if constexpr (H == kStream) v = __ldcs(reinterpret_cast<const float4 *>(p) + k);
             else if constexpr (H == kReadOnly) v = __ldg(reinterpret_cast<const float4 *>(p) + k);
-            else if constexpr (H == kL2) v = __ldcg(reinterpret_cast<const float4 *>(p) + k);
             else v = reinterpret_cast<const float4 *>(p)[k];
             o[4 * k] = v.x; o[4 * k + 1] = v.y; o[4 * k + 2] = v.z; o[4 * k + 3] = v.w;
         }
@@ -44,7 +41,6 @@ __device__ __forceinline__ void ldv(const float *__restrict__ p, float *o) {
             float2 v;
             if constexpr (H == kStream) v = __ldcs(reinterpret_cast<const float2 *>(p) + k);
             else if constexpr (H == kReadOnly) v = __ldg(reinterpret_cast<const float2 *>(p) + k);
-            else if constexpr (H == kL2) v = __ldcg(reinterpret_cast<const float2 *>(p) + k);
             else v = reinterpret_cast<const float2 *>(p)[k];
             o[2 * k] = v.x; o[2 * k + 1] = v.y;
         }
@@ -53,7 +49,6 @@ __device__ __forceinline__ void ldv(const float *__restrict__ p, float *o) {
         for (int k = 0; k < N; ++k) {
             if constexpr (H == kStream) o[k] = __ldcs(p + k);
             else if constexpr (H == kReadOnly) o[k] = __ldg(p + k);
-            else if constexpr (H == kL2) o[k] = __ldcg(p + k);
             else o[k] = p[k];
         }
     }
