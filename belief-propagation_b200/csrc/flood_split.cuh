@@ -141,7 +141,8 @@ __device__ __forceinline__ void split_finalize(const SplitArgs &a, bool want, do
 // (the second pass re-reads them, from L1).  Nodes grid-stride.  NV selects
 // the form of the loads (sweeps; the same results): 0 plain, 1 the loop
 // unrolled by 4 by the compiler, 2 the send indices and messages through
-// the read-only path.  Measured forms that were slower, on the 16.8M-node
+// the read-only path, 3 as 1 with the next node's row pointers and belief
+// loaded one round ahead.  Measured forms that were slower, on the 16.8M-node
 // graph with nodes renumbered by out-degree (ties by id): four messages
 // loaded before their use (0.43 ms against 0.34 ms per launch), warp tiles
 // staging a tile's messages through shared memory (0.45 ms), and a group of
@@ -167,13 +168,39 @@ __global__ void __launch_bounds__(kNodeThreads) k_flood_nodes(const SplitArgs a)
     const int mp = (int)((ctl->msg_parity0 + it) & 1u), qp = (int)((ctl->q_parity0 + it) & 1u);
     const float *__restrict__ m_new = mp ? a.s_msg0 : a.s_msg1;
     float *__restrict__ q_out = qp ? a.q0 : a.q1;
-    for (uint32_t v = blockIdx.x * NT + threadIdx.x; v < a.V; v += gridDim.x * NT) {
-        const uint32_t r0 = a.in_ptr[v], r1 = a.in_ptr[v + 1];
+    // NV 3: the next node's row pointers and belief are loaded one round
+    // ahead, so a node's chain starts at its in-edges' send indices
+    const uint32_t stride = gridDim.x * NT;
+    uint32_t v = blockIdx.x * NT + threadIdx.x;
+    uint32_t nr0 = 0, nr1 = 0;
+    float nb[MS];
+    if (NV == 3 && v < a.V) {
+        nr0 = a.in_ptr[v];
+        nr1 = a.in_ptr[v + 1];
+        ldv<MS, kStream>(a.belief + (size_t)v * MS, nb);
+    }
+    for (; v < a.V; v += stride) {
+        uint32_t r0, r1;
         float b[MS], prod[MS];
-        ldv<MS, kStream>(a.belief + (size_t)v * MS, b);
+        if constexpr (NV == 3) {
+            r0 = nr0;
+            r1 = nr1;
+#pragma unroll
+            for (int s = 0; s < MS; ++s) b[s] = nb[s];
+            const uint64_t vn = (uint64_t)v + stride;
+            if (vn < a.V) {
+                nr0 = a.in_ptr[vn];
+                nr1 = a.in_ptr[vn + 1];
+                ldv<MS, kStream>(a.belief + (size_t)vn * MS, nb);
+            }
+        } else {
+            r0 = a.in_ptr[v];
+            r1 = a.in_ptr[v + 1];
+            ldv<MS, kStream>(a.belief + (size_t)v * MS, b);
+        }
 #pragma unroll
         for (int s = 0; s < MS; ++s) prod[s] = 1.0f;
-        if constexpr (NV == 1) {
+        if constexpr (NV == 1 || NV == 3) {
 #pragma unroll 4
             for (uint32_t p = r0; p < r1; ++p) {
                 float mm[MS];

@@ -2094,6 +2094,7 @@ static int split_run(bp_graph *g, uint32_t k, uint32_t *nparts) {
         const int nv = env ? atoi(env) : 1;
         if (nv == 0) return split_run_nv<MS, SER, 0>(g, k, nparts);
         if (nv == 2) return split_run_nv<MS, SER, 2>(g, k, nparts);
+        if (nv == 3) return split_run_nv<MS, SER, 3>(g, k, nparts);
         return split_run_nv<MS, SER, 1>(g, k, nparts);
     }
     return split_run_nv<MS, SER, 0>(g, k, nparts);

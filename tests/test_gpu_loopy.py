@@ -325,7 +325,7 @@ def test_loopy_split_schedule_parity(bp, synth, restatement, O, monkeypatch, cas
             np.testing.assert_array_equal(f64[k], blk[k])
 
 
-@pytest.mark.parametrize("nodes_form", ["0", "1", "2"])
+@pytest.mark.parametrize("nodes_form", ["0", "1", "2", "3"])
 @pytest.mark.parametrize("range_nodes", ["1", "4096"])
 def test_loopy_split_schedule_ragged_power_law(bp, synth, restatement, O, monkeypatch, range_nodes, nodes_form):
     """The split schedule on a 2-state power-law graph whose edge count fills
