@@ -2083,21 +2083,23 @@ static int split_run_nv(bp_graph *g, uint32_t k, uint32_t *nparts) {
     return BP_OK;
 }
 
-// BP_SPLIT_NODES=0|1|2: the node pass's load form (sweeps, 2-state graphs;
-// 1, the default, measured 0.859 ms per iteration against 0.876 for 0 and
-// 0.864 for 2 on the 16.8M-node graph; a group of 4 lanes per node, each
-// lane repeating the node's products, measured 2.06 ms and was removed)
+// BP_SPLIT_NODES=0|1|2|3: the node pass's load form (sweeps, 2-state
+// graphs).  3, the default, loads the next node's row pointers and belief one
+// round ahead (32 registers, every thread slot of an SM): 0.767 ms per
+// iteration on the 16.8M-node graph against 0.782 for 1 (the compiler-
+// unrolled loop alone); with ties broken by id, forms 0-2 measured 0.876,
+// 0.859 and 0.864 ms; a group of 4 lanes per node, each lane repeating the
+// node's products, measured 2.06 ms and was removed.
 template <int MS, bool SER>
 static int split_run(bp_graph *g, uint32_t k, uint32_t *nparts) {
     if constexpr (MS == 2) {
         const char *env = getenv("BP_SPLIT_NODES");
-        const int nv = env ? atoi(env) : 1;
+        const int nv = env ? atoi(env) : 3;
         if (nv == 0) return split_run_nv<MS, SER, 0>(g, k, nparts);
         if (nv == 2) return split_run_nv<MS, SER, 2>(g, k, nparts);
-        if (nv == 3) return split_run_nv<MS, SER, 3>(g, k, nparts);
-        return split_run_nv<MS, SER, 1>(g, k, nparts);
+        if (nv == 1) return split_run_nv<MS, SER, 1>(g, k, nparts);
     }
-    return split_run_nv<MS, SER, 0>(g, k, nparts);
+    return split_run_nv<MS, SER, 3>(g, k, nparts);
 }
 
 template <int MS, bool UNI>
