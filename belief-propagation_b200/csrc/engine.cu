@@ -52,12 +52,7 @@ static void ensure_pool(int dev) {
     if (dev < 0 || dev >= 64) return;
     std::lock_guard<std::mutex> lock(g_pool_mutex);
     if (g_pool_ready[dev]) return;
-    // BP_L2_FETCH=<bytes>: the context's maximum L2 fetch granularity (a
-    // limit of this process's context, like its stack size; sweeps)
-    if (const char *env = getenv("BP_L2_FETCH")) {
-        const int gran = atoi(env);
-        if (gran == 32 || gran == 64 || gran == 128) cudaDeviceSetLimit(cudaLimitMaxL2FetchGranularity, (size_t)gran);
-    }
+
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
         uint64_t threshold = UINT64_MAX;
