@@ -112,19 +112,22 @@ int ensure_staging(bp_graph *g, size_t bytes) {
 
 // ---------------------------------------------------------------- kernels --
 
-// in_ptr from destination keys sorted ascending: in_ptr[v] = first position
-// whose key >= v
-__global__ void k_fill_ptr_from_sorted(const uint32_t *__restrict__ keys, uint32_t E, uint32_t V,
-                                       uint32_t *__restrict__ ptr) {
-    uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p > E) return;
-    uint32_t lo = (p == 0) ? 0u : keys[p - 1] + 1u;       // first node starting here
-    uint32_t hi = (p == E) ? V : keys[p];                  // last node starting here
-    for (uint32_t v = lo; v <= hi && v <= V; ++v) {
-        ptr[v] = (uint32_t)p;
-        if (v == 0xffffffffu) break;
-    }
+// row pointers from keys sorted ascending (ptr[v] = first position whose key
+// >= v), in two streaming passes: the end of each key's run is written at
+// end[key] (one write per key present; end is zeroed first), then ptr[v + 1]
+// = max(end[0..v]) and ptr[0] = 0.  A kernel that wrote ptr[lo..hi] for the
+// keys missing between two runs put long runs of absent keys (nodes without
+// in-edges, grouped together by the renumbering) on single threads.
+__global__ void k_run_ends(const uint32_t *__restrict__ keys, uint32_t E, uint32_t *__restrict__ end) {
+    const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= E) return;
+    const uint32_t k = keys[p];
+    if (p + 1 == E || keys[p + 1] != k) end[k] = (uint32_t)(p + 1);
 }
+
+struct MaxU32 {
+    __device__ __forceinline__ uint32_t operator()(uint32_t a, uint32_t b) const { return a > b ? a : b; }
+};
 
 // node_list (V entries, struct graph layout) -> ptr[V+1]
 __global__ void k_ptr_from_node_list(const uint32_t *__restrict__ nl, uint32_t V, uint32_t E,
@@ -320,6 +323,26 @@ static int bits_for(uint32_t n) {
 }
 
 // stable sort of (key, value) pairs by key, device memory
+// ptr[V + 1] from E keys sorted ascending, all below V (see k_run_ends)
+static int fill_ptr_from_sorted(bp_graph *g, const uint32_t *keys, uint32_t E, uint32_t V, uint32_t *ptr) {
+    BP_CUDA(cudaMemsetAsync(ptr, 0, sizeof(uint32_t), g->stream));
+    if (V == 0) return BP_OK;
+    uint32_t *end = nullptr;
+    BP_CUDA(cudaMallocAsync((void **)&end, sizeof(uint32_t) * V, g->stream));
+    BP_CUDA(cudaMemsetAsync(end, 0, sizeof(uint32_t) * V, g->stream));
+    if (E) k_run_ends<<<grid_for(E, 256), 256, 0, g->stream>>>(keys, E, end);
+    BP_CUDA(cudaGetLastError());
+    size_t temp = 0;
+    BP_CUDA(cub::DeviceScan::InclusiveScan(nullptr, temp, end, ptr + 1, MaxU32(), (int64_t)V, g->stream));
+    void *tmp = nullptr;
+    BP_CUDA(cudaMallocAsync(&tmp, temp, g->stream));
+    cudaError_t e = cub::DeviceScan::InclusiveScan(tmp, temp, end, ptr + 1, MaxU32(), (int64_t)V, g->stream);
+    cudaFreeAsync(tmp, g->stream);
+    cudaFreeAsync(end, g->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "DeviceScan::InclusiveScan", __FILE__, __LINE__);
+    return BP_OK;
+}
+
 static int radix_sort_pairs(bp_graph *g, const uint32_t *keys_in, uint32_t *keys_out,
                             const uint32_t *vals_in, uint32_t *vals_out, uint32_t n, uint32_t key_range) {
     if (n == 0) return BP_OK;
@@ -395,8 +418,7 @@ int ensure_out_csr(bp_graph *g) {
         BP_CUDA(cudaGetLastError());
     }
     if ((st = radix_sort_pairs(g, src_e, keys, iota, order, E, V))) return st;
-    k_fill_ptr_from_sorted<<<grid_for((uint64_t)E + 1, 256), 256, 0, g->stream>>>(keys, E, V, g->out_ptr);
-    BP_CUDA(cudaGetLastError());
+    if ((st = fill_ptr_from_sorted(g, keys, E, V, g->out_ptr))) return st;
     if (E) {
         k_out_arrays<<<grid_for(E, 256), 256, 0, g->stream>>>(order, g->edge_pos, g->pos_dst, E, g->out_pos,
                                                               g->out_dst);
@@ -737,8 +759,7 @@ static int create_impl(bp_graph *g, const bp_graph_desc *d) {
             BP_CUDA(cudaGetLastError());
         }
         if ((st = radix_sort_pairs(g, (const uint32_t *)dst, keys, iota, g->pos_edge, E, V))) return st;
-        k_fill_ptr_from_sorted<<<grid_for((uint64_t)E + 1, 256), 256, 0, g->stream>>>(keys, E, V, g->in_ptr);
-        BP_CUDA(cudaGetLastError());
+        if ((st = fill_ptr_from_sorted(g, keys, E, V, g->in_ptr))) return st;
         cudaFreeAsync(iota, g->stream);
         cudaFreeAsync(keys, g->stream);
     }
