@@ -7,7 +7,7 @@
 //   in_ptr   u32 [V+1]        row starts of each node's in-edges
 //   in_src   u32 [E]          source node of the edge at position p
 //   pos_edge u32 [E]          edge id at position p      (dest_nodes_to_edges_edge_list)
-//   edge_pos u32 [E]          position of edge id e
+//   edge_pos u32 [E]          position of edge id e (built on first use)
 //   pos_dims u8  [E]          x | y<<4 (source / destination state count); mixed graphs only
 //   node_s   u8  [V]          state count per node; mixed graphs only
 //   joint    f32 [E][MS][MS]  joint tables in position order, zero padded
@@ -207,6 +207,7 @@ void tree_clear(bp_graph *g);
 int tree_prepare_host(bp_graph *g, const uint32_t *levels, uint32_t num_levels);
 int tree_build_levels_gpu(bp_graph *g, uint32_t *levels, uint32_t *num_levels);
 int ensure_staging(bp_graph *g, size_t bytes);
+int ensure_edge_pos(bp_graph *g);
 int ensure_out_csr(bp_graph *g);
 int ensure_host_in_ptr(bp_graph *g);
 // split flooding schedule: build g->split with source ranges of

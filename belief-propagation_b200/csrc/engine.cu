@@ -146,7 +146,7 @@ __global__ void k_positions(const uint32_t *__restrict__ pos_edge, const uint32_
     uint32_t e = pos_edge[p];
     uint32_t s = src[e];
     in_src[p] = s;
-    edge_pos[e] = (uint32_t)p;
+    if (edge_pos) edge_pos[e] = (uint32_t)p;
     if (pos_dims) pos_dims[p] = (uint8_t)(node_s[s] | (node_s[dst[e]] << 4));
 }
 
@@ -398,9 +398,23 @@ int ensure_host_in_ptr(bp_graph *g) {
 
 // src-sorted CSR for the tree schedule: out-edges of a node in insertion
 // order (graph.c:249-283), as positions and destination nodes
+// the inverse of pos_edge, for the callers that walk edges in id order (the
+// source-sorted CSR, the edge schedule); a graph build skips it: its scatter
+// of E 4-byte stores at random positions cost more DRAM traffic than any
+// other step of the build
+int ensure_edge_pos(bp_graph *g) {
+    if (g->edge_pos || g->E == 0) return BP_OK;
+    int st;
+    if ((st = dev_alloc(g, (void **)&g->edge_pos, sizeof(uint32_t) * (size_t)g->E))) return st;
+    k_invert_perm<<<grid_for(g->E, 256), 256, 0, g->stream>>>(g->pos_edge, g->E, g->edge_pos);
+    BP_CUDA(cudaGetLastError());
+    return BP_OK;
+}
+
 int ensure_out_csr(bp_graph *g) {
     if (g->out_ptr) return BP_OK;
     int st;
+    if ((st = ensure_edge_pos(g))) return st;
     uint32_t E = g->E, V = g->V;
     if ((st = dev_alloc(g, (void **)&g->out_ptr, sizeof(uint32_t) * ((size_t)V + 1)))) return st;
     if ((st = dev_alloc(g, (void **)&g->out_pos, sizeof(uint32_t) * (size_t)E))) return st;
@@ -584,7 +598,7 @@ static int create_impl(bp_graph *g, const bp_graph_desc *d) {
     if ((st = dev_alloc(g, (void **)&g->in_ptr, sizeof(uint32_t) * ((size_t)V + 1 + kArrayPadNodes)))) return st;
     if ((st = dev_alloc(g, (void **)&g->in_src, sizeof(uint32_t) * ((size_t)E + kArrayPadEdges)))) return st;
     if ((st = dev_alloc(g, (void **)&g->pos_edge, sizeof(uint32_t) * (size_t)E))) return st;
-    if ((st = dev_alloc(g, (void **)&g->edge_pos, sizeof(uint32_t) * (size_t)E))) return st;
+    // edge_pos (position of each edge id) is built on first use (ensure_edge_pos)
     if ((st = dev_alloc(g, (void **)&g->node_s, (size_t)V))) return st;
     if (!g->uniform && (st = dev_alloc(g, (void **)&g->pos_dims, (size_t)E))) return st;
     if ((st = dev_alloc(g, (void **)&g->joint, sizeof(float) * ms * ms * ((size_t)E + kArrayPadEdges)))) return st;
@@ -767,7 +781,7 @@ static int create_impl(bp_graph *g, const bp_graph_desc *d) {
     if (E) {
         k_positions<<<grid_for(E, 256), 256, 0, g->stream>>>(g->pos_edge, (const uint32_t *)src,
                                                              (const uint32_t *)dst, E, g->node_s, g->in_src,
-                                                             g->edge_pos, g->pos_dims);
+                                                             nullptr, g->pos_dims);
         BP_CUDA(cudaGetLastError());
     }
 

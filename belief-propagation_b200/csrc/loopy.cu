@@ -2501,7 +2501,7 @@ int bp_loopy(bp_graph *g, const bp_loopy_options *opt, bp_loopy_result *res) {
     if (fgrid) grid_blocks = std::max(grid_blocks, (serial ? 10u : 2u) * fgrid);
     if ((st = ensure_partials(g, grid_blocks))) return st;
     if (serial && (st = ensure_absdiff(g))) return st;
-    if (opt->schedule == BP_SCHEDULE_EDGE && (st = ensure_runs(g))) return st;
+    if (opt->schedule == BP_SCHEDULE_EDGE && ((st = ensure_runs(g)) || (st = ensure_edge_pos(g)))) return st;
 
     const uint32_t n_launch = ce <= 1 ? max_it : ((max_it + ce - 1) / ce) * ce;
     uint32_t chunk = opt->graph_chunk;
