@@ -137,17 +137,38 @@ __global__ void k_ptr_from_node_list(const uint32_t *__restrict__ nl, uint32_t V
     if (v == V) ptr[V] = E;
 }
 
+// in_src (and pos_dims) at every position from the edge ids there: a
+// gather by edge id (graphs given with the caller's destination CSR)
 __global__ void k_positions(const uint32_t *__restrict__ pos_edge, const uint32_t *__restrict__ src,
                             const uint32_t *__restrict__ dst, uint32_t E,
                             const uint8_t *__restrict__ node_s, uint32_t *__restrict__ in_src,
-                            uint32_t *__restrict__ edge_pos, uint8_t *__restrict__ pos_dims) {
+                            uint8_t *__restrict__ pos_dims) {
     uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= E) return;
     uint32_t e = pos_edge[p];
     uint32_t s = src[e];
     in_src[p] = s;
-    if (edge_pos) edge_pos[e] = (uint32_t)p;
     if (pos_dims) pos_dims[p] = (uint8_t)(node_s[s] | (node_s[dst[e]] << 4));
+}
+
+// the destination sort carries (source, edge id) as one 64-bit value, so
+// in_src and pos_edge come out of the sort in position order without a
+// gather by edge id (each such random 4-byte read cost about 128 B of DRAM)
+__global__ void k_pack_src_id(const uint32_t *__restrict__ src, uint32_t E, uint64_t *__restrict__ out) {
+    const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < E) out[e] = ((uint64_t)src[e] << 32) | e;
+}
+
+__global__ void k_unpack_positions(const uint64_t *__restrict__ vals, const uint32_t *__restrict__ dst_sorted,
+                                   uint32_t E, const uint8_t *__restrict__ node_s, uint32_t *__restrict__ in_src,
+                                   uint32_t *__restrict__ pos_edge, uint8_t *__restrict__ pos_dims) {
+    const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= E) return;
+    const uint64_t v = vals[p];
+    const uint32_t s = (uint32_t)(v >> 32);
+    in_src[p] = s;
+    pos_edge[p] = (uint32_t)v;
+    if (pos_dims) pos_dims[p] = (uint8_t)(node_s[s] | (node_s[dst_sorted[p]] << 4));
 }
 
 __global__ void k_states_u8(const uint32_t *__restrict__ s32, uint32_t V, uint32_t uniform,
@@ -343,8 +364,9 @@ static int fill_ptr_from_sorted(bp_graph *g, const uint32_t *keys, uint32_t E, u
     return BP_OK;
 }
 
+template <typename T>
 static int radix_sort_pairs(bp_graph *g, const uint32_t *keys_in, uint32_t *keys_out,
-                            const uint32_t *vals_in, uint32_t *vals_out, uint32_t n, uint32_t key_range) {
+                            const T *vals_in, T *vals_out, uint32_t n, uint32_t key_range) {
     if (n == 0) return BP_OK;
     size_t temp = 0;
     int end_bit = bits_for(key_range + 1);
@@ -764,24 +786,33 @@ static int create_impl(bp_graph *g, const bp_graph_desc *d) {
         if (own_nl) cudaFreeAsync(nl, g->stream);
         if (own_el) cudaFreeAsync(el, g->stream);
     } else {
-        // stable sort of edge ids by destination
-        uint32_t *iota = nullptr, *keys = nullptr;
-        BP_CUDA(cudaMallocAsync((void **)&iota, sizeof(uint32_t) * (E ? E : 1), g->stream));
+        // stable sort of (source, edge id) by destination
+        uint64_t *vals = nullptr, *vals_sorted = nullptr;
+        uint32_t *keys = nullptr;
+        BP_CUDA(cudaMallocAsync((void **)&vals, sizeof(uint64_t) * (E ? E : 1), g->stream));
+        BP_CUDA(cudaMallocAsync((void **)&vals_sorted, sizeof(uint64_t) * (E ? E : 1), g->stream));
         BP_CUDA(cudaMallocAsync((void **)&keys, sizeof(uint32_t) * (E ? E : 1), g->stream));
         if (E) {
-            k_iota<<<grid_for(E, 256), 256, 0, g->stream>>>(iota, E);
+            k_pack_src_id<<<grid_for(E, 256), 256, 0, g->stream>>>((const uint32_t *)src, E, vals);
             BP_CUDA(cudaGetLastError());
         }
-        if ((st = radix_sort_pairs(g, (const uint32_t *)dst, keys, iota, g->pos_edge, E, V))) return st;
+        if ((st = radix_sort_pairs(g, (const uint32_t *)dst, keys, (const uint64_t *)vals, vals_sorted, E, V)))
+            return st;
         if ((st = fill_ptr_from_sorted(g, keys, E, V, g->in_ptr))) return st;
-        cudaFreeAsync(iota, g->stream);
+        if (E) {
+            k_unpack_positions<<<grid_for(E, 256), 256, 0, g->stream>>>(vals_sorted, keys, E, g->node_s, g->in_src,
+                                                                        g->pos_edge, g->pos_dims);
+            BP_CUDA(cudaGetLastError());
+        }
+        cudaFreeAsync(vals, g->stream);
+        cudaFreeAsync(vals_sorted, g->stream);
         cudaFreeAsync(keys, g->stream);
     }
     trace.mark("dest sort");
-    if (E) {
+    if (E && d->dest_node_list && d->dest_edge_list) {
         k_positions<<<grid_for(E, 256), 256, 0, g->stream>>>(g->pos_edge, (const uint32_t *)src,
                                                              (const uint32_t *)dst, E, g->node_s, g->in_src,
-                                                             nullptr, g->pos_dims);
+                                                             g->pos_dims);
         BP_CUDA(cudaGetLastError());
     }
 
