@@ -693,3 +693,29 @@ def test_reserve_cached_memory_then_build_and_solve(bp, synth, restatement, O):
     ora = restatement.loopy(O.OracleGraph(net), 1e-3, 30)
     assert_same(gpu_loopy(bp, net, 1e-3, 30), ora, 2)
     assert lib.bp_release_cached_memory() == 0
+
+
+@pytest.mark.parametrize("reorder", [False, True], ids=["ids", "renumbered"])
+def test_loopy_long_runs_of_nodes_without_in_edges(bp, synth, restatement, O, reorder):
+    """Row pointers from the sorted destinations when long runs of nodes have
+    no in-edges: the first 3000 nodes, 2500 in the middle and the last 2000
+    receive none (renumbered, such nodes of one out-degree are also grouped
+    together).  The oracle's results, and the edge schedule's."""
+    rng = np.random.default_rng(23)
+    V = 10000
+    receivers = np.concatenate([np.arange(3000, 5000), np.arange(7500, 8000)]).astype(np.uint32)
+    E = 24000
+    src = rng.integers(0, V, E).astype(np.uint32)
+    dst = rng.choice(receivers, E).astype(np.uint32)
+    keep = src != dst
+    src, dst = src[keep], dst[keep]
+    j = rng.random((len(src), 2, 2), dtype=np.float32)
+    j /= j.sum(axis=2, keepdims=True)
+    b = rng.random((V, 2), dtype=np.float32)
+    b /= b.sum(axis=1, keepdims=True)
+    net = synth.Network(np.full(V, 2, np.uint32), b, np.zeros(V, np.uint8), src, dst, j)
+    ora = restatement.loopy(O.OracleGraph(net), 1e-3, 30)
+    assert_same(gpu_loopy(bp, net, 1e-3, 30, reorder=reorder), ora, 2)
+    if not reorder:
+        ora_e = restatement.loopy(O.OracleGraph(net), 1e-3, 30, schedule="edge")
+        assert_same(gpu_loopy(bp, net, 1e-3, 30, schedule="edge"), ora_e, 2)
