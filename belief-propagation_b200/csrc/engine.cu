@@ -222,9 +222,14 @@ __global__ void k_beliefs_out(const float *__restrict__ b, uint32_t ld, uint32_t
 }
 
 // out-degree histogram and the renumbering by decreasing out-degree
+// histogram of node ids: the lanes of a warp holding the same id add their
+// count with one atomic (edge lists grouped by source, and a power-law
+// graph's hubs, otherwise queue thousands of atomics on one address)
 __global__ void k_out_degree(const uint32_t *__restrict__ src, uint32_t E, uint32_t *__restrict__ deg) {
-    uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e < E) atomicAdd(deg + src[e], 1u);
+    const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t key = e < E ? src[e] : 0xffffffffu;
+    const unsigned same = __match_any_sync(0xffffffffu, key);
+    if (e < E && (threadIdx.x & 31u) == (unsigned)(__ffs(same) - 1)) atomicAdd(deg + key, (unsigned)__popc(same));
 }
 
 // sort keys: decreasing out-degree; with indeg, then increasing in-degree
