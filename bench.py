@@ -17,7 +17,8 @@ e2e    the same metric through the public C-ABI with host (pinned) buffers:
        every step uploads the graph (edges, tables, priors), builds the
        destination-sorted layout on the GPU, runs, and reads the beliefs back;
        the steps are pipelined as a serving loop runs them (step k+1's upload
-       and build on a second stream and host thread during step k's solve),
+       and build on a second stream and host thread, and step k-1's read-back
+       on a third host thread, during step k's solve),
        timed by wall clock from the first upload to the last read; the
        median of three such runs.  The loop reserves its device memory once
        at start-up (bp_reserve_cached_memory).
@@ -1082,32 +1083,42 @@ def main():
 
         # pipelined, as a serving loop runs it: a second host thread builds
         # graph k+1 (pinned-host upload, device CSR build, beliefs) on its own
-        # stream while this thread solves graph k and reads its beliefs back;
-        # every step's copies and work stay inside the timed region, which
-        # runs from before the first build to after the last read
+        # stream while this thread solves graph k and a third reads graph
+        # k-1's beliefs back; every step's copies and work stay inside the
+        # timed region, which runs from before the first build to after the
+        # last read
         from concurrent.futures import ThreadPoolExecutor
         # equal stream priorities: a low-priority build starves for a whole
         # CUDA-graph chunk of the solve at each of its host synchronisations
-        streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+        streams = [torch.cuda.Stream() for _ in range(3)]
         outs = [out_h, torch.empty((V, S), dtype=torch.float32).pin_memory()]
 
         def build(k):
-            gk = BPGraph(V, src_h, dst_h, joint_h, uniform_states=2, stream=streams[k % 2].cuda_stream,
+            gk = BPGraph(V, src_h, dst_h, joint_h, uniform_states=2, stream=streams[k % 3].cuda_stream,
                          reorder=bool(a.reorder))
             gk.set_beliefs(bel_h)
             return gk
 
+        def finish(gk, k):
+            gk.beliefs(out=outs[k % 2])
+            gk.close()
+
         def pipelined(n):
-            with ThreadPoolExecutor(max_workers=1) as ex:
+            # three host threads: this one solves graph k while one builds
+            # graph k+1 and another reads graph k-1's beliefs back (device to
+            # pinned host) and releases it; the run ends after the last read
+            with ThreadPoolExecutor(max_workers=1) as ex, ThreadPoolExecutor(max_workers=1) as rd:
                 fut = ex.submit(build, 0)
+                reads = []
                 for k in range(n):
                     gk = fut.result()
                     if k + 1 < n:
                         fut = ex.submit(build, k + 1)
                     gk.init_messages()
                     gk.loopy(0.0, a.iterations, delta="f64")
-                    gk.beliefs(out=outs[k % 2])
-                    gk.close()
+                    reads.append(rd.submit(finish, gk, k))
+                for r in reads:
+                    r.result()
 
         pipelined(2)
         barrier()
@@ -1124,7 +1135,8 @@ def main():
                "ms_per_step": ems, "steps": a.e2e_steps,
                "timing": "wall clock over all steps, first build included; median of 3 runs",
                "runs_ms_per_step": [round(r, 2) for r in runs],
-               "pipelined": "the build of step k+1 (its H2D copies included) overlaps the solve of step k",
+               "pipelined": "the build of step k+1 (its H2D copies included) and the read-back of step k-1 overlap "
+                            "the solve of step k",
                "sequential_ms_per_step": round(max_over_ranks(seq_ms, dist), 2),
                "pool_reserved_bytes": reserve,
                "phases_wall_ms": {k: round(v, 2) for k, v in phases.items()}}
