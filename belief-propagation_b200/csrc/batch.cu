@@ -57,7 +57,6 @@ struct BatchArgs {
     float tol;
     uint32_t max_it;
     int serial, init;
-    int row_lanes;        // edge phase with S lanes per edge where kRowLanes<S>
 };
 
 // the reference's serial fp32 sum of x[0, n) (graph.c:1300-1309), one thread
@@ -121,11 +120,6 @@ __device__ float net_serial_sum_block(const float *x, uint64_t n, float *buf, ui
     return r;
 }
 
-// the edge phase with S lanes per edge, for state counts that divide a warp
-// and whose tables span several lines per thread (BatchArgs::row_lanes;
-// BP_BATCH_ROW_LANES=0 keeps a thread per edge)
-template <int S> constexpr bool kRowLanes = (S == 4 || S == 8);
-
 template <int S, bool SER>
 __device__ void solve_network(const BatchArgs &a, uint32_t n, double *red, int *s_flag, double *s_tot, float *s_res,
                               float *sbuf) {
@@ -180,69 +174,24 @@ __device__ void solve_network(const BatchArgs &a, uint32_t n, double *red, int *
         const float *q_in = q[it & 1];
         float *q_out = q[(it + 1) & 1];
         double dsum = 0.0;
-        bool lanes_done = false;
-        if constexpr (kRowLanes<S>) {
-          if (a.row_lanes) {
-            lanes_done = true;
-            // S lanes per edge, lane r computing row r of J q: a warp reads
-            // 32 / S consecutive edges' tables as one contiguous run (with a
-            // thread per edge each lane's S * S floats sat in a different
-            // line).  Every lane forms the row sums' total itself, adding
-            // the rows in order from its group's lanes, so each value is
-            // send_msg's.
-            constexpr uint32_t EPW = 32u / S;
-            const uint32_t lane = tid & 31u, row = lane % S, first = lane - row;
-            const uint32_t nw = T >> 5;
-            for (uint32_t p0 = (tid >> 5) * EPW; p0 < E; p0 += nw * EPW) {
-                const uint32_t p = p0 + lane / S;
-                const bool ok = p < E;
-                float part = 0.0f, o = 0.0f;
-                if (ok) {
-                    float qq[S], jr[S];
-                    ldv<S>(q_in + (size_t)src[p] * S, qq);
-                    ldv<S, kStream>(J + (size_t)p * S * S + (size_t)row * S, jr);
-                    o = m_old[(size_t)p * S + row];
+        for (uint32_t p = tid; p < E; p += T) {
+            float qq[S], m[S], o[S];
+            ldv<S>(q_in + (size_t)src[p] * S, qq);
+            ldv<S>(m_old + (size_t)p * S, o);
+            send_msg<S, true>(J + (size_t)p * S * S, qq, S, S, m);
+            float ad[S];
 #pragma unroll
-                    for (int c = 0; c < S; ++c) part = FADD(part, FMUL(jr[c], qq[c]));
-                }
-                float tot = 0.0f;
-#pragma unroll
-                for (int i = 0; i < S; ++i) tot = FADD(tot, __shfl_sync(0xffffffffu, part, (int)(first + i)));
-                if (tot <= 0.0f) tot = 1.0f;
-                const float m = FDIV(part, tot);
-                if (ok) {
-                    float d = FSUB(o, m);
-                    if (d != d) d = 0.0f;
-                    d = fabsf(d);
-                    dsum += (double)d;
-                    if constexpr (SER)
-                        a.absdiff[(size_t)(it & 1u) * a.ad_stride + ni.msg_off +
-                                  (size_t)a.pos_edge[ni.edge_off + p] * S + row] = d;
-                    m_new[(size_t)p * S + row] = m;
-                }
+            for (int k = 0; k < S; ++k) {
+                float d = FSUB(o[k], m[k]);
+                if (d != d) d = 0.0f;
+                ad[k] = fabsf(d);
+                dsum += (double)ad[k];
             }
-          }
-        }
-        if (!lanes_done) {
-            for (uint32_t p = tid; p < E; p += T) {
-                float qq[S], m[S], o[S];
-                ldv<S>(q_in + (size_t)src[p] * S, qq);
-                ldv<S>(m_old + (size_t)p * S, o);
-                send_msg<S, true>(J + (size_t)p * S * S, qq, S, S, m);
-                float ad[S];
-#pragma unroll
-                for (int k = 0; k < S; ++k) {
-                    float d = FSUB(o[k], m[k]);
-                    if (d != d) d = 0.0f;
-                    ad[k] = fabsf(d);
-                    dsum += (double)ad[k];
-                }
-                if constexpr (SER)
-                    stv<S>(a.absdiff + (size_t)(it & 1u) * a.ad_stride + ni.msg_off +
-                               (size_t)a.pos_edge[ni.edge_off + p] * S,
-                           ad);
-                stv<S>(m_new + (size_t)p * S, m);
-            }
+            if constexpr (SER)
+                stv<S>(a.absdiff + (size_t)(it & 1u) * a.ad_stride + ni.msg_off +
+                           (size_t)a.pos_edge[ni.edge_off + p] * S,
+                       ad);
+            stv<S>(m_new + (size_t)p * S, m);
         }
         __syncthreads();
         for (uint32_t v = tid; v < V; v += T) {
@@ -397,11 +346,9 @@ __device__ void solve_network(const BatchArgs &a, uint32_t n, double *red, int *
     __syncthreads();
 }
 
-// fp64 delta: at most 64 registers, so two 512-thread blocks share an SM
-// (blocks of up to 1024 threads); serial delta: blocks of up to 512 threads
 template <int S, bool SER>
-__global__ void __launch_bounds__(SER ? 512 : 1024, 1) k_batch_solve(const BatchArgs a, const uint32_t *__restrict__ order,
-                                                                    uint32_t count, uint32_t *queue) {
+__global__ void k_batch_solve(const BatchArgs a, const uint32_t *__restrict__ order, uint32_t count,
+                              uint32_t *queue) {
     __shared__ double red[32];
     __shared__ int s_flag;
     __shared__ uint32_t s_next;
@@ -519,8 +466,6 @@ static BatchArgs batch_args(bp_batch *bt, float tol, uint32_t max_it, int serial
     a.max_it = max_it;
     a.serial = serial;
     a.init = init;
-    const char *rl = getenv("BP_BATCH_ROW_LANES");
-    a.row_lanes = (rl && rl[0] == '0') ? 0 : 1;
     return a;
 }
 
@@ -736,7 +681,7 @@ static int batch_create_impl(bp_batch *bt, uint32_t N, const bp_graph_desc *desc
 // ---- autotuning of threads per block, cached on disk ---------------------
 // kernel revision in the autotune key: a cached block size belongs to the
 // kernel it was timed on
-constexpr int kTuneRevision = 4;
+constexpr int kTuneRevision = 3;
 
 static std::string tune_key(bp_batch *bt, const Group &gr, int serial) {
     uint64_t V = 0, E = 0;
