@@ -817,8 +817,6 @@ static int u_backward(bp_unrolled *u) {
                                      u->epart);
         }
         if constexpr (S <= 4) {
-            if (batch == 4 && minb == 3)
-                return u_launch(k_u_bwd<S, 4, 3>, gb, BT, st, g, mode, send, b_t, gbar, xn, out, xo, u->epart, pb);
             if (batch == 4)
                 return u_launch(k_u_bwd<S, 4>, gb, BT, st, g, mode, send, b_t, gbar, xn, out, xo, u->epart, pb);
             if (minb == 3)
