@@ -59,14 +59,7 @@ struct UGraph {
     const uint32_t *pos_out;   // slot in the source-sorted order of the edge at position p
     const uint8_t *pos_tab;
     const float *tables;   // [K][S][S] = log_pair (log joint tables)
-    const uint2 *tile_src;     // per kStTileNodes-node tile: lowest, highest source of its in-edges
 };
-
-// the staged adjoint (k_u_bwd_st): nodes per tile, and the source states and
-// x adjoint slots a tile stages in shared memory at most
-constexpr uint32_t kStTileNodes = 512;
-constexpr uint32_t kStSrcCap = 2048;
-constexpr uint32_t kStXcCap = 2560;
 
 // in-edges whose loads one thread issues together
 template <int S> constexpr int u_batch() { return S <= 4 ? 4 : 2; }
@@ -387,13 +380,11 @@ __global__ void __launch_bounds__(bwd_threads<S>()) k_u_pair_grad(const UGraph g
 // Pbar = the adjoint of the node's summed log-messages, from lbbar_t(v) and
 // lQbar_{t+1}(v) (the gather of iteration t+1's x adjoint terms in v's
 // source-sorted slots); mode 1 is the initial step lQ_1 = lb_0 + lP
-// (xc_base: the slot held at xc_next[0], when the slots sit staged in shared
-// memory)
 template <int S>
 __device__ __forceinline__ void bwd_node_step(const UGraph &g, int mode, uint32_t v, const float *__restrict__ lb_t,
                                               const float *__restrict__ lbbar_t, const float *__restrict__ xc_next,
                                               float *__restrict__ lbbar_out, float *__restrict__ pbar_out,
-                                              float *Pbar, uint32_t xc_base = 0) {
+                                              float *Pbar) {
     float gb[S], gq[S];
 #pragma unroll
     for (int i = 0; i < S; ++i) {
@@ -401,7 +392,7 @@ __device__ __forceinline__ void bwd_node_step(const UGraph &g, int mode, uint32_
         gq[i] = 0.0f;
     }
     if (lbbar_t) ldv<S>(lbbar_t + (size_t)v * S, gb);
-    if (xc_next) sum_slots<S>(xc_next, g.out_ptr[v] - xc_base, g.out_ptr[v + 1] - xc_base, gq);
+    if (xc_next) sum_slots<S>(xc_next, g.out_ptr[v], g.out_ptr[v + 1], gq);
     float out[S];
     if (mode == 0) {
         float lb[S], gs = 0.0f;
@@ -521,91 +512,6 @@ __global__ void __launch_bounds__(bwd_threads<S>(), MB) k_u_bwd(const UGraph g, 
     if (pbar_out) return;
     block_partial_add<S, NT, REG>(acc, sacc, wred, epart + (size_t)blockIdx.x * S * S, sm);
 }
-
-// The same step (1 <= S <= 4) with a tile's operands staged in shared
-// memory: a block takes kStTileNodes consecutive nodes, copies the source
-// states of the tile's in-edges (one contiguous range of node ids, when it
-// fits kStSrcCap) and the tile's x adjoint slots of iteration t+1 (one
-// contiguous range of the source-sorted order, when it fits kStXcCap) with
-// coalesced loads, and then runs k_u_bwd's per-node work against those
-// copies.  A node's chain of dependent global loads (row pointers, in-edge
-// sources, their states; out-slots) becomes one level (the in-edge records).
-// Every value and every sum is k_u_bwd's.
-template <int S>
-__global__ void __launch_bounds__(bwd_threads<S>(), 3)
-    k_u_bwd_st(const UGraph g, int mode, const float *__restrict__ send, const float *__restrict__ lb_t,
-               const float *__restrict__ lbbar_t, const float *__restrict__ xc_next, float *__restrict__ lbbar_out,
-               float *__restrict__ xc, double *__restrict__ epart, float *__restrict__ pbar_out) {
-    static_assert(S <= 4, "register accumulators");
-    constexpr int NT = bwd_threads<S>();
-    constexpr int B = 2;
-    extern __shared__ __align__(16) float dyn[];
-    float *s_send = dyn;                    // kStSrcCap * S
-    float *s_xc = dyn + kStSrcCap * S;      // kStXcCap * S
-    __shared__ __align__(16) float sm[2 * kUMaxTables * S * S];
-    __shared__ float wred[NT / 32][S * S];
-    griddep_launch_dependents();
-    load_tables_smem<S>(g, sm);
-    griddep_wait();
-    float acc[S * S];
-#pragma unroll
-    for (int k = 0; k < S * S; ++k) acc[k] = 0.0f;
-    const bool one_table = pbar_out == nullptr;
-    const uint32_t ntiles = (g.V + kStTileNodes - 1) / kStTileNodes;
-    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const uint32_t v0 = tile * kStTileNodes, v1 = min(v0 + kStTileNodes, g.V);
-        const uint2 sr = g.tile_src[tile];
-        const bool st_src = sr.y >= sr.x && sr.y - sr.x < kStSrcCap;
-        const uint32_t q0 = g.out_ptr[v0], q1 = g.out_ptr[v1];
-        const bool st_xc = xc_next != nullptr && q1 - q0 <= kStXcCap;
-        if (st_src)
-            for (uint32_t i = threadIdx.x; i < (sr.y - sr.x + 1) * S; i += NT) s_send[i] = send[(size_t)sr.x * S + i];
-        if (st_xc)
-            for (uint32_t i = threadIdx.x; i < (q1 - q0) * S; i += NT) s_xc[i] = xc_next[(size_t)q0 * S + i];
-        __syncthreads();
-        const float *x_base = st_src ? s_send : send;
-        const uint32_t x_off = st_src ? sr.x : 0u;
-        for (uint32_t v = v0 + threadIdx.x; v < v1; v += NT) {
-            const uint32_t r0 = g.in_ptr[v], r1 = g.in_ptr[v + 1];
-            float Pbar[S];
-            bwd_node_step<S>(g, mode, v, lb_t, lbbar_t, st_xc ? s_xc : xc_next, lbbar_out, pbar_out, Pbar,
-                             st_xc ? q0 : 0u);
-            float ps = 0.0f;
-#pragma unroll
-            for (int i = 0; i < S; ++i) ps += Pbar[i];
-            for (uint32_t p0 = r0; p0 < r1; p0 += B) {
-                uint32_t src[B], slot[B];
-                uint8_t tb[B];
-#pragma unroll
-                for (int b = 0; b < B; ++b)
-                    if (p0 + b < r1) {
-                        src[b] = g.in_src[p0 + b];
-                        tb[b] = g.pos_tab[p0 + b];
-                        slot[b] = g.pos_out[p0 + b];
-                    }
-#pragma unroll
-                for (int b = 0; b < B; ++b) {
-                    if (p0 + b >= r1) break;
-                    float x[S];
-                    ldv<S>(x_base + (size_t)(src[b] - x_off) * S, x);
-                    float jr[S * S];
-                    ldv<S * S>(edge_table<S>(sm, tb[b]), jr);
-                    float e[S], ci[S], c[S];
-                    bwd_edge<S>(jr, x, Pbar, ps, e, ci, c);
-                    if (one_table) add_table_outer<S, NT, true>(acc, nullptr, ci, e, (tb[b] & 0x80u) != 0);
-                    stv<S>(xc + (size_t)slot[b] * S, c);
-                }
-            }
-        }
-        __syncthreads();   // the staged copies are rewritten by the next tile
-    }
-    // several tables: k_u_pair_grad adds the table adjoint
-    if (pbar_out) return;
-    block_partial_add<S, NT, true>(acc, nullptr, wred, epart + (size_t)blockIdx.x * S * S, sm);
-}
-
-template <int S>
-constexpr size_t st_smem_bytes() { return sizeof(float) * (size_t)(kStSrcCap + kStXcCap) * S; }
 
 // ---- the one-table adjoint on the tensor cores (5 <= S <= 8) ------------
 // With one shared table J, the table adjoint is J (.) sum over edges of
@@ -787,7 +693,6 @@ struct bp_unrolled {
     uint32_t *in_ptr = nullptr, *in_src = nullptr, *out_ptr = nullptr, *pos_out = nullptr;
     uint8_t *pos_tab = nullptr;
     float *tables = nullptr;
-    uint2 *tile_src = nullptr;                  // per staged-adjoint tile: lowest, highest in-edge source
     float *ck_b = nullptr, *ck_q = nullptr;    // [nck][V][S]
     float *seg_b = nullptr, *seg_q = nullptr;  // [2][ck][V][S] (slot 0 unused), by segment parity
     cudaStream_t side = nullptr;                // the backward's recompute stream
@@ -823,12 +728,11 @@ static bool u_pdl() {
 }
 
 template <typename... KArgs, typename... Args>
-static int u_launch_smem(void (*kern)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t st,
-                         Args... args) {
+static int u_launch(void (*kern)(KArgs...), unsigned grid, unsigned block, cudaStream_t st, Args... args) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(block);
-    cfg.dynamicSmemBytes = smem;
+    cfg.dynamicSmemBytes = 0;
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -838,33 +742,6 @@ static int u_launch_smem(void (*kern)(KArgs...), unsigned grid, unsigned block, 
     cudaError_t e = cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
     if (e != cudaSuccess) return cuda_fail(e, "cudaLaunchKernelEx", __FILE__, __LINE__);
     return BP_OK;
-}
-
-template <typename... KArgs, typename... Args>
-static int u_launch(void (*kern)(KArgs...), unsigned grid, unsigned block, cudaStream_t st, Args... args) {
-    return u_launch_smem(kern, grid, block, 0, st, args...);
-}
-
-// the staged adjoint's dynamic shared memory, allowed once per process and
-// state count (before any capture: bp_unrolled_create calls it)
-template <int S>
-static int st_prepare() {
-    if constexpr (S <= 4) {
-        static bool done = false;
-        if (!done) {
-            BP_CUDA(cudaFuncSetAttribute(k_u_bwd_st<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)st_smem_bytes<S>()));
-            done = true;
-        }
-    }
-    return BP_OK;
-}
-
-// BP_UBWD_STAGE=1: the adjoint with the tile's operands staged in shared
-// memory (1-4 states)
-static bool ubwd_stage() {
-    const char *env = getenv("BP_UBWD_STAGE");
-    return env && env[0] == '1';
 }
 
 // in-edges per batch of the adjoint kernel (BP_UBWD_BATCH=2|4, 1-4 states)
@@ -878,7 +755,7 @@ static int ubwd_env(const char *name, int dflt, int alt) {
 // into a CUDA graph, replayed on every call
 template <int S>
 static int u_forward(bp_unrolled *u) {
-    const UGraph g{u->V, u->K, u->in_ptr, u->in_src, u->out_ptr, u->pos_out, u->pos_tab, u->tables, u->tile_src};
+    const UGraph g{u->V, u->K, u->in_ptr, u->in_src, u->out_ptr, u->pos_out, u->pos_tab, u->tables};
     const size_t VS = (size_t)u->V * S;
     const unsigned gv = grid_for(u->V, kUThreads);
     cudaStream_t st = u->stream;
@@ -916,7 +793,7 @@ static int u_forward(bp_unrolled *u) {
 // entry; gtheta_buf, glogp_buf receive the gradients)
 template <int S>
 static int u_backward(bp_unrolled *u) {
-    const UGraph g{u->V, u->K, u->in_ptr, u->in_src, u->out_ptr, u->pos_out, u->pos_tab, u->tables, u->tile_src};
+    const UGraph g{u->V, u->K, u->in_ptr, u->in_src, u->out_ptr, u->pos_out, u->pos_tab, u->tables};
     const size_t VS = (size_t)u->V * S;
     const unsigned gv = grid_for(u->V, kUThreads);
     constexpr int BT = bwd_threads<S>();
@@ -928,10 +805,6 @@ static int u_backward(bp_unrolled *u) {
     // 85 registers (3 blocks per SM) instead of 64 (4 blocks)
     const int minb = ubwd_env("BP_UBWD_MINB", 4, 3);
     const unsigned gb = mma ? grid_for(u->V, kMmaThreads * 2) : grid_for(u->V, BT * npt);
-    const bool stage = S <= 4 && ubwd_stage();
-    // the staged adjoint takes a tile per block (its partial rows fit epart:
-    // kStTileNodes >= 64 nodes per block)
-    const unsigned gst = grid_for(u->V, kStTileNodes);
     // the recompute keeps the forward's grid, a thread per node: on smaller
     // grids beside the adjoint (80-296 blocks) it became the critical path
     const unsigned rgrid = gv;
@@ -944,9 +817,6 @@ static int u_backward(bp_unrolled *u) {
                                      u->epart);
         }
         if constexpr (S <= 4) {
-            if (stage)
-                return u_launch_smem(k_u_bwd_st<S>, gst, BT, st_smem_bytes<S>(), st, g, mode, send, b_t, gbar, xn, out,
-                                     xo, u->epart, pb);
             if (batch == 4)
                 return u_launch(k_u_bwd<S, 4>, gb, BT, st, g, mode, send, b_t, gbar, xn, out, xo, u->epart, pb);
             if (minb == 3)
@@ -954,7 +824,7 @@ static int u_backward(bp_unrolled *u) {
         }
         return u_launch(k_u_bwd<S, 2>, gb, BT, st, g, mode, send, b_t, gbar, xn, out, xo, u->epart, pb);
     };
-    BP_CUDA(cudaMemsetAsync(u->epart, 0, sizeof(double) * u->K * std::max(gb, gst) * S * S, st));
+    BP_CUDA(cudaMemsetAsync(u->epart, 0, sizeof(double) * u->K * gb * S * S, st));
     // several tables: the table adjoint of each backward step, one pass per table
     auto pair_grads = [&](const float *send) -> int {
         for (uint32_t k = 0; u->K > 1 && k < u->K; ++k) {
@@ -1026,7 +896,7 @@ static int u_backward(bp_unrolled *u) {
 
 static void u_free(bp_unrolled *u) {
     if (!u) return;
-    void *ptrs[] = {u->in_ptr, u->in_src, u->out_ptr, u->pos_out, u->pos_tab, u->tables, u->tile_src, u->ck_b, u->ck_q,
+    void *ptrs[] = {u->in_ptr, u->in_src, u->out_ptr, u->pos_out, u->pos_tab, u->tables, u->ck_b, u->ck_q,
                     u->seg_b, u->seg_q, u->pp_b, u->pp_q, u->bT, u->bbar[0], u->bbar[1], u->xc[0],
                     u->xc[1], u->epart, u->theta_buf, u->gtheta_buf, u->glogp_buf, u->pbar};
     for (void *p : ptrs)
@@ -1172,19 +1042,6 @@ int bp_unrolled_create(bp_unrolled **out, uint32_t V, uint32_t E, uint32_t S, ui
     }
     std::vector<uint32_t> ofill(out_ptr.begin(), out_ptr.end() - 1);
     for (uint32_t e = 0; e < E; ++e) pos_out[pos_of[e]] = ofill[src[e]]++;
-    // per staged-adjoint tile: the range of its in-edges' sources (lo > hi:
-    // no in-edge)
-    const uint32_t ntiles = (V + kStTileNodes - 1) / kStTileNodes;
-    std::vector<uint2> tile_src(ntiles ? ntiles : 1, make_uint2(1u, 0u));
-    for (uint32_t t = 0; t < ntiles; ++t) {
-        const uint32_t v0 = t * kStTileNodes, v1 = std::min(v0 + kStTileNodes, V);
-        uint32_t lo = 0xffffffffu, hi = 0;
-        for (uint32_t p = in_ptr[v0]; p < in_ptr[v1]; ++p) {
-            lo = std::min(lo, in_src[p]);
-            hi = std::max(hi, in_src[p]);
-        }
-        if (in_ptr[v1] > in_ptr[v0]) tile_src[t] = make_uint2(lo, hi);
-    }
     const size_t VS = (size_t)V * S;
     u->nblk = grid_for(V, 64);   // partial slots for the smallest backward block
     auto alloc = [&](void **p, size_t bytes) {
@@ -1192,8 +1049,7 @@ int bp_unrolled_create(bp_unrolled **out, uint32_t V, uint32_t E, uint32_t S, ui
     };
     bool ok = alloc((void **)&u->in_ptr, sizeof(uint32_t) * (V + 1)) && alloc((void **)&u->in_src, 4 * (size_t)E) &&
               alloc((void **)&u->out_ptr, sizeof(uint32_t) * (V + 1)) && alloc((void **)&u->pos_out, 4 * (size_t)E) &&
-              alloc((void **)&u->pos_tab, (size_t)E) &&
-              alloc((void **)&u->tile_src, sizeof(uint2) * tile_src.size()) && alloc((void **)&u->tables, sizeof(float) * K * S * S) &&
+              alloc((void **)&u->pos_tab, (size_t)E) && alloc((void **)&u->tables, sizeof(float) * K * S * S) &&
               alloc((void **)&u->ck_b, sizeof(float) * VS * u->nck) &&
               alloc((void **)&u->ck_q, sizeof(float) * VS * u->nck) &&
               alloc((void **)&u->seg_b, sizeof(float) * VS * 2 * ck) &&
@@ -1212,8 +1068,6 @@ int bp_unrolled_create(bp_unrolled **out, uint32_t V, uint32_t E, uint32_t S, ui
         return set_error(BP_ERR_NOMEM, "device allocation failed for the unrolled graph");
     }
     cudaMemcpyAsync(u->in_ptr, in_ptr.data(), 4 * (V + 1), cudaMemcpyHostToDevice, u->stream);
-    cudaMemcpyAsync(u->tile_src, tile_src.data(), sizeof(uint2) * tile_src.size(), cudaMemcpyHostToDevice,
-                    u->stream);
     cudaMemcpyAsync(u->out_ptr, out_ptr.data(), 4 * (V + 1), cudaMemcpyHostToDevice, u->stream);
     if (E) {
         cudaMemcpyAsync(u->in_src, in_src.data(), 4 * (size_t)E, cudaMemcpyHostToDevice, u->stream);
@@ -1230,13 +1084,6 @@ int bp_unrolled_create(bp_unrolled **out, uint32_t V, uint32_t E, uint32_t S, ui
     if (!evok) {
         u_free(u);
         return set_error(BP_ERR_CUDA, "stream or event creation failed");
-    }
-    {
-        auto prep = [&]() -> int { BP_DISPATCH_S(S, st_prepare); };
-        if (prep() != BP_OK) {
-            u_free(u);
-            return BP_ERR_CUDA;
-        }
     }
     if (cudaStreamSynchronize(u->stream) != cudaSuccess) {
         u_free(u);
