@@ -1054,7 +1054,10 @@ def main():
         # slack for the pool's fragmentation
         from belief_propagation_b200 import native as N
         reserve = 6 * int(graph_bytes)
-        N.check(N.load().bp_reserve_cached_memory(reserve))
+        if N.load().bp_reserve_cached_memory(reserve) != 0:
+            # not enough free memory for the reservation: the loop runs
+            # without one (and may see the pool's growth stalls)
+            reserve = 0
 
         def e2e_step(record=False):
             t0 = time.perf_counter()
