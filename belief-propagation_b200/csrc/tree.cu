@@ -291,24 +291,6 @@ __global__ void __launch_bounds__(256) k_tree_tail(const TreeTailArgs a) {
     }
 }
 
-// The last small waves of a level in one block: a warp per node (tail_node),
-// the block's barrier between two waves in place of a launch per wave.  Only
-// waves of at most kCtaTailNodes nodes go here (one or two rounds of the
-// block's 32 warps), so the block never holds up a wide wave.
-constexpr uint32_t kCtaTailNodes = 64;
-
-template <int MS, bool UNI>
-__global__ void __launch_bounds__(1024) k_tree_tail_cta(const TreeTailArgs a) {
-    griddep_launch_dependents();
-    griddep_wait();   // the kernels ahead (their messages) have finished
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    for (uint32_t w = a.w0; w < a.w1; ++w) {
-        const uint32_t lo = a.wave_off[w], n = a.wave_off[w + 1] - lo;
-        for (uint32_t k = warp; k < n; k += nwarps) tail_node<MS, UNI>(a, lo + k, lane);
-        __syncthreads();   // this wave's messages before the next wave reads them
-    }
-}
-
 // ---- the schedule-order arrays (TreeData::s_*, q_*) -----------------------
 // per schedule index: the node's in-edge range, index in level, state count
 // and out-degree (scanned into s_out)
@@ -665,38 +647,6 @@ static int launch_tail(bp_graph *g, uint32_t level, uint32_t wa, uint32_t wb, in
     return BP_OK;
 }
 
-// BP_TREE_CTA_TAIL=0: every small wave its own launch (read when the launch
-// sequence is built)
-static bool tree_cta_tail_on() {
-    const char *env = getenv("BP_TREE_CTA_TAIL");
-    return !(env && env[0] == '0');
-}
-
-// waves [wa, wb) of `level`, each of at most kCtaTailNodes nodes, in one block
-template <int MS, bool UNI>
-static int launch_cta_tail(bp_graph *g, uint32_t level, uint32_t wa, uint32_t wb, int mode) {
-    TreeData &t = g->tree;
-    TreeTailArgs a;
-    a.t = tree_args(g);
-    a.wave_off = t.d_wave_off;
-    a.w0 = wa;
-    a.w1 = wb;
-    a.level = level;
-    a.mode = mode;
-    a.bar = nullptr;
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(1);
-    cfg.blockDim = dim3(1024);
-    cfg.stream = g->stream;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = tree_pdl() ? 1 : 0;
-    BP_CUDA(cudaLaunchKernelEx(&cfg, k_tree_tail_cta<MS, UNI>, a));
-    return BP_OK;
-}
-
 // the waves of `level`; mode 0 (graph.h calls) reads and then sets the
 // visited flags, modes 1 and 2 (bp_tree's upward and downward passes) derive
 // them from the levels
@@ -704,13 +654,7 @@ template <int MS, bool UNI>
 static int launch_level(bp_graph *g, uint32_t level, int mode) {
     TreeData &t = g->tree;
     const uint32_t w0 = t.level_wave_begin[level], w1 = t.level_wave_begin[level + 1];
-    // the level's trailing run of small waves, for one block (two or more)
-    uint32_t wt = w1;
-    if (!tree_tail_on() && tree_cta_tail_on()) {
-        while (wt > w0 && t.wave_off[wt] - t.wave_off[wt - 1] <= kCtaTailNodes) --wt;
-        if (w1 - wt < 2) wt = w1;
-    }
-    for (uint32_t w = w0; w < wt; ++w) {
+    for (uint32_t w = w0; w < w1; ++w) {
         const uint32_t lo = t.wave_off[w], n = t.wave_off[w + 1] - lo;
         if (!n) continue;
         if (tree_tail_on() && wave_group(n) == 32) {
@@ -735,10 +679,6 @@ static int launch_level(bp_graph *g, uint32_t level, int mode) {
         }
         if (le != cudaSuccess) return cuda_fail(le, "cudaLaunchKernelEx", __FILE__, __LINE__);
         BP_CUDA(cudaGetLastError());
-    }
-    if (wt < w1) {
-        int st = launch_cta_tail<MS, UNI>(g, level, wt, w1, mode);
-        if (st) return st;
     }
     if (w1 > w0 && mode == 0) {
         const uint32_t lo = t.wave_off[w0], n = t.wave_off[w1] - lo;
