@@ -545,7 +545,11 @@ __device__ __forceinline__ void mma_tf32_16x8x8(float *d, const uint32_t *a, con
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
 
-template <int S>
+// PF 1: the in-edge range and the first in-edge's source state are loaded
+// ahead of the node step, and each round loads the next round's in-edge
+// (table id, slot, source state) before it works on its own, so the gather
+// of the source state overlaps a round of arithmetic
+template <int S, int PF = 1>
 __global__ void __launch_bounds__(kMmaThreads, 4) k_u_bwd_mma(const UGraph g, int mode, const float *__restrict__ send,
                                                              const float *__restrict__ lb_t,
                                                              const float *__restrict__ lbbar_t,
@@ -570,12 +574,26 @@ __global__ void __launch_bounds__(kMmaThreads, 4) k_u_bwd_mma(const UGraph g, in
         if (!__any_sync(0xffffffffu, active)) break;
         float Pbar[S], ps = 0.0f;
         uint32_t r0 = 0, r1 = 0;
+        uint8_t ntab = 0;   // PF: the next in-edge's table id, slot and source state
+        uint32_t nslot = 0;
+        float nx[S];
         if (active) {
+            if constexpr (PF) {
+                r0 = g.in_ptr[v];
+                r1 = g.in_ptr[v + 1];
+                if (r0 < r1) {
+                    ntab = g.pos_tab[r0];
+                    nslot = g.pos_out[r0];
+                    ldv<S>(send + (size_t)g.in_src[r0] * S, nx);
+                }
+            }
             bwd_node_step<S>(g, mode, v, lb_t, lbbar_t, xc_next, lbbar_out, nullptr, Pbar);
 #pragma unroll
             for (int i = 0; i < S; ++i) ps += Pbar[i];
-            r0 = g.in_ptr[v];
-            r1 = g.in_ptr[v + 1];
+            if constexpr (!PF) {
+                r0 = g.in_ptr[v];
+                r1 = g.in_ptr[v + 1];
+            }
         }
         for (uint32_t j = 0;; ++j) {
             const bool has = r0 + j < r1;
@@ -588,11 +606,26 @@ __global__ void __launch_bounds__(kMmaThreads, 4) k_u_bwd_mma(const UGraph g, in
             }
             if (has) {
                 const uint32_t p = r0 + j;
-                const uint8_t tab = g.pos_tab[p];
+                uint8_t tab;
+                uint32_t slot;
                 float x[S], e[S], ci[S], c[S];
-                ldv<S>(send + (size_t)g.in_src[p] * S, x);
+                if constexpr (PF) {
+                    tab = ntab;
+                    slot = nslot;
+#pragma unroll
+                    for (int i = 0; i < S; ++i) x[i] = nx[i];
+                    if (p + 1 < r1) {
+                        ntab = g.pos_tab[p + 1];
+                        nslot = g.pos_out[p + 1];
+                        ldv<S>(send + (size_t)g.in_src[p + 1] * S, nx);
+                    }
+                } else {
+                    tab = g.pos_tab[p];
+                    slot = g.pos_out[p];
+                    ldv<S>(send + (size_t)g.in_src[p] * S, x);
+                }
                 bwd_edge<S>(edge_table<S>(sm, tab), x, Pbar, ps, e, ci, c);
-                stv<S>(xc + (size_t)g.pos_out[p] * S, c);
+                stv<S>(xc + (size_t)slot * S, c);
 #pragma unroll
                 for (int i = 0; i < S; ++i) {
                     cs[i] = ci[i];
@@ -639,6 +672,235 @@ __global__ void __launch_bounds__(kMmaThreads, 4) k_u_bwd_mma(const UGraph g, in
         double t = 0.0;
         for (int w = 0; w < NW; ++w) t += (double)dred[w][ra][cb] + (double)dred[w][8 + cb][ra];
         epart[(size_t)blockIdx.x * S * S + k] += (double)sm[ra * S + cb] * t;
+    }
+}
+
+// ---- the one-table adjoint in pull form (one table, S <= 8) --------------
+// With one table J an edge's message depends only on its source's state and
+// the table's orientation (J or J^T), so a source can gather the x adjoint
+// of its out-edges itself instead of each destination scattering a per-edge
+// term into a slot.  For source u with e = exp(x_u - max), the row sums
+// sN = J e and sT = J^T e and their totals zN, zT (once per node, not once
+// per in-edge), and each out-edge u -> w of orientation o:
+//   ci = Pbar(w) / s_o - sum(Pbar(w)) / z_o
+// summed over the out-edges into cN (J edges) and cT (J^T edges):
+//   xbar_u[j] = e_j * sum_i (cN_i J_ij + cT_i J_ji)
+//   logJbar  += J (.) (cN (x) e + (cT (x) e)^T)
+// The kernel of step t finishes step t+1's edges from Pbar_{t+1} of the
+// out-neighbours (the previous launch's output) and then runs step t's node
+// step, writing Pbar_t: no E x S slot arrays, and the per-edge DRAM traffic
+// is the out-neighbour's id, the table id and the (cached) Pbar gather.
+//   mode 0, step t:  g = lbbar_t + xbar;  lbbar_{t-1} = g - b_t sum(g);
+//                    Pbar_t = lbbar_{t-1} + xbar            (x = lQ_{t+1})
+//   mode 1, lQ_1 = lb_0 + lP:  lbbar_0 = gin + xbar;  Pbar = xbar   (x = lQ_1)
+//   mode 2, priors:  a = gin + xbar;  theta_bar = a - softmax(theta) sum(a),
+//                    softmax(theta) = exp(lb_0)                  (x = lb_0)
+// x_next null (t = T): no out-edge terms.  Tables: S <= 4 keeps the S*S
+// accumulators in registers; 5 <= S <= 8 sums cN (x) e and cT (x) e of 32
+// nodes per warp round on the tensor cores as k_u_bwd_mma does.
+constexpr int kPullThreads = 128;
+
+template <int S>
+__device__ __forceinline__ void pull_out_edges(const UGraph &g, const uint32_t *__restrict__ out_dst,
+                                               const uint8_t *__restrict__ out_tab, const float *sm,
+                                               const float *__restrict__ pbar_next, uint32_t u, const float *x,
+                                               float *e, float *cn, float *ct, float *xbar) {
+    const uint32_t q0 = g.out_ptr[u], q1 = g.out_ptr[u + 1];
+    shifted_exp<S, true>(x, e);
+    float rn[S], rt[S], zn = 0.0f, zt = 0.0f;
+    row_sums<S>(sm, e, rn);
+    row_sums<S>(sm + S * S, e, rt);
+#pragma unroll
+    for (int i = 0; i < S; ++i) {
+        zn += rn[i];
+        zt += rt[i];
+    }
+    // reciprocals once per node (s_i and z lie in [1e-37, S max J])
+#pragma unroll
+    for (int i = 0; i < S; ++i) {
+        rn[i] = __fdividef(1.0f, rn[i]);
+        rt[i] = __fdividef(1.0f, rt[i]);
+        cn[i] = 0.0f;
+        ct[i] = 0.0f;
+    }
+    const float izn = __fdividef(1.0f, zn), izt = __fdividef(1.0f, zt);
+    for (uint32_t q = q0; q < q1; q += 2) {
+        const bool two = q + 1 < q1;
+        const uint32_t w0 = out_dst[q], w1 = two ? out_dst[q + 1] : w0;
+        const bool t0 = (out_tab[q] & 0x80u) != 0, t1 = two && (out_tab[q + 1] & 0x80u) != 0;
+        float p0[S], p1[S];
+        ldv<S>(pbar_next + (size_t)w0 * S, p0);
+        ldv<S>(pbar_next + (size_t)w1 * S, p1);
+        float s0 = 0.0f, s1 = 0.0f;
+#pragma unroll
+        for (int i = 0; i < S; ++i) {
+            s0 += p0[i];
+            s1 += p1[i];
+        }
+        const float a0 = s0 * (t0 ? izt : izn), a1 = s1 * (t1 ? izt : izn);
+#pragma unroll
+        for (int i = 0; i < S; ++i) {
+            const float c = p0[i] * (t0 ? rt[i] : rn[i]) - a0;
+            cn[i] += t0 ? 0.0f : c;
+            ct[i] += t0 ? c : 0.0f;
+        }
+        if (two) {
+#pragma unroll
+            for (int i = 0; i < S; ++i) {
+                const float c = p1[i] * (t1 ? rt[i] : rn[i]) - a1;
+                cn[i] += t1 ? 0.0f : c;
+                ct[i] += t1 ? c : 0.0f;
+            }
+        }
+    }
+    // the tables are read again from shared memory here rather than kept in
+    // registers across the out-edge loop (2 S^2 values)
+    asm volatile("" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < S; ++j) {
+        float t = 0.0f;
+#pragma unroll
+        for (int i = 0; i < S; ++i) t += cn[i] * sm[i * S + j] + ct[i] * sm[S * S + i * S + j];
+        xbar[j] = e[j] * t;
+    }
+}
+
+template <int S>
+__global__ void __launch_bounds__(kPullThreads, S <= 3 ? 8 : (S == 4 ? 6 : 4)) k_u_bwd_pull(
+    const UGraph g, const uint32_t *__restrict__ out_dst, const uint8_t *__restrict__ out_tab, int mode,
+    const float *__restrict__ x_next, const float *__restrict__ pbar_next, const float *__restrict__ lb_t,
+    const float *__restrict__ gin, float *__restrict__ gout, float *__restrict__ pbar_out, double *__restrict__ epart) {
+    static_assert(S >= 1 && S <= 8, "pull form: up to 8 states");
+    constexpr bool MMA = S >= 5;
+    constexpr int NT = kPullThreads, NW = NT / 32;
+    __shared__ __align__(16) float sm[2 * S * S];   // J and J^T
+    __shared__ __align__(16) float st_n[MMA ? NW : 1][32][8];
+    __shared__ __align__(16) float st_t[MMA ? NW : 1][32][8];
+    __shared__ __align__(16) float st_e[MMA ? NW : 1][32][8];
+    __shared__ float dred[MMA ? NW : 1][16][8];
+    __shared__ float wred[NW][MMA ? 1 : S * S];
+    griddep_launch_dependents();
+    load_tables_smem<S>(g, sm);
+    griddep_wait();
+    const bool edges = x_next != nullptr;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gq = lane >> 2, tq = lane & 3;
+    float acc[MMA ? 1 : S * S];
+#pragma unroll
+    for (int k = 0; k < (MMA ? 1 : S * S); ++k) acc[k] = 0.0f;
+    float d[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    for (uint32_t base = (blockIdx.x * NW + warp) * 32u;; base += gridDim.x * (uint32_t)NT) {
+        const uint32_t u = base + lane;
+        const bool active = u < g.V;
+        if (!__any_sync(0xffffffffu, active)) break;
+        float e[S], cn[S], ct[S], xb[S];
+#pragma unroll
+        for (int i = 0; i < S; ++i) {
+            e[i] = 0.0f;
+            cn[i] = 0.0f;
+            ct[i] = 0.0f;
+            xb[i] = 0.0f;
+        }
+        if (active) {
+            float gi[S], lb[S];
+            ldv<S>(gin + (size_t)u * S, gi);
+            if (mode == 0) ldv<S>(lb_t + (size_t)u * S, lb);
+            if (edges) {
+                float x[S];
+                ldv<S>(x_next + (size_t)u * S, x);
+                pull_out_edges<S>(g, out_dst, out_tab, sm, pbar_next, u, x, e, cn, ct, xb);
+            }
+            if (mode == 2) ldv<S>(x_next + (size_t)u * S, lb);   // lb_0 (an L1 hit)
+            float out[S], pb[S], gs = 0.0f;
+#pragma unroll
+            for (int i = 0; i < S; ++i) {
+                gi[i] += xb[i];
+                gs += gi[i];
+            }
+            if (mode == 0) {
+#pragma unroll
+                for (int i = 0; i < S; ++i) {
+                    out[i] = gi[i] - expf(lb[i]) * gs;
+                    pb[i] = out[i] + xb[i];
+                }
+            } else if (mode == 1) {
+#pragma unroll
+                for (int i = 0; i < S; ++i) {
+                    out[i] = gi[i];
+                    pb[i] = xb[i];
+                }
+            } else {
+#pragma unroll
+                for (int i = 0; i < S; ++i) out[i] = gi[i] - expf(lb[i]) * gs;
+            }
+            stv<S>(gout + (size_t)u * S, out);
+            if (mode != 2) stv<S>(pbar_out + (size_t)u * S, pb);
+            if constexpr (!MMA) {
+                if (edges) {
+#pragma unroll
+                    for (int i = 0; i < S; ++i)
+#pragma unroll
+                        for (int j = 0; j < S; ++j) acc[i * S + j] += cn[i] * e[j] + ct[j] * e[i];
+                }
+            }
+        }
+        if constexpr (MMA) {
+            if (edges) {
+                // A (16 x 32 nodes): rows 0-7 cN, rows 8-15 cT; B (32 nodes x 8): e
+                float pn[8], pt[8], pe[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    pn[i] = 0.0f;
+                    pt[i] = 0.0f;
+                    pe[i] = 0.0f;
+                }
+#pragma unroll
+                for (int i = 0; i < S; ++i) {
+                    pn[i] = cn[i];
+                    pt[i] = ct[i];
+                    pe[i] = e[i];
+                }
+                reinterpret_cast<float4 *>(st_n[warp][lane])[0] = make_float4(pn[0], pn[1], pn[2], pn[3]);
+                reinterpret_cast<float4 *>(st_n[warp][lane])[1] = make_float4(pn[4], pn[5], pn[6], pn[7]);
+                reinterpret_cast<float4 *>(st_t[warp][lane])[0] = make_float4(pt[0], pt[1], pt[2], pt[3]);
+                reinterpret_cast<float4 *>(st_t[warp][lane])[1] = make_float4(pt[4], pt[5], pt[6], pt[7]);
+                reinterpret_cast<float4 *>(st_e[warp][lane])[0] = make_float4(pe[0], pe[1], pe[2], pe[3]);
+                reinterpret_cast<float4 *>(st_e[warp][lane])[1] = make_float4(pe[4], pe[5], pe[6], pe[7]);
+                __syncwarp();
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int k0 = q * 8 + tq, k1 = k0 + 4;
+                    const float af[4] = {st_n[warp][k0][gq], st_t[warp][k0][gq], st_n[warp][k1][gq],
+                                         st_t[warp][k1][gq]};
+                    const float bf[2] = {st_e[warp][k0][gq], st_e[warp][k1][gq]};
+                    uint32_t ah[4], al[4], bh[2], bl[2];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) split_tf32(af[i], ah[i], al[i]);
+#pragma unroll
+                    for (int i = 0; i < 2; ++i) split_tf32(bf[i], bh[i], bl[i]);
+                    mma_tf32_16x8x8(d, ah, bh);
+                    mma_tf32_16x8x8(d, ah, bl);
+                    mma_tf32_16x8x8(d, al, bh);
+                }
+                __syncwarp();
+            }
+        }
+    }
+    if (!edges) return;   // uniform over the grid: no table adjoint in this launch
+    if constexpr (MMA) {
+        dred[warp][gq][2 * tq] = d[0];
+        dred[warp][gq][2 * tq + 1] = d[1];
+        dred[warp][gq + 8][2 * tq] = d[2];
+        dred[warp][gq + 8][2 * tq + 1] = d[3];
+        __syncthreads();
+        // logJbar[a][b] += J[a][b] * (N[a][b] + T[b][a])
+        for (int k = threadIdx.x; k < S * S; k += NT) {
+            const int ra = k / S, cb = k % S;
+            double t = 0.0;
+            for (int w = 0; w < NW; ++w) t += (double)dred[w][ra][cb] + (double)dred[w][8 + cb][ra];
+            epart[(size_t)blockIdx.x * S * S + k] += (double)sm[ra * S + cb] * t;
+        }
+    } else {
+        block_partial_add<S, NT, true>(acc, nullptr, wred, epart + (size_t)blockIdx.x * S * S, sm);
     }
 }
 
@@ -700,7 +962,11 @@ struct bp_unrolled {
     float *pp_b = nullptr, *pp_q = nullptr;    // [2][V][S]
     float *bT = nullptr;
     float *bbar[2] = {nullptr, nullptr};
-    float *xc[2] = {nullptr, nullptr};       // [E][S] x adjoint terms, source-sorted slots
+    float *xc[2] = {nullptr, nullptr};       // [E][S] x adjoint terms, source-sorted slots (scatter form)
+    bool pull = false;                       // the adjoint in pull form (one table, S <= 8)
+    uint32_t *out_dst = nullptr;             // [E] destination of source-sorted slot q (pull form)
+    uint8_t *out_tab = nullptr;              // [E] its table id (pull form)
+    float *pbv[2] = {nullptr, nullptr};      // [V][S] Pbar of steps t and t+1 (pull form)
     float *pbar = nullptr;                   // [V][S] node-step adjoint Pbar (several tables only)
     double *epart = nullptr;
     float *theta_buf = nullptr, *gtheta_buf = nullptr, *glogp_buf = nullptr;
@@ -791,6 +1057,82 @@ static int u_forward(bp_unrolled *u) {
 
 // the backward on the engine's own buffers (bbar[0] holds d loss / d lb_T on
 // entry; gtheta_buf, glogp_buf receive the gradients)
+// the backward in pull form (one table, S <= 8; see k_u_bwd_pull): kernel t
+// finishes step t+1's edges and runs step t's node step; then the initial
+// gather (mode 1) and the priors (mode 2).  Recompute and segment buffers as
+// in the scatter form below.
+template <int S>
+static int u_backward_pull(bp_unrolled *u) {
+    if constexpr (S > 8) {
+        return set_error(BP_ERR_STATE, "pull form with %d states", S);
+    } else {
+        const UGraph g{u->V, u->K, u->in_ptr, u->in_src, u->out_ptr, u->pos_out, u->pos_tab, u->tables};
+        const size_t VS = (size_t)u->V * S;
+        const unsigned gv = grid_for(u->V, kUThreads);
+        const unsigned gp = grid_for(u->V, kPullThreads * 2);
+        cudaStream_t st = u->stream;
+        int rc = BP_OK;
+        BP_CUDA(cudaMemsetAsync(u->epart, 0, sizeof(double) * gp * S * S, st));
+        auto step = [&](int mode, const float *xn, const float *pn, const float *b_t, const float *gin, float *gout,
+                        float *pout) -> int {
+            return u_launch(k_u_bwd_pull<S>, gp, kPullThreads, st, g, (const uint32_t *)u->out_dst,
+                            (const uint8_t *)u->out_tab, mode, xn, pn, b_t, gin, gout, pout, u->epart);
+        };
+        const uint32_t nseg = (u->T + u->ck - 1) / u->ck;
+        auto seg_b = [&](uint32_t s, uint32_t j) { return u->seg_b + ((size_t)(s & 1u) * u->ck + j) * VS; };
+        auto seg_q = [&](uint32_t s, uint32_t j) { return u->seg_q + ((size_t)(s & 1u) * u->ck + j) * VS; };
+        auto recompute = [&](uint32_t s) -> int {
+            const uint32_t t0 = s * u->ck, t_end = std::min(t0 + u->ck, u->T);
+            const float *ckb = u->ck_b + (size_t)s * VS, *ckq = u->ck_q + (size_t)s * VS;
+            for (uint32_t j = 1; j + t0 < t_end; ++j) {
+                const float *bi = (j == 1) ? ckb : seg_b(s, j - 1);
+                const float *qi = (j == 1) ? ckq : seg_q(s, j - 1);
+                int r = u_launch(k_u_iter<S>, gv, kUThreads, u->side, g, bi, qi, seg_b(s, j), seg_q(s, j));
+                if (r) return r;
+            }
+            return BP_OK;
+        };
+        int bc = 0, pc = 0;
+        const float *pn = nullptr;   // Pbar of step t+1 (none at t = T)
+        BP_CUDA(cudaEventRecord(u->ev_fork, st));
+        BP_CUDA(cudaStreamWaitEvent(u->side, u->ev_fork, 0));
+        BP_CUDA(cudaEventRecord(u->ev_rec[(nseg - 1) & 1u], u->side));
+        for (int s = (int)nseg - 1; s >= 0; --s) {
+            if (s >= 1) {
+                if ((uint32_t)s + 1 < nseg) BP_CUDA(cudaStreamWaitEvent(u->side, u->ev_bwd[(s + 1) & 1], 0));
+                if ((rc = recompute((uint32_t)s - 1))) return rc;
+                BP_CUDA(cudaEventRecord(u->ev_rec[(s - 1) & 1], u->side));
+            }
+            BP_CUDA(cudaStreamWaitEvent(st, u->ev_rec[s & 1], 0));
+            const uint32_t t0 = (uint32_t)s * u->ck, t_end = std::min(t0 + u->ck, u->T);
+            for (uint32_t t = t_end; t > t0; --t) {
+                const uint32_t j = t - t0 - 1;
+                const float *b_t = (t == u->T) ? u->bT
+                                   : (t == t_end) ? u->ck_b + (size_t)(s + 1) * VS
+                                                  : seg_b((uint32_t)s, j + 1);   // lb_t
+                // lQ_{t+1}: the next segment's checkpoint after the segment's last step
+                const float *q_next = (t == u->T) ? nullptr
+                                      : (t == t_end) ? u->ck_q + (size_t)(s + 1) * VS
+                                                     : seg_q((uint32_t)s, j + 1);
+                if ((rc = step(0, q_next, pn, b_t, u->bbar[bc], u->bbar[bc ^ 1], u->pbv[pc]))) return rc;
+                bc ^= 1;
+                pn = u->pbv[pc];
+                pc ^= 1;
+            }
+            BP_CUDA(cudaEventRecord(u->ev_bwd[s & 1], st));
+        }
+        BP_CUDA(cudaGetLastError());
+        // step 1's edges (x = lQ_1, checkpoint 0) and the initial gather lQ_1 = lb_0 + lP
+        if ((rc = step(1, u->ck_q, pn, nullptr, u->bbar[bc], u->bbar[bc ^ 1], u->pbv[pc]))) return rc;
+        bc ^= 1;
+        pn = u->pbv[pc];
+        // the initial gather's edges (x = lb_0) and the priors' log-softmax
+        if ((rc = step(2, u->ck_b, pn, nullptr, u->bbar[bc], u->gtheta_buf, nullptr))) return rc;
+        return u_launch(k_u_reduce_pair, S * S, 256u, st, (const double *)u->epart, gp, (uint32_t)(S * S),
+                        u->glogp_buf);
+    }
+}
+
 template <int S>
 static int u_backward(bp_unrolled *u) {
     const UGraph g{u->V, u->K, u->in_ptr, u->in_src, u->out_ptr, u->pos_out, u->pos_tab, u->tables};
@@ -799,6 +1141,8 @@ static int u_backward(bp_unrolled *u) {
     constexpr int BT = bwd_threads<S>();
     // one table and 5..8 states: the table adjoint on the tensor cores
     const bool mma = S >= 5 && S <= 8 && u->K == 1;
+    // the tensor-core adjoint's in-edge loads one round ahead (BP_UBWD_PF=0: in the round that uses them)
+    const bool mma_pf = ubwd_env("BP_UBWD_PF", 1, 0) == 1;
     const int batch = S <= 4 ? ubwd_env("BP_UBWD_BATCH", 2, 4) : 2;
     const uint32_t npt = (uint32_t)ubwd_env("BP_UBWD_NPT", (int)kBwdNodesPerThread, 1);
     // register cap of the adjoint kernel, 1-4 states: BP_UBWD_MINB=3 allows
@@ -813,7 +1157,10 @@ static int u_backward(bp_unrolled *u) {
     auto adjoint = [&](int mode, const float *send, const float *b_t, const float *gbar, const float *xn, float *out,
                        float *xo, float *pb) -> int {
         if constexpr (S >= 5 && S <= 8) {
-            if (mma) return u_launch(k_u_bwd_mma<S>, gb, kMmaThreads, st, g, mode, send, b_t, gbar, xn, out, xo,
+            if (mma && mma_pf)
+                return u_launch(k_u_bwd_mma<S, 1>, gb, kMmaThreads, st, g, mode, send, b_t, gbar, xn, out, xo,
+                                u->epart);
+            if (mma) return u_launch(k_u_bwd_mma<S, 0>, gb, kMmaThreads, st, g, mode, send, b_t, gbar, xn, out, xo,
                                      u->epart);
         }
         if constexpr (S <= 4) {
@@ -824,6 +1171,7 @@ static int u_backward(bp_unrolled *u) {
         }
         return u_launch(k_u_bwd<S, 2>, gb, BT, st, g, mode, send, b_t, gbar, xn, out, xo, u->epart, pb);
     };
+    if (u->pull) return u_backward_pull<S>(u);
     BP_CUDA(cudaMemsetAsync(u->epart, 0, sizeof(double) * u->K * gb * S * S, st));
     // several tables: the table adjoint of each backward step, one pass per table
     auto pair_grads = [&](const float *send) -> int {
@@ -898,7 +1246,8 @@ static void u_free(bp_unrolled *u) {
     if (!u) return;
     void *ptrs[] = {u->in_ptr, u->in_src, u->out_ptr, u->pos_out, u->pos_tab, u->tables, u->ck_b, u->ck_q,
                     u->seg_b, u->seg_q, u->pp_b, u->pp_q, u->bT, u->bbar[0], u->bbar[1], u->xc[0],
-                    u->xc[1], u->epart, u->theta_buf, u->gtheta_buf, u->glogp_buf, u->pbar};
+                    u->xc[1], u->epart, u->theta_buf, u->gtheta_buf, u->glogp_buf, u->pbar, u->out_dst,
+                    u->out_tab, u->pbv[0], u->pbv[1]};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (u->fwd_exec) cudaGraphExecDestroy(u->fwd_exec);
@@ -1042,6 +1391,19 @@ int bp_unrolled_create(bp_unrolled **out, uint32_t V, uint32_t E, uint32_t S, ui
     }
     std::vector<uint32_t> ofill(out_ptr.begin(), out_ptr.end() - 1);
     for (uint32_t e = 0; e < E; ++e) pos_out[pos_of[e]] = ofill[src[e]]++;
+    // one table and up to 8 states: the adjoint in pull form (BP_UBWD_PULL=0: the scatter form)
+    u->pull = K == 1 && S <= 8 && ubwd_env("BP_UBWD_PULL", 1, 0) == 1;
+    std::vector<uint32_t> odst;
+    std::vector<uint8_t> otab;
+    if (u->pull) {
+        odst.resize(E);
+        otab.resize(E);
+        for (uint32_t e = 0; e < E; ++e) {
+            const uint32_t q = pos_out[pos_of[e]];
+            odst[q] = dst[e];
+            otab[q] = tab[e];
+        }
+    }
     const size_t VS = (size_t)V * S;
     u->nblk = grid_for(V, 64);   // partial slots for the smallest backward block
     auto alloc = [&](void **p, size_t bytes) {
@@ -1057,8 +1419,11 @@ int bp_unrolled_create(bp_unrolled **out, uint32_t V, uint32_t E, uint32_t S, ui
               alloc((void **)&u->pp_b, sizeof(float) * VS * 2) && alloc((void **)&u->pp_q, sizeof(float) * VS * 2) &&
               alloc((void **)&u->bT, sizeof(float) * VS) && alloc((void **)&u->bbar[0], sizeof(float) * VS) &&
               alloc((void **)&u->bbar[1], sizeof(float) * VS) &&
-              alloc((void **)&u->xc[0], sizeof(float) * S * (size_t)E) &&
-              alloc((void **)&u->xc[1], sizeof(float) * S * (size_t)E) &&
+              (u->pull || (alloc((void **)&u->xc[0], sizeof(float) * S * (size_t)E) &&
+                           alloc((void **)&u->xc[1], sizeof(float) * S * (size_t)E))) &&
+              (!u->pull || (alloc((void **)&u->out_dst, 4 * (size_t)E) && alloc((void **)&u->out_tab, (size_t)E) &&
+                            alloc((void **)&u->pbv[0], sizeof(float) * VS) &&
+                            alloc((void **)&u->pbv[1], sizeof(float) * VS))) &&
               alloc((void **)&u->epart, sizeof(double) * K * u->nblk * S * S) &&
               (K == 1 || alloc((void **)&u->pbar, sizeof(float) * VS)) &&
               alloc((void **)&u->theta_buf, sizeof(float) * VS) && alloc((void **)&u->gtheta_buf, sizeof(float) * VS) &&
@@ -1073,6 +1438,10 @@ int bp_unrolled_create(bp_unrolled **out, uint32_t V, uint32_t E, uint32_t S, ui
         cudaMemcpyAsync(u->in_src, in_src.data(), 4 * (size_t)E, cudaMemcpyHostToDevice, u->stream);
         cudaMemcpyAsync(u->pos_out, pos_out.data(), 4 * (size_t)E, cudaMemcpyHostToDevice, u->stream);
         cudaMemcpyAsync(u->pos_tab, ptab.data(), (size_t)E, cudaMemcpyHostToDevice, u->stream);
+        if (u->pull) {
+            cudaMemcpyAsync(u->out_dst, odst.data(), 4 * (size_t)E, cudaMemcpyHostToDevice, u->stream);
+            cudaMemcpyAsync(u->out_tab, otab.data(), (size_t)E, cudaMemcpyHostToDevice, u->stream);
+        }
     }
     cudaEventCreate(&u->ev0);
     cudaEventCreate(&u->ev1);

@@ -360,7 +360,10 @@ int bp_batch_network_results(bp_batch *b, uint32_t *iterations, uint32_t *execut
  * bp_unrolled_backward maps d loss / d log-beliefs to gradients with respect
  * to log_unary and log_pair with a hand-written adjoint.  The forward keeps
  * the iteration state every checkpoint_every iterations; the backward
- * recomputes each segment from its checkpoint.  Tensor arguments of
+ * recomputes each segment from its checkpoint.  With one table and at most
+ * 8 states the adjoint runs in pull form (each source gathers its
+ * out-neighbours' message adjoints; BP_UBWD_PULL=0 selects the scatter form
+ * at create, which every other shape uses).  Tensor arguments of
  * forward/backward are device memory, 16-byte aligned; the graph arrays of
  * create are host memory.  At most 16 tables. */
 typedef struct bp_unrolled bp_unrolled;

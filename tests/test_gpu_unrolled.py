@@ -238,3 +238,26 @@ def test_unrolled_batch_of_grids_of_different_sides(bp):
     fd = (f(wp) - f(wm)) / (2 * h)
     assert abs(W.grad[0, i, j].item() - fd) <= 2e-4 * max(1e-3, abs(fd)) + 2e-6, (W.grad[0, i, j].item(), fd)
     eng.close()
+
+
+@pytest.mark.parametrize("side,S,T,ck", [(24, 4, 7, 3), (32, 8, 20, 5), (17, 5, 6, 6), (15, 1, 4, 2)])
+def test_unrolled_pull_adjoint_matches_scatter_adjoint(bp, side, S, T, ck, monkeypatch):
+    """One shared table and up to 8 states: the adjoint in pull form (each
+    source gathers the destinations' Pbar over its out-edges) against the
+    scatter form (each destination writes per-edge x adjoint terms into the
+    sources' slots, BP_UBWD_PULL=0).  Same forward bits, gradients equal to
+    fp32 rounding of the two summation orders."""
+    res = []
+    for pull in ("1", "0"):
+        monkeypatch.setenv("BP_UBWD_PULL", pull)
+        eng, theta, W, labels, _ = _setup(side, S, T, seed=side + S, ck=ck)
+        lb = eng(theta, W)
+        _loss(lb, labels).backward()
+        res.append((lb.detach().clone(), theta.grad.detach().clone(), W.grad.detach().clone()))
+        eng.close()
+    (lb1, gt1, gw1), (lb0, gt0, gw0) = res
+    assert np.array_equal(lb1.cpu().numpy(), lb0.cpu().numpy())
+    st = gt0.abs().max().item()
+    sw = gw0.abs().max().item()
+    np.testing.assert_allclose(gt1.cpu().numpy(), gt0.cpu().numpy(), rtol=1e-4, atol=1e-5 * st + 1e-9)
+    np.testing.assert_allclose(gw1.cpu().numpy(), gw0.cpu().numpy(), rtol=1e-4, atol=1e-5 * sw + 1e-9)
