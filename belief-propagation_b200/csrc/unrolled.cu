@@ -699,6 +699,10 @@ __global__ void __launch_bounds__(kMmaThreads, 4) k_u_bwd_mma(const UGraph g, in
 // accumulators in registers; 5 <= S <= 8 sums cN (x) e and cT (x) e of 32
 // nodes per warp round on the tensor cores as k_u_bwd_mma does.
 constexpr int kPullThreads = 128;
+// resident blocks per SM the pull kernel's registers are capped for (5-8
+// states, config 4's 256 grids: 25.1 ms forward+backward at 4, 24.0 at 5,
+// 25.0 at 6 with spills)
+template <int S> constexpr int pull_min_blocks() { return S <= 3 ? 8 : (S == 4 ? 6 : 5); }
 
 template <int S>
 __device__ __forceinline__ void pull_out_edges(const UGraph &g, const uint32_t *__restrict__ out_dst,
@@ -765,8 +769,8 @@ __device__ __forceinline__ void pull_out_edges(const UGraph &g, const uint32_t *
     }
 }
 
-template <int S>
-__global__ void __launch_bounds__(kPullThreads, S <= 3 ? 8 : (S == 4 ? 6 : 4)) k_u_bwd_pull(
+template <int S, int MB = pull_min_blocks<S>()>
+__global__ void __launch_bounds__(kPullThreads, MB) k_u_bwd_pull(
     const UGraph g, const uint32_t *__restrict__ out_dst, const uint8_t *__restrict__ out_tab, int mode,
     const float *__restrict__ x_next, const float *__restrict__ pbar_next, const float *__restrict__ lb_t,
     const float *__restrict__ gin, float *__restrict__ gout, float *__restrict__ pbar_out, double *__restrict__ epart) {
@@ -1073,8 +1077,18 @@ static int u_backward_pull(bp_unrolled *u) {
         cudaStream_t st = u->stream;
         int rc = BP_OK;
         BP_CUDA(cudaMemsetAsync(u->epart, 0, sizeof(double) * gp * S * S, st));
+        // 5-8 states: register cap for 5 (default), 4 or 6 resident blocks per SM (BP_UBWD_PULL_MB)
+        const int mb = S >= 5 ? ubwd_env("BP_UBWD_PULL_MB", ubwd_env("BP_UBWD_PULL_MB", 5, 4), 6) : 0;
         auto step = [&](int mode, const float *xn, const float *pn, const float *b_t, const float *gin, float *gout,
                         float *pout) -> int {
+            if constexpr (S >= 5) {
+                if (mb == 4)
+                    return u_launch(k_u_bwd_pull<S, 4>, gp, kPullThreads, st, g, (const uint32_t *)u->out_dst,
+                                    (const uint8_t *)u->out_tab, mode, xn, pn, b_t, gin, gout, pout, u->epart);
+                if (mb == 6)
+                    return u_launch(k_u_bwd_pull<S, 6>, gp, kPullThreads, st, g, (const uint32_t *)u->out_dst,
+                                    (const uint8_t *)u->out_tab, mode, xn, pn, b_t, gin, gout, pout, u->epart);
+            }
             return u_launch(k_u_bwd_pull<S>, gp, kPullThreads, st, g, (const uint32_t *)u->out_dst,
                             (const uint8_t *)u->out_tab, mode, xn, pn, b_t, gin, gout, pout, u->epart);
         };
