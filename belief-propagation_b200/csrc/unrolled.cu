@@ -1077,20 +1077,32 @@ static int u_backward_pull(bp_unrolled *u) {
         cudaStream_t st = u->stream;
         int rc = BP_OK;
         BP_CUDA(cudaMemsetAsync(u->epart, 0, sizeof(double) * gp * S * S, st));
-        // 5-8 states: register cap for 5 (default), 4 or 6 resident blocks per SM (BP_UBWD_PULL_MB)
-        const int mb = S >= 5 ? ubwd_env("BP_UBWD_PULL_MB", ubwd_env("BP_UBWD_PULL_MB", 5, 4), 6) : 0;
+        // 4-8 states: the register cap, in resident blocks per SM, may be set
+        // to 4, 5, 6 or 8 (BP_UBWD_PULL_MB; default pull_min_blocks)
+        int mb = 0;
+        if (S >= 4) {
+            const char *env = getenv("BP_UBWD_PULL_MB");
+            mb = env ? atoi(env) : 0;
+        }
         auto step = [&](int mode, const float *xn, const float *pn, const float *b_t, const float *gin, float *gout,
                         float *pout) -> int {
-            if constexpr (S >= 5) {
-                if (mb == 4)
-                    return u_launch(k_u_bwd_pull<S, 4>, gp, kPullThreads, st, g, (const uint32_t *)u->out_dst,
-                                    (const uint8_t *)u->out_tab, mode, xn, pn, b_t, gin, gout, pout, u->epart);
-                if (mb == 6)
-                    return u_launch(k_u_bwd_pull<S, 6>, gp, kPullThreads, st, g, (const uint32_t *)u->out_dst,
-                                    (const uint8_t *)u->out_tab, mode, xn, pn, b_t, gin, gout, pout, u->epart);
+            const uint32_t *od = u->out_dst;
+            const uint8_t *ot = u->out_tab;
+            if constexpr (S >= 4) {
+                switch (mb) {
+                case 4: return u_launch(k_u_bwd_pull<S, 4>, gp, kPullThreads, st, g, od, ot, mode, xn, pn, b_t, gin,
+                                        gout, pout, u->epart);
+                case 5: return u_launch(k_u_bwd_pull<S, 5>, gp, kPullThreads, st, g, od, ot, mode, xn, pn, b_t, gin,
+                                        gout, pout, u->epart);
+                case 6: return u_launch(k_u_bwd_pull<S, 6>, gp, kPullThreads, st, g, od, ot, mode, xn, pn, b_t, gin,
+                                        gout, pout, u->epart);
+                case 8: return u_launch(k_u_bwd_pull<S, 8>, gp, kPullThreads, st, g, od, ot, mode, xn, pn, b_t, gin,
+                                        gout, pout, u->epart);
+                default: break;
+                }
             }
-            return u_launch(k_u_bwd_pull<S>, gp, kPullThreads, st, g, (const uint32_t *)u->out_dst,
-                            (const uint8_t *)u->out_tab, mode, xn, pn, b_t, gin, gout, pout, u->epart);
+            return u_launch(k_u_bwd_pull<S>, gp, kPullThreads, st, g, od, ot, mode, xn, pn, b_t, gin, gout, pout,
+                            u->epart);
         };
         const uint32_t nseg = (u->T + u->ck - 1) / u->ck;
         auto seg_b = [&](uint32_t s, uint32_t j) { return u->seg_b + ((size_t)(s & 1u) * u->ck + j) * VS; };
