@@ -205,7 +205,7 @@ def test_bench_arguments_and_algorithmic_bytes(monkeypatch):
     monkeypatch.setattr(sys, "argv", ["bench.py"])
     a = bench.parse()
     assert (a.gpus, a.impl, a.workload, a.iterations) == (1, "bp", "power_law", 100)
-    assert a.warmup >= 3 and a.e2e_steps == 6 and a.batch_delta == "f64"
+    assert a.warmup >= 3 and a.e2e_steps == 12 and a.batch_delta == "f64"
     assert (a.nodes, a.edges) == (1 << 24, 1 << 26)
     for d in ("serial", "f64"):
         monkeypatch.setattr(sys, "argv", ["bench.py", "--workload", "batched", "--batch-delta", d])
