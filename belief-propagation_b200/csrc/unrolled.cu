@@ -699,10 +699,11 @@ __global__ void __launch_bounds__(kMmaThreads, 4) k_u_bwd_mma(const UGraph g, in
 // accumulators in registers; 5 <= S <= 8 sums cN (x) e and cT (x) e of 32
 // nodes per warp round on the tensor cores as k_u_bwd_mma does.
 constexpr int kPullThreads = 128;
-// resident blocks per SM the pull kernel's registers are capped for (5-8
-// states, config 4's 256 grids: 25.1 ms forward+backward at 4, 24.0 at 5,
-// 25.0 at 6 with spills)
-template <int S> constexpr int pull_min_blocks() { return S <= 3 ? 8 : (S == 4 ? 6 : 5); }
+// resident blocks per SM the pull kernel's registers are capped for.  5-8
+// states, 256 grids of 8 states: 25.1 ms forward+backward at 4, 24.0 at 5,
+// 25.0 at 6 (spills).  4 states, the 512x512 grid: 0.847 ms at 4 (86
+// registers), 0.837 at 6, 0.785 at 8 (64 registers, 44 B of spills)
+template <int S> constexpr int pull_min_blocks() { return S <= 4 ? 8 : 5; }
 
 template <int S>
 __device__ __forceinline__ void pull_out_edges(const UGraph &g, const uint32_t *__restrict__ out_dst,
