@@ -261,3 +261,45 @@ def test_unrolled_pull_adjoint_matches_scatter_adjoint(bp, side, S, T, ck, monke
     sw = gw0.abs().max().item()
     np.testing.assert_allclose(gt1.cpu().numpy(), gt0.cpu().numpy(), rtol=1e-4, atol=1e-5 * st + 1e-9)
     np.testing.assert_allclose(gw1.cpu().numpy(), gw0.cpu().numpy(), rtol=1e-4, atol=1e-5 * sw + 1e-9)
+
+
+@pytest.mark.parametrize("S,T,ck", [(3, 5, 2), (6, 4, 4), (8, 1, 1), (2, 7, 3)])
+def test_unrolled_pull_adjoint_on_irregular_graph(bp, S, T, ck, monkeypatch):
+    """One shared table on a random graph that is not a grid: sources with no
+    in-edges, sinks with no out-edges, isolated nodes, repeated edges, both
+    table orientations mixed at random, T = 1 included.  The pull-form adjoint
+    against the scatter form and against the fp64 torch reference."""
+    import torch
+    from belief_propagation_b200.unrolled import UnrolledBP, torch_unrolled
+    rng = np.random.default_rng(100 + S * 10 + T)
+    V, E = 300, 900
+    src = rng.integers(0, 200, E).astype(np.uint32)          # nodes 200.. send nothing
+    dst = rng.integers(40, 260, E).astype(np.uint32)         # nodes < 40 receive nothing, 260.. are isolated or sources
+    src[:20] = src[20:40]                                     # repeated edges
+    dst[:20] = dst[20:40]
+    tab = np.where(rng.random(E) < 0.5, 0, 0x80).astype(np.uint8)
+    theta0 = rng.normal(0, 1, (V, S))
+    W0 = rng.normal(0, 0.5, (1, S, S))
+    labels = torch.tensor(rng.integers(0, S, V), device="cuda")
+    res = []
+    for pull in ("1", "0"):
+        monkeypatch.setenv("BP_UBWD_PULL", pull)
+        theta = torch.tensor(theta0, dtype=torch.float32, device="cuda", requires_grad=True)
+        W = torch.tensor(W0, dtype=torch.float32, device="cuda", requires_grad=True)
+        eng = UnrolledBP(V, src, dst, tab, S, T, checkpoint_every=ck)
+        lb = eng(theta, W)
+        _loss(lb, labels).backward()
+        res.append((lb.detach().cpu().numpy(), theta.grad.cpu().numpy(), W.grad.cpu().numpy()))
+        eng.close()
+    (lb1, gt1, gw1), (lb0, gt0, gw0) = res
+    assert np.array_equal(lb1, lb0)
+    th64 = torch.tensor(theta0, dtype=torch.float64, device="cuda", requires_grad=True)
+    W64 = torch.tensor(W0, dtype=torch.float64, device="cuda", requires_grad=True)
+    _loss(torch_unrolled(th64, W64, src, dst, tab, T), labels).backward()
+    st = th64.grad.abs().max().item()
+    sw = W64.grad.abs().max().item()
+    for gt, gw in ((gt1, gw1), (gt0, gw0)):
+        np.testing.assert_allclose(gt, th64.grad.cpu().numpy(), atol=1e-3 * st + 1e-7)
+        np.testing.assert_allclose(gw, W64.grad.cpu().numpy(), rtol=1e-3, atol=1e-3 * sw + 1e-7)
+    np.testing.assert_allclose(gt1, gt0, rtol=1e-4, atol=1e-5 * st + 1e-9)
+    np.testing.assert_allclose(gw1, gw0, rtol=1e-4, atol=1e-5 * sw + 1e-9)
