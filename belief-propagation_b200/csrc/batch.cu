@@ -382,6 +382,7 @@ __global__ void k_batch_msgs_out(const float *__restrict__ m0, const float *__re
 
 struct Group {
     int S = 0;
+    uint32_t vmax = 0;             // networks of at most vmax nodes; 0: the larger ones
     std::vector<uint32_t> order;   // network ids, largest work first
     uint32_t *d_order = nullptr;
     uint32_t block = 0;            // threads per block (0 = not tuned yet)
@@ -444,6 +445,18 @@ static int launch_group_s(bp_batch *bt, Group &gr, const BatchArgs &a, uint32_t 
 }
 
 constexpr uint32_t kSumChunk = 1024;   // serial mode: 8 KB of dynamic shared memory per block
+
+// networks of at most this many nodes form a group of their own per state
+// count (BP_BATCH_SMALL_NODES; default 0: one group per state count).  On
+// the 4096-network batch (f64 delta) a bound of 512 nodes measured 35.2-35.5k
+// networks/s against 35.8-35.9k without; 256: 35.5k, 1024: 34.1k; serial
+// delta 26.7k either way.  Tuned alone, the small groups still take 512
+// threads per block: a small network's iteration is set by the block's
+// barriers and reductions, not by its idle threads.
+static uint32_t batch_small_nodes() {
+    const char *env = getenv("BP_BATCH_SMALL_NODES");
+    return env ? (uint32_t)strtoul(env, nullptr, 10) : 0u;
+}
 
 static BatchArgs batch_args(bp_batch *bt, float tol, uint32_t max_it, int serial, int init) {
     BatchArgs a;
@@ -642,22 +655,41 @@ static int batch_create_impl(bp_batch *bt, uint32_t N, const bp_graph_desc *desc
         BP_CUDA(cudaMemcpyAsync(bt->joint, h_joint.data(), sizeof(float) * joint_f, cudaMemcpyHostToDevice, bt->stream));
     }
 
-    // ---- groups by state count, largest work first
+    // ---- groups by state count and, optionally, size class (networks of
+    // at most small_nodes nodes in a group with its own launch shape, queue
+    // and stream)
+    const uint32_t small_nodes = batch_small_nodes();
+    auto work = [&](uint32_t n) {
+        const NetInfo &x = bt->info[n];
+        return (uint64_t)x.E * x.S * x.S + (uint64_t)x.V * x.S;
+    };
     for (uint32_t n = 0; n < N; ++n) {
         const int S = (int)bt->info[n].S;
-        auto it = std::find_if(bt->groups.begin(), bt->groups.end(), [&](const Group &g) { return g.S == S; });
+        const uint32_t vmax = (small_nodes && bt->info[n].V <= small_nodes) ? small_nodes : 0u;
+        auto it = std::find_if(bt->groups.begin(), bt->groups.end(),
+                               [&](const Group &g) { return g.S == S && g.vmax == vmax; });
         if (it == bt->groups.end()) {
             bt->groups.emplace_back();
             bt->groups.back().S = S;
+            bt->groups.back().vmax = vmax;
             it = bt->groups.end() - 1;
         }
         it->order.push_back(n);
     }
+    // the heaviest group is launched first
+    std::vector<uint64_t> gwork(bt->groups.size(), 0);
+    for (size_t gi = 0; gi < bt->groups.size(); ++gi)
+        for (uint32_t n : bt->groups[gi].order) gwork[gi] += work(n);
+    std::vector<size_t> gidx(bt->groups.size());
+    std::iota(gidx.begin(), gidx.end(), 0);
+    std::stable_sort(gidx.begin(), gidx.end(), [&](size_t x, size_t y) { return gwork[x] > gwork[y]; });
+    {
+        std::vector<Group> sorted;
+        for (size_t i : gidx) sorted.push_back(std::move(bt->groups[i]));
+        bt->groups = std::move(sorted);
+    }
     for (auto &gr : bt->groups) {
-        std::stable_sort(gr.order.begin(), gr.order.end(), [&](uint32_t x, uint32_t y) {
-            const NetInfo &a = bt->info[x], &b = bt->info[y];
-            return (uint64_t)a.E * a.S * a.S + (uint64_t)a.V * a.S > (uint64_t)b.E * b.S * b.S + (uint64_t)b.V * b.S;
-        });
+        std::stable_sort(gr.order.begin(), gr.order.end(), [&](uint32_t x, uint32_t y) { return work(x) > work(y); });
         BP_CUDA(cudaMalloc((void **)&gr.d_order, sizeof(uint32_t) * gr.order.size()));
         BP_CUDA(cudaMemcpyAsync(gr.d_order, gr.order.data(), sizeof(uint32_t) * gr.order.size(),
                                 cudaMemcpyHostToDevice, bt->stream));
@@ -681,7 +713,7 @@ static int batch_create_impl(bp_batch *bt, uint32_t N, const bp_graph_desc *desc
 // ---- autotuning of threads per block, cached on disk ---------------------
 // kernel revision in the autotune key: a cached block size belongs to the
 // kernel it was timed on
-constexpr int kTuneRevision = 3;
+constexpr int kTuneRevision = 4;
 
 static std::string tune_key(bp_batch *bt, const Group &gr, int serial) {
     uint64_t V = 0, E = 0;
@@ -698,8 +730,8 @@ static std::string tune_key(bp_batch *bt, const Group &gr, int serial) {
     cudaGetDevice(&dev);
     cudaGetDeviceProperties(&prop, dev);
     char buf[512];
-    snprintf(buf, sizeof buf, "%s|S=%d|log2V=%u|deg10=%u|nets=%llu|delta=%s|rev=%d", prop.name, gr.S, lv, deg10,
-             (unsigned long long)(cnt >= 1024 ? 1024 : cnt), serial ? "serial" : "f64", kTuneRevision);
+    snprintf(buf, sizeof buf, "%s|S=%d|vmax=%u|log2V=%u|deg10=%u|nets=%llu|delta=%s|rev=%d", prop.name, gr.S, gr.vmax,
+             lv, deg10, (unsigned long long)(cnt >= 1024 ? 1024 : cnt), serial ? "serial" : "f64", kTuneRevision);
     for (char *c = buf; *c; ++c)
         if (*c == ' ') *c = '_';
     return buf;
@@ -922,6 +954,20 @@ int bp_batch_autotune(bp_batch *bt, const bp_batch_options *o) {
         cudaGraphExecDestroy(bt->exec);
         bt->exec = nullptr;
     }
+    return BP_OK;
+}
+
+int bp_batch_get_groups(const bp_batch *bt, uint32_t *states, uint32_t *max_nodes, uint32_t *block, uint32_t *grid,
+                        uint32_t *count) {
+    if (!bt || !count) return set_error(BP_ERR_INVALID, "null argument");
+    const uint32_t n = (uint32_t)bt->groups.size();
+    for (uint32_t i = 0; i < n && i < *count; ++i) {
+        if (states) states[i] = (uint32_t)bt->groups[i].S;
+        if (max_nodes) max_nodes[i] = bt->groups[i].vmax;
+        if (block) block[i] = bt->groups[i].block;
+        if (grid) grid[i] = bt->groups[i].grid;
+    }
+    *count = n;
     return BP_OK;
 }
 

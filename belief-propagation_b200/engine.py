@@ -278,12 +278,21 @@ class BPBatch:
         N.check(self.lib.bp_batch_autotune(self.h, C.byref(self.options(**kw))))
         return self.block_threads()
 
+    def groups(self):
+        """The launch groups: state count, size bound (0 = the larger
+        networks), threads per block and blocks in flight, launch order."""
+        n = C.c_uint32(64)
+        st, vm, bl, gr = (np.zeros(64, np.uint32) for _ in range(4))
+        N.check(self.lib.bp_batch_get_groups(self.h, st.ctypes.data, vm.ctypes.data, bl.ctypes.data, gr.ctypes.data,
+                                             C.byref(n)))
+        return [{"states": int(st[i]), "max_nodes": int(vm[i]), "block": int(bl[i]), "grid": int(gr[i])}
+                for i in range(min(n.value, 64))]
+
     def block_threads(self):
-        n = C.c_uint32(16)
-        st = np.zeros(16, np.uint32)
-        bl = np.zeros(16, np.uint32)
-        N.check(self.lib.bp_batch_get_block_threads(self.h, st.ctypes.data, bl.ctypes.data, C.byref(n)))
-        return {int(st[i]): int(bl[i]) for i in range(n.value)}
+        """Threads per block by group: "S=<states>" for the larger networks
+        of a state count, "S=<states>,V<=<bound>" for its small ones."""
+        return {(f"S={g['states']}" + (f",V<={g['max_nodes']}" if g["max_nodes"] else "")): g["block"]
+                for g in self.groups()}
 
     def loopy(self, **kw):
         r = N.BatchResult()

@@ -108,7 +108,7 @@ BP_SYMBOLS = [
     "bp_tree_marginalize", "bp_tree", "bp_set_visited", "bp_get_visited", "bp_set_sync_mode",
     "bp_sync_host", "bp_graph_of", "bp_loopy_noalloc", "bp_release_cached_memory", "bp_reserve_cached_memory", "bp_batch_create", "bp_batch_destroy",
     "bp_batch_layout", "bp_batch_set_beliefs", "bp_batch_get_beliefs", "bp_batch_get_messages",
-    "bp_batch_default_options", "bp_batch_autotune", "bp_batch_get_block_threads", "bp_batch_loopy",
+    "bp_batch_default_options", "bp_batch_autotune", "bp_batch_get_block_threads", "bp_batch_get_groups", "bp_batch_loopy",
     "bp_batch_network_results", "bp_unrolled_create", "bp_unrolled_destroy", "bp_unrolled_set_stream",
     "bp_unrolled_forward", "bp_unrolled_backward",
 ]
@@ -167,6 +167,7 @@ def load(path=LIB_PATH):
         "bp_batch_default_options": ([C.POINTER(BatchOptions)], None),
         "bp_batch_autotune": ([vp, C.POINTER(BatchOptions)], i32),
         "bp_batch_get_block_threads": ([vp, vp, vp, C.POINTER(u32)], i32),
+        "bp_batch_get_groups": ([vp, vp, vp, vp, vp, C.POINTER(u32)], i32),
         "bp_batch_loopy": ([vp, C.POINTER(BatchOptions), C.POINTER(BatchResult)], i32),
         "bp_batch_network_results": ([vp, vp, vp, vp, vp], i32),
         "bp_unrolled_create": ([C.POINTER(vp), u32, u32, u32, u32, vp, vp, vp, u32, u32, vp], i32),

@@ -459,6 +459,7 @@ def run_batched(a, rank, world):
     prior = torch.from_numpy(b.pack_beliefs()).cuda()
     b.set_beliefs(prior)
     tuned = b.autotune(tol=1e-4, max_iterations=200, delta=a.batch_delta)
+    groups = b.groups()
 
     def step():
         b.set_beliefs(prior)
@@ -561,7 +562,7 @@ def run_batched(a, rank, world):
                                    "S in {2,3,4,8}, tol 1e-4 per network, max 200 iterations, seed 2",
                        "delta": a.batch_delta + (" (the reference's serial fp32 stopping rule, decided by bounds)"
                                                  if a.batch_delta == "serial" else " (deterministic fp64 sum)"),
-                       "nodes": int(sum(n.V for n in nets)), "edges": int(edges), "block_threads": tuned,
+                       "nodes": int(sum(n.V for n in nets)), "edges": int(edges), "block_threads": tuned, "groups": groups,
                        "generator_s": round(gen_s, 1), "l2": "batch working set larger than L2"},
             "converged": int(r["converged"]), "max_iterations_run": int(r["max_executed"]),
             "edge_msg_updates_per_s": updates / (ms / 1e3),

@@ -339,11 +339,23 @@ int bp_batch_set_beliefs(bp_batch *b, const float *beliefs, int memory);
 int bp_batch_get_beliefs(bp_batch *b, float *beliefs, int memory);
 int bp_batch_get_messages(bp_batch *b, float *messages, int memory);
 void bp_batch_default_options(bp_batch_options *o);
-/* times 64/128/256/512 threads per network block for each state-count group
- * on this batch, keeps the fastest (results cached in $BP_AUTOTUNE_CACHE,
- * default ~/.cache/bp_b200_autotune.txt); beliefs and messages are restored */
+/* The networks are grouped by state count; with BP_BATCH_SMALL_NODES=n
+ * (environment, read at create; default 0 = off) the networks of at most n
+ * nodes of a state count form a group of their own, with its own launch
+ * shape, work queue and stream.
+ * bp_batch_autotune times 64/128/256/512 threads per network block, and
+ * blocks in flight, for each group on this batch, keeps the fastest (results
+ * cached in $BP_AUTOTUNE_CACHE, default ~/.cache/bp_b200_autotune.txt);
+ * beliefs and messages are restored */
 int bp_batch_autotune(bp_batch *b, const bp_batch_options *o);
+/* per group (at most *count entries; *count returns the number of groups):
+ * its state count and threads per block (a state count appears once per size
+ * class) */
 int bp_batch_get_block_threads(const bp_batch *b, uint32_t *states, uint32_t *block, uint32_t *count);
+/* per group as above, plus max_nodes: the group's size bound (0 = none, the
+ * group of larger networks) and grid: its blocks in flight */
+int bp_batch_get_groups(const bp_batch *b, uint32_t *states, uint32_t *max_nodes, uint32_t *block, uint32_t *grid,
+                        uint32_t *count);
 /* the whole batch: one CUDA graph launch */
 int bp_batch_loopy(bp_batch *b, const bp_batch_options *o, bp_batch_result *r);
 int bp_batch_network_results(bp_batch *b, uint32_t *iterations, uint32_t *executed, int32_t *converged,

@@ -62,8 +62,12 @@ def test_batch_autotune_and_rerun(bp, small_batch, tmp_path, monkeypatch):
     try:
         b.set_beliefs()
         tuned = b.autotune(tol=1e-4, max_iterations=120)
-        assert set(tuned) == {n.uniform_states for n in small_batch}
+        assert {int(k.split(",")[0][2:]) for k in tuned} == {n.uniform_states for n in small_batch}
         assert all(v in (64, 128, 256, 512) for v in tuned.values())
+        groups = b.groups()
+        assert len(groups) == len(tuned)
+        for g in groups:
+            assert g["max_nodes"] == 0 and g["grid"] >= 1
         assert (tmp_path / "tune.txt").exists()
         b.loopy(tol=1e-4, max_iterations=120)
         first = b.beliefs().copy()
@@ -81,3 +85,36 @@ def test_batch_mixed_state_network_rejected(bp, synth):
     net = synth.random_tree(50, (2, 3), 0.0, seed=1)
     with pytest.raises(ValueError):
         BPBatch([net])
+
+
+def test_batch_size_classes_change_no_result(bp, small_batch, monkeypatch):
+    """With BP_BATCH_SMALL_NODES set, networks of at most that many nodes get
+    launch groups of their own; with the reference's serial delta every network's beliefs,
+    messages, iteration index and delta are the same with one group per
+    state count (BP_BATCH_SMALL_NODES=0) as with the split."""
+    from belief_propagation_b200.engine import BPBatch
+    out = []
+    for small in ("0", "256"):
+        monkeypatch.setenv("BP_BATCH_SMALL_NODES", small)
+        b = BPBatch(small_batch)
+        try:
+            groups = b.groups()
+            states = {n.uniform_states for n in small_batch}
+            if small == "0":
+                assert len(groups) == len(states) and all(g["max_nodes"] == 0 for g in groups)
+            else:
+                want = {(n.uniform_states, 256 if n.V <= 256 else 0) for n in small_batch}
+                assert {(g["states"], g["max_nodes"]) for g in groups} == want
+            b.set_beliefs()
+            b.loopy(tol=1e-4, max_iterations=120, delta="serial")
+            r = b.results()
+            out.append((b.beliefs().copy(), [b.messages(k).copy() for k in range(len(small_batch))],
+                        r["iterations"].copy(), r["delta"].copy()))
+        finally:
+            b.close()
+    (b0, m0, i0, d0), (b1, m1, i1, d1) = out
+    np.testing.assert_array_equal(b0, b1)
+    np.testing.assert_array_equal(i0, i1)
+    np.testing.assert_array_equal(d0, d1)
+    for x, y in zip(m0, m1):
+        np.testing.assert_array_equal(x, y)
